@@ -1,0 +1,210 @@
+/*
+ * orsp.h — C ABI of the B200-native PathFinder search library (liborsp.so).
+ *
+ * The library replaces the hot path of OrthoRoute's Manhattan PathFinder:
+ * per-net single-source shortest path on the lattice CSR, edge-cost update,
+ * ROI extraction, predecessor backtrace, path -> edge mapping, overuse count
+ * and history update.  Each entry point names the reference function it
+ * replaces (paths are relative to the OrthoRoute project root;
+ * UPF = orthoroute/algorithms/manhattan/unified_pathfinder.py,
+ * CD  = orthoroute/algorithms/manhattan/pathfinder/cuda_dijkstra.py).
+ *
+ * Conventions
+ *  - Plain C types only.  Pointers with the suffix `_d` are CUDA device
+ *    pointers on the device the graph was created on; `_h` are host pointers.
+ *  - `stream` is a cudaStream_t passed as uintptr_t (0 = legacy default stream).
+ *  - Every call returns an int status: ORSP_OK (0), ORSP_NO_PATH (1, not an
+ *    error: the reference returns None), or a negative error code.
+ *    orsp_last_error() returns a thread-local message for the last failure.
+ *  - Distances are IEEE fp32 computed with round-to-nearest additions
+ *    d[v] = min_u fl32(d[u] + w(u,v)); the fixpoint is unique, so results are
+ *    bit-identical to a sequential fp32 Dijkstra.  Costs must be >= 0
+ *    (+inf = blocked edge; NaN edges are never relaxed).
+ *  - Path tie-break: among predecessors u with fl32(d[u] + w(u,v)) == d[v]
+ *    and (d[u], rank(u)) < (d[v], rank(v)), the parent is the one with the
+ *    smallest (d[u], rank(u)), where rank is the ROI index (the position in
+ *    roi_nodes, i.e. global_to_roi[u]) or the global node id for full-graph
+ *    searches.  This is the order in which the reference heap Dijkstra
+ *    (UPF:1846-1878) settles nodes and keeps the first strictly better parent.
+ */
+#ifndef ORSP_H
+#define ORSP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define ORSP_API __attribute__((visibility("default")))
+#else
+#define ORSP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define ORSP_OK 0
+#define ORSP_NO_PATH 1          /* search finished, destination unreachable  */
+#define ORSP_ERR_ARG (-1)       /* invalid argument (checked on the host)    */
+#define ORSP_ERR_CUDA (-2)      /* a CUDA runtime call failed                */
+#define ORSP_ERR_TIMEOUT (-3)   /* device round / wait limit reached         */
+#define ORSP_ERR_OVERFLOW (-4)  /* a work queue or path buffer was too small */
+#define ORSP_ERR_NOMEM (-5)     /* device allocation failed                  */
+#define ORSP_ERR_INTERNAL (-6)  /* invariant broken (e.g. no predecessor)    */
+
+/* Version of this ABI; bumped on any signature change. */
+#define ORSP_ABI_VERSION 1
+ORSP_API int orsp_abi_version(void);
+ORSP_API const char *orsp_status_string(int status);
+ORSP_API const char *orsp_last_error(void);
+
+/* Profiling hook: when enabled, the search kernel of orsp_sssp (the
+ * persistent grid launch alone, without its init kernels) is bracketed by CUDA
+ * events on the caller's stream; orsp_profile_last returns the duration of
+ * the most recent one in milliseconds.  No counterpart in the reference. */
+ORSP_API int orsp_profile_enable(int on);
+ORSP_API int orsp_profile_last(float *kernel_ms);
+
+/* ---- graph ------------------------------------------------------------- */
+typedef struct orsp_graph orsp_graph;
+
+/* Uploads the CSR (host arrays) to `device` and builds the device-side
+ * transposed CSR used by the backtrace.  Replaces the graph ownership of
+ * CUDADijkstra.__init__ (CD:110-121) and CSRGraph (UPF:647-792).
+ * Nx, Ny, Nz describe the lattice (node = z*Nx*Ny + y*Nx + x, as
+ * KiCadGeometry.node_index, pathfinder/kicad_geometry.py:63-66); pass
+ * 0,0,0 for a graph that is not a lattice (bbox searches are then refused). */
+ORSP_API int orsp_graph_create(int32_t num_nodes, int64_t num_edges,
+                      const int32_t *indptr_h, const int32_t *indices_h,
+                      int32_t nx, int32_t ny, int32_t nz, int device,
+                      orsp_graph **out);
+ORSP_API int orsp_graph_destroy(orsp_graph *g);
+/* Device pointers of the uploaded CSR (indptr[N+1], indices[E]). */
+ORSP_API int orsp_graph_csr(orsp_graph *g, const int32_t **indptr_d,
+                   const int32_t **indices_d);
+/* Largest out-degree (known after create). */
+ORSP_API int orsp_graph_max_degree(orsp_graph *g, int32_t *out);
+
+/* ---- single search ----------------------------------------------------- */
+/* Single-source (or multi-seed) shortest path over the whole graph or over
+ * the ROI given by roi_map_d (global_to_roi, int32[N], -1 = outside), as one
+ * persistent cooperative launch (near-far delta-stepping with a bounded grid
+ * barrier).  Replaces SimpleDijkstra.find_path_roi (UPF:1801-1887) and
+ * CUDADijkstra.find_path_roi_gpu (CD:4909-4996).
+ *   seeds_d[nseeds]       start nodes (global ids); seed_cost_d may be NULL
+ *                          (all seeds start at 0.0) or give fp32 start costs.
+ *   dst                    target node, or -1 for a full search (no path).
+ *   delta                  near-far bucket width (> 0).
+ *   dist_out_d             optional fp32[N]; receives distances (nodes not
+ *                          settled before an early exit hold upper bounds).
+ *   path_out_d/path_cap    receives the node path seed..dst (global ids).
+ *   path_len_h             receives the path length (0 when no path).
+ *   rounds_h               optional: device rounds executed (for tuning).  */
+ORSP_API int orsp_sssp(orsp_graph *g, const float *cost_d, int32_t nseeds,
+              const int32_t *seeds_d, const float *seed_cost_d, int32_t dst,
+              const int32_t *roi_map_d, float delta, float *dist_out_d,
+              int32_t *path_out_d, int32_t path_cap, int32_t *path_len_h,
+              int32_t *rounds_h, uintptr_t stream);
+
+/* ---- batched searches (one launch, one CTA per search) ----------------- */
+/* K independent searches on shared fp32 costs, each inside an axis-aligned
+ * box ROI (inclusive bounds x0,x1,y0,y1,z0,z1 per search in bbox_d[6*K]).
+ * One persistent launch; each CTA runs a block-local near-far search per
+ * work item, backtraces it and maps the path to CSR edges.
+ * Replaces CUDADijkstra.find_paths_on_rois (CD:2014-2086) for box ROIs and
+ * the per-net loop body of _route_all (UPF:4475-4800) under fixed costs.
+ *   order_d               optional int32[K] processing order (e.g. largest
+ *                          box first); NULL = 0..K-1.
+ *   path_nodes_d/edges_d  int32[K*path_cap] outputs (edges_d may be NULL).
+ *   path_len_d            int32[K]: path length, 0 = no path, <0 = error. */
+ORSP_API int orsp_sssp_batch_bbox(orsp_graph *g, const float *cost_d, int32_t K,
+                         const int32_t *src_d, const int32_t *dst_d,
+                         const int32_t *bbox_d, const int32_t *order_d,
+                         float delta, int32_t *path_nodes_d,
+                         int32_t *path_edges_d, int32_t path_cap,
+                         int32_t *path_len_d, uintptr_t stream);
+
+/* ---- ROI extraction ---------------------------------------------------- */
+/* Bidirectional level-synchronous BFS ROI, as ROIExtractor.extract_roi_bfs
+ * (UPF:1636-1734): waves from src (mark 1) and dst (mark 2) alternate, a node
+ * reached by the other wave is marked 3 and ends the expansion; depth is
+ * limited to max_depth and the expansion stops early once more than
+ * 1.5*max_nodes nodes are marked.  The ROI is the marked nodes in ascending
+ * order, truncated to max_nodes with src/dst moved to the front exactly as
+ * the reference does.  roi_nodes_d needs room for N entries; g2r_d (int32[N],
+ * may be NULL) receives global_to_roi. */
+ORSP_API int orsp_roi_bfs(orsp_graph *g, int32_t src, int32_t dst, int32_t max_depth,
+                 int32_t max_nodes, int32_t *roi_nodes_d, int32_t *g2r_d,
+                 int32_t *roi_count_h, uintptr_t stream);
+
+/* global_to_roi (int32[N]) of an inclusive box [x0,x1,y0,y1,z0,z1] (host
+ * array box_h[6]): -1 outside, row-major local id inside.  The box ROI of the
+ * benchmark router (bounding box of the pins plus a margin), in the
+ * global_to_roi format that SimpleDijkstra.find_path_roi (UPF:1801) takes. */
+ORSP_API int orsp_roi_box_map(orsp_graph *g, const int32_t *box_h, int32_t *g2r_d,
+                     uintptr_t stream);
+
+/* ---- path -> edges ----------------------------------------------------- */
+/* For consecutive (u, v) of a node path, the first CSR edge u->v, as
+ * PathFinderRouter._path_to_edges (UPF:5463-5476).  Pairs without an edge are
+ * skipped like the reference does; edge_count_h receives the count. */
+ORSP_API int orsp_path_to_edges(orsp_graph *g, const int32_t *path_d, int32_t len,
+                       int32_t *edges_out_d, int32_t *edge_count_h,
+                       uintptr_t stream);
+
+/* ---- edge accounting (EdgeAccountant, UPF:799-1068) -------------------- */
+/* total = ((base*via_mult)*base_w)*bias + (pres_fac*inv_bias)*over
+ *         + hist_w*history [+ fmodf((float)e, 9973)*1e-6]
+ * with over = max(0, present_ema - cap), bias = layer_bias[edge_layer[e]] on
+ * planar edges (1 on vias) and inv_bias = 1/max(bias, 0.5); every operation
+ * rounds to fp32 in the numpy order of EdgeAccountant.update_costs
+ * (UPF:973-1043).  layer_bias_d/edge_layer_d/edge_kind_d may all be NULL
+ * (no layer bias, as when the reference passes None). */
+ORSP_API int orsp_update_costs(int64_t E, const float *base_d, const float *present_ema_d,
+                      const float *cap_d, const float *history_d,
+                      const uint8_t *edge_layer_d, const uint8_t *edge_kind_d,
+                      const float *layer_bias_d, float pres_fac, float hist_w,
+                      float via_mult, float base_w, int add_jitter,
+                      float *total_out_d, uintptr_t stream);
+
+/* ema = beta*present + (1-beta)*ema  (EdgeAccountant.update_present_ema,
+ * UPF:963-971); one_minus_beta is passed rounded as the caller computes it. */
+ORSP_API int orsp_update_present_ema(int64_t E, const float *present_d, float *ema_d,
+                            float beta, float one_minus_beta, uintptr_t stream);
+
+/* history = history*decay + min(gain*max(0, present - cap), cap_mult*base)
+ * (EdgeAccountant.update_history, UPF:898-961; base_d NULL = no clamp). */
+ORSP_API int orsp_update_history(int64_t E, float *history_d, const float *present_d,
+                        const float *cap_d, const float *base_d, float gain,
+                        float cap_mult, float decay, uintptr_t stream);
+
+/* (sum of max(0, present - cap), count of edges with present > cap), as
+ * EdgeAccountant.compute_overuse (UPF:838-876) without the via terms.  The
+ * sum is accumulated in fp64 and truncated like int(); out2_d is
+ * int64[2] on the device; out2_h (optional) receives a synchronous copy. */
+ORSP_API int orsp_overuse(int64_t E, const float *present_d, const float *cap_d,
+                 int64_t *out2_d, int64_t *out2_h, uintptr_t stream);
+
+/* present[e] = (float)usage[e] (refresh_from_canonical, UPF:814-819). */
+ORSP_API int orsp_present_from_usage(int64_t E, const int32_t *usage_d,
+                            float *present_d, uintptr_t stream);
+
+/* usage[edges[i]] += sign for i < n (EdgeAccountant.commit_path /
+ * clear_path, UPF:821-836).  present_d (optional) is kept in sync the way the
+ * reference does it: present += 1 on commit, present = max(0, present - 1) on
+ * clear; the usage count never drops below 0. */
+ORSP_API int orsp_commit_edges(int64_t n, const int32_t *edges_d, int32_t *usage_d,
+                      float *present_d, int32_t sign, uintptr_t stream);
+
+/* Batched commit of the paths produced by orsp_sssp_batch_bbox (path_len[k]
+ * nodes give path_len[k]-1 edges; entries with path_len < 2 are skipped). */
+ORSP_API int orsp_commit_batch(int32_t K, const int32_t *path_edges_d,
+                      const int32_t *path_len_d, int32_t path_cap,
+                      int32_t *usage_d, float *present_d, int32_t sign,
+                      uintptr_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ORSP_H */

@@ -1,0 +1,102 @@
+"""ORACLE - test infrastructure only.
+
+CPU restatement of the plain PathFinder loop that orthoroute_b200.negotiate
+runs on the GPU (steps of PathFinderRouter._pathfinder_negotiation,
+orthoroute/algorithms/manhattan/unified_pathfinder.py:3548-4259, and
+_route_all, UPF:4441-4823): numpy float32 accounting in the reference's
+expression order and the C heap Dijkstra on box ROIs.  Used to check that the
+device loop gives bit-identical per-iteration overuse and final routes.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from . import orsp_oracle as O
+
+
+def route_plain(lat, src, dst, cfg, base_cost=None, history_init=None, max_nets_per_iter=None):
+    """Returns dict(trace=[(over_sum, over_cnt, failed)], paths=[...], usage, converged, seconds)."""
+    from orthoroute_b200.lattice import bbox_with_margin  # pure numpy helper
+
+    t0 = time.perf_counter()
+    src = np.asarray(src, dtype=np.int32)
+    dst = np.asarray(dst, dtype=np.int32)
+    M = len(src)
+    E = lat.E
+    base = (lat.base_cost if base_cost is None else base_cost).astype(np.float32)
+    cap_paths = cfg.path_cap
+    boxes = bbox_with_margin(lat, src, dst, cfg.roi_margin)
+    full_box = np.array([[0, lat.nx - 1, 0, lat.ny - 1, 0, lat.nz - 1]], dtype=np.int32)
+    usage = np.zeros(E, dtype=np.int64)
+    capacity = np.ones(E, dtype=np.float32)
+    present_ema = np.zeros(E, dtype=np.float32)
+    history = np.zeros(E, dtype=np.float32) if history_init is None else history_init.astype(np.float32).copy()
+    net_paths = [np.zeros(0, np.int32) for _ in range(M)]
+    net_edges = [np.zeros(0, np.int32) for _ in range(M)]
+    pres_fac = cfg.pres_fac_init
+    trace = []
+    converged = False
+    for it in range(1, cfg.max_iterations + 1):
+        present = usage.astype(np.float32)
+        if it == 1:
+            present_ema = present.copy()
+        present_ema = O.update_present_ema(present, present_ema, beta=cfg.present_ema_beta)
+        cost = O.update_costs(base, present_ema, capacity, history, pres_fac, cfg.hist_cost_weight,
+                              add_jitter=cfg.add_jitter, via_cost_multiplier=cfg.via_cost_multiplier,
+                              base_cost_weight=cfg.base_cost_weight)
+        if it == 1 or cfg.reroute == "all":
+            idx = np.arange(M)
+        else:
+            over_e = present > capacity
+            idx = np.array([k for k in range(M) if len(net_paths[k]) < 2 or over_e[net_edges[k]].any()],
+                           dtype=np.int64)
+        if idx.size:
+            for k in idx:  # rip up
+                e = net_edges[k]
+                if e.size:
+                    np.subtract.at(usage, e, 1)
+                    np.maximum(usage, 0, out=usage)
+            nodes, lens = O.batch_bbox(lat.indptr, lat.indices, cost, lat.nx, lat.ny, lat.nz, src[idx], dst[idx],
+                                       boxes[idx], cap_paths)
+            if cfg.full_graph_retry:
+                fail = np.nonzero(lens < 2)[0]
+                if fail.size:
+                    n2, l2 = O.batch_bbox(lat.indptr, lat.indices, cost, lat.nx, lat.ny, lat.nz, src[idx][fail],
+                                          dst[idx][fail], np.repeat(full_box, fail.size, axis=0), cap_paths)
+                    nodes[fail] = n2
+                    lens[fail] = l2
+            for j, k in enumerate(idx):
+                L = int(lens[j])
+                if L >= 2:
+                    p = nodes[j, :L].copy()
+                    e = O.path_to_edges(lat.indptr, lat.indices, p)
+                    net_paths[k] = p
+                    net_edges[k] = e
+                    np.add.at(usage, e, 1)
+                else:
+                    net_paths[k] = np.zeros(0, np.int32)
+                    net_edges[k] = np.zeros(0, np.int32)
+        present = usage.astype(np.float32)
+        over_sum, over_cnt = O.compute_overuse(present, capacity)
+        failed = sum(1 for p in net_paths if len(p) < 2)
+        trace.append((over_sum, over_cnt, failed))
+        if over_sum == 0 and failed == 0:
+            converged = True
+            break
+        gain = cfg.hist_gain
+        if cfg.hist_gain_boost and it >= 8 and over_sum > 0:
+            gain = min(1.2, cfg.hist_gain * 1.25)
+        decay = cfg.history_decay if it >= cfg.history_decay_from else 1.0
+        history = O.update_history(history, present, capacity, gain, base_costs=base,
+                                   history_cap_multiplier=cfg.history_cap_multiplier, decay_factor=decay)
+        pres_fac = min(pres_fac * cfg.pres_fac_mult, cfg.pres_fac_max)
+    return {
+        "trace": trace,
+        "paths": net_paths,
+        "usage": usage.astype(np.int32),
+        "converged": converged,
+        "seconds": time.perf_counter() - t0,
+        "history": history,
+    }

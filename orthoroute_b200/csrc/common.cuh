@@ -1,0 +1,171 @@
+// Shared device helpers for liborsp: error plumbing, bounded waits, warp
+// aggregation and the graph context.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "orsp.h"
+
+#define ORSP_INF_BITS 0x7f800000u
+#define ORSP_FULL_MASK 0xffffffffu
+
+// Device-side error codes written into a status word; mapped to ORSP_ERR_*.
+#define DEV_OK 0
+#define DEV_ERR_TIMEOUT 1
+#define DEV_ERR_OVERFLOW 2
+#define DEV_ERR_INTERNAL 3
+#define DEV_ERR_PATH_OVERFLOW 4
+
+namespace orsp {
+
+// Thread-local message of the last failure (orsp_last_error).
+void set_error(const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+int dev_status_to_orsp(int dev);
+
+#define ORSP_CUDA(call)                                   \
+  do {                                                    \
+    cudaError_t _e = (call);                              \
+    if (_e != cudaSuccess) return orsp::cuda_fail(_e, #call); \
+  } while (0)
+
+struct Graph {
+  int device = 0;
+  int32_t N = 0;
+  int64_t E = 0;
+  int32_t nx = 0, ny = 0, nz = 0;
+  int32_t max_degree = 0;
+  int32_t max_in_degree = 0;
+  int num_sms = 0;
+  // forward CSR (device)
+  int32_t *indptr = nullptr;
+  int32_t *indices = nullptr;
+  // transposed CSR: for node v, in-edges k in [rptr[v], rptr[v+1]) come from
+  // rsrc[k] through forward edge reid[k]; sorted by (source, edge id).
+  int32_t *rptr = nullptr;
+  int32_t *rsrc = nullptr;
+  int32_t *reid = nullptr;
+  // single-search workspace (lazily allocated)
+  uint32_t *dist = nullptr;
+  int2 *near_q[2] = {nullptr, nullptr};
+  int2 *far_q[2] = {nullptr, nullptr};
+  int64_t qcap = 0, fcap = 0;
+  void *ctl = nullptr;     // device control block of the grid search
+  void *ctl_h = nullptr;   // pinned host mirror
+  // batched-search workspace (lazily grown)
+  void *batch_ws = nullptr;
+  size_t batch_ws_bytes = 0;
+  void *batch_ctl = nullptr;
+  // misc scratch
+  void *scratch = nullptr;
+  size_t scratch_bytes = 0;
+  void *pinned = nullptr;  // small pinned host buffer for results
+};
+
+int ensure_scratch(Graph *g, size_t bytes);
+
+}  // namespace orsp
+
+struct orsp_graph : public orsp::Graph {};
+
+// ---------------------------------------------------------------------------
+// device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long dev_globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned ld_cg_u32(const unsigned *p) { return __ldcg(p); }
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Grid-wide barrier for cooperative launches with a bounded wait: a block that
+// waits longer than timeout_ns records DEV_ERR_TIMEOUT and stops waiting, so a
+// logic error can never hang the GPU.  Every block must call it the same
+// number of times (the callers make all loop decisions from values read after
+// the barrier, which no block modifies until the next barrier).
+struct GridBarrier {
+  unsigned count;
+  unsigned gen;
+};
+
+__device__ __forceinline__ void grid_barrier(GridBarrier *b, unsigned nblocks,
+                                             int *err,
+                                             unsigned long long timeout_ns) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned g = ld_acquire_u32(&b->gen);
+    __threadfence();
+    unsigned prev = atomicAdd(&b->count, 1u);
+    if (prev == nblocks - 1) {
+      atomicExch(&b->count, 0u);
+      __threadfence();
+      atomicAdd(&b->gen, 1u);
+    } else {
+      unsigned long long t0 = dev_globaltimer();
+      unsigned spins = 0;
+      while (ld_acquire_u32(&b->gen) == g) {
+        if ((++spins & 63u) == 0 && dev_globaltimer() - t0 > timeout_ns) {
+          atomicCAS(err, DEV_OK, DEV_ERR_TIMEOUT);
+          break;
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// Warp-aggregated append of one int2 item per lane with `flag` set; `counter`
+// may live in global or shared memory.  Must be called by all 32 lanes.
+// Items that do not fit below `cap` are dropped (never written) and raise
+// DEV_ERR_OVERFLOW in *err.
+__device__ __forceinline__ void warp_append(int2 *buf, unsigned *counter,
+                                            int64_t cap, bool flag, int2 item,
+                                            int *err) {
+  unsigned m = __ballot_sync(ORSP_FULL_MASK, flag);
+  if (m == 0) return;
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(m) - 1;
+  unsigned base = 0;
+  if (lane == leader) base = atomicAdd(counter, (unsigned)__popc(m));
+  base = __shfl_sync(ORSP_FULL_MASK, base, leader);
+  if (flag) {
+    unsigned idx = base + __popc(m & lanemask_lt());
+    if ((int64_t)idx < cap) {
+      __stcg(&buf[idx], item);
+    } else {
+      atomicCAS(err, DEV_OK, DEV_ERR_OVERFLOW);
+    }
+  }
+}
+
+__device__ __forceinline__ unsigned warp_min_u32(unsigned v) {
+  return __reduce_min_sync(ORSP_FULL_MASK, v);
+}
+
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long t = __shfl_xor_sync(ORSP_FULL_MASK, v, o);
+    v = t < v ? t : v;
+  }
+  return v;
+}
+
+__device__ __forceinline__ float bits_f(unsigned u) { return __uint_as_float(u); }
+__device__ __forceinline__ unsigned f_bits(float f) { return __float_as_uint(f); }

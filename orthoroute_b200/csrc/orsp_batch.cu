@@ -1,0 +1,474 @@
+// Batched box-ROI searches: one persistent launch in which every CTA takes
+// searches from a shared work counter and runs each one as a block-local
+// near-far delta-stepping loop (__syncthreads rounds instead of grid
+// barriers), then backtraces it with one warp and maps the path to CSR edges.
+//
+// Replaces, for box ROIs, the per-net body of PathFinderRouter._route_all
+// (UPF:4475-4800: ROI -> find_path_roi -> _path_to_edges) and the batched
+// CUDADijkstra.find_paths_on_rois (CD:2014-2086).  Costs are read-only for the
+// whole launch, which is what the reference guarantees inside one negotiation
+// iteration (total_cost is computed once per iteration, UPF:3724-3732, and
+// _route_all reads it once, UPF:4459), so every search of the batch returns
+// the path the sequential loop would return for that net.
+//
+// Distances of boxes with at most `smem_nodes` nodes live in shared memory;
+// larger boxes use a per-CTA slot in global memory (L2-resident for the
+// working set).  Searches whose work queues overflow are reported with
+// path_len = -2 and are re-run by the host wrapper with larger queues.
+#include <algorithm>
+#include <climits>
+#include <cstdlib>
+#include <vector>
+
+#include "common.cuh"
+#include "fastdiv.cuh"
+
+namespace {
+
+constexpr int BATCH_THREADS = 512;
+
+// per-search status in path_len (< 0)
+constexpr int ST_ARG = -1;
+constexpr int ST_QUEUE = -2;
+constexpr int ST_PATHCAP = -3;
+constexpr int ST_ROUNDS = -4;
+constexpr int ST_INTERNAL = -5;
+
+struct BatchParams {
+  const int32_t *indptr, *indices, *rptr, *rsrc, *reid;
+  const float *cost;
+  int32_t nx, ny, nz;
+  FastDiv div_nx, div_plane;
+  int32_t K;
+  const int32_t *src, *dst, *bbox, *order;
+  int32_t *path_nodes, *path_edges, *path_len;
+  int32_t path_cap;
+  char *ws;
+  size_t slot_bytes;
+  int64_t qcap;
+  int32_t smem_nodes;
+  float delta;
+  unsigned *work_counter;
+  unsigned long long budget_ns;
+};
+
+struct Box {
+  int32_t x0, y0, z0, W, H, D;
+  FastDiv dw, dwh;
+  int32_t V;
+};
+
+__device__ __forceinline__ bool box_local(const BatchParams &p, const Box &b, int32_t gid,
+                                          int32_t *lid) {
+  const uint32_t z = p.div_plane.div((uint32_t)gid);
+  const uint32_t rem = (uint32_t)gid - z * (uint32_t)(p.nx * p.ny);
+  const uint32_t y = p.div_nx.div(rem);
+  const uint32_t x = rem - y * (uint32_t)p.nx;
+  const int32_t lx = (int32_t)x - b.x0, ly = (int32_t)y - b.y0, lz = (int32_t)z - b.z0;
+  if (lx < 0 || ly < 0 || lz < 0 || lx >= b.W || ly >= b.H || lz >= b.D) return false;
+  *lid = (lz * b.H + ly) * b.W + lx;
+  return true;
+}
+
+__device__ __forceinline__ int32_t box_global(const BatchParams &p, const Box &b, int32_t lid) {
+  const uint32_t lz = b.dwh.div((uint32_t)lid);
+  const uint32_t r = (uint32_t)lid - lz * (uint32_t)(b.W * b.H);
+  const uint32_t ly = b.dw.div(r);
+  const uint32_t lx = r - ly * (uint32_t)b.W;
+  return ((b.z0 + (int32_t)lz) * p.ny + (b.y0 + (int32_t)ly)) * p.nx + (b.x0 + (int32_t)lx);
+}
+
+template <bool SMEM>
+__device__ __forceinline__ uint32_t dist_ld(const uint32_t *d, int32_t i) {
+  if (SMEM) return *(volatile const uint32_t *)&d[i];
+  return __ldcg(&d[i]);
+}
+
+struct BlockCtl {
+  unsigned qcnt[3];
+  unsigned fcnt[4];
+  unsigned fmin[4];
+  int err;
+};
+
+// Block-local near-far search inside one box; same round structure as the
+// grid kernel (rotating counters, far generations), with __syncthreads.
+// Returns with the final distances of every node with d < d[dst] in `dist`.
+template <bool SMEM>
+__device__ void block_search(const BatchParams &p, const Box &b, int32_t src_l, int32_t dst_l,
+                             uint32_t *dist, int2 *nq0, int2 *nq1, int2 *fq0, int2 *fq1,
+                             BlockCtl *c, unsigned long long t_start) {
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const float INF_F = __int_as_float(0x7f800000);
+  int2 *nq[2] = {nq0, nq1};
+  int2 *fq[2] = {fq0, fq1};
+
+  for (int32_t i = threadIdx.x; i < b.V; i += blockDim.x) dist[i] = ORSP_INF_BITS;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 3; ++i) c->qcnt[i] = 0;
+    for (int i = 0; i < 4; ++i) { c->fcnt[i] = 0; c->fmin[i] = ORSP_INF_BITS; }
+    c->err = 0;
+    dist[src_l] = 0u;
+    fq0[0] = make_int2(src_l, 0);
+    c->fcnt[0] = 1;
+    c->fmin[0] = 0u;
+  }
+  __syncthreads();
+  const unsigned max_rounds = 4u * (unsigned)b.V + 1024u;
+  unsigned r = 0, g = 0;
+  float T = 0.0f;
+  for (;;) {
+    const unsigned n_in = min((unsigned)c->qcnt[r % 3], (unsigned)p.qcap);
+    if (n_in > 0) {
+      const int2 *inq = nq[r & 1];
+      int2 *outq = nq[(r + 1) & 1];
+      int2 *farq = fq[g & 1];
+      unsigned *out_cnt = &c->qcnt[(r + 1) % 3];
+      unsigned *far_cnt = &c->fcnt[g % 4];
+      for (unsigned base = warp * 32; base < n_in; base += nwarps * 32) {
+        const unsigned i = base + lane;
+        int beg = 0, end = 0;
+        unsigned dbits = 0;
+        if (i < n_in) {
+          const int2 it = __ldcg(&inq[i]);
+          if (dist_ld<SMEM>(dist, it.x) == (unsigned)it.y) {
+            const int32_t gv = box_global(p, b, it.x);
+            beg = __ldg(&p.indptr[gv]);
+            end = __ldg(&p.indptr[gv + 1]);
+            dbits = (unsigned)it.y;
+          }
+        }
+        const int deg = end - beg;
+        const int maxdeg = __reduce_max_sync(ORSP_FULL_MASK, deg);
+        const float d = bits_f(dbits);
+        unsigned fmin_local = ORSP_INF_BITS;
+        for (int k = 0; k < maxdeg; ++k) {
+          bool pn = false, pf = false;
+          int2 item = make_int2(0, 0);
+          if (k < deg) {
+            const int e = beg + k;
+            const int32_t w = __ldg(&p.indices[e]);
+            int32_t lw;
+            if (box_local(p, b, w, &lw)) {
+              const float nd = __fadd_rn(d, __ldg(&p.cost[e]));
+              if (nd < INF_F) {
+                const unsigned nb = f_bits(nd);
+                if (nb < dist_ld<SMEM>(dist, lw)) {
+                  const unsigned old = atomicMin(&dist[lw], nb);
+                  if (nb < old) {
+                    item = make_int2(lw, (int)nb);
+                    if (nd < T) pn = true; else pf = true;
+                  }
+                }
+              }
+            }
+          }
+          warp_append(outq, out_cnt, p.qcap, pn, item, &c->err);
+          warp_append(farq, far_cnt, p.qcap, pf, item, &c->err);
+          if (pf && (unsigned)item.y < fmin_local) fmin_local = (unsigned)item.y;
+        }
+        const unsigned wm = warp_min_u32(fmin_local);
+        if (lane == 0 && wm != ORSP_INF_BITS) atomicMin(&c->fmin[g % 4], wm);
+      }
+    } else {
+      const unsigned fc = min((unsigned)c->fcnt[g % 4], (unsigned)p.qcap);
+      if (fc == 0) break;
+      if (bits_f(dist_ld<SMEM>(dist, dst_l)) < T) break;
+      const float fm = bits_f(c->fmin[g % 4]);
+      float Tn = __fadd_rn(fm, p.delta);
+      if (!(Tn > fm)) Tn = __uint_as_float(f_bits(fm) + 1u);
+      const int2 *fin = fq[g & 1];
+      int2 *fout = fq[(g + 1) & 1];
+      int2 *outq = nq[(r + 1) & 1];
+      for (unsigned base = warp * 32; base < fc; base += nwarps * 32) {
+        const unsigned i = base + lane;
+        bool pn = false, pf = false;
+        int2 it = make_int2(0, 0);
+        if (i < fc) {
+          it = __ldcg(&fin[i]);
+          if (dist_ld<SMEM>(dist, it.x) == (unsigned)it.y) {
+            if (bits_f((unsigned)it.y) < Tn) pn = true; else pf = true;
+          }
+        }
+        warp_append(outq, &c->qcnt[(r + 1) % 3], p.qcap, pn, it, &c->err);
+        warp_append(fout, &c->fcnt[(g + 1) % 4], p.qcap, pf, it, &c->err);
+        const unsigned wm = warp_min_u32(pf ? (unsigned)it.y : ORSP_INF_BITS);
+        if (lane == 0 && wm != ORSP_INF_BITS) atomicMin(&c->fmin[(g + 1) % 4], wm);
+      }
+      if (threadIdx.x == 0) {
+        c->fcnt[(g + 2) % 4] = 0;
+        c->fmin[(g + 2) % 4] = ORSP_INF_BITS;
+      }
+      T = Tn;
+      ++g;
+    }
+    if (threadIdx.x == 0) {
+      c->qcnt[(r + 2) % 3] = 0;
+      if (r + 1 >= max_rounds || dev_globaltimer() - t_start > p.budget_ns)
+        atomicCAS(&c->err, DEV_OK, DEV_ERR_TIMEOUT);
+    }
+    __syncthreads();
+    if (c->err) break;
+    ++r;
+  }
+  __syncthreads();
+}
+
+// One warp: parent walk with the settle-order tie-break, fused with the
+// first-CSR-edge lookup of _path_to_edges.  Output in src -> dst order.
+template <bool SMEM>
+__device__ int block_backtrace(const BatchParams &p, const Box &b, int32_t src, int32_t dst,
+                               int32_t dst_l, const uint32_t *dist, int32_t *nodes,
+                               int32_t *edges) {
+  const int lane = threadIdx.x & 31;
+  unsigned dv = dist_ld<SMEM>(dist, dst_l);
+  if (dv == ORSP_INF_BITS) return 0;
+  int32_t v = dst, lv = dst_l;
+  int len = 0;
+  for (;;) {
+    if (len >= p.path_cap) return ST_PATHCAP;
+    if (lane == 0) nodes[len] = v;
+    ++len;
+    if (v == src) break;
+    const int kb = __ldg(&p.rptr[v]), ke = __ldg(&p.rptr[v + 1]);
+    unsigned long long best = ULLONG_MAX;
+    int32_t bu = -1;
+    for (int k0 = kb; k0 < ke; k0 += 32) {
+      const int k = k0 + lane;
+      if (k < ke) {
+        const int32_t u = __ldg(&p.rsrc[k]);
+        int32_t lu;
+        if (box_local(p, b, u, &lu)) {
+          const unsigned du = dist_ld<SMEM>(dist, lu);
+          if (du != ORSP_INF_BITS) {
+            const float s = __fadd_rn(bits_f(du), __ldg(&p.cost[__ldg(&p.reid[k])]));
+            if (f_bits(s) == dv && (du < dv || (du == dv && lu < lv))) {
+              const unsigned long long key = ((unsigned long long)du << 32) | (unsigned)lu;
+              if (key < best) { best = key; bu = u; }
+            }
+          }
+        }
+      }
+    }
+    const unsigned long long wbest = warp_min_u64(best);
+    if (wbest == ULLONG_MAX) return ST_INTERNAL;
+    const unsigned owner = __ballot_sync(ORSP_FULL_MASK, best == wbest && bu >= 0);
+    const int32_t u = __shfl_sync(ORSP_FULL_MASK, bu, __ffs(owner) - 1);
+    // first CSR edge u -> v: the smallest forward edge id among in-edges from u
+    int32_t emin = INT_MAX;
+    for (int k0 = kb; k0 < ke; k0 += 32) {
+      const int k = k0 + lane;
+      if (k < ke && __ldg(&p.rsrc[k]) == u) emin = min(emin, __ldg(&p.reid[k]));
+    }
+    emin = __reduce_min_sync(ORSP_FULL_MASK, emin);
+    if (edges && lane == 0 && len - 1 < p.path_cap) edges[len - 1] = emin;
+    v = u;
+    lv = (int32_t)(wbest & 0xffffffffu);
+    dv = (unsigned)(wbest >> 32);
+  }
+  __syncwarp();
+  for (int i = lane; i < len / 2; i += 32) {
+    const int32_t a = nodes[i], z = nodes[len - 1 - i];
+    nodes[i] = z;
+    nodes[len - 1 - i] = a;
+  }
+  if (edges) {
+    const int ne = len - 1;
+    for (int i = lane; i < ne / 2; i += 32) {
+      const int32_t a = edges[i], z = edges[ne - 1 - i];
+      edges[i] = z;
+      edges[ne - 1 - i] = a;
+    }
+  }
+  __syncwarp();
+  return len;
+}
+
+__global__ void __launch_bounds__(BATCH_THREADS) batch_bbox_kernel(BatchParams p) {
+  extern __shared__ uint32_t s_dist[];
+  __shared__ BlockCtl ctl;
+  __shared__ int s_item;
+  const unsigned long long t_start = dev_globaltimer();
+  char *slot = p.ws + (size_t)blockIdx.x * p.slot_bytes;
+  int2 *q = (int2 *)slot;
+  int2 *nq0 = q, *nq1 = q + p.qcap, *fq0 = q + 2 * p.qcap, *fq1 = q + 3 * p.qcap;
+  uint32_t *gdist = (uint32_t *)(slot + (size_t)4 * p.qcap * sizeof(int2));
+  for (;;) {
+    if (threadIdx.x == 0) s_item = (int)atomicAdd(p.work_counter, 1u);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();
+    if (it >= p.K) break;
+    const int k = p.order ? p.order[it] : it;
+    const int32_t *bb = p.bbox + 6 * (int64_t)k;
+    Box b;
+    b.x0 = bb[0];
+    b.y0 = bb[2];
+    b.z0 = bb[4];
+    b.W = bb[1] - bb[0] + 1;
+    b.H = bb[3] - bb[2] + 1;
+    b.D = bb[5] - bb[4] + 1;
+    b.V = b.W * b.H * b.D;
+    b.dw.init((uint32_t)b.W);
+    b.dwh.init((uint32_t)(b.W * b.H));
+    const int32_t src = p.src[k], dst = p.dst[k];
+    int32_t src_l = -1, dst_l = -1;
+    int32_t *nodes = p.path_nodes + (int64_t)k * p.path_cap;
+    int32_t *edges = p.path_edges ? p.path_edges + (int64_t)k * p.path_cap : nullptr;
+    const bool ok = src >= 0 && dst >= 0 && box_local(p, b, src, &src_l) &&
+                    box_local(p, b, dst, &dst_l);
+    if (!ok) {
+      if (threadIdx.x == 0) p.path_len[k] = ST_ARG;
+      continue;
+    }
+    const bool use_smem = b.V <= p.smem_nodes;
+    uint32_t *dist = use_smem ? s_dist : gdist;
+    if (use_smem)
+      block_search<true>(p, b, src_l, dst_l, dist, nq0, nq1, fq0, fq1, &ctl, t_start);
+    else
+      block_search<false>(p, b, src_l, dst_l, dist, nq0, nq1, fq0, fq1, &ctl, t_start);
+    int status;
+    if (ctl.err == DEV_ERR_OVERFLOW) status = ST_QUEUE;
+    else if (ctl.err) status = ST_ROUNDS;
+    else status = 0;
+    if (threadIdx.x < 32) {
+      int len = status;
+      if (status == 0) {
+        len = use_smem ? block_backtrace<true>(p, b, src, dst, dst_l, dist, nodes, edges)
+                       : block_backtrace<false>(p, b, src, dst, dst_l, dist, nodes, edges);
+      }
+      if (threadIdx.x == 0) p.path_len[k] = len;
+    }
+    __syncthreads();
+  }
+}
+
+int env_int(const char *name, int dflt) {
+  const char *s = getenv(name);
+  if (!s || !*s) return dflt;
+  return atoi(s);
+}
+
+}  // namespace
+
+using namespace orsp;
+
+extern "C" int orsp_sssp_batch_bbox(orsp_graph *g, const float *cost_d, int32_t K,
+                                    const int32_t *src_d, const int32_t *dst_d,
+                                    const int32_t *bbox_d, const int32_t *order_d,
+                                    float delta, int32_t *path_nodes_d,
+                                    int32_t *path_edges_d, int32_t path_cap,
+                                    int32_t *path_len_d, uintptr_t stream) {
+  if (!g || !cost_d || K < 0 || (K > 0 && (!src_d || !dst_d || !bbox_d || !path_nodes_d ||
+                                           !path_len_d)) || path_cap <= 0) {
+    set_error("batch_bbox: NULL argument or path_cap <= 0");
+    return ORSP_ERR_ARG;
+  }
+  if (g->nx <= 0) { set_error("batch_bbox: graph was created without lattice dims"); return ORSP_ERR_ARG; }
+  if (!(delta > 0.0f) || !(delta < 3.0e38f)) { set_error("delta must be finite and > 0"); return ORSP_ERR_ARG; }
+  if (K == 0) return ORSP_OK;
+  ORSP_CUDA(cudaSetDevice(g->device));
+  cudaStream_t st = (cudaStream_t)stream;
+
+  // Box volumes are needed on the host to size the per-CTA slots.
+  std::vector<int32_t> bb((size_t)6 * K);
+  ORSP_CUDA(cudaMemcpyAsync(bb.data(), bbox_d, bb.size() * 4, cudaMemcpyDeviceToHost, st));
+  ORSP_CUDA(cudaStreamSynchronize(st));
+  int64_t vmax = 1;
+  for (int32_t k = 0; k < K; ++k) {
+    const int32_t *b = &bb[(size_t)6 * k];
+    if (b[0] < 0 || b[2] < 0 || b[4] < 0 || b[1] >= g->nx || b[3] >= g->ny || b[5] >= g->nz ||
+        b[1] < b[0] || b[3] < b[2] || b[5] < b[4]) {
+      set_error("batch_bbox: box outside the lattice or empty");
+      return ORSP_ERR_ARG;
+    }
+    const int64_t v = (int64_t)(b[1] - b[0] + 1) * (b[3] - b[2] + 1) * (b[5] - b[4] + 1);
+    vmax = std::max(vmax, v);
+  }
+
+  const int ctas_per_sm = std::max(1, env_int("ORSP_BATCH_CTAS_PER_SM", 2));
+  const int smem_nodes = std::max(0, env_int("ORSP_BATCH_SMEM_NODES", 24 * 1024));
+  const size_t smem_bytes = (size_t)smem_nodes * 4;
+  ORSP_CUDA(cudaFuncSetAttribute(batch_bbox_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem_bytes));
+  const size_t ws_budget = (size_t)std::max(1, env_int("ORSP_BATCH_WS_MB", 16384)) << 20;
+
+  // Queue capacity: start at 2 items per node (plenty for lattice wavefronts),
+  // grow to the worst case (one item per directed edge) for re-runs.
+  int64_t qcap = 2 * vmax + 4096;
+  const int64_t qcap_max = (int64_t)std::max(1, g->max_degree) * vmax + 4096;
+  std::vector<int32_t> retry;
+  BatchParams p{};
+  p.indptr = g->indptr;
+  p.indices = g->indices;
+  p.rptr = g->rptr;
+  p.rsrc = g->rsrc;
+  p.reid = g->reid;
+  p.cost = cost_d;
+  p.nx = g->nx;
+  p.ny = g->ny;
+  p.nz = g->nz;
+  p.div_nx.init((uint32_t)g->nx);
+  p.div_plane.init((uint32_t)(g->nx * g->ny));
+  p.src = src_d;
+  p.dst = dst_d;
+  p.bbox = bbox_d;
+  p.path_nodes = path_nodes_d;
+  p.path_edges = path_edges_d;
+  p.path_len = path_len_d;
+  p.path_cap = path_cap;
+  p.smem_nodes = smem_nodes;
+  p.delta = delta;
+  p.budget_ns = 60ull * 1000000000ull;
+
+  const int32_t *order = order_d;
+  int32_t n_items = K;
+  int32_t *retry_d = nullptr;
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    const size_t slot_bytes = (((size_t)4 * qcap * sizeof(int2) + (size_t)vmax * 4) + 255) & ~(size_t)255;
+    int nslots = g->num_sms * ctas_per_sm;
+    nslots = (int)std::max<size_t>(1, std::min<size_t>((size_t)nslots, ws_budget / slot_bytes));
+    nslots = std::min<int>(nslots, n_items);
+    const size_t need = slot_bytes * nslots + 256;
+    if (g->batch_ws_bytes < need) {
+      cudaFree(g->batch_ws);
+      g->batch_ws = nullptr;
+      g->batch_ws_bytes = 0;
+      ORSP_CUDA(cudaMalloc(&g->batch_ws, need));
+      g->batch_ws_bytes = need;
+    }
+    if (!g->batch_ctl) ORSP_CUDA(cudaMalloc(&g->batch_ctl, 256));
+    ORSP_CUDA(cudaMemsetAsync(g->batch_ctl, 0, 4, st));
+    p.ws = (char *)g->batch_ws;
+    p.slot_bytes = slot_bytes;
+    p.qcap = qcap;
+    p.work_counter = (unsigned *)g->batch_ctl;
+    p.K = n_items;
+    p.order = order;
+    batch_bbox_kernel<<<nslots, BATCH_THREADS, smem_bytes, st>>>(p);
+    ORSP_CUDA(cudaGetLastError());
+
+    // Collect queue overflows for a re-run with larger queues.
+    std::vector<int32_t> lens(K);
+    ORSP_CUDA(cudaMemcpyAsync(lens.data(), path_len_d, (size_t)K * 4, cudaMemcpyDeviceToHost, st));
+    ORSP_CUDA(cudaStreamSynchronize(st));
+    retry.clear();
+    for (int32_t k = 0; k < K; ++k)
+      if (lens[k] == ST_QUEUE) retry.push_back(k);
+    if (retry.empty() || qcap >= qcap_max) break;
+    qcap = std::min(qcap_max, qcap * 4);
+    if (!retry_d) {
+      int rc = ensure_scratch(g, (size_t)K * 4);
+      if (rc) return rc;
+      retry_d = (int32_t *)g->scratch;
+    }
+    ORSP_CUDA(cudaMemcpyAsync(retry_d, retry.data(), retry.size() * 4, cudaMemcpyHostToDevice, st));
+    order = retry_d;
+    n_items = (int32_t)retry.size();
+  }
+  ORSP_CUDA(cudaStreamSynchronize(st));
+  return ORSP_OK;
+}

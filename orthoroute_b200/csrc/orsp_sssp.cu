@@ -1,0 +1,471 @@
+// Single search over the whole graph (or a global_to_roi ROI): one persistent
+// cooperative launch running near-far delta-stepping, then a one-warp
+// backtrace that applies the reference's settle-order tie-break.
+//
+// Replaces SimpleDijkstra.find_path_roi (UPF:1801-1887),
+// CUDADijkstra.find_path_roi_gpu (CD:4909) and the wavefront loop of
+// _run_near_far (CD:2770-3042).  Unlike the reference wavefront (which adds
+// jitter and stops a fixed number of iterations after the sink is reached,
+// CD:2974-2997), the loop here runs to the exact fp32 fixpoint for every node
+// with d < d[dst]: a near-far phase with threshold T settles every node whose
+// final distance is < T, so the search stops after the first phase that
+// leaves d[dst] < T.
+#include <algorithm>
+#include <climits>
+#include <cstdlib>
+
+#include "common.cuh"
+
+namespace {
+
+struct SsspCtl {
+  GridBarrier bar;
+  int err;
+  unsigned qcnt[3];   // near-queue counts, rotating by round % 3
+  unsigned fcnt[4];   // far-pile counts, rotating by far generation % 4
+  unsigned fmin[4];   // min distance bits pushed into each far generation
+  unsigned rounds;
+  int path_len;
+  int status;         // 0 = ok, 1 = no path
+  int pad;
+};
+
+struct SsspParams {
+  const int32_t *indptr;
+  const int32_t *indices;
+  const float *cost;
+  const int32_t *roi_map;    // global_to_roi or nullptr
+  const uint8_t *sink_mask;  // nodes that are settled but never expanded
+  uint32_t *dist;            // fp32 bits
+  int2 *nq[2];
+  int2 *fq[2];
+  int64_t qcap, fcap;
+  SsspCtl *ctl;
+  int32_t N;
+  int32_t dst;
+  float delta;
+  unsigned max_rounds;
+  unsigned long long wait_ns;
+  unsigned long long budget_ns;
+};
+
+__global__ void fill_u32_kernel(uint32_t *p, int64_t n, uint32_t v) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t s = (int64_t)gridDim.x * blockDim.x;
+  for (; i < n; i += s) p[i] = v;
+}
+
+// Control-block reset and seeding: every valid seed goes into far generation 0,
+// so the first round is a split round that opens the first bucket at
+// min(seed cost) + delta.
+__global__ void seed_kernel(SsspParams p, int32_t nseeds, const int32_t *seeds,
+                            const float *seed_cost) {
+  SsspCtl *c = p.ctl;
+  if (threadIdx.x == 0) {
+    c->bar.count = 0;
+    c->bar.gen = 0;
+    c->err = 0;
+    for (int i = 0; i < 3; ++i) c->qcnt[i] = 0;
+    for (int i = 0; i < 4; ++i) {
+      c->fcnt[i] = 0;
+      c->fmin[i] = ORSP_INF_BITS;
+    }
+    c->rounds = 0;
+    c->path_len = 0;
+    c->status = 0;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nseeds; i += blockDim.x) {
+    int s = seeds[i];
+    if (s < 0 || s >= p.N) continue;
+    if (p.roi_map && p.roi_map[s] < 0) continue;
+    float c0 = seed_cost ? seed_cost[i] : 0.0f;
+    if (!(c0 >= 0.0f) || !(c0 < __int_as_float(0x7f800000))) continue;
+    unsigned b = f_bits(c0);
+    atomicMin(&p.dist[s], b);
+    unsigned slot = atomicAdd(&c->fcnt[0], 1u);
+    if ((int64_t)slot < p.fcap) p.fq[0][slot] = make_int2(s, (int)b);
+    atomicMin(&c->fmin[0], b);
+  }
+}
+
+__global__ void __launch_bounds__(512) sssp_grid_kernel(SsspParams p) {
+  SsspCtl *ctl = p.ctl;
+  const unsigned nblocks = gridDim.x;
+  const int lane = threadIdx.x & 31;
+  const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const bool leader = (blockIdx.x == 0 && threadIdx.x == 0);
+  const unsigned long long t_start = dev_globaltimer();
+  const float INF_F = __int_as_float(0x7f800000);
+
+  unsigned r = 0, g = 0;
+  float T = 0.0f;
+  for (;;) {
+    // ---- decisions: values read here are not modified before the barrier
+    int err = (int)ld_acquire_u32((const unsigned *)&ctl->err);
+    if (err) break;
+    if (r >= p.max_rounds) {
+      if (leader) atomicCAS(&ctl->err, DEV_OK, DEV_ERR_TIMEOUT);
+      break;
+    }
+    unsigned n_in = ld_acquire_u32(&ctl->qcnt[r % 3]);
+    if ((int64_t)n_in > p.qcap) n_in = (unsigned)p.qcap;
+    if (n_in > 0) {
+      // ---- relaxation round over the near queue
+      const int2 *inq = p.nq[r & 1];
+      int2 *outq = p.nq[(r + 1) & 1];
+      int2 *farq = p.fq[g & 1];
+      unsigned *out_cnt = &ctl->qcnt[(r + 1) % 3];
+      unsigned *far_cnt = &ctl->fcnt[g % 4];
+      unsigned *far_min = &ctl->fmin[g % 4];
+      for (int64_t base = gwarp * 32; base < (int64_t)n_in; base += nwarps * 32) {
+        int64_t i = base + lane;
+        int beg = 0, end = 0;
+        unsigned dbits = 0;
+        if (i < (int64_t)n_in) {
+          int2 it = __ldcg(&inq[i]);
+          if (__ldcg(&p.dist[it.x]) == (unsigned)it.y &&
+              !(p.sink_mask && p.sink_mask[it.x])) {
+            beg = __ldg(&p.indptr[it.x]);
+            end = __ldg(&p.indptr[it.x + 1]);
+            dbits = (unsigned)it.y;
+          }
+        }
+        const int deg = end - beg;
+        const int maxdeg = __reduce_max_sync(ORSP_FULL_MASK, deg);
+        const float d = bits_f(dbits);
+        unsigned fmin_local = ORSP_INF_BITS;
+        for (int k = 0; k < maxdeg; ++k) {
+          bool pn = false, pf = false;
+          int2 item = make_int2(0, 0);
+          if (k < deg) {
+            const int e = beg + k;
+            const int w = __ldg(&p.indices[e]);
+            if (!p.roi_map || __ldg(&p.roi_map[w]) >= 0) {
+              const float nd = __fadd_rn(d, __ldg(&p.cost[e]));
+              if (nd < INF_F) {
+                const unsigned nb = f_bits(nd);
+                if (nb < __ldcg(&p.dist[w])) {
+                  const unsigned old = atomicMin(&p.dist[w], nb);
+                  if (nb < old) {
+                    item = make_int2(w, (int)nb);
+                    if (nd < T) pn = true; else pf = true;
+                  }
+                }
+              }
+            }
+          }
+          warp_append(outq, out_cnt, p.qcap, pn, item, &ctl->err);
+          warp_append(farq, far_cnt, p.fcap, pf, item, &ctl->err);
+          if (pf) fmin_local = fmin_local < item.y ? fmin_local : (unsigned)item.y;
+        }
+        const unsigned wm = warp_min_u32(fmin_local);
+        if (lane == 0 && wm != ORSP_INF_BITS) atomicMin(far_min, wm);
+      }
+    } else {
+      // ---- phase boundary: stop, or open the next bucket from the far pile
+      unsigned fc = ld_acquire_u32(&ctl->fcnt[g % 4]);
+      if ((int64_t)fc > p.fcap) fc = (unsigned)p.fcap;
+      bool done = (fc == 0);
+      if (!done && p.dst >= 0) {
+        const float dd = bits_f(__ldcg(&p.dist[p.dst]));
+        if (dd < T) done = true;
+      }
+      if (done) break;
+      const float fm = bits_f(ld_acquire_u32(&ctl->fmin[g % 4]));
+      float Tn = __fadd_rn(fm, p.delta);
+      if (!(Tn > fm)) Tn = __uint_as_float(f_bits(fm) + 1u);
+      const int2 *fin = p.fq[g & 1];
+      int2 *fout = p.fq[(g + 1) & 1];
+      int2 *outq = p.nq[(r + 1) & 1];
+      unsigned *out_cnt = &ctl->qcnt[(r + 1) % 3];
+      unsigned *fout_cnt = &ctl->fcnt[(g + 1) % 4];
+      unsigned *fout_min = &ctl->fmin[(g + 1) % 4];
+      for (int64_t base = gwarp * 32; base < (int64_t)fc; base += nwarps * 32) {
+        int64_t i = base + lane;
+        bool pn = false, pf = false;
+        int2 it = make_int2(0, 0);
+        if (i < (int64_t)fc) {
+          it = __ldcg(&fin[i]);
+          if (__ldcg(&p.dist[it.x]) == (unsigned)it.y) {
+            if (bits_f((unsigned)it.y) < Tn) pn = true; else pf = true;
+          }
+        }
+        warp_append(outq, out_cnt, p.qcap, pn, it, &ctl->err);
+        warp_append(fout, fout_cnt, p.fcap, pf, it, &ctl->err);
+        const unsigned wm = warp_min_u32(pf ? (unsigned)it.y : ORSP_INF_BITS);
+        if (lane == 0 && wm != ORSP_INF_BITS) atomicMin(fout_min, wm);
+      }
+      if (leader) {
+        ctl->fcnt[(g + 2) % 4] = 0;
+        ctl->fmin[(g + 2) % 4] = ORSP_INF_BITS;
+      }
+      T = Tn;
+      ++g;
+    }
+    if (leader) {
+      ctl->qcnt[(r + 2) % 3] = 0;
+      if (dev_globaltimer() - t_start > p.budget_ns) atomicCAS(&ctl->err, DEV_OK, DEV_ERR_TIMEOUT);
+    }
+    grid_barrier(&ctl->bar, nblocks, &ctl->err, p.wait_ns);
+    ++r;
+  }
+  if (leader) ctl->rounds = r;
+}
+
+struct BacktraceParams {
+  const float *cost;
+  const int32_t *roi_map;
+  const int32_t *rptr, *rsrc, *reid;
+  const uint32_t *dist;
+  const int32_t *seeds;
+  const float *seed_cost;
+  int32_t nseeds;
+  int32_t dst;
+  int32_t *path_out;
+  int32_t path_cap;
+  SsspCtl *ctl;
+};
+
+// One warp walks from dst towards the seeds.  At each node v the parent is the
+// in-neighbour u (inside the ROI) with fl32(d[u] + w(u,v)) == d[v] and the
+// smallest (d[u], rank(u)) that is below (d[v], rank(v)); a seed whose
+// distance still equals its start cost ends the walk.  (d, rank) strictly
+// decreases along the walk, so it always terminates.
+__global__ void backtrace_kernel(BacktraceParams p) {
+  const int lane = threadIdx.x & 31;
+  SsspCtl *ctl = p.ctl;
+  if (ctl->err) return;
+  unsigned dv = p.dist[p.dst];
+  if (dv == ORSP_INF_BITS) {
+    if (lane == 0) { ctl->path_len = 0; ctl->status = 1; }
+    return;
+  }
+  int v = p.dst;
+  int len = 0;
+  int err = 0;
+  for (;;) {
+    if (len >= p.path_cap) { err = DEV_ERR_PATH_OVERFLOW; break; }
+    if (lane == 0) p.path_out[len] = v;
+    ++len;
+    // seed that was never improved: the walk starts here
+    bool is_start = false;
+    for (int i = lane; i < p.nseeds; i += 32) {
+      if (p.seeds[i] == v) {
+        float c0 = p.seed_cost ? p.seed_cost[i] : 0.0f;
+        if (f_bits(c0) == dv) is_start = true;
+      }
+    }
+    if (__any_sync(ORSP_FULL_MASK, is_start)) break;
+    const int rv = p.roi_map ? p.roi_map[v] : v;
+    const int b = p.rptr[v], e = p.rptr[v + 1];
+    unsigned long long best = ULLONG_MAX;
+    int bu = -1;
+    for (int k0 = b; k0 < e; k0 += 32) {
+      const int k = k0 + lane;
+      if (k < e) {
+        const int u = p.rsrc[k];
+        const int ru = p.roi_map ? p.roi_map[u] : u;
+        if (ru >= 0) {
+          const unsigned du = p.dist[u];
+          if (du != ORSP_INF_BITS) {
+            const float s = __fadd_rn(bits_f(du), p.cost[p.reid[k]]);
+            if (f_bits(s) == dv && (du < dv || (du == dv && ru < rv))) {
+              const unsigned long long key = ((unsigned long long)du << 32) | (unsigned)ru;
+              if (key < best) { best = key; bu = u; }
+            }
+          }
+        }
+      }
+    }
+    const unsigned long long wbest = warp_min_u64(best);
+    if (wbest == ULLONG_MAX) { err = DEV_ERR_INTERNAL; break; }
+    const unsigned owner = __ballot_sync(ORSP_FULL_MASK, best == wbest && bu >= 0);
+    v = __shfl_sync(ORSP_FULL_MASK, bu, __ffs(owner) - 1);
+    dv = (unsigned)(wbest >> 32);
+  }
+  __syncwarp();
+  if (err) {
+    if (lane == 0) atomicCAS(&ctl->err, DEV_OK, err);
+    return;
+  }
+  for (int i = lane; i < len / 2; i += 32) {
+    int a = p.path_out[i];
+    int z = p.path_out[len - 1 - i];
+    p.path_out[i] = z;
+    p.path_out[len - 1 - i] = a;
+  }
+  if (lane == 0) { ctl->path_len = len; ctl->status = 0; }
+}
+
+unsigned long long env_u64(const char *name, unsigned long long dflt) {
+  const char *s = getenv(name);
+  if (!s || !*s) return dflt;
+  return strtoull(s, nullptr, 10);
+}
+
+int ensure_single_ws(orsp::Graph *g, bool need_dist) {
+  int64_t cap = g->E + (int64_t)g->N + 64;
+  if (need_dist && !g->dist) ORSP_CUDA(cudaMalloc(&g->dist, (size_t)g->N * 4));
+  if (g->qcap < cap) {
+    for (int i = 0; i < 2; ++i) {
+      cudaFree(g->near_q[i]);
+      cudaFree(g->far_q[i]);
+      g->near_q[i] = g->far_q[i] = nullptr;
+    }
+    g->qcap = g->fcap = 0;
+    for (int i = 0; i < 2; ++i) {
+      ORSP_CUDA(cudaMalloc(&g->near_q[i], (size_t)cap * sizeof(int2)));
+      ORSP_CUDA(cudaMalloc(&g->far_q[i], (size_t)cap * sizeof(int2)));
+    }
+    g->qcap = g->fcap = cap;
+  }
+  if (!g->ctl) ORSP_CUDA(cudaMalloc(&g->ctl, sizeof(SsspCtl)));
+  if (!g->ctl_h) ORSP_CUDA(cudaMallocHost(&g->ctl_h, sizeof(SsspCtl)));
+  return ORSP_OK;
+}
+
+// Optional timing of the search kernel itself (CUDA events on the launching
+// stream), for roofline reporting.
+struct KernelTimer {
+  bool on = false;
+  bool pending = false;
+  cudaEvent_t a = nullptr, b = nullptr;
+  float last_ms = 0.0f;
+};
+KernelTimer g_timer;
+
+}  // namespace
+
+extern "C" int orsp_profile_enable(int on) {
+  if (on && !g_timer.a) {
+    ORSP_CUDA(cudaEventCreate(&g_timer.a));
+    ORSP_CUDA(cudaEventCreate(&g_timer.b));
+  }
+  g_timer.on = on != 0;
+  return ORSP_OK;
+}
+
+extern "C" int orsp_profile_last(float *kernel_ms) {
+  if (!kernel_ms) { orsp::set_error("NULL argument"); return ORSP_ERR_ARG; }
+  if (g_timer.pending) {
+    ORSP_CUDA(cudaEventSynchronize(g_timer.b));
+    ORSP_CUDA(cudaEventElapsedTime(&g_timer.last_ms, g_timer.a, g_timer.b));
+    g_timer.pending = false;
+  }
+  *kernel_ms = g_timer.last_ms;
+  return ORSP_OK;
+}
+
+namespace orsp {
+
+// Shared by orsp_sssp and orsp_sssp_multi: seeds, runs the grid search to the
+// exact fixpoint (dst >= 0: until d[dst] is below the open bucket) and leaves
+// distances in `dist`.
+int run_grid_search(Graph *g, const float *cost_d, int32_t nseeds,
+                    const int32_t *seeds_d, const float *seed_cost_d,
+                    int32_t dst, const int32_t *roi_map_d,
+                    const uint8_t *sink_mask_d, float delta, uint32_t *dist,
+                    cudaStream_t st) {
+  SsspParams p{};
+  p.indptr = g->indptr;
+  p.indices = g->indices;
+  p.cost = cost_d;
+  p.roi_map = roi_map_d;
+  p.sink_mask = sink_mask_d;
+  p.dist = dist;
+  p.nq[0] = g->near_q[0];
+  p.nq[1] = g->near_q[1];
+  p.fq[0] = g->far_q[0];
+  p.fq[1] = g->far_q[1];
+  p.qcap = g->qcap;
+  p.fcap = g->fcap;
+  p.ctl = (SsspCtl *)g->ctl;
+  p.N = g->N;
+  p.dst = dst;
+  p.delta = delta;
+  p.max_rounds = (unsigned)env_u64("ORSP_MAX_ROUNDS", 4ull * g->N + 4096ull);
+  p.wait_ns = env_u64("ORSP_WAIT_NS", 2000000000ull);
+  p.budget_ns = env_u64("ORSP_BUDGET_NS", 20000000000ull);
+
+  fill_u32_kernel<<<std::min<int64_t>(((int64_t)g->N + 255) / 256, 4096), 256, 0, st>>>(
+      dist, g->N, ORSP_INF_BITS);
+  ORSP_CUDA(cudaGetLastError());
+  seed_kernel<<<1, 256, 0, st>>>(p, nseeds, seeds_d, seed_cost_d);
+  ORSP_CUDA(cudaGetLastError());
+
+  static int blocks_per_sm = -1;
+  if (blocks_per_sm < 0) {
+    int occ = 0;
+    ORSP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sssp_grid_kernel, 512, 0));
+    int want = (int)env_u64("ORSP_GRID_BLOCKS_PER_SM", 2);
+    blocks_per_sm = std::max(1, std::min(occ, want));
+  }
+  dim3 grid(g->num_sms * blocks_per_sm), block(512);
+  void *args[] = {&p};
+  if (g_timer.on) ORSP_CUDA(cudaEventRecord(g_timer.a, st));
+  ORSP_CUDA(cudaLaunchCooperativeKernel((void *)sssp_grid_kernel, grid, block, args, 0, st));
+  if (g_timer.on) {
+    ORSP_CUDA(cudaEventRecord(g_timer.b, st));
+    g_timer.pending = true;
+  }
+  return ORSP_OK;
+}
+
+}  // namespace orsp
+
+using namespace orsp;
+
+extern "C" int orsp_sssp(orsp_graph *g, const float *cost_d, int32_t nseeds,
+                         const int32_t *seeds_d, const float *seed_cost_d,
+                         int32_t dst, const int32_t *roi_map_d, float delta,
+                         float *dist_out_d, int32_t *path_out_d, int32_t path_cap,
+                         int32_t *path_len_h, int32_t *rounds_h, uintptr_t stream) {
+  if (!g || !cost_d || nseeds <= 0 || !seeds_d) { set_error("NULL graph/cost/seeds"); return ORSP_ERR_ARG; }
+  if (!(delta > 0.0f) || !(delta < 3.0e38f)) { set_error("delta must be finite and > 0"); return ORSP_ERR_ARG; }
+  if (dst < -1 || dst >= g->N) { set_error("dst out of range"); return ORSP_ERR_ARG; }
+  if (dst >= 0 && (!path_out_d || path_cap <= 0 || !path_len_h)) {
+    set_error("a destination needs path_out_d, path_cap > 0 and path_len_h");
+    return ORSP_ERR_ARG;
+  }
+  ORSP_CUDA(cudaSetDevice(g->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = ensure_single_ws(g, dist_out_d == nullptr);
+  if (rc) return rc;
+  uint32_t *dist = dist_out_d ? (uint32_t *)dist_out_d : g->dist;
+  rc = run_grid_search(g, cost_d, nseeds, seeds_d, seed_cost_d, dst, roi_map_d,
+                       nullptr, delta, dist, st);
+  if (rc) return rc;
+  if (dst >= 0) {
+    BacktraceParams b{};
+    b.cost = cost_d;
+    b.roi_map = roi_map_d;
+    b.rptr = g->rptr;
+    b.rsrc = g->rsrc;
+    b.reid = g->reid;
+    b.dist = dist;
+    b.seeds = seeds_d;
+    b.seed_cost = seed_cost_d;
+    b.nseeds = nseeds;
+    b.dst = dst;
+    b.path_out = path_out_d;
+    b.path_cap = path_cap;
+    b.ctl = (SsspCtl *)g->ctl;
+    backtrace_kernel<<<1, 32, 0, st>>>(b);
+    ORSP_CUDA(cudaGetLastError());
+  }
+  ORSP_CUDA(cudaMemcpyAsync(g->ctl_h, g->ctl, sizeof(SsspCtl), cudaMemcpyDeviceToHost, st));
+  ORSP_CUDA(cudaStreamSynchronize(st));
+  const SsspCtl *c = (const SsspCtl *)g->ctl_h;
+  if (rounds_h) *rounds_h = (int32_t)c->rounds;
+  if (c->err) return dev_status_to_orsp(c->err);
+  if (dst >= 0) {
+    *path_len_h = c->path_len;
+    if (c->status == 1 || c->path_len < 2) {
+      *path_len_h = 0;
+      return ORSP_NO_PATH;
+    }
+  }
+  return ORSP_OK;
+}

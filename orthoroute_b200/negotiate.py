@@ -1,0 +1,272 @@
+"""PathFinder negotiated-congestion routing on the device kernels.
+
+This is the loop of PathFinderRouter._pathfinder_negotiation
+(orthoroute/algorithms/manhattan/unified_pathfinder.py:3548-4259, "UPF") and
+_route_all (UPF:4441-4823) reduced to the plain PathFinder schedule the
+benchmark configurations name, with every array step on the GPU:
+
+  per iteration
+    present <- committed usage                         refresh_from_canonical  UPF:814
+    present_ema <- present (iteration 1), then EMA     update_present_ema      UPF:963, 3648-3654
+    total_cost <- base/present/history formula         update_costs            UPF:973, 3725
+    route the nets (rip up the old path, ROI, SSSP,    _route_all              UPF:4441
+      backtrace, path -> edges, commit)
+    present <- usage; overuse count                    compute_overuse         UPF:838, 3880
+    stop at zero overuse with every net routed         UPF:4023-4027, 4121
+    history update (raw present, cap 15*base,          update_history          UPF:898, 4030-4057
+      decay 0.98 from iteration 10, gain x1.25 <= 1.2 from iteration 8)
+    pres_fac <- min(pres_fac * mult, pres_fac_max)     UPF:4224
+
+Costs are computed once per iteration and are read-only while the nets are
+routed (UPF:4459, "Sequential routing with FIXED costs throughout
+iteration"), so each net's search depends only on that iteration's costs and
+its own ROI.  Two execution modes therefore give identical paths:
+
+* ``mode="sequential"``: one persistent grid search per net (the plain GPU
+  path, a host round trip per net);
+* ``mode="batched"``: every net of the iteration in one launch of the
+  batched box-ROI kernel, then one batched commit.
+
+Heuristics of the reference loop that are not part of plain PathFinder (layer
+bias, via pooling, hotset sampling with random.seed, barrel-conflict
+penalties, stagnation rip-up) are not applied here; the accounting entry
+points for them exist in the library and are exercised by the tests.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, ptr
+from .accounting import DeviceEdgeAccountant
+from .lattice import Lattice, bbox_with_margin
+from .roi import DeviceROIExtractor
+from .solver import DeviceGraph, _stream, as_device
+
+
+@dataclass
+class NegotiationConfig:
+    max_iterations: int = 30
+    pres_fac_init: float = 0.5
+    pres_fac_mult: float = 1.5
+    pres_fac_max: float = 64.0
+    hist_gain: float = 1.0
+    hist_gain_boost: bool = True
+    hist_cost_weight: float = 1.0
+    base_cost_weight: float = 1.0
+    via_cost_multiplier: float = 1.0
+    present_ema_beta: float = 0.4
+    history_cap_multiplier: float = 15.0
+    history_decay: float = 0.98
+    history_decay_from: int = 10
+    add_jitter: bool = True
+    roi: str = "bbox"  # "bbox" | "bfs" | "full"
+    roi_margin: int = 10
+    reroute: str = "all"  # "all" | "offenders"
+    full_graph_retry: bool = True
+    delta: Optional[float] = None
+    path_cap: int = 4096
+
+
+@dataclass
+class IterationStats:
+    iteration: int
+    pres_fac: float
+    routed: int
+    failed: int
+    over_sum: int
+    over_cnt: int
+    nets_searched: int
+    seconds: float
+
+
+@dataclass
+class RouteResult:
+    converged: bool
+    iterations: List[IterationStats]
+    seconds: float
+    paths: List[np.ndarray]
+    edge_usage: np.ndarray
+    wirelength: int
+    vias: int
+    meta: dict = field(default_factory=dict)
+
+    def overuse_trace(self):
+        return [(s.over_sum, s.over_cnt) for s in self.iterations]
+
+
+class PathFinder:
+    def __init__(self, lattice: Lattice, base_cost=None, config: Optional[NegotiationConfig] = None, device=None):
+        self.lat = lattice
+        self.cfg = config or NegotiationConfig()
+        self.dg = DeviceGraph.from_lattice(lattice, device=device)
+        self.device = self.dg.device
+        self.E = lattice.E
+        base = lattice.base_cost if base_cost is None else base_cost
+        self.base = as_device(base, torch.float32, self.device)
+        self.edge_kind = np.asarray(lattice.edge_kind)
+        self.roi = DeviceROIExtractor(self.dg, lattice=lattice, return_device=True)
+
+    # ------------------------------------------------------------------
+    def _offenders(self, acc, net_edges, net_lens, nets_all):
+        over = (acc.present > acc.capacity)
+        cap = net_edges.shape[1]
+        e = net_edges.clamp_min(0).long()
+        valid = torch.arange(cap, device=self.device)[None, :] < (net_lens.long() - 1).clamp_min(0)[:, None]
+        hit = (over[e] & valid).any(dim=1)
+        unrouted = net_lens < 2
+        return torch.nonzero(hit | unrouted).flatten()
+
+    def _route_batched(self, acc, cost, idx, src_d, dst_d, boxes_d, full_box_d, order_rank, net_nodes,
+                       net_edges, net_lens, delta):
+        lib = _lib.load()
+        cap = self.cfg.path_cap
+        K = int(idx.numel())
+        st = _stream()
+        old_e = net_edges[idx].contiguous()
+        old_l = net_lens[idx].contiguous()
+        check(lib.orsp_commit_batch(K, ptr(old_e), ptr(old_l), cap, ptr(acc.usage), ptr(acc.present), -1, st),
+              "orsp_commit_batch")
+        s = src_d[idx].contiguous()
+        t = dst_d[idx].contiguous()
+        b = boxes_d[idx].contiguous()
+        order = torch.argsort(order_rank[idx], stable=True).to(torch.int32)
+        nodes, edges, lens = self.dg.batch_bbox(cost, s, t, b, order=order, delta=delta, path_cap=cap)
+        if self.cfg.full_graph_retry:
+            fail = torch.nonzero(lens < 2).flatten()
+            if fail.numel() > 0:
+                fb = full_box_d.expand(int(fail.numel()), 6).contiguous()
+                n2, e2, l2 = self.dg.batch_bbox(cost, s[fail].contiguous(), t[fail].contiguous(), fb,
+                                                delta=delta, path_cap=cap)
+                nodes[fail] = n2
+                edges[fail] = e2
+                lens[fail] = l2
+        bad = lens < 0
+        if bool(bad.any()):
+            raise _lib.OrspError(int(lens[bad][0]), "orsp_sssp_batch_bbox", "per-search failure status")
+        net_nodes[idx] = nodes
+        net_edges[idx] = edges
+        net_lens[idx] = lens
+        check(lib.orsp_commit_batch(K, ptr(edges), ptr(lens), cap, ptr(acc.usage), ptr(acc.present), 1, st),
+              "orsp_commit_batch")
+
+    def _route_sequential(self, acc, cost, idx, src, dst, boxes, net_nodes, net_edges, net_lens, delta):
+        lib = _lib.load()
+        cap = self.cfg.path_cap
+        st = _stream()
+        lens_h = net_lens.cpu().numpy()
+        for k in idx.cpu().tolist():
+            L = int(lens_h[k])
+            if L >= 2:
+                check(lib.orsp_commit_edges(L - 1, ptr(net_edges[k]), ptr(acc.usage), ptr(acc.present), -1, st),
+                      "orsp_commit_edges")
+            if self.cfg.roi == "bbox":
+                g2r = self.roi.box_map(boxes[k])
+            elif self.cfg.roi == "bfs":
+                _, g2r = self.roi.extract_roi(int(src[k]), int(dst[k]))
+            else:
+                g2r = None
+            status, path, _ = self.dg.sssp(cost, int(src[k]), int(dst[k]), roi_map=g2r, delta=delta, path_cap=cap)
+            if (status != _lib.ORSP_OK or path is None or path.numel() < 2) and self.cfg.full_graph_retry \
+                    and g2r is not None:
+                status, path, _ = self.dg.sssp(cost, int(src[k]), int(dst[k]), roi_map=None, delta=delta,
+                                               path_cap=cap)
+            if status == _lib.ORSP_OK and path is not None and path.numel() >= 2:
+                n = int(path.numel())
+                e = self.dg.path_to_edges(path)
+                net_nodes[k, :n] = path
+                net_edges[k, : n - 1] = e
+                net_lens[k] = n
+                check(lib.orsp_commit_edges(n - 1, ptr(e), ptr(acc.usage), ptr(acc.present), 1, st),
+                      "orsp_commit_edges")
+            else:
+                net_lens[k] = 0
+
+    # ------------------------------------------------------------------
+    def route(self, src, dst, mode: str = "batched", history_init=None, callback=None) -> RouteResult:
+        cfg = self.cfg
+        if mode not in ("batched", "sequential"):
+            raise ValueError("mode must be 'batched' or 'sequential'")
+        if mode == "batched" and cfg.roi != "bbox":
+            raise ValueError("the batched kernel searches box ROIs (roi='bbox')")
+        dev = self.device
+        torch.cuda.synchronize(dev)
+        t_start = time.perf_counter()
+        src = np.ascontiguousarray(src, dtype=np.int32)
+        dst = np.ascontiguousarray(dst, dtype=np.int32)
+        M = len(src)
+        cap = cfg.path_cap
+        boxes = bbox_with_margin(self.lat, src, dst, cfg.roi_margin)
+        vol = (boxes[:, 1] - boxes[:, 0] + 1).astype(np.int64) * (boxes[:, 3] - boxes[:, 2] + 1) * \
+            (boxes[:, 5] - boxes[:, 4] + 1)
+        order_rank = torch.from_numpy(np.argsort(np.argsort(-vol, kind="stable"), kind="stable").astype(np.int64)).to(dev)
+        src_d = torch.from_numpy(src).to(dev)
+        dst_d = torch.from_numpy(dst).to(dev)
+        boxes_d = torch.from_numpy(boxes).to(dev)
+        full_box_d = torch.tensor([[0, self.lat.nx - 1, 0, self.lat.ny - 1, 0, self.lat.nz - 1]], dtype=torch.int32,
+                                  device=dev)
+        net_nodes = torch.zeros((M, cap), dtype=torch.int32, device=dev)
+        net_edges = torch.full((M, cap), -1, dtype=torch.int32, device=dev)
+        net_lens = torch.zeros(M, dtype=torch.int32, device=dev)
+        acc = DeviceEdgeAccountant(self.E, device=dev)
+        if history_init is not None:
+            acc.history.copy_(as_device(history_init, torch.float32, dev))
+        self.acc = acc
+        all_idx = torch.arange(M, device=dev)
+        pres_fac = cfg.pres_fac_init
+        stats: List[IterationStats] = []
+        converged = False
+        for it in range(1, cfg.max_iterations + 1):
+            t_it = time.perf_counter()
+            acc.refresh_from_canonical()
+            if it == 1:
+                acc.present_ema.copy_(acc.present)
+            acc.update_present_ema(beta=cfg.present_ema_beta)
+            acc.update_costs(self.base, pres_fac, cfg.hist_cost_weight, add_jitter=cfg.add_jitter,
+                             via_cost_multiplier=cfg.via_cost_multiplier, base_cost_weight=cfg.base_cost_weight)
+            cost = acc.total_cost
+            delta = cfg.delta if cfg.delta is not None else DeviceGraph.default_delta(cost)
+            if it == 1 or cfg.reroute == "all":
+                idx = all_idx
+            else:
+                idx = self._offenders(acc, net_edges, net_lens, all_idx)
+            if idx.numel() > 0:
+                if mode == "batched":
+                    self._route_batched(acc, cost, idx, src_d, dst_d, boxes_d, full_box_d, order_rank, net_nodes,
+                                        net_edges, net_lens, delta)
+                else:
+                    self._route_sequential(acc, cost, idx, src, dst, boxes, net_nodes, net_edges, net_lens, delta)
+            acc.refresh_from_canonical()
+            over_sum, over_cnt = acc.compute_overuse()
+            failed = int((net_lens < 2).sum().item())
+            stats.append(IterationStats(it, pres_fac, M - failed, failed, over_sum, over_cnt, int(idx.numel()),
+                                        time.perf_counter() - t_it))
+            if callback is not None:
+                callback(stats[-1])
+            if over_sum == 0 and failed == 0:
+                converged = True
+                break
+            gain = cfg.hist_gain
+            if cfg.hist_gain_boost and it >= 8 and over_sum > 0:
+                gain = min(1.2, cfg.hist_gain * 1.25)
+            decay = cfg.history_decay if it >= cfg.history_decay_from else 1.0
+            acc.update_history(gain, base_costs=self.base, history_cap_multiplier=cfg.history_cap_multiplier,
+                               decay_factor=decay, use_raw_present=True)
+            pres_fac = min(pres_fac * cfg.pres_fac_mult, cfg.pres_fac_max)
+        torch.cuda.synchronize(dev)
+        seconds = time.perf_counter() - t_start
+        lens_h = net_lens.cpu().numpy()
+        nodes_h = net_nodes.cpu().numpy()
+        edges_h = net_edges.cpu().numpy()
+        paths = [nodes_h[k, : lens_h[k]].copy() if lens_h[k] >= 2 else np.zeros(0, np.int32) for k in range(M)]
+        all_e = np.concatenate([edges_h[k, : max(lens_h[k] - 1, 0)] for k in range(M)]) if M else np.zeros(0)
+        all_e = all_e.astype(np.int64)
+        vias = int(self.edge_kind[all_e].sum()) if all_e.size else 0
+        wl = int(all_e.size - vias)
+        return RouteResult(converged, stats, seconds, paths, acc.usage.cpu().numpy(), wl, vias,
+                           meta={"mode": mode, "nets": M})
