@@ -102,8 +102,6 @@ __device__ void block_search(const BatchParams &p, const Box &b, int32_t src_l, 
   const int warp = threadIdx.x >> 5;
   const int nwarps = blockDim.x >> 5;
   const float INF_F = __int_as_float(0x7f800000);
-  int2 *nq[2] = {nq0, nq1};
-  int2 *fq[2] = {fq0, fq1};
 
   for (int32_t i = threadIdx.x; i < b.V; i += blockDim.x) dist[i] = ORSP_INF_BITS;
   __syncthreads();
@@ -123,9 +121,9 @@ __device__ void block_search(const BatchParams &p, const Box &b, int32_t src_l, 
   for (;;) {
     const unsigned n_in = min((unsigned)c->qcnt[r % 3], (unsigned)p.qcap);
     if (n_in > 0) {
-      const int2 *inq = nq[r & 1];
-      int2 *outq = nq[(r + 1) & 1];
-      int2 *farq = fq[g & 1];
+      const int2 *inq = ((r & 1) ? nq1 : nq0);
+      int2 *outq = (((r + 1) & 1) ? nq1 : nq0);
+      int2 *farq = ((g & 1) ? fq1 : fq0);
       unsigned *out_cnt = &c->qcnt[(r + 1) % 3];
       unsigned *far_cnt = &c->fcnt[g % 4];
       for (unsigned base = warp * 32; base < n_in; base += nwarps * 32) {
@@ -180,9 +178,9 @@ __device__ void block_search(const BatchParams &p, const Box &b, int32_t src_l, 
       const float fm = bits_f(c->fmin[g % 4]);
       float Tn = __fadd_rn(fm, p.delta);
       if (!(Tn > fm)) Tn = __uint_as_float(f_bits(fm) + 1u);
-      const int2 *fin = fq[g & 1];
-      int2 *fout = fq[(g + 1) & 1];
-      int2 *outq = nq[(r + 1) & 1];
+      const int2 *fin = ((g & 1) ? fq1 : fq0);
+      int2 *fout = (((g + 1) & 1) ? fq1 : fq0);
+      int2 *outq = (((r + 1) & 1) ? nq1 : nq0);
       for (unsigned base = warp * 32; base < fc; base += nwarps * 32) {
         const unsigned i = base + lane;
         bool pn = false, pf = false;
@@ -389,6 +387,13 @@ extern "C" int orsp_sssp_batch_bbox(orsp_graph *g, const float *cost_d, int32_t 
     vmax = std::max(vmax, v);
   }
 
+  if (order_d) {
+    std::vector<int32_t> ord(K);
+    ORSP_CUDA(cudaMemcpyAsync(ord.data(), order_d, (size_t)K * 4, cudaMemcpyDeviceToHost, st));
+    ORSP_CUDA(cudaStreamSynchronize(st));
+    for (int32_t k = 0; k < K; ++k)
+      if (ord[k] < 0 || ord[k] >= K) { set_error("batch_bbox: order entry out of range"); return ORSP_ERR_ARG; }
+  }
   const int ctas_per_sm = std::max(1, env_int("ORSP_BATCH_CTAS_PER_SM", 2));
   const int smem_nodes = std::max(0, env_int("ORSP_BATCH_SMEM_NODES", 24 * 1024));
   const size_t smem_bytes = (size_t)smem_nodes * 4;
@@ -422,7 +427,7 @@ extern "C" int orsp_sssp_batch_bbox(orsp_graph *g, const float *cost_d, int32_t 
   p.path_cap = path_cap;
   p.smem_nodes = smem_nodes;
   p.delta = delta;
-  p.budget_ns = 60ull * 1000000000ull;
+  p.budget_ns = 30ull * 1000000000ull;
 
   const int32_t *order = order_d;
   int32_t n_items = K;

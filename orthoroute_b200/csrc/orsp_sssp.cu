@@ -37,8 +37,8 @@ struct SsspParams {
   const int32_t *roi_map;    // global_to_roi or nullptr
   const uint8_t *sink_mask;  // nodes that are settled but never expanded
   uint32_t *dist;            // fp32 bits
-  int2 *nq[2];
-  int2 *fq[2];
+  int2 *nq0, *nq1;
+  int2 *fq0, *fq1;
   int64_t qcap, fcap;
   SsspCtl *ctl;
   int32_t N;
@@ -84,7 +84,7 @@ __global__ void seed_kernel(SsspParams p, int32_t nseeds, const int32_t *seeds,
     unsigned b = f_bits(c0);
     atomicMin(&p.dist[s], b);
     unsigned slot = atomicAdd(&c->fcnt[0], 1u);
-    if ((int64_t)slot < p.fcap) p.fq[0][slot] = make_int2(s, (int)b);
+    if ((int64_t)slot < p.fcap) p.fq0[slot] = make_int2(s, (int)b);
     atomicMin(&c->fmin[0], b);
   }
 }
@@ -113,9 +113,9 @@ __global__ void __launch_bounds__(512) sssp_grid_kernel(SsspParams p) {
     if ((int64_t)n_in > p.qcap) n_in = (unsigned)p.qcap;
     if (n_in > 0) {
       // ---- relaxation round over the near queue
-      const int2 *inq = p.nq[r & 1];
-      int2 *outq = p.nq[(r + 1) & 1];
-      int2 *farq = p.fq[g & 1];
+      const int2 *inq = ((r & 1) ? p.nq1 : p.nq0);
+      int2 *outq = (((r + 1) & 1) ? p.nq1 : p.nq0);
+      int2 *farq = ((g & 1) ? p.fq1 : p.fq0);
       unsigned *out_cnt = &ctl->qcnt[(r + 1) % 3];
       unsigned *far_cnt = &ctl->fcnt[g % 4];
       unsigned *far_min = &ctl->fmin[g % 4];
@@ -176,9 +176,9 @@ __global__ void __launch_bounds__(512) sssp_grid_kernel(SsspParams p) {
       const float fm = bits_f(ld_acquire_u32(&ctl->fmin[g % 4]));
       float Tn = __fadd_rn(fm, p.delta);
       if (!(Tn > fm)) Tn = __uint_as_float(f_bits(fm) + 1u);
-      const int2 *fin = p.fq[g & 1];
-      int2 *fout = p.fq[(g + 1) & 1];
-      int2 *outq = p.nq[(r + 1) & 1];
+      const int2 *fin = ((g & 1) ? p.fq1 : p.fq0);
+      int2 *fout = (((g + 1) & 1) ? p.fq1 : p.fq0);
+      int2 *outq = (((r + 1) & 1) ? p.nq1 : p.nq0);
       unsigned *out_cnt = &ctl->qcnt[(r + 1) % 3];
       unsigned *fout_cnt = &ctl->fcnt[(g + 1) % 4];
       unsigned *fout_min = &ctl->fmin[(g + 1) % 4];
@@ -375,10 +375,10 @@ int run_grid_search(Graph *g, const float *cost_d, int32_t nseeds,
   p.roi_map = roi_map_d;
   p.sink_mask = sink_mask_d;
   p.dist = dist;
-  p.nq[0] = g->near_q[0];
-  p.nq[1] = g->near_q[1];
-  p.fq[0] = g->far_q[0];
-  p.fq[1] = g->far_q[1];
+  p.nq0 = g->near_q[0];
+  p.nq1 = g->near_q[1];
+  p.fq0 = g->far_q[0];
+  p.fq1 = g->far_q[1];
   p.qcap = g->qcap;
   p.fcap = g->fcap;
   p.ctl = (SsspCtl *)g->ctl;

@@ -219,7 +219,7 @@ def board_footprints(
     ny: int,
     nz: int,
     nets: int,
-    footprints: int,
+    footprints: Optional[int],
     seed: int,
     rows: int = 2,
     cols: int = 50,
@@ -227,10 +227,16 @@ def board_footprints(
 ) -> Board:
     """Nets between connector footprints of rows x cols pins at 1-cell pitch on
     the top layer.  Each net joins two different random footprints; every pin
-    is used by at most one net (so a net endpoint never shares its escape edges
-    with another net)."""
+    is used by at most one net (a pin shared by more nets than its 3 escape
+    edges could never reach zero overuse).  footprints=None picks the smallest
+    count with 10 % spare pins."""
     lat = build_lattice(nx, ny, nz, **lat_kw)
     rng = np.random.default_rng(seed)
+    pins_per = rows * cols
+    if footprints is None:
+        footprints = int(np.ceil(1.1 * 2 * nets / pins_per))
+    if footprints * pins_per < 2 * nets:
+        raise ValueError("not enough pins for the nets")
     # non-overlapping placement with a 2-cell keep-out around each footprint
     occ = np.zeros((ny, nx), dtype=bool)
     origins = []
@@ -245,18 +251,21 @@ def board_footprints(
             continue
         occ[oy - 2 : oy + rows + 2, ox - 2 : ox + cols + 2] = True
         origins.append((ox, oy))
-    pins_per = rows * cols
     free = [list(rng.permutation(pins_per)) for _ in range(footprints)]
+    nfree = np.full(footprints, pins_per, dtype=np.float64)
     src = np.empty(nets, dtype=np.int64)
     dst = np.empty(nets, dtype=np.int64)
     for i in range(nets):
-        for _ in range(1000):
-            a, b = rng.choice(footprints, size=2, replace=False)
-            if free[a] and free[b]:
-                break
-        else:
+        # footprints drawn in proportion to their free pins
+        a = int(rng.choice(footprints, p=nfree / nfree.sum()))
+        w = nfree.copy()
+        w[a] = 0
+        if w.sum() == 0:
             raise RuntimeError("ran out of free pins")
+        b = int(rng.choice(footprints, p=w / w.sum()))
         pa, pb = free[a].pop(), free[b].pop()
+        nfree[a] -= 1
+        nfree[b] -= 1
         ax, ay = origins[a][0] + pa % cols, origins[a][1] + pa // cols
         bx, by = origins[b][0] + pb % cols, origins[b][1] + pb // cols
         src[i] = ay * nx + ax
