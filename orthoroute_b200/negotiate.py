@@ -116,8 +116,9 @@ class PathFinder:
     def _offenders(self, acc, net_edges, net_lens, nets_all):
         over = (acc.present > acc.capacity)
         cap = net_edges.shape[1]
-        e = net_edges.clamp_min(0).long()
+        # only the first len-1 entries of a row are edges of the net's path
         valid = torch.arange(cap, device=self.device)[None, :] < (net_lens.long() - 1).clamp_min(0)[:, None]
+        e = torch.where(valid, net_edges.long(), torch.zeros((), dtype=torch.long, device=self.device))
         hit = (over[e] & valid).any(dim=1)
         unrouted = net_lens < 2
         return torch.nonzero(hit | unrouted).flatten()

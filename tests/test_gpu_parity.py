@@ -179,6 +179,15 @@ def test_batch_bbox_matches_oracle():
     w = uniform_weights(lat, seed=5, blocked_frac=0.03)
     dg = DeviceGraph.from_lattice(lat)
     boxes, src, dst = random_boxes(lat, 300, seed=9, lo=(2, 2, 1), hi=(90, 70, 6))
+    # boxes larger than the shared-memory distance array (24K nodes) take the
+    # global-memory path of the kernel
+    rng = np.random.default_rng(1)
+    big_boxes = np.array([[0, 89, 0, 69, 0, 5], [3, 85, 1, 66, 0, 5], [0, 89, 10, 69, 0, 5]] * 4, np.int32)
+    bs = lat.node(rng.integers(3, 85, 12), rng.integers(10, 66, 12), rng.integers(0, 6, 12)).astype(np.int32)
+    bd = lat.node(rng.integers(3, 85, 12), rng.integers(10, 66, 12), rng.integers(0, 6, 12)).astype(np.int32)
+    boxes = np.concatenate([boxes, big_boxes])
+    src = np.concatenate([src, bs])
+    dst = np.concatenate([dst, bd])
     cap = 2048
     nodes, edges, lens = dg.batch_bbox(cuda(w), cuda(src), cuda(dst), cuda(boxes), path_cap=cap)
     ref_nodes, ref_lens = O.batch_bbox(lat.indptr, lat.indices, w, lat.nx, lat.ny, lat.nz, src, dst, boxes, cap)
