@@ -138,6 +138,23 @@ ORSP_API int orsp_roi_bfs(orsp_graph *g, int32_t src, int32_t dst, int32_t max_d
                  int32_t max_nodes, int32_t *roi_nodes_d, int32_t *g2r_d,
                  int32_t *roi_count_h, uintptr_t stream);
 
+/* Allocation-free variant of orsp_roi_bfs (no counterpart in the reference).
+ * For callers that cannot allocate device memory while routing - e.g. code
+ * running during CUDA stream capture, or a host application whose own
+ * allocator owns all device memory - this call allocates nothing: its work
+ * buffers live in one fixed device array inside liborsp.so (about 8.5 MB,
+ * held on every GPU that loads the library until exit).  Same arguments,
+ * semantics and results as orsp_roi_bfs, for graphs of at most
+ * ORSP_ROI_BFS_NOALLOC_MAX_NODES nodes; larger graphs get ORSP_ERR_ARG.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  All calls on a device share the
+ * array, so calls that overlap on the GPU (other streams, other threads)
+ * race and must be serialised by the caller. */
+#define ORSP_ROI_BFS_NOALLOC_MAX_NODES 524288
+ORSP_API int orsp_roi_bfs_noalloc(orsp_graph *g, int32_t src, int32_t dst, int32_t max_depth,
+                         int32_t max_nodes, int32_t *roi_nodes_d, int32_t *g2r_d,
+                         int32_t *roi_count_h, uintptr_t stream);
+
 /* global_to_roi (int32[N]) of an inclusive box [x0,x1,y0,y1,z0,z1] (host
  * array box_h[6]): -1 outside, row-major local id inside.  The box ROI of the
  * benchmark router (bounding box of the pins plus a margin), in the

@@ -49,6 +49,7 @@ _SIGS = {
                                  ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
     "orsp_sssp_batch_bbox": (ctypes.c_int, [_P, _P, _i32, _P, _P, _P, _P, _f32, _P, _P, _i32, _P, _u]),
     "orsp_roi_bfs": (ctypes.c_int, [_P, _i32, _i32, _i32, _i32, _P, _P, ctypes.POINTER(_i32), _u]),
+    "orsp_roi_bfs_noalloc": (ctypes.c_int, [_P, _i32, _i32, _i32, _i32, _P, _P, ctypes.POINTER(_i32), _u]),
     "orsp_roi_box_map": (ctypes.c_int, [_P, _P, _P, _u]),
     "orsp_path_to_edges": (ctypes.c_int, [_P, _P, _i32, _P, ctypes.POINTER(_i32), _u]),
     "orsp_update_costs": (ctypes.c_int, [_i64, _P, _P, _P, _P, _P, _P, _P, _f32, _f32, _f32, _f32,

@@ -9,6 +9,8 @@
 // which the frontier is processed.  The ROI is then the marked nodes in
 // ascending id order (np.where), produced by an order-preserving compaction.
 #include <algorithm>
+#include <mutex>
+#include <string>
 
 #include "common.cuh"
 
@@ -328,6 +330,109 @@ extern "C" int orsp_roi_bfs(orsp_graph *g, int32_t src, int32_t dst, int32_t max
   ORSP_CUDA(cudaStreamSynchronize(st));
   const int32_t *h = (const int32_t *)g->pinned;
   if (h[3]) { set_error("roi_bfs: queue overflow"); return ORSP_ERR_OVERFLOW; }
+  *roi_count_h = h[5];
+  return ORSP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free ROI extraction.
+//
+// orsp_roi_bfs keeps its work buffers (visit marks, the four wave queues and
+// the compaction tiles) in device memory that the library allocates with
+// cudaMalloc on first use.  Some callers cannot allow that: code running
+// while a stream is being captured into a CUDA graph, or inside a host that
+// owns all device memory through its own allocator and forbids allocations
+// on the routing path.  orsp_roi_bfs_noalloc gives them the same extraction
+// with its work buffers in one file-scope device array, so the call itself
+// allocates nothing.  The array is sized for graphs of at most
+// ORSP_ROI_BFS_NOALLOC_MAX_NODES nodes and every GPU that loads the library
+// holds it (about 8.5 MB) until the process exits.
+namespace {
+
+constexpr size_t kNaSeenBytes = ((size_t)ORSP_ROI_BFS_NOALLOC_MAX_NODES + 15) & ~(size_t)15;
+constexpr size_t kNaQueueBytes = (size_t)ORSP_ROI_BFS_NOALLOC_MAX_NODES * 4;
+constexpr size_t kNaTileBytes =
+    (((size_t)ORSP_ROI_BFS_NOALLOC_MAX_NODES + CMP_TILE - 1) / CMP_TILE * 4 + 15) & ~(size_t)15;
+constexpr size_t kNaBytes = kNaSeenBytes + 4 * kNaQueueBytes + kNaTileBytes + 64;
+
+// Shared by every call on a device; see orsp_roi_bfs_noalloc for the rules.
+static __device__ __align__(256) unsigned char g_roi_noalloc_scratch[kNaBytes];
+
+constexpr int kNaMaxDevices = 64;
+std::mutex g_na_mutex;
+void *g_na_ptr[kNaMaxDevices] = {};
+
+// Device address of the array on `device` (which must be current).  Looked up
+// once per device: host code cannot use the symbol itself as a device address.
+int noalloc_scratch(int device, unsigned char **out) {
+  std::lock_guard<std::mutex> lock(g_na_mutex);
+  if (device < 0 || device >= kNaMaxDevices) {
+    set_error("roi_bfs_noalloc: device ordinal out of range");
+    return ORSP_ERR_ARG;
+  }
+  if (!g_na_ptr[device]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_roi_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_roi_noalloc_scratch)");
+    g_na_ptr[device] = p;
+  }
+  *out = (unsigned char *)g_na_ptr[device];
+  return ORSP_OK;
+}
+
+}  // namespace
+
+extern "C" int orsp_roi_bfs_noalloc(orsp_graph *g, int32_t src, int32_t dst, int32_t max_depth,
+                                    int32_t max_nodes, int32_t *roi_nodes_d, int32_t *g2r_d,
+                                    int32_t *roi_count_h, uintptr_t stream) {
+  if (!g || !roi_nodes_d || !roi_count_h) { set_error("roi_bfs_noalloc: NULL argument"); return ORSP_ERR_ARG; }
+  if (g->N > ORSP_ROI_BFS_NOALLOC_MAX_NODES) {
+    set_error("roi_bfs_noalloc: graph has " + std::to_string(g->N) + " nodes, more than the " +
+              std::to_string(ORSP_ROI_BFS_NOALLOC_MAX_NODES) +
+              " its fixed work array holds; use orsp_roi_bfs");
+    return ORSP_ERR_ARG;
+  }
+  if (src < 0 || src >= g->N || dst < 0 || dst >= g->N) { set_error("roi_bfs_noalloc: src/dst out of range"); return ORSP_ERR_ARG; }
+  if (max_nodes <= 0) { set_error("roi_bfs_noalloc: max_nodes must be > 0"); return ORSP_ERR_ARG; }
+  ORSP_CUDA(cudaSetDevice(g->device));
+  unsigned char *base = nullptr;
+  int rc = noalloc_scratch(g->device, &base);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t N = g->N;
+  const int ntiles = (int)((N + CMP_TILE - 1) / CMP_TILE);
+  uint8_t *seen = base;
+  int32_t *q[4];
+  for (int i = 0; i < 4; ++i) q[i] = (int32_t *)(base + kNaSeenBytes + i * kNaQueueBytes);
+  int32_t *tiles = (int32_t *)(base + kNaSeenBytes + 4 * kNaQueueBytes);
+  int32_t *misc = (int32_t *)(base + kNaSeenBytes + 4 * kNaQueueBytes + kNaTileBytes);
+  BfsCtl *ctl = (BfsCtl *)misc;
+
+  // The array keeps the previous call's contents: the visit marks must start
+  // at zero; the queues, tile counts and counters are written before read.
+  ORSP_CUDA(cudaMemsetAsync(seen, 0, ((size_t)N + 15) & ~(size_t)15, st));
+  roi_bfs_kernel<<<1, BFS_THREADS, 0, st>>>(g->indptr, g->indices, g->N, src, dst, max_depth,
+                                            max_nodes, seen, q[0], q[1], q[2], q[3], ctl);
+  ORSP_CUDA(cudaGetLastError());
+  count_tiles_kernel<<<ntiles, CMP_THREADS, 0, st>>>(seen, g->N, tiles);
+  ORSP_CUDA(cudaGetLastError());
+  scan_tiles_kernel<<<1, 1024, 0, st>>>(tiles, ntiles, misc + 4);
+  ORSP_CUDA(cudaGetLastError());
+  write_tiles_kernel<<<ntiles, CMP_THREADS, 0, st>>>(seen, g->N, tiles, roi_nodes_d);
+  ORSP_CUDA(cudaGetLastError());
+  truncate_kernel<<<1, 32, 0, st>>>(roi_nodes_d, misc + 4, max_nodes, src, dst, misc + 5);
+  ORSP_CUDA(cudaGetLastError());
+  if (g2r_d) {
+    fill_i32_kernel<<<std::min<int64_t>((N + 255) / 256, 4096), 256, 0, st>>>(g2r_d, N, -1);
+    scatter_g2r_kernel<<<std::min<int64_t>((N + 255) / 256, 1024), 256, 0, st>>>(roi_nodes_d,
+                                                                                 misc + 5, g2r_d);
+    ORSP_CUDA(cudaGetLastError());
+  }
+  // g->pinned was allocated when the graph was created, not here.
+  ORSP_CUDA(cudaMemcpyAsync(g->pinned, misc, 24, cudaMemcpyDeviceToHost, st));
+  ORSP_CUDA(cudaStreamSynchronize(st));
+  const int32_t *h = (const int32_t *)g->pinned;
+  if (h[3]) { set_error("roi_bfs_noalloc: queue overflow"); return ORSP_ERR_OVERFLOW; }
   *roi_count_h = h[5];
   return ORSP_OK;
 }
