@@ -65,6 +65,10 @@ ORSP_API const char *orsp_last_error(void);
  * the most recent one in milliseconds.  No counterpart in the reference. */
 ORSP_API int orsp_profile_enable(int on);
 ORSP_API int orsp_profile_last(float *kernel_ms);
+/* Work counters of the last lattice search: {grid rounds, tile visits,
+ * sweep cycles, 0, ns loading tiles, ns sweeping, ns writing back,
+ * ns scheduling} (times summed over tile visits). */
+ORSP_API int orsp_profile_counters(int64_t *out8);
 
 /* ---- graph ------------------------------------------------------------- */
 typedef struct orsp_graph orsp_graph;

@@ -41,6 +41,7 @@ _SIGS = {
     "orsp_last_error": (ctypes.c_char_p, []),
     "orsp_profile_enable": (ctypes.c_int, [ctypes.c_int]),
     "orsp_profile_last": (ctypes.c_int, [ctypes.POINTER(_f32)]),
+    "orsp_profile_counters": (ctypes.c_int, [ctypes.POINTER(_i64)]),
     "orsp_graph_create": (ctypes.c_int, [_i32, _i64, _P, _P, _i32, _i32, _i32, ctypes.c_int, ctypes.POINTER(_P)]),
     "orsp_graph_destroy": (ctypes.c_int, [_P]),
     "orsp_graph_csr": (ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P)]),

@@ -23,6 +23,7 @@ SOURCES = [
     "orsp_batch.cu",
     "orsp_accounting.cu",
     "orsp_roi.cu",
+    "orsp_lattice.cu",
 ]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]

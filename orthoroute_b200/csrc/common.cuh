@@ -63,9 +63,36 @@ struct Graph {
   void *scratch = nullptr;
   size_t scratch_bytes = 0;
   void *pinned = nullptr;  // small pinned host buffer for results
+  // H/V lattice description, set when every CSR edge is a unit step along the
+  // layer's routing axis or a via to an adjacent layer (see orsp_lattice.cu)
+  bool lattice_ok = false;
+  int8_t layer_axis[64] = {};     // 0: no planar edges, 1: x, 2: y
+  int32_t *slot_eid = nullptr;    // [4][N] in-edge id per slot (-1 absent)
+  float *wslot = nullptr;         // [4][N] gathered in-edge weights
+  void *lat_ws = nullptr;         // tile lists, stamps and control block
+  size_t lat_ws_bytes = 0;
+  void *lat_ctl_h = nullptr;      // pinned mirror of the control block
 };
 
+// Optional timing of a search kernel (CUDA events on the launching stream),
+// enabled by orsp_profile_enable for roofline reporting.
+struct KernelTimer {
+  bool on = false;
+  bool pending = false;
+  cudaEvent_t a = nullptr, b = nullptr;
+  float last_ms = 0.0f;
+};
+extern KernelTimer g_timer;
+// rounds and tile visits of the last lattice search (orsp_profile_counters)
+extern int64_t g_counters[8];
+
 int ensure_scratch(Graph *g, size_t bytes);
+// orsp_lattice.cu
+int analyze_lattice(Graph *g, const int32_t *indptr_h, const int32_t *indices_h);
+void free_lattice(Graph *g);
+int run_lattice_search(Graph *g, const float *cost_d, int32_t nseeds, const int32_t *seeds_d,
+                       const float *seed_cost_d, uint32_t *dist, cudaStream_t st);
+int finish_lattice_search(Graph *g, int32_t *rounds_h);
 
 }  // namespace orsp
 

@@ -144,6 +144,13 @@ extern "C" int orsp_graph_create(int32_t N, int64_t E, const int32_t *indptr_h,
   }
   TRY(cudaMallocHost(&g->pinned, 4096));
 #undef TRY
+  if (nx > 0) {
+    int rc = analyze_lattice(g, indptr_h, indices_h);
+    if (rc) {
+      orsp_graph_destroy(g);
+      return rc;
+    }
+  }
   *out = g;
   return ORSP_OK;
 }
@@ -167,6 +174,7 @@ extern "C" int orsp_graph_destroy(orsp_graph *g) {
   cudaFree(g->batch_ctl);
   cudaFree(g->scratch);
   if (g->pinned) cudaFreeHost(g->pinned);
+  free_lattice(g);
   delete g;
   return ORSP_OK;
 }

@@ -1,0 +1,723 @@
+// Lattice search: single-source shortest paths on the H/V routing lattice by
+// shared-memory tile sweeps.
+//
+// The generic grid search (orsp_sssp.cu) needs one grid-wide round per hop of
+// the shortest-path tree (about 1 400 rounds on a 1000 x 1000 grid, each a
+// dependent memory chain plus a grid barrier).  On the routing lattice every
+// node has at most four in-edges - the two neighbours along its layer's
+// routing axis (x on H layers, y on V layers) and the vias to the layers above
+// and below - so a tile of TX x TY columns (all layers) can be relaxed to a
+// local fixpoint in shared memory with directional sweeps:
+//   x-runs on H layers, y-runs on V layers, z-runs through each via column,
+// each run a forward and a backward pass (so a straight wave crosses the tile
+// in one pass).  Tiles exchange only boundary improvements, once per grid
+// round, so the number of grid rounds drops by about the tile width.
+//
+// Every update is the fp32 round-to-nearest relaxation min(d[v], d[u] + w), so
+// the result is the unique fixpoint of the generic search, bit for bit, in any
+// order; the backtrace (orsp_sssp.cu) is shared.  A tile that has not
+// converged after MAX_CYCLES sweep cycles is simply revisited next round.
+//
+// Tiles in the next round's list: neighbours whose halo value improved (and
+// the tile itself if it did not converge).  Each tile is in a round's list at
+// most once (stamp[t] = last round it was queued for), so a tile is only ever
+// processed by one CTA per round and owns its nodes' distances.
+#include <algorithm>
+#include <cstdlib>
+#include <vector>
+
+#include "common.cuh"
+
+namespace {
+
+constexpr int MAX_CYCLES = 64;
+
+struct LatCtl {
+  GridBarrier bar;
+  int err;
+  unsigned lcnt[3];  // tile-list counts by round % 3
+  unsigned work[3];  // per-round work counters by round % 3
+  unsigned rounds;
+  unsigned visits;
+  unsigned long long cycles;
+  unsigned head, tail;  // tile queue positions (asynchronous schedule)
+  int pending;          // tiles queued or being visited
+  unsigned pad;
+  unsigned long long ns[4];  // time in load, sweeps, write-back, scheduling (sum over visits)
+};
+
+struct LatParams {
+  int32_t nx, ny, nz;
+  int32_t bx0, bx1, by0, by1, bz0, bz1;  // searched box (inclusive)
+  int32_t ntx, nty;                       // tiles along x, y
+  const float4 *w4;                        // in-edge weights per node
+  uint32_t *dist;
+  int32_t *list0, *list1;
+  unsigned *stamp;
+  int32_t *qslot;  // asynchronous schedule: ring of tile ids (-1 = empty)
+  int *tstate;     // 0 idle, 1 queued, 2 visiting, 3 visiting and dirty
+  unsigned qcap;
+  LatCtl *ctl;
+  int8_t axis[64];
+  unsigned max_rounds;
+  unsigned long long wait_ns, budget_ns;
+};
+
+__global__ void fill_kernel(uint32_t *p, int64_t n, uint32_t v) {
+  const int64_t s = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += s) p[i] = v;
+}
+
+// In-edge weights of node v as one float4 {from lower axis neighbour, from
+// upper axis neighbour, via from below, via from above}; +inf where absent.
+__global__ void gather_kernel(const int32_t *__restrict__ slot_eid, const float *__restrict__ cost,
+                              float4 *__restrict__ w, int64_t n) {
+  const float INF_F = __int_as_float(0x7f800000);
+  const int64_t s = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += s) {
+    const int32_t e0 = slot_eid[v], e1 = slot_eid[n + v], e2 = slot_eid[2 * n + v], e3 = slot_eid[3 * n + v];
+    w[v] = make_float4(e0 >= 0 ? __ldg(&cost[e0]) : INF_F, e1 >= 0 ? __ldg(&cost[e1]) : INF_F,
+                       e2 >= 0 ? __ldg(&cost[e2]) : INF_F, e3 >= 0 ? __ldg(&cost[e3]) : INF_F);
+  }
+}
+
+template <int TX, int TY>
+__device__ __forceinline__ int tile_of(const LatParams &p, int32_t gx, int32_t gy) {
+  return ((gy - p.by0) / TY) * p.ntx + (gx - p.bx0) / TX;
+}
+
+template <int TX, int TY>
+__global__ void lattice_seed_kernel(LatParams p, int32_t nseeds, const int32_t *seeds,
+                                    const float *seed_cost) {
+  LatCtl *c = p.ctl;
+  if (threadIdx.x == 0) {
+    c->bar.count = 0;
+    c->bar.gen = 0;
+    c->err = 0;
+    for (int i = 0; i < 3; ++i) { c->lcnt[i] = 0; c->work[i] = 0; }
+    c->rounds = 0;
+    c->visits = 0;
+    c->cycles = 0;
+    c->head = 0;
+    c->tail = 0;
+    c->pending = 0;
+    for (int i = 0; i < 4; ++i) c->ns[i] = 0;
+  }
+  __syncthreads();
+  const int32_t plane = p.nx * p.ny;
+  for (int i = threadIdx.x; i < nseeds; i += blockDim.x) {
+    const int32_t s = seeds[i];
+    if (s < 0 || s >= plane * p.nz) continue;
+    const int32_t z = s / plane, r = s - z * plane, y = r / p.nx, x = r - y * p.nx;
+    if (x < p.bx0 || x > p.bx1 || y < p.by0 || y > p.by1 || z < p.bz0 || z > p.bz1) continue;
+    const float c0 = seed_cost ? seed_cost[i] : 0.0f;
+    if (!(c0 >= 0.0f) || !(c0 < __int_as_float(0x7f800000))) continue;
+    atomicMin(&p.dist[s], f_bits(c0));
+    const int t = tile_of<TX, TY>(p, x, y);
+    if (p.qslot) {
+      if (atomicCAS(&p.tstate[t], 0, 1) == 0) {
+        atomicAdd(&c->pending, 1);
+        const unsigned k = atomicAdd(&c->tail, 1u);
+        atomicExch(&p.qslot[k % p.qcap], t);
+      }
+    } else if (atomicMax(&p.stamp[t], 1u) < 1u) {
+      const unsigned k = atomicAdd(&c->lcnt[0], 1u);
+      p.list0[k] = t;
+    }
+  }
+}
+
+// One run of the sweep: cells c[1..n] at stride `ds`, with c[0] and c[n+1]
+// the halo values (when `halo`; otherwise the run starts and ends at c[1] and
+// c[n]).  Forward: c[i] = min(c[i], c[i-1] + wlo[i]); backward: c[i] =
+// min(c[i], c[i+1] + whi[i]); each step a single fp32 round-to-nearest add.
+// The run is walked in register chunks of 4 (loads first, then the dependent
+// min-plus chain) so that only one shared-memory round trip is exposed per
+// chunk.  Returns whether any cell decreased.
+__device__ __forceinline__ bool sweep_run(float *c, int ds, const float *wlo, const float *whi, int ws,
+                                          int n, bool halo = true) {
+  constexpr int K = 4;
+  bool chg = false;
+  float prev = halo ? c[0] : __int_as_float(0x7f800000);
+  for (int b = 1; b <= n; b += K) {
+    float cv[K], wv[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (b + k <= n) { cv[k] = c[(b + k) * ds]; wv[k] = wlo[(b + k) * ws]; }
+    unsigned dirty = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (b + k <= n) {
+        const float c2 = __fadd_rn(prev, wv[k]);
+        if (c2 < cv[k]) { cv[k] = c2; dirty |= 1u << k; }
+        prev = cv[k];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (dirty & (1u << k)) c[(b + k) * ds] = cv[k];
+    chg |= dirty != 0;
+  }
+  prev = halo ? c[(n + 1) * ds] : __int_as_float(0x7f800000);
+  for (int b = n; b >= 1; b -= K) {
+    float cv[K], wv[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (b - k >= 1) { cv[k] = c[(b - k) * ds]; wv[k] = whi[(b - k) * ws]; }
+    unsigned dirty = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (b - k >= 1) {
+        const float c2 = __fadd_rn(prev, wv[k]);
+        if (c2 < cv[k]) { cv[k] = c2; dirty |= 1u << k; }
+        prev = cv[k];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (dirty & (1u << k)) c[(b - k) * ds] = cv[k];
+    chg |= dirty != 0;
+  }
+  return chg;
+}
+
+// Relaxes one tile (all layers of the box) to a local fixpoint and publishes
+// improved values.  Called by all threads of the CTA.  Shared memory:
+// distances with a one-cell halo [nzb][TY+2][TX+3], then the interior in-edge
+// weights [4][nzb][TY][TX+1] and the interior distances as loaded
+// [nzb][TY][TX+1] (odd row strides: the row walks of the x-sweep and the
+// column walks of the y- and z-sweeps are bank-conflict free).
+template <int TX, int TY>
+__device__ void process_tile(const LatParams &p, int t, float *sd, const int *s_hl, int nh,
+                             const int *s_vl, int nv, int *s_flags, int *s_act) {
+  constexpr int SX = TX + 3;
+  constexpr int PS = (TY + 2) * SX;
+  constexpr int WSX = TX + 1;
+  constexpr int WPS = TY * WSX;
+  const float INF_F = __int_as_float(0x7f800000);
+  const int tx = t % p.ntx, ty = t / p.ntx;
+  const int32_t X0 = p.bx0 + tx * TX, Y0 = p.by0 + ty * TY;
+  const int tw = min(TX, p.bx1 - X0 + 1), th = min(TY, p.by1 - Y0 + 1);
+  const int nzb = p.bz1 - p.bz0 + 1;
+  const int64_t nxy = (int64_t)p.nx * p.ny;
+  const int64_t col0 = (int64_t)Y0 * p.nx + X0;  // node of (X0, Y0, z=0)
+  float *wlo = sd + nzb * PS;          // slot 0: from the lower axis neighbour
+  float *whi = wlo + nzb * WPS;        // slot 1: from the upper axis neighbour
+  float *wdn = whi + nzb * WPS;        // slot 2: via from below
+  float *wup = wdn + nzb * WPS;        // slot 3: via from above
+
+  float *orig = wup + nzb * WPS;        // interior distances as loaded
+  unsigned long long ts0 = 0;
+  if (threadIdx.x == 0) ts0 = dev_globaltimer();
+  if (threadIdx.x < 5) s_act[threadIdx.x] = 0;
+  if (threadIdx.x < 3) s_flags[threadIdx.x] = 0;
+  // ---- load.  Interior cells: distance and the four in-edge weights, four
+  // cells per thread in flight at a time.  Halo cells: only those the sweeps
+  // read (x-halo of H-layer rows, y-halo of V-layer columns).  Distances are
+  // read through L2 (other CTAs write them); weights are read-only.
+  // one thread per column (x, y) of the tile: its nzb cells' loads are
+  // issued back to back
+  for (int c = threadIdx.x; c < th * tw; c += blockDim.x) {
+    const int yy = c / tw + 1, xx = c - (yy - 1) * tw + 1;
+    const int64_t n0 = (int64_t)p.bz0 * nxy + col0 + (int64_t)(yy - 1) * p.nx + (xx - 1);
+    const int s0 = yy * SX + xx, w0 = (yy - 1) * WSX + (xx - 1);
+#pragma unroll 6
+    for (int z = 0; z < nzb; ++z) {
+      const int64_t node = n0 + z * nxy;
+      const float dv = bits_f(__ldcg(&p.dist[node]));
+      const float4 wv = __ldg(&p.w4[node]);
+      sd[z * PS + s0] = dv;
+      orig[z * WPS + w0] = dv;
+      wlo[z * WPS + w0] = wv.x;
+      whi[z * WPS + w0] = wv.y;
+      wdn[z * WPS + w0] = wv.z;
+      wup[z * WPS + w0] = wv.w;
+    }
+  }
+  {
+    // halo: 2 cells per H row and per V column
+    const int nhh = 2 * nh * th, nvh = 2 * nv * tw;
+    for (int i = threadIdx.x; i < nhh + nvh; i += blockDim.x) {
+      int z, xx, yy;
+      if (i < nhh) {
+        const int rowi = i >> 1;
+        z = s_hl[rowi / th];
+        yy = rowi % th + 1;
+        xx = (i & 1) ? tw + 1 : 0;
+      } else {
+        const int coli = (i - nhh) >> 1;
+        z = s_vl[coli / tw];
+        xx = coli % tw + 1;
+        yy = ((i - nhh) & 1) ? th + 1 : 0;
+      }
+      const int32_t gx = X0 + xx - 1, gy = Y0 + yy - 1;
+      float v = INF_F;
+      if (gx >= p.bx0 && gx <= p.bx1 && gy >= p.by0 && gy <= p.by1)
+        v = bits_f(__ldcg(&p.dist[(int64_t)(p.bz0 + z) * nxy + (int64_t)gy * p.nx + gx]));
+      sd[z * PS + yy * SX + xx] = v;
+    }
+  }
+  __syncthreads();
+  unsigned long long ts1 = 0;
+  if (threadIdx.x == 0) ts1 = dev_globaltimer();
+
+  // ---- sweep cycles.  Each cycle: the planar runs (x-runs on H layers and
+  // y-runs on V layers touch disjoint layers, so they run side by side), then
+  // the via runs along z.
+  bool converged = false;
+  int cyc = 0;
+  const int nplan = nh * th + nv * tw;
+  for (; cyc < MAX_CYCLES; ++cyc) {
+    if (threadIdx.x == 0) s_flags[(cyc + 1) % 3] = 0;
+    bool chg = false;
+    for (int rr = threadIdx.x; rr < nplan; rr += blockDim.x) {
+      float *cell;
+      int wo, ds, ws, n;
+      if (rr < nh * th) {  // x-run of an H-layer row
+        const int z = s_hl[rr / th], yy = rr % th + 1;
+        cell = sd + z * PS + yy * SX;
+        wo = z * WPS + (yy - 1) * WSX - 1;
+        ds = 1;
+        ws = 1;
+        n = tw;
+      } else {  // y-run of a V-layer column
+        const int q = rr - nh * th;
+        const int z = s_vl[q / tw], xx = q % tw + 1;
+        cell = sd + z * PS + xx;
+        wo = z * WPS + (xx - 1) - WSX;
+        ds = SX;
+        ws = WSX;
+        n = th;
+      }
+      chg |= sweep_run(cell, ds, wlo + wo, whi + wo, ws, n);
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < tw * th; c += blockDim.x) {
+      const int xx = c % tw + 1, yy = c / tw + 1;
+      // the z run has no halo: start the forward pass at layer 0 itself
+      float *col = sd + yy * SX + xx - PS;
+      const int wo = (yy - 1) * WSX + (xx - 1) - WPS;
+      chg |= sweep_run(col, PS, wdn + wo, wup + wo, WPS, nzb, /*halo=*/false);
+    }
+    if (chg) s_flags[cyc % 3] = 1;
+    __syncthreads();
+    if (!s_flags[cyc % 3]) { converged = true; break; }
+  }
+  unsigned long long ts2 = 0;
+  if (threadIdx.x == 0) {
+    ts2 = dev_globaltimer();
+    atomicAdd((unsigned long long *)&p.ctl->cycles, (unsigned long long)(cyc + 1));
+  }
+
+  // ---- publish improvements; mark neighbour tiles whose halo changed
+  const int interior = nzb * th * tw;
+  for (int i = threadIdx.x; i < interior; i += blockDim.x) {
+    const int z = i / (th * tw);
+    const int rem = i - z * th * tw;
+    const int yy = rem / tw + 1, xx = rem % tw + 1;
+    const float v = sd[z * PS + yy * SX + xx];
+    const int gz = p.bz0 + z;
+    const int64_t node = (int64_t)gz * nxy + col0 + (int64_t)(yy - 1) * p.nx + (xx - 1);
+    if (v < orig[z * WPS + (yy - 1) * WSX + (xx - 1)]) {
+      __stcg(&p.dist[node], f_bits(v));
+      const int ax = p.axis[gz];
+      if (ax == 1) {
+        if (xx == 1) s_act[0] = 1;
+        if (xx == tw) s_act[1] = 1;
+      } else if (ax == 2) {
+        if (yy == 1) s_act[2] = 1;
+        if (yy == th) s_act[3] = 1;
+      }
+    }
+  }
+  if (threadIdx.x == 0 && !converged) s_act[4] = 1;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned long long ts3 = dev_globaltimer();
+    atomicAdd(&p.ctl->ns[0], ts1 - ts0);
+    atomicAdd(&p.ctl->ns[1], ts2 - ts1);
+    atomicAdd(&p.ctl->ns[2], ts3 - ts2);
+  }
+}
+
+// Tiles to revisit after a visit of tile t: the neighbours whose halo value
+// improved (s_act[0..3] = left, right, down, up) and t itself if it did not
+// converge (s_act[4]).  Returns the count written to nb[0..4].
+__device__ __forceinline__ int revisit_list(const LatParams &p, int t, const int *s_act, int *nb) {
+  const int tx = t % p.ntx, ty = t / p.ntx;
+  int k = 0;
+  if (s_act[0] && tx > 0) nb[k++] = t - 1;
+  if (s_act[1] && tx < p.ntx - 1) nb[k++] = t + 1;
+  if (s_act[2] && ty > 0) nb[k++] = t - p.ntx;
+  if (s_act[3] && ty < p.nty - 1) nb[k++] = t + p.ntx;
+  if (s_act[4]) nb[k++] = t;
+  return k;
+}
+
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX * TY) lattice_tile_kernel(LatParams p) {
+  extern __shared__ float sd[];
+  __shared__ int s_hl[64], s_vl[64];
+  __shared__ int s_nh, s_nv;
+  __shared__ int s_flags[3];
+  __shared__ int s_act[5];
+  __shared__ int s_tile;
+  LatCtl *ctl = p.ctl;
+  const unsigned nblocks = gridDim.x;
+  const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+  const unsigned long long t_start = dev_globaltimer();
+  if (threadIdx.x == 0) {
+    int nh = 0, nv = 0;
+    for (int z = p.bz0; z <= p.bz1; ++z) {
+      if (p.axis[z] == 1) s_hl[nh++] = z - p.bz0;
+      else if (p.axis[z] == 2) s_vl[nv++] = z - p.bz0;
+    }
+    s_nh = nh;
+    s_nv = nv;
+  }
+  __syncthreads();
+  const int nh = s_nh, nv = s_nv;
+  unsigned r = 0;
+  for (;;) {
+    if (ld_acquire_u32((const unsigned *)&ctl->err)) break;
+    if (r >= p.max_rounds) {
+      if (leader) atomicCAS(&ctl->err, DEV_OK, DEV_ERR_TIMEOUT);
+      break;
+    }
+    const unsigned n_in = ld_acquire_u32(&ctl->lcnt[r % 3]);
+    if (n_in == 0) break;  // converged
+    const int32_t *inl = (r & 1) ? p.list1 : p.list0;
+    int32_t *outl = (r & 1) ? p.list0 : p.list1;
+    for (;;) {
+      if (threadIdx.x == 0) s_tile = (int)atomicAdd(&ctl->work[r % 3], 1u);
+      __syncthreads();
+      const int ti = s_tile;
+      __syncthreads();
+      if (ti >= (int)n_in) break;
+      const int t = __ldcg(&inl[ti]);
+      process_tile<TX, TY>(p, t, sd, s_hl, nh, s_vl, nv, s_flags, s_act);
+      if (threadIdx.x == 0) {
+        int nb[5];
+        const int k = revisit_list(p, t, s_act, nb);
+        for (int j = 0; j < k; ++j) {
+          if (atomicMax(&p.stamp[nb[j]], r + 2u) < r + 2u) {
+            const unsigned idx = atomicAdd(&ctl->lcnt[(r + 1) % 3], 1u);
+            __stcg(&outl[idx], nb[j]);  // idx < ntiles: each tile is queued once per round
+          }
+        }
+        atomicAdd(&ctl->visits, 1u);
+      }
+    }
+    if (leader) {
+      ctl->lcnt[(r + 2) % 3] = 0;
+      ctl->work[(r + 2) % 3] = 0;
+      if (dev_globaltimer() - t_start > p.budget_ns) atomicCAS(&ctl->err, DEV_OK, DEV_ERR_TIMEOUT);
+    }
+    grid_barrier(&ctl->bar, nblocks, &ctl->err, p.wait_ns);
+    ++r;
+  }
+  if (leader) ctl->rounds = r;
+}
+
+
+// ---------------------------------------------------------------------------
+// Asynchronous schedule: no grid barrier.  Tiles wait in a ring queue; each
+// CTA repeatedly takes the next tile, visits it and queues the tiles whose
+// halo it improved.  A tile is in the queue at most once (state 1) and is
+// visited by one CTA at a time (state 2); if its halo improves during a visit
+// (state 3) it queues itself again afterwards.  `pending` counts tiles in
+// states 1-3; it is raised before a tile is queued and lowered only after the
+// visiting CTA has queued everything it activated, so it reaches 0 only when
+// no tile can change again - the fixpoint.
+__device__ void queue_tile(const LatParams &p, int t) {
+  const unsigned k = atomicAdd(&p.ctl->tail, 1u);
+  atomicExch(&p.qslot[k % p.qcap], t);
+}
+
+// Returns false if the state machine could not be advanced (never expected;
+// recorded as an internal error by the caller).
+__device__ bool activate_tile(const LatParams &p, int t) {
+  for (int tries = 0; tries < 1024; ++tries) {
+    const int st = (int)ld_acquire_u32((const unsigned *)&p.tstate[t]);
+    if (st == 1 || st == 3) return true;
+    if (st == 0) {
+      if (atomicCAS(&p.tstate[t], 0, 1) == 0) {
+        atomicAdd(&p.ctl->pending, 1);
+        queue_tile(p, t);
+        return true;
+      }
+    } else if (st == 2) {
+      if (atomicCAS(&p.tstate[t], 2, 3) == 2) return true;
+    }
+  }
+  return false;
+}
+
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX * TY) lattice_async_kernel(LatParams p) {
+  extern __shared__ float sd[];
+  __shared__ int s_hl[64], s_vl[64];
+  __shared__ int s_nh, s_nv;
+  __shared__ int s_flags[3];
+  __shared__ int s_act[5];
+  __shared__ int s_tile;
+  LatCtl *ctl = p.ctl;
+  const unsigned long long t_start = dev_globaltimer();
+  if (threadIdx.x == 0) {
+    int nh = 0, nv = 0;
+    for (int z = p.bz0; z <= p.bz1; ++z) {
+      if (p.axis[z] == 1) s_hl[nh++] = z - p.bz0;
+      else if (p.axis[z] == 2) s_vl[nv++] = z - p.bz0;
+    }
+    s_nh = nh;
+    s_nv = nv;
+  }
+  __syncthreads();
+  const int nh = s_nh, nv = s_nv;
+  unsigned visits = 0;
+  unsigned long long sched_ns = 0;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const unsigned long long tq = dev_globaltimer();
+      int t = -1;
+      if (!ld_acquire_u32((const unsigned *)&ctl->err)) {
+        const unsigned pos = atomicAdd(&ctl->head, 1u);
+        int *slot = &p.qslot[pos % p.qcap];
+        const unsigned long long t0 = dev_globaltimer();
+        for (unsigned spins = 0;; ++spins) {
+          const int v = (int)ld_acquire_u32((const unsigned *)slot);
+          if (v >= 0) {
+            atomicExch(slot, -1);
+            t = v;
+            break;
+          }
+          if (ld_acquire_u32((const unsigned *)&ctl->pending) == 0) break;  // fixpoint reached
+          if (ld_acquire_u32((const unsigned *)&ctl->err)) break;
+          if ((spins & 31u) == 31u) {
+            const unsigned long long now = dev_globaltimer();
+            if (now - t0 > p.wait_ns || now - t_start > p.budget_ns) {
+              atomicCAS(&ctl->err, DEV_OK, DEV_ERR_TIMEOUT);
+              break;
+            }
+            __nanosleep(64);
+          }
+        }
+      }
+      if (t >= 0) {
+        atomicExch(&p.tstate[t], 2);
+        __threadfence();
+      }
+      s_tile = t;
+      sched_ns += dev_globaltimer() - tq;
+    }
+    __syncthreads();
+    const int t = s_tile;
+    __syncthreads();
+    if (t < 0) break;
+    process_tile<TX, TY>(p, t, sd, s_hl, nh, s_vl, nv, s_flags, s_act);
+    // neighbours are activated by threads 0..3 in parallel, after this
+    // tile's distances are visible
+    unsigned long long ta = 0;
+    if (threadIdx.x == 0) ta = dev_globaltimer();
+    if (threadIdx.x < 4) {
+      __threadfence();
+      const int tx = t % p.ntx, ty = t / p.ntx;
+      const int d = threadIdx.x;
+      int nb = -1;
+      if (s_act[d]) {
+        if (d == 0 && tx > 0) nb = t - 1;
+        if (d == 1 && tx < p.ntx - 1) nb = t + 1;
+        if (d == 2 && ty > 0) nb = t - p.ntx;
+        if (d == 3 && ty < p.nty - 1) nb = t + p.ntx;
+      }
+      if (nb >= 0 && !activate_tile(p, nb)) atomicCAS(&ctl->err, DEV_OK, DEV_ERR_INTERNAL);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      // leave the visiting state: back to idle, or queued again when dirty
+      // (halo changed meanwhile) or not converged
+      if (s_act[4] || atomicCAS(&p.tstate[t], 2, 0) != 2) {
+        atomicExch(&p.tstate[t], 1);
+        queue_tile(p, t);
+      } else {
+        atomicSub(&ctl->pending, 1);
+      }
+      ++visits;
+      sched_ns += dev_globaltimer() - ta;
+    }
+  }
+  if (threadIdx.x == 0) {
+    atomicAdd(&ctl->visits, visits);
+    atomicAdd(&ctl->ns[3], sched_ns);
+  }
+}
+
+unsigned long long env_u64(const char *name, unsigned long long dflt) {
+  const char *s = getenv(name);
+  if (!s || !*s) return dflt;
+  return strtoull(s, nullptr, 10);
+}
+
+template <int TX, int TY>
+int launch_lattice(orsp::Graph *g, LatParams &p, int32_t nseeds, const int32_t *seeds,
+                   const float *seed_cost, cudaStream_t st) {
+  p.ntx = (p.bx1 - p.bx0 + TX) / TX;
+  p.nty = (p.by1 - p.by0 + TY) / TY;
+  const int64_t ntiles = (int64_t)p.ntx * p.nty;
+  const bool async = env_u64("ORSP_LAT_ASYNC", 1) != 0;
+  const size_t list_b = (((size_t)ntiles * 4) + 255) & ~(size_t)255;
+  const unsigned qcap = (unsigned)(ntiles + 4 * g->num_sms * 4 + 64);
+  const size_t q_b = (((size_t)qcap * 4) + 255) & ~(size_t)255;
+  const size_t need = 4 * list_b + q_b + 256;
+  if (g->lat_ws_bytes < need) {
+    cudaFree(g->lat_ws);
+    g->lat_ws = nullptr;
+    g->lat_ws_bytes = 0;
+    ORSP_CUDA(cudaMalloc(&g->lat_ws, need));
+    g->lat_ws_bytes = need;
+  }
+  if (!g->lat_ctl_h) ORSP_CUDA(cudaMallocHost(&g->lat_ctl_h, sizeof(LatCtl)));
+  char *b = (char *)g->lat_ws;
+  p.list0 = (int32_t *)b;
+  p.list1 = (int32_t *)(b + list_b);
+  p.stamp = (unsigned *)(b + 2 * list_b);
+  p.tstate = (int *)(b + 3 * list_b);
+  p.qslot = async ? (int32_t *)(b + 4 * list_b) : nullptr;
+  p.qcap = qcap;
+  p.ctl = (LatCtl *)(b + 4 * list_b + q_b);
+  ORSP_CUDA(cudaMemsetAsync(p.stamp, 0, (size_t)ntiles * 4, st));
+  ORSP_CUDA(cudaMemsetAsync(p.tstate, 0, (size_t)ntiles * 4, st));
+  if (async) ORSP_CUDA(cudaMemsetAsync(p.qslot, 0xff, (size_t)qcap * 4, st));
+  lattice_seed_kernel<TX, TY><<<1, 256, 0, st>>>(p, nseeds, seeds, seed_cost);
+  ORSP_CUDA(cudaGetLastError());
+  const int nzb = p.bz1 - p.bz0 + 1;
+  const size_t smem = ((size_t)nzb * (TY + 2) * (TX + 3) + (size_t)5 * nzb * TY * (TX + 1)) * sizeof(float);
+  if (smem > 227 * 1024) {
+    orsp::set_error("lattice search: too many layers for the shared-memory tile");
+    return ORSP_ERR_ARG;
+  }
+  void *kfn = async ? (void *)lattice_async_kernel<TX, TY> : (void *)lattice_tile_kernel<TX, TY>;
+  ORSP_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0;
+  ORSP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, TX * TY, smem));
+  if (occ < 1) {
+    orsp::set_error("lattice search: kernel does not fit on an SM");
+    return ORSP_ERR_ARG;
+  }
+  const int want = (int)env_u64("ORSP_LAT_BLOCKS_PER_SM", 4);
+  const int bps = std::max(1, std::min(occ, want));
+  p.max_rounds = (unsigned)std::min<unsigned long long>(64ull * (unsigned long long)ntiles + 4096ull, 1ull << 30);
+  p.wait_ns = env_u64("ORSP_WAIT_NS", 2000000000ull);
+  p.budget_ns = env_u64("ORSP_BUDGET_NS", 20000000000ull);
+  void *args[] = {&p};
+  if (orsp::g_timer.on) ORSP_CUDA(cudaEventRecord(orsp::g_timer.a, st));
+  // Cooperative launch in both schedules: every CTA is resident, so a CTA
+  // waiting for a queue slot never blocks the CTA that will fill it.
+  ORSP_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(g->num_sms * bps), dim3(TX * TY), args, smem, st));
+  if (orsp::g_timer.on) {
+    ORSP_CUDA(cudaEventRecord(orsp::g_timer.b, st));
+    orsp::g_timer.pending = true;
+  }
+  ORSP_CUDA(cudaMemcpyAsync(g->lat_ctl_h, p.ctl, sizeof(LatCtl), cudaMemcpyDeviceToHost, st));
+  return ORSP_OK;
+}
+
+}  // namespace
+
+namespace orsp {
+
+int analyze_lattice(Graph *g, const int32_t *indptr_h, const int32_t *indices_h) {
+  g->lattice_ok = false;
+  if (g->nx <= 0 || g->ny <= 0 || g->nz <= 0 || g->nz > 64) return ORSP_OK;
+  const int32_t N = g->N, nx = g->nx, ny = g->ny;
+  const int64_t nxy = (int64_t)nx * ny;
+  std::vector<int8_t> axis(g->nz, -1);
+  std::vector<int32_t> slot((size_t)4 * N, -1);
+  for (int32_t u = 0; u < N; ++u) {
+    const int32_t zu = (int32_t)(u / nxy);
+    const int32_t ru = (int32_t)(u - zu * nxy);
+    const int32_t yu = ru / nx, xu = ru - yu * nx;
+    for (int32_t k = indptr_h[u]; k < indptr_h[u + 1]; ++k) {
+      const int32_t v = indices_h[k];
+      const int32_t zv = (int32_t)(v / nxy);
+      const int32_t rv = (int32_t)(v - zv * nxy);
+      const int32_t yv = rv / nx, xv = rv - yv * nx;
+      const int dz = zv - zu, dx = xv - xu, dy = yv - yu;
+      int s = -1;
+      if (dz == 0) {
+        int ax;
+        if (dy == 0 && (dx == 1 || dx == -1)) ax = 1;
+        else if (dx == 0 && (dy == 1 || dy == -1)) ax = 2;
+        else return ORSP_OK;  // not a unit planar step
+        if (axis[zu] == -1) axis[zu] = (int8_t)ax;
+        else if (axis[zu] != ax) return ORSP_OK;  // both axes on one layer
+        s = (dx + dy > 0) ? 0 : 1;  // entering v from its lower / upper neighbour
+      } else if (dx == 0 && dy == 0 && (dz == 1 || dz == -1)) {
+        s = dz > 0 ? 2 : 3;  // via from below / from above
+      } else {
+        return ORSP_OK;  // span > 1 or diagonal: not this lattice
+      }
+      int32_t &slotref = slot[(size_t)s * N + v];
+      if (slotref != -1) return ORSP_OK;  // parallel edges
+      slotref = k;
+    }
+  }
+  for (int z = 0; z < g->nz; ++z) g->layer_axis[z] = axis[z] < 0 ? 0 : axis[z];
+  ORSP_CUDA(cudaMalloc(&g->slot_eid, slot.size() * sizeof(int32_t)));
+  ORSP_CUDA(cudaMemcpy(g->slot_eid, slot.data(), slot.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  ORSP_CUDA(cudaMalloc(&g->wslot, slot.size() * sizeof(float)));
+  g->lattice_ok = true;
+  return ORSP_OK;
+}
+
+void free_lattice(Graph *g) {
+  cudaFree(g->slot_eid);
+  cudaFree(g->wslot);
+  cudaFree(g->lat_ws);
+  if (g->lat_ctl_h) cudaFreeHost(g->lat_ctl_h);
+  g->slot_eid = nullptr;
+  g->wslot = nullptr;
+  g->lat_ws = nullptr;
+  g->lat_ctl_h = nullptr;
+}
+
+// Full-lattice search (the box is the whole lattice).  Leaves the distances
+// in `dist`; finish_lattice_search reports the status after the stream sync.
+int run_lattice_search(Graph *g, const float *cost_d, int32_t nseeds, const int32_t *seeds_d,
+                       const float *seed_cost_d, uint32_t *dist, cudaStream_t st) {
+  const int64_t N = g->N;
+  gather_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 148 * 32), 256, 0, st>>>(
+      g->slot_eid, cost_d, (float4 *)g->wslot, N);
+  ORSP_CUDA(cudaGetLastError());
+  fill_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 148 * 32), 256, 0, st>>>(dist, N, ORSP_INF_BITS);
+  ORSP_CUDA(cudaGetLastError());
+  LatParams p{};
+  p.nx = g->nx;
+  p.ny = g->ny;
+  p.nz = g->nz;
+  p.bx0 = 0;
+  p.bx1 = g->nx - 1;
+  p.by0 = 0;
+  p.by1 = g->ny - 1;
+  p.bz0 = 0;
+  p.bz1 = g->nz - 1;
+  p.w4 = (const float4 *)g->wslot;
+  p.dist = dist;
+  for (int z = 0; z < 64; ++z) p.axis[z] = z < g->nz ? g->layer_axis[z] : 0;
+  const int tile = (int)env_u64("ORSP_LAT_TILE", 16);
+  if (tile == 32) return launch_lattice<32, 16>(g, p, nseeds, seeds_d, seed_cost_d, st);
+  return launch_lattice<16, 16>(g, p, nseeds, seeds_d, seed_cost_d, st);
+}
+
+int finish_lattice_search(Graph *g, int32_t *rounds_h) {
+  const LatCtl *c = (const LatCtl *)g->lat_ctl_h;
+  if (rounds_h) *rounds_h = (int32_t)c->rounds;
+  g_counters[0] = c->rounds;
+  g_counters[1] = c->visits;
+  g_counters[2] = (int64_t)c->cycles;
+  for (int i = 0; i < 4; ++i) g_counters[4 + i] = (int64_t)c->ns[i];
+  if (c->err) return dev_status_to_orsp(c->err);
+  return ORSP_OK;
+}
+
+}  // namespace orsp

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstdlib>
+#include <string>
 
 #include "common.cuh"
 
@@ -326,35 +327,36 @@ int ensure_single_ws(orsp::Graph *g, bool need_dist) {
   return ORSP_OK;
 }
 
-// Optional timing of the search kernel itself (CUDA events on the launching
-// stream), for roofline reporting.
-struct KernelTimer {
-  bool on = false;
-  bool pending = false;
-  cudaEvent_t a = nullptr, b = nullptr;
-  float last_ms = 0.0f;
-};
-KernelTimer g_timer;
-
 }  // namespace
 
+namespace orsp {
+KernelTimer g_timer;
+int64_t g_counters[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+}  // namespace orsp
+
 extern "C" int orsp_profile_enable(int on) {
-  if (on && !g_timer.a) {
-    ORSP_CUDA(cudaEventCreate(&g_timer.a));
-    ORSP_CUDA(cudaEventCreate(&g_timer.b));
+  if (on && !orsp::g_timer.a) {
+    ORSP_CUDA(cudaEventCreate(&orsp::g_timer.a));
+    ORSP_CUDA(cudaEventCreate(&orsp::g_timer.b));
   }
-  g_timer.on = on != 0;
+  orsp::g_timer.on = on != 0;
+  return ORSP_OK;
+}
+
+extern "C" int orsp_profile_counters(int64_t *out8) {
+  if (!out8) { orsp::set_error("NULL argument"); return ORSP_ERR_ARG; }
+  for (int i = 0; i < 8; ++i) out8[i] = orsp::g_counters[i];
   return ORSP_OK;
 }
 
 extern "C" int orsp_profile_last(float *kernel_ms) {
   if (!kernel_ms) { orsp::set_error("NULL argument"); return ORSP_ERR_ARG; }
-  if (g_timer.pending) {
-    ORSP_CUDA(cudaEventSynchronize(g_timer.b));
-    ORSP_CUDA(cudaEventElapsedTime(&g_timer.last_ms, g_timer.a, g_timer.b));
-    g_timer.pending = false;
+  if (orsp::g_timer.pending) {
+    ORSP_CUDA(cudaEventSynchronize(orsp::g_timer.b));
+    ORSP_CUDA(cudaEventElapsedTime(&orsp::g_timer.last_ms, orsp::g_timer.a, orsp::g_timer.b));
+    orsp::g_timer.pending = false;
   }
-  *kernel_ms = g_timer.last_ms;
+  *kernel_ms = orsp::g_timer.last_ms;
   return ORSP_OK;
 }
 
@@ -404,11 +406,11 @@ int run_grid_search(Graph *g, const float *cost_d, int32_t nseeds,
   }
   dim3 grid(g->num_sms * blocks_per_sm), block(512);
   void *args[] = {&p};
-  if (g_timer.on) ORSP_CUDA(cudaEventRecord(g_timer.a, st));
+  if (orsp::g_timer.on) ORSP_CUDA(cudaEventRecord(orsp::g_timer.a, st));
   ORSP_CUDA(cudaLaunchCooperativeKernel((void *)sssp_grid_kernel, grid, block, args, 0, st));
-  if (g_timer.on) {
-    ORSP_CUDA(cudaEventRecord(g_timer.b, st));
-    g_timer.pending = true;
+  if (orsp::g_timer.on) {
+    ORSP_CUDA(cudaEventRecord(orsp::g_timer.b, st));
+    orsp::g_timer.pending = true;
   }
   return ORSP_OK;
 }
@@ -434,9 +436,21 @@ extern "C" int orsp_sssp(orsp_graph *g, const float *cost_d, int32_t nseeds,
   int rc = ensure_single_ws(g, dist_out_d == nullptr);
   if (rc) return rc;
   uint32_t *dist = dist_out_d ? (uint32_t *)dist_out_d : g->dist;
-  rc = run_grid_search(g, cost_d, nseeds, seeds_d, seed_cost_d, dst, roi_map_d,
-                       nullptr, delta, dist, st);
-  if (rc) return rc;
+  // Full-graph searches on a recognised H/V lattice use the tile-sweep search
+  // (orsp_lattice.cu); ROI-restricted searches and other graphs use the
+  // generic near-far search.  ORSP_SSSP_IMPL=generic forces the latter.
+  const char *impl = getenv("ORSP_SSSP_IMPL");
+  const bool lattice = g->lattice_ok && roi_map_d == nullptr &&
+                       !(impl && std::string(impl) == "generic");
+  if (lattice) {
+    rc = run_lattice_search(g, cost_d, nseeds, seeds_d, seed_cost_d, dist, st);
+    if (rc) return rc;
+    ORSP_CUDA(cudaMemsetAsync(g->ctl, 0, sizeof(SsspCtl), st));
+  } else {
+    rc = run_grid_search(g, cost_d, nseeds, seeds_d, seed_cost_d, dst, roi_map_d,
+                         nullptr, delta, dist, st);
+    if (rc) return rc;
+  }
   if (dst >= 0) {
     BacktraceParams b{};
     b.cost = cost_d;
@@ -458,7 +472,12 @@ extern "C" int orsp_sssp(orsp_graph *g, const float *cost_d, int32_t nseeds,
   ORSP_CUDA(cudaMemcpyAsync(g->ctl_h, g->ctl, sizeof(SsspCtl), cudaMemcpyDeviceToHost, st));
   ORSP_CUDA(cudaStreamSynchronize(st));
   const SsspCtl *c = (const SsspCtl *)g->ctl_h;
-  if (rounds_h) *rounds_h = (int32_t)c->rounds;
+  if (lattice) {
+    rc = finish_lattice_search(g, rounds_h);
+    if (rc) return rc;
+  } else if (rounds_h) {
+    *rounds_h = (int32_t)c->rounds;
+  }
   if (c->err) return dev_status_to_orsp(c->err);
   if (dst >= 0) {
     *path_len_h = c->path_len;

@@ -119,9 +119,16 @@ def test_sssp_reference_lattice_duplicate_vias(golden):
         assert (p or []) == g[f"ref{k}_path"].tolist()
 
 
-@pytest.mark.parametrize("shape,blocked", [((60, 50, 6), 0.05), ((33, 17, 12), 0.0), ((128, 96, 4), 0.03)])
-def test_sssp_full_distances_bit_exact(shape, blocked):
-    lat = build_lattice(*shape)
+@pytest.mark.parametrize("impl", ["lattice16", "lattice32", "lattice16-rounds", "generic"])
+@pytest.mark.parametrize("shape,blocked,planar", [((60, 50, 6), 0.05, "all"), ((33, 17, 12), 0.0, "all"),
+                                                  ((128, 96, 4), 0.03, "all"), ((45, 70, 6), 0.02, "inner")])
+def test_sssp_full_distances_bit_exact(shape, blocked, planar, impl, monkeypatch):
+    """Full searches, both implementations (tile sweeps on the lattice, generic
+    near-far) and both tile sizes, bit-identical to the oracle."""
+    monkeypatch.setenv("ORSP_SSSP_IMPL", "generic" if impl == "generic" else "auto")
+    monkeypatch.setenv("ORSP_LAT_TILE", "32" if impl == "lattice32" else "16")
+    monkeypatch.setenv("ORSP_LAT_ASYNC", "0" if impl.endswith("rounds") else "1")
+    lat = build_lattice(*shape, planar=planar)
     w = uniform_weights(lat, seed=sum(shape), blocked_frac=blocked)
     dg = DeviceGraph.from_lattice(lat)
     wt = cuda(w)
