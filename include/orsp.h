@@ -189,6 +189,28 @@ ORSP_API int orsp_update_costs(int64_t E, const float *base_d, const float *pres
                       float via_mult, float base_w, int add_jitter,
                       float *total_out_d, uintptr_t stream);
 
+/* Live-usage costs for negotiation with a cost refresh after every net
+ * (classic PathFinder; the refresh the reference's
+ * EdgeAccountant.update_present_cost_only, UPF:1045-1068, is meant for):
+ *   total = ((base*via_mult)*base_w) + pres_fac*max(0, (usage+1) - cap)
+ *           + hist_w*history [+ fmodf((float)e, 9973)*1e-6]
+ * in the float32 order of update_costs, with present_ema replaced by the
+ * prospective usage.  edges_d == NULL refreshes all E edges; otherwise the
+ * n_edges listed ids (negative ids skipped). */
+ORSP_API int orsp_update_costs_live(int64_t E, const int32_t *edges_d, int64_t n_edges,
+                           const float *base_d, const int32_t *usage_d,
+                           const float *cap_d, const float *history_d, float pres_fac,
+                           float hist_w, float via_mult, float base_w, int add_jitter,
+                           float *total_out_d, uintptr_t stream);
+/* The same refresh over the path edges of a batch (rows of orsp_sssp_batch_bbox). */
+ORSP_API int orsp_update_costs_live_paths(int32_t K, const int32_t *path_edges_d,
+                                 const int32_t *path_len_d, int32_t path_cap,
+                                 const float *base_d, const int32_t *usage_d,
+                                 const float *cap_d, const float *history_d,
+                                 float pres_fac, float hist_w, float via_mult,
+                                 float base_w, int add_jitter, float *total_out_d,
+                                 uintptr_t stream);
+
 /* ema = beta*present + (1-beta)*ema  (EdgeAccountant.update_present_ema,
  * UPF:963-971); one_minus_beta is passed rounded as the caller computes it. */
 ORSP_API int orsp_update_present_ema(int64_t E, const float *present_d, float *ema_d,

@@ -38,7 +38,61 @@ def route_plain(lat, src, dst, cfg, base_cost=None, history_init=None, max_nets_
     pres_fac = cfg.pres_fac_init
     trace = []
     converged = False
+    net_policy = getattr(cfg, "cost_update", "iteration") == "net"
+    jitter = (np.arange(E, dtype=np.float32) % 9973 * np.float32(1e-6)) if cfg.add_jitter else None
+    adjusted = base * np.float32(cfg.via_cost_multiplier) * np.float32(cfg.base_cost_weight)
+
+    def live_cost(e):
+        """Live-usage cost of edges e (the GPU's orsp_update_costs_live)."""
+        over = np.maximum(np.float32(0), (usage[e].astype(np.float32) + np.float32(1)) - capacity[e])
+        t = (adjusted[e] + np.float32(pres_fac) * over) + np.float32(cfg.hist_cost_weight) * history[e]
+        if jitter is not None:
+            t = t + jitter[e]
+        return t.astype(np.float32)
+
     for it in range(1, cfg.max_iterations + 1):
+        if net_policy:
+            cost = live_cost(np.arange(E))
+            if it == 1 or cfg.reroute == "all":
+                idx = np.arange(M)
+            else:
+                over_e = usage.astype(np.float32) > capacity
+                idx = np.array([k for k in range(M) if len(net_paths[k]) < 2 or over_e[net_edges[k]].any()],
+                               dtype=np.int64)
+            for k in idx:  # sequential: rip up, search on live costs, commit
+                e = net_edges[k]
+                if e.size:
+                    np.subtract.at(usage, e, 1)
+                    np.maximum(usage, 0, out=usage)
+                    cost[e] = live_cost(e)
+                nodes, lens = O.batch_bbox(lat.indptr, lat.indices, cost, lat.nx, lat.ny, lat.nz, src[k:k + 1],
+                                           dst[k:k + 1], boxes[k:k + 1], cap_paths)
+                L = int(lens[0])
+                if L >= 2:
+                    p = nodes[0, :L].copy()
+                    en = O.path_to_edges(lat.indptr, lat.indices, p)
+                    net_paths[k] = p
+                    net_edges[k] = en
+                    np.add.at(usage, en, 1)
+                    cost[en] = live_cost(en)
+                else:
+                    net_paths[k] = np.zeros(0, np.int32)
+                    net_edges[k] = np.zeros(0, np.int32)
+            present = usage.astype(np.float32)
+            over_sum, over_cnt = O.compute_overuse(present, capacity)
+            failed = sum(1 for p in net_paths if len(p) < 2)
+            trace.append((over_sum, over_cnt, failed))
+            if over_sum == 0 and failed == 0:
+                converged = True
+                break
+            gain = cfg.hist_gain
+            if cfg.hist_gain_boost and it >= 8 and over_sum > 0:
+                gain = min(1.2, cfg.hist_gain * 1.25)
+            decay = cfg.history_decay if it >= cfg.history_decay_from else 1.0
+            history = O.update_history(history, present, capacity, gain, base_costs=base,
+                                       history_cap_multiplier=cfg.history_cap_multiplier, decay_factor=decay)
+            pres_fac = min(pres_fac * cfg.pres_fac_mult, cfg.pres_fac_max)
+            continue
         present = usage.astype(np.float32)
         if it == 1:
             present_ema = present.copy()

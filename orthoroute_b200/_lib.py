@@ -55,6 +55,10 @@ _SIGS = {
     "orsp_path_to_edges": (ctypes.c_int, [_P, _P, _i32, _P, ctypes.POINTER(_i32), _u]),
     "orsp_update_costs": (ctypes.c_int, [_i64, _P, _P, _P, _P, _P, _P, _P, _f32, _f32, _f32, _f32,
                                          ctypes.c_int, _P, _u]),
+    "orsp_update_costs_live": (ctypes.c_int, [_i64, _P, _i64, _P, _P, _P, _P, _f32, _f32, _f32, _f32,
+                                              ctypes.c_int, _P, _u]),
+    "orsp_update_costs_live_paths": (ctypes.c_int, [_i32, _P, _P, _i32, _P, _P, _P, _P, _f32, _f32, _f32,
+                                                    _f32, ctypes.c_int, _P, _u]),
     "orsp_update_present_ema": (ctypes.c_int, [_i64, _P, _P, _f32, _f32, _u]),
     "orsp_update_history": (ctypes.c_int, [_i64, _P, _P, _P, _P, _f32, _f32, _f32, _u]),
     "orsp_overuse": (ctypes.c_int, [_i64, _P, _P, _P, _P, _u]),

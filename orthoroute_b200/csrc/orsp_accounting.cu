@@ -58,6 +58,54 @@ __global__ void update_costs_kernel(int64_t E, const float *__restrict__ base,
   }
 }
 
+// Live-usage cost (classic PathFinder, the per-net refresh the reference's
+// EdgeAccountant.update_present_cost_only (UPF:1045-1068) is meant for):
+//   total = ((base*via_mult)*base_w) + pres_fac*max(0, (usage+1) - cap)
+//           + hist_w*history [+ jitter]
+// i.e. update_costs with present_ema replaced by the prospective usage if the
+// net being routed takes the edge.  Applied to every edge (edges == nullptr)
+// or to a list of edge ids (negative ids skipped; repeats are harmless).
+__device__ __forceinline__ float live_cost(int64_t e, const float *base, const int32_t *usage,
+                                           const float *cap, const float *hist, float pres_fac,
+                                           float hist_w, float via_mult, float base_w, int jitter) {
+  float over = __fsub_rn(__fadd_rn((float)usage[e], 1.0f), cap[e]);
+  over = over > 0.0f ? over : 0.0f;
+  const float adjusted = __fmul_rn(__fmul_rn(base[e], via_mult), base_w);
+  float total = __fadd_rn(__fadd_rn(adjusted, __fmul_rn(pres_fac, over)), __fmul_rn(hist_w, hist[e]));
+  if (jitter) total = __fadd_rn(total, __fmul_rn(fmodf(__ll2float_rn(e), 9973.0f), 1e-6f));
+  return total;
+}
+
+__global__ void live_costs_kernel(int64_t n, const int32_t *__restrict__ edges, const float *__restrict__ base,
+                                  const int32_t *__restrict__ usage, const float *__restrict__ cap,
+                                  const float *__restrict__ hist, float pres_fac, float hist_w,
+                                  float via_mult, float base_w, int jitter, float *__restrict__ out) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int64_t e = edges ? (int64_t)edges[i] : i;
+    if (e < 0) continue;
+    out[e] = live_cost(e, base, usage, cap, hist, pres_fac, hist_w, via_mult, base_w, jitter);
+  }
+}
+
+// Same over the paths of a batch (path_len[k]-1 edges of row k).
+__global__ void live_costs_paths_kernel(int32_t K, const int32_t *__restrict__ pe,
+                                        const int32_t *__restrict__ plen, int32_t cap_row,
+                                        const float *__restrict__ base, const int32_t *__restrict__ usage,
+                                        const float *__restrict__ cap, const float *__restrict__ hist,
+                                        float pres_fac, float hist_w, float via_mult, float base_w,
+                                        int jitter, float *__restrict__ out) {
+  for (int32_t k = blockIdx.x; k < K; k += gridDim.x) {
+    const int32_t len = plen[k];
+    if (len < 2) continue;
+    const int32_t ne = min(len - 1, cap_row);
+    for (int32_t i = threadIdx.x; i < ne; i += blockDim.x) {
+      const int32_t e = pe[(int64_t)k * cap_row + i];
+      if (e >= 0) out[e] = live_cost(e, base, usage, cap, hist, pres_fac, hist_w, via_mult, base_w, jitter);
+    }
+  }
+}
+
 // EdgeAccountant.update_present_ema (UPF:963-971).
 __global__ void ema_kernel(int64_t E, const float *__restrict__ present,
                            float *__restrict__ ema, float beta, float omb) {
@@ -368,5 +416,36 @@ extern "C" int orsp_path_to_edges(orsp_graph *g, const int32_t *path, int32_t le
   ORSP_CUDA(cudaMemcpyAsync(g->pinned, cnt_d, 4, cudaMemcpyDeviceToHost, st));
   ORSP_CUDA(cudaStreamSynchronize(st));
   *count_h = *(int32_t *)g->pinned;
+  return ORSP_OK;
+}
+
+extern "C" int orsp_update_costs_live(int64_t E, const int32_t *edges, int64_t n_edges,
+                                      const float *base, const int32_t *usage, const float *cap,
+                                      const float *hist, float pres_fac, float hist_w, float via_mult,
+                                      float base_w, int add_jitter, float *out, uintptr_t stream) {
+  if (E < 0 || !base || !usage || !cap || !hist || !out || (edges && n_edges < 0)) {
+    set_error("update_costs_live: NULL array or bad size");
+    return ORSP_ERR_ARG;
+  }
+  const int64_t n = edges ? n_edges : E;
+  if (n == 0) return ORSP_OK;
+  live_costs_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(n, edges, base, usage, cap, hist, pres_fac,
+                                                                  hist_w, via_mult, base_w, add_jitter, out);
+  ORSP_CUDA(cudaGetLastError());
+  return ORSP_OK;
+}
+
+extern "C" int orsp_update_costs_live_paths(int32_t K, const int32_t *pe, const int32_t *plen, int32_t cap_row,
+                                            const float *base, const int32_t *usage, const float *cap,
+                                            const float *hist, float pres_fac, float hist_w, float via_mult,
+                                            float base_w, int add_jitter, float *out, uintptr_t stream) {
+  if (K < 0 || cap_row <= 0 || (K > 0 && (!pe || !plen || !base || !usage || !cap || !hist || !out))) {
+    set_error("update_costs_live_paths: bad args");
+    return ORSP_ERR_ARG;
+  }
+  if (K == 0) return ORSP_OK;
+  live_costs_paths_kernel<<<std::min(K, 148 * 8), 128, 0, (cudaStream_t)stream>>>(
+      K, pe, plen, cap_row, base, usage, cap, hist, pres_fac, hist_w, via_mult, base_w, add_jitter, out);
+  ORSP_CUDA(cudaGetLastError());
   return ORSP_OK;
 }

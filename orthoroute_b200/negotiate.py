@@ -31,6 +31,22 @@ Heuristics of the reference loop that are not part of plain PathFinder (layer
 bias, via pooling, hotset sampling with random.seed, barrel-conflict
 penalties, stagnation rip-up) are not applied here; the accounting entry
 points for them exist in the library and are exercised by the tests.
+
+Cost policies (``NegotiationConfig.cost_update``):
+
+* ``"iteration"`` - the reference's: present_ema-based costs computed once per
+  iteration (above).  On the benchmark lattice this schedule oscillates and
+  does not reach zero overuse (neither does the reference's own loop).
+* ``"net"`` - classic PathFinder, the per-net refresh the reference's
+  EdgeAccountant.update_present_cost_only (UPF:1045-1068) is meant for: after
+  each net is ripped up or committed, the costs of the edges it touched are
+  recomputed from live usage, ``base*w + pres_fac*max(0, usage+1-cap) +
+  hist_w*history + jitter``, so every net sees the nets routed before it.  A
+  net's search reads only costs inside its box and its rip-up / commit touch
+  only edges inside its box, so nets whose boxes are pairwise disjoint see
+  exactly the sequential costs: batched mode launches one "level" of such
+  nets at a time (level(j) = 1 + max level of the earlier nets whose box
+  intersects j's), giving the sequential result bit for bit.
 """
 from __future__ import annotations
 
@@ -71,6 +87,7 @@ class NegotiationConfig:
     full_graph_retry: bool = True
     delta: Optional[float] = None
     path_cap: int = 4096
+    cost_update: str = "iteration"  # "iteration" (reference) | "net" (live usage)
 
 
 @dataclass
@@ -98,6 +115,23 @@ class RouteResult:
 
     def overuse_trace(self):
         return [(s.over_sum, s.over_cnt) for s in self.iterations]
+
+
+def level_schedule(boxes: np.ndarray) -> np.ndarray:
+    """level[j] = 1 + max(level[i] for i < j whose box intersects box j), 0
+    when none does; nets of one level have pairwise disjoint boxes and each
+    follows every earlier net it overlaps."""
+    M = len(boxes)
+    lv = np.zeros(M, dtype=np.int32)
+    if M == 0:
+        return lv
+    x0, x1, y0, y1, z0, z1 = (boxes[:, i] for i in range(6))
+    for j in range(1, M):
+        inter = ((x0[:j] <= x1[j]) & (x1[:j] >= x0[j]) & (y0[:j] <= y1[j]) & (y1[:j] >= y0[j])
+                 & (z0[:j] <= z1[j]) & (z1[:j] >= z0[j]))
+        if inter.any():
+            lv[j] = int(lv[:j][inter].max()) + 1
+    return lv
 
 
 class PathFinder:
@@ -188,6 +222,81 @@ class PathFinder:
             else:
                 net_lens[k] = 0
 
+    # ------------------------------------------------------------------ per-net costs
+    def _live(self, acc, pres_fac, edges=None, n=0):
+        cfg = self.cfg
+        check(_lib.load().orsp_update_costs_live(self.E, ptr(edges), int(n), ptr(self.base), ptr(acc.usage),
+                                                 ptr(acc.capacity), ptr(acc.history), float(pres_fac),
+                                                 float(cfg.hist_cost_weight), float(cfg.via_cost_multiplier),
+                                                 float(cfg.base_cost_weight), 1 if cfg.add_jitter else 0,
+                                                 ptr(acc.total_cost), _stream()), "orsp_update_costs_live")
+
+    def _live_paths(self, acc, pres_fac, edges, lens):
+        cfg = self.cfg
+        check(_lib.load().orsp_update_costs_live_paths(int(lens.numel()), ptr(edges), ptr(lens), int(edges.shape[1]),
+                                                       ptr(self.base), ptr(acc.usage), ptr(acc.capacity),
+                                                       ptr(acc.history), float(pres_fac), float(cfg.hist_cost_weight),
+                                                       float(cfg.via_cost_multiplier), float(cfg.base_cost_weight),
+                                                       1 if cfg.add_jitter else 0, ptr(acc.total_cost), _stream()),
+              "orsp_update_costs_live_paths")
+
+    def _route_net_sequential(self, acc, pres_fac, idx, src, dst, boxes, net_nodes, net_edges, net_lens, delta):
+        lib = _lib.load()
+        cap = self.cfg.path_cap
+        st = _stream()
+        cost = acc.total_cost
+        lens_h = net_lens.cpu().numpy()
+        for k in idx.cpu().tolist():
+            L = int(lens_h[k])
+            if L >= 2:
+                old = net_edges[k, : L - 1]
+                check(lib.orsp_commit_edges(L - 1, ptr(old), ptr(acc.usage), ptr(acc.present), -1, st),
+                      "orsp_commit_edges")
+                self._live(acc, pres_fac, old, L - 1)
+            g2r = self.roi.box_map(boxes[k])
+            status, path, _ = self.dg.sssp(cost, int(src[k]), int(dst[k]), roi_map=g2r, delta=delta, path_cap=cap)
+            if status == _lib.ORSP_OK and path is not None and path.numel() >= 2:
+                n = int(path.numel())
+                e = self.dg.path_to_edges(path)
+                net_nodes[k, :n] = path
+                net_edges[k, : n - 1] = e
+                net_lens[k] = n
+                lens_h[k] = n
+                check(lib.orsp_commit_edges(n - 1, ptr(e), ptr(acc.usage), ptr(acc.present), 1, st),
+                      "orsp_commit_edges")
+                self._live(acc, pres_fac, e, n - 1)
+            else:
+                net_lens[k] = 0
+                lens_h[k] = 0
+
+    def _route_net_batched(self, acc, pres_fac, idx, src_d, dst_d, boxes_d, boxes, order_levels, net_nodes,
+                           net_edges, net_lens, delta):
+        lib = _lib.load()
+        cap = self.cfg.path_cap
+        st = _stream()
+        cost = acc.total_cost
+        idx_h = idx.cpu().numpy()
+        lv = level_schedule(boxes[idx_h])
+        for L in range(int(lv.max()) + 1 if len(lv) else 0):
+            sel = torch.from_numpy(idx_h[lv == L]).to(self.device)
+            K = int(sel.numel())
+            old_e = net_edges[sel].contiguous()
+            old_l = net_lens[sel].contiguous()
+            check(lib.orsp_commit_batch(K, ptr(old_e), ptr(old_l), cap, ptr(acc.usage), ptr(acc.present), -1, st),
+                  "orsp_commit_batch")
+            self._live_paths(acc, pres_fac, old_e, old_l)
+            nodes, edges, lens = self.dg.batch_bbox(cost, src_d[sel].contiguous(), dst_d[sel].contiguous(),
+                                                    boxes_d[sel].contiguous(), delta=delta, path_cap=cap)
+            if K and int(lens.min().item()) < 0:
+                bad = lens[lens < 0]
+                raise _lib.OrspError(int(bad[0]), "orsp_sssp_batch_bbox", "per-search failure status")
+            net_nodes[sel] = nodes
+            net_edges[sel] = edges
+            net_lens[sel] = lens
+            check(lib.orsp_commit_batch(K, ptr(edges), ptr(lens), cap, ptr(acc.usage), ptr(acc.present), 1, st),
+                  "orsp_commit_batch")
+            self._live_paths(acc, pres_fac, edges, lens)
+
     # ------------------------------------------------------------------
     def route(self, src, dst, mode: str = "batched", history_init=None, callback=None) -> RouteResult:
         cfg = self.cfg
@@ -222,21 +331,37 @@ class PathFinder:
         pres_fac = cfg.pres_fac_init
         stats: List[IterationStats] = []
         converged = False
+        if cfg.cost_update not in ("iteration", "net"):
+            raise ValueError("cost_update must be 'iteration' or 'net'")
+        net_policy = cfg.cost_update == "net"
+        if net_policy and cfg.roi != "bbox":
+            raise ValueError("per-net costs are implemented for box ROIs")
+        acc.total_cost = torch.empty(self.E, dtype=torch.float32, device=dev)
         for it in range(1, cfg.max_iterations + 1):
             t_it = time.perf_counter()
             acc.refresh_from_canonical()
-            if it == 1:
-                acc.present_ema.copy_(acc.present)
-            acc.update_present_ema(beta=cfg.present_ema_beta)
-            acc.update_costs(self.base, pres_fac, cfg.hist_cost_weight, add_jitter=cfg.add_jitter,
-                             via_cost_multiplier=cfg.via_cost_multiplier, base_cost_weight=cfg.base_cost_weight)
+            if net_policy:
+                self._live(acc, pres_fac)
+            else:
+                if it == 1:
+                    acc.present_ema.copy_(acc.present)
+                acc.update_present_ema(beta=cfg.present_ema_beta)
+                acc.update_costs(self.base, pres_fac, cfg.hist_cost_weight, add_jitter=cfg.add_jitter,
+                                 via_cost_multiplier=cfg.via_cost_multiplier, base_cost_weight=cfg.base_cost_weight)
             cost = acc.total_cost
             delta = cfg.delta if cfg.delta is not None else DeviceGraph.default_delta(cost)
             if it == 1 or cfg.reroute == "all":
                 idx = all_idx
             else:
                 idx = self._offenders(acc, net_edges, net_lens, all_idx)
-            if idx.numel() > 0:
+            if idx.numel() > 0 and net_policy:
+                if mode == "batched":
+                    self._route_net_batched(acc, pres_fac, idx, src_d, dst_d, boxes_d, boxes, order_rank, net_nodes,
+                                            net_edges, net_lens, delta)
+                else:
+                    self._route_net_sequential(acc, pres_fac, idx, src, dst, boxes, net_nodes, net_edges, net_lens,
+                                               delta)
+            elif idx.numel() > 0:
                 if mode == "batched":
                     self._route_batched(acc, cost, idx, src_d, dst_d, boxes_d, full_box_d, order_rank, net_nodes,
                                         net_edges, net_lens, delta)
