@@ -604,7 +604,7 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int32_t nseeds, const int32_t *
     orsp::set_error("lattice search: kernel does not fit on an SM");
     return ORSP_ERR_ARG;
   }
-  const int want = (int)env_u64("ORSP_LAT_BLOCKS_PER_SM", 4);
+  const int want = (int)env_u64("ORSP_LAT_BLOCKS_PER_SM", 1);
   const int bps = std::max(1, std::min(occ, want));
   p.max_rounds = (unsigned)std::min<unsigned long long>(64ull * (unsigned long long)ntiles + 4096ull, 1ull << 30);
   p.wait_ns = env_u64("ORSP_WAIT_NS", 2000000000ull);
