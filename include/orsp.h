@@ -111,6 +111,29 @@ ORSP_API int orsp_sssp(orsp_graph *g, const float *cost_d, int32_t nseeds,
               int32_t *path_out_d, int32_t path_cap, int32_t *path_len_h,
               int32_t *rounds_h, uintptr_t stream);
 
+/* Multi-seed / multi-target search with portal costs, as
+ * SimpleDijkstra.find_path_multisource_multisink (UPF:1889-1989): seeds start
+ * at seed_cost (NULL = 0.0), the search runs to completion inside the ROI,
+ * targets are settled but never expanded, and the target with the smallest
+ * (double)d[t] + target_cost[t] wins (equal totals: the one settled first,
+ * i.e. smallest (d[t], rank)).  Targets must be distinct.  The path runs from
+ * a seed to the winning target (best_target_h, optional).  Also serves
+ * CUDADijkstra.find_path_fullgraph_gpu_seeds (CD:5467-5751) with zero costs;
+ * unlike that wavefront (which stops at the first target it reaches) the
+ * answer is the exact shortest one. */
+ORSP_API int orsp_sssp_multi(orsp_graph *g, const float *cost_d, int32_t nseeds,
+                    const int32_t *seeds_d, const float *seed_cost_d,
+                    int32_t ntargets, const int32_t *targets_d,
+                    const double *target_cost_d, const int32_t *roi_map_d,
+                    float delta, int32_t *path_out_d, int32_t path_cap,
+                    int32_t *path_len_h, int32_t *best_target_h, uintptr_t stream);
+
+/* global_to_roi from an allowed-node bitmap (uint32 words, bit v%32 of word
+ * v/32 set = allowed), rank = node id: the allowed_bitmap of
+ * find_path_fullgraph_gpu_seeds (CD:5467) as a roi_map. */
+ORSP_API int orsp_roi_from_bitmap(orsp_graph *g, const uint32_t *bitmap_d, int32_t *g2r_d,
+                         uintptr_t stream);
+
 /* ---- batched searches (one launch, one CTA per search) ----------------- */
 /* K independent searches on shared fp32 costs, each inside an axis-aligned
  * box ROI (inclusive bounds x0,x1,y0,y1,z0,z1 per search in bbox_d[6*K]).
@@ -128,6 +151,20 @@ ORSP_API int orsp_sssp_batch_bbox(orsp_graph *g, const float *cost_d, int32_t K,
                          float delta, int32_t *path_nodes_d,
                          int32_t *path_edges_d, int32_t path_cap,
                          int32_t *path_len_d, uintptr_t stream);
+
+/* The same batched search with node-range ROIs: search k stays inside nodes
+ * [ranges[2k], ranges[2k+1]) and ranks nodes by id - ranges[2k].  Built for
+ * graphs made of concatenated ROI-local CSRs - the 13-tuple batch of
+ * CUDADijkstra.find_paths_on_rois (CD:2014-2086, tuple format CD:55-91),
+ * where every ROI is its own block of node ids and the local order is the
+ * ROI index order.  src/dst and the returned paths are global ids of the
+ * concatenated graph. */
+ORSP_API int orsp_sssp_batch_ranges(orsp_graph *g, const float *cost_d, int32_t K,
+                           const int32_t *src_d, const int32_t *dst_d,
+                           const int32_t *ranges_d, const int32_t *order_d,
+                           float delta, int32_t *path_nodes_d,
+                           int32_t *path_edges_d, int32_t path_cap,
+                           int32_t *path_len_d, uintptr_t stream);
 
 /* ---- ROI extraction ---------------------------------------------------- */
 /* Bidirectional level-synchronous BFS ROI, as ROIExtractor.extract_roi_bfs
@@ -210,6 +247,49 @@ ORSP_API int orsp_update_costs_live_paths(int32_t K, const int32_t *path_edges_d
                                  float pres_fac, float hist_w, float via_mult,
                                  float base_w, int add_jitter, float *total_out_d,
                                  uintptr_t stream);
+
+/* ---- via pooling (column / segment capacity of via barrels) ------------ */
+/* Arrays use the reference's C order [Nx][Ny] and [Nx][Ny][segZ] with
+ * segZ = Nz - 2 (segment z -> z+1 at index z-1); usage and capacities are
+ * int32 (int16 / int8 in the reference).  Via edges are the CSR edges whose
+ * endpoints lie on different layers; their z range is clamped to 1..Nz-2
+ * (_build_via_edge_metadata, UPF:5389-5461). */
+
+/* Adds the via usage of the batch paths (path_len[k] nodes in row k) to
+ * col_use / seg_use (either may be NULL), as _accumulate_via_usage_for_path
+ * (UPF:2678-2724) does for every committed path in
+ * _rebuild_via_usage_from_committed (UPF:2726-2762).  The caller zeroes the
+ * arrays first. */
+ORSP_API int orsp_via_usage(orsp_graph *g, int32_t K, const int32_t *path_nodes_d,
+                   const int32_t *path_len_d, int32_t path_cap, int32_t *col_use_d,
+                   int32_t *seg_use_d, uintptr_t stream);
+/* pres = alpha*max(0, use-cap) + beta*pres for columns and segments, and the
+ * float32 running sum of seg_pres along z into seg_prefix (UPF:3622-3633;
+ * alpha 0.6, beta 0.4 by default).  A NULL pres array skips that part. */
+ORSP_API int orsp_via_present(int64_t ncol, int32_t segz, const int32_t *col_use_d,
+                     const int32_t *col_cap_d, float *col_pres_d,
+                     const int32_t *seg_use_d, const int32_t *seg_cap_d,
+                     float *seg_pres_d, float *seg_prefix_d, float alpha, float beta,
+                     uintptr_t stream);
+/* total[e] += pres_fac*penalty(e) on via edges with penalty > 0, penalty =
+ * (col_weight*col_pres[x][y] + seg_weight*(prefix[z_hi-2] - prefix[z_lo-2]))
+ * times the leave-hot-layer factor (1 - k*bias[z_lo])*(1 + 0.5*k*bias[z_hi])
+ * when layer_bias_d is given; bias_f64 selects the float32 or float64
+ * arithmetic the reference uses for that factor (its layer_bias array starts
+ * as float32 and becomes float64 after the first bias update).  As
+ * _apply_via_pooling_penalties (UPF:3243-3387). */
+ORSP_API int orsp_via_penalties(orsp_graph *g, const float *col_pres_d,
+                       const float *seg_prefix_d, const double *layer_bias_d,
+                       int bias_f64, double hot_layer_discount, float col_weight,
+                       float seg_weight, float pres_fac, float *total_cost_d,
+                       uintptr_t stream);
+/* total[e] = +inf on via edges whose column is at capacity or any of whose
+ * spanned segments is at capacity (_block_via_edges_with_collisions,
+ * UPF:3448-3546). */
+ORSP_API int orsp_via_hard_block(orsp_graph *g, const int32_t *col_use_d,
+                        const int32_t *col_cap_d, const int32_t *seg_use_d,
+                        const int32_t *seg_cap_d, float *total_cost_d,
+                        uintptr_t stream);
 
 /* ema = beta*present + (1-beta)*ema  (EdgeAccountant.update_present_ema,
  * UPF:963-971); one_minus_beta is passed rounded as the caller computes it. */

@@ -14,4 +14,9 @@ from .orsp_oracle import (  # noqa: F401
     update_present_ema,
     update_history,
     compute_overuse,
+    via_edge_metadata,
+    via_usage,
+    via_present,
+    via_penalties,
+    via_hard_block,
 )

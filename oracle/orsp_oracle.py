@@ -192,3 +192,102 @@ def compute_overuse(present, capacity):
     """EdgeAccountant.compute_overuse (UPF:838-876), edge part."""
     edge_over = np.maximum(0, present - capacity)
     return int(edge_over.sum()), int((edge_over > 0).sum())
+
+
+# ---------------------------------------------------------------------------
+# Via pooling restatements (UPF:2678-2724, 3243-3387, 3448-3546, 5389-5461)
+# ---------------------------------------------------------------------------
+
+def via_edge_metadata(indptr, indices, nx, ny, nz):
+    """(edge ids, x, y, z_lo, z_hi) of via edges (different layers), z range
+    clamped to 1..nz-2, ascending edge id (_build_via_edge_metadata)."""
+    indptr = np.asarray(indptr)
+    indices = np.asarray(indices)
+    plane = nx * ny
+    src = np.repeat(np.arange(len(indptr) - 1), np.diff(indptr))
+    zu = src // plane
+    zv = indices // plane
+    e = np.nonzero(zu != zv)[0]
+    u = src[e]
+    x = (u % plane) % nx
+    y = (u % plane) // nx
+    z_lo = np.clip(np.minimum(zu[e], zv[e]), 1, nz - 2)
+    z_hi = np.clip(np.maximum(zu[e], zv[e]), 1, nz - 2)
+    return e.astype(np.int32), x, y, z_lo, z_hi
+
+
+def via_usage(paths, nx, ny, nz, col_use, seg_use):
+    """Adds the via usage of node paths (_accumulate_via_usage_for_path)."""
+    plane = nx * ny
+    segz = max(nz - 2, 0)
+    for path in paths:
+        for u, v in zip(path, path[1:]):
+            zu, ru = divmod(int(u), plane)
+            zv, rv = divmod(int(v), plane)
+            if ru != rv or zu == zv:
+                continue
+            x, y = ru % nx, ru // nx
+            if col_use is not None:
+                col_use[x, y] += 1
+            if seg_use is not None:
+                lo = max(1, min(min(zu, zv), nz - 2))
+                hi = max(1, min(max(zu, zv), nz - 2))
+                for z in range(lo, hi):
+                    if 0 <= z - 1 < segz:
+                        seg_use[x, y, z - 1] += 1
+
+
+def via_present(col_use, col_cap, col_pres, seg_use, seg_cap, seg_pres, alpha=0.6, beta=0.4):
+    """Smoothed via present costs and the z prefix (UPF:3622-3633)."""
+    over = np.maximum(0, col_use - col_cap).astype(np.float32)
+    col_pres = alpha * over + beta * col_pres
+    over = np.maximum(0, seg_use - seg_cap).astype(np.float32)
+    seg_pres = alpha * over + beta * seg_pres
+    seg_prefix = np.cumsum(seg_pres, axis=2).astype(np.float32)
+    return col_pres.astype(np.float32), seg_pres.astype(np.float32), seg_prefix
+
+
+def via_penalties(total, meta, col_pres, seg_prefix, segz, layer_bias, pres_fac, col_weight=1.0,
+                  seg_weight=1.0, k=0.20):
+    """_apply_via_pooling_penalties, vectorised CPU path (UPF:3296-3380);
+    layer_bias keeps its dtype (float32 or float64) like the reference's."""
+    e, x, y, z_lo, z_hi = meta
+    total = total.copy()
+    pen = np.zeros(len(e), dtype=np.float32)
+    if col_pres is not None:
+        pen += col_weight * col_pres[x, y]
+    if seg_prefix is not None:
+        hi = z_hi - 2
+        lo = z_lo - 2
+        valid = z_hi > z_lo
+        hv = (hi >= 0) & (hi < segz)
+        lv = (lo >= 0) & (lo < segz)
+        ph = np.zeros(len(e), dtype=np.float32)
+        pl = np.zeros(len(e), dtype=np.float32)
+        ph[hv] = seg_prefix[x[hv], y[hv], hi[hv]]
+        pl[lv] = seg_prefix[x[lv], y[lv], lo[lv]]
+        pen += seg_weight * ((ph - pl) * valid)
+    if layer_bias is not None:
+        sb = layer_bias[z_lo]
+        db = layer_bias[z_hi]
+        pen *= (1.0 - k * np.maximum(sb, 0.0)) * (1.0 + 0.5 * k * np.maximum(db, 0.0))
+    m = pen > 0
+    total[e[m]] += pres_fac * pen[m]
+    return total
+
+
+def via_hard_block(total, meta, col_use, col_cap, seg_use, seg_cap, segz):
+    """_block_via_edges_with_collisions, CPU path (UPF:3499-3546)."""
+    e, x, y, z_lo, z_hi = meta
+    total = total.copy()
+    for i in range(len(e)):
+        xi, yi = int(x[i]), int(y[i])
+        blocked = col_use is not None and col_use[xi, yi] >= col_cap[xi, yi]
+        if not blocked and seg_use is not None:
+            for z in range(int(z_lo[i]), int(z_hi[i])):
+                if 0 <= z - 1 < segz and seg_use[xi, yi, z - 1] >= seg_cap[xi, yi, z - 1]:
+                    blocked = True
+                    break
+        if blocked:
+            total[e[i]] = np.float32("inf")
+    return total

@@ -48,7 +48,11 @@ _SIGS = {
     "orsp_graph_max_degree": (ctypes.c_int, [_P, ctypes.POINTER(_i32)]),
     "orsp_sssp": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _f32, _P, _P, _i32,
                                  ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
+    "orsp_sssp_multi": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _P, _P, _f32, _P, _i32,
+                                       ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
+    "orsp_roi_from_bitmap": (ctypes.c_int, [_P, _P, _P, _u]),
     "orsp_sssp_batch_bbox": (ctypes.c_int, [_P, _P, _i32, _P, _P, _P, _P, _f32, _P, _P, _i32, _P, _u]),
+    "orsp_sssp_batch_ranges": (ctypes.c_int, [_P, _P, _i32, _P, _P, _P, _P, _f32, _P, _P, _i32, _P, _u]),
     "orsp_roi_bfs": (ctypes.c_int, [_P, _i32, _i32, _i32, _i32, _P, _P, ctypes.POINTER(_i32), _u]),
     "orsp_roi_bfs_noalloc": (ctypes.c_int, [_P, _i32, _i32, _i32, _i32, _P, _P, ctypes.POINTER(_i32), _u]),
     "orsp_roi_box_map": (ctypes.c_int, [_P, _P, _P, _u]),
@@ -59,6 +63,10 @@ _SIGS = {
                                               ctypes.c_int, _P, _u]),
     "orsp_update_costs_live_paths": (ctypes.c_int, [_i32, _P, _P, _i32, _P, _P, _P, _P, _f32, _f32, _f32,
                                                     _f32, ctypes.c_int, _P, _u]),
+    "orsp_via_usage": (ctypes.c_int, [_P, _i32, _P, _P, _i32, _P, _P, _u]),
+    "orsp_via_present": (ctypes.c_int, [_i64, _i32, _P, _P, _P, _P, _P, _P, _P, _f32, _f32, _u]),
+    "orsp_via_penalties": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int, ctypes.c_double, _f32, _f32, _f32, _P, _u]),
+    "orsp_via_hard_block": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _u]),
     "orsp_update_present_ema": (ctypes.c_int, [_i64, _P, _P, _f32, _f32, _u]),
     "orsp_update_history": (ctypes.c_int, [_i64, _P, _P, _P, _P, _f32, _f32, _f32, _u]),
     "orsp_overuse": (ctypes.c_int, [_i64, _P, _P, _P, _P, _u]),

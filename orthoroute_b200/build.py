@@ -24,6 +24,7 @@ SOURCES = [
     "orsp_accounting.cu",
     "orsp_roi.cu",
     "orsp_lattice.cu",
+    "orsp_via.cu",
 ]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]

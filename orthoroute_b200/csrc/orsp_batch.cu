@@ -41,6 +41,7 @@ struct BatchParams {
   FastDiv div_nx, div_plane;
   int32_t K;
   const int32_t *src, *dst, *bbox, *order;
+  int range_mode;  // bbox holds [lo, hi) node ranges (2 per search) instead of boxes
   int32_t *path_nodes, *path_edges, *path_len;
   int32_t path_cap;
   char *ws;
@@ -52,14 +53,24 @@ struct BatchParams {
   unsigned long long budget_ns;
 };
 
+// A search's ROI: an inclusive lattice box (local id = row-major position in
+// the box), or a node-id range [lo, lo+V) of a graph made of concatenated
+// ROI-local CSRs (local id = node - lo).  Both orders follow the global id.
 struct Box {
   int32_t x0, y0, z0, W, H, D;
   FastDiv dw, dwh;
   int32_t V;
+  int32_t lo;    // range mode: first node
+  bool range;
 };
 
 __device__ __forceinline__ bool box_local(const BatchParams &p, const Box &b, int32_t gid,
                                           int32_t *lid) {
+  if (b.range) {
+    if (gid < b.lo || gid - b.lo >= b.V) return false;
+    *lid = gid - b.lo;
+    return true;
+  }
   const uint32_t z = p.div_plane.div((uint32_t)gid);
   const uint32_t rem = (uint32_t)gid - z * (uint32_t)(p.nx * p.ny);
   const uint32_t y = p.div_nx.div(rem);
@@ -71,6 +82,7 @@ __device__ __forceinline__ bool box_local(const BatchParams &p, const Box &b, in
 }
 
 __device__ __forceinline__ int32_t box_global(const BatchParams &p, const Box &b, int32_t lid) {
+  if (b.range) return b.lo + lid;
   const uint32_t lz = b.dwh.div((uint32_t)lid);
   const uint32_t r = (uint32_t)lid - lz * (uint32_t)(b.W * b.H);
   const uint32_t ly = b.dw.div(r);
@@ -301,17 +313,31 @@ __global__ void __launch_bounds__(BATCH_THREADS) batch_bbox_kernel(BatchParams p
     __syncthreads();
     if (it >= p.K) break;
     const int k = p.order ? p.order[it] : it;
-    const int32_t *bb = p.bbox + 6 * (int64_t)k;
     Box b;
-    b.x0 = bb[0];
-    b.y0 = bb[2];
-    b.z0 = bb[4];
-    b.W = bb[1] - bb[0] + 1;
-    b.H = bb[3] - bb[2] + 1;
-    b.D = bb[5] - bb[4] + 1;
-    b.V = b.W * b.H * b.D;
-    b.dw.init((uint32_t)b.W);
-    b.dwh.init((uint32_t)(b.W * b.H));
+    if (p.range_mode) {
+      const int32_t *rg = p.bbox + 2 * (int64_t)k;
+      b.range = true;
+      b.lo = rg[0];
+      b.V = rg[1] - rg[0];
+      b.x0 = b.y0 = b.z0 = 0;
+      b.W = b.V;
+      b.H = b.D = 1;
+      b.dw.init(1u);
+      b.dwh.init(1u);
+    } else {
+      const int32_t *bb = p.bbox + 6 * (int64_t)k;
+      b.range = false;
+      b.lo = 0;
+      b.x0 = bb[0];
+      b.y0 = bb[2];
+      b.z0 = bb[4];
+      b.W = bb[1] - bb[0] + 1;
+      b.H = bb[3] - bb[2] + 1;
+      b.D = bb[5] - bb[4] + 1;
+      b.V = b.W * b.H * b.D;
+      b.dw.init((uint32_t)b.W);
+      b.dwh.init((uint32_t)(b.W * b.H));
+    }
     const int32_t src = p.src[k], dst = p.dst[k];
     int32_t src_l = -1, dst_l = -1;
     int32_t *nodes = p.path_nodes + (int64_t)k * p.path_cap;
@@ -354,36 +380,45 @@ int env_int(const char *name, int dflt) {
 
 using namespace orsp;
 
-extern "C" int orsp_sssp_batch_bbox(orsp_graph *g, const float *cost_d, int32_t K,
-                                    const int32_t *src_d, const int32_t *dst_d,
-                                    const int32_t *bbox_d, const int32_t *order_d,
-                                    float delta, int32_t *path_nodes_d,
-                                    int32_t *path_edges_d, int32_t path_cap,
-                                    int32_t *path_len_d, uintptr_t stream) {
+static int run_batch(orsp_graph *g, const float *cost_d, int32_t K, const int32_t *src_d,
+                     const int32_t *dst_d, const int32_t *bbox_d, int range_mode,
+                     const int32_t *order_d, float delta, int32_t *path_nodes_d,
+                     int32_t *path_edges_d, int32_t path_cap, int32_t *path_len_d,
+                     uintptr_t stream) {
   if (!g || !cost_d || K < 0 || (K > 0 && (!src_d || !dst_d || !bbox_d || !path_nodes_d ||
                                            !path_len_d)) || path_cap <= 0) {
-    set_error("batch_bbox: NULL argument or path_cap <= 0");
+    set_error("batch search: NULL argument or path_cap <= 0");
     return ORSP_ERR_ARG;
   }
-  if (g->nx <= 0) { set_error("batch_bbox: graph was created without lattice dims"); return ORSP_ERR_ARG; }
+  if (!range_mode && g->nx <= 0) { set_error("batch_bbox: graph was created without lattice dims"); return ORSP_ERR_ARG; }
   if (!(delta > 0.0f) || !(delta < 3.0e38f)) { set_error("delta must be finite and > 0"); return ORSP_ERR_ARG; }
   if (K == 0) return ORSP_OK;
   ORSP_CUDA(cudaSetDevice(g->device));
   cudaStream_t st = (cudaStream_t)stream;
 
-  // Box volumes are needed on the host to size the per-CTA slots.
-  std::vector<int32_t> bb((size_t)6 * K);
+  // ROI sizes are needed on the host to size the per-CTA slots.
+  const int per = range_mode ? 2 : 6;
+  std::vector<int32_t> bb((size_t)per * K);
   ORSP_CUDA(cudaMemcpyAsync(bb.data(), bbox_d, bb.size() * 4, cudaMemcpyDeviceToHost, st));
   ORSP_CUDA(cudaStreamSynchronize(st));
   int64_t vmax = 1;
   for (int32_t k = 0; k < K; ++k) {
-    const int32_t *b = &bb[(size_t)6 * k];
-    if (b[0] < 0 || b[2] < 0 || b[4] < 0 || b[1] >= g->nx || b[3] >= g->ny || b[5] >= g->nz ||
-        b[1] < b[0] || b[3] < b[2] || b[5] < b[4]) {
-      set_error("batch_bbox: box outside the lattice or empty");
-      return ORSP_ERR_ARG;
+    const int32_t *b = &bb[(size_t)per * k];
+    int64_t v;
+    if (range_mode) {
+      if (b[0] < 0 || b[1] > g->N || b[1] <= b[0]) {
+        set_error("batch_ranges: node range outside the graph or empty");
+        return ORSP_ERR_ARG;
+      }
+      v = (int64_t)b[1] - b[0];
+    } else {
+      if (b[0] < 0 || b[2] < 0 || b[4] < 0 || b[1] >= g->nx || b[3] >= g->ny || b[5] >= g->nz ||
+          b[1] < b[0] || b[3] < b[2] || b[5] < b[4]) {
+        set_error("batch_bbox: box outside the lattice or empty");
+        return ORSP_ERR_ARG;
+      }
+      v = (int64_t)(b[1] - b[0] + 1) * (b[3] - b[2] + 1) * (b[5] - b[4] + 1);
     }
-    const int64_t v = (int64_t)(b[1] - b[0] + 1) * (b[3] - b[2] + 1) * (b[5] - b[4] + 1);
     vmax = std::max(vmax, v);
   }
 
@@ -416,11 +451,12 @@ extern "C" int orsp_sssp_batch_bbox(orsp_graph *g, const float *cost_d, int32_t 
   p.nx = g->nx;
   p.ny = g->ny;
   p.nz = g->nz;
-  p.div_nx.init((uint32_t)g->nx);
-  p.div_plane.init((uint32_t)(g->nx * g->ny));
+  p.div_nx.init((uint32_t)std::max(1, g->nx));
+  p.div_plane.init((uint32_t)std::max(1, g->nx * g->ny));
   p.src = src_d;
   p.dst = dst_d;
   p.bbox = bbox_d;
+  p.range_mode = range_mode;
   p.path_nodes = path_nodes_d;
   p.path_edges = path_edges_d;
   p.path_len = path_len_d;
@@ -476,4 +512,24 @@ extern "C" int orsp_sssp_batch_bbox(orsp_graph *g, const float *cost_d, int32_t 
   }
   ORSP_CUDA(cudaStreamSynchronize(st));
   return ORSP_OK;
+}
+
+extern "C" int orsp_sssp_batch_bbox(orsp_graph *g, const float *cost_d, int32_t K,
+                                    const int32_t *src_d, const int32_t *dst_d,
+                                    const int32_t *bbox_d, const int32_t *order_d,
+                                    float delta, int32_t *path_nodes_d,
+                                    int32_t *path_edges_d, int32_t path_cap,
+                                    int32_t *path_len_d, uintptr_t stream) {
+  return run_batch(g, cost_d, K, src_d, dst_d, bbox_d, 0, order_d, delta, path_nodes_d, path_edges_d,
+                   path_cap, path_len_d, stream);
+}
+
+extern "C" int orsp_sssp_batch_ranges(orsp_graph *g, const float *cost_d, int32_t K,
+                                      const int32_t *src_d, const int32_t *dst_d,
+                                      const int32_t *ranges_d, const int32_t *order_d,
+                                      float delta, int32_t *path_nodes_d,
+                                      int32_t *path_edges_d, int32_t path_cap,
+                                      int32_t *path_len_d, uintptr_t stream) {
+  return run_batch(g, cost_d, K, src_d, dst_d, ranges_d, 1, order_d, delta, path_nodes_d, path_edges_d,
+                   path_cap, path_len_d, stream);
 }

@@ -224,6 +224,7 @@ struct BacktraceParams {
   const float *seed_cost;
   int32_t nseeds;
   int32_t dst;
+  const int32_t *dst_d;  // when set, the target is read here (< 0: no path)
   int32_t *path_out;
   int32_t path_cap;
   SsspCtl *ctl;
@@ -238,12 +239,13 @@ __global__ void backtrace_kernel(BacktraceParams p) {
   const int lane = threadIdx.x & 31;
   SsspCtl *ctl = p.ctl;
   if (ctl->err) return;
-  unsigned dv = p.dist[p.dst];
+  const int32_t dst = p.dst_d ? *p.dst_d : p.dst;
+  unsigned dv = dst >= 0 ? p.dist[dst] : ORSP_INF_BITS;
   if (dv == ORSP_INF_BITS) {
     if (lane == 0) { ctl->path_len = 0; ctl->status = 1; }
     return;
   }
-  int v = p.dst;
+  int v = dst;
   int len = 0;
   int err = 0;
   for (;;) {
@@ -298,6 +300,53 @@ __global__ void backtrace_kernel(BacktraceParams p) {
     p.path_out[len - 1 - i] = a;
   }
   if (lane == 0) { ctl->path_len = len; ctl->status = 0; }
+}
+
+// Multi-sink winner, as find_path_multisource_multisink (UPF:1941-1975): the
+// target with the smallest (double)d[t] + target_cost; among equal totals the
+// one the heap pops first, i.e. the smallest (d[t], rank(t)).  One block.
+__global__ void pick_target_kernel(const uint32_t *dist, const int32_t *roi_map, int32_t nt,
+                                   const int32_t *targets, const double *tcost, int32_t N, int32_t *best) {
+  __shared__ double s_tot[256];
+  __shared__ unsigned long long s_key[256];
+  __shared__ int s_t[256];
+  double tot = __longlong_as_double(0x7ff0000000000000ll);
+  unsigned long long key = ULLONG_MAX;
+  int bt = -1;
+  for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+    const int t = targets[i];
+    if (t < 0 || t >= N) continue;
+    const int rank = roi_map ? roi_map[t] : t;
+    if (rank < 0) continue;
+    const unsigned d = dist[t];
+    if (d == ORSP_INF_BITS) continue;
+    const double c = (double)bits_f(d) + (tcost ? tcost[i] : 0.0);
+    const unsigned long long k = ((unsigned long long)d << 32) | (unsigned)rank;
+    if (c < tot || (c == tot && k < key)) { tot = c; key = k; bt = t; }
+  }
+  s_tot[threadIdx.x] = tot;
+  s_key[threadIdx.x] = key;
+  s_t[threadIdx.x] = bt;
+  __syncthreads();
+  for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+    if (threadIdx.x < off) {
+      const int j = threadIdx.x + off;
+      if (s_tot[j] < s_tot[threadIdx.x] || (s_tot[j] == s_tot[threadIdx.x] && s_key[j] < s_key[threadIdx.x])) {
+        s_tot[threadIdx.x] = s_tot[j];
+        s_key[threadIdx.x] = s_key[j];
+        s_t[threadIdx.x] = s_t[j];
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *best = s_t[0];
+}
+
+__global__ void mark_kernel(uint8_t *mask, int32_t n, const int32_t *nodes, int32_t N, uint8_t v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int t = nodes[i];
+    if (t >= 0 && t < N) mask[t] = v;
+  }
 }
 
 unsigned long long env_u64(const char *name, unsigned long long dflt) {
@@ -486,5 +535,80 @@ extern "C" int orsp_sssp(orsp_graph *g, const float *cost_d, int32_t nseeds,
       return ORSP_NO_PATH;
     }
   }
+  return ORSP_OK;
+}
+
+extern "C" int orsp_sssp_multi(orsp_graph *g, const float *cost_d, int32_t nseeds, const int32_t *seeds_d,
+                               const float *seed_cost_d, int32_t ntargets, const int32_t *targets_d,
+                               const double *target_cost_d, const int32_t *roi_map_d, float delta,
+                               int32_t *path_out_d, int32_t path_cap, int32_t *path_len_h,
+                               int32_t *best_target_h, uintptr_t stream) {
+  if (!g || !cost_d || nseeds <= 0 || !seeds_d || ntargets <= 0 || !targets_d || !path_out_d || path_cap <= 0 ||
+      !path_len_h) {
+    set_error("sssp_multi: NULL argument or empty seeds / targets");
+    return ORSP_ERR_ARG;
+  }
+  if (!(delta > 0.0f) || !(delta < 3.0e38f)) { set_error("delta must be finite and > 0"); return ORSP_ERR_ARG; }
+  ORSP_CUDA(cudaSetDevice(g->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = ensure_single_ws(g, true);
+  if (rc) return rc;
+  // scratch: sink mask (N bytes) + the winning target
+  const size_t mask_b = ((size_t)g->N + 255) & ~(size_t)255;
+  rc = ensure_scratch(g, mask_b + 256);
+  if (rc) return rc;
+  uint8_t *sink = (uint8_t *)g->scratch;
+  int32_t *best_d = (int32_t *)((char *)g->scratch + mask_b);
+  ORSP_CUDA(cudaMemsetAsync(sink, 0, mask_b, st));
+  mark_kernel<<<std::max(1, std::min(1024, (ntargets + 255) / 256)), 256, 0, st>>>(sink, ntargets, targets_d, g->N, 1);
+  ORSP_CUDA(cudaGetLastError());
+  rc = run_grid_search(g, cost_d, nseeds, seeds_d, seed_cost_d, -1, roi_map_d, sink, delta, g->dist, st);
+  if (rc) return rc;
+  pick_target_kernel<<<1, 256, 0, st>>>(g->dist, roi_map_d, ntargets, targets_d, target_cost_d, g->N, best_d);
+  ORSP_CUDA(cudaGetLastError());
+  BacktraceParams b{};
+  b.cost = cost_d;
+  b.roi_map = roi_map_d;
+  b.rptr = g->rptr;
+  b.rsrc = g->rsrc;
+  b.reid = g->reid;
+  b.dist = g->dist;
+  b.seeds = seeds_d;
+  b.seed_cost = seed_cost_d;
+  b.nseeds = nseeds;
+  b.dst = -1;
+  b.dst_d = best_d;
+  b.path_out = path_out_d;
+  b.path_cap = path_cap;
+  b.ctl = (SsspCtl *)g->ctl;
+  backtrace_kernel<<<1, 32, 0, st>>>(b);
+  ORSP_CUDA(cudaGetLastError());
+  ORSP_CUDA(cudaMemcpyAsync(g->ctl_h, g->ctl, sizeof(SsspCtl), cudaMemcpyDeviceToHost, st));
+  ORSP_CUDA(cudaMemcpyAsync((char *)g->pinned + 64, best_d, 4, cudaMemcpyDeviceToHost, st));
+  ORSP_CUDA(cudaStreamSynchronize(st));
+  const SsspCtl *c = (const SsspCtl *)g->ctl_h;
+  if (best_target_h) *best_target_h = *(const int32_t *)((const char *)g->pinned + 64);
+  if (c->err) return dev_status_to_orsp(c->err);
+  *path_len_h = c->path_len;
+  if (c->status == 1 || c->path_len < 2) {
+    *path_len_h = 0;
+    return ORSP_NO_PATH;
+  }
+  return ORSP_OK;
+}
+
+// Owner bitmap (bit v of word v/32 set = node allowed) to global_to_roi with
+// rank = node id, for CUDADijkstra.find_path_fullgraph_gpu_seeds's
+// allowed_bitmap (CD:5467).
+__global__ void bitmap_roi_kernel(const uint32_t *bits, int32_t N, int32_t *g2r) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < N; v += (int64_t)gridDim.x * blockDim.x)
+    g2r[v] = ((bits[v >> 5] >> (v & 31)) & 1u) ? (int32_t)v : -1;
+}
+
+extern "C" int orsp_roi_from_bitmap(orsp_graph *g, const uint32_t *bitmap_d, int32_t *g2r_d, uintptr_t stream) {
+  if (!g || !bitmap_d || !g2r_d) { set_error("roi_from_bitmap: NULL argument"); return ORSP_ERR_ARG; }
+  ORSP_CUDA(cudaSetDevice(g->device));
+  bitmap_roi_kernel<<<std::min(4096, (g->N + 255) / 256), 256, 0, (cudaStream_t)stream>>>(bitmap_d, g->N, g2r_d);
+  ORSP_CUDA(cudaGetLastError());
   return ORSP_OK;
 }

@@ -18,6 +18,7 @@ import torch
 
 from . import _lib
 from ._lib import check, ptr
+from ._lib import load as _load_lib
 
 DEFAULT_PATH_CAP = 1 << 16
 
@@ -131,6 +132,36 @@ class DeviceGraph:
         path = pbuf[: plen.value] if (dst >= 0 and st == _lib.ORSP_OK) else None
         return st, path, int(rounds.value)
 
+    def sssp_multi(self, cost: torch.Tensor, seeds, targets, seed_cost=None, target_cost=None,
+                   roi_map: Optional[torch.Tensor] = None, delta: Optional[float] = None,
+                   path_cap: Optional[int] = None):
+        """Exact multi-seed / multi-target search (targets are sinks).  Returns
+        (status, path tensor or None, best target id)."""
+        lib = _load_lib()
+        seeds_t = as_device(np.atleast_1d(seeds) if not isinstance(seeds, torch.Tensor) else seeds, torch.int32,
+                            self.device)
+        tg = as_device(np.atleast_1d(targets) if not isinstance(targets, torch.Tensor) else targets, torch.int32,
+                       self.device)
+        sc = None if seed_cost is None else as_device(seed_cost, torch.float32, self.device)
+        tc = None if target_cost is None else as_device(target_cost, torch.float64, self.device)
+        if delta is None:
+            delta = self.default_delta(cost)
+        cap = int(path_cap or min(self.N + 1, DEFAULT_PATH_CAP))
+        pbuf = self._path_buffer(cap)
+        plen = ctypes.c_int32(0)
+        best = ctypes.c_int32(-1)
+        st = check(lib.orsp_sssp_multi(self._h, ptr(cost), int(seeds_t.numel()), ptr(seeds_t), ptr(sc),
+                                       int(tg.numel()), ptr(tg), ptr(tc), ptr(roi_map), float(delta), ptr(pbuf), cap,
+                                       ctypes.byref(plen), ctypes.byref(best), _stream()), "orsp_sssp_multi")
+        path = pbuf[: plen.value] if st == _lib.ORSP_OK else None
+        return st, path, int(best.value)
+
+    def roi_from_bitmap(self, bitmap) -> torch.Tensor:
+        bm = as_device(bitmap, torch.int32, self.device) if not isinstance(bitmap, torch.Tensor) else bitmap
+        g2r = torch.empty(self.N, dtype=torch.int32, device=self.device)
+        check(_load_lib().orsp_roi_from_bitmap(self._h, ptr(bm), ptr(g2r), _stream()), "orsp_roi_from_bitmap")
+        return g2r
+
     def batch_bbox(self, cost: torch.Tensor, src: torch.Tensor, dst: torch.Tensor, bbox: torch.Tensor,
                    order: Optional[torch.Tensor] = None, delta: Optional[float] = None,
                    path_cap: int = 4096, with_edges: bool = True):
@@ -211,3 +242,112 @@ class GpuSolver:
         if st != _lib.ORSP_OK or path is None or path.numel() < 2:
             return None
         return path.cpu().tolist()
+
+    def find_path_multisource_multisink(self, src_seeds, dst_targets, costs, roi_nodes, global_to_roi):
+        """SimpleDijkstra.find_path_multisource_multisink (UPF:1889-1989):
+        seeds and targets are [(global node, cost)]; returns (path,
+        entry_layer, exit_layer) or None.  Repeated targets keep their last
+        cost, as the reference's dict does."""
+        cost = self._cost(costs)
+        g2r = as_device(global_to_roi, torch.int32, self.dg.device)
+        seeds = [int(n) for n, _ in src_seeds]
+        scost = np.asarray([float(c) for _, c in src_seeds], dtype=np.float32)
+        tmap = {}
+        for n, c in dst_targets:
+            tmap[int(n)] = float(c)
+        if not seeds or not tmap:
+            return None
+        st, path, _ = self.dg.sssp_multi(cost, seeds, list(tmap.keys()), seed_cost=scost,
+                                         target_cost=np.asarray(list(tmap.values()), dtype=np.float64), roi_map=g2r)
+        if st != _lib.ORSP_OK or path is None or path.numel() < 2:
+            return None
+        p = path.cpu().tolist()
+        plane = self.dg.nx * self.dg.ny if self.dg.nx > 0 else 0
+        if plane:
+            return p, p[0] // plane, p[-1] // plane
+        return p, 0, 0
+
+    def find_path_fullgraph_gpu_seeds(self, costs, src_seeds, dst_targets, ub_hint=None, *, allowed_bitmap=None,
+                                      use_bitmap=False):
+        """CUDADijkstra.find_path_fullgraph_gpu_seeds (CD:5467): path from the
+        best seed to the best target over the whole graph (restricted to the
+        allowed bitmap when use_bitmap), or None.  Exact shortest path; the
+        reference wavefront instead stops at the first target it reaches."""
+        if len(src_seeds) == 0 or len(dst_targets) == 0:
+            return None
+        cost = self._cost(costs)
+        roi = None
+        if use_bitmap and allowed_bitmap is not None:
+            bm = allowed_bitmap.get() if hasattr(allowed_bitmap, "get") else allowed_bitmap
+            roi = self.dg.roi_from_bitmap(np.asarray(bm).view(np.int32))
+        targets = np.unique(np.asarray(dst_targets, dtype=np.int32))
+        st, path, _ = self.dg.sssp_multi(cost, np.asarray(src_seeds, dtype=np.int32), targets, roi_map=roi)
+        if st != _lib.ORSP_OK or path is None or path.numel() < 2:
+            return None
+        return path.cpu().tolist()
+
+    def find_paths_on_rois(self, roi_batch, use_bitmap: bool = True):
+        """CUDADijkstra.find_paths_on_rois (CD:2014-2086): K ROI subgraphs given
+        as 13-tuples (src, dst, indptr, indices, weights, roi_size, bitmap,
+        bbox x 6) in ROI-local ids (CD:55-91).  Returns one path (local ids)
+        or None per ROI.  The local CSRs are concatenated into one graph and
+        searched in one launch with node-range ROIs; with use_bitmap a node
+        whose bit is clear is never entered (edges into it are +inf), as the
+        reference's IN_BITMAP check does (CD:237-239)."""
+        K = len(roi_batch)
+        if K == 0:
+            return []
+        node_off = [0]
+        edge_off = [0]
+        for t in roi_batch:
+            node_off.append(node_off[-1] + int(len(t[2]) - 1))
+            edge_off.append(edge_off[-1] + int(len(t[3])))
+        Ntot, Etot = node_off[-1], edge_off[-1]
+        indptr = np.empty(Ntot + 1, dtype=np.int64)
+        indices = np.empty(Etot, dtype=np.int32)
+        weights = np.empty(Etot, dtype=np.float32)
+        src = np.empty(K, dtype=np.int32)
+        dst = np.empty(K, dtype=np.int32)
+        ranges = np.empty((K, 2), dtype=np.int32)
+        for k, t in enumerate(roi_batch):
+            s_, d_, ip, ix, w = t[0], t[1], t[2], t[3], t[4]
+            ip = (ip.get() if hasattr(ip, "get") else np.asarray(ip)).astype(np.int64)
+            ix = (ix.get() if hasattr(ix, "get") else np.asarray(ix)).astype(np.int64)
+            w = (w.get() if hasattr(w, "get") else np.asarray(w)).astype(np.float32).copy()
+            n0, e0 = node_off[k], edge_off[k]
+            n = node_off[k + 1] - n0
+            bm = t[6] if len(t) > 6 else None
+            if use_bitmap and bm is not None:
+                bm = (bm.get() if hasattr(bm, "get") else np.asarray(bm)).astype(np.uint32).reshape(-1)
+                word = ix >> 5
+                ok = (word < len(bm)) & (((bm[np.minimum(word, len(bm) - 1)] >> (ix & 31).astype(np.uint32)) & 1) == 1)
+                w[~ok] = np.float32(np.inf)
+            indptr[n0: n0 + n + 1] = ip + e0
+            indices[e0: e0 + len(ix)] = ix + n0
+            weights[e0: e0 + len(ix)] = w
+            src[k] = int(s_) + n0
+            dst[k] = int(d_) + n0
+            ranges[k] = (n0, n0 + n)
+        if Etot >= 2 ** 31 or Ntot >= 2 ** 31:
+            raise ValueError("ROI batch too large for int32 ids")
+        dg = DeviceGraph(indptr.astype(np.int32), indices, device=self.dg.device)
+        wt = torch.from_numpy(weights).to(self.dg.device)
+        cap = int(max(n1 - n0 for n0, n1 in ranges) + 1)
+        lib = _load_lib()
+        nodes = torch.empty((K, cap), dtype=torch.int32, device=self.dg.device)
+        lens = torch.zeros(K, dtype=torch.int32, device=self.dg.device)
+        # keep the device copies referenced until the launch has been issued
+        src_d = torch.from_numpy(src).to(self.dg.device)
+        dst_d = torch.from_numpy(dst).to(self.dg.device)
+        ranges_d = torch.from_numpy(ranges).to(self.dg.device)
+        check(lib.orsp_sssp_batch_ranges(dg.handle, ptr(wt), K, ptr(src_d), ptr(dst_d), ptr(ranges_d), None,
+                                         float(DeviceGraph.default_delta(wt)), ptr(nodes), None, cap, ptr(lens),
+                                         _stream()), "orsp_sssp_batch_ranges")
+        lens_h = lens.cpu().numpy()
+        nodes_h = nodes.cpu().numpy()
+        out = []
+        for k in range(K):
+            L = int(lens_h[k])
+            out.append((nodes_h[k, :L] - node_off[k]).tolist() if L >= 2 else None)
+        dg.close()
+        return out

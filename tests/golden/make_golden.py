@@ -18,6 +18,11 @@ Outputs (small .npz files, committed):
   golden_accounting.npz EdgeAccountant.update_costs / update_history /
                         update_present_ema / compute_overuse (UPF:799-1068).
   golden_path_edges.npz PathFinderRouter._path_to_edges (UPF:5463-5476).
+  golden_via.npz        _accumulate_via_usage_for_path (UPF:2678-2724),
+                        _apply_via_pooling_penalties (UPF:3243-3387, float32
+                        and float64 layer bias) and
+                        _block_via_edges_with_collisions (UPF:3448-3546) on the
+                        reference's own blind/buried-via lattice.
 UPF = orthoroute/algorithms/manhattan/unified_pathfinder.py.
 """
 from __future__ import annotations
@@ -257,6 +262,91 @@ def gen_path_edges(upf, graph, rng):
     return out
 
 
+def gen_via(upf, graph, lat, rng):
+    """Via pooling on the reference's own lattice (blind/buried vias of every
+    span): _accumulate_via_usage_for_path, _apply_via_pooling_penalties
+    (float32 and float64 layer bias) and _block_via_edges_with_collisions,
+    each called on a stub router holding just the attributes they read."""
+    from types import SimpleNamespace
+
+    Nx, Ny, Nz = lat.x_steps, lat.y_steps, lat.layers
+    segz = Nz - 2
+    indptr = np.asarray(graph.indptr, dtype=np.int32)
+    indices = np.asarray(graph.indices, dtype=np.int32)
+    N = len(indptr) - 1
+    E = len(indices)
+
+    def stub():
+        st = SimpleNamespace()
+        st.graph = graph
+        st.lattice = lat
+        st.config = SimpleNamespace(use_gpu=False, via_column_weight=1.0, via_segment_weight=1.0,
+                                    via_hot_layer_discount=0.20)
+        st._Nx, st._Ny, st._Nz, st._segZ = Nx, Ny, Nz, segz
+        return st
+
+    st = stub()
+    upf.PathFinderRouter._identify_via_edges(st)
+    upf.PathFinderRouter._build_via_edge_metadata(st)
+    # random walks as committed paths
+    paths = []
+    for _ in range(60):
+        u = int(rng.integers(0, N))
+        path = [u]
+        for _ in range(int(rng.integers(2, 30))):
+            b, e = indptr[u], indptr[u + 1]
+            if e == b:
+                break
+            u = int(indices[rng.integers(b, e)])
+            path.append(u)
+        paths.append(path)
+    st.via_col_use = np.zeros((Nx, Ny), dtype=np.int16)
+    st.via_seg_use = np.zeros((Nx, Ny, segz), dtype=np.int16)
+    for pth in paths:
+        upf.PathFinderRouter._accumulate_via_usage_for_path(st, pth, net_id=None)
+    out = {"via_dims": np.array([Nx, Ny, Nz], dtype=np.int32), "npaths": np.int32(len(paths)),
+           "col_use": st.via_col_use.copy(), "seg_use": st.via_seg_use.copy()}
+    for i, pth in enumerate(paths):
+        out[f"vpath{i}"] = np.asarray(pth, dtype=np.int32)
+    col_cap = np.full((Nx, Ny), 4, dtype=np.int16)
+    seg_cap = np.full((Nx, Ny, segz), 2, dtype=np.int8)
+    col_cap[rng.random((Nx, Ny)) < 0.3] = 1
+    seg_cap[rng.random((Nx, Ny, segz)) < 0.3] = 1
+    out["col_cap"] = col_cap
+    out["seg_cap"] = seg_cap
+    # smoothing inputs / outputs are produced below with the reference's
+    # inline expressions restated in oracle.via_present; the penalties use
+    # random present fields so that every branch is exercised
+    col_pres = (rng.random((Nx, Ny)) * 2).astype(np.float32)
+    col_pres[rng.random((Nx, Ny)) < 0.5] = 0
+    seg_pres = (rng.random((Nx, Ny, segz)) * 2).astype(np.float32)
+    seg_prefix = np.cumsum(seg_pres, axis=2).astype(np.float32)
+    total0 = (rng.random(E) * 3).astype(np.float32)
+    out.update(col_pres=col_pres, seg_pres=seg_pres, seg_prefix=seg_prefix, total0=total0)
+    for tag, bias in (("f32", np.array([1.0, 1.3, 0.8, 1.7, 1.1], dtype=np.float32)[:Nz]),
+                      ("f64", np.array([1.0, 1.31, 0.77, 1.62, 1.05], dtype=np.float64)[:Nz])):
+        st2 = stub()
+        st2._via_edge_metadata = st._via_edge_metadata
+        st2.via_col_pres = col_pres.copy()
+        st2.via_seg_pres = seg_pres.copy()
+        st2.via_seg_prefix = seg_prefix.copy()
+        st2.layer_bias = bias
+        st2.accounting = SimpleNamespace(total_cost=total0.copy(), use_gpu=False)
+        upf.PathFinderRouter._apply_via_pooling_penalties(st2, 2.25)
+        out[f"bias_{tag}"] = bias
+        out[f"pen_{tag}"] = np.asarray(st2.accounting.total_cost, dtype=np.float32)
+    st3 = stub()
+    st3._via_edge_metadata = st._via_edge_metadata
+    st3.via_col_use = st.via_col_use.copy()
+    st3.via_col_cap = col_cap
+    st3.via_seg_use = st.via_seg_use.copy()
+    st3.via_seg_cap = seg_cap
+    st3.accounting = SimpleNamespace(total_cost=total0.copy(), use_gpu=False)
+    upf.PathFinderRouter._block_via_edges_with_collisions(st3)
+    out["blocked"] = np.asarray(st3.accounting.total_cost, dtype=np.float32)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -287,6 +377,8 @@ def main():
     np.savez_compressed(HERE / "golden_roi.npz", **gen_roi(upf, rng))
     np.savez_compressed(HERE / "golden_accounting.npz", **gen_accounting(upf, rng, ref_arrays))
     np.savez_compressed(HERE / "golden_path_edges.npz", **gen_path_edges(upf, graph, rng))
+    ref_lat = upf.Lattice3D((0.0, 0.0, 4.0, 3.2), 0.4, 5)
+    np.savez_compressed(HERE / "golden_via.npz", **gen_via(upf, graph, ref_lat, np.random.default_rng(77)))
     for f in sorted(HERE.glob("golden_*.npz")):
         print(f.name, f.stat().st_size)
 

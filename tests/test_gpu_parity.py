@@ -248,3 +248,142 @@ def test_path_to_edges_matches_reference(golden):
     for k in range(int(g["n"])):
         e = dg.path_to_edges(cuda(g[f"p{k}"]))
         assert np.array_equal(e.cpu().numpy(), g[f"e{k}"])
+
+
+# ---------------------------------------------------------------- via pooling
+def test_via_kernels_match_reference(golden):
+    import oracle as O2
+
+    g = golden("golden_via.npz")
+    d = golden("golden_dijkstra.npz")
+    nx, ny, nz = (int(v) for v in g["via_dims"])
+    segz = nz - 2
+    dg = DeviceGraph(d["ref_indptr"], d["ref_indices"], nx, ny, nz)
+    lib = _lib.load()
+    st = int(torch.cuda.current_stream().cuda_stream)
+    # usage from the committed paths
+    paths = [g[f"vpath{i}"] for i in range(int(g["npaths"]))]
+    cap = max(len(p) for p in paths)
+    nodes = np.zeros((len(paths), cap), np.int32)
+    lens = np.array([len(p) for p in paths], np.int32)
+    for i, p in enumerate(paths):
+        nodes[i, : len(p)] = p
+    # device copies are bound to names so they stay alive across each call
+    nodes_d, lens_d = cuda(nodes), cuda(lens)
+    col = torch.zeros(nx * ny, dtype=torch.int32, device="cuda")
+    seg = torch.zeros(nx * ny * segz, dtype=torch.int32, device="cuda")
+    assert lib.orsp_via_usage(dg.handle, len(paths), _lib.ptr(nodes_d), _lib.ptr(lens_d), cap,
+                              _lib.ptr(col), _lib.ptr(seg), st) == 0
+    assert np.array_equal(col.cpu().numpy().reshape(nx, ny), g["col_use"])
+    assert np.array_equal(seg.cpu().numpy().reshape(nx, ny, segz), g["seg_use"])
+    col_pres_in, seg_prefix_in = cuda(g["col_pres"]), cuda(g["seg_prefix"])
+    col_cap, seg_cap = cuda(g["col_cap"].astype(np.int32)), cuda(g["seg_cap"].astype(np.int32))
+    # penalties (float32 and float64 layer bias)
+    for tag in ("f32", "f64"):
+        total = cuda(g["total0"].copy())
+        bias = cuda(g[f"bias_{tag}"].astype(np.float64))
+        assert lib.orsp_via_penalties(dg.handle, _lib.ptr(col_pres_in), _lib.ptr(seg_prefix_in), _lib.ptr(bias),
+                                      1 if tag == "f64" else 0, 0.20, 1.0, 1.0, 2.25, _lib.ptr(total), st) == 0
+        assert np.array_equal(_bits(total.cpu().numpy()), _bits(g[f"pen_{tag}"])), tag
+    # hard block
+    total = cuda(g["total0"].copy())
+    assert lib.orsp_via_hard_block(dg.handle, _lib.ptr(col), _lib.ptr(col_cap), _lib.ptr(seg), _lib.ptr(seg_cap),
+                                   _lib.ptr(total), st) == 0
+    assert np.array_equal(_bits(total.cpu().numpy()), _bits(g["blocked"]))
+    # present smoothing + prefix vs the oracle restatement
+    cp_ref, sp_ref, pre_ref = O2.via_present(g["col_use"], g["col_cap"], g["col_pres"], g["seg_use"], g["seg_cap"],
+                                             g["seg_pres"])
+    col_pres = cuda(g["col_pres"].copy())
+    seg_pres = cuda(g["seg_pres"].copy())
+    prefix = torch.zeros_like(seg_pres)
+    assert lib.orsp_via_present(nx * ny, segz, _lib.ptr(col), _lib.ptr(col_cap), _lib.ptr(col_pres), _lib.ptr(seg),
+                                _lib.ptr(seg_cap), _lib.ptr(seg_pres), _lib.ptr(prefix), 0.6, 0.4, st) == 0
+    assert np.array_equal(_bits(col_pres.cpu().numpy()), _bits(cp_ref))
+    assert np.array_equal(_bits(seg_pres.cpu().numpy()), _bits(sp_ref))
+    assert np.array_equal(_bits(prefix.cpu().numpy()), _bits(pre_ref))
+
+
+# ------------------------------------------------------- multi-source / sink
+def test_sssp_multi_matches_oracle():
+    """Seeds with start costs, targets with portal costs (targets are sinks),
+    inside BFS ROIs and on the whole graph: same winner and same path as the
+    oracle restatement of find_path_multisource_multisink."""
+    lat = build_lattice(50, 40, 6)
+    w = uniform_weights(lat, seed=21, blocked_frac=0.03)
+    solver = GpuSolver(DeviceGraph.from_lattice(lat))
+    rng = np.random.default_rng(5)
+    for i in range(24):
+        ns, nt = int(rng.integers(1, 5)), int(rng.integers(1, 6))
+        nodes = rng.choice(lat.N, size=ns + nt, replace=False)
+        seeds, targets = nodes[:ns], nodes[ns:]
+        scost = (rng.integers(0, 4, size=ns) * 0.5).astype(np.float32)
+        tcost = rng.integers(0, 4, size=nt) * 0.25
+        if i % 2:
+            roi, g2r = O.roi_bfs(lat.indptr, lat.indices, int(seeds[0]), int(targets[0]), 40, 50_000)
+        else:
+            roi = np.arange(lat.N, dtype=np.int32)
+            g2r = roi
+        ref, _, _, best = O.dijkstra(lat.indptr, lat.indices, w, seeds, roi_map=g2r, seed_cost=scost,
+                                     targets=targets, target_cost=tcost)
+        got = solver.find_path_multisource_multisink(list(zip(seeds.tolist(), scost.tolist())),
+                                                     list(zip(targets.tolist(), tcost.tolist())), w, roi, g2r)
+        if len(ref) < 2:
+            assert got is None
+        else:
+            assert got is not None and got[0] == ref.tolist(), f"case {i}"
+    # whole graph, allowed bitmap
+    allowed = np.ones((lat.N + 31) // 32, dtype=np.uint32)
+    allowed[:] = 0xFFFFFFFF
+    blocked_nodes = rng.choice(lat.N, size=lat.N // 10, replace=False)
+    for v in blocked_nodes:
+        allowed[v >> 5] &= ~np.uint32(1 << (v & 31))
+    ok = np.ones(lat.N, bool)
+    ok[blocked_nodes] = False
+    g2r = np.where(ok, np.arange(lat.N), -1).astype(np.int32)
+    seeds = np.array([v for v in rng.choice(lat.N, 20) if ok[v]][:3], np.int32)
+    targets = np.array([v for v in rng.choice(lat.N, 20) if ok[v]][:4], np.int32)
+    ref, *_ = O.dijkstra(lat.indptr, lat.indices, w, seeds, roi_map=g2r, targets=targets)
+    got = solver.find_path_fullgraph_gpu_seeds(w, seeds, targets, allowed_bitmap=allowed, use_bitmap=True)
+    assert (got or []) == (ref.tolist() if len(ref) > 1 else [])
+
+
+def test_find_paths_on_rois_local_csr_batch():
+    """13-tuple ROI batch (ROI-local CSRs) in one launch, with and without the
+    per-ROI bitmap, against the oracle on each local CSR."""
+    from orthoroute_b200.lattice import build_lattice as bl
+
+    rng = np.random.default_rng(17)
+    lat = bl(40, 30, 4)
+    w = uniform_weights(lat, seed=2, blocked_frac=0.02)
+    solver = GpuSolver(DeviceGraph.from_lattice(lat))
+    batch, refs = [], []
+    for k in range(40):
+        s, d = (int(v) for v in rng.choice(lat.N, size=2, replace=False))
+        roi, g2r = O.roi_bfs(lat.indptr, lat.indices, s, d, int(rng.integers(3, 30)), 50_000)
+        # local CSR of the ROI-induced subgraph, in ROI-index order
+        ip = [0]
+        ix, wl = [], []
+        for u in roi:
+            for e in range(lat.indptr[u], lat.indptr[u + 1]):
+                v = lat.indices[e]
+                if g2r[v] >= 0:
+                    ix.append(g2r[v])
+                    wl.append(w[e])
+            ip.append(len(ix))
+        ip = np.asarray(ip, np.int32)
+        ix = np.asarray(ix, np.int32)
+        wl = np.asarray(wl, np.float32)
+        n = len(roi)
+        bm = np.full((n + 31) // 32, 0xFFFFFFFF, dtype=np.uint32)
+        if k % 3 == 0:  # clear some bits (never the endpoints)
+            for v in rng.choice(n, size=max(1, n // 8), replace=False):
+                if v not in (g2r[s], g2r[d]):
+                    bm[v >> 5] &= ~np.uint32(1 << (v & 31))
+        wl_ref = wl.copy()
+        ok = ((bm[ix >> 5] >> (ix & 31).astype(np.uint32)) & 1) == 1
+        wl_ref[~ok] = np.inf
+        ref, *_ = O.dijkstra(ip, ix, wl_ref, [int(g2r[s])], dst=int(g2r[d]))
+        batch.append((int(g2r[s]), int(g2r[d]), ip, ix, wl, n, bm, 0, 0, 0, 0, 0, 0))
+        refs.append(ref.tolist() if len(ref) > 1 else None)
+    got = solver.find_paths_on_rois(batch, use_bitmap=True)
+    assert got == refs

@@ -109,3 +109,29 @@ def test_jitter_rounding_beyond_2_24():
     fi = i.astype(np.float32)
     b = np.fmod(fi, np.float32(9973)) * np.float32(1e-6)
     assert np.array_equal(a.view(np.uint32), b.astype(np.float32).view(np.uint32))
+
+
+def _via_meta(golden):
+    g = golden("golden_via.npz")
+    d = golden("golden_dijkstra.npz")
+    nx, ny, nz = (int(v) for v in g["via_dims"])
+    meta = O.via_edge_metadata(d["ref_indptr"], d["ref_indices"], nx, ny, nz)
+    return g, d, (nx, ny, nz), meta
+
+
+def test_via_usage_matches_reference(golden):
+    g, _, (nx, ny, nz), _ = _via_meta(golden)
+    col = np.zeros((nx, ny), np.int64)
+    seg = np.zeros((nx, ny, nz - 2), np.int64)
+    O.via_usage([g[f"vpath{i}"] for i in range(int(g["npaths"]))], nx, ny, nz, col, seg)
+    assert np.array_equal(col, g["col_use"]) and np.array_equal(seg, g["seg_use"])
+
+
+def test_via_penalties_and_hard_block_match_reference(golden):
+    g, _, (nx, ny, nz), meta = _via_meta(golden)
+    for tag in ("f32", "f64"):
+        out = O.via_penalties(g["total0"], meta, g["col_pres"], g["seg_prefix"], nz - 2, g[f"bias_{tag}"], 2.25)
+        assert np.array_equal(out.view(np.uint32), g[f"pen_{tag}"].view(np.uint32)), tag
+    out = O.via_hard_block(g["total0"], meta, g["col_use"], g["col_cap"], g["seg_use"], g["seg_cap"], nz - 2)
+    assert np.array_equal(out.view(np.uint32), g["blocked"].view(np.uint32))
+    assert np.isinf(out).sum() > 0
