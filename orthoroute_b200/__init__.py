@@ -6,11 +6,14 @@ Public entry points mirror the reference router's hot-path interfaces:
 * ``DeviceEdgeAccountant`` - router.accounting (EdgeAccountant interface)
 * ``DeviceROIExtractor``   - router.roi_extractor (ROIExtractor interface)
 * ``PathFinder``           - the negotiation loop on the device kernels
+* ``install``              - wires the GPU solver into a reference PathFinderRouter
 """
 from .lattice import Lattice, Board, build_lattice  # noqa: F401
 
+from .shim import install  # noqa: F401,E402
+
 __all__ = ["Lattice", "Board", "build_lattice", "GpuSolver", "DeviceGraph", "DeviceEdgeAccountant",
-           "DeviceROIExtractor", "PathFinder", "NegotiationConfig"]
+           "DeviceROIExtractor", "PathFinder", "NegotiationConfig", "install"]
 
 
 def __getattr__(name):

@@ -218,13 +218,21 @@ class GpuSolver:
         self._cost_cache = (None, None)
 
     def _cost(self, costs) -> torch.Tensor:
-        if isinstance(costs, torch.Tensor) and costs.is_cuda:
+        """Device copy of the cost array.  The router calls once per net with the
+        same host array, which it also rewrites in place between iterations
+        (via pooling, UPF:3381/3443/5298), so the cached device copy is reused
+        only when the host bits are unchanged."""
+        if isinstance(costs, torch.Tensor):
             return as_device(costs, torch.float32, self.dg.device)
-        key = id(costs)
-        if self._cost_cache[0] == key:
-            return self._cost_cache[1]
-        t = as_device(costs, torch.float32, self.dg.device)
-        self._cost_cache = (key, t)
+        if hasattr(costs, "__cuda_array_interface__"):  # cupy array from a GPU-mode router
+            return as_device(torch.as_tensor(costs, device=self.dg.device), torch.float32, self.dg.device)
+        host = np.ascontiguousarray(np.asarray(costs), dtype=np.float32)
+        prev_host, prev_dev = self._cost_cache
+        if prev_host is not None and prev_host.shape == host.shape and \
+                np.array_equal(prev_host.view(np.uint32), host.view(np.uint32)):
+            return prev_dev
+        t = torch.from_numpy(host).to(self.dg.device)
+        self._cost_cache = (host.copy(), t)
         return t
 
     def find_path_roi_gpu(self, src: int, dst: int, costs, roi_nodes, global_to_roi) -> Optional[List[int]]:
@@ -351,3 +359,12 @@ class GpuSolver:
             out.append((nodes_h[k, :L] - node_off[k]).tolist() if L >= 2 else None)
         dg.close()
         return out
+
+    def path_to_edges_list(self, node_path) -> list:
+        """PathFinderRouter._path_to_edges (UPF:5463-5476) on the device: the
+        first CSR edge u->v for each consecutive pair, pairs without an edge
+        skipped; returns a Python list like the reference."""
+        if len(node_path) < 2:
+            return []
+        p = torch.as_tensor(np.asarray(node_path, dtype=np.int32)).to(self.dg.device)
+        return self.dg.path_to_edges(p).cpu().tolist()
