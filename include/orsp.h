@@ -92,14 +92,18 @@ ORSP_API int orsp_graph_max_degree(orsp_graph *g, int32_t *out);
 
 /* ---- single search ----------------------------------------------------- */
 /* Single-source (or multi-seed) shortest path over the whole graph or over
- * the ROI given by roi_map_d (global_to_roi, int32[N], -1 = outside), as one
- * persistent cooperative launch (near-far delta-stepping with a bounded grid
- * barrier).  Replaces SimpleDijkstra.find_path_roi (UPF:1801-1887) and
+ * the ROI given by roi_map_d (global_to_roi, int32[N], -1 = outside).  A
+ * full-graph search on a recognised H/V lattice runs the tile-sweep search;
+ * other searches run one persistent cooperative launch of near-far
+ * delta-stepping with a bounded grid barrier.  Replaces SimpleDijkstra.find_path_roi (UPF:1801-1887) and
  * CUDADijkstra.find_path_roi_gpu (CD:4909-4996).
  *   seeds_d[nseeds]       start nodes (global ids); seed_cost_d may be NULL
  *                          (all seeds start at 0.0) or give fp32 start costs.
  *   dst                    target node, or -1 for a full search (no path).
- *   delta                  near-far bucket width (> 0).
+ *   delta                  near-far bucket width (> 0), or 0 to let the
+ *                          library choose it on the device (twice the mean
+ *                          of a strided sample of the finite costs).  It
+ *                          changes the work, never the distances or path.
  *   dist_out_d             optional fp32[N]; receives distances (nodes not
  *                          settled before an early exit hold upper bounds).
  *   path_out_d/path_cap    receives the node path seed..dst (global ids).
@@ -143,6 +147,7 @@ ORSP_API int orsp_roi_from_bitmap(orsp_graph *g, const uint32_t *bitmap_d, int32
  * the per-net loop body of _route_all (UPF:4475-4800) under fixed costs.
  *   order_d               optional int32[K] processing order (e.g. largest
  *                          box first); NULL = 0..K-1.
+ *   delta                  bucket width as for orsp_sssp (0: device choice).
  *   path_nodes_d/edges_d  int32[K*path_cap] outputs (edges_d may be NULL).
  *   path_len_d            int32[K]: path length, 0 = no path, <0 = error. */
 ORSP_API int orsp_sssp_batch_bbox(orsp_graph *g, const float *cost_d, int32_t K,

@@ -63,6 +63,7 @@ struct Graph {
   void *scratch = nullptr;
   size_t scratch_bytes = 0;
   void *pinned = nullptr;  // small pinned host buffer for results
+  float *auto_delta = nullptr;  // [2] device bucket widths chosen by the library (single, batch)
   // H/V lattice description, set when every CSR edge is a unit step along the
   // layer's routing axis or a via to an adjacent layer (see orsp_lattice.cu)
   bool lattice_ok = false;
@@ -87,6 +88,10 @@ extern KernelTimer g_timer;
 extern int64_t g_counters[8];
 
 int ensure_scratch(Graph *g, size_t bytes);
+// Bucket width chosen on the device when the caller passes delta == 0: twice
+// the mean of a strided sample (<= 65536 entries) of the finite costs, 1.0 if
+// none is finite.  Writes *out; never blocks the host.  (orsp_sssp.cu)
+int launch_auto_delta(const float *cost_d, int64_t E, float *out_d, cudaStream_t st);
 // orsp_lattice.cu
 int analyze_lattice(Graph *g, const int32_t *indptr_h, const int32_t *indices_h);
 void free_lattice(Graph *g);

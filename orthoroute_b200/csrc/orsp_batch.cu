@@ -49,6 +49,7 @@ struct BatchParams {
   int64_t qcap;
   int32_t smem_nodes;
   float delta;
+  const float *delta_d;  // device bucket width (overrides delta) or nullptr
   unsigned *work_counter;
   unsigned long long budget_ns;
 };
@@ -188,7 +189,7 @@ __device__ void block_search(const BatchParams &p, const Box &b, int32_t src_l, 
       if (fc == 0) break;
       if (bits_f(dist_ld<SMEM>(dist, dst_l)) < T) break;
       const float fm = bits_f(c->fmin[g % 4]);
-      float Tn = __fadd_rn(fm, p.delta);
+      float Tn = __fadd_rn(fm, p.delta_d ? *p.delta_d : p.delta);
       if (!(Tn > fm)) Tn = __uint_as_float(f_bits(fm) + 1u);
       const int2 *fin = ((g & 1) ? fq1 : fq0);
       int2 *fout = (((g + 1) & 1) ? fq1 : fq0);
@@ -391,7 +392,7 @@ static int run_batch(orsp_graph *g, const float *cost_d, int32_t K, const int32_
     return ORSP_ERR_ARG;
   }
   if (!range_mode && g->nx <= 0) { set_error("batch_bbox: graph was created without lattice dims"); return ORSP_ERR_ARG; }
-  if (!(delta > 0.0f) || !(delta < 3.0e38f)) { set_error("delta must be finite and > 0"); return ORSP_ERR_ARG; }
+  if (!(delta >= 0.0f) || !(delta < 3.0e38f)) { set_error("delta must be finite and >= 0 (0: chosen on the device)"); return ORSP_ERR_ARG; }
   if (K == 0) return ORSP_OK;
   ORSP_CUDA(cudaSetDevice(g->device));
   cudaStream_t st = (cudaStream_t)stream;
@@ -463,6 +464,12 @@ static int run_batch(orsp_graph *g, const float *cost_d, int32_t K, const int32_
   p.path_cap = path_cap;
   p.smem_nodes = smem_nodes;
   p.delta = delta;
+  p.delta_d = nullptr;
+  if (delta == 0.0f) {
+    int rc = launch_auto_delta(cost_d, g->E, g->auto_delta + 1, st);
+    if (rc) return rc;
+    p.delta_d = g->auto_delta + 1;
+  }
   p.budget_ns = 30ull * 1000000000ull;
 
   const int32_t *order = order_d;

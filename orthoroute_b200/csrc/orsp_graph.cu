@@ -143,6 +143,7 @@ extern "C" int orsp_graph_create(int32_t N, int64_t E, const int32_t *indptr_h,
     TRY(cudaMemcpy(g->reid, reid.data(), (size_t)E * 4, cudaMemcpyHostToDevice));
   }
   TRY(cudaMallocHost(&g->pinned, 4096));
+  TRY(cudaMalloc(&g->auto_delta, 2 * sizeof(float)));
 #undef TRY
   if (nx > 0) {
     int rc = analyze_lattice(g, indptr_h, indices_h);
@@ -173,6 +174,7 @@ extern "C" int orsp_graph_destroy(orsp_graph *g) {
   cudaFree(g->batch_ws);
   cudaFree(g->batch_ctl);
   cudaFree(g->scratch);
+  cudaFree(g->auto_delta);
   if (g->pinned) cudaFreeHost(g->pinned);
   free_lattice(g);
   delete g;

@@ -45,10 +45,50 @@ struct SsspParams {
   int32_t N;
   int32_t dst;
   float delta;
+  const float *delta_d;  // device bucket width (overrides delta) or nullptr
   unsigned max_rounds;
   unsigned long long wait_ns;
   unsigned long long budget_ns;
 };
+
+// One block: twice the mean of a strided sample of the finite costs.  The
+// bucket width only changes how many near-far phases a search takes, never
+// its distances or paths.
+__global__ void auto_delta_kernel(const float *cost, int64_t E, int64_t step, float *out) {
+  __shared__ double s_sum[32];
+  __shared__ long long s_cnt[32];
+  double sum = 0.0;
+  long long cnt = 0;
+  for (int64_t i = (int64_t)threadIdx.x * step; i < E; i += (int64_t)blockDim.x * step) {
+    const float c = cost[i];
+    if (c >= 0.0f && c < __int_as_float(0x7f800000)) {
+      sum += (double)c;
+      ++cnt;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sum += __shfl_down_sync(0xffffffffu, sum, o);
+    cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    s_sum[w] = sum;
+    s_cnt[w] = cnt;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    long long n = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+      t += s_sum[k];
+      n += s_cnt[k];
+    }
+    float d = n ? (float)(2.0 * t / (double)n) : 1.0f;
+    if (!(d >= 1e-6f)) d = 1e-6f;
+    if (!(d < 3.0e38f)) d = 3.0e38f;
+    *out = d;
+  }
+}
 
 __global__ void fill_u32_kernel(uint32_t *p, int64_t n, uint32_t v) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -99,6 +139,7 @@ __global__ void __launch_bounds__(512) sssp_grid_kernel(SsspParams p) {
   const bool leader = (blockIdx.x == 0 && threadIdx.x == 0);
   const unsigned long long t_start = dev_globaltimer();
   const float INF_F = __int_as_float(0x7f800000);
+  const float delta = p.delta_d ? *p.delta_d : p.delta;
 
   unsigned r = 0, g = 0;
   float T = 0.0f;
@@ -175,7 +216,7 @@ __global__ void __launch_bounds__(512) sssp_grid_kernel(SsspParams p) {
       }
       if (done) break;
       const float fm = bits_f(ld_acquire_u32(&ctl->fmin[g % 4]));
-      float Tn = __fadd_rn(fm, p.delta);
+      float Tn = __fadd_rn(fm, delta);
       if (!(Tn > fm)) Tn = __uint_as_float(f_bits(fm) + 1u);
       const int2 *fin = ((g & 1) ? p.fq1 : p.fq0);
       int2 *fout = (((g + 1) & 1) ? p.fq1 : p.fq0);
@@ -412,6 +453,13 @@ extern "C" int orsp_profile_last(float *kernel_ms) {
 namespace orsp {
 
 // Shared by orsp_sssp and orsp_sssp_multi: seeds, runs the grid search to the
+int launch_auto_delta(const float *cost_d, int64_t E, float *out_d, cudaStream_t st) {
+  const int64_t step = std::max<int64_t>(1, E / 65536);
+  auto_delta_kernel<<<1, 1024, 0, st>>>(cost_d, E, step, out_d);
+  ORSP_CUDA(cudaGetLastError());
+  return ORSP_OK;
+}
+
 // exact fixpoint (dst >= 0: until d[dst] is below the open bucket) and leaves
 // distances in `dist`.
 int run_grid_search(Graph *g, const float *cost_d, int32_t nseeds,
@@ -436,6 +484,12 @@ int run_grid_search(Graph *g, const float *cost_d, int32_t nseeds,
   p.N = g->N;
   p.dst = dst;
   p.delta = delta;
+  p.delta_d = nullptr;
+  if (delta == 0.0f) {
+    int rc = launch_auto_delta(cost_d, g->E, g->auto_delta, st);
+    if (rc) return rc;
+    p.delta_d = g->auto_delta;
+  }
   p.max_rounds = (unsigned)env_u64("ORSP_MAX_ROUNDS", 4ull * g->N + 4096ull);
   p.wait_ns = env_u64("ORSP_WAIT_NS", 2000000000ull);
   p.budget_ns = env_u64("ORSP_BUDGET_NS", 20000000000ull);
@@ -474,7 +528,7 @@ extern "C" int orsp_sssp(orsp_graph *g, const float *cost_d, int32_t nseeds,
                          float *dist_out_d, int32_t *path_out_d, int32_t path_cap,
                          int32_t *path_len_h, int32_t *rounds_h, uintptr_t stream) {
   if (!g || !cost_d || nseeds <= 0 || !seeds_d) { set_error("NULL graph/cost/seeds"); return ORSP_ERR_ARG; }
-  if (!(delta > 0.0f) || !(delta < 3.0e38f)) { set_error("delta must be finite and > 0"); return ORSP_ERR_ARG; }
+  if (!(delta >= 0.0f) || !(delta < 3.0e38f)) { set_error("delta must be finite and >= 0 (0: chosen on the device)"); return ORSP_ERR_ARG; }
   if (dst < -1 || dst >= g->N) { set_error("dst out of range"); return ORSP_ERR_ARG; }
   if (dst >= 0 && (!path_out_d || path_cap <= 0 || !path_len_h)) {
     set_error("a destination needs path_out_d, path_cap > 0 and path_len_h");
@@ -548,7 +602,7 @@ extern "C" int orsp_sssp_multi(orsp_graph *g, const float *cost_d, int32_t nseed
     set_error("sssp_multi: NULL argument or empty seeds / targets");
     return ORSP_ERR_ARG;
   }
-  if (!(delta > 0.0f) || !(delta < 3.0e38f)) { set_error("delta must be finite and > 0"); return ORSP_ERR_ARG; }
+  if (!(delta >= 0.0f) || !(delta < 3.0e38f)) { set_error("delta must be finite and >= 0 (0: chosen on the device)"); return ORSP_ERR_ARG; }
   ORSP_CUDA(cudaSetDevice(g->device));
   cudaStream_t st = (cudaStream_t)stream;
   int rc = ensure_single_ws(g, true);

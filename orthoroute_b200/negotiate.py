@@ -349,7 +349,7 @@ class PathFinder:
                 acc.update_costs(self.base, pres_fac, cfg.hist_cost_weight, add_jitter=cfg.add_jitter,
                                  via_cost_multiplier=cfg.via_cost_multiplier, base_cost_weight=cfg.base_cost_weight)
             cost = acc.total_cost
-            delta = cfg.delta if cfg.delta is not None else DeviceGraph.default_delta(cost)
+            delta = cfg.delta if cfg.delta is not None else 0.0  # 0: chosen on the device
             if it == 1 or cfg.reroute == "all":
                 idx = all_idx
             else:

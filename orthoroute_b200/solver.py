@@ -73,6 +73,7 @@ class DeviceGraph:
         self._path_buf = None
         self._edge_buf = None
         self._g2r_buf = None
+        self._seed_buf = None
 
     @classmethod
     def from_lattice(cls, lat, device=None) -> "DeviceGraph":
@@ -99,29 +100,24 @@ class DeviceGraph:
             self._path_buf = torch.empty(cap, dtype=torch.int32, device=self.device)
         return self._path_buf
 
-    @staticmethod
-    def default_delta(cost: torch.Tensor) -> float:
-        """Bucket width: twice the mean of a strided sample of finite costs."""
-        n = cost.numel()
-        step = max(1, n // 65536)
-        s = cost[::step]
-        s = s[torch.isfinite(s)]
-        if s.numel() == 0:
-            return 1.0
-        m = float(s.mean())
-        return max(2.0 * m, 1e-6)
-
     # --------------------------------------------------------------- searches
     def sssp(self, cost: torch.Tensor, seeds, dst: int = -1, roi_map: Optional[torch.Tensor] = None,
              seed_cost: Optional[torch.Tensor] = None, delta: Optional[float] = None,
              dist_out: Optional[torch.Tensor] = None, path_cap: Optional[int] = None):
-        """Runs the persistent grid search.  Returns (status, path tensor (device,
-        int32, possibly empty), rounds)."""
+        """One search (orsp_sssp: the lattice tile sweep or the generic grid
+        search).  Returns (status, path tensor (device, int32, possibly empty),
+        rounds)."""
         lib = _lib.load()
-        seeds_t = as_device(np.atleast_1d(seeds) if not isinstance(seeds, torch.Tensor) else seeds,
-                            torch.int32, self.device)
+        if isinstance(seeds, (int, np.integer)):
+            # one seed: a device fill instead of a host->device copy
+            if self._seed_buf is None:
+                self._seed_buf = torch.empty(1, dtype=torch.int32, device=self.device)
+            seeds_t = self._seed_buf.fill_(int(seeds))
+        else:
+            seeds_t = as_device(np.atleast_1d(seeds) if not isinstance(seeds, torch.Tensor) else seeds,
+                                torch.int32, self.device)
         if delta is None:
-            delta = self.default_delta(cost)
+            delta = 0.0  # chosen on the device
         cap = int(path_cap or min(self.N + 1, DEFAULT_PATH_CAP))
         pbuf = self._path_buffer(cap) if dst >= 0 else None
         plen = ctypes.c_int32(0)
@@ -145,7 +141,7 @@ class DeviceGraph:
         sc = None if seed_cost is None else as_device(seed_cost, torch.float32, self.device)
         tc = None if target_cost is None else as_device(target_cost, torch.float64, self.device)
         if delta is None:
-            delta = self.default_delta(cost)
+            delta = 0.0  # chosen on the device
         cap = int(path_cap or min(self.N + 1, DEFAULT_PATH_CAP))
         pbuf = self._path_buffer(cap)
         plen = ctypes.c_int32(0)
@@ -170,7 +166,7 @@ class DeviceGraph:
         lib = _lib.load()
         K = int(src.numel())
         if delta is None:
-            delta = self.default_delta(cost)
+            delta = 0.0  # chosen on the device
         nodes = torch.empty((K, path_cap), dtype=torch.int32, device=self.device)
         edges = torch.empty((K, path_cap), dtype=torch.int32, device=self.device) if with_edges else None
         lens = torch.zeros(K, dtype=torch.int32, device=self.device)
@@ -349,7 +345,7 @@ class GpuSolver:
         dst_d = torch.from_numpy(dst).to(self.dg.device)
         ranges_d = torch.from_numpy(ranges).to(self.dg.device)
         check(lib.orsp_sssp_batch_ranges(dg.handle, ptr(wt), K, ptr(src_d), ptr(dst_d), ptr(ranges_d), None,
-                                         float(DeviceGraph.default_delta(wt)), ptr(nodes), None, cap, ptr(lens),
+                                         0.0, ptr(nodes), None, cap, ptr(lens),
                                          _stream()), "orsp_sssp_batch_ranges")
         lens_h = lens.cpu().numpy()
         nodes_h = nodes.cpu().numpy()

@@ -135,7 +135,7 @@ def test_sssp_full_distances_bit_exact(shape, blocked, planar, impl, monkeypatch
     rng = np.random.default_rng(7)
     for s in rng.choice(lat.N, size=3, replace=False):
         _, ref_dist, _, _ = O.dijkstra(lat.indptr, lat.indices, w, [int(s)])
-        for delta in (0.37, 2.0, 1e4):
+        for delta in (0.37, 2.0, 1e4, 0.0):  # 0.0: width chosen on the device
             dist = torch.empty(lat.N, dtype=torch.float32, device="cuda")
             st, _, rounds = dg.sssp(wt, int(s), -1, delta=delta, dist_out=dist)
             assert st == _lib.ORSP_OK
@@ -176,9 +176,10 @@ def test_sssp_edge_cases():
     # path longer than path_cap -> overflow error, not a fault
     with pytest.raises(_lib.OrspError):
         dg.sssp(wt, 0, lat.N - 1, path_cap=3)
-    # bad delta rejected on the host
-    with pytest.raises(_lib.OrspError):
-        dg.sssp(wt, 0, 1, delta=0.0)
+    # bad delta rejected on the host (0.0 means "chosen on the device")
+    for bad in (-1.0, float("nan"), float("inf")):
+        with pytest.raises(_lib.OrspError):
+            dg.sssp(wt, 0, 1, delta=bad)
 
 
 def test_batch_bbox_matches_oracle():
