@@ -41,6 +41,12 @@ NX, NY, NZ = 1000, 1000, 12
 NSRC = 64
 BLOCKED = 0.05
 SEED = 20261203
+# DRAM bytes (read + write) per lattice node of one lattice_async_kernel launch,
+# from ncu (dram__bytes_read.sum + dram__bytes_write.sum) on one full search of
+# a 600x600x12 lattice: 95.78 MB for 4.32 M nodes.  The search settles every
+# node, and its traffic is the gathered weights plus the distances read once,
+# so it scales with the node count.
+LAT_DRAM_BYTES_PER_NODE = 95.78e6 / (600 * 600 * 12)
 
 
 def _peaks():
@@ -342,7 +348,9 @@ def run_ours(args, world, rank, local):
                 "h2d_bytes_per_step": int(w.nbytes), "d2h_bytes_per_step": int(lat.N * 4 * len(sources))},
         "gpu_launches": int(launches * 4),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 5), "traffic": None,
+                     "frac": round(achieved / peak, 5),
+                     "traffic": int(LAT_DRAM_BYTES_PER_NODE * lat.N),
+                     "traffic_source": "ncu dram bytes of a 600x600x12 launch, scaled by node count",
                      "kernel": "lattice_async_kernel", "peak_kind": peak_kind,
                      "bytes_per_launch": int(bytes_alg / len(sources)),
                      "avg_launch_ms": round(avg_kernel_ms, 4)},
