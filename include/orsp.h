@@ -115,6 +115,19 @@ ORSP_API int orsp_sssp(orsp_graph *g, const float *cost_d, int32_t nseeds,
               int32_t *path_out_d, int32_t path_cap, int32_t *path_len_h,
               int32_t *rounds_h, uintptr_t stream);
 
+/* The same search inside an axis-aligned box ROI (inclusive bounds
+ * x0,x1,y0,y1,z0,z1 in the host array box_h[6]): identical, bit for bit, to
+ * orsp_sssp with roi_map_d = the orsp_roi_box_map of the box (the bounding
+ * box + margin ROI of the benchmark router, searched by
+ * SimpleDijkstra.find_path_roi, UPF:1801-1887; the box-local index order is
+ * the node-id order).  On a recognised H/V lattice only the box's tiles are
+ * gathered and swept; dist_out_d (optional) is +inf outside the box. */
+ORSP_API int orsp_sssp_box(orsp_graph *g, const float *cost_d, int32_t nseeds,
+                  const int32_t *seeds_d, const float *seed_cost_d, int32_t dst,
+                  const int32_t *box_h, float delta, float *dist_out_d,
+                  int32_t *path_out_d, int32_t path_cap, int32_t *path_len_h,
+                  int32_t *rounds_h, uintptr_t stream);
+
 /* Multi-seed / multi-target search with portal costs, as
  * SimpleDijkstra.find_path_multisource_multisink (UPF:1889-1989): seeds start
  * at seed_cost (NULL = 0.0), the search runs to completion inside the ROI,

@@ -48,6 +48,8 @@ _SIGS = {
     "orsp_graph_max_degree": (ctypes.c_int, [_P, ctypes.POINTER(_i32)]),
     "orsp_sssp": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _f32, _P, _P, _i32,
                                  ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
+    "orsp_sssp_box": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _f32, _P, _P, _i32,
+                                     ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
     "orsp_sssp_multi": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _P, _P, _f32, _P, _i32,
                                        ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
     "orsp_roi_from_bitmap": (ctypes.c_int, [_P, _P, _P, _u]),

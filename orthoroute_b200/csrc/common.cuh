@@ -64,6 +64,7 @@ struct Graph {
   size_t scratch_bytes = 0;
   void *pinned = nullptr;  // small pinned host buffer for results
   float *auto_delta = nullptr;  // [2] device bucket widths chosen by the library (single, batch)
+  int32_t *box_g2r = nullptr;   // [N] box ROI map for box searches on the generic path (lazy)
   // H/V lattice description, set when every CSR edge is a unit step along the
   // layer's routing axis or a via to an adjacent layer (see orsp_lattice.cu)
   bool lattice_ok = false;
@@ -96,7 +97,7 @@ int launch_auto_delta(const float *cost_d, int64_t E, float *out_d, cudaStream_t
 int analyze_lattice(Graph *g, const int32_t *indptr_h, const int32_t *indices_h);
 void free_lattice(Graph *g);
 int run_lattice_search(Graph *g, const float *cost_d, int32_t nseeds, const int32_t *seeds_d,
-                       const float *seed_cost_d, uint32_t *dist, cudaStream_t st);
+                       const float *seed_cost_d, const int32_t *box, uint32_t *dist, cudaStream_t st);
 int finish_lattice_search(Graph *g, int32_t *rounds_h);
 
 }  // namespace orsp

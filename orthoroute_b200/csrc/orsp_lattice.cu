@@ -81,6 +81,24 @@ __global__ void gather_kernel(const int32_t *__restrict__ slot_eid, const float 
   }
 }
 
+// The same gather for the nodes of a box only (x fastest, then y, then z).
+__global__ void gather_box_kernel(const int32_t *__restrict__ slot_eid, const float *__restrict__ cost,
+                                  float4 *__restrict__ w, int64_t n, int32_t nx, int32_t ny, int32_t x0,
+                                  int32_t bw, int32_t y0, int32_t bh, int32_t z0, int64_t count) {
+  const float INF_F = __int_as_float(0x7f800000);
+  const int64_t s = (int64_t)gridDim.x * blockDim.x;
+  const int64_t plane = (int64_t)bw * bh;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += s) {
+    const int64_t z = i / plane;
+    const int64_t r = i - z * plane;
+    const int32_t y = (int32_t)(r / bw), x = (int32_t)(r - (int64_t)y * bw);
+    const int64_t v = ((int64_t)(z0 + z) * ny + (y0 + y)) * nx + (x0 + x);
+    const int32_t e0 = slot_eid[v], e1 = slot_eid[n + v], e2 = slot_eid[2 * n + v], e3 = slot_eid[3 * n + v];
+    w[v] = make_float4(e0 >= 0 ? __ldg(&cost[e0]) : INF_F, e1 >= 0 ? __ldg(&cost[e1]) : INF_F,
+                       e2 >= 0 ? __ldg(&cost[e2]) : INF_F, e3 >= 0 ? __ldg(&cost[e3]) : INF_F);
+  }
+}
+
 template <int TX, int TY>
 __device__ __forceinline__ int tile_of(const LatParams &p, int32_t gx, int32_t gy) {
   return ((gy - p.by0) / TY) * p.ntx + (gx - p.bx0) / TX;
@@ -681,13 +699,27 @@ void free_lattice(Graph *g) {
   g->lat_ctl_h = nullptr;
 }
 
-// Full-lattice search (the box is the whole lattice).  Leaves the distances
-// in `dist`; finish_lattice_search reports the status after the stream sync.
+// Search over the box [x0,x1]x[y0,y1]x[z0,z1] (box == nullptr: the whole
+// lattice).  Every distance is reset to +inf, so nodes outside the box stay
+// unreachable for the backtrace; only the box's weights are gathered and only
+// its tiles are visited.  Leaves the distances in `dist`;
+// finish_lattice_search reports the status after the stream sync.
 int run_lattice_search(Graph *g, const float *cost_d, int32_t nseeds, const int32_t *seeds_d,
-                       const float *seed_cost_d, uint32_t *dist, cudaStream_t st) {
+                       const float *seed_cost_d, const int32_t *box, uint32_t *dist, cudaStream_t st) {
   const int64_t N = g->N;
-  gather_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 148 * 32), 256, 0, st>>>(
-      g->slot_eid, cost_d, (float4 *)g->wslot, N);
+  const int32_t full[6] = {0, g->nx - 1, 0, g->ny - 1, 0, g->nz - 1};
+  const int32_t *b = box ? box : full;
+  const bool whole = b[0] == 0 && b[1] == g->nx - 1 && b[2] == 0 && b[3] == g->ny - 1 && b[4] == 0 &&
+                     b[5] == g->nz - 1;
+  if (whole) {
+    gather_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 148 * 32), 256, 0, st>>>(
+        g->slot_eid, cost_d, (float4 *)g->wslot, N);
+  } else {
+    const int32_t bw = b[1] - b[0] + 1, bh = b[3] - b[2] + 1;
+    const int64_t count = (int64_t)bw * bh * (b[5] - b[4] + 1);
+    gather_box_kernel<<<(int)std::min<int64_t>((count + 255) / 256, 148 * 32), 256, 0, st>>>(
+        g->slot_eid, cost_d, (float4 *)g->wslot, N, g->nx, g->ny, b[0], bw, b[2], bh, b[4], count);
+  }
   ORSP_CUDA(cudaGetLastError());
   fill_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 148 * 32), 256, 0, st>>>(dist, N, ORSP_INF_BITS);
   ORSP_CUDA(cudaGetLastError());
@@ -695,12 +727,12 @@ int run_lattice_search(Graph *g, const float *cost_d, int32_t nseeds, const int3
   p.nx = g->nx;
   p.ny = g->ny;
   p.nz = g->nz;
-  p.bx0 = 0;
-  p.bx1 = g->nx - 1;
-  p.by0 = 0;
-  p.by1 = g->ny - 1;
-  p.bz0 = 0;
-  p.bz1 = g->nz - 1;
+  p.bx0 = b[0];
+  p.bx1 = b[1];
+  p.by0 = b[2];
+  p.by1 = b[3];
+  p.bz0 = b[4];
+  p.bz1 = b[5];
   p.w4 = (const float4 *)g->wslot;
   p.dist = dist;
   for (int z = 0; z < 64; ++z) p.axis[z] = z < g->nz ? g->layer_axis[z] : 0;

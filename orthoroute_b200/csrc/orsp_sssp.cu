@@ -522,11 +522,12 @@ int run_grid_search(Graph *g, const float *cost_d, int32_t nseeds,
 
 using namespace orsp;
 
-extern "C" int orsp_sssp(orsp_graph *g, const float *cost_d, int32_t nseeds,
-                         const int32_t *seeds_d, const float *seed_cost_d,
-                         int32_t dst, const int32_t *roi_map_d, float delta,
-                         float *dist_out_d, int32_t *path_out_d, int32_t path_cap,
-                         int32_t *path_len_h, int32_t *rounds_h, uintptr_t stream) {
+// One search over the whole graph, the ROI of roi_map_d, or the box box_h
+// (at most one of the two).  Shared by orsp_sssp and orsp_sssp_box.
+static int sssp_impl(orsp_graph *g, const float *cost_d, int32_t nseeds, const int32_t *seeds_d,
+                     const float *seed_cost_d, int32_t dst, const int32_t *roi_map_d, const int32_t *box_h,
+                     float delta, float *dist_out_d, int32_t *path_out_d, int32_t path_cap,
+                     int32_t *path_len_h, int32_t *rounds_h, uintptr_t stream) {
   if (!g || !cost_d || nseeds <= 0 || !seeds_d) { set_error("NULL graph/cost/seeds"); return ORSP_ERR_ARG; }
   if (!(delta >= 0.0f) || !(delta < 3.0e38f)) { set_error("delta must be finite and >= 0 (0: chosen on the device)"); return ORSP_ERR_ARG; }
   if (dst < -1 || dst >= g->N) { set_error("dst out of range"); return ORSP_ERR_ARG; }
@@ -539,14 +540,21 @@ extern "C" int orsp_sssp(orsp_graph *g, const float *cost_d, int32_t nseeds,
   int rc = ensure_single_ws(g, dist_out_d == nullptr);
   if (rc) return rc;
   uint32_t *dist = dist_out_d ? (uint32_t *)dist_out_d : g->dist;
-  // Full-graph searches on a recognised H/V lattice use the tile-sweep search
-  // (orsp_lattice.cu); ROI-restricted searches and other graphs use the
-  // generic near-far search.  ORSP_SSSP_IMPL=generic forces the latter.
+  // Full-graph and box searches on a recognised H/V lattice use the
+  // tile-sweep search (orsp_lattice.cu); node-set ROIs and other graphs use
+  // the generic near-far search, a box there becoming its ROI map.
+  // ORSP_SSSP_IMPL=generic forces the latter.
   const char *impl = getenv("ORSP_SSSP_IMPL");
   const bool lattice = g->lattice_ok && roi_map_d == nullptr &&
                        !(impl && std::string(impl) == "generic");
+  if (box_h && !lattice) {
+    if (!g->box_g2r) ORSP_CUDA(cudaMalloc(&g->box_g2r, (size_t)g->N * 4));
+    rc = orsp_roi_box_map(g, box_h, g->box_g2r, stream);
+    if (rc) return rc;
+    roi_map_d = g->box_g2r;
+  }
   if (lattice) {
-    rc = run_lattice_search(g, cost_d, nseeds, seeds_d, seed_cost_d, dist, st);
+    rc = run_lattice_search(g, cost_d, nseeds, seeds_d, seed_cost_d, box_h, dist, st);
     if (rc) return rc;
     ORSP_CUDA(cudaMemsetAsync(g->ctl, 0, sizeof(SsspCtl), st));
   } else {
@@ -590,6 +598,32 @@ extern "C" int orsp_sssp(orsp_graph *g, const float *cost_d, int32_t nseeds,
     }
   }
   return ORSP_OK;
+}
+
+extern "C" int orsp_sssp(orsp_graph *g, const float *cost_d, int32_t nseeds,
+                         const int32_t *seeds_d, const float *seed_cost_d,
+                         int32_t dst, const int32_t *roi_map_d, float delta,
+                         float *dist_out_d, int32_t *path_out_d, int32_t path_cap,
+                         int32_t *path_len_h, int32_t *rounds_h, uintptr_t stream) {
+  return sssp_impl(g, cost_d, nseeds, seeds_d, seed_cost_d, dst, roi_map_d, nullptr, delta, dist_out_d,
+                   path_out_d, path_cap, path_len_h, rounds_h, stream);
+}
+
+extern "C" int orsp_sssp_box(orsp_graph *g, const float *cost_d, int32_t nseeds,
+                             const int32_t *seeds_d, const float *seed_cost_d, int32_t dst,
+                             const int32_t *box_h, float delta, float *dist_out_d,
+                             int32_t *path_out_d, int32_t path_cap, int32_t *path_len_h,
+                             int32_t *rounds_h, uintptr_t stream) {
+  if (!g || !box_h) { set_error("sssp_box: NULL graph or box"); return ORSP_ERR_ARG; }
+  if (g->nx <= 0) { set_error("sssp_box: graph has no lattice dims"); return ORSP_ERR_ARG; }
+  const int32_t *b = box_h;
+  if (b[0] < 0 || b[2] < 0 || b[4] < 0 || b[1] >= g->nx || b[3] >= g->ny || b[5] >= g->nz ||
+      b[1] < b[0] || b[3] < b[2] || b[5] < b[4]) {
+    set_error("sssp_box: box outside the lattice or empty");
+    return ORSP_ERR_ARG;
+  }
+  return sssp_impl(g, cost_d, nseeds, seeds_d, seed_cost_d, dst, nullptr, box_h, delta, dist_out_d,
+                   path_out_d, path_cap, path_len_h, rounds_h, stream);
 }
 
 extern "C" int orsp_sssp_multi(orsp_graph *g, const float *cost_d, int32_t nseeds, const int32_t *seeds_d,

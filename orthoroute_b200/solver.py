@@ -128,6 +128,26 @@ class DeviceGraph:
         path = pbuf[: plen.value] if (dst >= 0 and st == _lib.ORSP_OK) else None
         return st, path, int(rounds.value)
 
+    def sssp_box(self, cost: torch.Tensor, src: int, dst: int, box, delta: Optional[float] = None,
+                 dist_out: Optional[torch.Tensor] = None, path_cap: Optional[int] = None):
+        """One search inside the inclusive box (x0, x1, y0, y1, z0, z1): the
+        result of sssp() with the box's ROI map, without building the map.
+        Returns (status, path tensor or None, rounds)."""
+        lib = _lib.load()
+        if self._seed_buf is None:
+            self._seed_buf = torch.empty(1, dtype=torch.int32, device=self.device)
+        seeds_t = self._seed_buf.fill_(int(src))
+        bx = (ctypes.c_int32 * 6)(*[int(v) for v in box])
+        cap = int(path_cap or min(self.N + 1, DEFAULT_PATH_CAP))
+        pbuf = self._path_buffer(cap) if dst >= 0 else None
+        plen = ctypes.c_int32(0)
+        rounds = ctypes.c_int32(0)
+        st = check(lib.orsp_sssp_box(self._h, ptr(cost), 1, ptr(seeds_t), None, int(dst), bx,
+                                     float(0.0 if delta is None else delta), ptr(dist_out), ptr(pbuf), cap,
+                                     ctypes.byref(plen), ctypes.byref(rounds), _stream()), "orsp_sssp_box")
+        path = pbuf[: plen.value] if (dst >= 0 and st == _lib.ORSP_OK) else None
+        return st, path, int(rounds.value)
+
     def sssp_multi(self, cost: torch.Tensor, seeds, targets, seed_cost=None, target_cost=None,
                    roi_map: Optional[torch.Tensor] = None, delta: Optional[float] = None,
                    path_cap: Optional[int] = None):

@@ -388,3 +388,48 @@ def test_find_paths_on_rois_local_csr_batch():
         refs.append(ref.tolist() if len(ref) > 1 else None)
     got = solver.find_paths_on_rois(batch, use_bitmap=True)
     assert got == refs
+
+
+@pytest.mark.parametrize("impl", ["lattice16", "lattice32", "lattice16-rounds", "generic"])
+def test_sssp_box_matches_box_roi_and_oracle(impl, monkeypatch):
+    """orsp_sssp_box == orsp_sssp with the box's ROI map == the oracle with that
+    ROI: distances (full searches) and paths, for boxes at the border, thin
+    boxes, single-layer boxes and endpoints outside the box."""
+    monkeypatch.setenv("ORSP_SSSP_IMPL", "generic" if impl == "generic" else "auto")
+    monkeypatch.setenv("ORSP_LAT_TILE", "32" if impl == "lattice32" else "16")
+    monkeypatch.setenv("ORSP_LAT_ASYNC", "0" if impl.endswith("rounds") else "1")
+    lat = build_lattice(75, 58, 6)
+    w = uniform_weights(lat, seed=21, blocked_frac=0.04)
+    dg = DeviceGraph.from_lattice(lat)
+    wt = cuda(w)
+    rng = np.random.default_rng(13)
+    nxy = lat.nx * lat.ny
+    boxes = [(0, 74, 0, 57, 0, 5), (0, 20, 30, 57, 0, 5), (40, 74, 0, 15, 1, 4), (10, 11, 5, 50, 0, 5),
+             (5, 60, 20, 20, 0, 5), (3, 40, 3, 40, 2, 2), (17, 49, 9, 33, 0, 3)]
+    for k, b in enumerate(boxes):
+        x0, x1, y0, y1, z0, z1 = b
+        g2r = np.full(lat.N, -1, np.int32)
+        zz, yy, xx = np.meshgrid(np.arange(z0, z1 + 1), np.arange(y0, y1 + 1), np.arange(x0, x1 + 1), indexing="ij")
+        inside = (zz * nxy + yy * lat.nx + xx).ravel()
+        g2r[inside] = np.arange(inside.size, dtype=np.int32)
+        for j in range(4):
+            s = int(inside[rng.integers(inside.size)])
+            d = int(inside[rng.integers(inside.size)]) if j < 3 else int(rng.integers(lat.N))
+            ref, ref_dist, _, _ = O.dijkstra(lat.indptr, lat.indices, w, [s], dst=-1, roi_map=g2r)
+            dist = torch.empty(lat.N, dtype=torch.float32, device="cuda")
+            st, _, _ = dg.sssp_box(wt, s, -1, b, dist_out=dist)
+            assert st == _lib.ORSP_OK
+            assert np.array_equal(_bits(dist.cpu().numpy()), _bits(ref_dist)), f"box {k} src {s}"
+            refp, *_ = O.dijkstra(lat.indptr, lat.indices, w, [s], dst=d, roi_map=g2r)
+            st, p, _ = dg.sssp_box(wt, s, d, b)
+            got = p.cpu().tolist() if (st == _lib.ORSP_OK and p is not None) else []
+            assert got == (refp.tolist() if len(refp) > 1 else []), f"box {k} {s}->{d}"
+            st2, p2, _ = dg.sssp(wt, s, d, roi_map=cuda(g2r))
+            got2 = p2.cpu().tolist() if (st2 == _lib.ORSP_OK and p2 is not None) else []
+            assert got2 == got
+    # a source outside the box reaches nothing
+    st, p, _ = dg.sssp_box(wt, 0, 5, (10, 20, 10, 20, 0, 5))
+    assert st == _lib.ORSP_NO_PATH
+    for bad in [(0, 75, 0, 10, 0, 5), (5, 4, 0, 10, 0, 5), (0, 10, -1, 10, 0, 5), (0, 10, 0, 10, 0, 6)]:
+        with pytest.raises(_lib.OrspError):
+            dg.sssp_box(wt, 0, 5, bad)
