@@ -89,6 +89,12 @@ ORSP_API int orsp_graph_csr(orsp_graph *g, const int32_t **indptr_d,
                    const int32_t **indices_d);
 /* Largest out-degree (known after create). */
 ORSP_API int orsp_graph_max_degree(orsp_graph *g, int32_t *out);
+/* 1 when the graph was recognised as an H/V routing lattice (every edge a
+ * unit step along its layer's axis or a via between adjacent layers, no
+ * parallel edges): full-graph and box searches then use the tile sweeps and
+ * orsp_route_nets is available.  0 otherwise.  (No reference counterpart:
+ * the reference has one search path for every graph.) */
+ORSP_API int orsp_graph_is_lattice(orsp_graph *g, int32_t *out);
 
 /* ---- single search ----------------------------------------------------- */
 /* Single-source (or multi-seed) shortest path over the whole graph or over
@@ -183,6 +189,37 @@ ORSP_API int orsp_sssp_batch_ranges(orsp_graph *g, const float *cost_d, int32_t 
                            float delta, int32_t *path_nodes_d,
                            int32_t *path_edges_d, int32_t path_cap,
                            int32_t *path_len_d, uintptr_t stream);
+
+/* ---- routing loop ------------------------------------------------------ */
+/* Routes nets with per-net live costs, as the per-net body of _route_all
+ * (UPF:4475-4800) with the live-usage cost refresh of orsp_update_costs_live.
+ * For each net k = order_h[i] (i < K, each net at most once): rip up its
+ * previous path (row k of net_edges_d, net_lens_d[k] nodes; usage -1 and live
+ * costs of those edges), search src_h[k] -> dst_h[k] inside its box
+ * (box_h[6k..6k+5], as orsp_sssp_box) on the costs as they are now, write the
+ * node path, its edges (first CSR edge per pair, UPF:5463) and its length
+ * (0 = no path; also when src lies outside the box) into row k, then commit
+ * it (usage +1, live costs).
+ *   group_ptr_h[G+1]   optional: the order is cut into groups
+ *                      [group_ptr[q], group_ptr[q+1]) of at most 1024 nets with
+ *                      pairwise disjoint boxes (checked); a group's nets are
+ *                      ripped up, searched in one tile-sweep launch and
+ *                      committed together.  NULL: one net per group.
+ * With every net's previous path inside its box (boxes that never shrink),
+ * nets of one group read and write disjoint edges, so the result is bit for
+ * bit the one-net-at-a-time result in the same order (the host loop over
+ * orsp_commit_edges / orsp_update_costs_live / orsp_sssp_box /
+ * orsp_path_to_edges).  Everything is enqueued without host synchronisation
+ * (one sync at the end).  Rows are path_cap wide; src_h, dst_h and box_h are
+ * host arrays over all M nets.  Needs a graph recognised as an H/V lattice.
+ * usage_d/present_d/cost_d are updated in place. */
+ORSP_API int orsp_route_nets(orsp_graph *g, int32_t M, const int32_t *src_h, const int32_t *dst_h,
+                    const int32_t *box_h, int32_t K, const int32_t *order_h, int32_t G,
+                    const int32_t *group_ptr_h, int32_t *net_nodes_d, int32_t *net_edges_d,
+                    int32_t path_cap, int32_t *net_lens_d, float *cost_d, const float *base_d,
+                    int32_t *usage_d, float *present_d, const float *cap_d, const float *hist_d,
+                    float pres_fac, float hist_w, float via_mult, float base_w, int32_t jitter,
+                    uintptr_t stream);
 
 /* ---- ROI extraction ---------------------------------------------------- */
 /* Bidirectional level-synchronous BFS ROI, as ROIExtractor.extract_roi_bfs

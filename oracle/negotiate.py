@@ -16,6 +16,22 @@ import numpy as np
 from . import orsp_oracle as O
 
 
+def _first_fit_rounds(boxes, idx):
+    """idx regrouped into rounds: a net joins the lowest round holding no box
+    that meets its box; rounds concatenated in order."""
+    rounds = []
+    for k in idx:
+        bk = boxes[k]
+        for r in rounds:
+            if not any(bk[0] <= boxes[q][1] and boxes[q][0] <= bk[1] and bk[2] <= boxes[q][3] and
+                       boxes[q][2] <= bk[3] and bk[4] <= boxes[q][5] and boxes[q][4] <= bk[5] for q in r):
+                r.append(k)
+                break
+        else:
+            rounds.append([k])
+    return np.array([k for r in rounds for k in r], dtype=np.int64)
+
+
 def route_plain(lat, src, dst, cfg, base_cost=None, history_init=None, max_nets_per_iter=None):
     """Returns dict(trace=[(over_sum, over_cnt, failed)], paths=[...], usage, converged, seconds)."""
     from orthoroute_b200.lattice import bbox_with_margin  # pure numpy helper
@@ -27,7 +43,11 @@ def route_plain(lat, src, dst, cfg, base_cost=None, history_init=None, max_nets_
     E = lat.E
     base = (lat.base_cost if base_cost is None else base_cost).astype(np.float32)
     cap_paths = cfg.path_cap
-    boxes = bbox_with_margin(lat, src, dst, cfg.roi_margin)
+    margins = np.full(M, cfg.roi_margin, dtype=np.int64)
+    streak = np.zeros(M, dtype=np.int64)
+    boxes = bbox_with_margin(lat, src, dst, margins)
+    stall_grow = getattr(cfg, "stall_grow", 0)
+    net_order = getattr(cfg, "net_order", "index")
     full_box = np.array([[0, lat.nx - 1, 0, lat.ny - 1, 0, lat.nz - 1]], dtype=np.int32)
     usage = np.zeros(E, dtype=np.int64)
     capacity = np.ones(E, dtype=np.float32)
@@ -53,12 +73,21 @@ def route_plain(lat, src, dst, cfg, base_cost=None, history_init=None, max_nets_
     for it in range(1, cfg.max_iterations + 1):
         if net_policy:
             cost = live_cost(np.arange(E))
-            if it == 1 or cfg.reroute == "all":
-                idx = np.arange(M)
-            else:
-                over_e = usage.astype(np.float32) > capacity
-                idx = np.array([k for k in range(M) if len(net_paths[k]) < 2 or over_e[net_edges[k]].any()],
-                               dtype=np.int64)
+            over_e = usage.astype(np.float32) > capacity
+            off = np.array([k for k in range(M) if len(net_paths[k]) < 2 or over_e[net_edges[k]].any()],
+                           dtype=np.int64)
+            idx = np.arange(M) if (it == 1 or cfg.reroute == "all") else off
+            if stall_grow > 0 and it > 1:
+                # a net offending stall_iterations times running: margin += stall_grow
+                offset = set(off.tolist())
+                for k in range(M):
+                    streak[k] = streak[k] + 1 if k in offset else 0
+                    if streak[k] >= cfg.stall_iterations:
+                        margins[k] += stall_grow
+                        streak[k] = 0
+                boxes = bbox_with_margin(lat, src, dst, margins)
+            if net_order == "disjoint":
+                idx = _first_fit_rounds(boxes, idx)
             for k in idx:  # sequential: rip up, search on live costs, commit
                 e = net_edges[k]
                 if e.size:

@@ -46,10 +46,13 @@ _SIGS = {
     "orsp_graph_destroy": (ctypes.c_int, [_P]),
     "orsp_graph_csr": (ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P)]),
     "orsp_graph_max_degree": (ctypes.c_int, [_P, ctypes.POINTER(_i32)]),
+    "orsp_graph_is_lattice": (ctypes.c_int, [_P, ctypes.POINTER(_i32)]),
     "orsp_sssp": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _f32, _P, _P, _i32,
                                  ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
     "orsp_sssp_box": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _f32, _P, _P, _i32,
                                      ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
+    "orsp_route_nets": (ctypes.c_int, [_P, _i32, _P, _P, _P, _i32, _P, _i32, _P, _P, _P, _i32, _P, _P, _P, _P, _P,
+                                       _P, _P, _f32, _f32, _f32, _f32, _i32, _u]),
     "orsp_sssp_multi": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _P, _P, _f32, _P, _i32,
                                        ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
     "orsp_roi_from_bitmap": (ctypes.c_int, [_P, _P, _P, _u]),

@@ -25,6 +25,7 @@ SOURCES = [
     "orsp_roi.cu",
     "orsp_lattice.cu",
     "orsp_via.cu",
+    "orsp_route.cu",
 ]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -65,6 +65,12 @@ struct Graph {
   void *pinned = nullptr;  // small pinned host buffer for results
   float *auto_delta = nullptr;  // [2] device bucket widths chosen by the library (single, batch)
   int32_t *box_g2r = nullptr;   // [N] box ROI map for box searches on the generic path (lazy)
+  // routing loop (orsp_route.cu): error word, per-call net tables (device)
+  // and their pinned staging copy
+  void *route_ws = nullptr;
+  void *route_tab_d = nullptr;
+  void *route_tab_h = nullptr;
+  size_t route_tab_bytes = 0;
   // H/V lattice description, set when every CSR edge is a unit step along the
   // layer's routing axis or a via to an adjacent layer (see orsp_lattice.cu)
   bool lattice_ok = false;
@@ -74,6 +80,7 @@ struct Graph {
   void *lat_ws = nullptr;         // tile lists, stamps and control block
   size_t lat_ws_bytes = 0;
   void *lat_ctl_h = nullptr;      // pinned mirror of the control block
+  void *lat_box_d = nullptr;      // tile table of a single-box search
 };
 
 // Optional timing of a search kernel (CUDA events on the launching stream),
@@ -96,8 +103,38 @@ int launch_auto_delta(const float *cost_d, int64_t E, float *out_d, cudaStream_t
 // orsp_lattice.cu
 int analyze_lattice(Graph *g, const int32_t *indptr_h, const int32_t *indices_h);
 void free_lattice(Graph *g);
+// One box of a lattice search, with its tiles' place in the launch's tile
+// numbering (tiles of TX x TY columns, x fastest, box after box).
+struct LatBox {
+  int32_t x0, x1, y0, y1, z0, z1;
+  int32_t ntx, nty;  // tiles along x and y
+  int32_t tile0;     // id of the box's first tile
+};
+// Tile width of the lattice search (ORSP_LAT_TILE: 16 or 32); the height is 16.
+int lattice_tile_w();
+// Fills out[i] for boxes_h[6i..6i+5] and returns the total tile count.
+int64_t make_lat_boxes(const int32_t *boxes_h, int32_t nbox, LatBox *out);
+struct LatOptions {
+  bool fill_box_only = false;  // reset distances inside the boxes only (the caller's backtrace checks the box)
+  bool copy_ctl = true;        // copy the control block to the pinned mirror (finish_lattice_search)
+  int *err_d = nullptr;        // out: device address of the launch's error word
+};
+// One box (nullptr: the whole lattice).  Stages its tile table through the
+// graph's pinned buffer, so the calling entry point must synchronise before
+// it returns.
 int run_lattice_search(Graph *g, const float *cost_d, int32_t nseeds, const int32_t *seeds_d,
-                       const float *seed_cost_d, const int32_t *box, uint32_t *dist, cudaStream_t st);
+                       const float *seed_cost_d, const int32_t *box, uint32_t *dist, cudaStream_t st,
+                       LatOptions *opt = nullptr);
+// Several pairwise disjoint boxes searched in one launch, sharing the
+// distance array: boxes_h (host, 6 ints per box) sizes the launch, lboxes_d
+// (device, from make_lat_boxes) is what the kernel reads and must stay valid
+// until the launch has run.  Each seed starts in the box that contains it.
+int run_lattice_boxes(Graph *g, const float *cost_d, int32_t nseeds, const int32_t *seeds_d,
+                      const float *seed_cost_d, int32_t nbox, const int32_t *boxes_h, const LatBox *lboxes_d,
+                      uint32_t *dist, cudaStream_t st, LatOptions *opt = nullptr);
+// Grows the lattice workspace for launches of up to `ntiles` tiles, so that
+// later launches never reallocate it (a reallocation synchronises).
+int reserve_lattice_ws(Graph *g, int64_t ntiles);
 int finish_lattice_search(Graph *g, int32_t *rounds_h);
 
 }  // namespace orsp

@@ -175,6 +175,10 @@ extern "C" int orsp_graph_destroy(orsp_graph *g) {
   cudaFree(g->batch_ctl);
   cudaFree(g->scratch);
   cudaFree(g->auto_delta);
+  cudaFree(g->route_ws);
+  cudaFree(g->route_tab_d);
+  if (g->route_tab_h) cudaFreeHost(g->route_tab_h);
+  cudaFree(g->box_g2r);
   if (g->pinned) cudaFreeHost(g->pinned);
   free_lattice(g);
   delete g;
@@ -192,5 +196,11 @@ extern "C" int orsp_graph_csr(orsp_graph *g, const int32_t **indptr_d,
 extern "C" int orsp_graph_max_degree(orsp_graph *g, int32_t *out) {
   if (!g || !out) { set_error("NULL argument"); return ORSP_ERR_ARG; }
   *out = g->max_degree;
+  return ORSP_OK;
+}
+
+extern "C" int orsp_graph_is_lattice(orsp_graph *g, int32_t *out) {
+  if (!g || !out) { set_error("NULL argument"); return ORSP_ERR_ARG; }
+  *out = g->lattice_ok ? 1 : 0;
   return ORSP_OK;
 }

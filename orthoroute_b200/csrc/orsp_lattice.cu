@@ -46,10 +46,12 @@ struct LatCtl {
   unsigned long long ns[4];  // time in load, sweeps, write-back, scheduling (sum over visits)
 };
 
+using orsp::LatBox;
+
 struct LatParams {
   int32_t nx, ny, nz;
-  int32_t bx0, bx1, by0, by1, bz0, bz1;  // searched box (inclusive)
-  int32_t ntx, nty;                       // tiles along x, y
+  int32_t nbox;
+  const LatBox *boxes;                     // searched boxes (pairwise disjoint)
   const float4 *w4;                        // in-edge weights per node
   uint32_t *dist;
   int32_t *list0, *list1;
@@ -66,6 +68,19 @@ struct LatParams {
 __global__ void fill_kernel(uint32_t *p, int64_t n, uint32_t v) {
   const int64_t s = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += s) p[i] = v;
+}
+
+// The same fill over the nodes of a box (x fastest).
+__global__ void fill_box_kernel(uint32_t *p, int32_t nx, int32_t ny, int32_t x0, int32_t bw, int32_t y0,
+                                int32_t bh, int32_t z0, int64_t count, uint32_t v) {
+  const int64_t s = (int64_t)gridDim.x * blockDim.x;
+  const int64_t plane = (int64_t)bw * bh;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += s) {
+    const int64_t z = i / plane;
+    const int64_t r = i - z * plane;
+    const int32_t y = (int32_t)(r / bw), x = (int32_t)(r - (int64_t)y * bw);
+    p[((int64_t)(z0 + z) * ny + (y0 + y)) * nx + (x0 + x)] = v;
+  }
 }
 
 // In-edge weights of node v as one float4 {from lower axis neighbour, from
@@ -99,9 +114,35 @@ __global__ void gather_box_kernel(const int32_t *__restrict__ slot_eid, const fl
   }
 }
 
+__device__ __forceinline__ LatBox load_box(const LatParams &p, int b) {
+  const int32_t *q = (const int32_t *)(p.boxes + b);
+  LatBox B;
+  B.x0 = __ldg(q + 0);
+  B.x1 = __ldg(q + 1);
+  B.y0 = __ldg(q + 2);
+  B.y1 = __ldg(q + 3);
+  B.z0 = __ldg(q + 4);
+  B.z1 = __ldg(q + 5);
+  B.ntx = __ldg(q + 6);
+  B.nty = __ldg(q + 7);
+  B.tile0 = __ldg(q + 8);
+  return B;
+}
+
+// Box of tile t: the last box whose first tile is <= t.
+__device__ __forceinline__ int box_of_tile(const LatParams &p, int t) {
+  int lo = 0, hi = p.nbox - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&p.boxes[mid].tile0) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 template <int TX, int TY>
-__device__ __forceinline__ int tile_of(const LatParams &p, int32_t gx, int32_t gy) {
-  return ((gy - p.by0) / TY) * p.ntx + (gx - p.bx0) / TX;
+__device__ __forceinline__ int tile_of(const LatBox &B, int32_t gx, int32_t gy) {
+  return B.tile0 + ((gy - B.y0) / TY) * B.ntx + (gx - B.x0) / TX;
 }
 
 template <int TX, int TY>
@@ -127,11 +168,17 @@ __global__ void lattice_seed_kernel(LatParams p, int32_t nseeds, const int32_t *
     const int32_t s = seeds[i];
     if (s < 0 || s >= plane * p.nz) continue;
     const int32_t z = s / plane, r = s - z * plane, y = r / p.nx, x = r - y * p.nx;
-    if (x < p.bx0 || x > p.bx1 || y < p.by0 || y > p.by1 || z < p.bz0 || z > p.bz1) continue;
+    int bi = -1;
+    LatBox B;
+    for (int b = 0; b < p.nbox && bi < 0; ++b) {
+      B = load_box(p, b);
+      if (x >= B.x0 && x <= B.x1 && y >= B.y0 && y <= B.y1 && z >= B.z0 && z <= B.z1) bi = b;
+    }
+    if (bi < 0) continue;
     const float c0 = seed_cost ? seed_cost[i] : 0.0f;
     if (!(c0 >= 0.0f) || !(c0 < __int_as_float(0x7f800000))) continue;
     atomicMin(&p.dist[s], f_bits(c0));
-    const int t = tile_of<TX, TY>(p, x, y);
+    const int t = tile_of<TX, TY>(B, x, y);
     if (p.qslot) {
       if (atomicCAS(&p.tstate[t], 0, 1) == 0) {
         atomicAdd(&c->pending, 1);
@@ -205,18 +252,43 @@ __device__ __forceinline__ bool sweep_run(float *c, int ds, const float *wlo, co
 // weights [4][nzb][TY][TX+1] and the interior distances as loaded
 // [nzb][TY][TX+1] (odd row strides: the row walks of the x-sweep and the
 // column walks of the y- and z-sweeps are bank-conflict free).
+// Layer lists of the box being visited: H layers (x-runs) and V layers
+// (y-runs) as offsets from the box's z0.  Recomputed when a CTA moves to a
+// tile of another box.
+struct LayerLists {
+  int hl[64], vl[64];
+  int nh, nv;
+  int box;
+};
+
 template <int TX, int TY>
-__device__ void process_tile(const LatParams &p, int t, float *sd, const int *s_hl, int nh,
-                             const int *s_vl, int nv, int *s_flags, int *s_act) {
+__device__ __forceinline__ void process_tile(const LatParams &p, int t, float *sd, LayerLists &L, int *s_flags,
+                                             int *s_act) {
+  const int bi = box_of_tile(p, t);
+  const LatBox B = load_box(p, bi);
+  if (threadIdx.x == 0 && L.box != bi) {
+    int nh = 0, nv = 0;
+    for (int z = B.z0; z <= B.z1; ++z) {
+      if (p.axis[z] == 1) L.hl[nh++] = z - B.z0;
+      else if (p.axis[z] == 2) L.vl[nv++] = z - B.z0;
+    }
+    L.nh = nh;
+    L.nv = nv;
+    L.box = bi;
+  }
+  __syncthreads();
+  const int *s_hl = L.hl, *s_vl = L.vl;
+  const int nh = L.nh, nv = L.nv;
   constexpr int SX = TX + 3;
   constexpr int PS = (TY + 2) * SX;
   constexpr int WSX = TX + 1;
   constexpr int WPS = TY * WSX;
   const float INF_F = __int_as_float(0x7f800000);
-  const int tx = t % p.ntx, ty = t / p.ntx;
-  const int32_t X0 = p.bx0 + tx * TX, Y0 = p.by0 + ty * TY;
-  const int tw = min(TX, p.bx1 - X0 + 1), th = min(TY, p.by1 - Y0 + 1);
-  const int nzb = p.bz1 - p.bz0 + 1;
+  const int lt = t - B.tile0;
+  const int tx = lt % B.ntx, ty = lt / B.ntx;
+  const int32_t X0 = B.x0 + tx * TX, Y0 = B.y0 + ty * TY;
+  const int tw = min(TX, B.x1 - X0 + 1), th = min(TY, B.y1 - Y0 + 1);
+  const int nzb = B.z1 - B.z0 + 1;
   const int64_t nxy = (int64_t)p.nx * p.ny;
   const int64_t col0 = (int64_t)Y0 * p.nx + X0;  // node of (X0, Y0, z=0)
   float *wlo = sd + nzb * PS;          // slot 0: from the lower axis neighbour
@@ -237,7 +309,7 @@ __device__ void process_tile(const LatParams &p, int t, float *sd, const int *s_
   // issued back to back
   for (int c = threadIdx.x; c < th * tw; c += blockDim.x) {
     const int yy = c / tw + 1, xx = c - (yy - 1) * tw + 1;
-    const int64_t n0 = (int64_t)p.bz0 * nxy + col0 + (int64_t)(yy - 1) * p.nx + (xx - 1);
+    const int64_t n0 = (int64_t)B.z0 * nxy + col0 + (int64_t)(yy - 1) * p.nx + (xx - 1);
     const int s0 = yy * SX + xx, w0 = (yy - 1) * WSX + (xx - 1);
 #pragma unroll 6
     for (int z = 0; z < nzb; ++z) {
@@ -270,8 +342,8 @@ __device__ void process_tile(const LatParams &p, int t, float *sd, const int *s_
       }
       const int32_t gx = X0 + xx - 1, gy = Y0 + yy - 1;
       float v = INF_F;
-      if (gx >= p.bx0 && gx <= p.bx1 && gy >= p.by0 && gy <= p.by1)
-        v = bits_f(__ldcg(&p.dist[(int64_t)(p.bz0 + z) * nxy + (int64_t)gy * p.nx + gx]));
+      if (gx >= B.x0 && gx <= B.x1 && gy >= B.y0 && gy <= B.y1)
+        v = bits_f(__ldcg(&p.dist[(int64_t)(B.z0 + z) * nxy + (int64_t)gy * p.nx + gx]));
       sd[z * PS + yy * SX + xx] = v;
     }
   }
@@ -334,7 +406,7 @@ __device__ void process_tile(const LatParams &p, int t, float *sd, const int *s_
     const int rem = i - z * th * tw;
     const int yy = rem / tw + 1, xx = rem % tw + 1;
     const float v = sd[z * PS + yy * SX + xx];
-    const int gz = p.bz0 + z;
+    const int gz = B.z0 + z;
     const int64_t node = (int64_t)gz * nxy + col0 + (int64_t)(yy - 1) * p.nx + (xx - 1);
     if (v < orig[z * WPS + (yy - 1) * WSX + (xx - 1)]) {
       __stcg(&p.dist[node], f_bits(v));
@@ -362,12 +434,14 @@ __device__ void process_tile(const LatParams &p, int t, float *sd, const int *s_
 // improved (s_act[0..3] = left, right, down, up) and t itself if it did not
 // converge (s_act[4]).  Returns the count written to nb[0..4].
 __device__ __forceinline__ int revisit_list(const LatParams &p, int t, const int *s_act, int *nb) {
-  const int tx = t % p.ntx, ty = t / p.ntx;
+  const LatBox B = load_box(p, box_of_tile(p, t));
+  const int lt = t - B.tile0;
+  const int tx = lt % B.ntx, ty = lt / B.ntx;
   int k = 0;
   if (s_act[0] && tx > 0) nb[k++] = t - 1;
-  if (s_act[1] && tx < p.ntx - 1) nb[k++] = t + 1;
-  if (s_act[2] && ty > 0) nb[k++] = t - p.ntx;
-  if (s_act[3] && ty < p.nty - 1) nb[k++] = t + p.ntx;
+  if (s_act[1] && tx < B.ntx - 1) nb[k++] = t + 1;
+  if (s_act[2] && ty > 0) nb[k++] = t - B.ntx;
+  if (s_act[3] && ty < B.nty - 1) nb[k++] = t + B.ntx;
   if (s_act[4]) nb[k++] = t;
   return k;
 }
@@ -375,8 +449,7 @@ __device__ __forceinline__ int revisit_list(const LatParams &p, int t, const int
 template <int TX, int TY>
 __global__ void __launch_bounds__(TX * TY) lattice_tile_kernel(LatParams p) {
   extern __shared__ float sd[];
-  __shared__ int s_hl[64], s_vl[64];
-  __shared__ int s_nh, s_nv;
+  __shared__ LayerLists s_layers;
   __shared__ int s_flags[3];
   __shared__ int s_act[5];
   __shared__ int s_tile;
@@ -384,17 +457,8 @@ __global__ void __launch_bounds__(TX * TY) lattice_tile_kernel(LatParams p) {
   const unsigned nblocks = gridDim.x;
   const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
   const unsigned long long t_start = dev_globaltimer();
-  if (threadIdx.x == 0) {
-    int nh = 0, nv = 0;
-    for (int z = p.bz0; z <= p.bz1; ++z) {
-      if (p.axis[z] == 1) s_hl[nh++] = z - p.bz0;
-      else if (p.axis[z] == 2) s_vl[nv++] = z - p.bz0;
-    }
-    s_nh = nh;
-    s_nv = nv;
-  }
+  if (threadIdx.x == 0) s_layers.box = -1;
   __syncthreads();
-  const int nh = s_nh, nv = s_nv;
   unsigned r = 0;
   for (;;) {
     if (ld_acquire_u32((const unsigned *)&ctl->err)) break;
@@ -413,7 +477,7 @@ __global__ void __launch_bounds__(TX * TY) lattice_tile_kernel(LatParams p) {
       __syncthreads();
       if (ti >= (int)n_in) break;
       const int t = __ldcg(&inl[ti]);
-      process_tile<TX, TY>(p, t, sd, s_hl, nh, s_vl, nv, s_flags, s_act);
+      process_tile<TX, TY>(p, t, sd, s_layers, s_flags, s_act);
       if (threadIdx.x == 0) {
         int nb[5];
         const int k = revisit_list(p, t, s_act, nb);
@@ -474,24 +538,14 @@ __device__ bool activate_tile(const LatParams &p, int t) {
 template <int TX, int TY>
 __global__ void __launch_bounds__(TX * TY) lattice_async_kernel(LatParams p) {
   extern __shared__ float sd[];
-  __shared__ int s_hl[64], s_vl[64];
-  __shared__ int s_nh, s_nv;
+  __shared__ LayerLists s_layers;
   __shared__ int s_flags[3];
   __shared__ int s_act[5];
   __shared__ int s_tile;
   LatCtl *ctl = p.ctl;
   const unsigned long long t_start = dev_globaltimer();
-  if (threadIdx.x == 0) {
-    int nh = 0, nv = 0;
-    for (int z = p.bz0; z <= p.bz1; ++z) {
-      if (p.axis[z] == 1) s_hl[nh++] = z - p.bz0;
-      else if (p.axis[z] == 2) s_vl[nv++] = z - p.bz0;
-    }
-    s_nh = nh;
-    s_nv = nv;
-  }
+  if (threadIdx.x == 0) s_layers.box = -1;
   __syncthreads();
-  const int nh = s_nh, nv = s_nv;
   unsigned visits = 0;
   unsigned long long sched_ns = 0;
   for (;;) {
@@ -532,21 +586,23 @@ __global__ void __launch_bounds__(TX * TY) lattice_async_kernel(LatParams p) {
     const int t = s_tile;
     __syncthreads();
     if (t < 0) break;
-    process_tile<TX, TY>(p, t, sd, s_hl, nh, s_vl, nv, s_flags, s_act);
+    process_tile<TX, TY>(p, t, sd, s_layers, s_flags, s_act);
     // neighbours are activated by threads 0..3 in parallel, after this
     // tile's distances are visible
     unsigned long long ta = 0;
     if (threadIdx.x == 0) ta = dev_globaltimer();
     if (threadIdx.x < 4) {
       __threadfence();
-      const int tx = t % p.ntx, ty = t / p.ntx;
+      const LatBox B = load_box(p, box_of_tile(p, t));
+      const int lt = t - B.tile0;
+      const int tx = lt % B.ntx, ty = lt / B.ntx;
       const int d = threadIdx.x;
       int nb = -1;
       if (s_act[d]) {
         if (d == 0 && tx > 0) nb = t - 1;
-        if (d == 1 && tx < p.ntx - 1) nb = t + 1;
-        if (d == 2 && ty > 0) nb = t - p.ntx;
-        if (d == 3 && ty < p.nty - 1) nb = t + p.ntx;
+        if (d == 1 && tx < B.ntx - 1) nb = t + 1;
+        if (d == 2 && ty > 0) nb = t - B.ntx;
+        if (d == 3 && ty < B.nty - 1) nb = t + B.ntx;
       }
       if (nb >= 0 && !activate_tile(p, nb)) atomicCAS(&ctl->err, DEV_OK, DEV_ERR_INTERNAL);
     }
@@ -576,17 +632,22 @@ unsigned long long env_u64(const char *name, unsigned long long dflt) {
   return strtoull(s, nullptr, 10);
 }
 
-template <int TX, int TY>
-int launch_lattice(orsp::Graph *g, LatParams &p, int32_t nseeds, const int32_t *seeds,
-                   const float *seed_cost, cudaStream_t st) {
-  p.ntx = (p.bx1 - p.bx0 + TX) / TX;
-  p.nty = (p.by1 - p.by0 + TY) / TY;
-  const int64_t ntiles = (int64_t)p.ntx * p.nty;
-  const bool async = env_u64("ORSP_LAT_ASYNC", 1) != 0;
-  const size_t list_b = (((size_t)ntiles * 4) + 255) & ~(size_t)255;
-  const unsigned qcap = (unsigned)(ntiles + 4 * g->num_sms * 4 + 64);
-  const size_t q_b = (((size_t)qcap * 4) + 255) & ~(size_t)255;
-  const size_t need = 4 * list_b + q_b + 256;
+// Workspace layout for ntiles tiles: 4 tile arrays (lists, stamps, states),
+// the ring queue, then the control block.
+struct WsLayout {
+  size_t list_b, q_b, total;
+  unsigned qcap;
+};
+WsLayout ws_layout(const orsp::Graph *g, int64_t ntiles) {
+  WsLayout w;
+  w.list_b = (((size_t)ntiles * 4) + 255) & ~(size_t)255;
+  w.qcap = (unsigned)(ntiles + 4 * g->num_sms * 4 + 64);
+  w.q_b = (((size_t)w.qcap * 4) + 255) & ~(size_t)255;
+  w.total = 4 * w.list_b + w.q_b + 256;
+  return w;
+}
+
+int grow_ws(orsp::Graph *g, size_t need) {
   if (g->lat_ws_bytes < need) {
     cudaFree(g->lat_ws);
     g->lat_ws = nullptr;
@@ -595,6 +656,18 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int32_t nseeds, const int32_t *
     g->lat_ws_bytes = need;
   }
   if (!g->lat_ctl_h) ORSP_CUDA(cudaMallocHost(&g->lat_ctl_h, sizeof(LatCtl)));
+  return ORSP_OK;
+}
+
+template <int TX, int TY>
+int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_t nseeds, const int32_t *seeds,
+                   const float *seed_cost, cudaStream_t st, orsp::LatOptions *opt) {
+  const bool async = env_u64("ORSP_LAT_ASYNC", 1) != 0;
+  const WsLayout L = ws_layout(g, ntiles);
+  const size_t list_b = L.list_b, q_b = L.q_b;
+  const unsigned qcap = L.qcap;
+  int rc0 = grow_ws(g, L.total);
+  if (rc0) return rc0;
   char *b = (char *)g->lat_ws;
   p.list0 = (int32_t *)b;
   p.list1 = (int32_t *)(b + list_b);
@@ -603,12 +676,12 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int32_t nseeds, const int32_t *
   p.qslot = async ? (int32_t *)(b + 4 * list_b) : nullptr;
   p.qcap = qcap;
   p.ctl = (LatCtl *)(b + 4 * list_b + q_b);
-  ORSP_CUDA(cudaMemsetAsync(p.stamp, 0, (size_t)ntiles * 4, st));
+  if (opt) opt->err_d = &p.ctl->err;
+  if (!async) ORSP_CUDA(cudaMemsetAsync(p.stamp, 0, (size_t)ntiles * 4, st));
   ORSP_CUDA(cudaMemsetAsync(p.tstate, 0, (size_t)ntiles * 4, st));
   if (async) ORSP_CUDA(cudaMemsetAsync(p.qslot, 0xff, (size_t)qcap * 4, st));
   lattice_seed_kernel<TX, TY><<<1, 256, 0, st>>>(p, nseeds, seeds, seed_cost);
   ORSP_CUDA(cudaGetLastError());
-  const int nzb = p.bz1 - p.bz0 + 1;
   const size_t smem = ((size_t)nzb * (TY + 2) * (TX + 3) + (size_t)5 * nzb * TY * (TX + 1)) * sizeof(float);
   if (smem > 227 * 1024) {
     orsp::set_error("lattice search: too many layers for the shared-memory tile");
@@ -636,7 +709,8 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int32_t nseeds, const int32_t *
     ORSP_CUDA(cudaEventRecord(orsp::g_timer.b, st));
     orsp::g_timer.pending = true;
   }
-  ORSP_CUDA(cudaMemcpyAsync(g->lat_ctl_h, p.ctl, sizeof(LatCtl), cudaMemcpyDeviceToHost, st));
+  if (!opt || opt->copy_ctl)
+    ORSP_CUDA(cudaMemcpyAsync(g->lat_ctl_h, p.ctl, sizeof(LatCtl), cudaMemcpyDeviceToHost, st));
   return ORSP_OK;
 }
 
@@ -692,53 +766,110 @@ void free_lattice(Graph *g) {
   cudaFree(g->slot_eid);
   cudaFree(g->wslot);
   cudaFree(g->lat_ws);
+  cudaFree(g->lat_box_d);
   if (g->lat_ctl_h) cudaFreeHost(g->lat_ctl_h);
+  g->lat_box_d = nullptr;
   g->slot_eid = nullptr;
   g->wslot = nullptr;
   g->lat_ws = nullptr;
   g->lat_ctl_h = nullptr;
 }
 
-// Search over the box [x0,x1]x[y0,y1]x[z0,z1] (box == nullptr: the whole
-// lattice).  Every distance is reset to +inf, so nodes outside the box stay
-// unreachable for the backtrace; only the box's weights are gathered and only
-// its tiles are visited.  Leaves the distances in `dist`;
-// finish_lattice_search reports the status after the stream sync.
-int run_lattice_search(Graph *g, const float *cost_d, int32_t nseeds, const int32_t *seeds_d,
-                       const float *seed_cost_d, const int32_t *box, uint32_t *dist, cudaStream_t st) {
+int lattice_tile_w() { return env_u64("ORSP_LAT_TILE", 16) == 32 ? 32 : 16; }
+
+int reserve_lattice_ws(Graph *g, int64_t ntiles) { return grow_ws(g, ws_layout(g, ntiles).total); }
+
+int64_t make_lat_boxes(const int32_t *boxes_h, int32_t nbox, LatBox *out) {
+  const int TX = lattice_tile_w(), TY = 16;
+  int64_t t0 = 0;
+  for (int32_t i = 0; i < nbox; ++i) {
+    const int32_t *b = boxes_h + 6 * (int64_t)i;
+    LatBox &B = out[i];
+    B.x0 = b[0];
+    B.x1 = b[1];
+    B.y0 = b[2];
+    B.y1 = b[3];
+    B.z0 = b[4];
+    B.z1 = b[5];
+    B.ntx = (b[1] - b[0] + TX) / TX;
+    B.nty = (b[3] - b[2] + TY) / TY;
+    B.tile0 = (int32_t)t0;
+    t0 += (int64_t)B.ntx * B.nty;
+  }
+  return t0;
+}
+
+// Searches pairwise disjoint boxes in one launch.  Distances are reset to
+// +inf everywhere (or, with opt->fill_box_only, inside the boxes only - the
+// caller's backtrace must then test box membership); only the boxes' weights
+// are gathered and only their tiles are visited.  Leaves the distances in
+// `dist`; finish_lattice_search reports the status after the stream sync.
+int run_lattice_boxes(Graph *g, const float *cost_d, int32_t nseeds, const int32_t *seeds_d,
+                      const float *seed_cost_d, int32_t nbox, const int32_t *boxes_h, const LatBox *lboxes_d,
+                      uint32_t *dist, cudaStream_t st, LatOptions *opt) {
   const int64_t N = g->N;
-  const int32_t full[6] = {0, g->nx - 1, 0, g->ny - 1, 0, g->nz - 1};
-  const int32_t *b = box ? box : full;
-  const bool whole = b[0] == 0 && b[1] == g->nx - 1 && b[2] == 0 && b[3] == g->ny - 1 && b[4] == 0 &&
-                     b[5] == g->nz - 1;
+  const int TX = lattice_tile_w(), TY = 16;
+  int64_t ntiles = 0;
+  int nzb = 1;
+  bool whole = false;
+  for (int32_t i = 0; i < nbox; ++i) {
+    const int32_t *b = boxes_h + 6 * (int64_t)i;
+    ntiles += (int64_t)((b[1] - b[0] + TX) / TX) * ((b[3] - b[2] + TY) / TY);
+    nzb = std::max(nzb, b[5] - b[4] + 1);
+    whole = whole || (b[0] == 0 && b[1] == g->nx - 1 && b[2] == 0 && b[3] == g->ny - 1 && b[4] == 0 &&
+                      b[5] == g->nz - 1);
+  }
   if (whole) {
     gather_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 148 * 32), 256, 0, st>>>(
         g->slot_eid, cost_d, (float4 *)g->wslot, N);
+    ORSP_CUDA(cudaGetLastError());
   } else {
-    const int32_t bw = b[1] - b[0] + 1, bh = b[3] - b[2] + 1;
-    const int64_t count = (int64_t)bw * bh * (b[5] - b[4] + 1);
-    gather_box_kernel<<<(int)std::min<int64_t>((count + 255) / 256, 148 * 32), 256, 0, st>>>(
-        g->slot_eid, cost_d, (float4 *)g->wslot, N, g->nx, g->ny, b[0], bw, b[2], bh, b[4], count);
+    for (int32_t i = 0; i < nbox; ++i) {
+      const int32_t *b = boxes_h + 6 * (int64_t)i;
+      const int32_t bw = b[1] - b[0] + 1, bh = b[3] - b[2] + 1;
+      const int64_t count = (int64_t)bw * bh * (b[5] - b[4] + 1);
+      gather_box_kernel<<<(int)std::min<int64_t>((count + 255) / 256, 148 * 32), 256, 0, st>>>(
+          g->slot_eid, cost_d, (float4 *)g->wslot, N, g->nx, g->ny, b[0], bw, b[2], bh, b[4], count);
+      ORSP_CUDA(cudaGetLastError());
+    }
   }
-  ORSP_CUDA(cudaGetLastError());
-  fill_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 148 * 32), 256, 0, st>>>(dist, N, ORSP_INF_BITS);
-  ORSP_CUDA(cudaGetLastError());
+  if (opt && opt->fill_box_only && !whole) {
+    for (int32_t i = 0; i < nbox; ++i) {
+      const int32_t *b = boxes_h + 6 * (int64_t)i;
+      const int32_t bw = b[1] - b[0] + 1, bh = b[3] - b[2] + 1;
+      const int64_t count = (int64_t)bw * bh * (b[5] - b[4] + 1);
+      fill_box_kernel<<<(int)std::min<int64_t>((count + 255) / 256, 148 * 32), 256, 0, st>>>(
+          dist, g->nx, g->ny, b[0], bw, b[2], bh, b[4], count, ORSP_INF_BITS);
+      ORSP_CUDA(cudaGetLastError());
+    }
+  } else {
+    fill_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 148 * 32), 256, 0, st>>>(dist, N, ORSP_INF_BITS);
+    ORSP_CUDA(cudaGetLastError());
+  }
   LatParams p{};
   p.nx = g->nx;
   p.ny = g->ny;
   p.nz = g->nz;
-  p.bx0 = b[0];
-  p.bx1 = b[1];
-  p.by0 = b[2];
-  p.by1 = b[3];
-  p.bz0 = b[4];
-  p.bz1 = b[5];
+  p.nbox = nbox;
+  p.boxes = lboxes_d;
   p.w4 = (const float4 *)g->wslot;
   p.dist = dist;
   for (int z = 0; z < 64; ++z) p.axis[z] = z < g->nz ? g->layer_axis[z] : 0;
-  const int tile = (int)env_u64("ORSP_LAT_TILE", 16);
-  if (tile == 32) return launch_lattice<32, 16>(g, p, nseeds, seeds_d, seed_cost_d, st);
-  return launch_lattice<16, 16>(g, p, nseeds, seeds_d, seed_cost_d, st);
+  if (TX == 32) return launch_lattice<32, 16>(g, p, ntiles, nzb, nseeds, seeds_d, seed_cost_d, st, opt);
+  return launch_lattice<16, 16>(g, p, ntiles, nzb, nseeds, seeds_d, seed_cost_d, st, opt);
+}
+
+int run_lattice_search(Graph *g, const float *cost_d, int32_t nseeds, const int32_t *seeds_d,
+                       const float *seed_cost_d, const int32_t *box, uint32_t *dist, cudaStream_t st,
+                       LatOptions *opt) {
+  const int32_t full[6] = {0, g->nx - 1, 0, g->ny - 1, 0, g->nz - 1};
+  const int32_t *b = box ? box : full;
+  if (!g->lat_box_d) ORSP_CUDA(cudaMalloc(&g->lat_box_d, sizeof(LatBox)));
+  LatBox *hb = (LatBox *)((char *)g->pinned + 1024);
+  make_lat_boxes(b, 1, hb);
+  ORSP_CUDA(cudaMemcpyAsync(g->lat_box_d, hb, sizeof(LatBox), cudaMemcpyHostToDevice, st));
+  return run_lattice_boxes(g, cost_d, nseeds, seeds_d, seed_cost_d, 1, b, (const LatBox *)g->lat_box_d, dist, st,
+                           opt);
 }
 
 int finish_lattice_search(Graph *g, int32_t *rounds_h) {

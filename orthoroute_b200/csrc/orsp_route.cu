@@ -1,0 +1,336 @@
+// Per-net routing loop on the device: the body of _route_all
+// (orthoroute/algorithms/manhattan/unified_pathfinder.py:4475-4800, "UPF")
+// with per-net live costs, for box ROIs on the H/V lattice.  The nets are
+// taken in the given order, in groups whose boxes are pairwise disjoint (one
+// net per group is the plain loop).  For each group, four steps are enqueued
+// on one stream with no host synchronisation:
+//   1. rip up the nets' previous paths: usage -1 on their edges (clear_path,
+//      UPF:829) and the live cost of those edges recomputed;
+//   2. one tile-sweep launch over the group's boxes (orsp_lattice.cu),
+//      distances reset inside the boxes only;
+//   3. one warp per net: backtrace inside its box (the parent rule of
+//      orsp_sssp, rank = node id = box-local order), path -> edges (first CSR
+//      edge u->v, UPF:5463), path and length written into the net's row;
+//   4. commit: usage +1 on the new edges (commit_path, UPF:821) and their live
+//      costs recomputed.
+// Each step reads what the previous one wrote, in stream order.  A net's
+// search reads only costs of edges inside its box, and its rip-up and commit
+// touch only edges inside its box, so nets with disjoint boxes do not see
+// each other: the result equals routing the same order one net at a time,
+// which equals the host loop over orsp_commit_edges / orsp_update_costs_live
+// / orsp_sssp_box / orsp_path_to_edges, bit for bit.  Device-side errors
+// (search timeout, path overflow) are folded into one error word that the
+// host reads after the last group.
+#include <algorithm>
+#include <climits>
+#include <vector>
+
+#include "accounting.cuh"
+
+namespace {
+
+using orsp::apply_usage;
+using orsp::LatBox;
+using orsp::live_cost;
+
+struct LiveParams {
+  int32_t *usage;
+  float *present;
+  const float *base, *capa, *hist;
+  float pres_fac, hist_w, via_mult, base_w;
+  int jitter;
+  float *cost;
+};
+
+// Steps 1 and 4 for the nets of one group: block j takes net order[j], the
+// len-1 edges of its row, usage +-1 and live costs.  The edges of a shortest
+// path are distinct and the group's boxes are disjoint, so each edge is
+// handled by one thread.
+__global__ void route_commit_kernel(const int32_t *order, const int32_t *edges, const int32_t *lens, int32_t cap,
+                                    int32_t sign, LiveParams lp) {
+  const int32_t k = order[blockIdx.x];
+  const int32_t len = lens[k];
+  if (len < 2) return;
+  const int32_t ne = min(len - 1, cap);
+  const int32_t *row = edges + (int64_t)k * cap;
+  for (int32_t i = threadIdx.x; i < ne; i += blockDim.x) {
+    const int32_t e = row[i];
+    if (e < 0) continue;
+    apply_usage(lp.usage, lp.present, e, sign);
+    lp.cost[e] = live_cost(e, lp.base, lp.usage, lp.capa, lp.hist, lp.pres_fac, lp.hist_w, lp.via_mult,
+                           lp.base_w, lp.jitter);
+  }
+}
+
+struct RouteBt {
+  const float *cost;
+  const int32_t *indptr, *indices;
+  const int32_t *rptr, *rsrc, *reid;
+  const uint32_t *dist;
+  int32_t nx, ny;
+  // the group's nets: net ids, sources (-1: source outside its box), targets, boxes
+  const int32_t *order, *src, *dst;
+  const LatBox *boxes;
+  int32_t *net_nodes, *net_edges, *net_lens;
+  int32_t cap;
+  const int *search_err;  // the group search's error word
+  int *route_err;
+};
+
+__device__ __forceinline__ bool in_box(const RouteBt &p, const LatBox &B, int32_t u) {
+  const int32_t plane = p.nx * p.ny;
+  const int32_t z = u / plane, r = u - z * plane, y = r / p.nx, x = r - y * p.nx;
+  return x >= B.x0 && x <= B.x1 && y >= B.y0 && y <= B.y1 && z >= B.z0 && z <= B.z1;
+}
+
+// Step 3, one warp per net of the group (block j: net order[j]).  Parent of
+// v: the in-neighbour u inside the net's box with fl32(d[u] + w(u,v)) == d[v]
+// and the smallest (d[u], u) below (d[v], v); the source (distance 0) ends
+// the walk.  Nodes outside the box hold distances of other boxes or of
+// earlier searches, hence the box test.
+__global__ void route_backtrace_kernel(RouteBt p) {
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x;
+  const int32_t k = p.order[j];
+  const int32_t src = p.src[j], dst = p.dst[j];
+  const LatBox B = p.boxes[j];
+  int32_t *nodes = p.net_nodes + (int64_t)k * p.cap;
+  int32_t *edges = p.net_edges + (int64_t)k * p.cap;
+  int32_t *len_out = p.net_lens + k;
+  const int serr = *p.search_err;
+  if (serr) {
+    if (lane == 0) {
+      atomicCAS(p.route_err, DEV_OK, serr);
+      *len_out = 0;
+    }
+    return;
+  }
+  unsigned dv = (src >= 0 && in_box(p, B, dst)) ? p.dist[dst] : ORSP_INF_BITS;
+  if (dv == ORSP_INF_BITS || dst == src) {
+    if (lane == 0) *len_out = 0;
+    return;
+  }
+  int v = dst;
+  int len = 0;
+  int err = 0;
+  for (;;) {
+    if (len >= p.cap) { err = DEV_ERR_PATH_OVERFLOW; break; }
+    if (lane == 0) nodes[len] = v;
+    ++len;
+    if (v == src && dv == 0u) break;
+    const int b = p.rptr[v], e = p.rptr[v + 1];
+    unsigned long long best = ULLONG_MAX;
+    int bu = -1;
+    for (int k0 = b; k0 < e; k0 += 32) {
+      const int kk = k0 + lane;
+      if (kk < e) {
+        const int u = p.rsrc[kk];
+        if (in_box(p, B, u)) {
+          const unsigned du = p.dist[u];
+          if (du != ORSP_INF_BITS) {
+            const float s = __fadd_rn(bits_f(du), p.cost[p.reid[kk]]);
+            if (f_bits(s) == dv && (du < dv || (du == dv && u < v))) {
+              const unsigned long long key = ((unsigned long long)du << 32) | (unsigned)u;
+              if (key < best) { best = key; bu = u; }
+            }
+          }
+        }
+      }
+    }
+    const unsigned long long wbest = warp_min_u64(best);
+    if (wbest == ULLONG_MAX) { err = DEV_ERR_INTERNAL; break; }
+    const unsigned owner = __ballot_sync(ORSP_FULL_MASK, best == wbest && bu >= 0);
+    v = __shfl_sync(ORSP_FULL_MASK, bu, __ffs(owner) - 1);
+    dv = (unsigned)(wbest >> 32);
+  }
+  __syncwarp();
+  if (err) {
+    if (lane == 0) {
+      atomicCAS(p.route_err, DEV_OK, err);
+      *len_out = 0;
+    }
+    return;
+  }
+  for (int i = lane; i < len / 2; i += 32) {
+    const int a = nodes[i], z = nodes[len - 1 - i];
+    nodes[i] = z;
+    nodes[len - 1 - i] = a;
+  }
+  __syncwarp();
+  for (int i = lane; i < len - 1; i += 32) {
+    const int u = nodes[i], w = nodes[i + 1];
+    int eid = -1;
+    for (int e = p.indptr[u]; e < p.indptr[u + 1]; ++e)
+      if (p.indices[e] == w) { eid = e; break; }
+    edges[i] = eid;
+  }
+  __syncwarp();
+  if (lane == 0) *len_out = len;
+}
+
+bool box_ok(const orsp::Graph *g, const int32_t *b) {
+  return b[0] >= 0 && b[2] >= 0 && b[4] >= 0 && b[1] < g->nx && b[3] < g->ny && b[5] < g->nz && b[0] <= b[1] &&
+         b[2] <= b[3] && b[4] <= b[5];
+}
+
+bool boxes_meet(const int32_t *a, const int32_t *b) {
+  return a[0] <= b[1] && b[0] <= a[1] && a[2] <= b[3] && b[2] <= a[3] && a[4] <= b[5] && b[4] <= a[5];
+}
+
+bool node_in(const orsp::Graph *g, int32_t u, const int32_t *b) {
+  const int64_t plane = (int64_t)g->nx * g->ny;
+  const int32_t z = (int32_t)(u / plane), r = (int32_t)(u - z * plane), y = r / g->nx, x = r - y * g->nx;
+  return x >= b[0] && x <= b[1] && y >= b[2] && y <= b[3] && z >= b[4] && z <= b[5];
+}
+
+constexpr int32_t kMaxGroup = 1024;
+
+}  // namespace
+
+using namespace orsp;
+
+extern "C" int orsp_route_nets(orsp_graph *g, int32_t M, const int32_t *src_h, const int32_t *dst_h,
+                               const int32_t *box_h, int32_t K, const int32_t *order_h, int32_t G,
+                               const int32_t *group_ptr_h, int32_t *net_nodes_d, int32_t *net_edges_d,
+                               int32_t path_cap, int32_t *net_lens_d, float *cost_d, const float *base_d,
+                               int32_t *usage_d, float *present_d, const float *cap_d, const float *hist_d,
+                               float pres_fac, float hist_w, float via_mult, float base_w, int32_t jitter,
+                               uintptr_t stream) {
+  if (!g || M < 0 || K < 0 || path_cap < 2) { set_error("route_nets: bad sizes"); return ORSP_ERR_ARG; }
+  if (K == 0) return ORSP_OK;
+  if (!src_h || !dst_h || !box_h || !order_h || !net_nodes_d || !net_edges_d || !net_lens_d || !cost_d ||
+      !base_d || !usage_d || !cap_d || !hist_d) {
+    set_error("route_nets: NULL array");
+    return ORSP_ERR_ARG;
+  }
+  if (!g->lattice_ok) { set_error("route_nets: needs a graph recognised as an H/V lattice"); return ORSP_ERR_ARG; }
+  // groups: [group_ptr[q], group_ptr[q+1]) of the order; NULL = one net each
+  std::vector<int32_t> gp;
+  if (group_ptr_h) {
+    if (G < 1 || group_ptr_h[0] != 0 || group_ptr_h[G] != K) {
+      set_error("route_nets: group_ptr must run from 0 to K");
+      return ORSP_ERR_ARG;
+    }
+    gp.assign(group_ptr_h, group_ptr_h + G + 1);
+  } else {
+    gp.resize((size_t)K + 1);
+    for (int32_t i = 0; i <= K; ++i) gp[i] = i;
+  }
+  const int32_t ngroups = (int32_t)gp.size() - 1;
+  std::vector<int32_t> seen((size_t)M, 0);
+  for (int32_t i = 0; i < K; ++i) {
+    const int32_t k = order_h[i];
+    if (k < 0 || k >= M) { set_error("route_nets: order entry out of range"); return ORSP_ERR_ARG; }
+    if (seen[k]++) { set_error("route_nets: a net appears twice in the order"); return ORSP_ERR_ARG; }
+    if (src_h[k] < 0 || src_h[k] >= g->N || dst_h[k] < 0 || dst_h[k] >= g->N) {
+      set_error("route_nets: src/dst out of range");
+      return ORSP_ERR_ARG;
+    }
+    if (!box_ok(g, box_h + 6 * (int64_t)k)) {
+      set_error("route_nets: box outside the lattice or empty");
+      return ORSP_ERR_ARG;
+    }
+  }
+  for (int32_t q = 0; q < ngroups; ++q) {
+    const int32_t a = gp[q], b = gp[q + 1];
+    if (b < a || b - a > kMaxGroup) { set_error("route_nets: group sizes must be 0..1024"); return ORSP_ERR_ARG; }
+    for (int32_t i = a; i < b; ++i)
+      for (int32_t j = a; j < i; ++j)
+        if (boxes_meet(box_h + 6 * (int64_t)order_h[i], box_h + 6 * (int64_t)order_h[j])) {
+          set_error("route_nets: boxes of one group must be pairwise disjoint");
+          return ORSP_ERR_ARG;
+        }
+  }
+  ORSP_CUDA(cudaSetDevice(g->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!g->dist) ORSP_CUDA(cudaMalloc(&g->dist, (size_t)g->N * 4));
+  if (!g->route_ws) ORSP_CUDA(cudaMalloc(&g->route_ws, 256));
+  // per-call tables in route order: net id, source (-1 when outside its box),
+  // target, box (LatBox; tile ids restart at 0 in each group).  Staged in
+  // pinned memory and copied once; the call synchronises before returning,
+  // so the staging buffer is free again for the next call.
+  const size_t need = (size_t)K * (3 * sizeof(int32_t) + sizeof(LatBox)) + 256;
+  if (g->route_tab_bytes < need) {
+    cudaFree(g->route_tab_d);
+    if (g->route_tab_h) cudaFreeHost(g->route_tab_h);
+    g->route_tab_d = nullptr;
+    g->route_tab_h = nullptr;
+    g->route_tab_bytes = 0;
+    ORSP_CUDA(cudaMalloc(&g->route_tab_d, need));
+    ORSP_CUDA(cudaMallocHost(&g->route_tab_h, need));
+    g->route_tab_bytes = need;
+  }
+  char *th = (char *)g->route_tab_h;
+  int32_t *t_order = (int32_t *)th;
+  int32_t *t_src = t_order + K;
+  int32_t *t_dst = t_src + K;
+  LatBox *t_box = (LatBox *)(((uintptr_t)(t_dst + K) + 63) & ~(uintptr_t)63);
+  std::vector<int32_t> boxes_o((size_t)K * 6);
+  for (int32_t i = 0; i < K; ++i) {
+    const int32_t k = order_h[i];
+    const int32_t *b = box_h + 6 * (int64_t)k;
+    t_order[i] = k;
+    t_src[i] = node_in(g, src_h[k], b) ? src_h[k] : -1;
+    t_dst[i] = dst_h[k];
+    for (int c = 0; c < 6; ++c) boxes_o[(size_t)i * 6 + c] = b[c];
+  }
+  int64_t max_tiles = 1;
+  for (int32_t q = 0; q < ngroups; ++q) {
+    const int32_t a = gp[q], b = gp[q + 1];
+    max_tiles = std::max<int64_t>(max_tiles, make_lat_boxes(boxes_o.data() + (size_t)a * 6, b - a, t_box + a));
+  }
+  const size_t off_box = (size_t)((char *)t_box - th);
+  char *td = (char *)g->route_tab_d;
+  const int32_t *d_order = (const int32_t *)td;
+  const int32_t *d_src = d_order + K;
+  const int32_t *d_dst = d_src + K;
+  const LatBox *d_box = (const LatBox *)(td + off_box);
+  ORSP_CUDA(cudaMemcpyAsync(td, th, off_box + (size_t)K * sizeof(LatBox), cudaMemcpyHostToDevice, st));
+  int rc = reserve_lattice_ws(g, max_tiles);
+  if (rc) return rc;
+  int *route_err = (int *)g->route_ws;
+  ORSP_CUDA(cudaMemsetAsync(route_err, 0, sizeof(int), st));
+
+  LiveParams lp{usage_d, present_d, base_d, cap_d, hist_d, pres_fac, hist_w, via_mult, base_w, jitter, cost_d};
+  for (int32_t q = 0; q < ngroups; ++q) {
+    const int32_t a = gp[q], n = gp[q + 1] - gp[q];
+    if (n == 0) continue;
+    route_commit_kernel<<<n, 256, 0, st>>>(d_order + a, net_edges_d, net_lens_d, path_cap, -1, lp);
+    ORSP_CUDA(cudaGetLastError());
+    LatOptions opt;
+    opt.fill_box_only = true;
+    opt.copy_ctl = false;
+    rc = run_lattice_boxes(g, cost_d, n, d_src + a, nullptr, n, boxes_o.data() + (size_t)a * 6, d_box + a, g->dist,
+                           st, &opt);
+    if (rc) return rc;
+    RouteBt bt{};
+    bt.cost = cost_d;
+    bt.indptr = g->indptr;
+    bt.indices = g->indices;
+    bt.rptr = g->rptr;
+    bt.rsrc = g->rsrc;
+    bt.reid = g->reid;
+    bt.dist = g->dist;
+    bt.nx = g->nx;
+    bt.ny = g->ny;
+    bt.order = d_order + a;
+    bt.src = d_src + a;
+    bt.dst = d_dst + a;
+    bt.boxes = d_box + a;
+    bt.net_nodes = net_nodes_d;
+    bt.net_edges = net_edges_d;
+    bt.net_lens = net_lens_d;
+    bt.cap = path_cap;
+    bt.search_err = opt.err_d;
+    bt.route_err = route_err;
+    route_backtrace_kernel<<<n, 32, 0, st>>>(bt);
+    ORSP_CUDA(cudaGetLastError());
+    route_commit_kernel<<<n, 256, 0, st>>>(d_order + a, net_edges_d, net_lens_d, path_cap, 1, lp);
+    ORSP_CUDA(cudaGetLastError());
+  }
+  int *err_h = (int *)g->pinned + 32;
+  ORSP_CUDA(cudaMemcpyAsync(err_h, route_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  ORSP_CUDA(cudaStreamSynchronize(st));
+  if (*err_h) return dev_status_to_orsp(*err_h);
+  return ORSP_OK;
+}

@@ -88,6 +88,10 @@ class NegotiationConfig:
     delta: Optional[float] = None
     path_cap: int = 4096
     cost_update: str = "iteration"  # "iteration" (reference) | "net" (live usage)
+    native_loop: bool = True  # per-net policy on a lattice: orsp_route_nets (no host round trip per net)
+    net_order: str = "index"  # "index" | "disjoint": first-fit rounds of pairwise disjoint boxes
+    stall_grow: int = 0  # cells added to the margin of a net that offends stall_iterations times running
+    stall_iterations: int = 2
 
 
 @dataclass
@@ -132,6 +136,51 @@ def level_schedule(boxes: np.ndarray) -> np.ndarray:
         if inter.any():
             lv[j] = int(lv[:j][inter].max()) + 1
     return lv
+
+
+GROUP_MAX = 1024  # nets per device launch (orsp_route_nets group limit)
+
+
+def level_groups(idx: np.ndarray, lv: np.ndarray, group_max: int = GROUP_MAX):
+    """Order and group_ptr for orsp_route_nets: the nets of each level in their
+    original order, level after level, each level cut into chunks of at most
+    group_max nets.  Every net still follows each earlier net whose box meets
+    its own, so the result equals routing `idx` one net at a time."""
+    order = []
+    ptr_ = [0]
+    for L in range(int(lv.max()) + 1 if len(lv) else 0):
+        sel = idx[lv == L]
+        for a in range(0, len(sel), group_max):
+            chunk = sel[a:a + group_max]
+            order.append(chunk)
+            ptr_.append(ptr_[-1] + len(chunk))
+    order = np.concatenate(order).astype(np.int32) if order else np.zeros(0, np.int32)
+    return order, np.asarray(ptr_, dtype=np.int32)
+
+
+def disjoint_order(boxes: np.ndarray, idx: np.ndarray) -> np.ndarray:
+    """Nets of idx reordered into first-fit rounds: each net joins the first
+    round whose boxes it does not meet; rounds are concatenated.  Under this
+    order the level schedule of the nets is exactly the rounds, so one launch
+    per round gives the one-net-at-a-time result of the same order."""
+    idx = np.asarray(idx)
+    if idx.size == 0:
+        return idx
+    b = boxes[idx]
+    rnd = np.full(idx.size, -1, dtype=np.int64)
+    nrounds = 0
+    for j in range(idx.size):
+        r = 0
+        if j:
+            p = b[:j]
+            meet = ((p[:, 0] <= b[j, 1]) & (b[j, 0] <= p[:, 1]) & (p[:, 2] <= b[j, 3]) & (b[j, 2] <= p[:, 3])
+                    & (p[:, 4] <= b[j, 5]) & (b[j, 4] <= p[:, 5]))
+            taken = np.zeros(nrounds + 1, dtype=bool)
+            taken[rnd[:j][meet]] = True
+            r = int(np.argmin(taken))
+        rnd[j] = r
+        nrounds = max(nrounds, r + 1)
+    return idx[np.argsort(rnd, kind="stable")]
 
 
 class PathFinder:
@@ -240,7 +289,32 @@ class PathFinder:
                                                        1 if cfg.add_jitter else 0, ptr(acc.total_cost), _stream()),
               "orsp_update_costs_live_paths")
 
+    def _route_nets_device(self, acc, pres_fac, order, groups, src, dst, boxes, net_nodes, net_edges, net_lens):
+        """orsp_route_nets over `order` (host int32), cut into `groups` (host
+        int32 group_ptr, or None for one net per group)."""
+        cfg = self.cfg
+        order = np.ascontiguousarray(order, dtype=np.int32)
+        boxes_c = np.ascontiguousarray(boxes, dtype=np.int32)
+        gp = None if groups is None else np.ascontiguousarray(groups, dtype=np.int32)
+        check(_lib.load().orsp_route_nets(
+            self.dg.handle, int(len(src)), ptr(src), ptr(dst), ptr(boxes_c), int(order.size), ptr(order),
+            0 if gp is None else int(gp.size - 1), ptr(gp), ptr(net_nodes), ptr(net_edges), int(net_nodes.shape[1]),
+            ptr(net_lens), ptr(acc.total_cost), ptr(self.base), ptr(acc.usage), ptr(acc.present), ptr(acc.capacity),
+            ptr(acc.history), float(pres_fac), float(cfg.hist_cost_weight), float(cfg.via_cost_multiplier),
+            float(cfg.base_cost_weight), 1 if cfg.add_jitter else 0, _stream()), "orsp_route_nets")
+
     def _route_net_sequential(self, acc, pres_fac, idx, src, dst, boxes, net_nodes, net_edges, net_lens, delta):
+        if self.cfg.native_loop and self.dg.is_lattice:
+            self._route_nets_device(acc, pres_fac, idx.cpu().numpy(), None, src, dst, boxes, net_nodes, net_edges,
+                                    net_lens)
+        else:
+            self._route_net_sequential_host(acc, pres_fac, idx, src, dst, boxes, net_nodes, net_edges, net_lens,
+                                            delta)
+
+    def _route_net_sequential_host(self, acc, pres_fac, idx, src, dst, boxes, net_nodes, net_edges, net_lens,
+                                   delta):
+        """The same loop driven from the host, one net at a time (the plain
+        form the device loop is checked against)."""
         lib = _lib.load()
         cap = self.cfg.path_cap
         st = _stream()
@@ -253,8 +327,13 @@ class PathFinder:
                 check(lib.orsp_commit_edges(L - 1, ptr(old), ptr(acc.usage), ptr(acc.present), -1, st),
                       "orsp_commit_edges")
                 self._live(acc, pres_fac, old, L - 1)
-            g2r = self.roi.box_map(boxes[k])
-            status, path, _ = self.dg.sssp(cost, int(src[k]), int(dst[k]), roi_map=g2r, delta=delta, path_cap=cap)
+            if self.dg.is_lattice:
+                status, path, _ = self.dg.sssp_box(cost, int(src[k]), int(dst[k]), boxes[k], delta=delta,
+                                                   path_cap=cap)
+            else:
+                g2r = self.roi.box_map(boxes[k])
+                status, path, _ = self.dg.sssp(cost, int(src[k]), int(dst[k]), roi_map=g2r, delta=delta,
+                                               path_cap=cap)
             if status == _lib.ORSP_OK and path is not None and path.numel() >= 2:
                 n = int(path.numel())
                 e = self.dg.path_to_edges(path)
@@ -270,7 +349,12 @@ class PathFinder:
                 lens_h[k] = 0
 
     def _route_net_batched(self, acc, pres_fac, idx, src_d, dst_d, boxes_d, boxes, order_levels, net_nodes,
-                           net_edges, net_lens, delta):
+                           net_edges, net_lens, delta, src=None, dst=None):
+        if self.cfg.native_loop and self.dg.is_lattice and src is not None:
+            idx_h = idx.cpu().numpy()
+            order, groups = level_groups(idx_h, level_schedule(boxes[idx_h]))
+            self._route_nets_device(acc, pres_fac, order, groups, src, dst, boxes, net_nodes, net_edges, net_lens)
+            return
         lib = _lib.load()
         cap = self.cfg.path_cap
         st = _stream()
@@ -311,7 +395,9 @@ class PathFinder:
         dst = np.ascontiguousarray(dst, dtype=np.int32)
         M = len(src)
         cap = cfg.path_cap
-        boxes = bbox_with_margin(self.lat, src, dst, cfg.roi_margin)
+        margins = np.full(M, cfg.roi_margin, dtype=np.int64)
+        streak = np.zeros(M, dtype=np.int64)
+        boxes = bbox_with_margin(self.lat, src, dst, margins)
         vol = (boxes[:, 1] - boxes[:, 0] + 1).astype(np.int64) * (boxes[:, 3] - boxes[:, 2] + 1) * \
             (boxes[:, 5] - boxes[:, 4] + 1)
         order_rank = torch.from_numpy(np.argsort(np.argsort(-vol, kind="stable"), kind="stable").astype(np.int64)).to(dev)
@@ -350,14 +436,27 @@ class PathFinder:
                                  via_cost_multiplier=cfg.via_cost_multiplier, base_cost_weight=cfg.base_cost_weight)
             cost = acc.total_cost
             delta = cfg.delta if cfg.delta is not None else 0.0  # 0: chosen on the device
-            if it == 1 or cfg.reroute == "all":
-                idx = all_idx
-            else:
-                idx = self._offenders(acc, net_edges, net_lens, all_idx)
+            off = None
+            if it > 1 and (cfg.reroute != "all" or cfg.stall_grow > 0):
+                off = self._offenders(acc, net_edges, net_lens, all_idx)
+            idx = all_idx if (it == 1 or cfg.reroute == "all") else off
+            if cfg.stall_grow > 0 and off is not None:
+                # nets that offended stall_iterations times running get a wider box
+                hit = np.zeros(M, dtype=bool)
+                hit[off.cpu().numpy()] = True
+                streak = np.where(hit, streak + 1, 0)
+                grow = streak >= cfg.stall_iterations
+                if grow.any():
+                    margins[grow] += cfg.stall_grow
+                    streak[grow] = 0
+                    boxes = bbox_with_margin(self.lat, src, dst, margins)
+                    boxes_d = torch.from_numpy(boxes).to(dev)
+            if cfg.net_order == "disjoint" and idx.numel() > 1:
+                idx = torch.from_numpy(disjoint_order(boxes, idx.cpu().numpy()).astype(np.int64)).to(dev)
             if idx.numel() > 0 and net_policy:
                 if mode == "batched":
                     self._route_net_batched(acc, pres_fac, idx, src_d, dst_d, boxes_d, boxes, order_rank, net_nodes,
-                                            net_edges, net_lens, delta)
+                                            net_edges, net_lens, delta, src=src, dst=dst)
                 else:
                     self._route_net_sequential(acc, pres_fac, idx, src, dst, boxes, net_nodes, net_edges, net_lens,
                                                delta)

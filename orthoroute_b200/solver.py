@@ -68,6 +68,9 @@ class DeviceGraph:
         md = ctypes.c_int32()
         check(lib.orsp_graph_max_degree(self._h, ctypes.byref(md)), "orsp_graph_max_degree")
         self.max_degree = int(md.value)
+        il = ctypes.c_int32()
+        check(lib.orsp_graph_is_lattice(self._h, ctypes.byref(il)), "orsp_graph_is_lattice")
+        self.is_lattice = bool(il.value)
         self.indptr_host = indptr
         self.indices_host = indices
         self._path_buf = None

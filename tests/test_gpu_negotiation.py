@@ -31,13 +31,16 @@ def test_negotiation_batched_sequential_oracle(reroute):
     assert np.array_equal(rs.edge_usage, ref["usage"])
 
 
-@pytest.mark.parametrize("reroute", ["all", "offenders"])
-def test_negotiation_per_net_costs_levels_match_sequential_and_oracle(reroute):
+@pytest.mark.parametrize("reroute,order,grow", [("all", "index", 0), ("offenders", "index", 0),
+                                                ("offenders", "disjoint", 0), ("offenders", "disjoint", 3)])
+def test_negotiation_per_net_costs_levels_match_sequential_and_oracle(reroute, order, grow):
     """Per-net (live usage) costs: the level-batched run equals the one-search-
-    per-net run and the oracle, per iteration and per net."""
+    per-net run and the oracle, per iteration and per net, also with the
+    first-fit disjoint order and with box growth for stalled nets."""
     b = board_uniform_pins(48, 40, 4, 70, seed=8)
-    cfg = NegotiationConfig(max_iterations=5, reroute=reroute, roi_margin=3, cost_update="net",
-                            full_graph_retry=False)
+    cfg = NegotiationConfig(max_iterations=5 if grow == 0 else 8, reroute=reroute, roi_margin=3,
+                            cost_update="net", full_graph_retry=False, net_order=order, stall_grow=grow,
+                            stall_iterations=1 if grow else 2)
     ref = route_plain(b.lattice, b.src, b.dst, cfg)
     pf = PathFinder(b.lattice, config=cfg)
     rb = pf.route(b.src, b.dst, mode="batched")
@@ -49,3 +52,92 @@ def test_negotiation_per_net_costs_levels_match_sequential_and_oracle(reroute):
         assert np.array_equal(rb.paths[k], ref["paths"][k]), f"net {k} (batched)"
         assert np.array_equal(rs.paths[k], ref["paths"][k]), f"net {k} (sequential)"
     assert np.array_equal(rb.edge_usage, ref["usage"])
+
+
+@pytest.mark.parametrize("reroute", ["all", "offenders"])
+def test_device_routing_loop_equals_host_loop_and_oracle(reroute):
+    """orsp_route_nets (the whole per-net loop enqueued on the device) equals
+    the host-driven loop and the oracle: overuse per iteration, every path,
+    the final usage and the final live costs."""
+    import dataclasses
+
+    b = board_uniform_pins(56, 44, 6, 90, seed=12)
+    cfg = NegotiationConfig(max_iterations=6, reroute=reroute, roi_margin=4, cost_update="net",
+                            full_graph_retry=False)
+    ref = route_plain(b.lattice, b.src, b.dst, cfg)
+    pf = PathFinder(b.lattice, config=cfg)
+    assert pf.dg.is_lattice
+    rd = pf.route(b.src, b.dst, mode="sequential")
+    cost_dev = pf.acc.total_cost.cpu().numpy()
+    pf_h = PathFinder(b.lattice, config=dataclasses.replace(cfg, native_loop=False))
+    rh = pf_h.route(b.src, b.dst, mode="sequential")
+    cost_host = pf_h.acc.total_cost.cpu().numpy()
+    tr_ref = [(s, c) for s, c, _ in ref["trace"]]
+    assert rd.overuse_trace() == tr_ref
+    assert rh.overuse_trace() == tr_ref
+    for k in range(len(b.src)):
+        assert np.array_equal(rd.paths[k], ref["paths"][k]), f"net {k} (device loop)"
+        assert np.array_equal(rh.paths[k], ref["paths"][k]), f"net {k} (host loop)"
+    assert np.array_equal(rd.edge_usage, ref["usage"])
+    assert np.array_equal(rh.edge_usage, ref["usage"])
+    assert np.array_equal(cost_dev.view(np.uint32), cost_host.view(np.uint32))
+
+
+def test_route_nets_group_contract():
+    """orsp_route_nets: overlapping boxes in one group, a repeated net and a
+    group_ptr that does not end at K are rejected on the host; a source
+    outside its box gives no path; level groups equal one-net-at-a-time
+    routing, costs included."""
+    from orthoroute_b200 import _lib
+    from orthoroute_b200._lib import ptr
+    from orthoroute_b200.accounting import DeviceEdgeAccountant
+    from orthoroute_b200.lattice import bbox_with_margin
+    from orthoroute_b200.negotiate import level_groups, level_schedule
+
+    b = board_uniform_pins(64, 48, 4, 40, seed=21)
+    lat = b.lattice
+    pf = PathFinder(lat, config=NegotiationConfig(cost_update="net"))
+    lib = _lib.load()
+    M = len(b.src)
+    boxes = np.ascontiguousarray(bbox_with_margin(lat, b.src, b.dst, 2))
+    cap = 512
+
+    def run(order, groups, boxes_=boxes):
+        acc = DeviceEdgeAccountant(lat.E, device=pf.device)
+        acc.total_cost = pf.base.clone()
+        nodes = torch.zeros((M, cap), dtype=torch.int32, device=pf.device)
+        edges = torch.full((M, cap), -1, dtype=torch.int32, device=pf.device)
+        lens = torch.zeros(M, dtype=torch.int32, device=pf.device)
+        order = np.ascontiguousarray(order, dtype=np.int32)
+        gp = None if groups is None else np.ascontiguousarray(groups, dtype=np.int32)
+        st = lib.orsp_route_nets(pf.dg.handle, M, ptr(np.ascontiguousarray(b.src, np.int32)), ptr(b.dst),
+                                 ptr(np.ascontiguousarray(boxes_, np.int32)), int(order.size), ptr(order),
+                                 0 if gp is None else int(gp.size - 1), ptr(gp), ptr(nodes), ptr(edges), cap,
+                                 ptr(lens), ptr(acc.total_cost), ptr(pf.base), ptr(acc.usage), ptr(acc.present),
+                                 ptr(acc.capacity), ptr(acc.history), 0.5, 1.0, 1.0, 1.0, 1, 0)
+        torch.cuda.synchronize()
+        return st, nodes.cpu().numpy(), lens.cpu().numpy(), acc.usage.cpu().numpy(), acc.total_cost.cpu().numpy()
+
+    lv = level_schedule(boxes)
+    order, groups = level_groups(np.arange(M), lv)
+    assert groups.size - 1 < M  # some launch holds several nets
+    st1, n1, l1, u1, c1 = run(np.arange(M), None)
+    st2, n2, l2, u2, c2 = run(order, groups)
+    assert st1 == 0 and st2 == 0
+    assert np.array_equal(l1, l2) and np.array_equal(u1, u2)
+    assert np.array_equal(c1.view(np.uint32), c2.view(np.uint32))
+    for k in range(M):
+        assert np.array_equal(n1[k, : l1[k]], n2[k, : l2[k]])
+    i, j = next((i, j) for i in range(M) for j in range(i) if
+                boxes[i, 0] <= boxes[j, 1] and boxes[j, 0] <= boxes[i, 1] and
+                boxes[i, 2] <= boxes[j, 3] and boxes[j, 2] <= boxes[i, 3])
+    assert run([j, i], [0, 2])[0] == _lib.ORSP_ERR_ARG
+    assert run([0, 0], None)[0] == _lib.ORSP_ERR_ARG
+    assert run(np.arange(M), [0, M // 2])[0] == _lib.ORSP_ERR_ARG
+    # net 0 gets a box that does not hold its source: no path for it
+    bx = boxes.copy()
+    sx, sy = int(b.src[0] % lat.nx), int((b.src[0] // lat.nx) % lat.ny)
+    bx[0] = (0, 3, 0, 3, 0, lat.nz - 1) if (sx > 3 or sy > 3) else (60, 63, 44, 47, 0, lat.nz - 1)
+    st3, _, l3, _, _ = run(np.arange(M), None, boxes_=bx)
+    assert st3 == 0 and l3[0] == 0
+
