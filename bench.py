@@ -16,6 +16,11 @@ the weights copied from pinned host memory and every distance array copied
 back each step.  With N > 1 (torchrun) every rank runs its own replica of the
 workload (different seeds) - the search does not shard - and the times are the
 max over ranks.
+
+The `routing` object reports seconds to a zero-overuse route on two boards
+(100x100x4 with 200 nets; the 600x600x18 backplane with 8 000 nets, one GPU
+only), plain vs batched, with the routes checked identical; --no-route skips
+it.
 """
 from __future__ import annotations
 
@@ -228,6 +233,63 @@ def route_c1(dev, with_cpu: bool):
     return out
 
 
+def route_c3(dev, with_cpu: bool):
+    """Backplane board (600x600x18 lattice, 8 000 two-pin nets between 2x50-pin
+    connector footprints, one net per pin, ROI = bounding box + 10 cells)
+    routed to zero overuse with per-net live costs: plain (one search launch
+    per net, the device loop orsp_route_nets) vs batched (one launch per round
+    of pairwise disjoint boxes).  Both take the nets in the same first-fit
+    disjoint-round order and widen the box of a net that offends twice
+    running by 10 cells, so their routes are identical (checked here)."""
+    from orthoroute_b200.lattice import board_footprints
+    from orthoroute_b200.negotiate import NegotiationConfig, PathFinder
+
+    b = board_footprints(600, 600, 18, 8000, None, seed=3)
+    cfg = NegotiationConfig(max_iterations=40, cost_update="net", reroute="offenders", roi_margin=10,
+                            full_graph_retry=False, net_order="disjoint", stall_grow=10, stall_iterations=2)
+    pf = PathFinder(b.lattice, config=cfg, device=dev)
+    rb = pf.route(b.src, b.dst, mode="batched")
+    rs = pf.route(b.src, b.dst, mode="sequential")
+    same = rb.overuse_trace() == rs.overuse_trace() and all(
+        np.array_equal(x, y) for x, y in zip(rb.paths, rs.paths)) and np.array_equal(rb.edge_usage, rs.edge_usage)
+    searches = int(sum(s.nets_searched for s in rb.iterations))
+    out = {
+        "workload": "600x600x18 lattice, 8000 nets between 2x50 connector footprints, bbox+10 ROI, "
+                    "per-net live costs, offenders rerouted, disjoint-round order",
+        "converged": bool(rb.converged),
+        "iterations": len(rb.iterations),
+        "searches": searches,
+        "sec_batched": round(rb.seconds, 3),
+        "sec_plain": round(rs.seconds, 3),
+        "speedup_batched_vs_plain": round(rs.seconds / rb.seconds, 2),
+        "identical_routes": bool(same),
+        "wirelength": rb.wirelength,
+        "vias": rb.vias,
+        "overuse_trace": [s.over_sum for s in rb.iterations],
+    }
+    if with_cpu:
+        # The C oracle of one box search (heap Dijkstra, fp32) on a sample of
+        # iteration-1 nets, scaled to the run's search count: a full CPU run of
+        # this board takes hours.
+        import oracle as O
+
+        O.build_oracle()
+        lat = b.lattice
+        from orthoroute_b200.lattice import bbox_with_margin
+
+        boxes = bbox_with_margin(lat, b.src, b.dst, 10)
+        sample = np.random.default_rng(0).choice(len(b.src), size=12, replace=False)
+        t0 = time.perf_counter()
+        for k in sample:
+            O.batch_bbox(lat.indptr, lat.indices, lat.base_cost, lat.nx, lat.ny, lat.nz, b.src[k:k + 1],
+                         b.dst[k:k + 1], boxes[k:k + 1], 8192)
+        per = (time.perf_counter() - t0) / len(sample)
+        out["cpu_oracle_sec_per_search"] = round(per, 4)
+        out["cpu_oracle_sec_extrapolated"] = round(per * searches, 1)
+        out["cpu_oracle_sample"] = f"{len(sample)} iteration-1 box searches, 1 core, scaled to {searches} searches"
+    return out
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -321,7 +383,12 @@ def run_ours(args, world, rank, local):
     e2e_ms = reduce_max(e0.elapsed_time(e1), world)
     e2e_value = reduce_sum(e_relaxed * e2e_steps, world) / (e2e_ms / 1e3) / 1e9
 
-    routing = route_c1(dev, with_cpu=(rank == 0 and world == 1 and not args.no_cpu)) if not args.no_route else None
+    routing = None
+    if not args.no_route:
+        with_cpu = rank == 0 and world == 1 and not args.no_cpu
+        routing = {"c1": route_c1(dev, with_cpu=with_cpu)}
+        if world == 1:
+            routing["c3"] = route_c3(dev, with_cpu=with_cpu)
     result = {
         "metric": METRIC,
         "value": round(value, 4),
