@@ -20,7 +20,9 @@ max over ranks.
 The `routing` object reports seconds to a zero-overuse route on two boards
 (100x100x4 with 200 nets; the 600x600x18 backplane with 8 000 nets, one GPU
 only), plain vs batched, with the routes checked identical; --no-route skips
-it.
+it.  The `batch_sweep` object reports the batched uneven-ROI sweep (4 096 box
+searches, one GPU only): one search per launch vs the default and the tuned
+batch plan; --no-sweep skips it.
 """
 from __future__ import annotations
 
@@ -290,6 +292,86 @@ def route_c3(dev, with_cpu: bool):
     return out
 
 
+def sweep_c4(dev, nsearch: int = 4096):
+    """Batched uneven-ROI sweep: 4 096 independent box searches on one shared
+    fp32 cost array (400x400x16 lattice, weights uniform in [1,2), vias 3.0,
+    3 % blocked), box sides log-uniform per axis (x, y in [20, 400], z in
+    [4, 16]), source and target uniform in each box.  Three runs of the same
+    searches: one search per launch (orsp_sssp_box), the default batch plan
+    (one CTA per search), and the plan the autotuner picks per ROI-size
+    bucket; the paths must be identical."""
+    import torch
+
+    from orthoroute_b200.autotune import tune_batch
+    from orthoroute_b200.lattice import box_edge_count, build_lattice, random_boxes, uniform_weights
+    from orthoroute_b200.solver import DeviceGraph
+
+    lat = build_lattice(400, 400, 16)
+    w = uniform_weights(lat, seed=SEED + 4, blocked_frac=0.03)
+    boxes, src, dst = random_boxes(lat, nsearch, seed=SEED + 5, lo=(20, 20, 4), hi=(400, 400, 16))
+    dg = DeviceGraph.from_lattice(lat, device=dev)
+    wt = torch.from_numpy(w).to(dev)
+    s_d = torch.from_numpy(src).to(dev)
+    t_d = torch.from_numpy(dst).to(dev)
+    b_d = torch.from_numpy(boxes).to(dev)
+    cap = 4096
+    roi_edges = int(box_edge_count(lat, boxes).sum())
+
+    def timed(fn):
+        fn()  # warm-up (workspaces)
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / 1e3, out
+
+    def one_per_launch():
+        lens = np.zeros(nsearch, np.int32)
+        rows = []
+        for k in range(nsearch):
+            st, p, _ = dg.sssp_box(wt, int(src[k]), int(dst[k]), boxes[k], path_cap=cap)
+            rows.append(p.clone() if p is not None else None)
+        return rows
+
+    def batch():
+        return dg.batch_bbox(wt, s_d, t_d, b_d, path_cap=cap, with_edges=True)
+
+    t_single, rows = timed(one_per_launch)
+    dg.set_batch_plan(None)
+    t_default, (n0, _, l0) = timed(batch)
+    t0 = time.perf_counter()
+    tune = tune_batch(dg, wt, s_d, t_d, boxes, sample=1024, path_cap=cap)
+    t_tune = time.perf_counter() - t0
+    t_tuned, (n1, _, l1) = timed(batch)
+    l0, l1 = l0.cpu().numpy(), l1.cpu().numpy()
+    n0, n1 = n0.cpu().numpy(), n1.cpu().numpy()
+    same = np.array_equal(l0, l1) and all(np.array_equal(n0[k, : l0[k]], n1[k, : l1[k]]) for k in range(nsearch))
+    same_single = all(
+        (rows[k] is None and l0[k] < 2) or (rows[k] is not None and l0[k] == rows[k].numel() and
+                                              np.array_equal(rows[k].cpu().numpy(), n0[k, : l0[k]]))
+        for k in range(nsearch))
+    vol = ((boxes[:, 1] - boxes[:, 0] + 1).astype(np.int64) * (boxes[:, 3] - boxes[:, 2] + 1) *
+           (boxes[:, 5] - boxes[:, 4] + 1))
+    return {
+        "workload": f"{nsearch} box searches on a 400x400x16 lattice, sides log-uniform per axis "
+                    "(x,y 20..400, z 4..16), 3% blocked, shared fp32 costs",
+        "mean_roi_nodes": int(vol.mean()),
+        "roi_edges_total": roi_edges,
+        "searches_per_s_one_per_launch": round(nsearch / t_single, 1),
+        "searches_per_s_default_plan": round(nsearch / t_default, 1),
+        "searches_per_s_tuned": round(nsearch / t_tuned, 1),
+        "gteps_tuned": round(roi_edges / t_tuned / 1e9, 3),
+        "gteps_unit": "directed ROI edges of all searches per second",
+        "speedup_tuned_vs_one_per_launch": round(t_single / t_tuned, 2),
+        "sec_tuning": round(t_tune, 2),
+        "plan": [{k: v for k, v in b.items()} for b in tune.plan],
+        "identical_paths": bool(same and same_single),
+    }
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -389,6 +471,7 @@ def run_ours(args, world, rank, local):
         routing = {"c1": route_c1(dev, with_cpu=with_cpu)}
         if world == 1:
             routing["c3"] = route_c3(dev, with_cpu=with_cpu)
+    batch_sweep = sweep_c4(dev) if (world == 1 and not args.no_sweep) else None
     result = {
         "metric": METRIC,
         "value": round(value, 4),
@@ -423,6 +506,7 @@ def run_ours(args, world, rank, local):
                      "avg_launch_ms": round(avg_kernel_ms, 4)},
         "clocks": clk,
         "routing": routing,
+        "batch_sweep": batch_sweep,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         result["cpu_baseline"] = cpu_baseline(lat, w, sources, threads=os.cpu_count() or 1)
@@ -490,7 +574,8 @@ def main():
     ap.add_argument("--sources", type=int, default=NSRC)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-check", action="store_true", help="skip the parity check before timing")
-    ap.add_argument("--no-route", action="store_true", help="skip the config-1 routing measurement")
+    ap.add_argument("--no-route", action="store_true", help="skip the routing measurements")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the batched uneven-ROI sweep")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:

@@ -164,8 +164,8 @@ ORSP_API int orsp_roi_from_bitmap(orsp_graph *g, const uint32_t *bitmap_d, int32
  * work item, backtraces it and maps the path to CSR edges.
  * Replaces CUDADijkstra.find_paths_on_rois (CD:2014-2086) for box ROIs and
  * the per-net loop body of _route_all (UPF:4475-4800) under fixed costs.
- *   order_d               optional int32[K] processing order (e.g. largest
- *                          box first); NULL = 0..K-1.
+ *   order_d               optional int32[K] processing order, a permutation
+ *                          of 0..K-1 (e.g. largest box first); NULL = 0..K-1.
  *   delta                  bucket width as for orsp_sssp (0: device choice).
  *   path_nodes_d/edges_d  int32[K*path_cap] outputs (edges_d may be NULL).
  *   path_len_d            int32[K]: path length, 0 = no path, <0 = error. */
@@ -189,6 +189,23 @@ ORSP_API int orsp_sssp_batch_ranges(orsp_graph *g, const float *cost_d, int32_t 
                            float delta, int32_t *path_nodes_d,
                            int32_t *path_edges_d, int32_t path_cap,
                            int32_t *path_len_d, uintptr_t stream);
+
+/* Tuning plan for orsp_sssp_batch_bbox (no counterpart in the reference,
+ * whose batch search has one fixed configuration).  Boxes are put into
+ * buckets by node count: bucket i takes the boxes with
+ * max_nodes[i-1] < V <= max_nodes[i] (the last bucket takes every larger box
+ * too).  Per bucket:
+ *   impl 0   one CTA per search (block-local near-far) with bucket width
+ *            delta[i] (0: the call's); all impl-0 searches of a call share
+ *            one launch of the largest ctas_per_sm of their buckets CTAs per
+ *            SM (0: default 2);
+ *   impl 1   tile sweeps over many boxes per launch, each box with its own
+ *            distance slice, tile width tile_w[i] (16 or 32); used on graphs
+ *            recognised as H/V lattices, impl 0 otherwise.
+ * nb = 0 restores the default (impl 0 for every box).  Every plan gives the
+ * same paths, bit for bit; the plan only changes the time. */
+ORSP_API int orsp_batch_set_plan(orsp_graph *g, int32_t nb, const int64_t *max_nodes, const int32_t *impl,
+                        const float *delta, const int32_t *tile_w, const int32_t *ctas_per_sm);
 
 /* ---- routing loop ------------------------------------------------------ */
 /* Routes nets with per-net live costs, as the per-net body of _route_all

@@ -51,6 +51,7 @@ _SIGS = {
                                  ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
     "orsp_sssp_box": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _f32, _P, _P, _i32,
                                      ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
+    "orsp_batch_set_plan": (ctypes.c_int, [_P, _i32, _P, _P, _P, _P, _P]),
     "orsp_route_nets": (ctypes.c_int, [_P, _i32, _P, _P, _P, _i32, _P, _i32, _P, _P, _P, _i32, _P, _P, _P, _P, _P,
                                        _P, _P, _f32, _f32, _f32, _f32, _i32, _u]),
     "orsp_sssp_multi": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _P, _P, _f32, _P, _i32,

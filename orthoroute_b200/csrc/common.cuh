@@ -68,6 +68,19 @@ struct Graph {
   // routing loop (orsp_route.cu): error word, per-call net tables (device)
   // and their pinned staging copy
   void *route_ws = nullptr;
+  // batched search: tuning plan (orsp_batch_set_plan), item lists, and the
+  // distance arena and tile tables of boxes searched by tile sweeps
+  int32_t plan_nb = 0;
+  int64_t plan_max_nodes[8];
+  int32_t plan_impl[8], plan_tile[8], plan_ctas[8];
+  float plan_delta[8];
+  int32_t *batch_idx = nullptr;
+  size_t batch_idx_bytes = 0;
+  uint32_t *blat_dist = nullptr;
+  size_t blat_dist_bytes = 0;
+  void *blat_tab_d = nullptr;
+  void *blat_tab_h = nullptr;
+  size_t blat_tab_bytes = 0;
   void *route_tab_d = nullptr;
   void *route_tab_h = nullptr;
   size_t route_tab_bytes = 0;
@@ -109,12 +122,20 @@ struct LatBox {
   int32_t x0, x1, y0, y1, z0, z1;
   int32_t ntx, nty;  // tiles along x and y
   int32_t tile0;     // id of the box's first tile
+  int32_t pad;
+  int64_t dbase;     // -1: distances indexed by node id in the shared array;
+                     // >= 0: the box's own slice, box-local row-major from here
 };
 // Tile width of the lattice search (ORSP_LAT_TILE: 16 or 32); the height is 16.
 int lattice_tile_w();
-// Fills out[i] for boxes_h[6i..6i+5] and returns the total tile count.
-int64_t make_lat_boxes(const int32_t *boxes_h, int32_t nbox, LatBox *out);
+// Fills out[i] for boxes_h[6i..6i+5] (tile width tile_w, 0 = lattice_tile_w(),
+// shared distances) and returns the total tile count.
+int64_t make_lat_boxes(const int32_t *boxes_h, int32_t nbox, LatBox *out, int tile_w = 0);
 struct LatOptions {
+  int tile_w = 0;              // tile width (0: lattice_tile_w()); the tables must use the same
+  bool private_dist = false;   // boxes have their own slices (dbase >= 0): seed i starts box i, and
+                               // `dist` is the slice arena of private_count entries, all reset
+  int64_t private_count = 0;
   bool fill_box_only = false;  // reset distances inside the boxes only (the caller's backtrace checks the box)
   bool copy_ctl = true;        // copy the control block to the pinned mirror (finish_lattice_search)
   int *err_d = nullptr;        // out: device address of the launch's error word

@@ -50,6 +50,7 @@ struct BatchParams {
   int32_t smem_nodes;
   float delta;
   const float *delta_d;  // device bucket width (overrides delta) or nullptr
+  const float *delta_k;  // per-search bucket width (> 0 overrides the above) or nullptr
   unsigned *work_counter;
   unsigned long long budget_ns;
 };
@@ -110,7 +111,7 @@ struct BlockCtl {
 template <bool SMEM>
 __device__ void block_search(const BatchParams &p, const Box &b, int32_t src_l, int32_t dst_l,
                              uint32_t *dist, int2 *nq0, int2 *nq1, int2 *fq0, int2 *fq1,
-                             BlockCtl *c, unsigned long long t_start) {
+                             BlockCtl *c, unsigned long long t_start, float delta) {
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int nwarps = blockDim.x >> 5;
@@ -189,7 +190,7 @@ __device__ void block_search(const BatchParams &p, const Box &b, int32_t src_l, 
       if (fc == 0) break;
       if (bits_f(dist_ld<SMEM>(dist, dst_l)) < T) break;
       const float fm = bits_f(c->fmin[g % 4]);
-      float Tn = __fadd_rn(fm, p.delta_d ? *p.delta_d : p.delta);
+      float Tn = __fadd_rn(fm, delta);
       if (!(Tn > fm)) Tn = __uint_as_float(f_bits(fm) + 1u);
       const int2 *fin = ((g & 1) ? fq1 : fq0);
       int2 *fout = (((g + 1) & 1) ? fq1 : fq0);
@@ -351,10 +352,12 @@ __global__ void __launch_bounds__(BATCH_THREADS) batch_bbox_kernel(BatchParams p
     }
     const bool use_smem = b.V <= p.smem_nodes;
     uint32_t *dist = use_smem ? s_dist : gdist;
+    const float dk = p.delta_k ? p.delta_k[k] : 0.0f;
+    const float delta = dk > 0.0f ? dk : (p.delta_d ? *p.delta_d : p.delta);
     if (use_smem)
-      block_search<true>(p, b, src_l, dst_l, dist, nq0, nq1, fq0, fq1, &ctl, t_start);
+      block_search<true>(p, b, src_l, dst_l, dist, nq0, nq1, fq0, fq1, &ctl, t_start, delta);
     else
-      block_search<false>(p, b, src_l, dst_l, dist, nq0, nq1, fq0, fq1, &ctl, t_start);
+      block_search<false>(p, b, src_l, dst_l, dist, nq0, nq1, fq0, fq1, &ctl, t_start, delta);
     int status;
     if (ctl.err == DEV_ERR_OVERFLOW) status = ST_QUEUE;
     else if (ctl.err) status = ST_ROUNDS;
@@ -377,60 +380,164 @@ int env_int(const char *name, int dflt) {
   return atoi(s);
 }
 
+// Backtrace of the searches done by tile sweeps with their own distance
+// slices: one warp per search (block j: item[j], box boxes[j]), the same walk,
+// parent rule, first-CSR-edge lookup and status codes as block_backtrace, with
+// the distances read from the box's slice (box-local row-major order, which is
+// the node-id order, so the ranks agree).
+struct LatBt {
+  const float *cost;
+  const int32_t *rptr, *rsrc, *reid;
+  const uint32_t *dist;  // slice arena
+  int32_t nx, ny;
+  const orsp::LatBox *boxes;
+  const int32_t *item, *src, *dst;  // per box: search id, source, target (global ids)
+  int32_t *path_nodes, *path_edges, *path_len;
+  int32_t path_cap;
+  const int *search_err;
+};
+
+__device__ __forceinline__ bool lat_local(const LatBt &p, const orsp::LatBox &B, int32_t u, int64_t *li) {
+  const int32_t plane = p.nx * p.ny;
+  const int32_t z = u / plane, r = u - z * plane, y = r / p.nx, x = r - y * p.nx;
+  if (x < B.x0 || x > B.x1 || y < B.y0 || y > B.y1 || z < B.z0 || z > B.z1) return false;
+  const int64_t bw = B.x1 - B.x0 + 1, bh = B.y1 - B.y0 + 1;
+  *li = ((int64_t)(z - B.z0) * bh + (y - B.y0)) * bw + (x - B.x0);
+  return true;
+}
+
+__global__ void lat_batch_backtrace_kernel(LatBt p) {
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x;
+  const int32_t k = p.item[j];
+  const orsp::LatBox B = p.boxes[j];
+  const int32_t src = p.src[j], dst = p.dst[j];
+  int32_t *nodes = p.path_nodes + (int64_t)k * p.path_cap;
+  int32_t *edges = p.path_edges ? p.path_edges + (int64_t)k * p.path_cap : nullptr;
+  int64_t ls, ld;
+  if (src < 0 || dst < 0 || !lat_local(p, B, src, &ls) || !lat_local(p, B, dst, &ld)) {
+    if (lane == 0) p.path_len[k] = ST_ARG;
+    return;
+  }
+  if (*p.search_err) {
+    if (lane == 0) p.path_len[k] = ST_ROUNDS;
+    return;
+  }
+  const uint32_t *dist = p.dist + B.dbase;
+  unsigned dv = dist[ld];
+  if (dv == ORSP_INF_BITS) {
+    if (lane == 0) p.path_len[k] = 0;
+    return;
+  }
+  int32_t v = dst;
+  int64_t lv = ld;
+  int len = 0, status = 0;
+  for (;;) {
+    if (len >= p.path_cap) { status = ST_PATHCAP; break; }
+    if (lane == 0) nodes[len] = v;
+    ++len;
+    if (v == src) break;
+    const int kb = __ldg(&p.rptr[v]), ke = __ldg(&p.rptr[v + 1]);
+    unsigned long long best = ULLONG_MAX;
+    int32_t bu = -1;
+    for (int k0 = kb; k0 < ke; k0 += 32) {
+      const int kk = k0 + lane;
+      if (kk < ke) {
+        const int32_t u = __ldg(&p.rsrc[kk]);
+        int64_t lu;
+        if (lat_local(p, B, u, &lu)) {
+          const unsigned du = dist[lu];
+          if (du != ORSP_INF_BITS) {
+            const float s = __fadd_rn(bits_f(du), __ldg(&p.cost[__ldg(&p.reid[kk])]));
+            if (f_bits(s) == dv && (du < dv || (du == dv && lu < lv))) {
+              const unsigned long long key = ((unsigned long long)du << 32) | (unsigned)lu;
+              if (key < best) { best = key; bu = u; }
+            }
+          }
+        }
+      }
+    }
+    const unsigned long long wbest = warp_min_u64(best);
+    if (wbest == ULLONG_MAX) { status = ST_INTERNAL; break; }
+    const unsigned owner = __ballot_sync(ORSP_FULL_MASK, best == wbest && bu >= 0);
+    const int32_t u = __shfl_sync(ORSP_FULL_MASK, bu, __ffs(owner) - 1);
+    int32_t emin = INT_MAX;
+    for (int k0 = kb; k0 < ke; k0 += 32) {
+      const int kk = k0 + lane;
+      if (kk < ke && __ldg(&p.rsrc[kk]) == u) emin = min(emin, __ldg(&p.reid[kk]));
+    }
+    emin = __reduce_min_sync(ORSP_FULL_MASK, emin);
+    if (edges && lane == 0 && len - 1 < p.path_cap) edges[len - 1] = emin;
+    v = u;
+    lv = (int64_t)(wbest & 0xffffffffu);
+    dv = (unsigned)(wbest >> 32);
+  }
+  __syncwarp();
+  if (status) {
+    if (lane == 0) p.path_len[k] = status;
+    return;
+  }
+  for (int i = lane; i < len / 2; i += 32) {
+    const int32_t a = nodes[i], z = nodes[len - 1 - i];
+    nodes[i] = z;
+    nodes[len - 1 - i] = a;
+  }
+  if (edges) {
+    const int ne = len - 1;
+    for (int i = lane; i < ne / 2; i += 32) {
+      const int32_t a = edges[i], z = edges[ne - 1 - i];
+      edges[i] = z;
+      edges[ne - 1 - i] = a;
+    }
+  }
+  __syncwarp();
+  if (lane == 0) p.path_len[k] = len;
+}
+
+
 }  // namespace
 
 using namespace orsp;
 
-static int run_batch(orsp_graph *g, const float *cost_d, int32_t K, const int32_t *src_d,
-                     const int32_t *dst_d, const int32_t *bbox_d, int range_mode,
-                     const int32_t *order_d, float delta, int32_t *path_nodes_d,
-                     int32_t *path_edges_d, int32_t path_cap, int32_t *path_len_d,
-                     uintptr_t stream) {
-  if (!g || !cost_d || K < 0 || (K > 0 && (!src_d || !dst_d || !bbox_d || !path_nodes_d ||
-                                           !path_len_d)) || path_cap <= 0) {
-    set_error("batch search: NULL argument or path_cap <= 0");
-    return ORSP_ERR_ARG;
-  }
-  if (!range_mode && g->nx <= 0) { set_error("batch_bbox: graph was created without lattice dims"); return ORSP_ERR_ARG; }
-  if (!(delta >= 0.0f) || !(delta < 3.0e38f)) { set_error("delta must be finite and >= 0 (0: chosen on the device)"); return ORSP_ERR_ARG; }
-  if (K == 0) return ORSP_OK;
-  ORSP_CUDA(cudaSetDevice(g->device));
-  cudaStream_t st = (cudaStream_t)stream;
+namespace {
 
-  // ROI sizes are needed on the host to size the per-CTA slots.
+
+int64_t box_volume(const int32_t *b, int range_mode) {
+  if (range_mode) return (int64_t)b[1] - b[0];
+  return (int64_t)(b[1] - b[0] + 1) * (b[3] - b[2] + 1) * (b[5] - b[4] + 1);
+}
+
+int grow_dev(void **p, size_t *have, size_t need) {
+  if (*have >= need) return ORSP_OK;
+  cudaFree(*p);
+  *p = nullptr;
+  *have = 0;
+  ORSP_CUDA(cudaMalloc(p, need));
+  *have = need;
+  return ORSP_OK;
+}
+
+// Searches `items` with one CTA per search (the block-local near-far kernel),
+// in the order given, queue overflows re-run with 4x larger queues.
+int run_batch_cta(orsp_graph *g, const float *cost_d, int32_t K, const std::vector<int32_t> &items, const int32_t *src_d,
+                  const int32_t *dst_d, const int32_t *bbox_d, const std::vector<int32_t> &bb, int range_mode,
+                  float delta, const std::vector<float> &delta_k, int ctas_per_sm, int32_t *path_nodes_d,
+                  int32_t *path_edges_d, int32_t path_cap, int32_t *path_len_d, cudaStream_t st) {
+  const int32_t n = (int32_t)items.size();
+  if (n == 0) return ORSP_OK;
   const int per = range_mode ? 2 : 6;
-  std::vector<int32_t> bb((size_t)per * K);
-  ORSP_CUDA(cudaMemcpyAsync(bb.data(), bbox_d, bb.size() * 4, cudaMemcpyDeviceToHost, st));
-  ORSP_CUDA(cudaStreamSynchronize(st));
   int64_t vmax = 1;
-  for (int32_t k = 0; k < K; ++k) {
-    const int32_t *b = &bb[(size_t)per * k];
-    int64_t v;
-    if (range_mode) {
-      if (b[0] < 0 || b[1] > g->N || b[1] <= b[0]) {
-        set_error("batch_ranges: node range outside the graph or empty");
-        return ORSP_ERR_ARG;
-      }
-      v = (int64_t)b[1] - b[0];
-    } else {
-      if (b[0] < 0 || b[2] < 0 || b[4] < 0 || b[1] >= g->nx || b[3] >= g->ny || b[5] >= g->nz ||
-          b[1] < b[0] || b[3] < b[2] || b[5] < b[4]) {
-        set_error("batch_bbox: box outside the lattice or empty");
-        return ORSP_ERR_ARG;
-      }
-      v = (int64_t)(b[1] - b[0] + 1) * (b[3] - b[2] + 1) * (b[5] - b[4] + 1);
-    }
-    vmax = std::max(vmax, v);
-  }
+  for (int32_t k : items) vmax = std::max(vmax, box_volume(&bb[(size_t)per * k], range_mode));
+  // device: order (n), retry list (n), per-search widths (K, when given)
+  const bool per_k = !delta_k.empty();
+  int rc = grow_dev((void **)&g->batch_idx, &g->batch_idx_bytes, (size_t)n * 8 + (per_k ? (size_t)K * 4 : 0) + 256);
+  if (rc) return rc;
+  int32_t *order_all = g->batch_idx;
+  int32_t *retry_d = g->batch_idx + n;
+  float *dk_d = per_k ? (float *)(g->batch_idx + 2 * (size_t)n) : nullptr;
+  ORSP_CUDA(cudaMemcpyAsync(order_all, items.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st));
+  if (per_k) ORSP_CUDA(cudaMemcpyAsync(dk_d, delta_k.data(), (size_t)K * 4, cudaMemcpyHostToDevice, st));
 
-  if (order_d) {
-    std::vector<int32_t> ord(K);
-    ORSP_CUDA(cudaMemcpyAsync(ord.data(), order_d, (size_t)K * 4, cudaMemcpyDeviceToHost, st));
-    ORSP_CUDA(cudaStreamSynchronize(st));
-    for (int32_t k = 0; k < K; ++k)
-      if (ord[k] < 0 || ord[k] >= K) { set_error("batch_bbox: order entry out of range"); return ORSP_ERR_ARG; }
-  }
-  const int ctas_per_sm = std::max(1, env_int("ORSP_BATCH_CTAS_PER_SM", 2));
   const int smem_nodes = std::max(0, env_int("ORSP_BATCH_SMEM_NODES", 24 * 1024));
   const size_t smem_bytes = (size_t)smem_nodes * 4;
   ORSP_CUDA(cudaFuncSetAttribute(batch_bbox_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -441,7 +548,6 @@ static int run_batch(orsp_graph *g, const float *cost_d, int32_t K, const int32_
   // grow to the worst case (one item per directed edge) for re-runs.
   int64_t qcap = 2 * vmax + 4096;
   const int64_t qcap_max = (int64_t)std::max(1, g->max_degree) * vmax + 4096;
-  std::vector<int32_t> retry;
   BatchParams p{};
   p.indptr = g->indptr;
   p.indices = g->indices;
@@ -465,19 +571,20 @@ static int run_batch(orsp_graph *g, const float *cost_d, int32_t K, const int32_
   p.smem_nodes = smem_nodes;
   p.delta = delta;
   p.delta_d = nullptr;
+  p.delta_k = dk_d;
   if (delta == 0.0f) {
-    int rc = launch_auto_delta(cost_d, g->E, g->auto_delta + 1, st);
+    rc = launch_auto_delta(cost_d, g->E, g->auto_delta + 1, st);
     if (rc) return rc;
     p.delta_d = g->auto_delta + 1;
   }
   p.budget_ns = 30ull * 1000000000ull;
 
-  const int32_t *order = order_d;
-  int32_t n_items = K;
-  int32_t *retry_d = nullptr;
+  const int32_t *order = order_all;
+  int32_t n_items = n;
+  std::vector<int32_t> lens, retry, retry_h;
   for (int attempt = 0; attempt < 4; ++attempt) {
     const size_t slot_bytes = (((size_t)4 * qcap * sizeof(int2) + (size_t)vmax * 4) + 255) & ~(size_t)255;
-    int nslots = g->num_sms * ctas_per_sm;
+    int nslots = g->num_sms * std::max(1, ctas_per_sm);
     nslots = (int)std::max<size_t>(1, std::min<size_t>((size_t)nslots, ws_budget / slot_bytes));
     nslots = std::min<int>(nslots, n_items);
     const size_t need = slot_bytes * nslots + 256;
@@ -499,25 +606,258 @@ static int run_batch(orsp_graph *g, const float *cost_d, int32_t K, const int32_
     batch_bbox_kernel<<<nslots, BATCH_THREADS, smem_bytes, st>>>(p);
     ORSP_CUDA(cudaGetLastError());
 
-    // Collect queue overflows for a re-run with larger queues.
-    std::vector<int32_t> lens(K);
+    // Collect queue overflows (of this call's items) for a re-run with larger queues.
+    lens.resize((size_t)K);
     ORSP_CUDA(cudaMemcpyAsync(lens.data(), path_len_d, (size_t)K * 4, cudaMemcpyDeviceToHost, st));
     ORSP_CUDA(cudaStreamSynchronize(st));
     retry.clear();
-    for (int32_t k = 0; k < K; ++k)
+    const std::vector<int32_t> &cur = (attempt == 0) ? items : retry_h;
+    for (int32_t k : cur)
       if (lens[k] == ST_QUEUE) retry.push_back(k);
     if (retry.empty() || qcap >= qcap_max) break;
     qcap = std::min(qcap_max, qcap * 4);
-    if (!retry_d) {
-      int rc = ensure_scratch(g, (size_t)K * 4);
-      if (rc) return rc;
-      retry_d = (int32_t *)g->scratch;
-    }
     ORSP_CUDA(cudaMemcpyAsync(retry_d, retry.data(), retry.size() * 4, cudaMemcpyHostToDevice, st));
     order = retry_d;
     n_items = (int32_t)retry.size();
+    retry_h = retry;
+  }
+  return ORSP_OK;
+}
+
+// Searches `items` (box ROIs) by tile sweeps, many boxes per launch, each box
+// with its own distance slice so that boxes may overlap.  Items are taken in
+// chunks whose slices fit the arena (ORSP_BATCH_LAT_MB, default 4096 MB).
+int run_batch_lat(orsp_graph *g, const float *cost_d, int32_t K, const std::vector<int32_t> &items,
+                  const std::vector<int32_t> &bb, const std::vector<int32_t> &src_h,
+                  const std::vector<int32_t> &dst_h, int tile_w, int32_t *path_nodes_d, int32_t *path_edges_d,
+                  int32_t path_cap, int32_t *path_len_d, cudaStream_t st) {
+  (void)K;
+  const size_t n = items.size();
+  if (n == 0) return ORSP_OK;
+  const int64_t arena_cells = ((int64_t)std::max(64, env_int("ORSP_BATCH_LAT_MB", 4096)) << 20) / 4;
+  size_t a = 0;
+  while (a < n) {
+    // chunk [a, b): slices within the arena (a single larger box gets its own chunk)
+    size_t b = a;
+    int64_t cells = 0;
+    while (b < n && b - a < 65536) {
+      const int64_t v = box_volume(&bb[(size_t)6 * items[b]], 0);
+      if (b > a && cells + v > arena_cells) break;
+      cells += v;
+      ++b;
+    }
+    const int32_t m = (int32_t)(b - a);
+    int rc = grow_dev((void **)&g->blat_dist, &g->blat_dist_bytes, (size_t)cells * 4 + 256);
+    if (rc) return rc;
+    // tables: boxes (LatBox), item ids, sources, targets - staged in pinned
+    // memory, copied once per chunk; the chunk is synchronised before the
+    // staging buffer is reused
+    const size_t tab = (size_t)m * sizeof(LatBox) + (size_t)m * 12 + 256;
+    if (g->blat_tab_bytes < tab) {
+      cudaFree(g->blat_tab_d);
+      if (g->blat_tab_h) cudaFreeHost(g->blat_tab_h);
+      g->blat_tab_d = nullptr;
+      g->blat_tab_h = nullptr;
+      g->blat_tab_bytes = 0;
+      ORSP_CUDA(cudaMalloc(&g->blat_tab_d, tab));
+      ORSP_CUDA(cudaMallocHost(&g->blat_tab_h, tab));
+      g->blat_tab_bytes = tab;
+    }
+    LatBox *hb = (LatBox *)g->blat_tab_h;
+    int32_t *h_item = (int32_t *)(hb + m);
+    int32_t *h_src = h_item + m;
+    int32_t *h_dst = h_src + m;
+    std::vector<int32_t> boxes((size_t)m * 6);
+    for (int32_t j = 0; j < m; ++j) {
+      const int32_t k = items[a + j];
+      for (int c = 0; c < 6; ++c) boxes[(size_t)j * 6 + c] = bb[(size_t)6 * k + c];
+      h_item[j] = k;
+      h_src[j] = src_h[k];
+      h_dst[j] = dst_h[k];
+    }
+    const int64_t ntiles = make_lat_boxes(boxes.data(), m, hb, tile_w);
+    int64_t base = 0;
+    for (int32_t j = 0; j < m; ++j) {
+      hb[j].dbase = base;
+      base += box_volume(&boxes[(size_t)j * 6], 0);
+    }
+    ORSP_CUDA(cudaMemcpyAsync(g->blat_tab_d, g->blat_tab_h, (size_t)m * sizeof(LatBox) + (size_t)m * 12,
+                              cudaMemcpyHostToDevice, st));
+    const LatBox *db = (const LatBox *)g->blat_tab_d;
+    const int32_t *d_item = (const int32_t *)(db + m);
+    const int32_t *d_src = d_item + m;
+    const int32_t *d_dst = d_src + m;
+    rc = reserve_lattice_ws(g, ntiles);
+    if (rc) return rc;
+    LatOptions opt;
+    opt.tile_w = tile_w;
+    opt.private_dist = true;
+    opt.private_count = cells;
+    opt.copy_ctl = false;
+    rc = run_lattice_boxes(g, cost_d, m, d_src, nullptr, m, boxes.data(), db, g->blat_dist, st, &opt);
+    if (rc) return rc;
+    LatBt bt{};
+    bt.cost = cost_d;
+    bt.rptr = g->rptr;
+    bt.rsrc = g->rsrc;
+    bt.reid = g->reid;
+    bt.dist = g->blat_dist;
+    bt.nx = g->nx;
+    bt.ny = g->ny;
+    bt.boxes = db;
+    bt.item = d_item;
+    bt.src = d_src;
+    bt.dst = d_dst;
+    bt.path_nodes = path_nodes_d;
+    bt.path_edges = path_edges_d;
+    bt.path_len = path_len_d;
+    bt.path_cap = path_cap;
+    bt.search_err = opt.err_d;
+    lat_batch_backtrace_kernel<<<m, 32, 0, st>>>(bt);
+    ORSP_CUDA(cudaGetLastError());
+    ORSP_CUDA(cudaStreamSynchronize(st));
+    a = b;
+  }
+  return ORSP_OK;
+}
+
+// Bucket of a box of v nodes under the graph's plan.
+int plan_bucket(const orsp::Graph *g, int64_t v) {
+  for (int i = 0; i < g->plan_nb - 1; ++i)
+    if (v <= g->plan_max_nodes[i]) return i;
+  return g->plan_nb - 1;
+}
+
+}  // namespace
+
+static int run_batch(orsp_graph *g, const float *cost_d, int32_t K, const int32_t *src_d,
+                     const int32_t *dst_d, const int32_t *bbox_d, int range_mode,
+                     const int32_t *order_d, float delta, int32_t *path_nodes_d,
+                     int32_t *path_edges_d, int32_t path_cap, int32_t *path_len_d,
+                     uintptr_t stream) {
+  if (!g || !cost_d || K < 0 || (K > 0 && (!src_d || !dst_d || !bbox_d || !path_nodes_d ||
+                                           !path_len_d)) || path_cap <= 0) {
+    set_error("batch search: NULL argument or path_cap <= 0");
+    return ORSP_ERR_ARG;
+  }
+  if (!range_mode && g->nx <= 0) { set_error("batch_bbox: graph was created without lattice dims"); return ORSP_ERR_ARG; }
+  if (!(delta >= 0.0f) || !(delta < 3.0e38f)) { set_error("delta must be finite and >= 0 (0: chosen on the device)"); return ORSP_ERR_ARG; }
+  if (K == 0) return ORSP_OK;
+  ORSP_CUDA(cudaSetDevice(g->device));
+  cudaStream_t st = (cudaStream_t)stream;
+
+  // ROI sizes are needed on the host to size the work.
+  const int per = range_mode ? 2 : 6;
+  std::vector<int32_t> bb((size_t)per * K);
+  ORSP_CUDA(cudaMemcpyAsync(bb.data(), bbox_d, bb.size() * 4, cudaMemcpyDeviceToHost, st));
+  std::vector<int32_t> ord(K);
+  if (order_d) ORSP_CUDA(cudaMemcpyAsync(ord.data(), order_d, (size_t)K * 4, cudaMemcpyDeviceToHost, st));
+  ORSP_CUDA(cudaStreamSynchronize(st));
+  for (int32_t k = 0; k < K; ++k) {
+    const int32_t *b = &bb[(size_t)per * k];
+    if (range_mode) {
+      if (b[0] < 0 || b[1] > g->N || b[1] <= b[0]) {
+        set_error("batch_ranges: node range outside the graph or empty");
+        return ORSP_ERR_ARG;
+      }
+    } else if (b[0] < 0 || b[2] < 0 || b[4] < 0 || b[1] >= g->nx || b[3] >= g->ny || b[5] >= g->nz ||
+               b[1] < b[0] || b[3] < b[2] || b[5] < b[4]) {
+      set_error("batch_bbox: box outside the lattice or empty");
+      return ORSP_ERR_ARG;
+    }
+  }
+  if (order_d) {
+    std::vector<char> seen(K, 0);
+    for (int32_t k = 0; k < K; ++k) {
+      if (ord[k] < 0 || ord[k] >= K || seen[ord[k]]) {
+        set_error("batch_bbox: order must be a permutation of 0..K-1");
+        return ORSP_ERR_ARG;
+      }
+      seen[ord[k]] = 1;
+    }
+  } else {
+    for (int32_t k = 0; k < K; ++k) ord[k] = k;
+  }
+  // items per bucket, in the processing order
+  const bool tuned = g->plan_nb > 0 && !range_mode;
+  const int nb = tuned ? g->plan_nb : 1;
+  std::vector<std::vector<int32_t>> bucket(nb);
+  for (int32_t i = 0; i < K; ++i) {
+    const int32_t k = ord[i];
+    bucket[tuned ? plan_bucket(g, box_volume(&bb[(size_t)per * k], range_mode)) : 0].push_back(k);
+  }
+  // Tile-sweep buckets first (one launch per tile width), then every
+  // one-CTA-per-search item in a single launch, each with its bucket's width,
+  // so that searches of all sizes share the GPU.
+  std::vector<int32_t> src_h, dst_h;
+  std::vector<int32_t> cta_items;
+  std::vector<float> delta_k;
+  int cta_ctas = 0;
+  for (int tw : {16, 32}) {
+    std::vector<int32_t> lat_items;
+    for (int i = 0; i < nb; ++i)
+      if (tuned && g->plan_impl[i] == 1 && g->lattice_ok && g->plan_tile[i] == tw)
+        lat_items.insert(lat_items.end(), bucket[i].begin(), bucket[i].end());
+    if (lat_items.empty()) continue;
+    if (src_h.empty()) {
+      src_h.resize(K);
+      dst_h.resize(K);
+      ORSP_CUDA(cudaMemcpyAsync(src_h.data(), src_d, (size_t)K * 4, cudaMemcpyDeviceToHost, st));
+      ORSP_CUDA(cudaMemcpyAsync(dst_h.data(), dst_d, (size_t)K * 4, cudaMemcpyDeviceToHost, st));
+      ORSP_CUDA(cudaStreamSynchronize(st));
+    }
+    int rc = run_batch_lat(g, cost_d, K, lat_items, bb, src_h, dst_h, tw, path_nodes_d, path_edges_d, path_cap,
+                           path_len_d, st);
+    if (rc) return rc;
+  }
+  for (int i = 0; i < nb; ++i) {
+    if (tuned && g->plan_impl[i] == 1 && g->lattice_ok) continue;
+    if (bucket[i].empty()) continue;
+    if (tuned) {
+      if (delta_k.empty()) delta_k.assign(K, 0.0f);
+      for (int32_t k : bucket[i]) delta_k[k] = g->plan_delta[i];
+      cta_ctas = std::max(cta_ctas, g->plan_ctas[i]);
+    }
+    cta_items.insert(cta_items.end(), bucket[i].begin(), bucket[i].end());
+  }
+  if (!cta_items.empty()) {
+    // processing order of the caller, across buckets
+    if (tuned) {
+      std::vector<int32_t> pos(K);
+      for (int32_t i = 0; i < K; ++i) pos[ord[i]] = i;
+      std::stable_sort(cta_items.begin(), cta_items.end(), [&](int32_t x, int32_t y) { return pos[x] < pos[y]; });
+    }
+    const int ctas = cta_ctas > 0 ? cta_ctas : std::max(1, env_int("ORSP_BATCH_CTAS_PER_SM", 2));
+    int rc = run_batch_cta(g, cost_d, K, cta_items, src_d, dst_d, bbox_d, bb, range_mode, delta, delta_k, ctas,
+                           path_nodes_d, path_edges_d, path_cap, path_len_d, st);
+    if (rc) return rc;
   }
   ORSP_CUDA(cudaStreamSynchronize(st));
+  return ORSP_OK;
+}
+
+extern "C" int orsp_batch_set_plan(orsp_graph *g, int32_t nb, const int64_t *max_nodes, const int32_t *impl,
+                                   const float *delta, const int32_t *tile_w, const int32_t *ctas_per_sm) {
+  if (!g || nb < 0 || nb > 8) { set_error("batch_set_plan: 0..8 buckets"); return ORSP_ERR_ARG; }
+  if (nb > 0 && (!max_nodes || !impl || !delta || !tile_w || !ctas_per_sm)) {
+    set_error("batch_set_plan: NULL array");
+    return ORSP_ERR_ARG;
+  }
+  for (int i = 0; i < nb; ++i) {
+    if (i > 0 && max_nodes[i] <= max_nodes[i - 1]) { set_error("batch_set_plan: max_nodes must increase"); return ORSP_ERR_ARG; }
+    if (impl[i] != 0 && impl[i] != 1) { set_error("batch_set_plan: impl must be 0 or 1"); return ORSP_ERR_ARG; }
+    if (!(delta[i] >= 0.0f) || !(delta[i] < 3.0e38f)) { set_error("batch_set_plan: delta must be finite and >= 0"); return ORSP_ERR_ARG; }
+    if (impl[i] == 1 && tile_w[i] != 16 && tile_w[i] != 32) { set_error("batch_set_plan: tile width must be 16 or 32"); return ORSP_ERR_ARG; }
+    if (ctas_per_sm[i] < 0 || ctas_per_sm[i] > 8) { set_error("batch_set_plan: ctas_per_sm must be 0..8"); return ORSP_ERR_ARG; }
+  }
+  g->plan_nb = nb;
+  for (int i = 0; i < nb; ++i) {
+    g->plan_max_nodes[i] = max_nodes[i];
+    g->plan_impl[i] = impl[i];
+    g->plan_delta[i] = delta[i];
+    g->plan_tile[i] = impl[i] == 1 ? tile_w[i] : 16;
+    g->plan_ctas[i] = ctas_per_sm[i];
+  }
   return ORSP_OK;
 }
 

@@ -176,6 +176,10 @@ extern "C" int orsp_graph_destroy(orsp_graph *g) {
   cudaFree(g->scratch);
   cudaFree(g->auto_delta);
   cudaFree(g->route_ws);
+  cudaFree(g->batch_idx);
+  cudaFree(g->blat_dist);
+  cudaFree(g->blat_tab_d);
+  if (g->blat_tab_h) cudaFreeHost(g->blat_tab_h);
   cudaFree(g->route_tab_d);
   if (g->route_tab_h) cudaFreeHost(g->route_tab_h);
   cudaFree(g->box_g2r);

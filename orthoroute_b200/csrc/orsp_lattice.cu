@@ -51,7 +51,8 @@ using orsp::LatBox;
 struct LatParams {
   int32_t nx, ny, nz;
   int32_t nbox;
-  const LatBox *boxes;                     // searched boxes (pairwise disjoint)
+  int32_t seed_per_box;                    // seed i starts box i (boxes with their own distances)
+  const LatBox *boxes;                     // searched boxes (disjoint unless each has its own distances)
   const float4 *w4;                        // in-edge weights per node
   uint32_t *dist;
   int32_t *list0, *list1;
@@ -126,7 +127,15 @@ __device__ __forceinline__ LatBox load_box(const LatParams &p, int b) {
   B.ntx = __ldg(q + 6);
   B.nty = __ldg(q + 7);
   B.tile0 = __ldg(q + 8);
+  B.dbase = __ldg((const long long *)(p.boxes + b) + 5);
   return B;
+}
+
+// Index of cell (x, y, z) of box B in the distance array.
+__device__ __forceinline__ int64_t dist_index(const LatParams &p, const LatBox &B, int32_t x, int32_t y, int32_t z) {
+  if (B.dbase < 0) return ((int64_t)z * p.ny + y) * p.nx + x;
+  const int64_t bw = B.x1 - B.x0 + 1, bh = B.y1 - B.y0 + 1;
+  return B.dbase + ((int64_t)(z - B.z0) * bh + (y - B.y0)) * bw + (x - B.x0);
 }
 
 // Box of tile t: the last box whose first tile is <= t.
@@ -170,24 +179,41 @@ __global__ void lattice_seed_kernel(LatParams p, int32_t nseeds, const int32_t *
     const int32_t z = s / plane, r = s - z * plane, y = r / p.nx, x = r - y * p.nx;
     int bi = -1;
     LatBox B;
-    for (int b = 0; b < p.nbox && bi < 0; ++b) {
-      B = load_box(p, b);
-      if (x >= B.x0 && x <= B.x1 && y >= B.y0 && y <= B.y1 && z >= B.z0 && z <= B.z1) bi = b;
+    if (p.seed_per_box) {
+      if (i < p.nbox) {
+        B = load_box(p, i);
+        if (x >= B.x0 && x <= B.x1 && y >= B.y0 && y <= B.y1 && z >= B.z0 && z <= B.z1) bi = i;
+      }
+    } else {
+      for (int b = 0; b < p.nbox && bi < 0; ++b) {
+        B = load_box(p, b);
+        if (x >= B.x0 && x <= B.x1 && y >= B.y0 && y <= B.y1 && z >= B.z0 && z <= B.z1) bi = b;
+      }
     }
     if (bi < 0) continue;
     const float c0 = seed_cost ? seed_cost[i] : 0.0f;
     if (!(c0 >= 0.0f) || !(c0 < __int_as_float(0x7f800000))) continue;
-    atomicMin(&p.dist[s], f_bits(c0));
+    atomicMin(&p.dist[dist_index(p, B, x, y, z)], f_bits(c0));
+    // The seed's tile and its neighbours in the box: a tile visit publishes
+    // only cells it improved, and a seed is set before any visit, so a seed
+    // on a tile edge reaches the next tile through that tile's halo only.
     const int t = tile_of<TX, TY>(B, x, y);
-    if (p.qslot) {
-      if (atomicCAS(&p.tstate[t], 0, 1) == 0) {
-        atomicAdd(&c->pending, 1);
-        const unsigned k = atomicAdd(&c->tail, 1u);
-        atomicExch(&p.qslot[k % p.qcap], t);
+    const int lt = t - B.tile0, tx = lt % B.ntx, ty = lt / B.ntx;
+    const int nb[5] = {t, tx > 0 ? t - 1 : -1, tx < B.ntx - 1 ? t + 1 : -1, ty > 0 ? t - B.ntx : -1,
+                       ty < B.nty - 1 ? t + B.ntx : -1};
+    for (int j = 0; j < 5; ++j) {
+      const int q = nb[j];
+      if (q < 0) continue;
+      if (p.qslot) {
+        if (atomicCAS(&p.tstate[q], 0, 1) == 0) {
+          atomicAdd(&c->pending, 1);
+          const unsigned k = atomicAdd(&c->tail, 1u);
+          atomicExch(&p.qslot[k % p.qcap], q);
+        }
+      } else if (atomicMax(&p.stamp[q], 1u) < 1u) {
+        const unsigned k = atomicAdd(&c->lcnt[0], 1u);
+        p.list0[k] = q;
       }
-    } else if (atomicMax(&p.stamp[t], 1u) < 1u) {
-      const unsigned k = atomicAdd(&c->lcnt[0], 1u);
-      p.list0[k] = t;
     }
   }
 }
@@ -310,11 +336,13 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
   for (int c = threadIdx.x; c < th * tw; c += blockDim.x) {
     const int yy = c / tw + 1, xx = c - (yy - 1) * tw + 1;
     const int64_t n0 = (int64_t)B.z0 * nxy + col0 + (int64_t)(yy - 1) * p.nx + (xx - 1);
+    const int64_t d0 = dist_index(p, B, X0 + xx - 1, Y0 + yy - 1, B.z0);
+    const int64_t dz = B.dbase < 0 ? nxy : (int64_t)(B.x1 - B.x0 + 1) * (B.y1 - B.y0 + 1);
     const int s0 = yy * SX + xx, w0 = (yy - 1) * WSX + (xx - 1);
 #pragma unroll 6
     for (int z = 0; z < nzb; ++z) {
       const int64_t node = n0 + z * nxy;
-      const float dv = bits_f(__ldcg(&p.dist[node]));
+      const float dv = bits_f(__ldcg(&p.dist[d0 + z * dz]));
       const float4 wv = __ldg(&p.w4[node]);
       sd[z * PS + s0] = dv;
       orig[z * WPS + w0] = dv;
@@ -343,7 +371,7 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
       const int32_t gx = X0 + xx - 1, gy = Y0 + yy - 1;
       float v = INF_F;
       if (gx >= B.x0 && gx <= B.x1 && gy >= B.y0 && gy <= B.y1)
-        v = bits_f(__ldcg(&p.dist[(int64_t)(B.z0 + z) * nxy + (int64_t)gy * p.nx + gx]));
+        v = bits_f(__ldcg(&p.dist[dist_index(p, B, gx, gy, B.z0 + z)]));
       sd[z * PS + yy * SX + xx] = v;
     }
   }
@@ -407,9 +435,8 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
     const int yy = rem / tw + 1, xx = rem % tw + 1;
     const float v = sd[z * PS + yy * SX + xx];
     const int gz = B.z0 + z;
-    const int64_t node = (int64_t)gz * nxy + col0 + (int64_t)(yy - 1) * p.nx + (xx - 1);
     if (v < orig[z * WPS + (yy - 1) * WSX + (xx - 1)]) {
-      __stcg(&p.dist[node], f_bits(v));
+      __stcg(&p.dist[dist_index(p, B, X0 + xx - 1, Y0 + yy - 1, gz)], f_bits(v));
       const int ax = p.axis[gz];
       if (ax == 1) {
         if (xx == 1) s_act[0] = 1;
@@ -779,8 +806,8 @@ int lattice_tile_w() { return env_u64("ORSP_LAT_TILE", 16) == 32 ? 32 : 16; }
 
 int reserve_lattice_ws(Graph *g, int64_t ntiles) { return grow_ws(g, ws_layout(g, ntiles).total); }
 
-int64_t make_lat_boxes(const int32_t *boxes_h, int32_t nbox, LatBox *out) {
-  const int TX = lattice_tile_w(), TY = 16;
+int64_t make_lat_boxes(const int32_t *boxes_h, int32_t nbox, LatBox *out, int tile_w) {
+  const int TX = tile_w ? tile_w : lattice_tile_w(), TY = 16;
   int64_t t0 = 0;
   for (int32_t i = 0; i < nbox; ++i) {
     const int32_t *b = boxes_h + 6 * (int64_t)i;
@@ -794,6 +821,8 @@ int64_t make_lat_boxes(const int32_t *boxes_h, int32_t nbox, LatBox *out) {
     B.ntx = (b[1] - b[0] + TX) / TX;
     B.nty = (b[3] - b[2] + TY) / TY;
     B.tile0 = (int32_t)t0;
+    B.pad = 0;
+    B.dbase = -1;
     t0 += (int64_t)B.ntx * B.nty;
   }
   return t0;
@@ -808,7 +837,10 @@ int run_lattice_boxes(Graph *g, const float *cost_d, int32_t nseeds, const int32
                       const float *seed_cost_d, int32_t nbox, const int32_t *boxes_h, const LatBox *lboxes_d,
                       uint32_t *dist, cudaStream_t st, LatOptions *opt) {
   const int64_t N = g->N;
-  const int TX = lattice_tile_w(), TY = 16;
+  const int TX = (opt && opt->tile_w) ? opt->tile_w : lattice_tile_w(), TY = 16;
+  if (TX != 16 && TX != 32) { set_error("lattice search: tile width must be 16 or 32"); return ORSP_ERR_ARG; }
+  const bool priv = opt && opt->private_dist;
+  int64_t vol_sum = 0;
   int64_t ntiles = 0;
   int nzb = 1;
   bool whole = false;
@@ -816,10 +848,13 @@ int run_lattice_boxes(Graph *g, const float *cost_d, int32_t nseeds, const int32
     const int32_t *b = boxes_h + 6 * (int64_t)i;
     ntiles += (int64_t)((b[1] - b[0] + TX) / TX) * ((b[3] - b[2] + TY) / TY);
     nzb = std::max(nzb, b[5] - b[4] + 1);
+    vol_sum += (int64_t)(b[1] - b[0] + 1) * (b[3] - b[2] + 1) * (b[5] - b[4] + 1);
     whole = whole || (b[0] == 0 && b[1] == g->nx - 1 && b[2] == 0 && b[3] == g->ny - 1 && b[4] == 0 &&
                       b[5] == g->nz - 1);
   }
-  if (whole) {
+  // overlapping boxes (own distances) may hold more cells than the lattice:
+  // then one gather of every node is cheaper than one per box
+  if (whole || (priv && vol_sum >= N)) {
     gather_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 148 * 32), 256, 0, st>>>(
         g->slot_eid, cost_d, (float4 *)g->wslot, N);
     ORSP_CUDA(cudaGetLastError());
@@ -833,7 +868,11 @@ int run_lattice_boxes(Graph *g, const float *cost_d, int32_t nseeds, const int32
       ORSP_CUDA(cudaGetLastError());
     }
   }
-  if (opt && opt->fill_box_only && !whole) {
+  if (priv) {
+    fill_kernel<<<(int)std::min<int64_t>((opt->private_count + 255) / 256, 148 * 32), 256, 0, st>>>(
+        dist, opt->private_count, ORSP_INF_BITS);
+    ORSP_CUDA(cudaGetLastError());
+  } else if (opt && opt->fill_box_only && !whole) {
     for (int32_t i = 0; i < nbox; ++i) {
       const int32_t *b = boxes_h + 6 * (int64_t)i;
       const int32_t bw = b[1] - b[0] + 1, bh = b[3] - b[2] + 1;
@@ -851,6 +890,7 @@ int run_lattice_boxes(Graph *g, const float *cost_d, int32_t nseeds, const int32
   p.ny = g->ny;
   p.nz = g->nz;
   p.nbox = nbox;
+  p.seed_per_box = priv ? 1 : 0;
   p.boxes = lboxes_d;
   p.w4 = (const float4 *)g->wslot;
   p.dist = dist;

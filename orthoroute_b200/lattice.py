@@ -320,3 +320,22 @@ def random_boxes(lat: Lattice, count: int, seed: int, lo=(20, 20, 4), hi=(400, 4
     src = lat.node(sx, sy, sz).astype(np.int32)
     dst = lat.node(tx, ty, tz).astype(np.int32)
     return boxes, src, dst
+
+
+def box_edge_count(lat: Lattice, boxes: np.ndarray) -> np.ndarray:
+    """Directed edges with both ends inside each box (the graph a box-ROI
+    search runs on), for lattices with adjacent-layer vias."""
+    if lat.meta.get("vias", "adjacent") != "adjacent" or lat.meta.get("duplicate_vias", False):
+        raise ValueError("box_edge_count: adjacent, single vias only")
+    dirs = layer_directions(lat.nz)
+    if lat.meta.get("planar", "all") == "inner":
+        dirs = [d if 0 < z < lat.nz - 1 else "" for z, d in enumerate(dirs)]
+    b = np.asarray(boxes, dtype=np.int64)
+    bw, bh, bd = b[:, 1] - b[:, 0] + 1, b[:, 3] - b[:, 2] + 1, b[:, 5] - b[:, 4] + 1
+    has_h = np.array(["h" in d for d in dirs], dtype=np.int64)
+    has_v = np.array(["v" in d for d in dirs], dtype=np.int64)
+    ch = np.concatenate([[0], np.cumsum(has_h)])
+    cv = np.concatenate([[0], np.cumsum(has_v)])
+    nh = ch[b[:, 5] + 1] - ch[b[:, 4]]
+    nv = cv[b[:, 5] + 1] - cv[b[:, 4]]
+    return 2 * (nh * (bw - 1) * bh + nv * bw * (bh - 1) + bw * bh * (bd - 1))

@@ -181,6 +181,23 @@ class DeviceGraph:
         check(_load_lib().orsp_roi_from_bitmap(self._h, ptr(bm), ptr(g2r), _stream()), "orsp_roi_from_bitmap")
         return g2r
 
+    def set_batch_plan(self, buckets=None):
+        """Tuning plan of batch_bbox: a list of dicts {max_nodes, impl (0: one
+        CTA per search, 1: tile sweeps), delta (0: the call's), tile_w,
+        ctas_per_sm (0: default)}, by increasing max_nodes; None or [] restores
+        the default.  The paths do not depend on the plan."""
+        buckets = buckets or []
+        n = len(buckets)
+        mx = np.array([int(b["max_nodes"]) for b in buckets], dtype=np.int64)
+        im = np.array([int(b.get("impl", 0)) for b in buckets], dtype=np.int32)
+        de = np.array([float(b.get("delta", 0.0)) for b in buckets], dtype=np.float32)
+        tw = np.array([int(b.get("tile_w", 16)) for b in buckets], dtype=np.int32)
+        cp = np.array([int(b.get("ctas_per_sm", 0)) for b in buckets], dtype=np.int32)
+        check(_lib.load().orsp_batch_set_plan(self._h, n, ptr(mx) if n else None, ptr(im) if n else None,
+                                              ptr(de) if n else None, ptr(tw) if n else None,
+                                              ptr(cp) if n else None), "orsp_batch_set_plan")
+        self.batch_plan = list(buckets)
+
     def batch_bbox(self, cost: torch.Tensor, src: torch.Tensor, dst: torch.Tensor, bbox: torch.Tensor,
                    order: Optional[torch.Tensor] = None, delta: Optional[float] = None,
                    path_cap: int = 4096, with_edges: bool = True):

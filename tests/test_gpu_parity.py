@@ -182,10 +182,25 @@ def test_sssp_edge_cases():
             dg.sssp(wt, 0, 1, delta=bad)
 
 
-def test_batch_bbox_matches_oracle():
+BATCH_PLANS = {
+    "default": None,
+    "sweeps16": [{"max_nodes": 1 << 40, "impl": 1, "tile_w": 16}],
+    "sweeps32": [{"max_nodes": 1 << 40, "impl": 1, "tile_w": 32}],
+    "mixed": [{"max_nodes": 800, "impl": 0, "delta": 0.75, "ctas_per_sm": 1},
+              {"max_nodes": 6000, "impl": 0, "delta": 4.0, "ctas_per_sm": 3},
+              {"max_nodes": 1 << 40, "impl": 1, "tile_w": 16}],
+}
+
+
+@pytest.mark.parametrize("plan", list(BATCH_PLANS))
+def test_batch_bbox_matches_oracle(plan):
+    """Batched box searches under every tuning plan (one CTA per search, tile
+    sweeps with a distance slice per box, mixed by box size) equal the oracle:
+    every path and every edge list."""
     lat = build_lattice(90, 70, 6)
     w = uniform_weights(lat, seed=5, blocked_frac=0.03)
     dg = DeviceGraph.from_lattice(lat)
+    dg.set_batch_plan(BATCH_PLANS[plan])
     boxes, src, dst = random_boxes(lat, 300, seed=9, lo=(2, 2, 1), hi=(90, 70, 6))
     # boxes larger than the shared-memory distance array (24K nodes) take the
     # global-memory path of the kernel
@@ -433,3 +448,65 @@ def test_sssp_box_matches_box_roi_and_oracle(impl, monkeypatch):
     for bad in [(0, 75, 0, 10, 0, 5), (5, 4, 0, 10, 0, 5), (0, 10, -1, 10, 0, 5), (0, 10, 0, 10, 0, 6)]:
         with pytest.raises(_lib.OrspError):
             dg.sssp_box(wt, 0, 5, bad)
+
+
+def test_batch_plans_agree_on_status_codes():
+    """The per-search status of batch_bbox is the same under both
+    implementations: source outside its box (-1), unreachable target (0),
+    src == dst (one node), and ordinary paths."""
+    lat = build_lattice(40, 30, 4)
+    w = uniform_weights(lat, seed=3, blocked_frac=0.0)
+    w2 = w.copy()
+    w2[lat.indices == lat.node(20, 15, 2)] = np.inf  # node (20,15,2) cannot be entered
+    dg = DeviceGraph.from_lattice(lat)
+    boxes = np.array([[0, 9, 0, 9, 0, 3], [5, 30, 5, 25, 0, 3], [0, 39, 0, 29, 0, 3], [2, 12, 2, 12, 1, 2]],
+                     np.int32)
+    src = np.array([lat.node(20, 20, 0), lat.node(6, 6, 0), lat.node(1, 1, 3), lat.node(5, 5, 1)], np.int32)
+    dst = np.array([lat.node(3, 3, 0), lat.node(20, 15, 2), lat.node(38, 28, 0), lat.node(5, 5, 1)], np.int32)
+    out = {}
+    for name in ("default", "sweeps16"):
+        dg.set_batch_plan(BATCH_PLANS[name])
+        nodes, edges, lens = dg.batch_bbox(cuda(w2), cuda(src), cuda(dst), cuda(boxes), path_cap=512)
+        out[name] = (lens.cpu().numpy(), nodes.cpu().numpy())
+    la, na = out["default"]
+    lb, nb = out["sweeps16"]
+    assert la.tolist() == lb.tolist()
+    assert la[0] == -1 and la[1] == 0 and la[3] == 1 and la[2] >= 2
+    assert np.array_equal(na[2, : la[2]], nb[2, : lb[2]])
+
+
+@pytest.mark.parametrize("impl", ["lattice16", "lattice32", "lattice16-rounds"])
+def test_seed_on_tile_edge_single_layer_box(impl, monkeypatch):
+    """A seed on a tile edge must reach the next tile even when no other cell
+    of that edge improves: single-layer boxes (one routing axis), source on
+    the first row or column of a tile, target in the neighbouring tile."""
+    monkeypatch.setenv("ORSP_SSSP_IMPL", "auto")
+    monkeypatch.setenv("ORSP_LAT_TILE", "32" if impl == "lattice32" else "16")
+    monkeypatch.setenv("ORSP_LAT_ASYNC", "0" if impl.endswith("rounds") else "1")
+    lat = build_lattice(90, 70, 6)
+    w = uniform_weights(lat, seed=5, blocked_frac=0.0)
+    dg = DeviceGraph.from_lattice(lat)
+    wt = cuda(w)
+    tw = 32 if impl == "lattice32" else 16
+    # V layer (z=2): y-runs; H layer (z=1): x-runs
+    cases = [((62, 63, 50, 68, 2, 2), (62, 66, 2), (62, 51, 2)),
+             ((10, 11, 3, 60, 2, 2), (10, 3 + 16, 2), (10, 4, 2)),
+             ((5, 5 + tw + 8, 7, 8, 1, 1), (5 + tw, 7, 1), (6, 7, 1)),
+             ((5, 5 + tw + 8, 7, 8, 1, 1), (5 + tw - 1, 8, 1), (5 + tw + 7, 8, 1))]
+    nxy = lat.nx * lat.ny
+    for box, s3, d3 in cases:
+        s, d = int(lat.node(*s3)), int(lat.node(*d3))
+        g2r = np.full(lat.N, -1, np.int32)
+        x0, x1, y0, y1, z0, z1 = box
+        zz, yy, xx = np.meshgrid(np.arange(z0, z1 + 1), np.arange(y0, y1 + 1), np.arange(x0, x1 + 1), indexing="ij")
+        inside = (zz * nxy + yy * lat.nx + xx).ravel()
+        g2r[inside] = np.arange(inside.size, dtype=np.int32)
+        ref, *_ = O.dijkstra(lat.indptr, lat.indices, w, [s], dst=d, roi_map=g2r)
+        assert len(ref) > 1
+        st, p, _ = dg.sssp_box(wt, s, d, box)
+        assert st == _lib.ORSP_OK and p.cpu().tolist() == ref.tolist(), f"{box} {s3}->{d3}"
+        dg.set_batch_plan([{"max_nodes": 1 << 40, "impl": 1, "tile_w": tw}])
+        nodes, _, lens = dg.batch_bbox(wt, cuda(np.array([s], np.int32)), cuda(np.array([d], np.int32)),
+                                       cuda(np.array([box], np.int32)), path_cap=512)
+        L = int(lens[0])
+        assert L == len(ref) and nodes[0, :L].cpu().tolist() == ref.tolist()
