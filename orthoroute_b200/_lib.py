@@ -52,6 +52,15 @@ _SIGS = {
     "orsp_sssp_box": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _f32, _P, _P, _i32,
                                      ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
     "orsp_batch_set_plan": (ctypes.c_int, [_P, _i32, _P, _P, _P, _P, _P]),
+    "orsp_warm_conv3d": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _i32, _i32, _i32, _i32, _i32, _i32, _u]),
+    "orsp_warm_wgrad": (ctypes.c_int, [_P, _P, _P, _P, _P, _i32, _i32, _i32, _i32, _i32, _u]),
+    "orsp_warm_pool": (ctypes.c_int, [_P, _P, _i32, _i32, _i32, _i32, _u]),
+    "orsp_warm_spread": (ctypes.c_int, [_P, _P, _i32, _i32, _i32, _i32, _f32, _u]),
+    "orsp_warm_gather4": (ctypes.c_int, [_P, _P, _i32, _i32, _i32, _i32, _u]),
+    "orsp_warm_add": (ctypes.c_int, [_P, _P, _P, _i64, _u]),
+    "orsp_warm_mse": (ctypes.c_int, [_P, _P, _P, _P, _P, _i64, _i32, _i32, _f32, _u]),
+    "orsp_warm_adam": (ctypes.c_int, [_P, _P, _P, _P, _i64, _f32, _f32, _f32, _f32, _f32, _u]),
+    "orsp_warm_pack_weights": (ctypes.c_int, [_P, _P, _i32, _i32, _i32, _u]),
     "orsp_route_nets": (ctypes.c_int, [_P, _i32, _P, _P, _P, _i32, _P, _i32, _P, _P, _P, _i32, _P, _P, _P, _P, _P,
                                        _P, _P, _f32, _f32, _f32, _f32, _i32, _u]),
     "orsp_sssp_multi": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _P, _P, _f32, _P, _i32,

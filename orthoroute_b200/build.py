@@ -26,6 +26,7 @@ SOURCES = [
     "orsp_lattice.cu",
     "orsp_via.cu",
     "orsp_route.cu",
+    "orsp_warm.cu",
 ]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -1,0 +1,313 @@
+"""Learned history warm start for PathFinder.
+
+A small 3D convolutional net predicts, from the pins and the airwires of a
+board, the history cost field PathFinder ends with; routing then starts from
+that history instead of zero.  Plain zero-history PathFinder stays the
+fallback and the judge: a warm run counts only when it reaches zero overuse,
+and if it has not converged within 1.5x the plain run's iterations the plain
+run is used.
+
+Network (all layers run by the kernels of orsp_warm.cu, bf16 activations
+[D][H][W][C] with fp32 accumulation): a 4-level U-net over the routing grid,
+32 channels at every level, two 3x3x3 convolutions + ReLU per encoder level,
+2x2 average pooling in x/y between levels (the layer count is small and is
+kept), nearest upsampling + skip addition + one convolution per decoder
+level, and a 3x3x3 head with 16 output channels of which two are used: the
+mean history of a node's planar out-edges and of its via out-edges,
+predicted as log1p(history).
+
+Inputs per cell (16 channels, unused ones zero): pin density on the pin
+layer, blurred pin density, airwire (pin-to-pin segment) crossing density,
+net bounding-box coverage, H-layer flag, V-layer flag, layer position.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, ptr
+from .lattice import Lattice, layer_directions
+
+F_IN = 16   # input channels (padded)
+F_OUT = 16  # head channels (2 used)
+USED = 2
+
+
+def _st() -> int:
+    return int(torch.cuda.current_stream().cuda_stream)
+
+
+# ----------------------------------------------------------------- features
+def _box_blur(a: np.ndarray, r: int) -> np.ndarray:
+    """Mean over a (2r+1)^2 window (edges: smaller window), float32."""
+    c = np.pad(a.astype(np.float64), ((1, 0), (1, 0))).cumsum(0).cumsum(1)
+    H, W = a.shape
+    y0 = np.clip(np.arange(H) - r, 0, H)
+    y1 = np.clip(np.arange(H) + r + 1, 0, H)
+    x0 = np.clip(np.arange(W) - r, 0, W)
+    x1 = np.clip(np.arange(W) + r + 1, 0, W)
+    s = c[y1][:, x1] - c[y0][:, x1] - c[y1][:, x0] + c[y0][:, x0]
+    n = (y1 - y0)[:, None] * (x1 - x0)[None, :]
+    return (s / n).astype(np.float32)
+
+
+def board_features(lat: Lattice, src: np.ndarray, dst: np.ndarray) -> np.ndarray:
+    """float32 [nz][ny][nx][16] input features of a board (host)."""
+    nx, ny, nz = lat.nx, lat.ny, lat.nz
+    sx, sy, sz = (np.asarray(v) for v in lat.coords(np.asarray(src)))
+    dx, dy, dz = (np.asarray(v) for v in lat.coords(np.asarray(dst)))
+    pins = np.zeros((ny, nx), np.float32)
+    np.add.at(pins, (sy, sx), 1.0)
+    np.add.at(pins, (dy, dx), 1.0)
+    # airwire crossing density: each pin-to-pin segment rasterised at unit steps
+    air = np.zeros((ny, nx), np.float32)
+    for a, b, c, d in zip(sx, sy, dx, dy):
+        n = int(max(abs(int(c) - int(a)), abs(int(d) - int(b)))) + 1
+        xs = np.rint(np.linspace(a, c, n)).astype(np.int64)
+        ys = np.rint(np.linspace(b, d, n)).astype(np.int64)
+        air[ys, xs] += 1.0
+    cov = np.zeros((ny + 1, nx + 1), np.float32)
+    x0, x1 = np.minimum(sx, dx), np.maximum(sx, dx) + 1
+    y0, y1 = np.minimum(sy, dy), np.maximum(sy, dy) + 1
+    np.add.at(cov, (y0, x0), 1.0)
+    np.add.at(cov, (y0, x1), -1.0)
+    np.add.at(cov, (y1, x0), -1.0)
+    np.add.at(cov, (y1, x1), 1.0)
+    cov = cov.cumsum(0).cumsum(1)[:ny, :nx]
+    dirs = layer_directions(nz)
+    f = np.zeros((nz, ny, nx, F_IN), np.float32)
+    pin_layer = int(np.bincount(np.concatenate([sz, dz]).astype(np.int64), minlength=nz).argmax())
+    f[pin_layer, :, :, 0] = pins
+    f[:, :, :, 1] = _box_blur(pins, 4)[None] * 4.0
+    f[:, :, :, 2] = _box_blur(air, 2)[None] * 0.5
+    f[:, :, :, 3] = cov[None] / 64.0
+    for z, d in enumerate(dirs):
+        f[z, :, :, 4] = 1.0 if "h" in d else 0.0
+        f[z, :, :, 5] = 1.0 if "v" in d else 0.0
+        f[z, :, :, 6] = z / max(1, nz - 1)
+    return f
+
+
+def node_targets(lat: Lattice, history: np.ndarray) -> np.ndarray:
+    """float32 [nz][ny][nx][2]: log1p of the mean history of each node's planar
+    and via out-edges (0 where it has none)."""
+    src = lat.edge_src
+    kind = np.asarray(lat.edge_kind)
+    out = np.zeros((lat.N, 2), np.float64)
+    cnt = np.zeros((lat.N, 2), np.float64)
+    np.add.at(out, (src, kind.astype(np.int64)), history.astype(np.float64))
+    np.add.at(cnt, (src, kind.astype(np.int64)), 1.0)
+    mean = np.where(cnt > 0, out / np.maximum(cnt, 1), 0.0)
+    return np.log1p(mean).astype(np.float32).reshape(lat.nz, lat.ny, lat.nx, 2)
+
+
+def history_from_prediction(lat: Lattice, pred: np.ndarray, scale: float = 1.0) -> np.ndarray:
+    """Per-edge history (float32[E]) from node predictions [nz][ny][nx][2]:
+    every out-edge of a node gets expm1 of its kind's channel, times scale."""
+    p = np.expm1(np.maximum(pred.reshape(lat.N, 2).astype(np.float64), 0.0))
+    kind = np.asarray(lat.edge_kind).astype(np.int64)
+    return (p[lat.edge_src, kind] * scale).astype(np.float32)
+
+
+# ----------------------------------------------------------------- the net
+@dataclass
+class Layer:
+    name: str
+    cin: int
+    cout: int
+    relu: bool
+
+
+def architecture(C: int = 32) -> List[Layer]:
+    L = [Layer("e0a", F_IN, C, True), Layer("e0b", C, C, True),
+         Layer("e1a", C, C, True), Layer("e1b", C, C, True),
+         Layer("e2a", C, C, True), Layer("e2b", C, C, True),
+         Layer("e3a", C, C, True), Layer("e3b", C, C, True),
+         Layer("d2", C, C, True), Layer("d1", C, C, True), Layer("d0", C, C, True),
+         Layer("head", C, F_OUT, False)]
+    return L
+
+
+class WarmNet:
+    """The U-net, its fp32 master weights and Adam state, on one GPU."""
+
+    def __init__(self, C: int = 32, device=None, seed: int = 0):
+        self.device = torch.device(device) if device is not None else torch.device("cuda")
+        self.C = C
+        self.layers = architecture(C)
+        g = torch.Generator().manual_seed(seed)
+        self.w: Dict[str, torch.Tensor] = {}
+        self.b: Dict[str, torch.Tensor] = {}
+        for l in self.layers:
+            std = math.sqrt(2.0 / (27 * l.cin)) if l.relu else math.sqrt(1.0 / (27 * l.cin))
+            self.w[l.name] = (torch.randn(27, l.cin, l.cout, generator=g) * std).to(self.device)
+            self.b[l.name] = torch.zeros(l.cout, device=self.device)
+        self.m = {k: torch.zeros_like(v) for k, v in list(self.w.items()) + [("b_" + k, v) for k, v in self.b.items()]}
+        self.v = {k: torch.zeros_like(v) for k, v in self.m.items()}
+        self.t = 0
+        self._packed: Dict[str, torch.Tensor] = {}
+
+    # weights as the conv kernel reads them
+    def _pack(self, name: str, transpose: bool) -> torch.Tensor:
+        l = next(x for x in self.layers if x.name == name)
+        key = name + ("/T" if transpose else "")
+        out = self._packed.get(key)
+        if out is None:
+            out = torch.empty(27 * l.cin * l.cout, dtype=torch.bfloat16, device=self.device)
+            self._packed[key] = out
+        check(_lib.load().orsp_warm_pack_weights(ptr(self.w[name]), ptr(out), l.cin, l.cout, 1 if transpose else 0,
+                                                 _st()), "orsp_warm_pack_weights")
+        return out
+
+    def _conv(self, x, name, D, H, W, out_f32=False):
+        l = next(y for y in self.layers if y.name == name)
+        if out_f32:
+            y = torch.empty(D, H, W, l.cout, dtype=torch.float32, device=self.device)
+            yb, yf = None, y
+        else:
+            y = torch.empty(D, H, W, l.cout, dtype=torch.bfloat16, device=self.device)
+            yb, yf = y, None
+        check(_lib.load().orsp_warm_conv3d(ptr(x), None, ptr(self._packed[name]), ptr(self.b[name]), ptr(yb),
+                                           ptr(yf), D, H, W, l.cin, l.cout, 1 if l.relu else 0, _st()),
+              "orsp_warm_conv3d")
+        return y
+
+    def _pool(self, x, D, H, W):
+        y = torch.empty(D, H // 2, W // 2, x.shape[-1], dtype=torch.bfloat16, device=self.device)
+        check(_lib.load().orsp_warm_pool(ptr(x), ptr(y), D, H, W, x.shape[-1], _st()), "orsp_warm_pool")
+        return y
+
+    def _spread(self, xc, D, H, W, scale):
+        y = torch.empty(D, H, W, xc.shape[-1], dtype=torch.bfloat16, device=self.device)
+        check(_lib.load().orsp_warm_spread(ptr(xc), ptr(y), D, H, W, xc.shape[-1], float(scale), _st()),
+              "orsp_warm_spread")
+        return y
+
+    def _gather4(self, xf, D, H, W):
+        y = torch.empty(D, H // 2, W // 2, xf.shape[-1], dtype=torch.bfloat16, device=self.device)
+        check(_lib.load().orsp_warm_gather4(ptr(xf), ptr(y), D, H, W, xf.shape[-1], _st()), "orsp_warm_gather4")
+        return y
+
+    def _add(self, a, b):
+        y = torch.empty_like(a)
+        check(_lib.load().orsp_warm_add(ptr(a), ptr(b), ptr(y), a.numel(), _st()), "orsp_warm_add")
+        return y
+
+    # -------------------------------------------------------------- forward
+    def forward(self, x: torch.Tensor, keep: bool = False):
+        """x: bf16 [D][H][W][16], H and W multiples of 8.  Returns the fp32
+        head output [D][H][W][16] (and the activations when keep)."""
+        D, H, W = x.shape[:3]
+        if H % 8 or W % 8:
+            raise ValueError("warm net: H and W must be multiples of 8")
+        for l in self.layers:
+            self._pack(l.name, False)
+        a = {"x": x}
+        dims = [(D, H, W), (D, H // 2, W // 2), (D, H // 4, W // 4), (D, H // 8, W // 8)]
+        h = x
+        for lev in range(4):
+            d = dims[lev]
+            if lev > 0:
+                h = self._pool(a[f"e{lev - 1}b"], *dims[lev - 1])
+                a[f"p{lev}"] = h
+            a[f"e{lev}a"] = self._conv(h, f"e{lev}a", *d)
+            a[f"e{lev}b"] = self._conv(a[f"e{lev}a"], f"e{lev}b", *d)
+        h = a["e3b"]
+        for lev in (2, 1, 0):
+            d = dims[lev]
+            up = self._spread(h, *d, 1.0)
+            a[f"m{lev}"] = self._add(up, a[f"e{lev}b"])
+            h = self._conv(a[f"m{lev}"], f"d{lev}", *d)
+            a[f"d{lev}"] = h
+        out = self._conv(h, "head", D, H, W, out_f32=True)
+        return (out, a) if keep else out
+
+    # ------------------------------------------------------------- backward
+    def _conv_back(self, x_in, y_out, dy, name, D, H, W, need_dx=True):
+        """Gradients of one conv layer: accumulates dW, db; returns dx."""
+        l = next(z for z in self.layers if z.name == name)
+        lib = _lib.load()
+        mask = y_out if l.relu else None
+        check(lib.orsp_warm_wgrad(ptr(x_in), ptr(dy), ptr(mask), ptr(self.gw[name]), ptr(self.gb[name]), D, H, W,
+                                  l.cin, l.cout, _st()), "orsp_warm_wgrad")
+        if not need_dx:
+            return None
+        wt = self._pack(name, True)
+        dx = torch.empty(D, H, W, l.cin, dtype=torch.bfloat16, device=self.device)
+        check(lib.orsp_warm_conv3d(ptr(dy), ptr(mask), ptr(wt), None, ptr(dx), None, D, H, W, l.cout, l.cin, 0,
+                                   _st()), "orsp_warm_conv3d")
+        return dx
+
+    def backward(self, a: dict, dout: torch.Tensor):
+        """dout: bf16 gradient of the head output [D][H][W][16].  Fills
+        self.gw / self.gb (fp32)."""
+        self.gw = {k: torch.zeros_like(v) for k, v in self.w.items()}
+        self.gb = {k: torch.zeros_like(v) for k, v in self.b.items()}
+        D, H, W = a["x"].shape[:3]
+        dims = [(D, H, W), (D, H // 2, W // 2), (D, H // 4, W // 4), (D, H // 8, W // 8)]
+        g = self._conv_back(a["d0"], None, dout, "head", *dims[0])
+        skip_g = {}
+        for lev in (0, 1, 2):
+            d = dims[lev]
+            gm = self._conv_back(a[f"m{lev}"], a[f"d{lev}"], g, f"d{lev}", *d)
+            skip_g[lev] = gm  # gradient into e{lev}b through the skip addition
+            # gradient into the coarser level through the upsampling
+            g = self._gather4(gm, *d)
+        # bottleneck and encoder
+        for lev in (3, 2, 1, 0):
+            d = dims[lev]
+            ge_b = g if lev == 3 else self._add(g, skip_g[lev])
+            ge_a = self._conv_back(a[f"e{lev}a"], a[f"e{lev}b"], ge_b, f"e{lev}b", *d)
+            x_in = a["x"] if lev == 0 else a[f"p{lev}"]
+            gx = self._conv_back(x_in, a[f"e{lev}a"], ge_a, f"e{lev}a", *d, need_dx=lev > 0)
+            if lev > 0:
+                g = self._spread(gx, *dims[lev - 1], 0.25)  # adjoint of 2x2 averaging
+
+    def loss_grad(self, out: torch.Tensor, target: torch.Tensor, weight: Optional[torch.Tensor] = None):
+        """MSE over the two used channels; returns (loss tensor [1], dout bf16)."""
+        D, H, W = out.shape[:3]
+        nvox = D * H * W
+        dout = torch.empty(D, H, W, F_OUT, dtype=torch.bfloat16, device=self.device)
+        loss = torch.zeros(1, dtype=torch.float32, device=self.device)
+        check(_lib.load().orsp_warm_mse(ptr(out), ptr(target), ptr(weight), ptr(dout), ptr(loss), nvox, F_OUT, USED,
+                                        1.0 / (nvox * USED), _st()), "orsp_warm_mse")
+        return loss, dout
+
+    def step(self, lr: float = 1e-3, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8, wd: float = 0.0):
+        self.t += 1
+        lr_t = lr * math.sqrt(1 - b2 ** self.t) / (1 - b1 ** self.t)
+        lib = _lib.load()
+        for k in self.w:
+            for p, g, key in ((self.w[k], self.gw[k], k), (self.b[k], self.gb[k], "b_" + k)):
+                check(lib.orsp_warm_adam(ptr(p), ptr(g), ptr(self.m[key]), ptr(self.v[key]), p.numel(), float(lr_t),
+                                         float(b1), float(b2), float(eps), float(wd), _st()), "orsp_warm_adam")
+
+    # ------------------------------------------------------------ utilities
+    def state(self) -> dict:
+        out = {}
+        for k in self.w:
+            out["w_" + k] = self.w[k].cpu().numpy()
+            out["b_" + k] = self.b[k].cpu().numpy()
+        return out
+
+    def load_state(self, st: dict):
+        for k in self.w:
+            self.w[k].copy_(torch.from_numpy(np.asarray(st["w_" + k], np.float32)))
+            self.b[k].copy_(torch.from_numpy(np.asarray(st["b_" + k], np.float32)))
+
+    def predict(self, feats: np.ndarray) -> np.ndarray:
+        """feats float32 [D][H][W][16] (any H, W: padded to multiples of 8 with
+        zeros) -> float32 [D][H][W][2] (log1p history per node and kind)."""
+        D, H, W = feats.shape[:3]
+        Hp, Wp = (H + 7) // 8 * 8, (W + 7) // 8 * 8
+        x = np.zeros((D, Hp, Wp, F_IN), np.float32)
+        x[:, :H, :W] = feats
+        xt = torch.from_numpy(x).to(self.device).to(torch.bfloat16)
+        out = self.forward(xt)
+        return out[:, :H, :W, :USED].cpu().numpy()
