@@ -255,6 +255,26 @@ def route_c3(dev, with_cpu: bool):
     same = rb.overuse_trace() == rs.overuse_trace() and all(
         np.array_equal(x, y) for x, y in zip(rb.paths, rs.paths)) and np.array_equal(rb.edge_usage, rs.edge_usage)
     searches = int(sum(s.nets_searched for s in rb.iterations))
+    # batched + learned warm start (orthoroute_b200/data/warm_history.npz):
+    # features, inference and the history mapping count in its time; the
+    # run gets at most 1.5x the plain iterations, else the plain route is used
+    import dataclasses
+    import math
+
+    import torch
+
+    from orthoroute_b200.warm import load_pretrained, warm_history
+
+    net, scale = load_pretrained(device=dev)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    h0 = warm_history(net, b.lattice, b.src, b.dst, scale)
+    torch.cuda.synchronize(dev)
+    t_pred = time.perf_counter() - t0
+    pf.cfg = dataclasses.replace(cfg, max_iterations=int(math.ceil(1.5 * len(rs.iterations))))
+    rw = pf.route(b.src, b.dst, mode="batched", history_init=h0)
+    pf.cfg = cfg
+    warm_sec = t_pred + rw.seconds + (0.0 if rw.converged else rb.seconds)
     out = {
         "workload": "600x600x18 lattice, 8000 nets between 2x50 connector footprints, bbox+10 ROI, "
                     "per-net live costs, offenders rerouted, disjoint-round order",
@@ -268,6 +288,22 @@ def route_c3(dev, with_cpu: bool):
         "wirelength": rb.wirelength,
         "vias": rb.vias,
         "overuse_trace": [s.over_sum for s in rb.iterations],
+        "warm": {
+            "sec_batched_warm": round(warm_sec, 3),
+            "sec_prediction": round(t_pred, 3),
+            "converged": bool(rw.converged),
+            "fell_back_to_plain": not rw.converged,
+            "iterations": len(rw.iterations),
+            "searches": int(sum(s.nets_searched for s in rw.iterations)),
+            "history_scale": scale,
+            "speedup_vs_plain": round(rs.seconds / warm_sec, 2),
+            "speedup_vs_batched": round(rb.seconds / warm_sec, 2),
+            "wirelength": rw.wirelength,
+            "vias": rw.vias,
+            "wirelength_delta_pct": round(100.0 * (rw.wirelength - rb.wirelength) / max(1, rb.wirelength), 3),
+            "vias_delta_pct": round(100.0 * (rw.vias - rb.vias) / max(1, rb.vias), 3),
+            "overuse_trace": [s.over_sum for s in rw.iterations],
+        },
     }
     if with_cpu:
         # The C oracle of one box search (heap Dijkstra, fp32) on a sample of

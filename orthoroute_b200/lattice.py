@@ -234,7 +234,8 @@ def board_footprints(
     rng = np.random.default_rng(seed)
     pins_per = rows * cols
     if footprints is None:
-        footprints = int(np.ceil(1.1 * 2 * nets / pins_per))
+        # every net joins two different footprints, so at least two
+        footprints = max(2, int(np.ceil(1.1 * 2 * nets / pins_per)))
     if footprints * pins_per < 2 * nets:
         raise ValueError("not enough pins for the nets")
     # non-overlapping placement with a 2-cell keep-out around each footprint

@@ -85,8 +85,8 @@ def board_features(lat: Lattice, src: np.ndarray, dst: np.ndarray) -> np.ndarray
     pin_layer = int(np.bincount(np.concatenate([sz, dz]).astype(np.int64), minlength=nz).argmax())
     f[pin_layer, :, :, 0] = pins
     f[:, :, :, 1] = _box_blur(pins, 4)[None] * 4.0
-    f[:, :, :, 2] = _box_blur(air, 2)[None] * 0.5
-    f[:, :, :, 3] = cov[None] / 64.0
+    f[:, :, :, 2] = _box_blur(air, 2)[None] / 8.0
+    f[:, :, :, 3] = cov[None] / 32.0
     for z, d in enumerate(dirs):
         f[z, :, :, 4] = 1.0 if "h" in d else 0.0
         f[z, :, :, 5] = 1.0 if "v" in d else 0.0
@@ -94,17 +94,23 @@ def board_features(lat: Lattice, src: np.ndarray, dst: np.ndarray) -> np.ndarray
     return f
 
 
-def node_targets(lat: Lattice, history: np.ndarray) -> np.ndarray:
+def node_targets(lat: Lattice, history: np.ndarray, blur: int = 0) -> np.ndarray:
     """float32 [nz][ny][nx][2]: log1p of the mean history of each node's planar
-    and via out-edges (0 where it has none)."""
-    src = lat.edge_src
+    and via out-edges (0 where it has none), optionally averaged over a
+    (2 blur + 1)^2 window in x/y (a smooth congestion map)."""
+    src = lat.edge_src()
     kind = np.asarray(lat.edge_kind)
     out = np.zeros((lat.N, 2), np.float64)
     cnt = np.zeros((lat.N, 2), np.float64)
     np.add.at(out, (src, kind.astype(np.int64)), history.astype(np.float64))
     np.add.at(cnt, (src, kind.astype(np.int64)), 1.0)
     mean = np.where(cnt > 0, out / np.maximum(cnt, 1), 0.0)
-    return np.log1p(mean).astype(np.float32).reshape(lat.nz, lat.ny, lat.nx, 2)
+    t = np.log1p(mean).astype(np.float32).reshape(lat.nz, lat.ny, lat.nx, 2)
+    if blur > 0:
+        for z in range(lat.nz):
+            for c in range(2):
+                t[z, :, :, c] = _box_blur(t[z, :, :, c], blur)
+    return t
 
 
 def history_from_prediction(lat: Lattice, pred: np.ndarray, scale: float = 1.0) -> np.ndarray:
@@ -112,7 +118,7 @@ def history_from_prediction(lat: Lattice, pred: np.ndarray, scale: float = 1.0) 
     every out-edge of a node gets expm1 of its kind's channel, times scale."""
     p = np.expm1(np.maximum(pred.reshape(lat.N, 2).astype(np.float64), 0.0))
     kind = np.asarray(lat.edge_kind).astype(np.int64)
-    return (p[lat.edge_src, kind] * scale).astype(np.float32)
+    return (p[lat.edge_src(), kind] * scale).astype(np.float32)
 
 
 # ----------------------------------------------------------------- the net
@@ -311,3 +317,21 @@ class WarmNet:
         xt = torch.from_numpy(x).to(self.device).to(torch.bfloat16)
         out = self.forward(xt)
         return out[:, :H, :W, :USED].cpu().numpy()
+
+
+DEFAULT_WEIGHTS = __import__("pathlib").Path(__file__).resolve().parent / "data" / "warm_history.npz"
+
+
+def load_pretrained(path=None, device=None) -> Tuple["WarmNet", float]:
+    """The shipped network (trained by orthoroute_b200.warm_train) and its
+    history scale."""
+    st = dict(np.load(path or DEFAULT_WEIGHTS))
+    net = WarmNet(C=32, device=device)
+    net.load_state({k: v.astype(np.float32) for k, v in st.items() if k != "scale"})
+    return net, float(st.get("scale", 1.0))
+
+
+def warm_history(net: "WarmNet", lat: Lattice, src, dst, scale: float) -> np.ndarray:
+    """Initial per-edge history for a board: features -> net -> edges."""
+    pred = net.predict(board_features(lat, np.asarray(src), np.asarray(dst)))
+    return history_from_prediction(lat, pred, scale)

@@ -93,3 +93,27 @@ def test_warm_training_lowers_loss():
         net.step(lr=3e-3)
         losses.append(float(loss))
     assert losses[-1] < 0.5 * losses[0]
+
+
+def test_shipped_warm_start_gains_over_zero_history():
+    """The shipped network (orthoroute_b200/data/warm_history.npz, trained on
+    seeds 2000+) on an unseen 300x300x18 board at the backplane's net density:
+    starting from its predicted history, PathFinder reaches zero overuse with
+    fewer searches than from zero history, at wirelength within 2 %."""
+    from orthoroute_b200.lattice import board_footprints
+    from orthoroute_b200.negotiate import PathFinder
+    from orthoroute_b200.warm import load_pretrained, warm_history
+    from orthoroute_b200.warm_train import route_config
+
+    b = board_footprints(300, 300, 18, 2000, None, seed=77)
+    pf = PathFinder(b.lattice, config=route_config(60))
+    r0 = pf.route(b.src, b.dst, mode="batched")
+    net, scale = load_pretrained()
+    rw = pf.route(b.src, b.dst, mode="batched", history_init=warm_history(net, b.lattice, b.src, b.dst, scale))
+    s0 = sum(s.nets_searched for s in r0.iterations)
+    sw = sum(s.nets_searched for s in rw.iterations)
+    print(f"zero history: {len(r0.iterations)} iterations, {s0} searches; warm: {len(rw.iterations)} iterations, "
+          f"{sw} searches; wirelength {r0.wirelength} -> {rw.wirelength}")
+    assert r0.converged and rw.converged
+    assert sw < s0
+    assert abs(rw.wirelength - r0.wirelength) <= 0.02 * r0.wirelength
