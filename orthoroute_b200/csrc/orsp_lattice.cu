@@ -131,9 +131,13 @@ __device__ __forceinline__ LatBox load_box(const LatParams &p, int b) {
   return B;
 }
 
-// Index of cell (x, y, z) of box B in the distance array.
+// Index of cell (x, y, z) of box B in the distance array: the node id
+// (shared distances) or the box's own slice (PRIV, B.dbase >= 0).  The search
+// kernels are compiled once per mode, so the shared mode carries no slice
+// arithmetic.
+template <bool PRIV>
 __device__ __forceinline__ int64_t dist_index(const LatParams &p, const LatBox &B, int32_t x, int32_t y, int32_t z) {
-  if (B.dbase < 0) return ((int64_t)z * p.ny + y) * p.nx + x;
+  if (!PRIV || B.dbase < 0) return ((int64_t)z * p.ny + y) * p.nx + x;
   const int64_t bw = B.x1 - B.x0 + 1, bh = B.y1 - B.y0 + 1;
   return B.dbase + ((int64_t)(z - B.z0) * bh + (y - B.y0)) * bw + (x - B.x0);
 }
@@ -193,7 +197,8 @@ __global__ void lattice_seed_kernel(LatParams p, int32_t nseeds, const int32_t *
     if (bi < 0) continue;
     const float c0 = seed_cost ? seed_cost[i] : 0.0f;
     if (!(c0 >= 0.0f) || !(c0 < __int_as_float(0x7f800000))) continue;
-    atomicMin(&p.dist[dist_index(p, B, x, y, z)], f_bits(c0));
+    atomicMin(&p.dist[p.seed_per_box ? dist_index<true>(p, B, x, y, z) : dist_index<false>(p, B, x, y, z)],
+              f_bits(c0));
     // The seed's tile and its neighbours in the box: a tile visit publishes
     // only cells it improved, and a seed is set before any visit, so a seed
     // on a tile edge reaches the next tile through that tile's halo only.
@@ -287,7 +292,7 @@ struct LayerLists {
   int box;
 };
 
-template <int TX, int TY>
+template <int TX, int TY, bool PRIV>
 __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *sd, LayerLists &L, int *s_flags,
                                              int *s_act) {
   const int bi = box_of_tile(p, t);
@@ -336,8 +341,8 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
   for (int c = threadIdx.x; c < th * tw; c += blockDim.x) {
     const int yy = c / tw + 1, xx = c - (yy - 1) * tw + 1;
     const int64_t n0 = (int64_t)B.z0 * nxy + col0 + (int64_t)(yy - 1) * p.nx + (xx - 1);
-    const int64_t d0 = dist_index(p, B, X0 + xx - 1, Y0 + yy - 1, B.z0);
-    const int64_t dz = B.dbase < 0 ? nxy : (int64_t)(B.x1 - B.x0 + 1) * (B.y1 - B.y0 + 1);
+    const int64_t d0 = dist_index<PRIV>(p, B, X0 + xx - 1, Y0 + yy - 1, B.z0);
+    const int64_t dz = (!PRIV || B.dbase < 0) ? nxy : (int64_t)(B.x1 - B.x0 + 1) * (B.y1 - B.y0 + 1);
     const int s0 = yy * SX + xx, w0 = (yy - 1) * WSX + (xx - 1);
 #pragma unroll 6
     for (int z = 0; z < nzb; ++z) {
@@ -371,7 +376,7 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
       const int32_t gx = X0 + xx - 1, gy = Y0 + yy - 1;
       float v = INF_F;
       if (gx >= B.x0 && gx <= B.x1 && gy >= B.y0 && gy <= B.y1)
-        v = bits_f(__ldcg(&p.dist[dist_index(p, B, gx, gy, B.z0 + z)]));
+        v = bits_f(__ldcg(&p.dist[dist_index<PRIV>(p, B, gx, gy, B.z0 + z)]));
       sd[z * PS + yy * SX + xx] = v;
     }
   }
@@ -436,7 +441,7 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
     const float v = sd[z * PS + yy * SX + xx];
     const int gz = B.z0 + z;
     if (v < orig[z * WPS + (yy - 1) * WSX + (xx - 1)]) {
-      __stcg(&p.dist[dist_index(p, B, X0 + xx - 1, Y0 + yy - 1, gz)], f_bits(v));
+      __stcg(&p.dist[dist_index<PRIV>(p, B, X0 + xx - 1, Y0 + yy - 1, gz)], f_bits(v));
       const int ax = p.axis[gz];
       if (ax == 1) {
         if (xx == 1) s_act[0] = 1;
@@ -473,7 +478,7 @@ __device__ __forceinline__ int revisit_list(const LatParams &p, int t, const int
   return k;
 }
 
-template <int TX, int TY>
+template <int TX, int TY, bool PRIV>
 __global__ void __launch_bounds__(TX * TY) lattice_tile_kernel(LatParams p) {
   extern __shared__ float sd[];
   __shared__ LayerLists s_layers;
@@ -504,7 +509,7 @@ __global__ void __launch_bounds__(TX * TY) lattice_tile_kernel(LatParams p) {
       __syncthreads();
       if (ti >= (int)n_in) break;
       const int t = __ldcg(&inl[ti]);
-      process_tile<TX, TY>(p, t, sd, s_layers, s_flags, s_act);
+      process_tile<TX, TY, PRIV>(p, t, sd, s_layers, s_flags, s_act);
       if (threadIdx.x == 0) {
         int nb[5];
         const int k = revisit_list(p, t, s_act, nb);
@@ -562,7 +567,7 @@ __device__ bool activate_tile(const LatParams &p, int t) {
   return false;
 }
 
-template <int TX, int TY>
+template <int TX, int TY, bool PRIV>
 __global__ void __launch_bounds__(TX * TY) lattice_async_kernel(LatParams p) {
   extern __shared__ float sd[];
   __shared__ LayerLists s_layers;
@@ -613,7 +618,7 @@ __global__ void __launch_bounds__(TX * TY) lattice_async_kernel(LatParams p) {
     const int t = s_tile;
     __syncthreads();
     if (t < 0) break;
-    process_tile<TX, TY>(p, t, sd, s_layers, s_flags, s_act);
+    process_tile<TX, TY, PRIV>(p, t, sd, s_layers, s_flags, s_act);
     // neighbours are activated by threads 0..3 in parallel, after this
     // tile's distances are visible
     unsigned long long ta = 0;
@@ -714,7 +719,9 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
     orsp::set_error("lattice search: too many layers for the shared-memory tile");
     return ORSP_ERR_ARG;
   }
-  void *kfn = async ? (void *)lattice_async_kernel<TX, TY> : (void *)lattice_tile_kernel<TX, TY>;
+  const bool priv = opt && opt->private_dist;
+  void *kfn = async ? (priv ? (void *)lattice_async_kernel<TX, TY, true> : (void *)lattice_async_kernel<TX, TY, false>)
+                    : (priv ? (void *)lattice_tile_kernel<TX, TY, true> : (void *)lattice_tile_kernel<TX, TY, false>);
   ORSP_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
   ORSP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, TX * TY, smem));
