@@ -238,6 +238,51 @@ ORSP_API int orsp_route_nets(orsp_graph *g, int32_t M, const int32_t *src_h, con
                     float pres_fac, float hist_w, float via_mult, float base_w, int32_t jitter,
                     uintptr_t stream);
 
+/* ---- negotiation bookkeeping ------------------------------------------- */
+/* The per-iteration loops the reference runs in Python over all committed
+ * nets.  Nets come in the router's dict order as concatenated node paths or
+ * edge lists with int64 offsets off_d[M+1]; net_ids_d[m] is net m's integer
+ * id (PathFinderRouter._get_net_id). */
+
+/* Node ownership, _rebuild_node_owner (UPF:2762-2837).  First the committed
+ * via barrels: every node of every via step (same x, y; different z) of net
+ * m, over the whole z span, gets net m's id; where several nets cover a node
+ * the last one in order wins, as the reference's sequential overwrite.  Then
+ * the escape-via keepouts keep_nodes_d[K] / keep_ids_d[K] (the
+ * _via_keepouts_map entries with z > 0, in dict order): an entry claims its
+ * node if no barrel owns it, the first entry per node winning.  owner_d
+ * int32[N], -1 = free. */
+ORSP_API int orsp_node_owner(orsp_graph *g, int32_t M, const int32_t *paths_d, const int64_t *off_d,
+                    const int32_t *net_ids_d, int32_t K, const int32_t *keep_nodes_d,
+                    const int32_t *keep_ids_d, int32_t *owner_d, uintptr_t stream);
+
+/* Via barrel conflicts, _detect_barrel_conflicts (UPF:5478-5569): an edge of
+ * net m whose source or target node is owned by another net.  count_h
+ * receives the number of conflicting (net, edge) entries, duplicates
+ * included, as the reference's count; mask_d (uint8[E], optional) marks the
+ * conflicting edges. */
+ORSP_API int orsp_barrel_conflicts(orsp_graph *g, int32_t M, const int32_t *edges_d, const int64_t *off_d,
+                          const int32_t *net_ids_d, const int32_t *owner_d, uint8_t *mask_d,
+                          int64_t *count_h, uintptr_t stream);
+
+/* The Phase-1 barrel penalty of _pathfinder_negotiation (UPF:3852-3871):
+ * present[e] += penalty once for every marked edge (numpy fancy-index add). */
+ORSP_API int orsp_barrel_penalty(int64_t E, const uint8_t *mask_d, float *present_d, float penalty,
+                        uintptr_t stream);
+
+/* Per-net scores of _order_nets_by_difficulty (UPF:4401-4439) and
+ * _build_hotset (UPF:5009-5140), with over = max(0, present - cap) and
+ * hot(e) = over + 0.1 * history > 0.5 in float32:
+ *   congestion_d[m] = sum over net m's edges of over / max(1, count)  (float64)
+ *   impact_d[m]     = sum over net m's hot edges of over               (float64)
+ *   offender_d[m]   = 1 if net m has a hot edge
+ * Sums run in list order in float64, as Python's sum of float(over[e]).
+ * hot_count_h (optional) receives the number of hot edges in the graph.
+ * Each output pointer may be NULL. */
+ORSP_API int orsp_net_scores(orsp_graph *g, int32_t M, const int32_t *edges_d, const int64_t *off_d,
+                    const float *present_d, const float *cap_d, const float *hist_d, double *congestion_d,
+                    double *impact_d, uint8_t *offender_d, int64_t *hot_count_h, uintptr_t stream);
+
 /* ---- ROI extraction ---------------------------------------------------- */
 /* Bidirectional level-synchronous BFS ROI, as ROIExtractor.extract_roi_bfs
  * (UPF:1636-1734): waves from src (mark 1) and dst (mark 2) alternate, a node

@@ -27,6 +27,7 @@ SOURCES = [
     "orsp_via.cu",
     "orsp_route.cu",
     "orsp_warm.cu",
+    "orsp_bookkeeping.cu",
 ]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -65,6 +65,7 @@ struct Graph {
   void *pinned = nullptr;  // small pinned host buffer for results
   float *auto_delta = nullptr;  // [2] device bucket widths chosen by the library (single, batch)
   int32_t *box_g2r = nullptr;   // [N] box ROI map for box searches on the generic path (lazy)
+  int32_t *edge_src = nullptr;  // [E] source node of each edge (lazy, bookkeeping kernels)
   // routing loop (orsp_route.cu): error word, per-call net tables (device)
   // and their pinned staging copy
   void *route_ws = nullptr;

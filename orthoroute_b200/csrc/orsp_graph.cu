@@ -183,6 +183,7 @@ extern "C" int orsp_graph_destroy(orsp_graph *g) {
   cudaFree(g->route_tab_d);
   if (g->route_tab_h) cudaFreeHost(g->route_tab_h);
   cudaFree(g->box_g2r);
+  cudaFree(g->edge_src);
   if (g->pinned) cudaFreeHost(g->pinned);
   free_lattice(g);
   delete g;
