@@ -283,6 +283,15 @@ __device__ __forceinline__ bool sweep_run(float *c, int ds, const float *wlo, co
 // weights [4][nzb][TY][TX+1] and the interior distances as loaded
 // [nzb][TY][TX+1] (odd row strides: the row walks of the x-sweep and the
 // column walks of the y- and z-sweeps are bank-conflict free).
+// Barrier of the threads that visit tiles: the whole block, or (SPEC) the
+// first NW threads only - named barrier 1 - while a scheduler warp runs beside
+// them.
+template <int NW, bool SPEC>
+__device__ __forceinline__ void tile_sync() {
+  if (SPEC) asm volatile("bar.sync 1, %0;" ::"r"(NW) : "memory");
+  else __syncthreads();
+}
+
 // Layer lists of the box being visited: H layers (x-runs) and V layers
 // (y-runs) as offsets from the box's z0.  Recomputed when a CTA moves to a
 // tile of another box.
@@ -292,7 +301,7 @@ struct LayerLists {
   int box;
 };
 
-template <int TX, int TY, bool PRIV>
+template <int TX, int TY, bool PRIV, bool SPEC>
 __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *sd, LayerLists &L, int *s_flags,
                                              int *s_act) {
   const int bi = box_of_tile(p, t);
@@ -307,7 +316,7 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
     L.nv = nv;
     L.box = bi;
   }
-  __syncthreads();
+  tile_sync<TX * TY, SPEC>();
   const int *s_hl = L.hl, *s_vl = L.vl;
   const int nh = L.nh, nv = L.nv;
   constexpr int SX = TX + 3;
@@ -338,7 +347,7 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
   // read through L2 (other CTAs write them); weights are read-only.
   // one thread per column (x, y) of the tile: its nzb cells' loads are
   // issued back to back
-  for (int c = threadIdx.x; c < th * tw; c += blockDim.x) {
+  for (int c = threadIdx.x; c < th * tw; c += (TX * TY)) {
     const int yy = c / tw + 1, xx = c - (yy - 1) * tw + 1;
     const int64_t n0 = (int64_t)B.z0 * nxy + col0 + (int64_t)(yy - 1) * p.nx + (xx - 1);
     const int64_t d0 = dist_index<PRIV>(p, B, X0 + xx - 1, Y0 + yy - 1, B.z0);
@@ -360,7 +369,7 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
   {
     // halo: 2 cells per H row and per V column
     const int nhh = 2 * nh * th, nvh = 2 * nv * tw;
-    for (int i = threadIdx.x; i < nhh + nvh; i += blockDim.x) {
+    for (int i = threadIdx.x; i < nhh + nvh; i += (TX * TY)) {
       int z, xx, yy;
       if (i < nhh) {
         const int rowi = i >> 1;
@@ -380,7 +389,7 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
       sd[z * PS + yy * SX + xx] = v;
     }
   }
-  __syncthreads();
+  tile_sync<TX * TY, SPEC>();
   unsigned long long ts1 = 0;
   if (threadIdx.x == 0) ts1 = dev_globaltimer();
 
@@ -393,7 +402,7 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
   for (; cyc < MAX_CYCLES; ++cyc) {
     if (threadIdx.x == 0) s_flags[(cyc + 1) % 3] = 0;
     bool chg = false;
-    for (int rr = threadIdx.x; rr < nplan; rr += blockDim.x) {
+    for (int rr = threadIdx.x; rr < nplan; rr += (TX * TY)) {
       float *cell;
       int wo, ds, ws, n;
       if (rr < nh * th) {  // x-run of an H-layer row
@@ -414,8 +423,8 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
       }
       chg |= sweep_run(cell, ds, wlo + wo, whi + wo, ws, n);
     }
-    __syncthreads();
-    for (int c = threadIdx.x; c < tw * th; c += blockDim.x) {
+    tile_sync<TX * TY, SPEC>();
+    for (int c = threadIdx.x; c < tw * th; c += (TX * TY)) {
       const int xx = c % tw + 1, yy = c / tw + 1;
       // the z run has no halo: start the forward pass at layer 0 itself
       float *col = sd + yy * SX + xx - PS;
@@ -423,7 +432,7 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
       chg |= sweep_run(col, PS, wdn + wo, wup + wo, WPS, nzb, /*halo=*/false);
     }
     if (chg) s_flags[cyc % 3] = 1;
-    __syncthreads();
+    tile_sync<TX * TY, SPEC>();
     if (!s_flags[cyc % 3]) { converged = true; break; }
   }
   unsigned long long ts2 = 0;
@@ -434,7 +443,7 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
 
   // ---- publish improvements; mark neighbour tiles whose halo changed
   const int interior = nzb * th * tw;
-  for (int i = threadIdx.x; i < interior; i += blockDim.x) {
+  for (int i = threadIdx.x; i < interior; i += (TX * TY)) {
     const int z = i / (th * tw);
     const int rem = i - z * th * tw;
     const int yy = rem / tw + 1, xx = rem % tw + 1;
@@ -453,7 +462,7 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
     }
   }
   if (threadIdx.x == 0 && !converged) s_act[4] = 1;
-  __syncthreads();
+  tile_sync<TX * TY, SPEC>();
   if (threadIdx.x == 0) {
     const unsigned long long ts3 = dev_globaltimer();
     atomicAdd(&p.ctl->ns[0], ts1 - ts0);
@@ -509,7 +518,7 @@ __global__ void __launch_bounds__(TX * TY) lattice_tile_kernel(LatParams p) {
       __syncthreads();
       if (ti >= (int)n_in) break;
       const int t = __ldcg(&inl[ti]);
-      process_tile<TX, TY, PRIV>(p, t, sd, s_layers, s_flags, s_act);
+      process_tile<TX, TY, PRIV, false>(p, t, sd, s_layers, s_flags, s_act);
       if (threadIdx.x == 0) {
         int nb[5];
         const int k = revisit_list(p, t, s_act, nb);
@@ -618,7 +627,7 @@ __global__ void __launch_bounds__(TX * TY) lattice_async_kernel(LatParams p) {
     const int t = s_tile;
     __syncthreads();
     if (t < 0) break;
-    process_tile<TX, TY, PRIV>(p, t, sd, s_layers, s_flags, s_act);
+    process_tile<TX, TY, PRIV, false>(p, t, sd, s_layers, s_flags, s_act);
     // neighbours are activated by threads 0..3 in parallel, after this
     // tile's distances are visible
     unsigned long long ta = 0;
@@ -656,6 +665,136 @@ __global__ void __launch_bounds__(TX * TY) lattice_async_kernel(LatParams p) {
     atomicAdd(&ctl->visits, visits);
     atomicAdd(&ctl->ns[3], sched_ns);
   }
+}
+
+// Scheduler side of a finished visit of tile t with neighbour flags act:
+// activate the neighbours whose halo improved, then leave the visiting state
+// (idle, or queued again when dirty or not converged).  `pending` drops only
+// after everything the visit activated is queued.
+__device__ void finish_visit(const LatParams &p, int t, const int *act) {
+  __threadfence();
+  const LatBox B = load_box(p, box_of_tile(p, t));
+  const int lt = t - B.tile0, tx = lt % B.ntx, ty = lt / B.ntx;
+  const int nbs[4] = {(act[0] && tx > 0) ? t - 1 : -1, (act[1] && tx < B.ntx - 1) ? t + 1 : -1,
+                      (act[2] && ty > 0) ? t - B.ntx : -1, (act[3] && ty < B.nty - 1) ? t + B.ntx : -1};
+#pragma unroll
+  for (int d = 0; d < 4; ++d)
+    if (nbs[d] >= 0 && !activate_tile(p, nbs[d])) atomicCAS(&p.ctl->err, DEV_OK, DEV_ERR_INTERNAL);
+  if (act[4] || atomicCAS(&p.tstate[t], 2, 0) != 2) {
+    atomicExch(&p.tstate[t], 1);
+    queue_tile(p, t);
+  } else {
+    atomicSub(&p.ctl->pending, 1);
+  }
+}
+
+// Warp-specialised asynchronous schedule.  The block has NW = TX*TY worker
+// threads that visit tiles and one scheduler warp whose lane 0 does all queue
+// work, so that the chain of global atomics of a visit (pop, activation of the
+// neighbours, the tile's own state transition) overlaps the workers' loads and
+// sweeps instead of stalling them.
+//
+// Handoff protocol.  Handoff k hands tile cur_k (or -1: stop) to the workers
+// through s_cur, at named barrier 2, which all NW + 32 threads pass exactly
+// once per handoff (the scheduler warp passes it once per loop iteration, the
+// workers once before each visit; both stop after the handoff that carries
+// -1).  The workers visit cur_k with their own named barrier 1, write the
+// visit's neighbour flags into s_act[k & 1] and, after a device fence, set
+// s_done = k.  The scheduler finishes visit k (activations, state
+// transition) once s_done == k - in its wait loop for the next tile, or just
+// after the next handoff - so it never waits for work that only its own
+// finished tile would create.  The flags of visit k stay intact until visit
+// k + 2 starts, and the scheduler reads them before handoff k + 2.
+template <int TX, int TY, bool PRIV>
+__global__ void __launch_bounds__(TX * TY + 32, 1) lattice_spec_kernel(LatParams p) {
+  constexpr int NW = TX * TY;
+  extern __shared__ float sd[];
+  __shared__ LayerLists s_layers;
+  __shared__ int s_flags[3];
+  __shared__ int s_act[2][5];
+  __shared__ volatile int s_cur;
+  __shared__ volatile int s_done;
+  LatCtl *ctl = p.ctl;
+  if (threadIdx.x == 0) s_layers.box = -1;
+  if (threadIdx.x == NW) s_done = 0;
+  __syncthreads();
+  if (threadIdx.x < NW) {
+    // ---------------------------------------------------------- workers
+    unsigned long long idle_ns = 0;
+    for (int k = 1;; ++k) {
+      unsigned long long tw = 0;
+      if (threadIdx.x == 0) tw = dev_globaltimer();
+      asm volatile("bar.sync 2, %0;" ::"r"(NW + 32) : "memory");
+      if (threadIdx.x == 0) idle_ns += dev_globaltimer() - tw;
+      const int t = s_cur;
+      if (t < 0) break;
+      process_tile<TX, TY, PRIV, true>(p, t, sd, s_layers, s_flags, s_act[k & 1]);
+      // process_tile ended with barrier 1: every write of the visit is done
+      if (threadIdx.x == 0) {
+        __threadfence();
+        s_done = k;
+      }
+    }
+    if (threadIdx.x == 0) atomicAdd(&ctl->ns[3], idle_ns);
+    return;
+  }
+  // ------------------------------------------------------------ scheduler
+  const int lane = threadIdx.x & 31;
+  const unsigned long long t_start = dev_globaltimer();
+  int cur = -1;          // tile of the last handoff
+  int k = 0;             // index of the last handoff
+  bool finished = true;  // visit k finished by the scheduler (or none yet)
+  unsigned visits = 0;
+  for (;;) {
+    int next = -1;
+    if (lane == 0) {
+      long long pos = -1;
+      const unsigned long long t0 = dev_globaltimer();
+      for (unsigned spins = 0;; ++spins) {
+        if (!finished && s_done == k) {
+          finish_visit(p, cur, s_act[k & 1]);
+          ++visits;
+          finished = true;
+        }
+        if (ld_acquire_u32((const unsigned *)&ctl->err)) break;
+        if (pos < 0) pos = (long long)atomicAdd(&ctl->head, 1u);
+        int *slot = &p.qslot[(unsigned)pos % p.qcap];
+        const int v = (int)ld_acquire_u32((const unsigned *)slot);
+        if (v >= 0) {
+          atomicExch(slot, -1);
+          atomicExch(&p.tstate[v], 2);
+          __threadfence();
+          next = v;
+          break;
+        }
+        if (finished && ld_acquire_u32((const unsigned *)&ctl->pending) == 0) break;  // fixpoint reached
+        if ((spins & 31u) == 31u) {
+          const unsigned long long now = dev_globaltimer();
+          if (now - t0 > p.wait_ns || now - t_start > p.budget_ns) {
+            atomicCAS(&ctl->err, DEV_OK, DEV_ERR_TIMEOUT);
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      s_cur = next;
+      __threadfence_block();
+    }
+    next = __shfl_sync(0xffffffffu, next, 0);
+    __syncwarp();
+    asm volatile("bar.sync 2, %0;" ::"r"(NW + 32) : "memory");  // handoff k + 1
+    // the workers reached this barrier only after finishing visit k
+    if (lane == 0 && !finished) {
+      finish_visit(p, cur, s_act[k & 1]);
+      ++visits;
+      finished = true;
+    }
+    if (next < 0) break;
+    cur = next;
+    ++k;
+    finished = false;
+  }
+  if (lane == 0) atomicAdd(&ctl->visits, visits);
 }
 
 unsigned long long env_u64(const char *name, unsigned long long dflt) {
@@ -720,11 +859,16 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
     return ORSP_ERR_ARG;
   }
   const bool priv = opt && opt->private_dist;
-  void *kfn = async ? (priv ? (void *)lattice_async_kernel<TX, TY, true> : (void *)lattice_async_kernel<TX, TY, false>)
-                    : (priv ? (void *)lattice_tile_kernel<TX, TY, true> : (void *)lattice_tile_kernel<TX, TY, false>);
+  // ORSP_LAT_SPEC=1: the warp-specialised asynchronous schedule
+  const bool spec = async && env_u64("ORSP_LAT_SPEC", 0) != 0;
+  void *kfn;
+  if (spec) kfn = priv ? (void *)lattice_spec_kernel<TX, TY, true> : (void *)lattice_spec_kernel<TX, TY, false>;
+  else if (async) kfn = priv ? (void *)lattice_async_kernel<TX, TY, true> : (void *)lattice_async_kernel<TX, TY, false>;
+  else kfn = priv ? (void *)lattice_tile_kernel<TX, TY, true> : (void *)lattice_tile_kernel<TX, TY, false>;
+  const int threads = TX * TY + (spec ? 32 : 0);
   ORSP_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
-  ORSP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, TX * TY, smem));
+  ORSP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, threads, smem));
   if (occ < 1) {
     orsp::set_error("lattice search: kernel does not fit on an SM");
     return ORSP_ERR_ARG;
@@ -738,7 +882,7 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   if (orsp::g_timer.on) ORSP_CUDA(cudaEventRecord(orsp::g_timer.a, st));
   // Cooperative launch in both schedules: every CTA is resident, so a CTA
   // waiting for a queue slot never blocks the CTA that will fill it.
-  ORSP_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(g->num_sms * bps), dim3(TX * TY), args, smem, st));
+  ORSP_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(g->num_sms * bps), dim3(threads), args, smem, st));
   if (orsp::g_timer.on) {
     ORSP_CUDA(cudaEventRecord(orsp::g_timer.b, st));
     orsp::g_timer.pending = true;

@@ -119,15 +119,23 @@ def test_sssp_reference_lattice_duplicate_vias(golden):
         assert (p or []) == g[f"ref{k}_path"].tolist()
 
 
-@pytest.mark.parametrize("impl", ["lattice16", "lattice32", "lattice16-rounds", "generic"])
+def _lattice_env(monkeypatch, impl):
+    """Selects the search implementation: generic near-far, or the tile sweeps
+    with tile width 16/32 and the asynchronous, warp-specialised or round
+    schedule."""
+    monkeypatch.setenv("ORSP_SSSP_IMPL", "generic" if impl == "generic" else "auto")
+    monkeypatch.setenv("ORSP_LAT_TILE", "32" if impl == "lattice32" else "16")
+    monkeypatch.setenv("ORSP_LAT_ASYNC", "0" if impl.endswith("rounds") else "1")
+    monkeypatch.setenv("ORSP_LAT_SPEC", "1" if impl.endswith("spec") else "0")
+
+
+@pytest.mark.parametrize("impl", ["lattice16", "lattice32", "lattice16-rounds", "lattice16-spec", "generic"])
 @pytest.mark.parametrize("shape,blocked,planar", [((60, 50, 6), 0.05, "all"), ((33, 17, 12), 0.0, "all"),
                                                   ((128, 96, 4), 0.03, "all"), ((45, 70, 6), 0.02, "inner")])
 def test_sssp_full_distances_bit_exact(shape, blocked, planar, impl, monkeypatch):
     """Full searches, both implementations (tile sweeps on the lattice, generic
-    near-far) and both tile sizes, bit-identical to the oracle."""
-    monkeypatch.setenv("ORSP_SSSP_IMPL", "generic" if impl == "generic" else "auto")
-    monkeypatch.setenv("ORSP_LAT_TILE", "32" if impl == "lattice32" else "16")
-    monkeypatch.setenv("ORSP_LAT_ASYNC", "0" if impl.endswith("rounds") else "1")
+    near-far), both tile sizes and every schedule, bit-identical to the oracle."""
+    _lattice_env(monkeypatch, impl)
     lat = build_lattice(*shape, planar=planar)
     w = uniform_weights(lat, seed=sum(shape), blocked_frac=blocked)
     dg = DeviceGraph.from_lattice(lat)
@@ -405,14 +413,12 @@ def test_find_paths_on_rois_local_csr_batch():
     assert got == refs
 
 
-@pytest.mark.parametrize("impl", ["lattice16", "lattice32", "lattice16-rounds", "generic"])
+@pytest.mark.parametrize("impl", ["lattice16", "lattice32", "lattice16-rounds", "lattice16-spec", "generic"])
 def test_sssp_box_matches_box_roi_and_oracle(impl, monkeypatch):
     """orsp_sssp_box == orsp_sssp with the box's ROI map == the oracle with that
     ROI: distances (full searches) and paths, for boxes at the border, thin
     boxes, single-layer boxes and endpoints outside the box."""
-    monkeypatch.setenv("ORSP_SSSP_IMPL", "generic" if impl == "generic" else "auto")
-    monkeypatch.setenv("ORSP_LAT_TILE", "32" if impl == "lattice32" else "16")
-    monkeypatch.setenv("ORSP_LAT_ASYNC", "0" if impl.endswith("rounds") else "1")
+    _lattice_env(monkeypatch, impl)
     lat = build_lattice(75, 58, 6)
     w = uniform_weights(lat, seed=21, blocked_frac=0.04)
     dg = DeviceGraph.from_lattice(lat)
@@ -475,14 +481,12 @@ def test_batch_plans_agree_on_status_codes():
     assert np.array_equal(na[2, : la[2]], nb[2, : lb[2]])
 
 
-@pytest.mark.parametrize("impl", ["lattice16", "lattice32", "lattice16-rounds"])
+@pytest.mark.parametrize("impl", ["lattice16", "lattice32", "lattice16-rounds", "lattice16-spec"])
 def test_seed_on_tile_edge_single_layer_box(impl, monkeypatch):
     """A seed on a tile edge must reach the next tile even when no other cell
     of that edge improves: single-layer boxes (one routing axis), source on
     the first row or column of a tile, target in the neighbouring tile."""
-    monkeypatch.setenv("ORSP_SSSP_IMPL", "auto")
-    monkeypatch.setenv("ORSP_LAT_TILE", "32" if impl == "lattice32" else "16")
-    monkeypatch.setenv("ORSP_LAT_ASYNC", "0" if impl.endswith("rounds") else "1")
+    _lattice_env(monkeypatch, impl)
     lat = build_lattice(90, 70, 6)
     w = uniform_weights(lat, seed=5, blocked_frac=0.0)
     dg = DeviceGraph.from_lattice(lat)
