@@ -283,6 +283,19 @@ ORSP_API int orsp_net_scores(orsp_graph *g, int32_t M, const int32_t *edges_d, c
                     const float *present_d, const float *cap_d, const float *hist_d, double *congestion_d,
                     double *impact_d, uint8_t *offender_d, int64_t *hot_count_h, uintptr_t stream);
 
+/* Geometry emission, PathFinderRouter._generate_geometry_from_paths
+ * (UPF:5749-5834): net m's node path paths_d[off_d[m] .. off_d[m+1]) becomes
+ * straight track runs and vias with the reference's rules (outer-layer
+ * planar steps dropped, non-unit or off-axis planar steps skipped, runs
+ * flushed at vias and turns).  Net m writes rows starting at off_d[m] of
+ * tracks_d (int32 [.][3]: run start node, run end node, layer) and vias_d
+ * (int32 [.][3]: node, from layer, to layer), and its counts to
+ * ntracks_d[m] / nvias_d[m].  layer_axis_h[z] (host, nz entries): 1 for 'h'
+ * layers (x moves only), anything else for layers checked as 'v'. */
+ORSP_API int orsp_emit_geometry(orsp_graph *g, int32_t M, const int32_t *paths_d, const int64_t *off_d,
+                       const int8_t *layer_axis_h, int32_t *tracks_d, int32_t *vias_d, int32_t *ntracks_d,
+                       int32_t *nvias_d, uintptr_t stream);
+
 /* ---- ROI extraction ---------------------------------------------------- */
 /* Bidirectional level-synchronous BFS ROI, as ROIExtractor.extract_roi_bfs
  * (UPF:1636-1734): waves from src (mark 1) and dst (mark 2) alternate, a node

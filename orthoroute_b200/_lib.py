@@ -65,6 +65,7 @@ _SIGS = {
     "orsp_barrel_conflicts": (ctypes.c_int, [_P, _i32, _P, _P, _P, _P, _P, ctypes.POINTER(_i64), _u]),
     "orsp_barrel_penalty": (ctypes.c_int, [_i64, _P, _P, _f32, _u]),
     "orsp_net_scores": (ctypes.c_int, [_P, _i32, _P, _P, _P, _P, _P, _P, _P, _P, ctypes.POINTER(_i64), _u]),
+    "orsp_emit_geometry": (ctypes.c_int, [_P, _i32, _P, _P, _P, _P, _P, _P, _P, _u]),
     "orsp_route_nets": (ctypes.c_int, [_P, _i32, _P, _P, _P, _i32, _P, _i32, _P, _P, _P, _i32, _P, _P, _P, _P, _P,
                                        _P, _P, _f32, _f32, _f32, _f32, _i32, _u]),
     "orsp_sssp_multi": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _P, _P, _f32, _P, _i32,

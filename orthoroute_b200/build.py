@@ -28,6 +28,7 @@ SOURCES = [
     "orsp_route.cu",
     "orsp_warm.cu",
     "orsp_bookkeeping.cu",
+    "orsp_geometry.cu",
 ]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]

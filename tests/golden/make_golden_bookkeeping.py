@@ -11,6 +11,7 @@ router (oracle/ref_harness.py), then, on that router's state:
   the barrel penalty of _pathfinder_negotiation   UPF:3852-3871  -> present after
   PathFinderRouter._order_nets_by_difficulty      UPF:4401-4439  -> net order
   PathFinderRouter._build_hotset                  UPF:5009-5140  -> hotset
+  PathFinderRouter._generate_geometry_from_paths  UPF:5749-5897  -> tracks, vias
 
 Output: golden_bookkeeping.npz (UPF = orthoroute/algorithms/manhattan/
 unified_pathfinder.py).  Net names are stored by index (net k is "N{k}").
@@ -97,8 +98,23 @@ def main():
         out[pfx + "hot_cap"] = np.int32(r.config.hotset_cap)
         out[pfx + "hotset"] = np.array(sorted(names.index(n) for n in hot), np.int32)
         out[pfx + "hot_clean_after"] = np.array([r._net_clean_iters.get(n, 0) for n in names], np.int32)
+        # geometry of the committed paths (world coordinates, layer indices)
+        tracks, vias = r._generate_geometry_from_paths()
+        lnames = list(r.config.layer_names)
+        lidx = lambda nm: lnames.index(nm) if nm in lnames else int(nm[1:])  # noqa: E731
+        out[pfx + "tracks"] = np.array([[names.index(t["net"]), lidx(t["layer"])] for t in tracks],
+                                       np.int32).reshape(-1, 2)
+        out[pfx + "track_xy"] = np.array([[t["x1"], t["y1"], t["x2"], t["y2"]] for t in tracks],
+                                         np.float64).reshape(-1, 4)
+        out[pfx + "vias"] = np.array([[names.index(v["net"]), lidx(v["from_layer"]), lidx(v["to_layer"])]
+                                      for v in vias], np.int32).reshape(-1, 3)
+        out[pfx + "via_xy"] = np.array([[v["x"], v["y"]] for v in vias], np.float64).reshape(-1, 2)
+        geom = r.lattice.geom
+        out[pfx + "geom"] = np.array([geom.grid_min_x, geom.grid_min_y, geom.pitch], np.float64)
+        out[pfx + "layer_names"] = np.array(lnames)
+        out[pfx + "layer_dir"] = np.array([r.lattice.get_legal_axis(z) for z in range(nz)])
         print(f"case {c}: {len(order)} routed nets, owned nodes {(r.node_owner >= 0).sum()}, conflicts {cnt}, "
-              f"hotset {len(hot)}")
+              f"hotset {len(hot)}, tracks {len(tracks)}, vias {len(vias)}")
     np.savez_compressed(HERE / "golden_bookkeeping.npz", **out)
 
 

@@ -99,3 +99,53 @@ def test_device_bookkeeping_matches_reference(golden, c):
     hs = build_hotset(dg, tasks, edges, {n for n in order if len(paths[n]) > 0}, pres0, capd, histd, it, clean,
                       last, cap, ripped={names[1]})
     assert sorted(names.index(n) for n in hs) == g[p + "hotset"].tolist()
+
+
+def _golden_geometry(g, c, names):
+    p = f"c{c}_"
+    ln = [str(v) for v in g[p + "layer_names"]]
+    tracks = [(names[int(n)], int(l), tuple(float(v) for v in xy)) for (n, l), xy in zip(g[p + "tracks"],
+                                                                                       g[p + "track_xy"])]
+    vias = [(names[int(n)], int(a), int(b), tuple(float(v) for v in xy)) for (n, a, b), xy in zip(g[p + "vias"],
+                                                                                                 g[p + "via_xy"])]
+    return ln, [str(v) for v in g[p + "layer_dir"]], tuple(float(v) for v in g[p + "geom"]), tracks, vias
+
+
+@pytest.mark.parametrize("c", [0, 1])
+def test_oracle_geometry_matches_reference(golden, c):
+    import oracle.geometry as OG
+    from orthoroute_b200.geometry import _quantize
+
+    g = golden("golden_bookkeeping.npz")
+    b, names, order, paths, edges, tasks, ids, keep = _case(g, c)
+    lat = b.lattice
+    ln, dirs, (gx, gy, pitch), tracks, vias = _golden_geometry(g, c, names)
+    out = OG.emit([paths[n] for n in order], lat.nx, lat.ny, lat.nz, dirs)
+    plane = lat.nx * lat.ny
+
+    def xy(node):
+        r = node % plane
+        return (float(_quantize(gx + (r % lat.nx) * pitch, gx, pitch)),
+                float(_quantize(gy + (r // lat.nx) * pitch, gy, pitch)))
+
+    got_t, got_v = [], []
+    for n, (tr, vi) in zip(order, out):
+        got_t += [(n, z, xy(a) + xy(bb)) for a, bb, z in tr]
+        got_v += [(n, min(z0, z1), max(z0, z1), xy(v)) for v, z0, z1 in vi]
+    assert got_t == tracks
+    assert got_v == vias
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("c", [0, 1])
+def test_device_geometry_matches_reference(golden, c):
+    from orthoroute_b200.geometry import generate_geometry
+    from orthoroute_b200.solver import DeviceGraph
+
+    g = golden("golden_bookkeeping.npz")
+    b, names, order, paths, edges, tasks, ids, keep = _case(g, c)
+    ln, dirs, (gx, gy, pitch), tracks, vias = _golden_geometry(g, c, names)
+    dg = DeviceGraph.from_lattice(b.lattice)
+    t, v = generate_geometry(dg, paths, dirs, gx, gy, pitch, ln, grid_pitch=pitch)
+    assert [(d["net"], ln.index(d["layer"]), (d["x1"], d["y1"], d["x2"], d["y2"])) for d in t] == tracks
+    assert [(d["net"], ln.index(d["from_layer"]), ln.index(d["to_layer"]), (d["x"], d["y"])) for d in v] == vias
