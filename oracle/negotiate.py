@@ -88,6 +88,21 @@ def route_plain(lat, src, dst, cfg, base_cost=None, history_init=None, max_nets_
                 boxes = bbox_with_margin(lat, src, dst, margins)
             if net_order == "disjoint":
                 idx = _first_fit_rounds(boxes, idx)
+            if it == 1 and getattr(cfg, "first_pass", "sequential") == "independent":
+                # first pass: every net on the initial costs, then all committed
+                nodes, lens = O.batch_bbox(lat.indptr, lat.indices, cost, lat.nx, lat.ny, lat.nz, src[idx], dst[idx],
+                                           boxes[idx], cap_paths)
+                for j, k in enumerate(idx):
+                    L = int(lens[j])
+                    if L >= 2:
+                        p = nodes[j, :L].copy()
+                        net_paths[k] = p
+                        net_edges[k] = O.path_to_edges(lat.indptr, lat.indices, p)
+                        np.add.at(usage, net_edges[k], 1)
+                    else:
+                        net_paths[k] = np.zeros(0, np.int32)
+                        net_edges[k] = np.zeros(0, np.int32)
+                idx = np.zeros(0, np.int64)
             for k in idx:  # sequential: rip up, search on live costs, commit
                 e = net_edges[k]
                 if e.size:

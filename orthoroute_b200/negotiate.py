@@ -92,6 +92,8 @@ class NegotiationConfig:
     net_order: str = "index"  # "index" | "disjoint": first-fit rounds of pairwise disjoint boxes
     stall_grow: int = 0  # cells added to the margin of a net that offends stall_iterations times running
     stall_iterations: int = 2
+    first_pass: str = "sequential"  # per-net costs: "sequential", or "independent" (iteration 1 on fixed costs)
+    batch_plan: Optional[list] = None  # DeviceGraph.set_batch_plan for the batched searches
 
 
 @dataclass
@@ -249,13 +251,19 @@ class PathFinder:
             if L >= 2:
                 check(lib.orsp_commit_edges(L - 1, ptr(net_edges[k]), ptr(acc.usage), ptr(acc.present), -1, st),
                       "orsp_commit_edges")
-            if self.cfg.roi == "bbox":
-                g2r = self.roi.box_map(boxes[k])
-            elif self.cfg.roi == "bfs":
-                _, g2r = self.roi.extract_roi(int(src[k]), int(dst[k]))
+            if self.cfg.roi == "bbox" and self.dg.is_lattice:
+                g2r = "box"
+                status, path, _ = self.dg.sssp_box(cost, int(src[k]), int(dst[k]), boxes[k], delta=delta,
+                                                   path_cap=cap)
             else:
-                g2r = None
-            status, path, _ = self.dg.sssp(cost, int(src[k]), int(dst[k]), roi_map=g2r, delta=delta, path_cap=cap)
+                if self.cfg.roi == "bbox":
+                    g2r = self.roi.box_map(boxes[k])
+                elif self.cfg.roi == "bfs":
+                    _, g2r = self.roi.extract_roi(int(src[k]), int(dst[k]))
+                else:
+                    g2r = None
+                status, path, _ = self.dg.sssp(cost, int(src[k]), int(dst[k]), roi_map=g2r, delta=delta,
+                                               path_cap=cap)
             if (status != _lib.ORSP_OK or path is None or path.numel() < 2) and self.cfg.full_graph_retry \
                     and g2r is not None:
                 status, path, _ = self.dg.sssp(cost, int(src[k]), int(dst[k]), roi_map=None, delta=delta,
@@ -423,6 +431,10 @@ class PathFinder:
         if net_policy and cfg.roi != "bbox":
             raise ValueError("per-net costs are implemented for box ROIs")
         acc.total_cost = torch.empty(self.E, dtype=torch.float32, device=dev)
+        if cfg.batch_plan is not None:
+            self.dg.set_batch_plan(cfg.batch_plan)
+        if cfg.first_pass not in ("sequential", "independent"):
+            raise ValueError("first_pass must be 'sequential' or 'independent'")
         for it in range(1, cfg.max_iterations + 1):
             t_it = time.perf_counter()
             acc.refresh_from_canonical()
@@ -453,7 +465,16 @@ class PathFinder:
                     boxes_d = torch.from_numpy(boxes).to(dev)
             if cfg.net_order == "disjoint" and idx.numel() > 1:
                 idx = torch.from_numpy(disjoint_order(boxes, idx.cpu().numpy()).astype(np.int64)).to(dev)
-            if idx.numel() > 0 and net_policy:
+            independent = net_policy and it == 1 and cfg.first_pass == "independent"
+            if independent and idx.numel() > 0:
+                # first pass: every net searched on the same (initial) costs,
+                # then all committed - one batch launch in batched mode
+                if mode == "batched":
+                    self._route_batched(acc, cost, idx, src_d, dst_d, boxes_d, full_box_d, order_rank, net_nodes,
+                                        net_edges, net_lens, delta)
+                else:
+                    self._route_sequential(acc, cost, idx, src, dst, boxes, net_nodes, net_edges, net_lens, delta)
+            elif idx.numel() > 0 and net_policy:
                 if mode == "batched":
                     self._route_net_batched(acc, pres_fac, idx, src_d, dst_d, boxes_d, boxes, order_rank, net_nodes,
                                             net_edges, net_lens, delta, src=src, dst=dst)

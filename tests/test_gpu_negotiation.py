@@ -31,16 +31,21 @@ def test_negotiation_batched_sequential_oracle(reroute):
     assert np.array_equal(rs.edge_usage, ref["usage"])
 
 
-@pytest.mark.parametrize("reroute,order,grow", [("all", "index", 0), ("offenders", "index", 0),
-                                                ("offenders", "disjoint", 0), ("offenders", "disjoint", 3)])
-def test_negotiation_per_net_costs_levels_match_sequential_and_oracle(reroute, order, grow):
+@pytest.mark.parametrize("reroute,order,grow,first", [("all", "index", 0, "sequential"),
+                                                      ("offenders", "index", 0, "sequential"),
+                                                      ("offenders", "disjoint", 0, "sequential"),
+                                                      ("offenders", "disjoint", 3, "sequential"),
+                                                      ("offenders", "disjoint", 3, "independent")])
+def test_negotiation_per_net_costs_levels_match_sequential_and_oracle(reroute, order, grow, first):
     """Per-net (live usage) costs: the level-batched run equals the one-search-
     per-net run and the oracle, per iteration and per net, also with the
     first-fit disjoint order and with box growth for stalled nets."""
     b = board_uniform_pins(48, 40, 4, 70, seed=8)
     cfg = NegotiationConfig(max_iterations=5 if grow == 0 else 8, reroute=reroute, roi_margin=3,
                             cost_update="net", full_graph_retry=False, net_order=order, stall_grow=grow,
-                            stall_iterations=1 if grow else 2)
+                            stall_iterations=1 if grow else 2, first_pass=first,
+                            batch_plan=[{"max_nodes": 1 << 40, "impl": 1, "tile_w": 16}] if first == "independent"
+                            else None)
     ref = route_plain(b.lattice, b.src, b.dst, cfg)
     pf = PathFinder(b.lattice, config=cfg)
     rb = pf.route(b.src, b.dst, mode="batched")
