@@ -335,3 +335,56 @@ def warm_history(net: "WarmNet", lat: Lattice, src, dst, scale: float) -> np.nda
     """Initial per-edge history for a board: features -> net -> edges."""
     pred = net.predict(board_features(lat, np.asarray(src), np.asarray(dst)))
     return history_from_prediction(lat, pred, scale)
+
+
+def _main(argv=None):
+    """python -m orthoroute_b200.warm [--size 400] [--nz 18] [--seed 3] [--reps 3]:
+    the shipped network's prediction for a footprint board at the backplane's
+    net density; prints the time of the features, of one forward pass and of
+    its first 3x3x3 convolution (32 -> 32 channels, full resolution) with the
+    tensor-core rate that convolution reaches."""
+    import argparse
+    import json
+    import time
+
+    from .lattice import board_footprints
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--size", type=int, default=400)
+    ap.add_argument("--nz", type=int, default=18)
+    ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--reps", type=int, default=3)
+    a = ap.parse_args(argv)
+    nets = int(round(8000 / (600 * 600) * a.size * a.size))
+    b = board_footprints(a.size, a.size, a.nz, nets, None, seed=a.seed)
+    t0 = time.perf_counter()
+    feats = board_features(b.lattice, b.src, b.dst)
+    t_feat = time.perf_counter() - t0
+    net, scale = load_pretrained()
+    x = torch.from_numpy(feats).cuda().to(torch.bfloat16)
+    net.forward(x)  # warm-up
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.reps):
+        net.forward(x)
+    e1.record()
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1) / a.reps
+    D, H, W = x.shape[:3]
+    h = torch.empty(D, H, W, net.C, dtype=torch.bfloat16, device="cuda").uniform_()
+    net._pack("e0b", False)
+    e0.record()
+    for _ in range(a.reps):
+        net._conv(h, "e0b", D, H, W)
+    e1.record()
+    torch.cuda.synchronize()
+    conv_ms = e0.elapsed_time(e1) / a.reps
+    flops = 2.0 * 27 * net.C * net.C * D * H * W
+    print(json.dumps({"board": f"{a.size}x{a.size}x{a.nz}", "voxels": D * H * W, "features_s": round(t_feat, 3),
+                      "forward_ms": round(fwd_ms, 2), "conv32_ms": round(conv_ms, 3),
+                      "conv32_tflops": round(flops / (conv_ms / 1e3) / 1e12, 1), "history_scale": scale}))
+
+
+if __name__ == "__main__":
+    _main()
