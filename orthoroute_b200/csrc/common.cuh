@@ -90,7 +90,7 @@ struct Graph {
   bool lattice_ok = false;
   int8_t layer_axis[64] = {};     // 0: no planar edges, 1: x, 2: y
   int32_t *slot_eid = nullptr;    // [4][N] in-edge id per slot (-1 absent)
-  float *wslot = nullptr;         // [4][N] gathered in-edge weights
+  float *wslot = nullptr;         // [N] float4: gathered in-edge weights per node, by slot
   void *lat_ws = nullptr;         // tile lists, stamps and control block
   size_t lat_ws_bytes = 0;
   void *lat_ctl_h = nullptr;      // pinned mirror of the control block

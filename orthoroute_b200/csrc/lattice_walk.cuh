@@ -1,0 +1,104 @@
+// Predecessor walk on the H/V routing lattice.
+//
+// On the lattice every node v = (x, y, z) has at most four in-neighbours, one
+// per slot of the gathered in-edge weights w4[v] (orsp_lattice.cu):
+//   slot 0: the lower neighbour along the layer's axis (x-1 on H layers, y-1 on
+//           V layers), slot 1: the upper one (x+1 / y+1),
+//   slot 2: the via from below (z-1), slot 3: the via from above (z+1).
+// So the parent of v under the settle-order rule of the heap Dijkstra
+// (SimpleDijkstra.find_path_roi, unified_pathfinder.py:1846-1887: the
+// in-neighbour u with fl32(d[u] + w(u,v)) == d[v] and the smallest
+// (d[u], rank u) below (d[v], rank v)) needs one float4 and four distances,
+// all independent loads: one memory round trip per step of the walk, where a
+// walk over the transposed CSR needs three dependent ones (row pointer, source
+// list, distance).  Ranks are node ids (box searches rank nodes in id order,
+// and a box's own distance slice is laid out in that order too).
+#pragma once
+
+#include "common.cuh"
+
+namespace orsp {
+
+struct LatWalkGeom {
+  int32_t nx, ny, nz;
+  int8_t axis[64];  // 1: x moves (H layer), 2: y moves (V layer), 0: none
+};
+
+// Coordinates of a node id.
+__device__ __forceinline__ void lat_xyz(const LatWalkGeom &G, int64_t v, int32_t &x, int32_t &y, int32_t &z) {
+  const int64_t plane = (int64_t)G.nx * G.ny;
+  z = (int32_t)(v / plane);
+  const int64_t r = v - (int64_t)z * plane;
+  y = (int32_t)(r / G.nx);
+  x = (int32_t)(r - (int64_t)y * G.nx);
+}
+
+// Neighbour of (x, y, z) through slot s, or false if it leaves box B.
+__device__ __forceinline__ bool lat_slot_nbr(const LatWalkGeom &G, const LatBox &B, int s, int32_t x, int32_t y,
+                                             int32_t z, int32_t &ux, int32_t &uy, int32_t &uz) {
+  ux = x;
+  uy = y;
+  uz = z;
+  if (s < 2) {
+    const int d = s == 0 ? -1 : 1;
+    if (G.axis[z] == 1) ux += d;
+    else if (G.axis[z] == 2) uy += d;
+    else return false;
+  } else {
+    uz += s == 2 ? -1 : 1;
+  }
+  return ux >= B.x0 && ux <= B.x1 && uy >= B.y0 && uy <= B.y1 && uz >= B.z0 && uz <= B.z1;
+}
+
+// One step of the walk at v = (x, y, z) with distance bits dv.  DIST(x, y, z)
+// gives the distance bits of a node inside the box.  Returns the slot of the
+// parent (and its coordinates and distance bits), or -1 when no in-neighbour
+// qualifies.
+template <class DIST>
+__device__ __forceinline__ int lat_parent(const LatWalkGeom &G, const LatBox &B, const float4 *__restrict__ w4,
+                                          DIST dist, int32_t x, int32_t y, int32_t z, unsigned dv,
+                                          int32_t &px, int32_t &py, int32_t &pz, unsigned &pdu) {
+  const int64_t v = ((int64_t)z * G.ny + y) * G.nx + x;
+  const float4 wv = __ldcg(&w4[v]);
+  const float wk[4] = {wv.x, wv.y, wv.z, wv.w};
+  unsigned du[4];
+  int32_t ux[4], uy[4], uz[4];
+  bool ok[4];
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    ok[s] = lat_slot_nbr(G, B, s, x, y, z, ux[s], uy[s], uz[s]);
+    du[s] = ok[s] ? dist(ux[s], uy[s], uz[s]) : ORSP_INF_BITS;
+  }
+  unsigned long long best = ULLONG_MAX;
+  int bs = -1;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    if (!ok[s] || du[s] == ORSP_INF_BITS) continue;
+    if (f_bits(__fadd_rn(bits_f(du[s]), wk[s])) != dv) continue;
+    const int64_t u = ((int64_t)uz[s] * G.ny + uy[s]) * G.nx + ux[s];
+    if (!(du[s] < dv || (du[s] == dv && u < v))) continue;
+    const unsigned long long key = ((unsigned long long)du[s] << 32) | (unsigned long long)(uint32_t)u;
+    if (key < best) {
+      best = key;
+      bs = s;
+    }
+  }
+  if (bs >= 0) {
+    px = ux[bs];
+    py = uy[bs];
+    pz = uz[bs];
+    pdu = (unsigned)(best >> 32);
+  }
+  return bs;
+}
+
+// Slot of the in-edge u -> v between lattice neighbours u and v (node ids).
+__device__ __forceinline__ int lat_edge_slot(const LatWalkGeom &G, int64_t u, int64_t v) {
+  const int64_t plane = (int64_t)G.nx * G.ny;
+  const int64_t zu = u / plane, zv = v / plane;
+  if (zu < zv) return 2;
+  if (zu > zv) return 3;
+  return u < v ? 0 : 1;
+}
+
+}  // namespace orsp

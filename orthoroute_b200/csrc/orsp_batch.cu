@@ -22,6 +22,7 @@
 
 #include "common.cuh"
 #include "fastdiv.cuh"
+#include "lattice_walk.cuh"
 
 namespace {
 
@@ -381,15 +382,19 @@ int env_int(const char *name, int dflt) {
 }
 
 // Backtrace of the searches done by tile sweeps with their own distance
-// slices: one warp per search (block j: item[j], box boxes[j]), the same walk,
-// parent rule, first-CSR-edge lookup and status codes as block_backtrace, with
-// the distances read from the box's slice (box-local row-major order, which is
-// the node-id order, so the ranks agree).
+// slices: one warp per search (block j: item[j], box boxes[j]).  Lane 0 walks
+// with lat_parent (the parent rule of block_backtrace, one round trip per
+// step), reading distances from the box's slice (box-local row-major order,
+// which is the node-id order, so the ranks agree); then the lanes reverse the
+// path and map each step u -> v to the in-edge of v in u's slot (the first CSR
+// edge u -> v: the lattice has no parallel edges).  Same status codes as
+// block_backtrace.
 struct LatBt {
-  const float *cost;
-  const int32_t *rptr, *rsrc, *reid;
+  const float4 *w4;         // gathered in-edge weights (fresh inside the boxes)
+  const int32_t *slot_eid;  // [4][N] in-edge id per slot
+  int64_t N;
   const uint32_t *dist;  // slice arena
-  int32_t nx, ny;
+  orsp::LatWalkGeom geom;
   const orsp::LatBox *boxes;
   const int32_t *item, *src, *dst;  // per box: search id, source, target (global ids)
   int32_t *path_nodes, *path_edges, *path_len;
@@ -397,13 +402,8 @@ struct LatBt {
   const int *search_err;
 };
 
-__device__ __forceinline__ bool lat_local(const LatBt &p, const orsp::LatBox &B, int32_t u, int64_t *li) {
-  const int32_t plane = p.nx * p.ny;
-  const int32_t z = u / plane, r = u - z * plane, y = r / p.nx, x = r - y * p.nx;
-  if (x < B.x0 || x > B.x1 || y < B.y0 || y > B.y1 || z < B.z0 || z > B.z1) return false;
-  const int64_t bw = B.x1 - B.x0 + 1, bh = B.y1 - B.y0 + 1;
-  *li = ((int64_t)(z - B.z0) * bh + (y - B.y0)) * bw + (x - B.x0);
-  return true;
+__device__ __forceinline__ bool lat_in_box(const orsp::LatBox &B, int32_t x, int32_t y, int32_t z) {
+  return x >= B.x0 && x <= B.x1 && y >= B.y0 && y <= B.y1 && z >= B.z0 && z <= B.z1;
 }
 
 __global__ void lat_batch_backtrace_kernel(LatBt p) {
@@ -414,8 +414,11 @@ __global__ void lat_batch_backtrace_kernel(LatBt p) {
   const int32_t src = p.src[j], dst = p.dst[j];
   int32_t *nodes = p.path_nodes + (int64_t)k * p.path_cap;
   int32_t *edges = p.path_edges ? p.path_edges + (int64_t)k * p.path_cap : nullptr;
-  int64_t ls, ld;
-  if (src < 0 || dst < 0 || !lat_local(p, B, src, &ls) || !lat_local(p, B, dst, &ld)) {
+  const int64_t N = (int64_t)p.geom.nx * p.geom.ny * p.geom.nz;
+  int32_t sx = 0, sy = 0, sz = 0, x = 0, y = 0, z = 0;
+  if (src >= 0 && src < N) orsp::lat_xyz(p.geom, src, sx, sy, sz);
+  if (dst >= 0 && dst < N) orsp::lat_xyz(p.geom, dst, x, y, z);
+  if (src < 0 || dst < 0 || src >= N || dst >= N || !lat_in_box(B, sx, sy, sz) || !lat_in_box(B, x, y, z)) {
     if (lane == 0) p.path_len[k] = ST_ARG;
     return;
   }
@@ -424,70 +427,53 @@ __global__ void lat_batch_backtrace_kernel(LatBt p) {
     return;
   }
   const uint32_t *dist = p.dist + B.dbase;
-  unsigned dv = dist[ld];
+  const int64_t bw = B.x1 - B.x0 + 1, bh = B.y1 - B.y0 + 1;
+  const int32_t bx0 = B.x0, by0 = B.y0, bz0 = B.z0;
+  auto dget = [dist, bw, bh, bx0, by0, bz0](int32_t a, int32_t b, int32_t c) {
+    return __ldcg(&dist[((int64_t)(c - bz0) * bh + (b - by0)) * bw + (a - bx0)]);
+  };
+  unsigned dv = dget(x, y, z);
   if (dv == ORSP_INF_BITS) {
     if (lane == 0) p.path_len[k] = 0;
     return;
   }
-  int32_t v = dst;
-  int64_t lv = ld;
   int len = 0, status = 0;
-  for (;;) {
-    if (len >= p.path_cap) { status = ST_PATHCAP; break; }
-    if (lane == 0) nodes[len] = v;
-    ++len;
-    if (v == src) break;
-    const int kb = __ldg(&p.rptr[v]), ke = __ldg(&p.rptr[v + 1]);
-    unsigned long long best = ULLONG_MAX;
-    int32_t bu = -1;
-    for (int k0 = kb; k0 < ke; k0 += 32) {
-      const int kk = k0 + lane;
-      if (kk < ke) {
-        const int32_t u = __ldg(&p.rsrc[kk]);
-        int64_t lu;
-        if (lat_local(p, B, u, &lu)) {
-          const unsigned du = dist[lu];
-          if (du != ORSP_INF_BITS) {
-            const float s = __fadd_rn(bits_f(du), __ldg(&p.cost[__ldg(&p.reid[kk])]));
-            if (f_bits(s) == dv && (du < dv || (du == dv && lu < lv))) {
-              const unsigned long long key = ((unsigned long long)du << 32) | (unsigned)lu;
-              if (key < best) { best = key; bu = u; }
-            }
-          }
-        }
+  if (lane == 0) {
+    int32_t v = dst;
+    for (;;) {
+      if (len >= p.path_cap) { status = ST_PATHCAP; break; }
+      nodes[len++] = v;
+      if (v == src) break;
+      int32_t px, py, pz;
+      unsigned pdu;
+      if (orsp::lat_parent(p.geom, B, p.w4, dget, x, y, z, dv, px, py, pz, pdu) < 0) {
+        status = ST_INTERNAL;
+        break;
       }
+      x = px;
+      y = py;
+      z = pz;
+      dv = pdu;
+      v = (int32_t)(((int64_t)z * p.geom.ny + y) * p.geom.nx + x);
     }
-    const unsigned long long wbest = warp_min_u64(best);
-    if (wbest == ULLONG_MAX) { status = ST_INTERNAL; break; }
-    const unsigned owner = __ballot_sync(ORSP_FULL_MASK, best == wbest && bu >= 0);
-    const int32_t u = __shfl_sync(ORSP_FULL_MASK, bu, __ffs(owner) - 1);
-    int32_t emin = INT_MAX;
-    for (int k0 = kb; k0 < ke; k0 += 32) {
-      const int kk = k0 + lane;
-      if (kk < ke && __ldg(&p.rsrc[kk]) == u) emin = min(emin, __ldg(&p.reid[kk]));
-    }
-    emin = __reduce_min_sync(ORSP_FULL_MASK, emin);
-    if (edges && lane == 0 && len - 1 < p.path_cap) edges[len - 1] = emin;
-    v = u;
-    lv = (int64_t)(wbest & 0xffffffffu);
-    dv = (unsigned)(wbest >> 32);
   }
+  len = __shfl_sync(ORSP_FULL_MASK, len, 0);
+  status = __shfl_sync(ORSP_FULL_MASK, status, 0);
   __syncwarp();
   if (status) {
     if (lane == 0) p.path_len[k] = status;
     return;
   }
   for (int i = lane; i < len / 2; i += 32) {
-    const int32_t a = nodes[i], z = nodes[len - 1 - i];
-    nodes[i] = z;
+    const int32_t a = nodes[i], zz = nodes[len - 1 - i];
+    nodes[i] = zz;
     nodes[len - 1 - i] = a;
   }
+  __syncwarp();
   if (edges) {
-    const int ne = len - 1;
-    for (int i = lane; i < ne / 2; i += 32) {
-      const int32_t a = edges[i], z = edges[ne - 1 - i];
-      edges[i] = z;
-      edges[ne - 1 - i] = a;
+    for (int i = lane; i < len - 1; i += 32) {
+      const int32_t u = nodes[i], w = nodes[i + 1];
+      edges[i] = __ldg(&p.slot_eid[(int64_t)orsp::lat_edge_slot(p.geom, u, w) * p.N + w]);
     }
   }
   __syncwarp();
@@ -697,13 +683,14 @@ int run_batch_lat(orsp_graph *g, const float *cost_d, int32_t K, const std::vect
     rc = run_lattice_boxes(g, cost_d, m, d_src, nullptr, m, boxes.data(), db, g->blat_dist, st, &opt);
     if (rc) return rc;
     LatBt bt{};
-    bt.cost = cost_d;
-    bt.rptr = g->rptr;
-    bt.rsrc = g->rsrc;
-    bt.reid = g->reid;
+    bt.w4 = (const float4 *)g->wslot;
+    bt.slot_eid = g->slot_eid;
+    bt.N = g->N;
     bt.dist = g->blat_dist;
-    bt.nx = g->nx;
-    bt.ny = g->ny;
+    bt.geom.nx = g->nx;
+    bt.geom.ny = g->ny;
+    bt.geom.nz = g->nz;
+    for (int z = 0; z < 64; ++z) bt.geom.axis[z] = z < g->nz ? g->layer_axis[z] : 0;
     bt.boxes = db;
     bt.item = d_item;
     bt.src = d_src;

@@ -26,11 +26,16 @@
 #include <vector>
 
 #include "accounting.cuh"
+#include "lattice_walk.cuh"
 
 namespace {
 
 using orsp::apply_usage;
+using orsp::lat_edge_slot;
+using orsp::lat_parent;
+using orsp::lat_xyz;
 using orsp::LatBox;
+using orsp::LatWalkGeom;
 using orsp::live_cost;
 
 struct LiveParams {
@@ -63,11 +68,11 @@ __global__ void route_commit_kernel(const int32_t *order, const int32_t *edges, 
 }
 
 struct RouteBt {
-  const float *cost;
-  const int32_t *indptr, *indices;
-  const int32_t *rptr, *rsrc, *reid;
+  const float4 *w4;         // gathered in-edge weights (fresh inside the group's boxes)
+  const int32_t *slot_eid;  // [4][N] in-edge id per slot
+  int64_t N;
   const uint32_t *dist;
-  int32_t nx, ny;
+  LatWalkGeom geom;
   // the group's nets: net ids, sources (-1: source outside its box), targets, boxes
   const int32_t *order, *src, *dst;
   const LatBox *boxes;
@@ -77,17 +82,14 @@ struct RouteBt {
   int *route_err;
 };
 
-__device__ __forceinline__ bool in_box(const RouteBt &p, const LatBox &B, int32_t u) {
-  const int32_t plane = p.nx * p.ny;
-  const int32_t z = u / plane, r = u - z * plane, y = r / p.nx, x = r - y * p.nx;
-  return x >= B.x0 && x <= B.x1 && y >= B.y0 && y <= B.y1 && z >= B.z0 && z <= B.z1;
-}
-
-// Step 3, one warp per net of the group (block j: net order[j]).  Parent of
-// v: the in-neighbour u inside the net's box with fl32(d[u] + w(u,v)) == d[v]
-// and the smallest (d[u], u) below (d[v], v); the source (distance 0) ends
+// Step 3, one warp per net of the group (block j: net order[j]).  Lane 0
+// walks from the target to the source with lat_parent (the parent rule of
+// orsp_sssp, rank = node id = box-local order); the source (distance 0) ends
 // the walk.  Nodes outside the box hold distances of other boxes or of
-// earlier searches, hence the box test.
+// earlier searches, so the walk never leaves the box.  Then the lanes reverse
+// the path and map each step u -> v to its CSR edge, the in-edge of v in the
+// slot that u occupies (the lattice has no parallel edges, so this is the
+// first CSR edge u -> v of path_to_edges).
 __global__ void route_backtrace_kernel(RouteBt p) {
   const int lane = threadIdx.x & 31;
   const int j = blockIdx.x;
@@ -105,44 +107,39 @@ __global__ void route_backtrace_kernel(RouteBt p) {
     }
     return;
   }
-  unsigned dv = (src >= 0 && in_box(p, B, dst)) ? p.dist[dst] : ORSP_INF_BITS;
-  if (dv == ORSP_INF_BITS || dst == src) {
-    if (lane == 0) *len_out = 0;
-    return;
-  }
-  int v = dst;
-  int len = 0;
-  int err = 0;
-  for (;;) {
-    if (len >= p.cap) { err = DEV_ERR_PATH_OVERFLOW; break; }
-    if (lane == 0) nodes[len] = v;
-    ++len;
-    if (v == src && dv == 0u) break;
-    const int b = p.rptr[v], e = p.rptr[v + 1];
-    unsigned long long best = ULLONG_MAX;
-    int bu = -1;
-    for (int k0 = b; k0 < e; k0 += 32) {
-      const int kk = k0 + lane;
-      if (kk < e) {
-        const int u = p.rsrc[kk];
-        if (in_box(p, B, u)) {
-          const unsigned du = p.dist[u];
-          if (du != ORSP_INF_BITS) {
-            const float s = __fadd_rn(bits_f(du), p.cost[p.reid[kk]]);
-            if (f_bits(s) == dv && (du < dv || (du == dv && u < v))) {
-              const unsigned long long key = ((unsigned long long)du << 32) | (unsigned)u;
-              if (key < best) { best = key; bu = u; }
-            }
-          }
+  int len = 0, err = 0;
+  if (lane == 0) {
+    int32_t x, y, z;
+    lat_xyz(p.geom, dst, x, y, z);
+    const bool dst_in = x >= B.x0 && x <= B.x1 && y >= B.y0 && y <= B.y1 && z >= B.z0 && z <= B.z1;
+    unsigned dv = (src >= 0 && dst_in) ? __ldcg(&p.dist[dst]) : ORSP_INF_BITS;
+    if (dv != ORSP_INF_BITS && dst != src) {
+      const int32_t nx = p.geom.nx, ny = p.geom.ny;
+      const uint32_t *dist = p.dist;
+      auto dget = [dist, nx, ny](int32_t a, int32_t b, int32_t c) {
+        return __ldcg(&dist[((int64_t)c * ny + b) * nx + a]);
+      };
+      int32_t v = dst;
+      for (;;) {
+        if (len >= p.cap) { err = DEV_ERR_PATH_OVERFLOW; break; }
+        nodes[len++] = v;
+        if (v == src && dv == 0u) break;
+        int32_t px, py, pz;
+        unsigned pdu;
+        if (lat_parent(p.geom, B, p.w4, dget, x, y, z, dv, px, py, pz, pdu) < 0) {
+          err = DEV_ERR_INTERNAL;
+          break;
         }
+        x = px;
+        y = py;
+        z = pz;
+        dv = pdu;
+        v = (int32_t)(((int64_t)z * ny + y) * nx + x);
       }
     }
-    const unsigned long long wbest = warp_min_u64(best);
-    if (wbest == ULLONG_MAX) { err = DEV_ERR_INTERNAL; break; }
-    const unsigned owner = __ballot_sync(ORSP_FULL_MASK, best == wbest && bu >= 0);
-    v = __shfl_sync(ORSP_FULL_MASK, bu, __ffs(owner) - 1);
-    dv = (unsigned)(wbest >> 32);
   }
+  len = __shfl_sync(ORSP_FULL_MASK, len, 0);
+  err = __shfl_sync(ORSP_FULL_MASK, err, 0);
   __syncwarp();
   if (err) {
     if (lane == 0) {
@@ -158,11 +155,8 @@ __global__ void route_backtrace_kernel(RouteBt p) {
   }
   __syncwarp();
   for (int i = lane; i < len - 1; i += 32) {
-    const int u = nodes[i], w = nodes[i + 1];
-    int eid = -1;
-    for (int e = p.indptr[u]; e < p.indptr[u + 1]; ++e)
-      if (p.indices[e] == w) { eid = e; break; }
-    edges[i] = eid;
+    const int32_t u = nodes[i], w = nodes[i + 1];
+    edges[i] = __ldg(&p.slot_eid[(int64_t)lat_edge_slot(p.geom, u, w) * p.N + w]);
   }
   __syncwarp();
   if (lane == 0) *len_out = len;
@@ -292,6 +286,11 @@ extern "C" int orsp_route_nets(orsp_graph *g, int32_t M, const int32_t *src_h, c
   ORSP_CUDA(cudaMemsetAsync(route_err, 0, sizeof(int), st));
 
   LiveParams lp{usage_d, present_d, base_d, cap_d, hist_d, pres_fac, hist_w, via_mult, base_w, jitter, cost_d};
+  LatWalkGeom geom{};
+  geom.nx = g->nx;
+  geom.ny = g->ny;
+  geom.nz = g->nz;
+  for (int z = 0; z < 64; ++z) geom.axis[z] = z < g->nz ? g->layer_axis[z] : 0;
   for (int32_t q = 0; q < ngroups; ++q) {
     const int32_t a = gp[q], n = gp[q + 1] - gp[q];
     if (n == 0) continue;
@@ -304,15 +303,11 @@ extern "C" int orsp_route_nets(orsp_graph *g, int32_t M, const int32_t *src_h, c
                            st, &opt);
     if (rc) return rc;
     RouteBt bt{};
-    bt.cost = cost_d;
-    bt.indptr = g->indptr;
-    bt.indices = g->indices;
-    bt.rptr = g->rptr;
-    bt.rsrc = g->rsrc;
-    bt.reid = g->reid;
+    bt.w4 = (const float4 *)g->wslot;
+    bt.slot_eid = g->slot_eid;
+    bt.N = g->N;
     bt.dist = g->dist;
-    bt.nx = g->nx;
-    bt.ny = g->ny;
+    bt.geom = geom;
     bt.order = d_order + a;
     bt.src = d_src + a;
     bt.dst = d_dst + a;

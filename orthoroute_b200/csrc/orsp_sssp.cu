@@ -16,6 +16,7 @@
 #include <string>
 
 #include "common.cuh"
+#include "lattice_walk.cuh"
 
 namespace {
 
@@ -343,6 +344,84 @@ __global__ void backtrace_kernel(BacktraceParams p) {
   if (lane == 0) { ctl->path_len = len; ctl->status = 0; }
 }
 
+// The same walk on a recognised H/V lattice after a tile-sweep search inside
+// box B: lat_parent gives each parent with one memory round trip (ranks are
+// node ids, as in the tile-sweep search).  Every lane computes the same
+// parent (the loads coalesce); the lanes split the seed test.
+using orsp::lat_parent;
+using orsp::lat_xyz;
+using orsp::LatBox;
+using orsp::LatWalkGeom;
+
+struct LatBacktraceParams {
+  const float4 *w4;
+  const uint32_t *dist;
+  LatWalkGeom geom;
+  LatBox box;
+  const int32_t *seeds;
+  const float *seed_cost;
+  int32_t nseeds;
+  int32_t dst;
+  int32_t *path_out;
+  int32_t path_cap;
+  SsspCtl *ctl;
+};
+
+__global__ void lat_backtrace_kernel(LatBacktraceParams p) {
+  const int lane = threadIdx.x & 31;
+  SsspCtl *ctl = p.ctl;
+  if (ctl->err) return;
+  const LatBox &B = p.box;
+  int32_t x, y, z;
+  lat_xyz(p.geom, p.dst, x, y, z);
+  const bool in = x >= B.x0 && x <= B.x1 && y >= B.y0 && y <= B.y1 && z >= B.z0 && z <= B.z1;
+  unsigned dv = in ? __ldcg(&p.dist[p.dst]) : ORSP_INF_BITS;
+  if (dv == ORSP_INF_BITS) {
+    if (lane == 0) { ctl->path_len = 0; ctl->status = 1; }
+    return;
+  }
+  const uint32_t *dist = p.dist;
+  const int32_t nx = p.geom.nx, ny = p.geom.ny;
+  auto dget = [dist, nx, ny](int32_t a, int32_t b, int32_t c) {
+    return __ldcg(&dist[((int64_t)c * ny + b) * nx + a]);
+  };
+  int32_t v = p.dst;
+  int len = 0, err = 0;
+  for (;;) {
+    if (len >= p.path_cap) { err = DEV_ERR_PATH_OVERFLOW; break; }
+    if (lane == 0) p.path_out[len] = v;
+    ++len;
+    bool is_start = false;
+    for (int i = lane; i < p.nseeds; i += 32) {
+      if (p.seeds[i] == v) {
+        const float c0 = p.seed_cost ? p.seed_cost[i] : 0.0f;
+        if (f_bits(c0) == dv) is_start = true;
+      }
+    }
+    if (__any_sync(ORSP_FULL_MASK, is_start)) break;
+    int32_t px, py, pz;
+    unsigned pdu;
+    if (lat_parent(p.geom, B, p.w4, dget, x, y, z, dv, px, py, pz, pdu) < 0) { err = DEV_ERR_INTERNAL; break; }
+    x = px;
+    y = py;
+    z = pz;
+    dv = pdu;
+    v = (int32_t)(((int64_t)z * ny + y) * nx + x);
+  }
+  __syncwarp();
+  if (err) {
+    if (lane == 0) atomicCAS(&ctl->err, DEV_OK, err);
+    return;
+  }
+  for (int i = lane; i < len / 2; i += 32) {
+    const int a = p.path_out[i];
+    const int zz = p.path_out[len - 1 - i];
+    p.path_out[i] = zz;
+    p.path_out[len - 1 - i] = a;
+  }
+  if (lane == 0) { ctl->path_len = len; ctl->status = 0; }
+}
+
 // Multi-sink winner, as find_path_multisource_multisink (UPF:1941-1975): the
 // target with the smallest (double)d[t] + target_cost; among equal totals the
 // one the heap pops first, i.e. the smallest (d[t], rank(t)).  One block.
@@ -562,7 +641,33 @@ static int sssp_impl(orsp_graph *g, const float *cost_d, int32_t nseeds, const i
                          nullptr, delta, dist, st);
     if (rc) return rc;
   }
-  if (dst >= 0) {
+  if (dst >= 0 && lattice) {
+    LatBacktraceParams b{};
+    b.w4 = (const float4 *)g->wslot;
+    b.dist = dist;
+    b.geom.nx = g->nx;
+    b.geom.ny = g->ny;
+    b.geom.nz = g->nz;
+    for (int z = 0; z < 64; ++z) b.geom.axis[z] = z < g->nz ? g->layer_axis[z] : 0;
+    const int32_t full[6] = {0, g->nx - 1, 0, g->ny - 1, 0, g->nz - 1};
+    const int32_t *bx = box_h ? box_h : full;
+    b.box.x0 = bx[0];
+    b.box.x1 = bx[1];
+    b.box.y0 = bx[2];
+    b.box.y1 = bx[3];
+    b.box.z0 = bx[4];
+    b.box.z1 = bx[5];
+    b.box.dbase = -1;
+    b.seeds = seeds_d;
+    b.seed_cost = seed_cost_d;
+    b.nseeds = nseeds;
+    b.dst = dst;
+    b.path_out = path_out_d;
+    b.path_cap = path_cap;
+    b.ctl = (SsspCtl *)g->ctl;
+    lat_backtrace_kernel<<<1, 32, 0, st>>>(b);
+    ORSP_CUDA(cudaGetLastError());
+  } else if (dst >= 0) {
     BacktraceParams b{};
     b.cost = cost_d;
     b.roi_map = roi_map_d;
