@@ -92,6 +92,71 @@ __device__ __forceinline__ int lat_parent(const LatWalkGeom &G, const LatBox &B,
   return bs;
 }
 
+// Cell i steps from (x, y, z) through slot s (the direction a straight run of
+// parents takes when every parent sits in slot s of its child), or false if
+// it leaves box B.
+__device__ __forceinline__ bool lat_run_cell(const LatWalkGeom &G, const LatBox &B, int s, int i, int32_t x,
+                                             int32_t y, int32_t z, int32_t &cx, int32_t &cy, int32_t &cz) {
+  cx = x;
+  cy = y;
+  cz = z;
+  if (s < 2) {
+    const int d = s == 0 ? -i : i;
+    if (G.axis[z] == 1) cx += d;
+    else if (G.axis[z] == 2) cy += d;
+    else if (i) return false;
+  } else {
+    cz += s == 2 ? -i : i;
+  }
+  return cx >= B.x0 && cx <= B.x1 && cy >= B.y0 && cy <= B.y1 && cz >= B.z0 && cz <= B.z1;
+}
+
+// The whole walk, by one full warp, from node (x, y, z) with distance bits dv
+// until STOP(node, dv) holds for the node just appended.  Nodes are appended
+// to out[0..cap) from the target back to the start.  Returns the length, or
+// -1 (more than cap nodes) / -2 (a node without a qualifying parent).
+//
+// Paths on the lattice are mostly straight runs, so each round lane i takes
+// the cell i steps ahead of the current node along the direction of the last
+// step and computes that cell's parent with lat_parent, all lanes at once (one
+// memory round trip).  Where the parent of lane i's cell is lane i+1's cell,
+// the run goes on; the first lane where it does not ends the round, and its
+// parent is the next current node.  Each lane's parent is the one the
+// sequential walk computes at that node (same distances, same rule), so the
+// nodes are those of the one-step walk; a round advances by up to 32 nodes.
+template <class DIST, class STOP>
+__device__ __forceinline__ int lat_walk_warp(const LatWalkGeom &G, const LatBox &B, const float4 *__restrict__ w4,
+                                             DIST dist, STOP stop, int32_t x, int32_t y, int32_t z, unsigned dv,
+                                             int32_t *out, int32_t cap) {
+  const int lane = threadIdx.x & 31;
+  int len = 0;
+  int s = 0;  // predicted slot: the direction of the last step
+  for (;;) {
+    int32_t cx, cy, cz;
+    const bool valid = lat_run_cell(G, B, s, lane, x, y, z, cx, cy, cz);
+    const int64_t c = ((int64_t)cz * G.ny + cy) * G.nx + cx;
+    const unsigned dc = lane == 0 ? dv : (valid ? dist(cx, cy, cz) : ORSP_INF_BITS);
+    const bool is_stop = valid && dc != ORSP_INF_BITS && stop(c, dc);
+    int ps = -1;
+    int32_t px = 0, py = 0, pz = 0;
+    unsigned pdu = 0;
+    if (valid && dc != ORSP_INF_BITS && !is_stop) ps = lat_parent(G, B, w4, dist, cx, cy, cz, dc, px, py, pz, pdu);
+    const bool cont = valid && !is_stop && ps == s && lane < 31;
+    const unsigned m = __ballot_sync(ORSP_FULL_MASK, cont);
+    const int last = __ffs(~m) - 1;  // lane 31 never continues
+    if (lane <= last && len + lane < cap) out[len + lane] = (int32_t)c;
+    if (len + last + 1 > cap) return -1;
+    len += last + 1;
+    if (__shfl_sync(ORSP_FULL_MASK, is_stop, last)) return len;
+    s = __shfl_sync(ORSP_FULL_MASK, ps, last);
+    if (s < 0) return -2;
+    x = __shfl_sync(ORSP_FULL_MASK, px, last);
+    y = __shfl_sync(ORSP_FULL_MASK, py, last);
+    z = __shfl_sync(ORSP_FULL_MASK, pz, last);
+    dv = __shfl_sync(ORSP_FULL_MASK, pdu, last);
+  }
+}
+
 // Slot of the in-edge u -> v between lattice neighbours u and v (node ids).
 __device__ __forceinline__ int lat_edge_slot(const LatWalkGeom &G, int64_t u, int64_t v) {
   const int64_t plane = (int64_t)G.nx * G.ny;

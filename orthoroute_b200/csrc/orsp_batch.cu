@@ -382,9 +382,8 @@ int env_int(const char *name, int dflt) {
 }
 
 // Backtrace of the searches done by tile sweeps with their own distance
-// slices: one warp per search (block j: item[j], box boxes[j]).  Lane 0 walks
-// with lat_parent (the parent rule of block_backtrace, one round trip per
-// step), reading distances from the box's slice (box-local row-major order,
+// slices: one warp per search (block j: item[j], box boxes[j]).  The warp
+// walks with lat_walk_warp (the parent rule of block_backtrace), reading distances from the box's slice (box-local row-major order,
 // which is the node-id order, so the ranks agree); then the lanes reverse the
 // path and map each step u -> v to the in-edge of v in u's slot (the first CSR
 // edge u -> v: the lattice has no parallel edges).  Same status codes as
@@ -437,28 +436,11 @@ __global__ void lat_batch_backtrace_kernel(LatBt p) {
     if (lane == 0) p.path_len[k] = 0;
     return;
   }
-  int len = 0, status = 0;
-  if (lane == 0) {
-    int32_t v = dst;
-    for (;;) {
-      if (len >= p.path_cap) { status = ST_PATHCAP; break; }
-      nodes[len++] = v;
-      if (v == src) break;
-      int32_t px, py, pz;
-      unsigned pdu;
-      if (orsp::lat_parent(p.geom, B, p.w4, dget, x, y, z, dv, px, py, pz, pdu) < 0) {
-        status = ST_INTERNAL;
-        break;
-      }
-      x = px;
-      y = py;
-      z = pz;
-      dv = pdu;
-      v = (int32_t)(((int64_t)z * p.geom.ny + y) * p.geom.nx + x);
-    }
-  }
-  len = __shfl_sync(ORSP_FULL_MASK, len, 0);
-  status = __shfl_sync(ORSP_FULL_MASK, status, 0);
+  auto at_src = [src](int64_t v, unsigned) { return v == src; };
+  int len = orsp::lat_walk_warp(p.geom, B, p.w4, dget, at_src, x, y, z, dv, nodes, p.path_cap);
+  int status = 0;
+  if (len == -1) status = ST_PATHCAP;
+  else if (len < 0) status = ST_INTERNAL;
   __syncwarp();
   if (status) {
     if (lane == 0) p.path_len[k] = status;

@@ -32,7 +32,7 @@ namespace {
 
 using orsp::apply_usage;
 using orsp::lat_edge_slot;
-using orsp::lat_parent;
+using orsp::lat_walk_warp;
 using orsp::lat_xyz;
 using orsp::LatBox;
 using orsp::LatWalkGeom;
@@ -82,8 +82,8 @@ struct RouteBt {
   int *route_err;
 };
 
-// Step 3, one warp per net of the group (block j: net order[j]).  Lane 0
-// walks from the target to the source with lat_parent (the parent rule of
+// Step 3, one warp per net of the group (block j: net order[j]).  The warp
+// walks from the target to the source with lat_walk_warp (the parent rule of
 // orsp_sssp, rank = node id = box-local order); the source (distance 0) ends
 // the walk.  Nodes outside the box hold distances of other boxes or of
 // earlier searches, so the walk never leaves the box.  Then the lanes reverse
@@ -108,38 +108,22 @@ __global__ void route_backtrace_kernel(RouteBt p) {
     return;
   }
   int len = 0, err = 0;
-  if (lane == 0) {
-    int32_t x, y, z;
-    lat_xyz(p.geom, dst, x, y, z);
-    const bool dst_in = x >= B.x0 && x <= B.x1 && y >= B.y0 && y <= B.y1 && z >= B.z0 && z <= B.z1;
-    unsigned dv = (src >= 0 && dst_in) ? __ldcg(&p.dist[dst]) : ORSP_INF_BITS;
-    if (dv != ORSP_INF_BITS && dst != src) {
-      const int32_t nx = p.geom.nx, ny = p.geom.ny;
-      const uint32_t *dist = p.dist;
-      auto dget = [dist, nx, ny](int32_t a, int32_t b, int32_t c) {
-        return __ldcg(&dist[((int64_t)c * ny + b) * nx + a]);
-      };
-      int32_t v = dst;
-      for (;;) {
-        if (len >= p.cap) { err = DEV_ERR_PATH_OVERFLOW; break; }
-        nodes[len++] = v;
-        if (v == src && dv == 0u) break;
-        int32_t px, py, pz;
-        unsigned pdu;
-        if (lat_parent(p.geom, B, p.w4, dget, x, y, z, dv, px, py, pz, pdu) < 0) {
-          err = DEV_ERR_INTERNAL;
-          break;
-        }
-        x = px;
-        y = py;
-        z = pz;
-        dv = pdu;
-        v = (int32_t)(((int64_t)z * ny + y) * nx + x);
-      }
-    }
+  int32_t x, y, z;
+  lat_xyz(p.geom, dst, x, y, z);
+  const bool dst_in = x >= B.x0 && x <= B.x1 && y >= B.y0 && y <= B.y1 && z >= B.z0 && z <= B.z1;
+  const unsigned dv = (src >= 0 && dst_in) ? __ldcg(&p.dist[dst]) : ORSP_INF_BITS;
+  if (dv != ORSP_INF_BITS && dst != src) {
+    const int32_t nx = p.geom.nx, ny = p.geom.ny;
+    const uint32_t *dist = p.dist;
+    auto dget = [dist, nx, ny](int32_t a, int32_t b, int32_t c) {
+      return __ldcg(&dist[((int64_t)c * ny + b) * nx + a]);
+    };
+    auto at_src = [src](int64_t v, unsigned d) { return v == src && d == 0u; };
+    len = lat_walk_warp(p.geom, B, p.w4, dget, at_src, x, y, z, dv, nodes, p.cap);
+    if (len == -1) err = DEV_ERR_PATH_OVERFLOW;
+    else if (len < 0) err = DEV_ERR_INTERNAL;
+    if (err) len = 0;
   }
-  len = __shfl_sync(ORSP_FULL_MASK, len, 0);
-  err = __shfl_sync(ORSP_FULL_MASK, err, 0);
   __syncwarp();
   if (err) {
     if (lane == 0) {

@@ -345,10 +345,9 @@ __global__ void backtrace_kernel(BacktraceParams p) {
 }
 
 // The same walk on a recognised H/V lattice after a tile-sweep search inside
-// box B: lat_parent gives each parent with one memory round trip (ranks are
-// node ids, as in the tile-sweep search).  Every lane computes the same
-// parent (the loads coalesce); the lanes split the seed test.
-using orsp::lat_parent;
+// box B: lat_walk_warp, up to 32 nodes of a straight run per memory round
+// trip (ranks are node ids, as in the tile-sweep search).
+using orsp::lat_walk_warp;
 using orsp::lat_xyz;
 using orsp::LatBox;
 using orsp::LatWalkGeom;
@@ -385,29 +384,19 @@ __global__ void lat_backtrace_kernel(LatBacktraceParams p) {
   auto dget = [dist, nx, ny](int32_t a, int32_t b, int32_t c) {
     return __ldcg(&dist[((int64_t)c * ny + b) * nx + a]);
   };
-  int32_t v = p.dst;
-  int len = 0, err = 0;
-  for (;;) {
-    if (len >= p.path_cap) { err = DEV_ERR_PATH_OVERFLOW; break; }
-    if (lane == 0) p.path_out[len] = v;
-    ++len;
-    bool is_start = false;
-    for (int i = lane; i < p.nseeds; i += 32) {
-      if (p.seeds[i] == v) {
-        const float c0 = p.seed_cost ? p.seed_cost[i] : 0.0f;
-        if (f_bits(c0) == dv) is_start = true;
-      }
-    }
-    if (__any_sync(ORSP_FULL_MASK, is_start)) break;
-    int32_t px, py, pz;
-    unsigned pdu;
-    if (lat_parent(p.geom, B, p.w4, dget, x, y, z, dv, px, py, pz, pdu) < 0) { err = DEV_ERR_INTERNAL; break; }
-    x = px;
-    y = py;
-    z = pz;
-    dv = pdu;
-    v = (int32_t)(((int64_t)z * ny + y) * nx + x);
-  }
+  const int32_t *seeds = p.seeds;
+  const float *seed_cost = p.seed_cost;
+  const int32_t nseeds = p.nseeds;
+  // a seed whose distance still equals its start cost ends the walk
+  auto at_start = [seeds, seed_cost, nseeds](int64_t v, unsigned d) {
+    for (int i = 0; i < nseeds; ++i)
+      if (seeds[i] == v && f_bits(seed_cost ? seed_cost[i] : 0.0f) == d) return true;
+    return false;
+  };
+  int len = lat_walk_warp(p.geom, B, p.w4, dget, at_start, x, y, z, dv, p.path_out, p.path_cap);
+  int err = 0;
+  if (len == -1) err = DEV_ERR_PATH_OVERFLOW;
+  else if (len < 0) err = DEV_ERR_INTERNAL;
   __syncwarp();
   if (err) {
     if (lane == 0) atomicCAS(&ctl->err, DEV_OK, err);
