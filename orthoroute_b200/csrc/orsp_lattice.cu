@@ -226,54 +226,115 @@ __global__ void lattice_seed_kernel(LatParams p, int32_t nseeds, const int32_t *
 // One run of the sweep: cells c[1..n] at stride `ds`, with c[0] and c[n+1]
 // the halo values (when `halo`; otherwise the run starts and ends at c[1] and
 // c[n]).  Forward: c[i] = min(c[i], c[i-1] + wlo[i]); backward: c[i] =
-// min(c[i], c[i+1] + whi[i]); each step a single fp32 round-to-nearest add.
-// The run is walked in register chunks of 4 (loads first, then the dependent
-// min-plus chain) so that only one shared-memory round trip is exposed per
-// chunk.  Returns whether any cell decreased.
+// min(c[i], c[i+1] + whi[i]); each step a single fp32 round-to-nearest add
+// and a min (fminf returns one of its operands; no NaN or -0 occurs here, so
+// the result is that of the compare-and-replace form, without a branch).  The
+// run is walked in register chunks of 4 (loads first, then the dependent
+// chain), and only decreased cells are stored.  Returns whether any cell
+// decreased.  Used for runs whose length is known only at run time (tiles cut
+// by the box edge, z-runs).
 __device__ __forceinline__ bool sweep_run(float *c, int ds, const float *wlo, const float *whi, int ws,
                                           int n, bool halo = true) {
   constexpr int K = 4;
   bool chg = false;
   float prev = halo ? c[0] : __int_as_float(0x7f800000);
   for (int b = 1; b <= n; b += K) {
-    float cv[K], wv[K];
+    float cv[K], wv[K], nv[K];
 #pragma unroll
     for (int k = 0; k < K; ++k)
       if (b + k <= n) { cv[k] = c[(b + k) * ds]; wv[k] = wlo[(b + k) * ws]; }
-    unsigned dirty = 0;
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      if (b + k <= n) {
-        const float c2 = __fadd_rn(prev, wv[k]);
-        if (c2 < cv[k]) { cv[k] = c2; dirty |= 1u << k; }
-        prev = cv[k];
-      }
-    }
 #pragma unroll
     for (int k = 0; k < K; ++k)
-      if (dirty & (1u << k)) c[(b + k) * ds] = cv[k];
-    chg |= dirty != 0;
+      if (b + k <= n) { nv[k] = fminf(__fadd_rn(prev, wv[k]), cv[k]); prev = nv[k]; }
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (b + k <= n && nv[k] < cv[k]) { c[(b + k) * ds] = nv[k]; chg = true; }
   }
   prev = halo ? c[(n + 1) * ds] : __int_as_float(0x7f800000);
   for (int b = n; b >= 1; b -= K) {
-    float cv[K], wv[K];
+    float cv[K], wv[K], nv[K];
 #pragma unroll
     for (int k = 0; k < K; ++k)
       if (b - k >= 1) { cv[k] = c[(b - k) * ds]; wv[k] = whi[(b - k) * ws]; }
-    unsigned dirty = 0;
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      if (b - k >= 1) {
-        const float c2 = __fadd_rn(prev, wv[k]);
-        if (c2 < cv[k]) { cv[k] = c2; dirty |= 1u << k; }
-        prev = cv[k];
-      }
-    }
 #pragma unroll
     for (int k = 0; k < K; ++k)
-      if (dirty & (1u << k)) c[(b - k) * ds] = cv[k];
-    chg |= dirty != 0;
+      if (b - k >= 1) { nv[k] = fminf(__fadd_rn(prev, wv[k]), cv[k]); prev = nv[k]; }
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (b - k >= 1 && nv[k] < cv[k]) { c[(b - k) * ds] = nv[k]; chg = true; }
   }
+  return chg;
+}
+
+// The same run for a full tile row or column: length N and strides known at
+// compile time, so every shared-memory access is an immediate offset from one
+// base, the whole run is in registers and the chain is one add and one min
+// per step.
+template <int N, int DS, int WS>
+__device__ __forceinline__ bool sweep_run_fixed(float *c, const float *wlo, const float *whi) {
+  float o[N], v[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) o[i] = c[(i + 1) * DS];
+  float prev = c[0];
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    v[i] = fminf(__fadd_rn(prev, wlo[(i + 1) * WS]), o[i]);
+    prev = v[i];
+  }
+  prev = c[(N + 1) * DS];
+#pragma unroll
+  for (int i = N - 1; i >= 0; --i) {
+    v[i] = fminf(__fadd_rn(prev, whi[(i + 1) * WS]), v[i]);
+    prev = v[i];
+  }
+  bool chg = false;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+    if (v[i] < o[i]) {
+      c[(i + 1) * DS] = v[i];
+      chg = true;
+    }
+  return chg;
+}
+
+// B consecutive cells of a z-run (stride DS, weights stride WS), forward
+// (UP: from below, weights wdn) or backward (from above, weights wup), with
+// the chain value carried in `prev`.
+template <int B, int DS, int WS, bool UP>
+__device__ __forceinline__ bool zrun_block(float *c, const float *w, float &prev) {
+  float o[B], v[B];
+#pragma unroll
+  for (int i = 0; i < B; ++i) o[i] = c[i * DS];
+#pragma unroll
+  for (int k = 0; k < B; ++k) {
+    const int i = UP ? k : B - 1 - k;
+    v[i] = fminf(__fadd_rn(prev, w[i * WS]), o[i]);
+    prev = v[i];
+  }
+  bool chg = false;
+#pragma unroll
+  for (int i = 0; i < B; ++i)
+    if (v[i] < o[i]) {
+      c[i * DS] = v[i];
+      chg = true;
+    }
+  return chg;
+}
+
+// z-run of a column: cells col[z * DS] for z = 0..n-1 (no halo), forward with
+// wdn, then backward with wup, in register blocks of 6.
+template <int DS, int WS>
+__device__ __forceinline__ bool zrun(float *col, const float *wdn, const float *wup, int n) {
+  constexpr int B = 6;
+  bool chg = false;
+  float prev = __int_as_float(0x7f800000);
+  int z = 0;
+  for (; z + B <= n; z += B) chg |= zrun_block<B, DS, WS, true>(col + z * DS, wdn + z * WS, prev);
+  for (; z < n; ++z) chg |= zrun_block<1, DS, WS, true>(col + z * DS, wdn + z * WS, prev);
+  prev = __int_as_float(0x7f800000);
+  z = n;
+  for (; z >= B; z -= B) chg |= zrun_block<B, DS, WS, false>(col + (z - B) * DS, wup + (z - B) * WS, prev);
+  for (; z > 0; --z) chg |= zrun_block<1, DS, WS, false>(col + (z - 1) * DS, wup + (z - 1) * WS, prev);
   return chg;
 }
 
@@ -353,7 +414,7 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
     const int64_t d0 = dist_index<PRIV>(p, B, X0 + xx - 1, Y0 + yy - 1, B.z0);
     const int64_t dz = (!PRIV || B.dbase < 0) ? nxy : (int64_t)(B.x1 - B.x0 + 1) * (B.y1 - B.y0 + 1);
     const int s0 = yy * SX + xx, w0 = (yy - 1) * WSX + (xx - 1);
-#pragma unroll 6
+#pragma unroll 12
     for (int z = 0; z < nzb; ++z) {
       const int64_t node = n0 + z * nxy;
       const float dv = bits_f(__ldcg(&p.dist[d0 + z * dz]));
@@ -399,37 +460,51 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
   bool converged = false;
   int cyc = 0;
   const int nplan = nh * th + nv * tw;
+  const bool full = tw == TX && th == TY;
   for (; cyc < MAX_CYCLES; ++cyc) {
     if (threadIdx.x == 0) s_flags[(cyc + 1) % 3] = 0;
     bool chg = false;
-    for (int rr = threadIdx.x; rr < nplan; rr += (TX * TY)) {
-      float *cell;
-      int wo, ds, ws, n;
-      if (rr < nh * th) {  // x-run of an H-layer row
-        const int z = s_hl[rr / th], yy = rr % th + 1;
-        cell = sd + z * PS + yy * SX;
-        wo = z * WPS + (yy - 1) * WSX - 1;
-        ds = 1;
-        ws = 1;
-        n = tw;
-      } else {  // y-run of a V-layer column
-        const int q = rr - nh * th;
-        const int z = s_vl[q / tw], xx = q % tw + 1;
-        cell = sd + z * PS + xx;
-        wo = z * WPS + (xx - 1) - WSX;
-        ds = SX;
-        ws = WSX;
-        n = th;
+    if (full) {
+      for (int rr = threadIdx.x; rr < nplan; rr += (TX * TY)) {
+        if (rr < nh * TY) {  // x-run of an H-layer row
+          const int z = s_hl[rr / TY], yy = rr % TY + 1;
+          const int wo = z * WPS + (yy - 1) * WSX - 1;
+          chg |= sweep_run_fixed<TX, 1, 1>(sd + z * PS + yy * SX, wlo + wo, whi + wo);
+        } else {  // y-run of a V-layer column
+          const int q = rr - nh * TY;
+          const int z = s_vl[q / TX], xx = q % TX + 1;
+          const int wo = z * WPS + (xx - 1) - WSX;
+          chg |= sweep_run_fixed<TY, SX, WSX>(sd + z * PS + xx, wlo + wo, whi + wo);
+        }
       }
-      chg |= sweep_run(cell, ds, wlo + wo, whi + wo, ws, n);
+    } else {
+      for (int rr = threadIdx.x; rr < nplan; rr += (TX * TY)) {
+        float *cell;
+        int wo, ds, ws, n;
+        if (rr < nh * th) {  // x-run of an H-layer row
+          const int z = s_hl[rr / th], yy = rr % th + 1;
+          cell = sd + z * PS + yy * SX;
+          wo = z * WPS + (yy - 1) * WSX - 1;
+          ds = 1;
+          ws = 1;
+          n = tw;
+        } else {  // y-run of a V-layer column
+          const int q = rr - nh * th;
+          const int z = s_vl[q / tw], xx = q % tw + 1;
+          cell = sd + z * PS + xx;
+          wo = z * WPS + (xx - 1) - WSX;
+          ds = SX;
+          ws = WSX;
+          n = th;
+        }
+        chg |= sweep_run(cell, ds, wlo + wo, whi + wo, ws, n);
+      }
     }
     tile_sync<TX * TY, SPEC>();
     for (int c = threadIdx.x; c < tw * th; c += (TX * TY)) {
       const int xx = c % tw + 1, yy = c / tw + 1;
-      // the z run has no halo: start the forward pass at layer 0 itself
-      float *col = sd + yy * SX + xx - PS;
-      const int wo = (yy - 1) * WSX + (xx - 1) - WPS;
-      chg |= sweep_run(col, PS, wdn + wo, wup + wo, WPS, nzb, /*halo=*/false);
+      const int wo = (yy - 1) * WSX + (xx - 1);
+      chg |= zrun<PS, WPS>(sd + yy * SX + xx, wdn + wo, wup + wo, nzb);
     }
     if (chg) s_flags[cyc % 3] = 1;
     tile_sync<TX * TY, SPEC>();
@@ -442,23 +517,30 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
   }
 
   // ---- publish improvements; mark neighbour tiles whose halo changed
-  const int interior = nzb * th * tw;
-  for (int i = threadIdx.x; i < interior; i += (TX * TY)) {
-    const int z = i / (th * tw);
-    const int rem = i - z * th * tw;
-    const int yy = rem / tw + 1, xx = rem % tw + 1;
-    const float v = sd[z * PS + yy * SX + xx];
-    const int gz = B.z0 + z;
-    if (v < orig[z * WPS + (yy - 1) * WSX + (xx - 1)]) {
-      __stcg(&p.dist[dist_index<PRIV>(p, B, X0 + xx - 1, Y0 + yy - 1, gz)], f_bits(v));
-      const int ax = p.axis[gz];
-      if (ax == 1) {
-        if (xx == 1) s_act[0] = 1;
-        if (xx == tw) s_act[1] = 1;
-      } else if (ax == 2) {
-        if (yy == 1) s_act[2] = 1;
-        if (yy == th) s_act[3] = 1;
+  // one thread per column (x, y) of the tile, all its layers: the layer's
+  // axis decides which tile edge a changed cell activates
+  const int64_t dzs = (!PRIV || B.dbase < 0) ? nxy : (int64_t)(B.x1 - B.x0 + 1) * (B.y1 - B.y0 + 1);
+  for (int c = threadIdx.x; c < th * tw; c += (TX * TY)) {
+    const int yy = c / tw + 1, xx = c - (yy - 1) * tw + 1;
+    const int64_t d0 = dist_index<PRIV>(p, B, X0 + xx - 1, Y0 + yy - 1, B.z0);
+    const int s0 = yy * SX + xx, w0 = (yy - 1) * WSX + (xx - 1);
+    bool ex = false, ey = false;
+    for (int z = 0; z < nzb; ++z) {
+      const float v = sd[z * PS + s0];
+      if (v < orig[z * WPS + w0]) {
+        __stcg(&p.dist[d0 + z * dzs], f_bits(v));
+        const int ax = p.axis[B.z0 + z];
+        ex |= ax == 1;
+        ey |= ax == 2;
       }
+    }
+    if (ex) {
+      if (xx == 1) s_act[0] = 1;
+      if (xx == tw) s_act[1] = 1;
+    }
+    if (ey) {
+      if (yy == 1) s_act[2] = 1;
+      if (yy == th) s_act[3] = 1;
     }
   }
   if (threadIdx.x == 0 && !converged) s_act[4] = 1;
