@@ -364,7 +364,7 @@ struct LayerLists {
 
 template <int TX, int TY, bool PRIV, bool SPEC>
 __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *sd, LayerLists &L, int *s_flags,
-                                             int *s_act) {
+                                             int *s_act, int *s_nb = nullptr) {
   const int bi = box_of_tile(p, t);
   const LatBox B = load_box(p, bi);
   if (threadIdx.x == 0 && L.box != bi) {
@@ -402,35 +402,72 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
   if (threadIdx.x == 0) ts0 = dev_globaltimer();
   if (threadIdx.x < 5) s_act[threadIdx.x] = 0;
   if (threadIdx.x < 3) s_flags[threadIdx.x] = 0;
-  // ---- load.  Interior cells: distance and the four in-edge weights, four
-  // cells per thread in flight at a time.  Halo cells: only those the sweeps
-  // read (x-halo of H-layer rows, y-halo of V-layer columns).  Distances are
-  // read through L2 (other CTAs write them); weights are read-only.
-  // one thread per column (x, y) of the tile: its nzb cells' loads are
-  // issued back to back
-  for (int c = threadIdx.x; c < th * tw; c += (TX * TY)) {
-    const int yy = c / tw + 1, xx = c - (yy - 1) * tw + 1;
-    const int64_t n0 = (int64_t)B.z0 * nxy + col0 + (int64_t)(yy - 1) * p.nx + (xx - 1);
-    const int64_t d0 = dist_index<PRIV>(p, B, X0 + xx - 1, Y0 + yy - 1, B.z0);
-    const int64_t dz = (!PRIV || B.dbase < 0) ? nxy : (int64_t)(B.x1 - B.x0 + 1) * (B.y1 - B.y0 + 1);
-    const int s0 = yy * SX + xx, w0 = (yy - 1) * WSX + (xx - 1);
-#pragma unroll 12
-    for (int z = 0; z < nzb; ++z) {
-      const int64_t node = n0 + z * nxy;
-      const float dv = bits_f(__ldcg(&p.dist[d0 + z * dz]));
-      const float4 wv = __ldg(&p.w4[node]);
-      sd[z * PS + s0] = dv;
-      orig[z * WPS + w0] = dv;
-      wlo[z * WPS + w0] = wv.x;
-      whi[z * WPS + w0] = wv.y;
-      wdn[z * WPS + w0] = wv.z;
-      wup[z * WPS + w0] = wv.w;
-    }
+  if (s_nb && threadIdx.x < 4) {  // neighbour tiles in the box: left, right, down, up (-1: box edge)
+    const int d = threadIdx.x;
+    s_nb[d] = d == 0 ? (tx > 0 ? t - 1 : -1)
+                     : d == 1 ? (tx < B.ntx - 1 ? t + 1 : -1)
+                              : d == 2 ? (ty > 0 ? t - B.ntx : -1) : (ty < B.nty - 1 ? t + B.ntx : -1);
   }
+  // ---- load.  Interior cells: distance and the four in-edge weights; halo
+  // cells: only those the sweeps read (x-halo of H-layer rows, y-halo of
+  // V-layer columns).  Distances are read through L2 (other CTAs write them);
+  // weights are read-only.  A thread's first halo cells are loaded before its
+  // column (one thread per column (x, y), twelve layers in flight at a time),
+  // so their round trip overlaps the column's.
   {
-    // halo: 2 cells per H row and per V column
     const int nhh = 2 * nh * th, nvh = 2 * nv * tw;
-    for (int i = threadIdx.x; i < nhh + nvh; i += (TX * TY)) {
+    constexpr int HB = 4;  // halo cells per thread in the first batch
+    float hv[HB];
+    int hs[HB];
+#pragma unroll
+    for (int k = 0; k < HB; ++k) {
+      const int i = threadIdx.x + k * (TX * TY);
+      hs[k] = -1;
+      hv[k] = INF_F;
+      if (i < nhh + nvh) {
+        int z, xx, yy;
+        if (i < nhh) {
+          const int rowi = i >> 1;
+          z = s_hl[rowi / th];
+          yy = rowi % th + 1;
+          xx = (i & 1) ? tw + 1 : 0;
+        } else {
+          const int coli = (i - nhh) >> 1;
+          z = s_vl[coli / tw];
+          xx = coli % tw + 1;
+          yy = ((i - nhh) & 1) ? th + 1 : 0;
+        }
+        const int32_t gx = X0 + xx - 1, gy = Y0 + yy - 1;
+        hs[k] = z * PS + yy * SX + xx;
+        if (gx >= B.x0 && gx <= B.x1 && gy >= B.y0 && gy <= B.y1)
+          hv[k] = bits_f(__ldcg(&p.dist[dist_index<PRIV>(p, B, gx, gy, B.z0 + z)]));
+      }
+    }
+    // the thread's column (x, y) of the tile (th * tw <= threads)
+    const int c = threadIdx.x;
+    if (c < th * tw) {
+      const int yy = c / tw + 1, xx = c - (yy - 1) * tw + 1;
+      const int64_t n0 = (int64_t)B.z0 * nxy + col0 + (int64_t)(yy - 1) * p.nx + (xx - 1);
+      const int64_t d0 = dist_index<PRIV>(p, B, X0 + xx - 1, Y0 + yy - 1, B.z0);
+      const int64_t dz = (!PRIV || B.dbase < 0) ? nxy : (int64_t)(B.x1 - B.x0 + 1) * (B.y1 - B.y0 + 1);
+      const int s0 = yy * SX + xx, w0 = (yy - 1) * WSX + (xx - 1);
+#pragma unroll 12
+      for (int z = 0; z < nzb; ++z) {
+        const float dv = bits_f(__ldcg(&p.dist[d0 + z * dz]));
+        const float4 wv = __ldg(&p.w4[n0 + z * nxy]);
+        const int wi = z * WPS + w0;
+        sd[z * PS + s0] = dv;
+        orig[wi] = dv;
+        wlo[wi] = wv.x;
+        whi[wi] = wv.y;
+        wdn[wi] = wv.z;
+        wup[wi] = wv.w;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < HB; ++k)
+      if (hs[k] >= 0) sd[hs[k]] = hv[k];
+    for (int i = threadIdx.x + HB * (TX * TY); i < nhh + nvh; i += (TX * TY)) {
       int z, xx, yy;
       if (i < nhh) {
         const int rowi = i >> 1;
@@ -570,7 +607,7 @@ __device__ __forceinline__ int revisit_list(const LatParams &p, int t, const int
 }
 
 template <int TX, int TY, bool PRIV>
-__global__ void __launch_bounds__(TX * TY) lattice_tile_kernel(LatParams p) {
+__global__ void __launch_bounds__(TX * TY, 1) lattice_tile_kernel(LatParams p) {
   extern __shared__ float sd[];
   __shared__ LayerLists s_layers;
   __shared__ int s_flags[3];
@@ -643,27 +680,25 @@ __device__ void queue_tile(const LatParams &p, int t) {
 // recorded as an internal error by the caller).
 __device__ bool activate_tile(const LatParams &p, int t) {
   for (int tries = 0; tries < 1024; ++tries) {
-    const int st = (int)ld_acquire_u32((const unsigned *)&p.tstate[t]);
-    if (st == 1 || st == 3) return true;
+    const int st = atomicCAS(&p.tstate[t], 0, 1);
     if (st == 0) {
-      if (atomicCAS(&p.tstate[t], 0, 1) == 0) {
-        atomicAdd(&p.ctl->pending, 1);
-        queue_tile(p, t);
-        return true;
-      }
-    } else if (st == 2) {
-      if (atomicCAS(&p.tstate[t], 2, 3) == 2) return true;
+      atomicAdd(&p.ctl->pending, 1);
+      queue_tile(p, t);
+      return true;
     }
+    if (st == 1 || st == 3) return true;
+    if (atomicCAS(&p.tstate[t], 2, 3) == 2) return true;  // visiting: mark dirty
   }
   return false;
 }
 
 template <int TX, int TY, bool PRIV>
-__global__ void __launch_bounds__(TX * TY) lattice_async_kernel(LatParams p) {
+__global__ void __launch_bounds__(TX * TY, 1) lattice_async_kernel(LatParams p) {
   extern __shared__ float sd[];
   __shared__ LayerLists s_layers;
   __shared__ int s_flags[3];
   __shared__ int s_act[5];
+  __shared__ int s_nb[4];
   __shared__ int s_tile;
   LatCtl *ctl = p.ctl;
   const unsigned long long t_start = dev_globaltimer();
@@ -709,24 +744,14 @@ __global__ void __launch_bounds__(TX * TY) lattice_async_kernel(LatParams p) {
     const int t = s_tile;
     __syncthreads();
     if (t < 0) break;
-    process_tile<TX, TY, PRIV, false>(p, t, sd, s_layers, s_flags, s_act);
+    process_tile<TX, TY, PRIV, false>(p, t, sd, s_layers, s_flags, s_act, s_nb);
     // neighbours are activated by threads 0..3 in parallel, after this
     // tile's distances are visible
     unsigned long long ta = 0;
     if (threadIdx.x == 0) ta = dev_globaltimer();
     if (threadIdx.x < 4) {
       __threadfence();
-      const LatBox B = load_box(p, box_of_tile(p, t));
-      const int lt = t - B.tile0;
-      const int tx = lt % B.ntx, ty = lt / B.ntx;
-      const int d = threadIdx.x;
-      int nb = -1;
-      if (s_act[d]) {
-        if (d == 0 && tx > 0) nb = t - 1;
-        if (d == 1 && tx < B.ntx - 1) nb = t + 1;
-        if (d == 2 && ty > 0) nb = t - B.ntx;
-        if (d == 3 && ty < B.nty - 1) nb = t + B.ntx;
-      }
+      const int nb = s_act[threadIdx.x] ? s_nb[threadIdx.x] : -1;
       if (nb >= 0 && !activate_tile(p, nb)) atomicCAS(&ctl->err, DEV_OK, DEV_ERR_INTERNAL);
     }
     __syncthreads();
