@@ -344,6 +344,36 @@ __device__ __forceinline__ bool zrun(float *col, const float *wdn, const float *
 // weights [4][nzb][TY][TX+1] and the interior distances as loaded
 // [nzb][TY][TX+1] (odd row strides: the row walks of the x-sweep and the
 // column walks of the y- and z-sweeps are bank-conflict free).
+// The distances and in-edge weights of one tile column (cells s0 + z * PS /
+// w0 + z * WPS in shared memory) in blocks of ZB layers, each block's loads
+// all issued before its stores.
+template <int ZB, int PS, int WPS>
+__device__ __forceinline__ void load_column_blocks_impl(const LatParams &p, int nzb, int64_t d0, int64_t dz,
+                                                        int64_t n0, int64_t nxy, float *sd, float *orig, float *wlo,
+                                                        float *whi, float *wdn, float *wup, int s0, int w0) {
+  for (int zb = 0; zb < nzb; zb += ZB) {
+    float dv[ZB];
+    float4 wv[ZB];
+#pragma unroll
+    for (int k = 0; k < ZB; ++k)
+      if (zb + k < nzb) {
+        dv[k] = bits_f(__ldcg(&p.dist[d0 + (zb + k) * dz]));
+        wv[k] = __ldg(&p.w4[n0 + (zb + k) * nxy]);
+      }
+#pragma unroll
+    for (int k = 0; k < ZB; ++k)
+      if (zb + k < nzb) {
+        const int z = zb + k, wi = z * WPS + w0;
+        sd[z * PS + s0] = dv[k];
+        orig[wi] = dv[k];
+        wlo[wi] = wv[k].x;
+        whi[wi] = wv[k].y;
+        wdn[wi] = wv[k].z;
+        wup[wi] = wv[k].w;
+      }
+  }
+}
+
 // Barrier of the threads that visit tiles: the whole block, or (SPEC) the
 // first NW threads only - named barrier 1 - while a scheduler warp runs beside
 // them.
@@ -362,7 +392,7 @@ struct LayerLists {
   int box;
 };
 
-template <int TX, int TY, bool PRIV, bool SPEC>
+template <int TX, int TY, bool PRIV, bool SPEC, bool DEEP = false>
 __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *sd, LayerLists &L, int *s_flags,
                                              int *s_act, int *s_nb = nullptr) {
   const int bi = box_of_tile(p, t);
@@ -412,8 +442,8 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
   // cells: only those the sweeps read (x-halo of H-layer rows, y-halo of
   // V-layer columns).  Distances are read through L2 (other CTAs write them);
   // weights are read-only.  A thread's first halo cells are loaded before its
-  // column (one thread per column (x, y), twelve layers in flight at a time),
-  // so their round trip overlaps the column's.
+  // column (one thread per column (x, y), up to 18 layers in flight at a
+  // time), so their round trip overlaps the column's.
   {
     const int nhh = 2 * nh * th, nvh = 2 * nv * tw;
     constexpr int HB = 4;  // halo cells per thread in the first batch
@@ -451,17 +481,24 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
       const int64_t d0 = dist_index<PRIV>(p, B, X0 + xx - 1, Y0 + yy - 1, B.z0);
       const int64_t dz = (!PRIV || B.dbase < 0) ? nxy : (int64_t)(B.x1 - B.x0 + 1) * (B.y1 - B.y0 + 1);
       const int s0 = yy * SX + xx, w0 = (yy - 1) * WSX + (xx - 1);
+      if constexpr (DEEP) {
+        // boxes of more than 12 layers: blocks of 18 layers, each fully
+        // unrolled and predicated, every load of a block issued before its
+        // stores (one round trip for up to 18 layers)
+        load_column_blocks_impl<18, PS, WPS>(p, nzb, d0, dz, n0, nxy, sd, orig, wlo, whi, wdn, wup, s0, w0);
+      } else {  // twelve layers in flight
 #pragma unroll 12
-      for (int z = 0; z < nzb; ++z) {
-        const float dv = bits_f(__ldcg(&p.dist[d0 + z * dz]));
-        const float4 wv = __ldg(&p.w4[n0 + z * nxy]);
-        const int wi = z * WPS + w0;
-        sd[z * PS + s0] = dv;
-        orig[wi] = dv;
-        wlo[wi] = wv.x;
-        whi[wi] = wv.y;
-        wdn[wi] = wv.z;
-        wup[wi] = wv.w;
+        for (int z = 0; z < nzb; ++z) {
+          const float dv = bits_f(__ldcg(&p.dist[d0 + z * dz]));
+          const float4 wv = __ldg(&p.w4[n0 + z * nxy]);
+          const int wi = z * WPS + w0;
+          sd[z * PS + s0] = dv;
+          orig[wi] = dv;
+          wlo[wi] = wv.x;
+          whi[wi] = wv.y;
+          wdn[wi] = wv.z;
+          wup[wi] = wv.w;
+        }
       }
     }
 #pragma unroll
@@ -692,7 +729,10 @@ __device__ bool activate_tile(const LatParams &p, int t) {
   return false;
 }
 
-template <int TX, int TY, bool PRIV>
+// DEEP: the instantiation for tiles of more than 12 layers (the column load
+// in 18-layer blocks); compiled separately so that each layer range gets its
+// own register allocation.
+template <int TX, int TY, bool PRIV, bool DEEP = false>
 __global__ void __launch_bounds__(TX * TY, 1) lattice_async_kernel(LatParams p) {
   extern __shared__ float sd[];
   __shared__ LayerLists s_layers;
@@ -744,7 +784,7 @@ __global__ void __launch_bounds__(TX * TY, 1) lattice_async_kernel(LatParams p) 
     const int t = s_tile;
     __syncthreads();
     if (t < 0) break;
-    process_tile<TX, TY, PRIV, false>(p, t, sd, s_layers, s_flags, s_act, s_nb);
+    process_tile<TX, TY, PRIV, false, DEEP>(p, t, sd, s_layers, s_flags, s_act, s_nb);
     // neighbours are activated by threads 0..3 in parallel, after this
     // tile's distances are visible
     unsigned long long ta = 0;
@@ -970,7 +1010,13 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   const bool spec = async && env_u64("ORSP_LAT_SPEC", 0) != 0;
   void *kfn;
   if (spec) kfn = priv ? (void *)lattice_spec_kernel<TX, TY, true> : (void *)lattice_spec_kernel<TX, TY, false>;
-  else if (async) kfn = priv ? (void *)lattice_async_kernel<TX, TY, true> : (void *)lattice_async_kernel<TX, TY, false>;
+  else if (async) {
+    kfn = priv ? (void *)lattice_async_kernel<TX, TY, true> : (void *)lattice_async_kernel<TX, TY, false>;
+    if constexpr (TX == 16) {  // deeper tiles: the instantiation with 18-layer column loads
+      if (nzb > 12)
+        kfn = priv ? (void *)lattice_async_kernel<TX, TY, true, true> : (void *)lattice_async_kernel<TX, TY, false, true>;
+    }
+  }
   else kfn = priv ? (void *)lattice_tile_kernel<TX, TY, true> : (void *)lattice_tile_kernel<TX, TY, false>;
   const int threads = TX * TY + (spec ? 32 : 0);
   ORSP_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

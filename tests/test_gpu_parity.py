@@ -413,6 +413,55 @@ def test_find_paths_on_rois_local_csr_batch():
     assert got == refs
 
 
+@pytest.mark.parametrize("impl", ["lattice16", "lattice16-rounds"])
+@pytest.mark.parametrize("shape", [(40, 36, 18), (35, 29, 13)])
+def test_deep_lattice_bit_exact(shape, impl, monkeypatch):
+    """Lattices and boxes of more than 12 layers (the tile kernel's deep
+    instantiation, with the column load in 18-layer blocks): full-search
+    distances, box paths in boxes deeper and shallower than 12 layers, and
+    batched box searches with a distance slice per box, all equal to the
+    oracle."""
+    _lattice_env(monkeypatch, impl)
+    lat = build_lattice(*shape)
+    w = uniform_weights(lat, seed=sum(shape), blocked_frac=0.04)
+    dg = DeviceGraph.from_lattice(lat)
+    wt = cuda(w)
+    rng = np.random.default_rng(3)
+    for s in rng.choice(lat.N, size=2, replace=False):
+        _, ref_dist, _, _ = O.dijkstra(lat.indptr, lat.indices, w, [int(s)])
+        dist = torch.empty(lat.N, dtype=torch.float32, device="cuda")
+        st, _, _ = dg.sssp(wt, int(s), -1, dist_out=dist)
+        assert st == _lib.ORSP_OK
+        assert np.array_equal(_bits(dist.cpu().numpy()), _bits(ref_dist)), f"src {s}"
+    nx, ny, nz = shape
+    nxy = nx * ny
+    for b in [(0, nx - 1, 0, ny - 1, 0, nz - 1), (3, nx - 5, 2, ny - 4, 0, nz - 1), (5, 30, 4, 20, 2, 9)]:
+        x0, x1, y0, y1, z0, z1 = b
+        g2r = np.full(lat.N, -1, np.int32)
+        zz, yy, xx = np.meshgrid(np.arange(z0, z1 + 1), np.arange(y0, y1 + 1), np.arange(x0, x1 + 1), indexing="ij")
+        inside = (zz * nxy + yy * nx + xx).ravel()
+        g2r[inside] = np.arange(inside.size, dtype=np.int32)
+        for _ in range(3):
+            s, d = (int(inside[rng.integers(inside.size)]) for _ in range(2))
+            refp, *_ = O.dijkstra(lat.indptr, lat.indices, w, [s], dst=d, roi_map=g2r)
+            st, p, _ = dg.sssp_box(wt, s, d, b)
+            got = p.cpu().tolist() if (st == _lib.ORSP_OK and p is not None) else []
+            assert got == (refp.tolist() if len(refp) > 1 else []), f"box {b} {s}->{d}"
+    dg.set_batch_plan([{"max_nodes": 1 << 40, "impl": 1, "tile_w": 16}])
+    boxes, src, dst = random_boxes(lat, 40, seed=11, lo=(4, 4, 13), hi=(nx, ny, nz))
+    cap = 1024
+    nodes, edges, lens = dg.batch_bbox(wt, cuda(src), cuda(dst), cuda(boxes), path_cap=cap)
+    ref_nodes, ref_lens = O.batch_bbox(lat.indptr, lat.indices, w, nx, ny, nz, src, dst, boxes, cap)
+    lens, nodes, edges = lens.cpu().numpy(), nodes.cpu().numpy(), edges.cpu().numpy()
+    for k in range(len(src)):
+        L = int(ref_lens[k])
+        if L < 2:
+            assert lens[k] < 2, f"search {k}: oracle has no path"
+            continue
+        assert lens[k] == L and np.array_equal(nodes[k, :L], ref_nodes[k, :L]), f"search {k}"
+        assert np.array_equal(edges[k, : L - 1], O.path_to_edges(lat.indptr, lat.indices, ref_nodes[k, :L]))
+
+
 @pytest.mark.parametrize("impl", ["lattice16", "lattice32", "lattice16-rounds", "lattice16-spec", "generic"])
 def test_sssp_box_matches_box_roi_and_oracle(impl, monkeypatch):
     """orsp_sssp_box == orsp_sssp with the box's ROI map == the oracle with that
