@@ -1,0 +1,240 @@
+"""Headless routing of an .ORP board into an .ORS solution on the GPU path.
+
+    python -m orthoroute_b200.headless board.ORP [-o board.ORS] [--max-iterations 200]
+                                       [--mode batched|plain] [--warm] [--pitch 0.4]
+
+The steps are those of the reference's `main.py headless` (main.py:287-622):
+read the board (orp.read_orp / orp_to_board_data), build the routing lattice
+and the pad-to-pad tasks, route with negotiated congestion, emit tracks and
+vias, write the solution (ors.write_ors).  The board -> problem mapping
+follows the reference's router:
+
+* routing area: the pads of nets with two or more pads, plus 3 mm
+  (PathFinderRouter._calc_bounds, unified_pathfinder.py:2254-2306); the board
+  outline plus 3 mm when no net has two pads;
+* grid: origin and extent rounded to the pitch, `int(span / pitch) + 1`
+  steps (KiCadGeometry, pathfinder/kicad_geometry.py:23-34); F.Cu vertical,
+  then alternating horizontal / vertical (kicad_geometry.py:41-49);
+* pads: snapped to the nearest grid point, clamped, on their layer (the index
+  of their first layer name; F.Cu otherwise) under the reference's pad keys,
+  later pads with the same key replacing earlier ones (_pad_key / _map_pads,
+  unified_pathfinder.py:2308-2385);
+* tasks: each net's first two pads (_parse_requests,
+  unified_pathfinder.py:2600-2650), a net whose two pads share a grid point
+  being a one-node route.
+
+Routing uses this package's lattice (planar edges on the inner layers of a
+board with more than two layers, vias between adjacent layers, base cost 1
+per grid step and 3 per via) and negotiate.PathFinder.  Pads are routed pad
+to pad: the reference's pad-escape portals (its default) are not planned here.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+from .lattice import Lattice, build_lattice, layer_directions
+from .orp import default_layer_names, orp_to_board_data, read_orp
+
+ROUTING_MARGIN = 3.0  # mm
+DEFAULT_PITCH = 0.4  # mm, the reference router's grid pitch
+
+
+@dataclass
+class HeadlessProblem:
+    lattice: Lattice
+    names: List[str]  # nets with a task, board order
+    src: np.ndarray  # int32 node ids
+    dst: np.ndarray
+    trivial: Dict[str, int]  # nets whose two pads share a grid point -> that node
+    grid_min_x: float
+    grid_min_y: float
+    pitch: float
+    layer_names: List[str]
+    layer_dirs: List[str]
+    pad_nodes: Dict[str, int] = field(default_factory=dict)
+
+
+def routing_bounds(board_data: dict) -> Tuple[float, float, float, float]:
+    xs, ys = [], []
+    for net in board_data.get("nets", {}).values():
+        pads = net.get("pads", [])
+        if len(pads) >= 2:
+            xs += [p.get("x", 0.0) for p in pads]
+            ys += [p.get("y", 0.0) for p in pads]
+    if xs:
+        return (min(xs) - ROUTING_MARGIN, min(ys) - ROUTING_MARGIN, max(xs) + ROUTING_MARGIN,
+                max(ys) + ROUTING_MARGIN)
+    b = board_data.get("bounds")
+    if b:
+        return (b[0] - ROUTING_MARGIN, b[1] - ROUTING_MARGIN, b[2] + ROUTING_MARGIN, b[3] + ROUTING_MARGIN)
+    return (0.0, 0.0, 100.0, 100.0)
+
+
+def grid_geometry(bounds, pitch: float):
+    """(grid_min_x, grid_min_y, x_steps, y_steps) with the reference's float
+    arithmetic (Python round: half to even)."""
+    min_x, min_y, max_x, max_y = bounds
+    gx0, gy0 = round(min_x / pitch) * pitch, round(min_y / pitch) * pitch
+    gx1, gy1 = round(max_x / pitch) * pitch, round(max_y / pitch) * pitch
+    return gx0, gy0, int((gx1 - gx0) / pitch) + 1, int((gy1 - gy0) / pitch) + 1
+
+
+def _pad_key(pad: dict, comp: str, pad_id: str) -> str:
+    if comp == "GENERIC_COMPONENT":
+        return f"{comp}_{pad_id}@{int(round(pad.get('x', 0.0) * 1000))},{int(round(pad.get('y', 0.0) * 1000))}"
+    return f"{comp}_{pad_id}"
+
+
+def build_problem(board_data: dict, pitch: float = DEFAULT_PITCH) -> HeadlessProblem:
+    """The routing lattice and tasks of a board_data dict."""
+    nz = int(board_data.get("layers", 2))
+    names = list(board_data.get("layer_names") or [])
+    if len(names) < nz:
+        names = default_layer_names(nz)
+    gx0, gy0, nx, ny = grid_geometry(routing_bounds(board_data), pitch)
+    lat = build_lattice(nx, ny, nz, planar="inner" if nz > 2 else "all", vias="adjacent")
+    plane = nx * ny
+
+    def pad_id(p):
+        return p.get("name", p.get("id", "")) or p.get("id", "")
+
+    def snap(p) -> int:
+        xi = min(max(round((p.get("x", 0.0) - gx0) / pitch), 0), nx - 1)
+        yi = min(max(round((p.get("y", 0.0) - gy0) / pitch), 0), ny - 1)
+        lay = (p.get("layers") or ["F.Cu"])[0]
+        z = names.index(lay) if lay in names else 0
+        return z * plane + yi * nx + xi
+
+    # components in the order the reference's headless flow builds them: the
+    # board's component list, then components first seen on net pads
+    order: List[str] = []
+    members: Dict[str, List[dict]] = {}
+    for c in board_data.get("components", []):
+        ref = c.get("reference", c.get("id", ""))
+        if ref and ref not in members:
+            members[ref] = []
+            order.append(ref)
+    for net in board_data.get("nets", {}).values():
+        for p in net.get("pads", []):
+            if not isinstance(p, dict):
+                continue
+            comp = p.get("component", "") or "GENERIC_COMPONENT"
+            if comp not in members:
+                members[comp] = []
+                order.append(comp)
+            members[comp].append(p)
+    pad_nodes: Dict[str, int] = {}
+    for comp in order:
+        for p in members[comp]:
+            pad_nodes[_pad_key(p, comp, pad_id(p))] = snap(p)
+
+    tnames, src, dst, trivial = [], [], [], {}
+    for net_id, net in board_data.get("nets", {}).items():
+        pads = [p for p in net.get("pads", []) if isinstance(p, dict)]
+        if len(pads) < 2:
+            continue
+        k1 = _pad_key(pads[0], pads[0].get("component", "") or "GENERIC_COMPONENT", pad_id(pads[0]))
+        k2 = _pad_key(pads[1], pads[1].get("component", "") or "GENERIC_COMPONENT", pad_id(pads[1]))
+        s, d = pad_nodes[k1], pad_nodes[k2]
+        if s != d:
+            tnames.append(net_id)
+            src.append(s)
+            dst.append(d)
+        else:
+            trivial[net_id] = s
+    return HeadlessProblem(lat, tnames, np.asarray(src, np.int32), np.asarray(dst, np.int32), trivial, gx0, gy0,
+                           pitch, names, layer_directions(nz), pad_nodes)
+
+
+def headless_config(max_iterations: int = 200):
+    """The negotiation schedule of headless runs: per-net live costs, only
+    offending nets rerouted, bbox + 10-cell ROIs with a full-lattice retry,
+    first-fit rounds of disjoint boxes."""
+    from .negotiate import NegotiationConfig
+    return NegotiationConfig(max_iterations=max_iterations, cost_update="net", reroute="offenders", roi_margin=10,
+                             full_graph_retry=True, net_order="disjoint")
+
+
+def route_board(board_data: dict, pitch: float = DEFAULT_PITCH, max_iterations: int = 200, mode: str = "batched",
+                warm: bool = False, config=None, device=None, log=None):
+    """Routes a board_data dict on the GPU (mode 'batched' or 'sequential').
+    Returns (problem, RouteResult, tracks, vias, iteration metrics)."""
+    from .geometry import generate_geometry
+    from .negotiate import PathFinder
+
+    prob = build_problem(board_data, pitch)
+    cfg = config or headless_config(max_iterations)
+    pf = PathFinder(prob.lattice, config=cfg, device=device)
+    hist = None
+    if warm:
+        from .warm import load_pretrained, warm_history
+        net, scale = load_pretrained(device=pf.device)
+        hist = warm_history(net, prob.lattice, prob.src, prob.dst, scale)
+    metrics = []
+
+    def cb(s):
+        metrics.append({"iteration": s.iteration, "overuse": s.over_cnt, "overflow": s.over_sum,
+                        "nets_routed": s.routed, "iteration_time": s.seconds})
+        if log:
+            log(f"iteration {s.iteration}: overuse {s.over_sum}/{s.over_cnt}, routed {s.routed}, {s.seconds:.2f} s")
+
+    res = pf.route(prob.src, prob.dst, mode=mode, callback=cb, history_init=hist)
+    net_paths = {}
+    for name, path in zip(prob.names, res.paths):
+        net_paths[name] = [int(v) for v in path] if path is not None and len(path) >= 2 else []
+    for name, node in prob.trivial.items():
+        net_paths[name] = [int(node)]
+    tracks, vias = generate_geometry(pf.dg, net_paths, prob.layer_dirs, prob.grid_min_x, prob.grid_min_y, pitch,
+                                     prob.layer_names, pitch)
+    return prob, res, tracks, vias, metrics
+
+
+def run_headless(orp_file: str, output_file: Optional[str] = None, max_iterations: int = 200,
+                 mode: str = "batched", warm: bool = False, pitch: float = DEFAULT_PITCH, log=print) -> dict:
+    """ORP in, ORS out; returns a summary of the run."""
+    from .ors import GeometryPayload, write_ors
+
+    t0 = time.perf_counter()
+    board_data = orp_to_board_data(read_orp(orp_file))
+    out = Path(output_file) if output_file else Path(orp_file).with_suffix(".ORS")
+    prob, res, tracks, vias, metrics = route_board(board_data, pitch, max_iterations, mode, warm, log=log)
+    total = time.perf_counter() - t0
+    routed = sum(1 for p in res.paths if p is not None and len(p) >= 2) + len(prob.trivial)
+    meta = {"orthoroute_version": "0.1.0", "board_name": board_data.get("filename", "board"), "total_time": total,
+            "iterations": len(metrics), "total_iterations": len(metrics), "converged": bool(res.converged),
+            "barrel_conflicts": 0, "nets_routed": routed, "wirelength": float(res.wirelength),
+            "via_count": len(vias), "track_count": len(tracks),
+            "overflow": metrics[-1]["overflow"] if metrics else 0}
+    write_ors(GeometryPayload(tracks, vias), metrics, meta, out)
+    summary = {"ors": str(out), "nets": len(prob.names) + len(prob.trivial), "routed": routed,
+               "converged": bool(res.converged), "iterations": len(metrics), "tracks": len(tracks),
+               "vias": len(vias), "seconds_total": round(total, 3), "seconds_route": round(res.seconds, 3),
+               "lattice": [prob.lattice.nx, prob.lattice.ny, prob.lattice.nz]}
+    if log:
+        log(json.dumps(summary))
+    return summary
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description="Route an .ORP board on the GPU and write an .ORS solution")
+    ap.add_argument("orp")
+    ap.add_argument("-o", "--output", default=None)
+    ap.add_argument("--max-iterations", type=int, default=200)
+    ap.add_argument("--mode", choices=["batched", "plain"], default="batched")
+    ap.add_argument("--warm", action="store_true", help="start from the learned history prediction")
+    ap.add_argument("--pitch", type=float, default=DEFAULT_PITCH)
+    a = ap.parse_args(argv)
+    s = run_headless(a.orp, a.output, a.max_iterations, "batched" if a.mode == "batched" else "sequential", a.warm,
+                     a.pitch)
+    return 0 if s["converged"] else 1
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

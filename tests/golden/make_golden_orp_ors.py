@@ -1,0 +1,189 @@
+"""Golden files for the .ORP / .ORS formats and the headless board mapping,
+produced by the reference's own code on a hand-made board.
+
+    python tests/golden/make_golden_orp_ors.py [--ref /root/reference]
+
+From the reference (orthoroute/infrastructure/serialization/orp_exporter.py,
+ors_exporter.py, main.py and algorithms/manhattan/unified_pathfinder.py):
+
+  golden_board.orp          export_board_to_orp(board_data dict)
+  golden_orp.json           {"board_data": the input dict,
+                             "converted": convert_orp_to_board_data(import_board_from_orp(golden_board.orp)),
+                             "mapping": grid and pad-to-pad tasks of UnifiedPathFinder.initialize_graph +
+                                        _parse_requests (portals off) on the Board main.py builds}
+  golden_solution.ors       export_solution_to_ors(payload, metrics, metadata)
+  golden_ors.json           {"inputs": payload / metrics / metadata,
+                             "imported": import_solution_from_ors(golden_solution.ors),
+                             "payload": convert_ors_to_geometry_payload(...) tracks and vias}
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import logging
+import os
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+
+
+def board_data():
+    """Pads of several kinds: component pads, pads without a component, a
+    through-hole pad, a B.Cu pad, an unconnected pad; nets of 1, 2 and 3 pads,
+    pads near a rounding tie of the grid (SHORT) and a net whose two pads
+    share a grid point (SAME)."""
+    names = ["F.Cu", "In1.Cu", "In2.Cu", "In3.Cu", "In4.Cu", "B.Cu"]
+    pads = []
+
+    def pad(comp, name, net, x, y, layers=("F.Cu",), drill=None):
+        pads.append({"component": comp, "name": name, "net_name": net, "net_code": 0, "x": x, "y": y,
+                     "width": 0.3, "height": 0.3, "drill": drill, "layers": list(layers), "type": "smd"})
+
+    for i in range(6):
+        pad("J1", str(i + 1), f"D{i}", 101.2 + 0.8 * i, 52.0)
+        pad("U2", f"A{i + 1}", f"D{i}", 104.0 + 1.2 * i, 61.7 - 0.4 * i)
+    pad("U2", "B1", "CLK", 108.3, 58.1)
+    pad("J1", "7", "CLK", 99.9, 50.3, layers=names, drill=0.8)
+    pad("", "", "CLK", 112.5, 55.55)
+    pad("R3", "1", "VBUS", 110.0, 49.8, layers=("B.Cu",))
+    pad("R3", "2", "VBUS", 103.0, 63.1)
+    pad("", "", "ALONE", 106.0, 57.0)
+    pad("U2", "B2", "", 107.0, 59.0)
+    pad("TP1", "1", "SHORT", 105.01, 54.99)
+    pad("TP2", "1", "SHORT", 105.05, 55.02)
+    pad("TP3", "1", "SAME", 106.4, 56.4)
+    pad("TP4", "1", "SAME", 106.45, 56.42)
+    nets = {}
+    for p in pads:
+        if p["net_name"]:
+            nets.setdefault(p["net_name"], {"name": p["net_name"], "code": 0, "pads": []})["pads"].append(p)
+    return {"filename": "golden.kicad_pcb", "x_min": 95.0, "y_min": 45.0, "x_max": 120.0, "y_max": 70.0,
+            "width": 25.0, "height": 25.0, "layers": len(names), "layer_names": names, "pads": pads, "nets": nets,
+            "grid_resolution": 0.4, "clearance": 0.15, "track_width": 0.2, "via_diameter": 0.5, "via_drill": 0.25}
+
+
+def reference_mapping(bd, upf_mod, models):
+    """Grid and tasks as main.py's headless flow builds them (main.py:355-422),
+    with the portals off (pad-to-pad tasks)."""
+    Board, Net, Pad, Component, Coordinate = models
+    board = Board(id="headless-board", name=bd.get("filename", "board"), layer_count=bd.get("layers", 2))
+    board.nets = []
+    comps = {}
+    for c in bd.get("components", []):
+        cid = c.get("reference", c.get("id", ""))
+        if cid:
+            comps[cid] = Component(id=cid, reference=cid, value=c.get("value", ""), footprint=c.get("footprint", ""),
+                                   position=Coordinate(x=c.get("x", 0.0), y=c.get("y", 0.0)),
+                                   angle=c.get("rotation", 0.0))
+    for net_id, info in bd.get("nets", {}).items():
+        net = Net(id=net_id, name=info.get("name", net_id))
+        net.pads = []
+        for pr in info.get("pads", []):
+            pname = pr.get("name", pr.get("id", ""))
+            cid = pr.get("component", "")
+            p = Pad(id=pname or pr.get("id", "pad"), component_id=cid, net_id=net_id,
+                    position=Coordinate(x=pr.get("x", 0.0), y=pr.get("y", 0.0)),
+                    size=(pr.get("width", 0.2), pr.get("height", 0.2)), drill_size=pr.get("drill"),
+                    layer=pr.get("layers", ["F.Cu"])[0] if pr.get("layers") else "F.Cu")
+            net.pads.append(p)
+            if not cid:
+                cid = "GENERIC_COMPONENT"
+                p.component_id = cid
+            if cid not in comps:
+                comps[cid] = Component(id=cid, reference=cid, value="", footprint="",
+                                       position=Coordinate(x=p.position.x, y=p.position.y), pads=[])
+            comps[cid].pads.append(p)
+        board.nets.append(net)
+    board.components = list(comps.values())
+    board._kicad_bounds = bd.get("bounds", None)
+    board.layer_names = bd.get("layer_names", [])
+    cfg = upf_mod.PathFinderConfig()
+    cfg.portal_enabled = False
+    pf = upf_mod.UnifiedPathFinder(config=cfg, use_gpu=False)
+    pf.initialize_graph(board)
+    tasks = pf._parse_requests(board.nets)
+    g = pf.lattice.geom
+    return {"x_steps": int(g.x_steps), "y_steps": int(g.y_steps), "layers": int(pf.lattice.layers),
+            "grid_min_x": float(g.grid_min_x), "grid_min_y": float(g.grid_min_y), "pitch": float(g.pitch),
+            "layer_directions": list(g.layer_directions), "tasks": {k: [int(a), int(b)] for k, (a, b) in tasks.items()},
+            "trivial": {k: int(v[0]) for k, v in pf.net_paths.items() if len(v) == 1}}
+
+
+def ors_inputs():
+    tracks = [
+        {"net": "D0", "layer": "In1.Cu", "x1": 101.2, "y1": 52.0, "x2": 101.2, "y2": 55.6, "width": 0.24},
+        {"net": "D0", "layer": "In2.Cu", "x1": 101.2, "y1": 55.6, "x2": 104.0, "y2": 55.6, "width": 0.24},
+        {"net_id": "CLK", "layer": "In3.Cu", "start": (99.9, 50.3), "end": (108.3, 50.3), "width": 0.2},
+        {"net_id": "VBUS", "layer": "In4.Cu", "start_x": 110.0, "start_y": 49.8, "end_x": 110.0, "end_y": 63.1},
+        {"layer": "In1.Cu", "x1": 1.0, "y1": 2.0, "x2": 3.0, "y2": 2.0},
+    ]
+    vias = [
+        {"net": "D0", "x": 101.2, "y": 52.0, "from_layer": "F.Cu", "to_layer": "In1.Cu", "diameter": 0.5,
+         "drill": 0.25},
+        {"net_id": "CLK", "position": (108.3, 50.3), "from_layer": "In3.Cu", "to_layer": "F.Cu", "size": 0.6,
+         "drill": 0.3},
+        {"net_id": "VBUS", "position": {"x": 110.0, "y": 63.1}, "from_layer": "In4.Cu", "to_layer": "B.Cu"},
+        {"net": "ALONE"},
+    ]
+    metrics = [
+        {"iteration": 1, "overuse": 12, "routed_nets": 7, "overflow": 30.5},
+        {"iteration": 2, "overuse_count": 3, "nets_routed": 8, "overflow_cost": 4.0, "wirelength": 88.2,
+         "vias": 9, "time": 0.25},
+        {"iteration": 3, "overuse": 0, "routed": 8, "iteration_time": 0.5, "via_count": 10},
+    ]
+    metadata = {"orthoroute_version": "0.2.0", "total_time": 12.5, "iterations": 3, "converged": True,
+                "barrel_conflicts": 0, "nets_routed": 8, "wirelength": 90.0, "via_count": 4, "track_count": 5,
+                "overflow": 0, "board_name": "golden"}
+    return tracks, vias, metrics, metadata
+
+
+def jsonable(o):
+    return json.loads(json.dumps(o))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    args = ap.parse_args()
+    os.environ["PYTHONDONTWRITEBYTECODE"] = "1"
+    sys.dont_write_bytecode = True
+    sys.path.insert(0, args.ref)
+    logging.disable(logging.CRITICAL)
+    from orthoroute.infrastructure.serialization.orp_exporter import (convert_orp_to_board_data,
+                                                                       export_board_to_orp, import_board_from_orp)
+    from orthoroute.infrastructure.serialization.ors_exporter import (convert_ors_to_geometry_payload,
+                                                                       export_solution_to_ors,
+                                                                       import_solution_from_ors)
+    import orthoroute.algorithms.manhattan.unified_pathfinder as upf
+    from orthoroute.domain.models.board import Board, Component, Coordinate, Net, Pad
+
+    bd = board_data()
+    orp_path = HERE / "golden_board.orp"
+    export_board_to_orp(json.loads(json.dumps(bd)), str(orp_path), compress=True)
+    converted = convert_orp_to_board_data(import_board_from_orp(str(orp_path)))
+    mapping = reference_mapping(converted, upf, (Board, Net, Pad, Component, Coordinate))
+    (HERE / "golden_orp.json").write_text(json.dumps({"board_data": bd, "converted": jsonable(converted),
+                                                      "mapping": mapping}, indent=1))
+
+    tracks, vias, metrics, metadata = ors_inputs()
+
+    class Payload:
+        pass
+
+    pl = Payload()
+    pl.tracks, pl.vias = tracks, vias
+    ors_path = HERE / "golden_solution.ors"
+    export_solution_to_ors(pl, metrics, metadata, str(ors_path), compress=True)
+    geom, meta = import_solution_from_ors(str(ors_path))
+    back = convert_ors_to_geometry_payload(geom)
+    (HERE / "golden_ors.json").write_text(json.dumps({
+        "inputs": {"tracks": jsonable(tracks), "vias": jsonable(vias), "metrics": metrics, "metadata": metadata},
+        "imported": {"geometry": geom, "metadata": meta},
+        "payload": {"tracks": jsonable(back.tracks), "vias": jsonable(back.vias)}}, indent=1))
+    print(f"nets {len(bd['nets'])}, tasks {len(mapping['tasks'])}, trivial {len(mapping['trivial'])}, "
+          f"grid {mapping['x_steps']}x{mapping['y_steps']}x{mapping['layers']}")
+
+
+if __name__ == "__main__":
+    main()

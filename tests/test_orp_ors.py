@@ -1,0 +1,128 @@
+"""The .ORP / .ORS formats and the headless board mapping against golden files
+written by the reference's own exporter, importer and router set-up
+(tests/golden/make_golden_orp_ors.py).  No GPU needed."""
+import gzip
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from orthoroute_b200.headless import build_problem
+from orthoroute_b200.lattice import board_uniform_pins
+from orthoroute_b200.orp import (board_data_to_orp, orp_to_board_data, read_orp, synthetic_board_data,
+                                 write_orp)
+from orthoroute_b200.ors import ors_to_geometry_payload, read_ors, solution_to_ors, write_ors
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def _json(o):
+    return json.loads(json.dumps(o))
+
+
+def _gz_json(path):
+    with gzip.open(path, "rt", encoding="utf-8") as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="module")
+def gorp():
+    return json.loads((GOLDEN / "golden_orp.json").read_text())
+
+
+@pytest.fixture(scope="module")
+def gors():
+    return json.loads((GOLDEN / "golden_ors.json").read_text())
+
+
+def test_read_and_convert_reference_orp(gorp):
+    """A file the reference wrote reads back as the reference reads it, and
+    converts to the reference's board_data."""
+    doc = read_orp(GOLDEN / "golden_board.orp")
+    assert doc == _gz_json(GOLDEN / "golden_board.orp")
+    assert _json(orp_to_board_data(doc)) == gorp["converted"]
+
+
+def test_write_orp_matches_reference(gorp):
+    """board_data -> ORP document: the reference's, field for field (the
+    export time aside)."""
+    ref = _gz_json(GOLDEN / "golden_board.orp")
+    ts = ref["metadata"]["export_timestamp"]
+    ours = board_data_to_orp(gorp["board_data"], filename="golden_board.orp", timestamp=ts)
+    assert _json(ours) == ref
+
+
+def test_headless_mapping_matches_reference(gorp):
+    """Grid, layer directions, pad-to-pad tasks (dict order) and one-node
+    routes of the reference's router set-up on the same board."""
+    m = gorp["mapping"]
+    prob = build_problem(gorp["converted"], pitch=m["pitch"])
+    lat = prob.lattice
+    assert (lat.nx, lat.ny, lat.nz) == (m["x_steps"], m["y_steps"], m["layers"])
+    assert prob.grid_min_x == m["grid_min_x"] and prob.grid_min_y == m["grid_min_y"]
+    assert prob.layer_dirs == m["layer_directions"]
+    tasks = {n: [int(s), int(d)] for n, s, d in zip(prob.names, prob.src, prob.dst)}
+    assert list(tasks.items()) == list(m["tasks"].items())
+    assert {k: int(v) for k, v in prob.trivial.items()} == m["trivial"]
+
+
+def test_ors_matches_reference(gors, tmp_path):
+    """Solution -> ORS document, read back, and back to the router's payload
+    form: the reference's results on mixed track / via / metric key styles."""
+    inp = gors["inputs"]
+
+    class Payload:
+        tracks = inp["tracks"]
+        vias = inp["vias"]
+
+    ref = _gz_json(GOLDEN / "golden_solution.ors")
+    ts = ref["metadata"]["export_timestamp"]
+    ours = solution_to_ors(Payload, inp["metrics"], inp["metadata"], timestamp=ts)
+    assert _json(ours) == ref
+    geom, meta = read_ors(GOLDEN / "golden_solution.ors")
+    assert _json([geom, meta]) == [gors["imported"]["geometry"], gors["imported"]["metadata"]]
+    back = ors_to_geometry_payload(geom)
+    assert _json([back.tracks, back.vias]) == [gors["payload"]["tracks"], gors["payload"]["vias"]]
+    # our own file reads back the same way
+    out = tmp_path / "s.ors"
+    doc = write_ors(Payload, inp["metrics"], inp["metadata"], out)
+    g2, m2 = read_ors(out)
+    assert _json(g2) == _json(doc["geometry"]) and _json(m2["statistics"]) == ref["statistics"]
+
+
+def test_format_errors(tmp_path):
+    with pytest.raises(FileNotFoundError):
+        read_orp(tmp_path / "missing.orp")
+    with pytest.raises(FileNotFoundError):
+        read_ors(tmp_path / "missing.ors")
+    for name, reader, sections in (("a.orp", read_orp, ["metadata", "board"]), ("a.ors", read_ors, ["metadata"])):
+        p = tmp_path / name
+        p.write_text(json.dumps({"metadata": {}}))
+        with pytest.raises(ValueError, match="Missing format_version"):
+            reader(p)
+        p.write_text(json.dumps({"format_version": "2.0"}))
+        with pytest.raises(ValueError, match="Unsupported"):
+            reader(p)
+        with gzip.open(p, "wt") as f:
+            json.dump({"format_version": "1.0", "metadata": {}}, f)
+        with pytest.raises(ValueError, match="Missing required sections"):
+            reader(p)
+    with pytest.raises(ValueError, match="Geometry cannot be None"):
+        solution_to_ors(None, [], {})
+
+
+def test_synthetic_board_round_trip(tmp_path):
+    """A benchmark board exported as .ORP maps back onto its own grid cells:
+    every pin keeps its (x, y, layer) up to the routing area's offset."""
+    b = board_uniform_pins(30, 24, 4, 12, seed=3)
+    path = tmp_path / "b.orp"
+    write_orp(synthetic_board_data(b), path)
+    prob = build_problem(orp_to_board_data(read_orp(path)))
+    assert prob.names == b.names
+    ox = round((10.0 - prob.grid_min_x) / 0.4)
+    oy = round((10.0 - prob.grid_min_y) / 0.4)
+    for a, c in ((b.src, prob.src), (b.dst, prob.dst)):
+        x, y, z = b.lattice.coords(a)
+        px, py, pz = prob.lattice.coords(c)
+        assert np.array_equal(px, x + ox) and np.array_equal(py, y + oy) and np.array_equal(pz, z)
