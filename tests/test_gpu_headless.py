@@ -44,7 +44,9 @@ def test_headless_orp_to_ors_matches_oracle(tmp_path, mode):
     expect_t, expect_v = {}, {}
     for name, (tracks, vias) in zip(prob.names, emit(ref["paths"], lat.nx, lat.ny, lat.nz, prob.layer_dirs)):
         expect_t[name] = [(prob.layer_names[z], xy(a), xy(c)) for a, c, z in tracks]
-        expect_v[name] = [(xy(n), prob.layer_names[z0], prob.layer_names[z1]) for n, z0, z1 in vias]
+        # the router's via dicts name the lower layer first
+        expect_v[name] = [(xy(n), prob.layer_names[min(z0, z1)], prob.layer_names[max(z0, z1)])
+                          for n, z0, z1 in vias]
     got_t = {n: [(t["layer"], (t["start"]["x"], t["start"]["y"]), (t["end"]["x"], t["end"]["y"]))
                  for t in d["tracks"]] for n, d in geom["by_net"].items()}
     got_v = {n: [((v["position"]["x"], v["position"]["y"]), v["from_layer"], v["to_layer"]) for v in d["vias"]]
