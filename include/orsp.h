@@ -95,6 +95,11 @@ ORSP_API int orsp_graph_max_degree(orsp_graph *g, int32_t *out);
  * orsp_route_nets is available.  0 otherwise.  (No reference counterpart:
  * the reference has one search path for every graph.) */
 ORSP_API int orsp_graph_is_lattice(orsp_graph *g, int32_t *out);
+/* Deepest box (layers) that one shared-memory tile of the lattice search holds
+ * at tile width tile_w (16 or 32; 0: the library's width).  Single and
+ * batched box searches deeper than this take the generic search; the device
+ * routing loop (orsp_route_nets) rejects them.  (No reference counterpart.) */
+ORSP_API int orsp_lattice_max_layers(int32_t tile_w, int32_t *out);
 
 /* ---- single search ----------------------------------------------------- */
 /* Single-source (or multi-seed) shortest path over the whole graph or over

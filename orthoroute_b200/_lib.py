@@ -47,6 +47,7 @@ _SIGS = {
     "orsp_graph_csr": (ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P)]),
     "orsp_graph_max_degree": (ctypes.c_int, [_P, ctypes.POINTER(_i32)]),
     "orsp_graph_is_lattice": (ctypes.c_int, [_P, ctypes.POINTER(_i32)]),
+    "orsp_lattice_max_layers": (ctypes.c_int, [_i32, ctypes.POINTER(_i32)]),
     "orsp_sssp": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _f32, _P, _P, _i32,
                                  ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
     "orsp_sssp_box": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _f32, _P, _P, _i32,

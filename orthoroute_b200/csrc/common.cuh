@@ -129,6 +129,9 @@ struct LatBox {
 };
 // Tile width of the lattice search (ORSP_LAT_TILE: 16 or 32); the height is 16.
 int lattice_tile_w();
+// Whether a tile of nzb layers at tile width tile_w (0: lattice_tile_w())
+// fits in shared memory.
+bool lattice_tile_fits(int nzb, int tile_w = 0);
 // Fills out[i] for boxes_h[6i..6i+5] (tile width tile_w, 0 = lattice_tile_w(),
 // shared distances) and returns the total tile count.
 int64_t make_lat_boxes(const int32_t *boxes_h, int32_t nbox, LatBox *out, int tile_w = 0);

@@ -762,11 +762,18 @@ static int run_batch(orsp_graph *g, const float *cost_d, int32_t K, const int32_
   std::vector<int32_t> cta_items;
   std::vector<float> delta_k;
   int cta_ctas = 0;
+  // a box deeper than a shared-memory tile holds goes to the CTA kernel
+  auto tile_ok = [&](int32_t k, int tw) {
+    if (range_mode) return true;
+    const int32_t *b = &bb[(size_t)per * k];
+    return lattice_tile_fits(b[5] - b[4] + 1, tw);
+  };
   for (int tw : {16, 32}) {
     std::vector<int32_t> lat_items;
     for (int i = 0; i < nb; ++i)
       if (tuned && g->plan_impl[i] == 1 && g->lattice_ok && g->plan_tile[i] == tw)
-        lat_items.insert(lat_items.end(), bucket[i].begin(), bucket[i].end());
+        for (int32_t k : bucket[i])
+          if (tile_ok(k, tw)) lat_items.push_back(k);
     if (lat_items.empty()) continue;
     if (src_h.empty()) {
       src_h.resize(K);
@@ -780,14 +787,20 @@ static int run_batch(orsp_graph *g, const float *cost_d, int32_t K, const int32_
     if (rc) return rc;
   }
   for (int i = 0; i < nb; ++i) {
-    if (tuned && g->plan_impl[i] == 1 && g->lattice_ok) continue;
-    if (bucket[i].empty()) continue;
+    std::vector<int32_t> items;
+    if (tuned && g->plan_impl[i] == 1 && g->lattice_ok) {
+      for (int32_t k : bucket[i])
+        if (!tile_ok(k, g->plan_tile[i])) items.push_back(k);
+    } else {
+      items = bucket[i];
+    }
+    if (items.empty()) continue;
     if (tuned) {
       if (delta_k.empty()) delta_k.assign(K, 0.0f);
-      for (int32_t k : bucket[i]) delta_k[k] = g->plan_delta[i];
+      for (int32_t k : items) delta_k[k] = g->plan_delta[i];
       cta_ctas = std::max(cta_ctas, g->plan_ctas[i]);
     }
-    cta_items.insert(cta_items.end(), bucket[i].begin(), bucket[i].end());
+    cta_items.insert(cta_items.end(), items.begin(), items.end());
   }
   if (!cta_items.empty()) {
     // processing order of the caller, across buckets

@@ -1108,6 +1108,12 @@ void free_lattice(Graph *g) {
 
 int lattice_tile_w() { return env_u64("ORSP_LAT_TILE", 16) == 32 ? 32 : 16; }
 
+bool lattice_tile_fits(int nzb, int tile_w) {
+  const int TX = tile_w ? tile_w : lattice_tile_w(), TY = 16;
+  const size_t smem = ((size_t)nzb * (TY + 2) * (TX + 3) + (size_t)5 * nzb * TY * (TX + 1)) * sizeof(float);
+  return smem <= 227 * 1024;
+}
+
 int reserve_lattice_ws(Graph *g, int64_t ntiles) { return grow_ws(g, ws_layout(g, ntiles).total); }
 
 int64_t make_lat_boxes(const int32_t *boxes_h, int32_t nbox, LatBox *out, int tile_w) {
@@ -1228,3 +1234,14 @@ int finish_lattice_search(Graph *g, int32_t *rounds_h) {
 }
 
 }  // namespace orsp
+
+extern "C" int orsp_lattice_max_layers(int32_t tile_w, int32_t *out) {
+  if (!out || (tile_w != 0 && tile_w != 16 && tile_w != 32)) {
+    orsp::set_error("lattice_max_layers: tile width must be 0, 16 or 32");
+    return ORSP_ERR_ARG;
+  }
+  int n = 0;
+  while (n < 64 && orsp::lattice_tile_fits(n + 1, tile_w)) ++n;
+  *out = n;
+  return ORSP_OK;
+}

@@ -208,6 +208,10 @@ extern "C" int orsp_route_nets(orsp_graph *g, int32_t M, const int32_t *src_h, c
       set_error("route_nets: box outside the lattice or empty");
       return ORSP_ERR_ARG;
     }
+    if (!lattice_tile_fits(box_h[6 * (int64_t)k + 5] - box_h[6 * (int64_t)k + 4] + 1)) {
+      set_error("route_nets: box deeper than a lattice tile holds (orsp_lattice_max_layers)");
+      return ORSP_ERR_ARG;
+    }
   }
   for (int32_t q = 0; q < ngroups; ++q) {
     const int32_t a = gp[q], b = gp[q + 1];

@@ -613,7 +613,10 @@ static int sssp_impl(orsp_graph *g, const float *cost_d, int32_t nseeds, const i
   // the generic near-far search, a box there becoming its ROI map.
   // ORSP_SSSP_IMPL=generic forces the latter.
   const char *impl = getenv("ORSP_SSSP_IMPL");
-  const bool lattice = g->lattice_ok && roi_map_d == nullptr &&
+  // (boxes deeper than a shared-memory tile holds, about 33 layers at tile
+  // width 16, also take the generic search)
+  const int depth = box_h ? box_h[5] - box_h[4] + 1 : g->nz;
+  const bool lattice = g->lattice_ok && roi_map_d == nullptr && lattice_tile_fits(depth) &&
                        !(impl && std::string(impl) == "generic");
   if (box_h && !lattice) {
     if (!g->box_g2r) ORSP_CUDA(cudaMalloc(&g->box_g2r, (size_t)g->N * 4));

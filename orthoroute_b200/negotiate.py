@@ -312,7 +312,7 @@ class PathFinder:
             float(cfg.base_cost_weight), 1 if cfg.add_jitter else 0, _stream()), "orsp_route_nets")
 
     def _route_net_sequential(self, acc, pres_fac, idx, src, dst, boxes, net_nodes, net_edges, net_lens, delta):
-        if self.cfg.native_loop and self.dg.is_lattice:
+        if self.cfg.native_loop and self.dg.route_loop_ok:
             self._route_nets_device(acc, pres_fac, idx.cpu().numpy(), None, src, dst, boxes, net_nodes, net_edges,
                                     net_lens)
         else:
@@ -358,7 +358,7 @@ class PathFinder:
 
     def _route_net_batched(self, acc, pres_fac, idx, src_d, dst_d, boxes_d, boxes, order_levels, net_nodes,
                            net_edges, net_lens, delta, src=None, dst=None):
-        if self.cfg.native_loop and self.dg.is_lattice and src is not None:
+        if self.cfg.native_loop and self.dg.route_loop_ok and src is not None:
             idx_h = idx.cpu().numpy()
             order, groups = level_groups(idx_h, level_schedule(boxes[idx_h]))
             self._route_nets_device(acc, pres_fac, order, groups, src, dst, boxes, net_nodes, net_edges, net_lens)

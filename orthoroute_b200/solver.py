@@ -71,6 +71,10 @@ class DeviceGraph:
         il = ctypes.c_int32()
         check(lib.orsp_graph_is_lattice(self._h, ctypes.byref(il)), "orsp_graph_is_lattice")
         self.is_lattice = bool(il.value)
+        ml = ctypes.c_int32()
+        check(lib.orsp_lattice_max_layers(0, ctypes.byref(ml)), "orsp_lattice_max_layers")
+        # the device routing loop needs every box in one shared-memory tile
+        self.route_loop_ok = self.is_lattice and self.nz <= int(ml.value)
         self.indptr_host = indptr
         self.indices_host = indices
         self._path_buf = None

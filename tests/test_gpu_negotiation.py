@@ -146,3 +146,17 @@ def test_route_nets_group_contract():
     st3, _, l3, _, _ = run(np.arange(M), None, boxes_=bx)
     assert st3 == 0 and l3[0] == 0
 
+
+def test_negotiation_on_lattice_deeper_than_a_tile():
+    """A 40-layer lattice (deeper than one shared-memory tile): the routing
+    loop runs on the host over box searches that take the generic kernel,
+    with the oracle's trace and paths."""
+    b = board_uniform_pins(14, 12, 40, 8, seed=6)
+    cfg = NegotiationConfig(max_iterations=4, roi_margin=3, cost_update="net", reroute="offenders")
+    ref = route_plain(b.lattice, b.src, b.dst, cfg)
+    pf = PathFinder(b.lattice, config=cfg)
+    assert not pf.dg.route_loop_ok
+    r = pf.route(b.src, b.dst, mode="sequential")
+    assert r.overuse_trace() == [(s, c) for s, c, _ in ref["trace"]]
+    for k in range(len(b.src)):
+        assert np.array_equal(r.paths[k], ref["paths"][k]), f"net {k}"

@@ -413,6 +413,69 @@ def test_find_paths_on_rois_local_csr_batch():
     assert got == refs
 
 
+def test_lattice_walk_long_runs_path_caps_and_deep_fallback():
+    """The warp walk of the lattice backtraces: a 200-node straight run (many
+    rounds of 32 lanes), a 30-layer via stack, path_cap exactly the path
+    length (accepted) and one less (an error, or an error status per search
+    in a batch); lattices deeper than a shared-memory tile take the generic
+    search and the host routing loop, with the oracle's results."""
+    lat = build_lattice(200, 6, 4)
+    w = lat.base_cost.astype(np.float32)
+    dg = DeviceGraph.from_lattice(lat)
+    wt = cuda(w)
+    s, d = int(lat.node(0, 2, 1)), int(lat.node(199, 2, 1))
+    ref, *_ = O.dijkstra(lat.indptr, lat.indices, w, [s], dst=d)
+    assert len(ref) == 200
+    full = (0, 199, 0, 5, 0, 3)
+    for cap in (200, 4096):
+        st, p, _ = dg.sssp_box(wt, s, d, full, path_cap=cap)
+        assert st == _lib.ORSP_OK and p.cpu().tolist() == ref.tolist()
+        st, p, _ = dg.sssp(wt, s, d, path_cap=cap)
+        assert st == _lib.ORSP_OK and p.cpu().tolist() == ref.tolist()
+    with pytest.raises(_lib.OrspError):
+        dg.sssp_box(wt, s, d, full, path_cap=199)
+    dg.set_batch_plan([{"max_nodes": 1 << 40, "impl": 1, "tile_w": 16}])
+    boxes = np.array([full, full], np.int32)
+    for cap, ok in ((200, True), (199, False)):
+        nodes, edges, lens = dg.batch_bbox(wt, cuda(np.array([s, d], np.int32)), cuda(np.array([d, s], np.int32)),
+                                           cuda(boxes), path_cap=cap)
+        lens = lens.cpu().numpy()
+        if ok:
+            assert lens.tolist() == [200, 200]
+            assert nodes.cpu().numpy()[0, :200].tolist() == ref.tolist()
+        else:
+            assert (lens < 0).all()
+
+    stack = build_lattice(6, 6, 30)
+    ws = stack.base_cost.astype(np.float32)
+    dgs = DeviceGraph.from_lattice(stack)
+    s, d = int(stack.node(3, 3, 0)), int(stack.node(3, 3, 29))
+    ref, *_ = O.dijkstra(stack.indptr, stack.indices, ws, [s], dst=d)
+    st, p, _ = dgs.sssp(cuda(ws), s, d)
+    assert st == _lib.ORSP_OK and p.cpu().tolist() == ref.tolist() and len(ref) == 30
+
+    deep = build_lattice(12, 10, 40)
+    wd = uniform_weights(deep, seed=2, blocked_frac=0.02)
+    dgd = DeviceGraph.from_lattice(deep)
+    assert dgd.is_lattice and not dgd.route_loop_ok
+    s = int(deep.node(1, 1, 0))
+    _, ref_dist, _, _ = O.dijkstra(deep.indptr, deep.indices, wd, [s])
+    dist = torch.empty(deep.N, dtype=torch.float32, device="cuda")
+    st, _, _ = dgd.sssp(cuda(wd), s, -1, dist_out=dist)
+    assert st == _lib.ORSP_OK and np.array_equal(_bits(dist.cpu().numpy()), _bits(ref_dist))
+    for b in [(0, 11, 0, 9, 0, 39), (2, 10, 1, 8, 5, 25)]:
+        x0, x1, y0, y1, z0, z1 = b
+        g2r = np.full(deep.N, -1, np.int32)
+        zz, yy, xx = np.meshgrid(np.arange(z0, z1 + 1), np.arange(y0, y1 + 1), np.arange(x0, x1 + 1),
+                                 indexing="ij")
+        inside = deep.node(xx, yy, zz).ravel()
+        g2r[inside] = np.arange(inside.size, dtype=np.int32)
+        s, d = int(inside[3]), int(inside[-5])
+        refp, *_ = O.dijkstra(deep.indptr, deep.indices, wd, [s], dst=d, roi_map=g2r)
+        st, p, _ = dgd.sssp_box(cuda(wd), s, d, b)
+        assert st == _lib.ORSP_OK and p.cpu().tolist() == refp.tolist(), b
+
+
 @pytest.mark.parametrize("impl", ["lattice16", "lattice16-rounds"])
 @pytest.mark.parametrize("shape", [(40, 36, 18), (35, 29, 13)])
 def test_deep_lattice_bit_exact(shape, impl, monkeypatch):
