@@ -85,6 +85,8 @@ struct Graph {
   void *route_tab_d = nullptr;
   void *route_tab_h = nullptr;
   size_t route_tab_bytes = 0;
+  cudaStream_t route_stream = nullptr;    // orsp_route_nets: stream its graphs are captured on
+  cudaEvent_t route_ev[2] = {nullptr, nullptr};  // ordering with the caller's stream
   // H/V lattice description, set when every CSR edge is a unit step along the
   // layer's routing axis or a via to an adjacent layer (see orsp_lattice.cu)
   bool lattice_ok = false;

@@ -182,6 +182,9 @@ extern "C" int orsp_graph_destroy(orsp_graph *g) {
   if (g->blat_tab_h) cudaFreeHost(g->blat_tab_h);
   cudaFree(g->route_tab_d);
   if (g->route_tab_h) cudaFreeHost(g->route_tab_h);
+  if (g->route_stream) cudaStreamDestroy(g->route_stream);
+  for (cudaEvent_t e : g->route_ev)
+    if (e) cudaEventDestroy(e);
   cudaFree(g->box_g2r);
   cudaFree(g->edge_src);
   if (g->pinned) cudaFreeHost(g->pinned);

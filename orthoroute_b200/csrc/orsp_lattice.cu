@@ -1035,7 +1035,20 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   if (orsp::g_timer.on) ORSP_CUDA(cudaEventRecord(orsp::g_timer.a, st));
   // Cooperative launch in both schedules: every CTA is resident, so a CTA
   // waiting for a queue slot never blocks the CTA that will fill it.
-  ORSP_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(g->num_sms * bps), dim3(threads), args, smem, st));
+  // (launched with the cooperative attribute rather than
+  // cudaLaunchCooperativeKernel, so that a stream capture keeps the
+  // co-residency guarantee in the graph's kernel node)
+  cudaLaunchConfig_t lc{};
+  lc.gridDim = dim3(g->num_sms * bps);
+  lc.blockDim = dim3(threads);
+  lc.dynamicSmemBytes = smem;
+  lc.stream = st;
+  cudaLaunchAttribute coop[1];
+  coop[0].id = cudaLaunchAttributeCooperative;
+  coop[0].val.cooperative = 1;
+  lc.attrs = coop;
+  lc.numAttrs = 1;
+  ORSP_CUDA(cudaLaunchKernelExC(&lc, kfn, args));
   if (orsp::g_timer.on) {
     ORSP_CUDA(cudaEventRecord(orsp::g_timer.b, st));
     orsp::g_timer.pending = true;

@@ -162,6 +162,7 @@ bool node_in(const orsp::Graph *g, int32_t u, const int32_t *b) {
 }
 
 constexpr int32_t kMaxGroup = 1024;
+constexpr int32_t kGraphGroups = 64;  // groups per captured CUDA graph
 
 }  // namespace
 
@@ -279,9 +280,11 @@ extern "C" int orsp_route_nets(orsp_graph *g, int32_t M, const int32_t *src_h, c
   geom.ny = g->ny;
   geom.nz = g->nz;
   for (int z = 0; z < 64; ++z) geom.axis[z] = z < g->nz ? g->layer_axis[z] : 0;
-  for (int32_t q = 0; q < ngroups; ++q) {
+  // Steps 1-4 of one group, enqueued on the stream.
+  auto enqueue_group = [&](int32_t q) -> int {
+    int rc = ORSP_OK;
     const int32_t a = gp[q], n = gp[q + 1] - gp[q];
-    if (n == 0) continue;
+    if (n == 0) return ORSP_OK;
     route_commit_kernel<<<n, 256, 0, st>>>(d_order + a, net_edges_d, net_lens_d, path_cap, -1, lp);
     ORSP_CUDA(cudaGetLastError());
     LatOptions opt;
@@ -310,10 +313,68 @@ extern "C" int orsp_route_nets(orsp_graph *g, int32_t M, const int32_t *src_h, c
     ORSP_CUDA(cudaGetLastError());
     route_commit_kernel<<<n, 256, 0, st>>>(d_order + a, net_edges_d, net_lens_d, path_cap, 1, lp);
     ORSP_CUDA(cudaGetLastError());
+    return rc;
+  };
+  // The groups are captured into CUDA graphs of up to kGraphGroups groups
+  // each; a chunk's graph is launched as soon as it is instantiated, so the
+  // GPU runs chunk k while the host captures chunk k + 1.  A chunk whose
+  // capture or instantiation fails is enqueued directly instead (same
+  // launches, same results).  ORSP_ROUTE_GRAPH=0 enqueues every group
+  // directly.
+  const char *ge = getenv("ORSP_ROUTE_GRAPH");
+  bool use_graph = !(ge && ge[0] == '0');
+  // Graphs are captured on a stream of the library's own (the caller's may be
+  // the legacy default stream, which cannot be captured), ordered after the
+  // caller's stream on entry and before it on exit.
+  const cudaStream_t caller = st;
+  if (use_graph) {
+    if (!g->route_stream) ORSP_CUDA(cudaStreamCreateWithFlags(&g->route_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t &e : g->route_ev)
+      if (!e) ORSP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ORSP_CUDA(cudaEventRecord(g->route_ev[0], caller));
+    ORSP_CUDA(cudaStreamWaitEvent(g->route_stream, g->route_ev[0], 0));
+    st = g->route_stream;
+  }
+  std::vector<cudaGraphExec_t> execs;
+  int rc_loop = ORSP_OK;
+  for (int32_t q0 = 0; q0 < ngroups && rc_loop == ORSP_OK; q0 += kGraphGroups) {
+    const int32_t q1 = std::min(ngroups, q0 + kGraphGroups);
+    bool done = false;
+    bool capturing = false;
+    if (use_graph) {
+      capturing = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      if (!capturing) (void)cudaGetLastError();  // enqueue directly, with no error left pending
+    }
+    if (capturing) {
+      int rc_c = ORSP_OK;
+      for (int32_t q = q0; q < q1 && rc_c == ORSP_OK; ++q) rc_c = enqueue_group(q);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+      cudaGraphExec_t exec = nullptr;
+      if (rc_c == ORSP_OK && ce == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+        if (cudaGraphLaunch(exec, st) == cudaSuccess) done = true;
+        execs.push_back(exec);
+      }
+      if (graph) cudaGraphDestroy(graph);
+      if (!done) (void)cudaGetLastError();  // clear the failed capture's error
+    }
+    for (int32_t q = q0; !done && q < q1 && rc_loop == ORSP_OK; ++q) rc_loop = enqueue_group(q);
+  }
+  if (rc_loop != ORSP_OK) {
+    cudaStreamSynchronize(st);
+    for (cudaGraphExec_t e : execs) cudaGraphExecDestroy(e);
+    return rc_loop;
+  }
+  if (use_graph) {  // the caller's stream continues after the last group
+    ORSP_CUDA(cudaEventRecord(g->route_ev[1], st));
+    ORSP_CUDA(cudaStreamWaitEvent(caller, g->route_ev[1], 0));
+    st = caller;
   }
   int *err_h = (int *)g->pinned + 32;
   ORSP_CUDA(cudaMemcpyAsync(err_h, route_err, sizeof(int), cudaMemcpyDeviceToHost, st));
-  ORSP_CUDA(cudaStreamSynchronize(st));
+  const cudaError_t se = cudaStreamSynchronize(st);
+  for (cudaGraphExec_t e : execs) cudaGraphExecDestroy(e);
+  ORSP_CUDA(se);
   if (*err_h) return dev_status_to_orsp(*err_h);
   return ORSP_OK;
 }
