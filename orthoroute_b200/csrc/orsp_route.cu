@@ -20,7 +20,9 @@
 // which equals the host loop over orsp_commit_edges / orsp_update_costs_live
 // / orsp_sssp_box / orsp_path_to_edges, bit for bit.  Device-side errors
 // (search timeout, path overflow) are folded into one error word that the
-// host reads after the last group.
+// host reads after the last group.  The groups' launches are captured into
+// CUDA graphs of kGraphGroups groups on a stream of the library's own (see
+// orsp_route_nets); the launches and their order are the same either way.
 #include <algorithm>
 #include <climits>
 #include <vector>
