@@ -7,6 +7,7 @@ From the reference (orthoroute/infrastructure/serialization/orp_exporter.py,
 ors_exporter.py, main.py and algorithms/manhattan/unified_pathfinder.py):
 
   golden_board.orp          export_board_to_orp(board_data dict)
+  golden_board_2l.orp       the same for a 2-layer board
   golden_orp.json           {"board_data": the input dict,
                              "converted": convert_orp_to_board_data(import_board_from_orp(golden_board.orp)),
                              "mapping": grid and pad-to-pad tasks of UnifiedPathFinder.initialize_graph +
@@ -61,6 +62,34 @@ def board_data():
     return {"filename": "golden.kicad_pcb", "x_min": 95.0, "y_min": 45.0, "x_max": 120.0, "y_max": 70.0,
             "width": 25.0, "height": 25.0, "layers": len(names), "layer_names": names, "pads": pads, "nets": nets,
             "grid_resolution": 0.4, "clearance": 0.15, "track_width": 0.2, "via_diameter": 0.5, "via_drill": 0.25}
+
+
+def board_data_two_layers():
+    """A 2-layer board (both layers carry both directions in the reference),
+    a component with two pads of the same name (the later one keeps the pad
+    key), pads without a component, and a net whose first two pads are on
+    B.Cu and F.Cu."""
+    names = ["F.Cu", "B.Cu"]
+    pads = []
+
+    def pad(comp, name, net, x, y, layers=("F.Cu",), drill=None):
+        pads.append({"component": comp, "name": name, "net_name": net, "net_code": 0, "x": x, "y": y,
+                     "width": 0.3, "height": 0.3, "drill": drill, "layers": list(layers), "type": "smd"})
+
+    pad("U1", "1", "A", 10.0, 10.0)
+    pad("U1", "1", "B", 12.4, 10.8)      # same pad key as the first pad
+    pad("U1", "2", "A", 18.2, 14.6, layers=("B.Cu",))
+    pad("J2", "1", "B", 9.3, 16.1, layers=names, drill=0.9)
+    pad("", "", "C", 11.11, 12.49)
+    pad("", "", "C", 15.55, 12.51, layers=("B.Cu",))
+    pad("J2", "2", "D", 14.0, 9.0, layers=("B.Cu",))
+    pad("U1", "3", "D", 16.0, 17.0)
+    nets = {}
+    for p in pads:
+        nets.setdefault(p["net_name"], {"name": p["net_name"], "code": 0, "pads": []})["pads"].append(p)
+    return {"filename": "two_layers.kicad_pcb", "x_min": 5.0, "y_min": 5.0, "x_max": 25.0, "y_max": 22.0,
+            "width": 20.0, "height": 17.0, "layers": 2, "layer_names": names, "pads": pads, "nets": nets,
+            "grid_resolution": 0.4}
 
 
 def reference_mapping(bd, upf_mod, models):
@@ -163,8 +192,15 @@ def main():
     export_board_to_orp(json.loads(json.dumps(bd)), str(orp_path), compress=True)
     converted = convert_orp_to_board_data(import_board_from_orp(str(orp_path)))
     mapping = reference_mapping(converted, upf, (Board, Net, Pad, Component, Coordinate))
+    bd2 = board_data_two_layers()
+    orp2 = HERE / "golden_board_2l.orp"
+    export_board_to_orp(json.loads(json.dumps(bd2)), str(orp2), compress=True)
+    converted2 = convert_orp_to_board_data(import_board_from_orp(str(orp2)))
+    mapping2 = reference_mapping(converted2, upf, (Board, Net, Pad, Component, Coordinate))
     (HERE / "golden_orp.json").write_text(json.dumps({"board_data": bd, "converted": jsonable(converted),
-                                                      "mapping": mapping}, indent=1))
+                                                      "mapping": mapping, "board_data_2l": bd2,
+                                                      "converted_2l": jsonable(converted2),
+                                                      "mapping_2l": mapping2}, indent=1))
 
     tracks, vias, metrics, metadata = ors_inputs()
 
@@ -181,8 +217,8 @@ def main():
         "inputs": {"tracks": jsonable(tracks), "vias": jsonable(vias), "metrics": metrics, "metadata": metadata},
         "imported": {"geometry": geom, "metadata": meta},
         "payload": {"tracks": jsonable(back.tracks), "vias": jsonable(back.vias)}}, indent=1))
-    print(f"nets {len(bd['nets'])}, tasks {len(mapping['tasks'])}, trivial {len(mapping['trivial'])}, "
-          f"grid {mapping['x_steps']}x{mapping['y_steps']}x{mapping['layers']}")
+    for m in (mapping, mapping2):
+        print(f"tasks {len(m['tasks'])}, trivial {len(m['trivial'])}, grid {m['x_steps']}x{m['y_steps']}x{m['layers']}")
 
 
 if __name__ == "__main__":
