@@ -2,10 +2,10 @@
 
 A small 3D convolutional net predicts, from the pins and the airwires of a
 board, the history cost field PathFinder ends with; routing then starts from
-that history instead of zero.  Plain zero-history PathFinder stays the
-fallback and the judge: a warm run counts only when it reaches zero overuse,
-and if it has not converged within 1.5x the plain run's iterations the plain
-run is used.
+that history instead of zero.  Plain zero-history PathFinder stays both the
+fallback and the yardstick: a warm run counts only when it reaches zero
+overuse, and if it has not converged within 1.5x the plain run's iterations
+the plain run is used.
 
 Network (all layers run by the kernels of orsp_warm.cu, bf16 activations
 [D][H][W][C] with fp32 accumulation): a 4-level U-net over the routing grid,
