@@ -58,7 +58,15 @@ class HeadlessProblem:
     pitch: float
     layer_names: List[str]
     layer_dirs: List[str]
-    pad_nodes: Dict[str, int] = field(default_factory=dict)
+    pad_nodes: Dict[str, int] = field(default_factory=dict)  # pad key -> grid node, the reference's order
+    components: List[Tuple[str, List[dict]]] = field(default_factory=list)  # (component, its pads)
+    net_pads: Dict[str, Tuple[str, str]] = field(default_factory=dict)  # net -> keys of its first two pads
+    portals: Dict[str, object] = field(default_factory=dict)  # pad key -> escapes.Portal (portal runs)
+    escape_tracks: List[dict] = field(default_factory=list)
+
+    @staticmethod
+    def pad_key(pad: dict, comp: str) -> str:
+        return _pad_key(pad, comp, _pad_id(pad))
 
 
 def routing_bounds(board_data: dict) -> Tuple[float, float, float, float]:
@@ -86,14 +94,22 @@ def grid_geometry(bounds, pitch: float):
     return gx0, gy0, int((gx1 - gx0) / pitch) + 1, int((gy1 - gy0) / pitch) + 1
 
 
+def _pad_id(p: dict) -> str:
+    return p.get("name", p.get("id", "")) or p.get("id", "")
+
+
 def _pad_key(pad: dict, comp: str, pad_id: str) -> str:
     if comp == "GENERIC_COMPONENT":
         return f"{comp}_{pad_id}@{int(round(pad.get('x', 0.0) * 1000))},{int(round(pad.get('y', 0.0) * 1000))}"
     return f"{comp}_{pad_id}"
 
 
-def build_problem(board_data: dict, pitch: float = DEFAULT_PITCH) -> HeadlessProblem:
-    """The routing lattice and tasks of a board_data dict."""
+def build_problem(board_data: dict, pitch: float = DEFAULT_PITCH, portals: bool = False,
+                  escape_seed: int = 42) -> HeadlessProblem:
+    """The routing lattice and tasks of a board_data dict.  With portals, the
+    pads escape to portals first (escapes.plan_escapes) and a net whose two
+    pads both have one is routed between its portals, as the reference does
+    with its default portal_enabled (unified_pathfinder.py:2629-2641)."""
     nz = int(board_data.get("layers", 2))
     names = list(board_data.get("layer_names") or [])
     if len(names) < nz:
@@ -102,8 +118,7 @@ def build_problem(board_data: dict, pitch: float = DEFAULT_PITCH) -> HeadlessPro
     lat = build_lattice(nx, ny, nz, planar="inner" if nz > 2 else "all", vias="adjacent")
     plane = nx * ny
 
-    def pad_id(p):
-        return p.get("name", p.get("id", "")) or p.get("id", "")
+    pad_id = _pad_id
 
     def snap(p) -> int:
         xi = min(max(round((p.get("x", 0.0) - gx0) / pitch), 0), nx - 1)
@@ -135,22 +150,37 @@ def build_problem(board_data: dict, pitch: float = DEFAULT_PITCH) -> HeadlessPro
         for p in members[comp]:
             pad_nodes[_pad_key(p, comp, pad_id(p))] = snap(p)
 
-    tnames, src, dst, trivial = [], [], [], {}
+    net_pads: Dict[str, Tuple[str, str]] = {}
     for net_id, net in board_data.get("nets", {}).items():
         pads = [p for p in net.get("pads", []) if isinstance(p, dict)]
         if len(pads) < 2:
             continue
-        k1 = _pad_key(pads[0], pads[0].get("component", "") or "GENERIC_COMPONENT", pad_id(pads[0]))
-        k2 = _pad_key(pads[1], pads[1].get("component", "") or "GENERIC_COMPONENT", pad_id(pads[1]))
-        s, d = pad_nodes[k1], pad_nodes[k2]
+        net_pads[net_id] = tuple(_pad_key(q, q.get("component", "") or "GENERIC_COMPONENT", pad_id(q))
+                                 for q in pads[:2])
+    prob = HeadlessProblem(lat, [], np.zeros(0, np.int32), np.zeros(0, np.int32), {}, gx0, gy0, pitch, names,
+                           layer_directions(nz), pad_nodes, [(c, members[c]) for c in order], net_pads)
+    if portals:
+        from .escapes import plan_escapes
+        prob.portals, prob.escape_tracks = plan_escapes(board_data, prob, seed=escape_seed)
+    tnames, src, dst, trivial = [], [], [], {}
+    for net_id, (k1, k2) in net_pads.items():
+        if k1 in prob.portals and k2 in prob.portals:
+            a, b = prob.portals[k1], prob.portals[k2]
+            s = a.entry_layer * plane + a.y_idx * nx + a.x_idx
+            d = b.entry_layer * plane + b.y_idx * nx + b.x_idx
+        else:
+            s, d = pad_nodes[k1], pad_nodes[k2]
         if s != d:
             tnames.append(net_id)
             src.append(s)
             dst.append(d)
         else:
             trivial[net_id] = s
-    return HeadlessProblem(lat, tnames, np.asarray(src, np.int32), np.asarray(dst, np.int32), trivial, gx0, gy0,
-                           pitch, names, layer_directions(nz), pad_nodes)
+    prob.names = tnames
+    prob.src = np.asarray(src, np.int32)
+    prob.dst = np.asarray(dst, np.int32)
+    prob.trivial = trivial
+    return prob
 
 
 def headless_config(max_iterations: int = 200):

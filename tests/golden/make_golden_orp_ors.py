@@ -8,10 +8,14 @@ ors_exporter.py, main.py and algorithms/manhattan/unified_pathfinder.py):
 
   golden_board.orp          export_board_to_orp(board_data dict)
   golden_board_2l.orp       the same for a 2-layer board
+  golden_board_fp.orp       the same for a board of componentless footprints (pad escapes)
   golden_orp.json           {"board_data": the input dict,
                              "converted": convert_orp_to_board_data(import_board_from_orp(golden_board.orp)),
                              "mapping": grid and pad-to-pad tasks of UnifiedPathFinder.initialize_graph +
-                                        _parse_requests (portals off) on the Board main.py builds}
+                                        _parse_requests (portals off) on the Board main.py builds,
+                             "portals": PadEscapePlanner portals and escape stubs
+                                        (precompute_all_pad_escapes) and the portal-to-portal tasks
+                                        of _parse_requests (portals on); per board}
   golden_solution.ors       export_solution_to_ors(payload, metrics, metadata)
   golden_ors.json           {"inputs": payload / metrics / metadata,
                              "imported": import_solution_from_ors(golden_solution.ors),
@@ -92,9 +96,57 @@ def board_data_two_layers():
             "grid_resolution": 0.4}
 
 
-def reference_mapping(bd, upf_mod, models):
-    """Grid and tasks as main.py's headless flow builds them (main.py:355-422),
-    with the portals off (pad-to-pad tasks)."""
+def board_data_footprints():
+    """Pad escapes under pressure: two footprints of componentless pads (2 rows
+    x 8 at one-cell pitch, so they enter the clearance set), nets joining
+    them, one-pad nets placed in escape paths as obstacles, and a net with a
+    pad off its grid column (dropped from escape planning)."""
+    names = ["F.Cu", "In1.Cu", "In2.Cu", "B.Cu"]
+    pads, nets = [], {}
+
+    def pad(net, x, y):
+        p = {"component": "", "name": "", "net_name": net, "net_code": 0, "x": round(x, 4), "y": round(y, 4),
+             "width": 0.3, "height": 0.3, "drill": None, "layers": ["F.Cu"], "type": "smd"}
+        pads.append(p)
+        nets.setdefault(net, {"name": net, "code": 0, "pads": []})["pads"].append(p)
+
+    for i in range(8):
+        for r in range(2):
+            k = 2 * i + r
+            pad(f"N{k}", 20.0 + 0.4 * i, 20.0 + 0.4 * r)
+    for i in range(8):
+        for r in range(2):
+            k = 2 * (7 - i) + (1 - r)
+            pad(f"N{k}", 24.8 + 0.4 * i, 27.2 + 0.4 * r)
+    for m, (x, y) in enumerate([(20.5, 21.6), (21.3, 19.0), (22.1, 22.0), (26.0, 26.5), (27.7, 28.9)]):
+        pad(f"OBS{m}", x, y)
+    pad("OFF", 22.25, 24.0)
+    pad("OFF", 26.0, 24.4)
+    return {"filename": "footprints.kicad_pcb", "x_min": 15.0, "y_min": 15.0, "x_max": 35.0, "y_max": 35.0,
+            "width": 20.0, "height": 20.0, "layers": len(names), "layer_names": names, "pads": pads,
+            "nets": nets, "grid_resolution": 0.4}
+
+
+def reference_portals(bd, upf_mod, models):
+    """Portals, escape stubs and portal-to-portal tasks of the reference's
+    default (portal_enabled) headless set-up (main.py:432-456)."""
+    board = _reference_board(bd, models)
+    cfg = upf_mod.PathFinderConfig()
+    cfg.portal_enabled = True
+    pf = upf_mod.UnifiedPathFinder(config=cfg, use_gpu=False)
+    pf.initialize_graph(board)
+    board._gui_pads = bd.get("pads", [])
+    tracks, _ = pf.precompute_all_pad_escapes(board)
+    tasks = pf._parse_requests(board.nets)
+    portals = [[pid, int(p.x_idx), int(p.y_idx), int(p.pad_layer), int(p.delta_steps), int(p.direction),
+                float(p.pad_x), float(p.pad_y), int(p.entry_layer)] for pid, p in pf.portals.items()]
+    return {"portals": portals, "escape_tracks": jsonable(tracks),
+            "tasks": {k: [int(a), int(b)] for k, (a, b) in tasks.items()},
+            "trivial": {k: int(v[0]) for k, v in pf.net_paths.items() if len(v) == 1}}
+
+
+def _reference_board(bd, models):
+    """The Board main.py's headless flow builds from board_data (main.py:355-422)."""
     Board, Net, Pad, Component, Coordinate = models
     board = Board(id="headless-board", name=bd.get("filename", "board"), layer_count=bd.get("layers", 2))
     board.nets = []
@@ -127,6 +179,13 @@ def reference_mapping(bd, upf_mod, models):
     board.components = list(comps.values())
     board._kicad_bounds = bd.get("bounds", None)
     board.layer_names = bd.get("layer_names", [])
+    return board
+
+
+def reference_mapping(bd, upf_mod, models):
+    """Grid and tasks as main.py's headless flow builds them, with the portals
+    off (pad-to-pad tasks)."""
+    board = _reference_board(bd, models)
     cfg = upf_mod.PathFinderConfig()
     cfg.portal_enabled = False
     pf = upf_mod.UnifiedPathFinder(config=cfg, use_gpu=False)
@@ -191,16 +250,27 @@ def main():
     orp_path = HERE / "golden_board.orp"
     export_board_to_orp(json.loads(json.dumps(bd)), str(orp_path), compress=True)
     converted = convert_orp_to_board_data(import_board_from_orp(str(orp_path)))
-    mapping = reference_mapping(converted, upf, (Board, Net, Pad, Component, Coordinate))
+    models = (Board, Net, Pad, Component, Coordinate)
+    mapping = reference_mapping(converted, upf, models)
     bd2 = board_data_two_layers()
     orp2 = HERE / "golden_board_2l.orp"
     export_board_to_orp(json.loads(json.dumps(bd2)), str(orp2), compress=True)
     converted2 = convert_orp_to_board_data(import_board_from_orp(str(orp2)))
-    mapping2 = reference_mapping(converted2, upf, (Board, Net, Pad, Component, Coordinate))
+    mapping2 = reference_mapping(converted2, upf, models)
+    bd3 = board_data_footprints()
+    orp3 = HERE / "golden_board_fp.orp"
+    export_board_to_orp(json.loads(json.dumps(bd3)), str(orp3), compress=True)
+    converted3 = convert_orp_to_board_data(import_board_from_orp(str(orp3)))
+    mapping3 = reference_mapping(converted3, upf, models)
+    portals = {sfx: reference_portals(cv, upf, models)
+               for sfx, cv in (("", converted), ("_2l", converted2), ("_fp", converted3))}
     (HERE / "golden_orp.json").write_text(json.dumps({"board_data": bd, "converted": jsonable(converted),
                                                       "mapping": mapping, "board_data_2l": bd2,
                                                       "converted_2l": jsonable(converted2),
-                                                      "mapping_2l": mapping2}, indent=1))
+                                                      "mapping_2l": mapping2, "board_data_fp": bd3,
+                                                      "converted_fp": jsonable(converted3),
+                                                      "mapping_fp": mapping3,
+                                                      **{"portals" + k: v for k, v in portals.items()}}, indent=1))
 
     tracks, vias, metrics, metadata = ors_inputs()
 
@@ -217,8 +287,10 @@ def main():
         "inputs": {"tracks": jsonable(tracks), "vias": jsonable(vias), "metrics": metrics, "metadata": metadata},
         "imported": {"geometry": geom, "metadata": meta},
         "payload": {"tracks": jsonable(back.tracks), "vias": jsonable(back.vias)}}, indent=1))
-    for m in (mapping, mapping2):
+    for m in (mapping, mapping2, mapping3):
         print(f"tasks {len(m['tasks'])}, trivial {len(m['trivial'])}, grid {m['x_steps']}x{m['y_steps']}x{m['layers']}")
+    for k, v in portals.items():
+        print(f"portals{k}: {len(v['portals'])} portals, {len(v['escape_tracks'])} escape tracks, {len(v['tasks'])} tasks")
 
 
 if __name__ == "__main__":

@@ -36,7 +36,7 @@ def gors():
     return json.loads((GOLDEN / "golden_ors.json").read_text())
 
 
-@pytest.mark.parametrize("suffix", ["", "_2l"])
+@pytest.mark.parametrize("suffix", ["", "_2l", "_fp"])
 def test_read_and_convert_reference_orp(gorp, suffix):
     """A file the reference wrote reads back as the reference reads it, and
     converts to the reference's board_data."""
@@ -46,7 +46,7 @@ def test_read_and_convert_reference_orp(gorp, suffix):
     assert _json(orp_to_board_data(doc)) == gorp["converted" + suffix]
 
 
-@pytest.mark.parametrize("suffix", ["", "_2l"])
+@pytest.mark.parametrize("suffix", ["", "_2l", "_fp"])
 def test_write_orp_matches_reference(gorp, suffix):
     """board_data -> ORP document: the reference's, field for field (the
     export time aside)."""
@@ -57,7 +57,7 @@ def test_write_orp_matches_reference(gorp, suffix):
     assert _json(ours) == ref
 
 
-@pytest.mark.parametrize("suffix", ["", "_2l"])
+@pytest.mark.parametrize("suffix", ["", "_2l", "_fp"])
 def test_headless_mapping_matches_reference(gorp, suffix):
     """Grid, layer directions, pad-to-pad tasks (dict order) and one-node
     routes of the reference's router set-up on the same board: a 6-layer
@@ -72,6 +72,23 @@ def test_headless_mapping_matches_reference(gorp, suffix):
     tasks = {n: [int(s), int(d)] for n, s, d in zip(prob.names, prob.src, prob.dst)}
     assert list(tasks.items()) == list(m["tasks"].items())
     assert {k: int(v) for k, v in prob.trivial.items()} == m["trivial"]
+
+
+@pytest.mark.parametrize("suffix", ["", "_2l", "_fp"])
+def test_pad_escapes_match_reference(gorp, suffix):
+    """Pad escapes and portals (orthoroute_b200.escapes) against the
+    reference's PadEscapePlanner in its default headless set-up: the same
+    portals in the same order (cell, length, direction, entry layer), the same
+    escape stubs, and the same portal-to-portal tasks."""
+    g = gorp["portals" + suffix]
+    prob = build_problem(gorp["converted" + suffix], portals=True)
+    got = [[pid, p.x_idx, p.y_idx, p.pad_layer, p.delta_steps, p.direction, p.pad_x, p.pad_y, p.entry_layer]
+           for pid, p in prob.portals.items()]
+    assert got == g["portals"]
+    assert _json(prob.escape_tracks) == g["escape_tracks"]
+    tasks = {n: [int(s), int(d)] for n, s, d in zip(prob.names, prob.src, prob.dst)}
+    assert list(tasks.items()) == list(g["tasks"].items())
+    assert {k: int(v) for k, v in prob.trivial.items()} == g["trivial"]
 
 
 def test_ors_matches_reference(gors, tmp_path):
