@@ -2,6 +2,7 @@
 
     python -m orthoroute_b200.headless board.ORP [-o board.ORS] [--max-iterations 200]
                                        [--mode batched|plain] [--warm] [--pitch 0.4]
+                                       [--no-portals]
 
 The steps are those of the reference's `main.py headless` (main.py:287-622):
 read the board (orp.read_orp / orp_to_board_data), build the routing lattice
@@ -25,8 +26,18 @@ follows the reference's router:
 
 Routing uses this package's lattice (planar edges on the inner layers of a
 board with more than two layers, vias between adjacent layers, base cost 1
-per grid step and 3 per via) and negotiate.PathFinder.  Pads are routed pad
-to pad: the reference's pad-escape portals (its default) are not planned here.
+per grid step and 3 per via) and negotiate.PathFinder.
+
+Portals (the reference's headless default, main.py:432-456; `--no-portals`
+routes pad to pad): every pad of a routable net escapes along its column to a
+portal (escapes.plan_escapes).  A net whose two pads both have a portal keeps
+the reference's portal-to-portal task (entry-layer nodes,
+unified_pathfinder.py:2629-2641), and its search runs between the portals'
+F.Cu nodes, the reference's only search seeds (_get_portal_seeds,
+unified_pathfinder.py:2495-2513), so the path itself drops the via from the
+end of the stub to a routing layer.  The escape stubs go in front of the
+routed tracks, duplicates removed by the reference's geometric key
+(emit_geometry, unified_pathfinder.py:5690-5722).
 """
 from __future__ import annotations
 
@@ -63,6 +74,9 @@ class HeadlessProblem:
     net_pads: Dict[str, Tuple[str, str]] = field(default_factory=dict)  # net -> keys of its first two pads
     portals: Dict[str, object] = field(default_factory=dict)  # pad key -> escapes.Portal (portal runs)
     escape_tracks: List[dict] = field(default_factory=list)
+    # search endpoints per task: src / dst, or the F.Cu nodes of both portals
+    search_src: np.ndarray = None
+    search_dst: np.ndarray = None
 
     @staticmethod
     def pad_key(pad: dict, comp: str) -> str:
@@ -162,25 +176,56 @@ def build_problem(board_data: dict, pitch: float = DEFAULT_PITCH, portals: bool 
     if portals:
         from .escapes import plan_escapes
         prob.portals, prob.escape_tracks = plan_escapes(board_data, prob, seed=escape_seed)
-    tnames, src, dst, trivial = [], [], [], {}
+    tnames, src, dst, ssrc, sdst, trivial = [], [], [], [], [], {}
     for net_id, (k1, k2) in net_pads.items():
         if k1 in prob.portals and k2 in prob.portals:
             a, b = prob.portals[k1], prob.portals[k2]
             s = a.entry_layer * plane + a.y_idx * nx + a.x_idx
             d = b.entry_layer * plane + b.y_idx * nx + b.x_idx
+            s0, d0 = a.y_idx * nx + a.x_idx, b.y_idx * nx + b.x_idx
+            if s0 == d0:  # both stubs end on one point: search between the entry-layer nodes
+                s0, d0 = s, d
         else:
             s, d = pad_nodes[k1], pad_nodes[k2]
+            s0, d0 = s, d
         if s != d:
             tnames.append(net_id)
             src.append(s)
             dst.append(d)
+            ssrc.append(s0)
+            sdst.append(d0)
         else:
             trivial[net_id] = s
     prob.names = tnames
     prob.src = np.asarray(src, np.int32)
     prob.dst = np.asarray(dst, np.int32)
+    prob.search_src = np.asarray(ssrc, np.int32)
+    prob.search_dst = np.asarray(sdst, np.int32)
     prob.trivial = trivial
     return prob
+
+
+def merge_escapes(escape_tracks: List[dict], tracks: List[dict], vias: List[dict]):
+    """Escape stubs in front of the routed tracks, later duplicates dropped
+    by (net, layer, ends and width to 0.001 mm); vias deduplicated by (net,
+    position, layers, drill, diameter) (unified_pathfinder.py:5690-5722)."""
+    def dedupe(items, key):
+        seen, out = set(), []
+        for it in items:
+            k = key(it)
+            if k not in seen:
+                seen.add(k)
+                out.append(it)
+        return out
+
+    if not escape_tracks:
+        return tracks, vias
+    t = dedupe(list(escape_tracks) + list(tracks),
+               lambda t: (t["net"], t["layer"], round(t["x1"], 3), round(t["y1"], 3), round(t["x2"], 3),
+                          round(t["y2"], 3), round(t["width"], 3)))
+    v = dedupe(list(vias), lambda v: (v["net"], round(v["x"], 3), round(v["y"], 3), v.get("from_layer"),
+                                      v.get("to_layer"), round(v.get("drill", 0), 3), round(v.get("diameter", 0), 3)))
+    return t, v
 
 
 def headless_config(max_iterations: int = 200):
@@ -193,20 +238,21 @@ def headless_config(max_iterations: int = 200):
 
 
 def route_board(board_data: dict, pitch: float = DEFAULT_PITCH, max_iterations: int = 200, mode: str = "batched",
-                warm: bool = False, config=None, device=None, log=None):
-    """Routes a board_data dict on the GPU (mode 'batched' or 'sequential').
-    Returns (problem, RouteResult, tracks, vias, iteration metrics)."""
+                warm: bool = False, config=None, device=None, log=None, portals: bool = True):
+    """Routes a board_data dict on the GPU (mode 'batched' or 'sequential'),
+    through pad-escape portals unless portals is False.  Returns (problem,
+    RouteResult, tracks, vias, iteration metrics)."""
     from .geometry import generate_geometry
     from .negotiate import PathFinder
 
-    prob = build_problem(board_data, pitch)
+    prob = build_problem(board_data, pitch, portals=portals)
     cfg = config or headless_config(max_iterations)
     pf = PathFinder(prob.lattice, config=cfg, device=device)
     hist = None
     if warm:
         from .warm import load_pretrained, warm_history
         net, scale = load_pretrained(device=pf.device)
-        hist = warm_history(net, prob.lattice, prob.src, prob.dst, scale)
+        hist = warm_history(net, prob.lattice, prob.search_src, prob.search_dst, scale)
     metrics = []
 
     def cb(s):
@@ -215,7 +261,7 @@ def route_board(board_data: dict, pitch: float = DEFAULT_PITCH, max_iterations: 
         if log:
             log(f"iteration {s.iteration}: overuse {s.over_sum}/{s.over_cnt}, routed {s.routed}, {s.seconds:.2f} s")
 
-    res = pf.route(prob.src, prob.dst, mode=mode, callback=cb, history_init=hist)
+    res = pf.route(prob.search_src, prob.search_dst, mode=mode, callback=cb, history_init=hist)
     net_paths = {}
     for name, path in zip(prob.names, res.paths):
         net_paths[name] = [int(v) for v in path] if path is not None and len(path) >= 2 else []
@@ -223,18 +269,21 @@ def route_board(board_data: dict, pitch: float = DEFAULT_PITCH, max_iterations: 
         net_paths[name] = [int(node)]
     tracks, vias = generate_geometry(pf.dg, net_paths, prob.layer_dirs, prob.grid_min_x, prob.grid_min_y, pitch,
                                      prob.layer_names, pitch)
+    tracks, vias = merge_escapes(prob.escape_tracks, tracks, vias)
     return prob, res, tracks, vias, metrics
 
 
 def run_headless(orp_file: str, output_file: Optional[str] = None, max_iterations: int = 200,
-                 mode: str = "batched", warm: bool = False, pitch: float = DEFAULT_PITCH, log=print) -> dict:
+                 mode: str = "batched", warm: bool = False, pitch: float = DEFAULT_PITCH, log=print,
+                 portals: bool = True) -> dict:
     """ORP in, ORS out; returns a summary of the run."""
     from .ors import GeometryPayload, write_ors
 
     t0 = time.perf_counter()
     board_data = orp_to_board_data(read_orp(orp_file))
     out = Path(output_file) if output_file else Path(orp_file).with_suffix(".ORS")
-    prob, res, tracks, vias, metrics = route_board(board_data, pitch, max_iterations, mode, warm, log=log)
+    prob, res, tracks, vias, metrics = route_board(board_data, pitch, max_iterations, mode, warm, log=log,
+                                                   portals=portals)
     total = time.perf_counter() - t0
     routed = sum(1 for p in res.paths if p is not None and len(p) >= 2) + len(prob.trivial)
     meta = {"orthoroute_version": "0.1.0", "board_name": board_data.get("filename", "board"), "total_time": total,
@@ -246,7 +295,8 @@ def run_headless(orp_file: str, output_file: Optional[str] = None, max_iteration
     summary = {"ors": str(out), "nets": len(prob.names) + len(prob.trivial), "routed": routed,
                "converged": bool(res.converged), "iterations": len(metrics), "tracks": len(tracks),
                "vias": len(vias), "seconds_total": round(total, 3), "seconds_route": round(res.seconds, 3),
-               "lattice": [prob.lattice.nx, prob.lattice.ny, prob.lattice.nz]}
+               "lattice": [prob.lattice.nx, prob.lattice.ny, prob.lattice.nz], "portals": len(prob.portals),
+               "escape_tracks": len(prob.escape_tracks)}
     if log:
         log(json.dumps(summary))
     return summary
@@ -260,9 +310,10 @@ def main(argv=None):
     ap.add_argument("--mode", choices=["batched", "plain"], default="batched")
     ap.add_argument("--warm", action="store_true", help="start from the learned history prediction")
     ap.add_argument("--pitch", type=float, default=DEFAULT_PITCH)
+    ap.add_argument("--no-portals", action="store_true", help="route pad to pad, without pad escapes")
     a = ap.parse_args(argv)
     s = run_headless(a.orp, a.output, a.max_iterations, "batched" if a.mode == "batched" else "sequential", a.warm,
-                     a.pitch)
+                     a.pitch, portals=not a.no_portals)
     return 0 if s["converged"] else 1
 
 

@@ -21,20 +21,11 @@ from orthoroute_b200.ors import read_ors  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("mode", ["batched", "sequential"])
-def test_headless_orp_to_ors_matches_oracle(tmp_path, mode):
-    b = board_uniform_pins(40, 32, 6, 30, seed=5)
-    orp = tmp_path / "board.orp"
-    ors = tmp_path / "board.ors"
-    write_orp(synthetic_board_data(b), orp)
-    s = run_headless(str(orp), str(ors), max_iterations=30, mode=mode, log=None)
-    geom, meta = read_ors(ors)
-
-    prob = build_problem(orp_to_board_data(read_orp(orp)))
+def _expected(prob, paths):
+    """Per net: (layer, start, end) of its tracks and (position, lower layer,
+    upper layer) of its vias, from the oracle's geometry emission of the
+    given paths mapped to board coordinates, escape stubs in front."""
     lat = prob.lattice
-    ref = route_plain(lat, prob.src, prob.dst, headless_config(30))
-    assert s["converged"] == bool(ref["converged"]) and s["converged"]
-    assert meta["statistics"]["converged"] is True
 
     def xy(node):
         r = int(node) % (lat.nx * lat.ny)
@@ -42,18 +33,61 @@ def test_headless_orp_to_ors_matches_oracle(tmp_path, mode):
                 float(_quantize(prob.grid_min_y + (r // lat.nx) * prob.pitch, prob.grid_min_y, prob.pitch)))
 
     expect_t, expect_v = {}, {}
-    for name, (tracks, vias) in zip(prob.names, emit(ref["paths"], lat.nx, lat.ny, lat.nz, prob.layer_dirs)):
-        expect_t[name] = [(prob.layer_names[z], xy(a), xy(c)) for a, c, z in tracks]
+    for t in prob.escape_tracks:
+        expect_t.setdefault(t["net"], []).append((t["layer"], (t["x1"], t["y1"]), (t["x2"], t["y2"])))
+    for name, (tracks, vias) in zip(prob.names, emit(paths, lat.nx, lat.ny, lat.nz, prob.layer_dirs)):
+        expect_t.setdefault(name, []).extend((prob.layer_names[z], xy(a), xy(c)) for a, c, z in tracks)
         # the router's via dicts name the lower layer first
         expect_v[name] = [(xy(n), prob.layer_names[min(z0, z1)], prob.layer_names[max(z0, z1)])
                           for n, z0, z1 in vias]
+    return expect_t, expect_v
+
+
+def _check(prob, ref, s, geom, meta):
+    assert s["converged"] == bool(ref["converged"]) and s["converged"]
+    assert meta["statistics"]["converged"] is True
+    expect_t, expect_v = _expected(prob, ref["paths"])
     got_t = {n: [(t["layer"], (t["start"]["x"], t["start"]["y"]), (t["end"]["x"], t["end"]["y"]))
                  for t in d["tracks"]] for n, d in geom["by_net"].items()}
     got_v = {n: [((v["position"]["x"], v["position"]["y"]), v["from_layer"], v["to_layer"]) for v in d["vias"]]
              for n, d in geom["by_net"].items()}
-    for name in prob.names:
-        assert got_t.get(name, []) == expect_t[name], name
-        assert got_v.get(name, []) == expect_v[name], name
+    for name in set(prob.names) | set(expect_t):
+        assert got_t.get(name, []) == expect_t.get(name, []), name
+        assert got_v.get(name, []) == expect_v.get(name, []), name
     assert meta["statistics"]["total_tracks"] == sum(len(v) for v in expect_t.values())
     assert meta["statistics"]["total_vias"] == sum(len(v) for v in expect_v.values())
     assert np.isfinite(s["seconds_total"])
+
+
+@pytest.mark.parametrize("mode", ["batched", "sequential"])
+def test_headless_orp_to_ors_matches_oracle(tmp_path, mode):
+    """Pad-to-pad routing (no escapes)."""
+    b = board_uniform_pins(40, 32, 6, 30, seed=5)
+    orp = tmp_path / "board.orp"
+    ors = tmp_path / "board.ors"
+    write_orp(synthetic_board_data(b), orp)
+    s = run_headless(str(orp), str(ors), max_iterations=30, mode=mode, log=None, portals=False)
+    geom, meta = read_ors(ors)
+    prob = build_problem(orp_to_board_data(read_orp(orp)))
+    assert not prob.escape_tracks
+    ref = route_plain(prob.lattice, prob.src, prob.dst, headless_config(30))
+    _check(prob, ref, s, geom, meta)
+
+
+@pytest.mark.parametrize("mode", ["batched", "sequential"])
+def test_headless_portals_match_oracle(tmp_path, mode):
+    """The default portal flow: pads escape to portals (stubs on F.Cu), the
+    searches run between the portals' F.Cu nodes, and the .ORS holds the
+    stubs in front of each net's routed tracks."""
+    b = board_uniform_pins(40, 32, 6, 30, seed=5)
+    orp = tmp_path / "board.orp"
+    ors = tmp_path / "board.ors"
+    write_orp(synthetic_board_data(b), orp)
+    s = run_headless(str(orp), str(ors), max_iterations=30, mode=mode, log=None)
+    geom, meta = read_ors(ors)
+    prob = build_problem(orp_to_board_data(read_orp(orp)), portals=True)
+    assert s["portals"] == len(prob.portals) > 0 and s["escape_tracks"] == len(prob.escape_tracks)
+    plane = prob.lattice.nx * prob.lattice.ny
+    assert np.all(prob.search_src < plane) and np.all(prob.search_dst < plane)  # F.Cu seeds
+    ref = route_plain(prob.lattice, prob.search_src, prob.search_dst, headless_config(30))
+    _check(prob, ref, s, geom, meta)

@@ -8,7 +8,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from orthoroute_b200.headless import build_problem
+from orthoroute_b200.headless import build_problem, merge_escapes
 from orthoroute_b200.lattice import board_uniform_pins
 from orthoroute_b200.orp import (board_data_to_orp, orp_to_board_data, read_orp, synthetic_board_data,
                                  write_orp)
@@ -89,6 +89,31 @@ def test_pad_escapes_match_reference(gorp, suffix):
     tasks = {n: [int(s), int(d)] for n, s, d in zip(prob.names, prob.src, prob.dst)}
     assert list(tasks.items()) == list(g["tasks"].items())
     assert {k: int(v) for k, v in prob.trivial.items()} == g["trivial"]
+    # the searches start and end on the portals' F.Cu nodes (the reference's only seeds)
+    plane = prob.lattice.nx * prob.lattice.ny
+    nx = prob.lattice.nx
+    for name, s0, d0, s, d in zip(prob.names, prob.search_src, prob.search_dst, prob.src, prob.dst):
+        k1, k2 = prob.net_pads[name]
+        if k1 in prob.portals and k2 in prob.portals:
+            a, b = prob.portals[k1], prob.portals[k2]
+            if (a.x_idx, a.y_idx) != (b.x_idx, b.y_idx):
+                assert (s0, d0) == (a.y_idx * nx + a.x_idx, b.y_idx * nx + b.x_idx)
+                assert s0 == s % plane and d0 == d % plane
+                continue
+        assert (s0, d0) == (s, d)
+
+
+def test_merge_escapes_dedupe():
+    """Escape stubs go in front; a routed track equal to a stub up to
+    0.001 mm is dropped, and so is a repeated via."""
+    esc = [{"net": "A", "layer": "F.Cu", "x1": 1.0, "y1": 2.0, "x2": 1.0, "y2": 3.2000004, "width": 0.24}]
+    tr = [{"net": "A", "layer": "F.Cu", "x1": 1.0, "y1": 2.0, "x2": 1.0, "y2": 3.2, "width": 0.24},
+          {"net": "B", "layer": "F.Cu", "x1": 1.0, "y1": 2.0, "x2": 1.0, "y2": 3.2, "width": 0.24}]
+    via = {"net": "A", "x": 1.0, "y": 3.2, "from_layer": "F.Cu", "to_layer": "In1.Cu", "diameter": 0.25,
+           "drill": 0.15}
+    t, v = merge_escapes(esc, tr, [via, dict(via)])
+    assert t == [esc[0], tr[1]] and v == [via]
+    assert merge_escapes([], tr, [via, dict(via)]) == (tr, [via, via])
 
 
 def test_ors_matches_reference(gors, tmp_path):
