@@ -731,9 +731,10 @@ __device__ bool activate_tile(const LatParams &p, int t) {
 
 // DEEP: the instantiation for tiles of more than 12 layers (the column load
 // in 18-layer blocks); compiled separately so that each layer range gets its
-// own register allocation.
-template <int TX, int TY, bool PRIV, bool DEEP = false>
-__global__ void __launch_bounds__(TX * TY, 1) lattice_async_kernel(LatParams p) {
+// own register allocation.  MINB: CTAs per SM the registers are sized for
+// (2 fits a 16 x 16 tile of up to 12 layers in 128 registers per thread).
+template <int TX, int TY, bool PRIV, bool DEEP = false, int MINB = 1>
+__global__ void __launch_bounds__(TX * TY, MINB) lattice_async_kernel(LatParams p) {
   extern __shared__ float sd[];
   __shared__ LayerLists s_layers;
   __shared__ int s_flags[3];
@@ -1008,6 +1009,9 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   const bool priv = opt && opt->private_dist;
   // ORSP_LAT_SPEC=1: the warp-specialised asynchronous schedule
   const bool spec = async && env_u64("ORSP_LAT_SPEC", 0) != 0;
+  // ORSP_LAT_BLOCKS_PER_SM: CTAs per SM (tiles of up to 12 layers at width
+  // 16 have an instantiation sized for 2)
+  const int want = (int)env_u64("ORSP_LAT_BLOCKS_PER_SM", 1);
   void *kfn;
   if (spec) kfn = priv ? (void *)lattice_spec_kernel<TX, TY, true> : (void *)lattice_spec_kernel<TX, TY, false>;
   else if (async) {
@@ -1015,6 +1019,9 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
     if constexpr (TX == 16) {  // deeper tiles: the instantiation with 18-layer column loads
       if (nzb > 12)
         kfn = priv ? (void *)lattice_async_kernel<TX, TY, true, true> : (void *)lattice_async_kernel<TX, TY, false, true>;
+      else if (want >= 2)
+        kfn = priv ? (void *)lattice_async_kernel<TX, TY, true, false, 2>
+                   : (void *)lattice_async_kernel<TX, TY, false, false, 2>;
     }
   }
   else kfn = priv ? (void *)lattice_tile_kernel<TX, TY, true> : (void *)lattice_tile_kernel<TX, TY, false>;
@@ -1026,7 +1033,6 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
     orsp::set_error("lattice search: kernel does not fit on an SM");
     return ORSP_ERR_ARG;
   }
-  const int want = (int)env_u64("ORSP_LAT_BLOCKS_PER_SM", 1);
   const int bps = std::max(1, std::min(occ, want));
   p.max_rounds = (unsigned)std::min<unsigned long long>(64ull * (unsigned long long)ntiles + 4096ull, 1ull << 30);
   p.wait_ns = env_u64("ORSP_WAIT_NS", 2000000000ull);
