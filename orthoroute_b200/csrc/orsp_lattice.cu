@@ -64,6 +64,7 @@ struct LatParams {
   int8_t axis[64];
   unsigned max_rounds;
   unsigned long long wait_ns, budget_ns;
+  int selfcont;
 };
 
 __global__ void fill_kernel(uint32_t *p, int64_t n, uint32_t v) {
@@ -394,7 +395,7 @@ struct LayerLists {
 
 template <int TX, int TY, bool PRIV, bool SPEC, bool DEEP = false>
 __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *sd, LayerLists &L, int *s_flags,
-                                             int *s_act, int *s_nb = nullptr) {
+                                             int *s_act, int *s_nb = nullptr, bool warm = false) {
   const int bi = box_of_tile(p, t);
   const LatBox B = load_box(p, bi);
   if (threadIdx.x == 0 && L.box != bi) {
@@ -475,7 +476,13 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
     }
     // the thread's column (x, y) of the tile (th * tw <= threads)
     const int c = threadIdx.x;
-    if (c < th * tw) {
+    if (warm && c < th * tw) {
+      // the same tile again: its interior and weights are still in shared
+      // memory and equal to what the last visit published
+      const int yy = c / tw + 1, xx = c - (yy - 1) * tw + 1;
+      const int s0 = yy * SX + xx, w0 = (yy - 1) * WSX + (xx - 1);
+      for (int z = 0; z < nzb; ++z) orig[z * WPS + w0] = sd[z * PS + s0];
+    } else if (c < th * tw) {
       const int yy = c / tw + 1, xx = c - (yy - 1) * tw + 1;
       const int64_t n0 = (int64_t)B.z0 * nxy + col0 + (int64_t)(yy - 1) * p.nx + (xx - 1);
       const int64_t d0 = dist_index<PRIV>(p, B, X0 + xx - 1, Y0 + yy - 1, B.z0);
@@ -704,7 +711,9 @@ __global__ void __launch_bounds__(TX * TY, 1) lattice_tile_kernel(LatParams p) {
 // CTA repeatedly takes the next tile, visits it and queues the tiles whose
 // halo it improved.  A tile is in the queue at most once (state 1) and is
 // visited by one CTA at a time (state 2); if its halo improves during a visit
-// (state 3) it queues itself again afterwards.  `pending` counts tiles in
+// (state 3) the same CTA visits it again at once (or, with that switched
+// off, queues it again).  Only the visiting CTA writes a tile's cells, so
+// the copy in its shared memory stays exact between the two visits.  `pending` counts tiles in
 // states 1-3; it is raised before a tile is queued and lowered only after the
 // visiting CTA has queued everything it activated, so it reaches 0 only when
 // no tile can change again - the fixpoint.
@@ -747,8 +756,10 @@ __global__ void __launch_bounds__(TX * TY, MINB) lattice_async_kernel(LatParams 
   __syncthreads();
   unsigned visits = 0;
   unsigned long long sched_ns = 0;
+  __shared__ int s_cont;
+  if (threadIdx.x == 0) s_cont = -1;
   for (;;) {
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && s_cont < 0) {
       const unsigned long long tq = dev_globaltimer();
       int t = -1;
       if (!ld_acquire_u32((const unsigned *)&ctl->err)) {
@@ -782,10 +793,11 @@ __global__ void __launch_bounds__(TX * TY, MINB) lattice_async_kernel(LatParams 
       sched_ns += dev_globaltimer() - tq;
     }
     __syncthreads();
-    const int t = s_tile;
+    const bool warm = s_cont >= 0;
+    const int t = warm ? s_cont : s_tile;
     __syncthreads();
     if (t < 0) break;
-    process_tile<TX, TY, PRIV, false, DEEP>(p, t, sd, s_layers, s_flags, s_act, s_nb);
+    process_tile<TX, TY, PRIV, false, DEEP>(p, t, sd, s_layers, s_flags, s_act, s_nb, warm);
     // neighbours are activated by threads 0..3 in parallel, after this
     // tile's distances are visible
     unsigned long long ta = 0;
@@ -799,15 +811,27 @@ __global__ void __launch_bounds__(TX * TY, MINB) lattice_async_kernel(LatParams 
     if (threadIdx.x == 0) {
       // leave the visiting state: back to idle, or queued again when dirty
       // (halo changed meanwhile) or not converged
+      s_cont = -1;
       if (s_act[4] || atomicCAS(&p.tstate[t], 2, 0) != 2) {
-        atomicExch(&p.tstate[t], 1);
-        queue_tile(p, t);
+        if (p.selfcont) {
+          // visit it again at once: the interior and weights are already in
+          // shared memory, so only the halo is read again, and there is no
+          // queue handoff.  Visiting again (state 2) is published before the
+          // halo is read.
+          atomicExch(&p.tstate[t], 2);
+          __threadfence();
+          s_cont = t;
+        } else {
+          atomicExch(&p.tstate[t], 1);
+          queue_tile(p, t);
+        }
       } else {
         atomicSub(&ctl->pending, 1);
       }
       ++visits;
       sched_ns += dev_globaltimer() - ta;
     }
+    __syncthreads();
   }
   if (threadIdx.x == 0) {
     atomicAdd(&ctl->visits, visits);
@@ -1036,6 +1060,8 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   const int bps = std::max(1, std::min(occ, want));
   p.max_rounds = (unsigned)std::min<unsigned long long>(64ull * (unsigned long long)ntiles + 4096ull, 1ull << 30);
   p.wait_ns = env_u64("ORSP_WAIT_NS", 2000000000ull);
+  // ORSP_LAT_SELF=0: a tile to visit again goes back to the queue instead
+  p.selfcont = (int)env_u64("ORSP_LAT_SELF", 1);
   p.budget_ns = env_u64("ORSP_BUDGET_NS", 20000000000ull);
   void *args[] = {&p};
   if (orsp::g_timer.on) ORSP_CUDA(cudaEventRecord(orsp::g_timer.a, st));
