@@ -6,8 +6,8 @@
 
 The steps are those of the reference's `main.py headless` (main.py:287-622):
 read the board (orp.read_orp / orp_to_board_data), build the routing lattice
-and the pad-to-pad tasks, route with negotiated congestion, emit tracks and
-vias, write the solution (ors.write_ors).  The board -> problem mapping
+and the tasks (portal to portal, or pad to pad), route with negotiated
+congestion, emit tracks and vias, write the solution (ors.write_ors).  The board -> problem mapping
 follows the reference's router:
 
 * routing area: the pads of nets with two or more pads, plus 3 mm
