@@ -21,6 +21,9 @@ order, give the reference's portals and escape stubs:
 * stub geometry: vertical from the pad, a 45-degree tail when the pad is off
   its grid column                                              PEP:960-1035
 
+The planner's gap-filling portals are switched off in the reference
+(PEP:333-334) and are not restated.
+
 Reference quirks kept for parity: pads are never skipped as through-hole
 (the board model's pads have no 'drill' attribute), every pad counts as an
 F.Cu pad, and only pads without a component (whose keys carry their

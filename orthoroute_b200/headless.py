@@ -173,7 +173,9 @@ def build_problem(board_data: dict, pitch: float = DEFAULT_PITCH, portals: bool 
                                  for q in pads[:2])
     prob = HeadlessProblem(lat, [], np.zeros(0, np.int32), np.zeros(0, np.int32), {}, gx0, gy0, pitch, names,
                            layer_directions(nz), pad_nodes, [(c, members[c]) for c in order], net_pads)
-    if portals:
+    # a one-layer board has no routing layer to enter (the reference's
+    # fallback there names layers 1 and 2, outside its lattice): pad to pad
+    if portals and nz >= 2:
         from .escapes import plan_escapes
         prob.portals, prob.escape_tracks = plan_escapes(board_data, prob, seed=escape_seed)
     tnames, src, dst, ssrc, sdst, trivial = [], [], [], [], [], {}

@@ -103,6 +103,17 @@ def test_pad_escapes_match_reference(gorp, suffix):
         assert (s0, d0) == (s, d)
 
 
+def test_one_layer_board_routes_pad_to_pad(gorp):
+    """A one-layer board has no routing layer for portals: its tasks stay
+    pad to pad and every node is inside the lattice."""
+    bd = dict(gorp["converted"], layers=1, layer_names=["F.Cu"])
+    prob = build_problem(bd, portals=True)
+    ref = build_problem(bd)
+    assert not prob.portals and not prob.escape_tracks
+    assert np.array_equal(prob.src, ref.src) and np.array_equal(prob.search_dst, ref.dst)
+    assert prob.lattice.nz == 1 and int(max(prob.src.max(), prob.dst.max())) < prob.lattice.N
+
+
 def test_merge_escapes_dedupe():
     """Escape stubs go in front; a routed track equal to a stub up to
     0.001 mm is dropped, and so is a repeated via."""
