@@ -117,8 +117,7 @@ def plan_escapes(board_data: dict, prob, seed: int = 42, grid_pitch: float = Non
 
     pad_list = []
     for comp, pads in prob.components:
-        for p in pads:
-            pid = prob.pad_key(p, comp)
+        for p, pid in pads:
             if pid not in routable:
                 continue
             px, py = p.get("x", 0.0), p.get("y", 0.0)

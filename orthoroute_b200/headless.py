@@ -70,17 +70,13 @@ class HeadlessProblem:
     layer_names: List[str]
     layer_dirs: List[str]
     pad_nodes: Dict[str, int] = field(default_factory=dict)  # pad key -> grid node, the reference's order
-    components: List[Tuple[str, List[dict]]] = field(default_factory=list)  # (component, its pads)
+    components: List[Tuple[str, List[Tuple[dict, str]]]] = field(default_factory=list)  # (component, [(pad, key)])
     net_pads: Dict[str, Tuple[str, str]] = field(default_factory=dict)  # net -> keys of its first two pads
     portals: Dict[str, object] = field(default_factory=dict)  # pad key -> escapes.Portal (portal runs)
     escape_tracks: List[dict] = field(default_factory=list)
     # search endpoints per task: src / dst, or the F.Cu nodes of both portals
     search_src: np.ndarray = None
     search_dst: np.ndarray = None
-
-    @staticmethod
-    def pad_key(pad: dict, comp: str) -> str:
-        return _pad_key(pad, comp, _pad_id(pad))
 
 
 def routing_bounds(board_data: dict) -> Tuple[float, float, float, float]:
@@ -108,10 +104,6 @@ def grid_geometry(bounds, pitch: float):
     return gx0, gy0, int((gx1 - gx0) / pitch) + 1, int((gy1 - gy0) / pitch) + 1
 
 
-def _pad_id(p: dict) -> str:
-    return p.get("name", p.get("id", "")) or p.get("id", "")
-
-
 def _pad_key(pad: dict, comp: str, pad_id: str) -> str:
     if comp == "GENERIC_COMPONENT":
         return f"{comp}_{pad_id}@{int(round(pad.get('x', 0.0) * 1000))},{int(round(pad.get('y', 0.0) * 1000))}"
@@ -132,8 +124,6 @@ def build_problem(board_data: dict, pitch: float = DEFAULT_PITCH, portals: bool 
     lat = build_lattice(nx, ny, nz, planar="inner" if nz > 2 else "all", vias="adjacent")
     plane = nx * ny
 
-    pad_id = _pad_id
-
     def snap(p) -> int:
         xi = min(max(round((p.get("x", 0.0) - gx0) / pitch), 0), nx - 1)
         yi = min(max(round((p.get("y", 0.0) - gy0) / pitch), 0), ny - 1)
@@ -142,35 +132,37 @@ def build_problem(board_data: dict, pitch: float = DEFAULT_PITCH, portals: bool 
         return z * plane + yi * nx + xi
 
     # components in the order the reference's headless flow builds them: the
-    # board's component list, then components first seen on net pads
+    # board's component list, then components first seen on net pads.  A
+    # pad's id is its name, else its id, else pad_<k> with k the number of
+    # pads built before it, nets in order (main.py:397-411).
     order: List[str] = []
-    members: Dict[str, List[dict]] = {}
+    members: Dict[str, List[Tuple[dict, str]]] = {}
     for c in board_data.get("components", []):
         ref = c.get("reference", c.get("id", ""))
         if ref and ref not in members:
             members[ref] = []
             order.append(ref)
-    for net in board_data.get("nets", {}).values():
+    net_pads: Dict[str, Tuple[str, str]] = {}
+    k = 0
+    for net_id, net in board_data.get("nets", {}).items():
+        keys = []
         for p in net.get("pads", []):
             if not isinstance(p, dict):
                 continue
             comp = p.get("component", "") or "GENERIC_COMPONENT"
+            key = _pad_key(p, comp, p.get("name", p.get("id", "")) or p.get("id", f"pad_{k}"))
+            k += 1
+            keys.append(key)
             if comp not in members:
                 members[comp] = []
                 order.append(comp)
-            members[comp].append(p)
+            members[comp].append((p, key))
+        if len(keys) >= 2:
+            net_pads[net_id] = (keys[0], keys[1])
     pad_nodes: Dict[str, int] = {}
     for comp in order:
-        for p in members[comp]:
-            pad_nodes[_pad_key(p, comp, pad_id(p))] = snap(p)
-
-    net_pads: Dict[str, Tuple[str, str]] = {}
-    for net_id, net in board_data.get("nets", {}).items():
-        pads = [p for p in net.get("pads", []) if isinstance(p, dict)]
-        if len(pads) < 2:
-            continue
-        net_pads[net_id] = tuple(_pad_key(q, q.get("component", "") or "GENERIC_COMPONENT", pad_id(q))
-                                 for q in pads[:2])
+        for p, key in members[comp]:
+            pad_nodes[key] = snap(p)
     prob = HeadlessProblem(lat, [], np.zeros(0, np.int32), np.zeros(0, np.int32), {}, gx0, gy0, pitch, names,
                            layer_directions(nz), pad_nodes, [(c, members[c]) for c in order], net_pads)
     # a one-layer board has no routing layer to enter (the reference's

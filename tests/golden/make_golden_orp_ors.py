@@ -157,17 +157,21 @@ def _reference_board(bd, models):
             comps[cid] = Component(id=cid, reference=cid, value=c.get("value", ""), footprint=c.get("footprint", ""),
                                    position=Coordinate(x=c.get("x", 0.0), y=c.get("y", 0.0)),
                                    angle=c.get("rotation", 0.0))
+    n_pads = 0
     for net_id, info in bd.get("nets", {}).items():
         net = Net(id=net_id, name=info.get("name", net_id))
         net.pads = []
         for pr in info.get("pads", []):
+            if not isinstance(pr, dict):
+                continue
             pname = pr.get("name", pr.get("id", ""))
             cid = pr.get("component", "")
-            p = Pad(id=pname or pr.get("id", "pad"), component_id=cid, net_id=net_id,
+            p = Pad(id=pname or pr.get("id", f"pad_{n_pads}"), component_id=cid, net_id=net_id,
                     position=Coordinate(x=pr.get("x", 0.0), y=pr.get("y", 0.0)),
                     size=(pr.get("width", 0.2), pr.get("height", 0.2)), drill_size=pr.get("drill"),
                     layer=pr.get("layers", ["F.Cu"])[0] if pr.get("layers") else "F.Cu")
             net.pads.append(p)
+            n_pads += 1
             if not cid:
                 cid = "GENERIC_COMPONENT"
                 p.component_id = cid
