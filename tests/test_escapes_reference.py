@@ -1,10 +1,13 @@
-"""Pad escapes (orthoroute_b200.escapes) against the reference's own
+"""The headless board mapping and pad escapes (orthoroute_b200.headless,
+orthoroute_b200.escapes) against the reference's own router set-up and
 PadEscapePlanner on seeded random boards (CPU only; needs the reference
-source tree and is skipped where it is absent).  The boards mix clearance-set
-footprints, pads of several sizes, pads slightly off their grid column (kept,
-with a 45-degree stub tail) and far off it (dropped), and one-pad obstacle
-nets, so that column planning, shortening, the clearance checks and the
-random entry layers all come into play."""
+source tree and is skipped where it is absent).  The escape boards mix
+clearance-set footprints, pads of several sizes, pads slightly off their grid
+column (kept, with a 45-degree stub tail) and far off it (dropped), and
+one-pad obstacle nets, so that column planning, shortening, the clearance
+checks and the random entry layers all come into play.  The mapping boards
+mix component pads with repeated names, componentless pads with and without
+ids, pads on other layers and pads on grid-rounding ties."""
 import importlib.util
 import json
 import logging
@@ -99,3 +102,57 @@ def test_pad_escapes_equal_reference_on_random_boards(reference, seed):
     tasks = {n: [int(s), int(d)] for n, s, d in zip(prob.names, prob.src, prob.dst)}
     assert list(tasks.items()) == list(ref["tasks"].items())
     assert {k: int(v) for k, v in prob.trivial.items()} == ref["trivial"]
+
+
+def random_component_board(seed: int) -> dict:
+    """Named component pads on random layers, repeated pad names within a
+    component (the later pad keeps the key), componentless pads with and
+    without ids, pads near grid-rounding ties, nets of one to four pads."""
+    rng = np.random.default_rng(seed)
+    nz = int(rng.choice([2, 3, 4, 8]))
+    names = ["F.Cu"] + [f"In{i}.Cu" for i in range(1, nz - 1)] + ["B.Cu"]
+    pads, nets, comps = [], {}, []
+    for c in range(int(rng.integers(2, 6))):
+        comps.append({"reference": f"U{c}", "x": 30.0, "y": 30.0})
+    for n in range(int(rng.integers(6, 16))):
+        net = f"S{n}"
+        for m in range(int(rng.integers(1, 5))):
+            kind = rng.integers(0, 4)
+            x = 20.0 + 15.0 * float(rng.random())
+            y = 20.0 + 15.0 * float(rng.random())
+            if kind == 3:  # on a rounding tie of the 0.4 grid
+                x = 20.0 + 0.4 * int(rng.integers(0, 30)) + 0.2
+            p = {"net_name": net, "net_code": n, "x": round(x, 3), "y": round(y, 3), "width": 0.3, "height": 0.3,
+                 "drill": None, "type": "smd",
+                 "layers": [names[int(rng.integers(0, nz))]] if rng.random() < 0.5 else ["F.Cu"]}
+            if kind == 0:
+                p.update(component="", name="")
+            elif kind == 1:
+                p.update(component="", name="", id=f"P{n}_{m}")
+            else:
+                p.update(component=f"U{int(rng.integers(0, len(comps)))}", name=str(int(rng.integers(1, 6))))
+            pads.append(p)
+            nets.setdefault(net, {"name": net, "code": n, "pads": []})["pads"].append(p)
+    return {"filename": f"comp{seed}.kicad_pcb", "x_min": 15.0, "y_min": 15.0, "x_max": 40.0, "y_max": 40.0,
+            "width": 25.0, "height": 25.0, "layers": nz, "layer_names": names, "pads": pads, "nets": nets,
+            "components": comps, "grid_resolution": 0.4}
+
+
+@pytest.mark.timeout(600)
+@pytest.mark.parametrize("seed", [21, 22, 23, 24, 25, 26])
+def test_headless_mapping_equals_reference_on_random_boards(reference, seed):
+    """Grid, layer directions, pad-to-pad tasks (dict order) and one-node
+    routes against the reference router's set-up of the same board."""
+    from orthoroute_b200.headless import build_problem
+
+    gmod, upf, models = reference
+    bd = json.loads(json.dumps(random_component_board(seed)))
+    m = gmod.reference_mapping(bd, upf, models)
+    prob = build_problem(bd, pitch=m["pitch"])
+    lat = prob.lattice
+    assert (lat.nx, lat.ny, lat.nz) == (m["x_steps"], m["y_steps"], m["layers"])
+    assert prob.grid_min_x == m["grid_min_x"] and prob.grid_min_y == m["grid_min_y"]
+    assert prob.layer_dirs == m["layer_directions"]
+    tasks = {n: [int(s), int(d)] for n, s, d in zip(prob.names, prob.src, prob.dst)}
+    assert list(tasks.items()) == list(m["tasks"].items())
+    assert {k: int(v) for k, v in prob.trivial.items()} == m["trivial"]
