@@ -1,0 +1,133 @@
+"""The oracle against the reference's own CPU code on seeded random inputs,
+beyond the fixed golden vectors (CPU only; needs the reference source tree
+and is skipped where it is absent): SimpleDijkstra.find_path_roi on random
+lattices, costs and ROIs (integer costs, where the reference's float64 path
+sums equal fp32), ROIExtractor.extract_roi_bfs with random depths and node
+caps, and the EdgeAccountant updates with random parameters."""
+import logging
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle as O
+from orthoroute_b200.lattice import build_lattice
+
+REF = Path(os.environ.get("ORTHOROUTE_REFERENCE", "/root/reference"))
+pytestmark = pytest.mark.skipif(not (REF / "orthoroute").exists(), reason="reference source tree not available")
+
+
+class _Graph:
+    """The CSR attributes the reference's solver and ROI classes read."""
+
+    def __init__(self, indptr, indices):
+        self.indptr = indptr
+        self.indices = indices
+        self.base_costs = None
+        self.xp = np
+
+
+@pytest.fixture(scope="module")
+def upf():
+    os.environ["PYTHONDONTWRITEBYTECODE"] = "1"
+    sys.dont_write_bytecode = True
+    if str(REF) not in sys.path:
+        sys.path.insert(0, str(REF))
+    logging.disable(logging.CRITICAL)
+    import orthoroute.algorithms.manhattan.unified_pathfinder as m
+
+    return m
+
+
+@pytest.mark.timeout(600)
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_dijkstra_equals_reference_on_random_lattices(upf, seed):
+    rng = np.random.default_rng(100 + seed)
+    dims = [(int(rng.integers(3, 14)), int(rng.integers(3, 14)), int(rng.integers(1, 7))) for _ in range(3)]
+    for nx, ny, nz in dims:
+        lat = build_lattice(nx, ny, nz)
+        g = _Graph(lat.indptr, lat.indices)
+        solver = upf.SimpleDijkstra(g, lattice=None)
+        ex = upf.ROIExtractor(g, use_gpu=False, lattice=None)
+        cost = rng.integers(1, 8, size=lat.E).astype(np.float32)
+        cost[lat.edge_kind == 1] = np.float32(rng.choice([2.0, 3.0, 5.0]))
+        cost[rng.random(lat.E) < rng.choice([0.0, 0.05, 0.2])] = np.float32(np.inf)
+        for j in range(10):
+            s, d = (int(v) for v in rng.choice(lat.N, size=2, replace=False))
+            if j % 2 == 0:
+                roi = np.arange(lat.N, dtype=np.int32)
+                g2r = np.arange(lat.N, dtype=np.int32)
+            else:
+                roi, g2r = ex.extract_roi_bfs(s, d, initial_radius=int(rng.integers(1, 10)))
+            ref = upf.SimpleDijkstra.find_path_roi(solver, s, d, cost, roi, g2r)
+            m = np.full(lat.N, -1, np.int32)
+            m[np.asarray(roi)] = np.arange(len(roi), dtype=np.int32)
+            p, *_ = O.dijkstra(lat.indptr, lat.indices, cost, [s], dst=d, roi_map=m)
+            got = p.tolist() if len(p) > 1 else None
+            assert got == (list(map(int, ref)) if ref else None), (nx, ny, nz, s, d)
+
+
+@pytest.mark.timeout(600)
+@pytest.mark.parametrize("seed", [1, 2])
+def test_roi_bfs_equals_reference_on_random_cases(upf, seed):
+    rng = np.random.default_rng(200 + seed)
+    lat = build_lattice(int(rng.integers(10, 30)), int(rng.integers(10, 30)), int(rng.integers(2, 6)))
+    g = _Graph(lat.indptr, lat.indices)
+    for _ in range(16):
+        max_nodes = int(rng.choice([50_000, 800, 200, 60]))
+        ex = upf.ROIExtractor(g, use_gpu=False, lattice=None)
+        ex.max_roi_nodes = max_nodes
+        s, d = (int(v) for v in rng.choice(lat.N, size=2, replace=False))
+        depth = int(rng.integers(1, 60))
+        ref, _ = ex.extract_roi_bfs(s, d, initial_radius=depth)
+        roi, g2r = O.roi_bfs(lat.indptr, lat.indices, s, d, min(depth, 150), max_nodes)
+        assert np.array_equal(roi, np.asarray(ref, np.int32)), (s, d, depth, max_nodes)
+        assert np.array_equal(g2r[roi], np.arange(len(roi)))
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3, 4])
+def test_accounting_equals_reference_with_random_parameters(upf, seed):
+    rng = np.random.default_rng(300 + seed)
+    E, L = int(rng.integers(1000, 30000)), int(rng.integers(2, 10))
+    base = rng.choice(np.array([0.4, 0.7, 1.0, 3.0], np.float32), size=E)
+    present = rng.integers(0, 5, size=E).astype(np.float32)
+    ema = (rng.random(E) * 3).astype(np.float32)
+    cap = rng.choice(np.array([1.0, 2.0], np.float32), size=E)
+    hist = (rng.random(E) * 5).astype(np.float32)
+    edge_layer = rng.integers(0, L, size=E).astype(np.uint8)
+    edge_kind = (rng.random(E) < 0.4).astype(np.uint8)
+    bias = (0.3 + 1.7 * rng.random(L)).astype(np.float32)
+    for _ in range(3):
+        pf, hw = float(rng.choice([0.5, 1.5, 7.59375, 64.0])), float(rng.choice([1.0, 10.0, 12.0]))
+        vm, bw = float(rng.choice([0.5, 1.0, 1.5])), float(rng.choice([0.01, 0.3, 1.0]))
+        jit, ub = bool(rng.random() < 0.5), bool(rng.random() < 0.5)
+        acc = upf.EdgeAccountant(E, use_gpu=False)
+        acc.present_ema, acc.capacity, acc.history = ema.copy(), cap.copy(), hist.copy()
+        acc.update_costs(base, pf, hw, add_jitter=jit, via_cost_multiplier=vm, base_cost_weight=bw,
+                         edge_layer=edge_layer if ub else None, layer_bias_per_layer=bias if ub else None,
+                         edge_kind=edge_kind if ub else None)
+        got = O.update_costs(base, ema, cap, hist, pf, hw, add_jitter=jit, via_cost_multiplier=vm,
+                             base_cost_weight=bw, edge_layer=edge_layer if ub else None,
+                             layer_bias_per_layer=bias if ub else None, edge_kind=edge_kind if ub else None)
+        assert np.array_equal(np.asarray(acc.total_cost, np.float32).view(np.uint32),
+                              np.asarray(got, np.float32).view(np.uint32))
+        gain, capm = float(rng.choice([0.25, 1.0, 1.2])), float(rng.choice([10.0, 15.0]))
+        decay, use_base = float(rng.choice([0.98, 1.0])), bool(rng.random() < 0.5)
+        acc = upf.EdgeAccountant(E, use_gpu=False)
+        acc.present, acc.present_ema, acc.capacity, acc.history = present.copy(), ema.copy(), cap.copy(), hist.copy()
+        acc.update_history(gain, base_costs=base if use_base else None, history_cap_multiplier=capm,
+                           decay_factor=decay, use_raw_present=True)
+        got = O.update_history(hist.copy(), present, cap, gain, base_costs=base if use_base else None,
+                               history_cap_multiplier=capm, decay_factor=decay)
+        assert np.array_equal(np.asarray(acc.history, np.float32).view(np.uint32),
+                              np.asarray(got, np.float32).view(np.uint32))
+    acc = upf.EdgeAccountant(E, use_gpu=False)
+    acc.present, acc.present_ema = present.copy(), ema.copy()
+    acc.update_present_ema(beta=0.4)
+    assert np.array_equal(np.asarray(acc.present_ema, np.float32).view(np.uint32),
+                          np.asarray(O.update_present_ema(present, ema, 0.4), np.float32).view(np.uint32))
+    acc = upf.EdgeAccountant(E, use_gpu=False)
+    acc.present, acc.capacity = present.copy(), cap.copy()
+    assert tuple(acc.compute_overuse(None)) == O.compute_overuse(present, cap)
