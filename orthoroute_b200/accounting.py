@@ -8,7 +8,7 @@ is still available as a dict view for callers that read it.
 """
 from __future__ import annotations
 
-from typing import Dict, List, Tuple
+from typing import Dict, Tuple
 
 import numpy as np
 import torch

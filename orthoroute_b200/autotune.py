@@ -18,7 +18,7 @@ plan may only change the time), and installs the fastest plan on the graph
 from __future__ import annotations
 
 from dataclasses import dataclass, field
-from typing import Dict, List, Optional, Sequence
+from typing import Dict, List, Sequence
 
 import numpy as np
 import torch

@@ -18,7 +18,7 @@ from __future__ import annotations
 
 import ctypes
 import random
-from typing import Dict, Iterable, List, Optional, Sequence, Set, Tuple
+from typing import Dict, List, Optional, Sequence, Set, Tuple
 
 import numpy as np
 import torch

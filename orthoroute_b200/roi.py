@@ -2,8 +2,6 @@
 (orthoroute/algorithms/manhattan/unified_pathfinder.py:1345-1780)."""
 from __future__ import annotations
 
-import ctypes
-
 import numpy as np
 import torch
 

@@ -11,7 +11,7 @@ fp32 semantics of SimpleDijkstra.find_path_roi (UPF:1801-1887).
 from __future__ import annotations
 
 import ctypes
-from typing import List, Optional, Sequence
+from typing import List, Optional
 
 import numpy as np
 import torch

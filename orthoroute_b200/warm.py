@@ -22,7 +22,6 @@ net bounding-box coverage, H-layer flag, V-layer flag, layer position.
 """
 from __future__ import annotations
 
-import ctypes
 import math
 from dataclasses import dataclass
 from typing import Dict, List, Optional, Tuple

@@ -6,7 +6,6 @@ import subprocess
 from pathlib import Path
 
 import numpy as np
-import pytest
 
 REPO = Path(__file__).resolve().parent.parent
 

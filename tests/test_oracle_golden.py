@@ -1,7 +1,6 @@
 """The oracle is pinned to golden vectors produced by the reference's own code
 (tests/golden/make_golden.py).  CPU only."""
 import numpy as np
-import pytest
 
 import oracle as O
 

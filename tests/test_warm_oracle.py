@@ -2,7 +2,6 @@
 central finite differences in float64, and its weight layout against a
 direct evaluation of the convolution sum.  CPU only."""
 import numpy as np
-import pytest
 import torch
 
 from oracle import warm_ref as R
