@@ -31,6 +31,7 @@ coordinates) enter the clearance set.
 """
 from __future__ import annotations
 
+import math
 import random
 from dataclasses import dataclass
 from typing import Dict, List, Tuple
@@ -56,21 +57,32 @@ class Portal:
 
 def _clearance_set(board_data: dict, pad_keys) -> Dict[str, dict]:
     """Pads whose keys carry coordinates ('...@x_um,y_um'), matched to the
-    board's pads by position (first key within 0.01 mm)."""
+    board's pads by position: for each pad, the first key (in key order)
+    within 0.01 mm on both axes.  The keys are bucketed in 0.01 mm cells, so
+    each pad tests only the keys of the cells around it with the same
+    comparison."""
+    cells: Dict[Tuple[int, int], List[Tuple[int, str, float, float]]] = {}
+    for order, pid in enumerate(pad_keys):
+        if "@" not in pid:
+            continue
+        try:
+            xu, yu = map(int, pid.split("@")[1].split(","))
+        except ValueError:
+            continue
+        kx, ky = xu / 1000.0, yu / 1000.0
+        cells.setdefault((math.floor(kx / 0.01), math.floor(ky / 0.01)), []).append((order, pid, kx, ky))
     geoms = {}
-    keys = list(pad_keys)
     for p in board_data.get("pads", []):
         x, y = p["x"], p["y"]
-        for pid in keys:
-            if "@" not in pid:
-                continue
-            try:
-                xu, yu = map(int, pid.split("@")[1].split(","))
-            except ValueError:
-                continue
-            if abs(xu / 1000.0 - x) < 0.01 and abs(yu / 1000.0 - y) < 0.01:
-                geoms[pid] = {"x": x, "y": y, "width": p["width"], "height": p["height"]}
-                break
+        cx, cy = math.floor(x / 0.01), math.floor(y / 0.01)
+        best = None
+        for dx in (-2, -1, 0, 1, 2):  # a key within 0.01 mm lies at most one cell away; two for rounding
+            for dy in (-2, -1, 0, 1, 2):
+                for order, pid, kx, ky in cells.get((cx + dx, cy + dy), ()):
+                    if (best is None or order < best[0]) and abs(kx - x) < 0.01 and abs(ky - y) < 0.01:
+                        best = (order, pid)
+        if best is not None:
+            geoms[best[1]] = {"x": x, "y": y, "width": p["width"], "height": p["height"]}
     return geoms
 
 
@@ -156,14 +168,30 @@ def plan_escapes(board_data: dict, prob, seed: int = 42, grid_pitch: float = Non
                 room = MAX_STEPS
             top = max(min(MAX_STEPS, room, edge), MIN_STEPS)
             plan.append([pid, yi, d, rng.randint(MIN_STEPS, top), px, py])
-        for it in range(100):  # pairwise shortening of overlapping escapes
+        # Pairwise shortening of overlapping escapes, pairs in (i, j) order.
+        # Lengths stay within MIN_STEPS..MAX_STEPS and the column is sorted
+        # by row, so pads more than 2 * MAX_STEPS + 1 rows apart never
+        # overlap; only those pairs are skipped (they neither hit nor change
+        # a length).
+        n = len(plan)
+        reach = 2 * MAX_STEPS + 1
+        for it in range(100):
             hit = False
-            for i in range(len(plan)):
-                for j in range(i + 1, len(plan)):
-                    a, b = plan[i], plan[j]
-                    ya, yb = a[1] + a[2] * a[3], b[1] + b[2] * b[3]
-                    lo_a, hi_a = min(a[1], ya), max(a[1], ya)
-                    lo_b, hi_b = min(b[1], yb), max(b[1], yb)
+            for i in range(n):
+                a = plan[i]
+                ya0 = a[1]
+                for j in range(i + 1, n):
+                    b = plan[j]
+                    if b[1] - ya0 > reach:
+                        break
+                    if a[2] > 0:
+                        lo_a, hi_a = ya0, ya0 + a[3]
+                    else:
+                        lo_a, hi_a = ya0 - a[3], ya0
+                    if b[2] > 0:
+                        lo_b, hi_b = b[1], b[1] + b[3]
+                    else:
+                        lo_b, hi_b = b[1] - b[3], b[1]
                     if not (hi_a + 1 < lo_b or hi_b + 1 < lo_a):
                         hit = True
                         if it % 2 == 0:

@@ -30,7 +30,9 @@ def _golden_module():
     return mod
 
 
-def random_board(seed: int) -> dict:
+def random_board(seed: int, rows: int = 30) -> dict:
+    """rows: the span of footprint origins in grid rows (tall boards put many
+    pads, far apart, in the same columns)."""
     rng = np.random.default_rng(seed)
     nz = int(rng.choice([2, 4, 6]))
     names = ["F.Cu"] + [f"In{i}.Cu" for i in range(1, nz - 1)] + ["B.Cu"]
@@ -47,8 +49,8 @@ def random_board(seed: int) -> dict:
     nfp = int(rng.integers(2, 5))
     sites = []
     for f in range(nfp):
-        x0 = 20.0 + 0.4 * int(rng.integers(0, 30))
-        y0 = 20.0 + 0.4 * int(rng.integers(0, 30))
+        x0 = 20.0 + 0.4 * int(rng.integers(0, 12 if rows > 30 else 30))
+        y0 = 20.0 + 0.4 * int(rng.integers(0, rows))
         rows, cols = int(rng.integers(1, 3)), int(rng.integers(3, 9))
         w = float(rng.choice([0.25, 0.3, 0.45]))
         for c in range(cols):
@@ -67,9 +69,9 @@ def random_board(seed: int) -> dict:
     for m in range(int(rng.integers(3, 8))):
         pad(f"OBS{m}", 20.0 + 12.0 * float(rng.random()), 20.0 + 12.0 * float(rng.random()),
             float(rng.choice([0.3, 0.6])), float(rng.choice([0.3, 0.6])))
-    return {"filename": f"random{seed}.kicad_pcb", "x_min": 15.0, "y_min": 15.0, "x_max": 40.0, "y_max": 40.0,
-            "width": 25.0, "height": 25.0, "layers": nz, "layer_names": names, "pads": pads, "nets": nets,
-            "grid_resolution": 0.4}
+    return {"filename": f"random{seed}.kicad_pcb", "x_min": 15.0, "y_min": 15.0, "x_max": 40.0,
+            "y_max": 25.0 + 0.4 * rows, "width": 25.0, "height": 10.0 + 0.4 * rows, "layers": nz,
+            "layer_names": names, "pads": pads, "nets": nets, "grid_resolution": 0.4}
 
 
 @pytest.fixture(scope="module")
@@ -86,12 +88,13 @@ def reference():
 
 
 @pytest.mark.timeout(600)
-@pytest.mark.parametrize("seed", [11, 12, 13, 14, 15, 16])
-def test_pad_escapes_equal_reference_on_random_boards(reference, seed):
+@pytest.mark.parametrize("seed,rows", [(11, 30), (12, 30), (13, 30), (14, 30), (15, 30), (16, 30), (17, 160),
+                                       (18, 160)])
+def test_pad_escapes_equal_reference_on_random_boards(reference, seed, rows):
     from orthoroute_b200.headless import build_problem
 
     gmod, upf, models = reference
-    bd = json.loads(json.dumps(random_board(seed)))
+    bd = json.loads(json.dumps(random_board(seed, rows)))
     ref = gmod.reference_portals(bd, upf, models)
     prob = build_problem(bd, portals=True)
     got = [[pid, p.x_idx, p.y_idx, p.pad_layer, p.delta_steps, p.direction, p.pad_x, p.pad_y, p.entry_layer]
