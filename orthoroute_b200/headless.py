@@ -199,6 +199,21 @@ def build_problem(board_data: dict, pitch: float = DEFAULT_PITCH, portals: bool 
     return prob
 
 
+def portal_collisions(prob: HeadlessProblem) -> int:
+    """Grid points where the portals of two or more pads of different nets
+    end.  Their escape stubs meet there (a short in the planner's output),
+    and on this lattice the nets also share the portal's single via edge, so
+    the route cannot reach zero overuse while any remain."""
+    pad_net = {}
+    for net, (k1, k2) in prob.net_pads.items():
+        pad_net.setdefault(k1, net)
+        pad_net.setdefault(k2, net)
+    nets_at: Dict[Tuple[int, int], set] = {}
+    for pid, pt in prob.portals.items():
+        nets_at.setdefault((pt.x_idx, pt.y_idx), set()).add(pad_net.get(pid, pid))
+    return sum(1 for v in nets_at.values() if len(v) > 1)
+
+
 def merge_escapes(escape_tracks: List[dict], tracks: List[dict], vias: List[dict]):
     """Escape stubs in front of the routed tracks, later duplicates dropped
     by (net, layer, ends and width to 0.001 mm); vias deduplicated by (net,
@@ -290,7 +305,10 @@ def run_headless(orp_file: str, output_file: Optional[str] = None, max_iteration
                "converged": bool(res.converged), "iterations": len(metrics), "tracks": len(tracks),
                "vias": len(vias), "seconds_total": round(total, 3), "seconds_route": round(res.seconds, 3),
                "lattice": [prob.lattice.nx, prob.lattice.ny, prob.lattice.nz], "portals": len(prob.portals),
-               "escape_tracks": len(prob.escape_tracks)}
+               "escape_tracks": len(prob.escape_tracks), "portal_collisions": portal_collisions(prob)}
+    if log and summary["portal_collisions"]:
+        log(f"warning: {summary['portal_collisions']} grid points hold the portals of two nets "
+            "(their escape stubs meet); route with --no-portals to avoid them")
     if log:
         log(json.dumps(summary))
     return summary

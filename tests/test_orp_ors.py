@@ -103,6 +103,29 @@ def test_pad_escapes_match_reference(gorp, suffix):
         assert (s0, d0) == (s, d)
 
 
+def test_portal_collisions_counted():
+    """Grid points where portals of different nets meet: none on the golden
+    boards, and a planted one (a third net's portal moved onto another's)
+    counts once."""
+    import copy
+    import json as _j
+
+    from orthoroute_b200.headless import portal_collisions
+
+    g = _j.loads((GOLDEN / "golden_orp.json").read_text())
+    for sfx in ("", "_2l", "_fp"):
+        prob = build_problem(g["converted" + sfx], portals=True)
+        assert portal_collisions(prob) == 0
+    prob = build_problem(g["converted_fp"], portals=True)
+    keys = list(prob.portals)
+    pad_net = {k: n for n, ks in prob.net_pads.items() for k in ks}
+    a = keys[0]
+    b = next(k for k in keys if pad_net.get(k) != pad_net.get(a))
+    prob.portals[b] = copy.copy(prob.portals[b])
+    prob.portals[b].x_idx, prob.portals[b].y_idx = prob.portals[a].x_idx, prob.portals[a].y_idx
+    assert portal_collisions(prob) == 1
+
+
 def test_one_layer_board_routes_pad_to_pad(gorp):
     """A one-layer board has no routing layer for portals: its tasks stay
     pad to pad and every node is inside the lattice."""
