@@ -124,10 +124,14 @@ def orp_to_board_data(orp: Dict[str, Any]) -> Dict[str, Any]:
             "type": kind,
         })
 
+    # each net's pads in pad order (grouped once instead of a scan per net)
+    by_net: Dict[str, List[Dict[str, Any]]] = {}
+    for p in pads:
+        by_net.setdefault(p["net_name"], []).append(p)
     nets = {}
     for n in orp.get("nets", []):
         name = n.get("name", "")
-        nets[name] = {"name": name, "code": 0, "pads": [p for p in pads if p["net_name"] == name]}
+        nets[name] = {"name": name, "code": 0, "pads": list(by_net.get(name, ()))}
 
     drc = orp.get("drc_rules", {})
     rules = drc.get("default", {})
@@ -189,9 +193,12 @@ def board_data_to_orp(board_data: Dict[str, Any], filename: str = "board.orp",
             "angle": 0.0,
         })
 
+    by_net: Dict[Any, List[int]] = {}
+    for i, p in enumerate(pads_in):
+        by_net.setdefault(p.get("net_name"), []).append(i)
     nets = []
     for name, net in bd.get("nets", {}).items():
-        members = [(i, p) for i, p in enumerate(pads_in) if p.get("net_name") == name]
+        members = [(i, pads_in[i]) for i in by_net.get(name, ())]
         terminals = []
         for i, p in members:
             layers = p.get("layers", ["F.Cu"])
