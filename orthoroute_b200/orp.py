@@ -61,10 +61,12 @@ def _load_json(path: Path) -> Dict[str, Any]:
 
 def _dump_json(data: Dict[str, Any], path: Path, compress: bool) -> None:
     path.parent.mkdir(parents=True, exist_ok=True)
-    opener = (lambda: gzip.open(path, "wt", encoding="utf-8")) if compress else (
+    # gzip level 6: a quarter of level 9's time for a file about 5 % larger
+    opener = (lambda: gzip.open(path, "wt", encoding="utf-8", compresslevel=6)) if compress else (
         lambda: open(path, "w", encoding="utf-8"))
+    text = json.dumps(data, indent=2, ensure_ascii=False)  # one write: the same text as json.dump
     with opener() as f:
-        json.dump(data, f, indent=2, ensure_ascii=False)
+        f.write(text)
 
 
 def read_orp(path) -> Dict[str, Any]:
