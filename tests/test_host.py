@@ -31,6 +31,14 @@ def test_library_exports_header_symbols():
     assert L.orsp_status_string(-3) == b"device timeout"
 
 
+def test_integration_guide_names_every_entry_point():
+    """Every entry point the headers declare appears in the integration
+    guide, which maps each to the reference interface it replaces."""
+    guide = (REPO / "INTEGRATION.md").read_text()
+    missing = [s for s in _header_symbols() if s not in guide]
+    assert not missing, missing
+
+
 def test_host_validation_without_gpu():
     """Argument checks run on the host before any CUDA call."""
     from orthoroute_b200 import _lib
