@@ -53,7 +53,9 @@ extern "C" {
 #define ORSP_ERR_NOMEM (-5)     /* device allocation failed                  */
 #define ORSP_ERR_INTERNAL (-6)  /* invariant broken (e.g. no predecessor)    */
 
-/* Version of this ABI; bumped on any signature change. */
+/* Version of this ABI; bumped on any signature change.  This function, the
+ * status names and the last-error message have no counterpart in the
+ * reference, which signals failures with Python exceptions or None. */
 #define ORSP_ABI_VERSION 1
 ORSP_API int orsp_abi_version(void);
 ORSP_API const char *orsp_status_string(int status);
@@ -84,10 +86,11 @@ ORSP_API int orsp_graph_create(int32_t num_nodes, int64_t num_edges,
                       int32_t nx, int32_t ny, int32_t nz, int device,
                       orsp_graph **out);
 ORSP_API int orsp_graph_destroy(orsp_graph *g);
-/* Device pointers of the uploaded CSR (indptr[N+1], indices[E]). */
+/* Device pointers of the uploaded CSR (indptr[N+1], indices[E]) and its
+ * largest out-degree, for callers that share them; no counterpart in the
+ * reference, which keeps its CSR on the host (CD:119-121). */
 ORSP_API int orsp_graph_csr(orsp_graph *g, const int32_t **indptr_d,
                    const int32_t **indices_d);
-/* Largest out-degree (known after create). */
 ORSP_API int orsp_graph_max_degree(orsp_graph *g, int32_t *out);
 /* 1 when the graph was recognised as an H/V routing lattice (every edge a
  * unit step along its layer's axis or a via between adjacent layers, no
@@ -208,7 +211,8 @@ ORSP_API int orsp_sssp_batch_ranges(orsp_graph *g, const float *cost_d, int32_t 
  *            distance slice, tile width tile_w[i] (16 or 32); used on graphs
  *            recognised as H/V lattices, impl 0 otherwise.
  * nb = 0 restores the default (impl 0 for every box).  Every plan gives the
- * same paths, bit for bit; the plan only changes the time. */
+ * same paths, bit for bit; the plan only changes the time.  No counterpart in
+ * the reference. */
 ORSP_API int orsp_batch_set_plan(orsp_graph *g, int32_t nb, const int64_t *max_nodes, const int32_t *impl,
                         const float *delta, const int32_t *tile_w, const int32_t *ctas_per_sm);
 
@@ -374,7 +378,8 @@ ORSP_API int orsp_update_costs_live(int64_t E, const int32_t *edges_d, int64_t n
                            const float *cap_d, const float *history_d, float pres_fac,
                            float hist_w, float via_mult, float base_w, int add_jitter,
                            float *total_out_d, uintptr_t stream);
-/* The same refresh over the path edges of a batch (rows of orsp_sssp_batch_bbox). */
+/* The same refresh (update_present_cost_only, UPF:1045-1068) over the path
+ * edges of a batch (rows of orsp_sssp_batch_bbox). */
 ORSP_API int orsp_update_costs_live_paths(int32_t K, const int32_t *path_edges_d,
                                  const int32_t *path_len_d, int32_t path_cap,
                                  const float *base_d, const int32_t *usage_d,
@@ -455,8 +460,9 @@ ORSP_API int orsp_present_from_usage(int64_t E, const int32_t *usage_d,
 ORSP_API int orsp_commit_edges(int64_t n, const int32_t *edges_d, int32_t *usage_d,
                       float *present_d, int32_t sign, uintptr_t stream);
 
-/* Batched commit of the paths produced by orsp_sssp_batch_bbox (path_len[k]
- * nodes give path_len[k]-1 edges; entries with path_len < 2 are skipped). */
+/* commit_path / clear_path (UPF:821-836) for every path of a batch produced
+ * by orsp_sssp_batch_bbox (path_len[k] nodes give path_len[k]-1 edges;
+ * entries with path_len < 2 are skipped). */
 ORSP_API int orsp_commit_batch(int32_t K, const int32_t *path_edges_d,
                       const int32_t *path_len_d, int32_t path_cap,
                       int32_t *usage_d, float *present_d, int32_t sign,
