@@ -2,8 +2,9 @@
 beyond the fixed golden vectors (CPU only; needs the reference source tree
 and is skipped where it is absent): SimpleDijkstra.find_path_roi on random
 lattices, costs and ROIs (integer costs, where the reference's float64 path
-sums equal fp32), ROIExtractor.extract_roi_bfs with random depths and node
-caps, and the EdgeAccountant updates with random parameters."""
+sums equal fp32), find_path_multisource_multisink with seed and portal
+costs, ROIExtractor.extract_roi_bfs with random depths and node caps, and the
+EdgeAccountant updates with random parameters."""
 import logging
 import os
 import sys
@@ -131,3 +132,37 @@ def test_accounting_equals_reference_with_random_parameters(upf, seed):
     acc = upf.EdgeAccountant(E, use_gpu=False)
     acc.present, acc.capacity = present.copy(), cap.copy()
     assert tuple(acc.compute_overuse(None)) == O.compute_overuse(present, cap)
+
+
+@pytest.mark.timeout(600)
+@pytest.mark.parametrize("seed", [1, 2])
+def test_multisource_multisink_equals_reference(upf, seed):
+    """find_path_multisource_multisink: seeds with start costs, targets with
+    portal costs (sinks; the best total wins, ties to the target settled
+    first), whole graph and BFS ROIs."""
+    rng = np.random.default_rng(400 + seed)
+    lat = build_lattice(int(rng.integers(6, 16)), int(rng.integers(6, 16)), int(rng.integers(2, 6)))
+    g = _Graph(lat.indptr, lat.indices)
+    solver = upf.SimpleDijkstra(g, lattice=None)
+    ex = upf.ROIExtractor(g, use_gpu=False, lattice=None)
+    cost = rng.integers(1, 6, size=lat.E).astype(np.float32)
+    cost[rng.random(lat.E) < 0.05] = np.float32(np.inf)
+    for i in range(16):
+        ns, nt = int(rng.integers(1, 5)), int(rng.integers(1, 6))
+        nodes = rng.choice(lat.N, size=ns + nt, replace=False)
+        seeds, targets = nodes[:ns], nodes[ns:]
+        scost = rng.integers(0, 4, size=ns) * 0.5
+        tcost = rng.integers(0, 4, size=nt) * 0.25
+        if i % 2:
+            roi, g2r = ex.extract_roi_bfs(int(seeds[0]), int(targets[0]), initial_radius=int(rng.integers(2, 12)))
+        else:
+            roi = np.arange(lat.N, dtype=np.int32)
+            g2r = np.arange(lat.N, dtype=np.int32)
+        ref = solver.find_path_multisource_multisink(list(zip(seeds.tolist(), scost.tolist())),
+                                                     list(zip(targets.tolist(), tcost.tolist())), cost, roi, g2r)
+        m = np.full(lat.N, -1, np.int32)
+        m[np.asarray(roi)] = np.arange(len(roi), dtype=np.int32)
+        p, *_ = O.dijkstra(lat.indptr, lat.indices, cost, seeds, roi_map=m, seed_cost=scost.astype(np.float32),
+                           targets=targets, target_cost=tcost)
+        got = p.tolist() if len(p) > 1 else None
+        assert got == (list(map(int, ref[0])) if ref else None), (i, seeds, targets)
