@@ -3,8 +3,9 @@ beyond the fixed golden vectors (CPU only; needs the reference source tree
 and is skipped where it is absent): SimpleDijkstra.find_path_roi on random
 lattices, costs and ROIs (integer costs, where the reference's float64 path
 sums equal fp32), find_path_multisource_multisink with seed and portal
-costs, ROIExtractor.extract_roi_bfs with random depths and node caps, and the
-EdgeAccountant updates with random parameters."""
+costs, ROIExtractor.extract_roi_bfs with random depths and node caps, the
+EdgeAccountant updates with random parameters, and the geometry emission
+(_generate_geometry_from_paths) on random walks."""
 import logging
 import os
 import sys
@@ -166,3 +167,71 @@ def test_multisource_multisink_equals_reference(upf, seed):
                            targets=targets, target_cost=tcost)
         got = p.tolist() if len(p) > 1 else None
         assert got == (list(map(int, ref[0])) if ref else None), (i, seeds, targets)
+
+
+def _random_path(rng, nx, ny, nz, dirs, n):
+    """A walk on the lattice: mostly legal planar steps along each layer's
+    axis and vias between adjacent layers, with a few illegal steps (a jump,
+    a step across the layer's axis) for the reference's guards to drop."""
+    x, y, z = int(rng.integers(0, nx)), int(rng.integers(0, ny)), int(rng.integers(0, nz))
+    path = [z * nx * ny + y * nx + x]
+    for _ in range(n):
+        r = rng.random()
+        if r < 0.2 and nz > 1:
+            z2 = z + (1 if (z == 0 or (rng.random() < 0.5 and z < nz - 1)) else -1)
+            z = min(max(z2, 0), nz - 1)
+        elif r < 0.25:
+            x = int(rng.integers(0, nx))  # a jump
+        else:
+            horizontal = dirs[z] == "h" if r < 0.95 else dirs[z] != "h"  # 5 %: across the axis
+            step = 1 if rng.random() < 0.7 else -1
+            if horizontal:
+                x = min(max(x + step, 0), nx - 1)
+            else:
+                y = min(max(y + step, 0), ny - 1)
+        node = z * nx * ny + y * nx + x
+        if node != path[-1]:
+            path.append(node)
+    return path
+
+
+@pytest.mark.parametrize("nz", [2, 4, 6])
+def test_geometry_equals_reference_on_random_paths(upf, nz):
+    """_generate_geometry_from_paths (with _segment_world / _via_world) on
+    random walks, against the oracle's emission mapped to board coordinates
+    as orthoroute_b200.geometry maps the device's."""
+    import types
+
+    from oracle.geometry import emit
+    from orthoroute_b200.geometry import _quantize
+
+    rng = np.random.default_rng(500 + nz)
+    lat = upf.Lattice3D((10.3, 20.1, 18.7, 27.5), 0.4, nz)
+    nx, ny = lat.x_steps, lat.y_steps
+    dirs = [lat.get_legal_axis(z) for z in range(nz)]
+    names = ["F.Cu"] + [f"In{i}.Cu" for i in range(1, nz - 1)] + ["B.Cu"]
+    net_paths = {f"N{k}": _random_path(rng, nx, ny, nz, dirs, int(rng.integers(1, 60))) for k in range(40)}
+    obj = types.SimpleNamespace(lattice=lat, net_paths=net_paths,
+                                config=types.SimpleNamespace(layer_names=names, grid_pitch=0.4))
+    obj._segment_world = types.MethodType(upf.PathFinderRouter._segment_world, obj)
+    obj._via_world = types.MethodType(upf.PathFinderRouter._via_world, obj)
+    ref_tracks, ref_vias = upf.PathFinderRouter._generate_geometry_from_paths(obj)
+
+    gx0, gy0, plane = lat.geom.grid_min_x, lat.geom.grid_min_y, nx * ny
+
+    def xy(node):
+        r = int(node) % plane
+        return (float(_quantize(gx0 + (r % nx) * 0.4, gx0, 0.4)), float(_quantize(gy0 + (r // nx) * 0.4, gy0, 0.4)))
+
+    tracks, vias = [], []
+    for name, (tr, vi) in zip(net_paths, emit(list(net_paths.values()), nx, ny, nz, dirs)):
+        for a, b, z in tr:
+            (x1, y1), (x2, y2) = xy(a), xy(b)
+            tracks.append({"net": name, "layer": names[z], "x1": x1, "y1": y1, "x2": x2, "y2": y2, "width": 0.4 * 0.6})
+        for n, z0, z1 in vi:
+            x, y = xy(n)
+            vias.append({"net": name, "x": x, "y": y, "from_layer": names[min(z0, z1)],
+                         "to_layer": names[max(z0, z1)], "diameter": 0.25, "drill": 0.15})
+    assert len(ref_vias) > 0 and (nz == 2 or len(ref_tracks) > 0)
+    assert tracks == ref_tracks
+    assert vias == ref_vias
