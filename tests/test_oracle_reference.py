@@ -4,8 +4,9 @@ and is skipped where it is absent): SimpleDijkstra.find_path_roi on random
 lattices, costs and ROIs (integer costs, where the reference's float64 path
 sums equal fp32), find_path_multisource_multisink with seed and portal
 costs, ROIExtractor.extract_roi_bfs with random depths and node caps, the
-EdgeAccountant updates with random parameters, and the geometry emission
-(_generate_geometry_from_paths) on random walks."""
+EdgeAccountant updates with random parameters, the geometry emission
+(_generate_geometry_from_paths) on random walks, and the negotiation's net
+selection (_build_hotset, _order_nets_by_difficulty) on random states."""
 import logging
 import os
 import sys
@@ -235,3 +236,52 @@ def test_geometry_equals_reference_on_random_paths(upf, nz):
     assert len(ref_vias) > 0 and (nz == 2 or len(ref_tracks) > 0)
     assert tracks == ref_tracks
     assert vias == ref_vias
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_hotset_and_difficulty_order_equal_reference(upf, seed):
+    """_build_hotset over several iterations (freeze-clean counters, cooldown,
+    the seeded 60/40 sample) and _order_nets_by_difficulty (seeded global
+    random rotation), on random edge lists and congestion, against the host
+    logic of orthoroute_b200.bookkeeping with the oracle's per-net scores."""
+    import random
+    import types
+
+    from oracle.bookkeeping import net_scores
+    from orthoroute_b200.bookkeeping import difficulty_order, select_hotset
+
+    rng = np.random.default_rng(600 + seed)
+    nx, ny, nz = 40, 30, 4
+    E = 5000
+    names = [f"N{k}" for k in range(int(rng.integers(150, 400)))]
+    tasks = {n: (int(rng.integers(0, nx * ny * nz)), int(rng.integers(0, nx * ny * nz))) for n in names}
+    net_to_edges = {n: sorted(set(rng.integers(0, E, size=int(rng.integers(1, 30))).tolist()))
+                    for n in names if rng.random() < 0.9}
+    edge_to_nets = {}
+    for n, es in net_to_edges.items():
+        for e in es:
+            edge_to_nets.setdefault(e, set()).add(n)
+    routed = {n for n in net_to_edges if rng.random() < 0.95}
+    obj = types.SimpleNamespace(
+        accounting=types.SimpleNamespace(use_gpu=False, present=None, capacity=np.ones(E, np.float32), history=None),
+        config=types.SimpleNamespace(hotset_cap=int(rng.choice([64, 150, 512])), freeze_after_clean=3),
+        net_paths={n: ([1, 2] if n in routed else []) for n in names}, _net_to_edges=net_to_edges,
+        _edge_to_nets=edge_to_nets, iteration=0,
+        lattice=types.SimpleNamespace(idx_to_coord=lambda i: (i % (nx * ny) % nx, i % (nx * ny) // nx, i // (nx * ny))))
+    clean, last = {}, {}
+    keys = list(net_to_edges)
+    for it in range(1, 7):
+        present = rng.integers(0, 3, size=E).astype(np.float32) * (rng.random(E) < (0.3 if it < 5 else 0.0))
+        history = (rng.random(E) * 4).astype(np.float32) * (rng.random(E) < 0.1)
+        obj.accounting.present, obj.accounting.history, obj.iteration = present, history, it
+        ripped = set(rng.choice(names, size=3, replace=False).tolist()) if it % 2 else None
+        ref = upf.PathFinderRouter._build_hotset(obj, tasks, ripped)
+        cong, imp, off, hot = net_scores([net_to_edges[n] for n in keys], present, obj.accounting.capacity, history)
+        got = select_hotset(tasks, keys, imp, off, hot, routed, it, clean, last, obj.config.hotset_cap, 3, ripped)
+        assert got == ref, it
+        assert clean == getattr(obj, "_net_clean_iters", {}) and last == getattr(obj, "_last_reroute_iter", {})
+        random.seed(1000 * seed + it)
+        ref_order = upf.PathFinderRouter._order_nets_by_difficulty(obj, tasks)
+        random.seed(1000 * seed + it)
+        got_order = difficulty_order(tasks, dict(zip(keys, (float(c) for c in cong))), nx, ny)
+        assert got_order == ref_order, it
