@@ -5,8 +5,9 @@ lattices, costs and ROIs (integer costs, where the reference's float64 path
 sums equal fp32), find_path_multisource_multisink with seed and portal
 costs, ROIExtractor.extract_roi_bfs with random depths and node caps, the
 EdgeAccountant updates with random parameters, the geometry emission
-(_generate_geometry_from_paths) on random walks, and the negotiation's net
-selection (_build_hotset, _order_nets_by_difficulty) on random states."""
+(_generate_geometry_from_paths) on random walks, and the negotiation
+bookkeeping (_rebuild_node_owner, _detect_barrel_conflicts, _build_hotset,
+_order_nets_by_difficulty) on random states."""
 import logging
 import os
 import sys
@@ -285,3 +286,52 @@ def test_hotset_and_difficulty_order_equal_reference(upf, seed):
         random.seed(1000 * seed + it)
         got_order = difficulty_order(tasks, dict(zip(keys, (float(c) for c in cong))), nx, ny)
         assert got_order == ref_order, it
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_node_owner_and_barrel_conflicts_equal_reference(upf, seed):
+    """_rebuild_node_owner (via barrels, last net wins; escape-via keepouts on
+    free nodes, first entry wins) and _detect_barrel_conflicts on random
+    overlapping paths, against the oracle's restatements."""
+    import types
+
+    import oracle.bookkeeping as OB
+
+    rng = np.random.default_rng(700 + seed)
+    nx, ny, nz = int(rng.integers(8, 20)), int(rng.integers(8, 20)), int(rng.integers(3, 7))
+    lat = build_lattice(nx, ny, nz)
+    plane = nx * ny
+    paths = {}
+    for k in range(int(rng.integers(10, 40))):
+        u = int(rng.integers(0, lat.N))
+        path = [u]
+        for _ in range(int(rng.integers(0, 40))):
+            nb = lat.indices[lat.indptr[u]:lat.indptr[u + 1]]
+            if len(nb) == 0:
+                break
+            u = int(nb[rng.integers(0, len(nb))])
+            path.append(u)
+        paths[f"N{k}"] = path
+    keep = {}
+    for _ in range(int(rng.integers(0, 30))):
+        keep[(int(rng.integers(0, nz)), int(rng.integers(0, nx)), int(rng.integers(0, ny)))] = \
+            f"N{int(rng.integers(0, len(paths) + 3))}"
+    obj = types.SimpleNamespace(
+        lattice=types.SimpleNamespace(idx_to_coord=lambda i: (i % plane % nx, i % plane // nx, i // plane),
+                                      node_idx=lambda x, y, z: z * plane + y * nx + x, num_nodes=lat.N, layers=nz),
+        graph=types.SimpleNamespace(indptr=lat.indptr, indices=lat.indices), net_paths=paths,
+        _via_keepouts_map=keep, node_owner=np.full(lat.N, -1, np.int32), net_id_map={}, next_net_id=0)
+    for m in ("_get_net_id", "_ensure_edge_src_map", "_path_to_edges"):
+        setattr(obj, m, types.MethodType(getattr(upf.PathFinderRouter, m), obj))
+    upf.PathFinderRouter._rebuild_node_owner(obj)
+    ref_owner = obj.node_owner.copy()
+    ref_conf, ref_cnt = upf.PathFinderRouter._detect_barrel_conflicts(obj)
+    ids = obj.net_id_map
+    order = [n for n, p in paths.items() if len(p) >= 2]
+    owner = OB.node_owner(lat.N, nx, ny, [paths[n] for n in order], [ids[n] for n in order],
+                          [(z, x, y, ids[n]) for (z, x, y), n in keep.items()])
+    assert np.array_equal(owner, ref_owner)
+    edges = [O.path_to_edges(lat.indptr, lat.indices, np.asarray(paths[n], np.int32)) for n in order]
+    conf, cnt = OB.barrel_conflicts(lat.indptr, lat.indices, edges, [ids[n] for n in order], owner)
+    assert cnt == ref_cnt and np.array_equal(np.asarray(conf), np.asarray(ref_conf))
+    assert (ref_owner >= 0).any() and (seed == 1 or ref_cnt > 0)
