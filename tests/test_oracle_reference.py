@@ -7,7 +7,7 @@ costs, ROIExtractor.extract_roi_bfs with random depths and node caps, the
 EdgeAccountant updates with random parameters, the geometry emission
 (_generate_geometry_from_paths) on random walks, and the negotiation
 bookkeeping (_rebuild_node_owner, _detect_barrel_conflicts, _build_hotset,
-_order_nets_by_difficulty) on random states."""
+_order_nets_by_difficulty) and the via pooling on random states."""
 import logging
 import os
 import sys
@@ -335,3 +335,36 @@ def test_node_owner_and_barrel_conflicts_equal_reference(upf, seed):
     conf, cnt = OB.barrel_conflicts(lat.indptr, lat.indices, edges, [ids[n] for n in order], owner)
     assert cnt == ref_cnt and np.array_equal(np.asarray(conf), np.asarray(ref_conf))
     assert (ref_owner >= 0).any() and (seed == 1 or ref_cnt > 0)
+
+
+@pytest.mark.parametrize("seed,layers", [(1, 3), (2, 4), (3, 5)])
+def test_via_pooling_equals_reference_on_random_states(upf, seed, layers):
+    """Via usage, pooling penalties (float32 and float64 layer bias) and the
+    hard block of full via columns / segments on the reference's own
+    Lattice3D graph (blind and buried vias of every span), with random paths,
+    capacities and present fields (tests/golden/make_golden.py gen_via with
+    other seeds and sizes)."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("make_golden", Path(__file__).resolve().parent / "golden" /
+                                                  "make_golden.py")
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    rng = np.random.default_rng(800 + seed)
+    w, h = 0.4 * int(rng.integers(6, 14)), 0.4 * int(rng.integers(6, 14))
+    lat = upf.Lattice3D((0.0, 0.0, w, h), 0.4, layers)
+    graph = lat.build_graph(via_cost=0.7, use_gpu=False)
+    g = mg.gen_via(upf, graph, lat, rng)
+    nx, ny, nz = (int(v) for v in g["via_dims"])
+    indptr, indices = np.asarray(graph.indptr, np.int32), np.asarray(graph.indices, np.int32)
+    meta = O.via_edge_metadata(indptr, indices, nx, ny, nz)
+    col = np.zeros((nx, ny), np.int64)
+    seg = np.zeros((nx, ny, max(nz - 2, 0)), np.int64)
+    O.via_usage([g[f"vpath{i}"] for i in range(int(g["npaths"]))], nx, ny, nz, col, seg)
+    assert np.array_equal(col, g["col_use"]) and np.array_equal(seg, g["seg_use"])
+    assert col.sum() > 0
+    for tag in ("f32", "f64"):
+        out = O.via_penalties(g["total0"], meta, g["col_pres"], g["seg_prefix"], nz - 2, g[f"bias_{tag}"], 2.25)
+        assert np.array_equal(out.view(np.uint32), g[f"pen_{tag}"].view(np.uint32)), tag
+    out = O.via_hard_block(g["total0"], meta, g["col_use"], g["col_cap"], g["seg_use"], g["seg_cap"], nz - 2)
+    assert np.array_equal(out.view(np.uint32), g["blocked"].view(np.uint32))
