@@ -54,15 +54,17 @@ class _OracleSolver:
 
 
 @pytest.mark.parametrize("nx,ny,nz,nets,seed,iters", [(20, 20, 4, 8, 2, 3), (24, 18, 6, 14, 5, 4),
-                                                       (18, 22, 4, 12, 7, 5), (22, 20, 6, 16, 9, 5)])
+                                                       (18, 22, 4, 12, 7, 5), (22, 20, 6, 16, 9, 5),
+                                                       (36, 30, 4, 120, 11, 3)])
 def test_install_routes_every_roi_through_the_gpu_solver(nx, ny, nz, nets, seed, iters):
     """Every search of the run with the solver installed equals the reference
     CPU Dijkstra's on the same inputs, except exact fp32 ties.  Those arise
-    when a path must cross the reference's owner-aware via keepouts (cost
-    1e9, boards under 100 nets, UPF:3150-3241): the float32 sum absorbs the
-    rest of the path, and the reference's float64 sums break the tie
-    differently.  A run without such a tie is the reference's own run,
-    iteration for iteration and path for path."""
+    when a path must cross an edge the reference blocks at a via keepout with
+    cost 1e9 (_apply_via_keepouts_to_graph UPF:3067-3148, and the
+    owner-aware keepouts of boards under 100 nets, UPF:3150-3241): the
+    float32 sum absorbs the rest of the path, and the reference's float64
+    sums break the tie differently.  A run without such a tie is the
+    reference's own run, iteration for iteration and path for path."""
     import oracle.ref_harness as H
     from oracle.ref_harness import run_reference
     from orthoroute_b200.lattice import board_uniform_pins
