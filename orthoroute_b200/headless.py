@@ -201,9 +201,10 @@ def build_problem(board_data: dict, pitch: float = DEFAULT_PITCH, portals: bool 
 
 def portal_collisions(prob: HeadlessProblem) -> int:
     """Grid points where the portals of two or more pads of different nets
-    end.  Their escape stubs meet there (a short in the planner's output),
-    and on this lattice the nets also share the portal's single via edge, so
-    the route cannot reach zero overuse while any remain."""
+    end.  Their escape stubs meet there (a short in the planner's output).
+    On this lattice a portal's F.Cu node has one via edge each way, so two
+    searches that both leave (or both enter) the point share a directed edge
+    and the route cannot reach zero overuse."""
     pad_net = {}
     for net, (k1, k2) in prob.net_pads.items():
         pad_net.setdefault(k1, net)
@@ -308,7 +309,7 @@ def run_headless(orp_file: str, output_file: Optional[str] = None, max_iteration
                "escape_tracks": len(prob.escape_tracks), "portal_collisions": portal_collisions(prob)}
     if log and summary["portal_collisions"]:
         log(f"warning: {summary['portal_collisions']} grid points hold the portals of two nets "
-            "(their escape stubs meet); route with --no-portals to avoid them")
+            "(their escape stubs meet, and the nets may share a via edge); --no-portals avoids them")
     if log:
         log(json.dumps(summary))
     return summary
