@@ -215,6 +215,21 @@ def portal_collisions(prob: HeadlessProblem) -> int:
     return sum(1 for v in nets_at.values() if len(v) > 1)
 
 
+def forced_overuse(prob: HeadlessProblem) -> int:
+    """A lower bound on the edges that stay overused: on a board of more than
+    two layers an F.Cu node has no planar edges and one via edge each way, so
+    every F.Cu search endpoint that several searches leave (or several enter)
+    keeps that directed edge overused.  0 on boards of one or two layers."""
+    if prob.lattice.nz <= 2:
+        return 0
+    plane = prob.lattice.nx * prob.lattice.ny
+    out = 0
+    for ends in (prob.search_src, prob.search_dst):
+        vals, counts = np.unique(np.asarray(ends, np.int64), return_counts=True)
+        out += int(np.sum((counts > 1) & (vals < plane)))
+    return out
+
+
 def merge_escapes(escape_tracks: List[dict], tracks: List[dict], vias: List[dict]):
     """Escape stubs in front of the routed tracks, later duplicates dropped
     by (net, layer, ends and width to 0.001 mm); vias deduplicated by (net,
@@ -306,7 +321,8 @@ def run_headless(orp_file: str, output_file: Optional[str] = None, max_iteration
                "converged": bool(res.converged), "iterations": len(metrics), "tracks": len(tracks),
                "vias": len(vias), "seconds_total": round(total, 3), "seconds_route": round(res.seconds, 3),
                "lattice": [prob.lattice.nx, prob.lattice.ny, prob.lattice.nz], "portals": len(prob.portals),
-               "escape_tracks": len(prob.escape_tracks), "portal_collisions": portal_collisions(prob)}
+               "escape_tracks": len(prob.escape_tracks), "portal_collisions": portal_collisions(prob),
+               "forced_overuse": forced_overuse(prob)}
     if log and summary["portal_collisions"]:
         log(f"warning: {summary['portal_collisions']} grid points hold the portals of two nets "
             "(their escape stubs meet, and the nets may share a via edge); --no-portals avoids them")

@@ -126,6 +126,28 @@ def test_portal_collisions_counted():
     assert portal_collisions(prob) == 1
 
 
+def test_forced_overuse_bound():
+    """F.Cu search endpoints shared in the same direction force overused via
+    edges on boards of more than two layers; endpoints shared in opposite
+    directions do not, and 2-layer boards have planar F.Cu edges."""
+    from orthoroute_b200.headless import forced_overuse
+
+    b = board_uniform_pins(40, 32, 6, 30, seed=5)
+    prob = build_problem(orp_to_board_data(board_data_to_orp(synthetic_board_data(b))), portals=True)
+    assert int(max(prob.search_src.max(), prob.search_dst.max())) < prob.lattice.nx * prob.lattice.ny  # F.Cu
+    assert forced_overuse(prob) == 0
+    s0, d0 = int(prob.search_src[0]), int(prob.search_dst[0])
+    prob.search_dst[1] = s0  # opposite directions: still routable
+    assert forced_overuse(prob) == 0
+    prob.search_src[2] = s0  # two searches leave s0
+    prob.search_dst[3] = d0  # two searches enter d0
+    assert forced_overuse(prob) == 2
+    b2 = board_uniform_pins(30, 24, 2, 12, seed=3)
+    p2 = build_problem(synthetic_board_data(b2), portals=True)
+    p2.search_src[1] = p2.search_src[0]
+    assert forced_overuse(p2) == 0
+
+
 def test_one_layer_board_routes_pad_to_pad(gorp):
     """A one-layer board has no routing layer for portals: its tasks stay
     pad to pad and every node is inside the lattice."""
