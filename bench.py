@@ -192,7 +192,7 @@ def cpu_baseline(lat, w, sources, threads: int, budget_s: float = 20.0):
 
 
 def route_c1(dev, with_cpu: bool):
-    """Config 1 board (100x100x4, 200 two-pin nets, pins uniform on the top
+    """The 100x100x4 board (200 two-pin nets, pins uniform on the top
     layer, seeded) routed to zero overuse with per-net live costs, offenders
     rerouted after iteration 1: plain (one search per net) vs batched (one
     launch per level of disjoint boxes).  Identical routes by construction
