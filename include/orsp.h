@@ -104,12 +104,25 @@ ORSP_API int orsp_graph_is_lattice(orsp_graph *g, int32_t *out);
  * routing loop (orsp_route_nets) rejects them.  (No reference counterpart.) */
 ORSP_API int orsp_lattice_max_layers(int32_t tile_w, int32_t *out);
 
+/* Declares, for the next search on this graph only, that the contents of
+ * cost_d are identified by `generation` (non-zero; the caller changes it
+ * whenever it writes the array).  A whole-lattice tile search first gathers
+ * the costs into per-node in-edge weights (16 B per node); it skips that
+ * gather when the declaration names the same array and generation as the
+ * last whole gather (e.g. many sources searched on one fixed cost array, as
+ * the reference routes every net of an iteration on one total_cost,
+ * UPF:3724-3732, 4463).  Without a declaration every search gathers.  No
+ * counterpart in the reference. */
+ORSP_API int orsp_graph_cost_generation(orsp_graph *g, const float *cost_d, uint64_t generation);
+
 /* ---- single search ----------------------------------------------------- */
 /* Single-source (or multi-seed) shortest path over the whole graph or over
- * the ROI given by roi_map_d (global_to_roi, int32[N], -1 = outside).  A
- * full-graph search on a recognised H/V lattice runs the tile-sweep search;
- * other searches run one persistent cooperative launch of near-far
- * delta-stepping with a bounded grid barrier.  Replaces SimpleDijkstra.find_path_roi (UPF:1801-1887) and
+ * the ROI given by roi_map_d (global_to_roi, int32[N], -1 = outside).  On a
+ * recognised H/V lattice it runs the tile-sweep search: over the whole
+ * lattice, or, with a ROI, over the ROI's bounding box (reduced on the
+ * device) with every edge into or out of the ROI at +inf, ties ranked by
+ * global_to_roi.  Other graphs run one persistent cooperative launch of
+ * near-far delta-stepping with a bounded grid barrier.  Replaces SimpleDijkstra.find_path_roi (UPF:1801-1887) and
  * CUDADijkstra.find_path_roi_gpu (CD:4909-4996).
  *   seeds_d[nseeds]       start nodes (global ids); seed_cost_d may be NULL
  *                          (all seeds start at 0.0) or give fp32 start costs.
@@ -128,6 +141,20 @@ ORSP_API int orsp_sssp(orsp_graph *g, const float *cost_d, int32_t nseeds,
               const int32_t *roi_map_d, float delta, float *dist_out_d,
               int32_t *path_out_d, int32_t path_cap, int32_t *path_len_h,
               int32_t *rounds_h, uintptr_t stream);
+
+/* One search from src to dst over the ROI given as its node list (the
+ * roi_nodes array SimpleDijkstra.find_path_roi, UPF:1801-1887, and
+ * CUDADijkstra.find_path_roi_gpu, CD:4909-4996, take, int32[n_roi], device):
+ * the ROI index of roi_nodes_d[i] is i (a repeated node keeps its last
+ * index, as the reference's global_to_roi[roi_nodes] = arange(R) does), and
+ * ties between equal distances go to the smaller ROI index.  The call builds
+ * its global_to_roi on the device from the list, in a map the graph keeps at
+ * -1 between calls, so a caller passes O(R) data per search instead of an
+ * int32[N] map.  Path (global ids, src..dst) as orsp_sssp; ORSP_NO_PATH when
+ * src or dst is outside the ROI or unreachable. */
+ORSP_API int orsp_sssp_roi_nodes(orsp_graph *g, const float *cost_d, int32_t src, int32_t dst,
+                        const int32_t *roi_nodes_d, int64_t n_roi, int32_t *path_out_d,
+                        int32_t path_cap, int32_t *path_len_h, uintptr_t stream);
 
 /* The same search inside an axis-aligned box ROI (inclusive bounds
  * x0,x1,y0,y1,z0,z1 in the host array box_h[6]): identical, bit for bit, to
@@ -151,7 +178,9 @@ ORSP_API int orsp_sssp_box(orsp_graph *g, const float *cost_d, int32_t nseeds,
  * a seed to the winning target (best_target_h, optional).  Also serves
  * CUDADijkstra.find_path_fullgraph_gpu_seeds (CD:5467-5751) with zero costs;
  * unlike that wavefront (which stops at the first target it reaches) the
- * answer is the exact shortest one. */
+ * answer is the exact shortest one.  On a recognised H/V lattice it runs the
+ * tile-sweep search over the ROI's bounding box with the targets' out-edges
+ * at +inf. */
 ORSP_API int orsp_sssp_multi(orsp_graph *g, const float *cost_d, int32_t nseeds,
                     const int32_t *seeds_d, const float *seed_cost_d,
                     int32_t ntargets, const int32_t *targets_d,
@@ -318,18 +347,31 @@ ORSP_API int orsp_roi_bfs(orsp_graph *g, int32_t src, int32_t dst, int32_t max_d
                  int32_t max_nodes, int32_t *roi_nodes_d, int32_t *g2r_d,
                  int32_t *roi_count_h, uintptr_t stream);
 
+/* orsp_roi_bfs with extra must-keep nodes, as extract_roi_bfs with
+ * portal_seeds (UPF:1700-1731): the must-keep list is src, dst and then the
+ * keep_d[0..nkeep) nodes not already listed (device array, nkeep <= 256);
+ * those missing from the BFS are appended after the ascending part in that
+ * order, and the truncation to max_nodes moves every must-keep node that
+ * lies at or past max_nodes to the front, as the reference swaps them. */
+ORSP_API int orsp_roi_bfs_keep(orsp_graph *g, int32_t src, int32_t dst, int32_t max_depth,
+                      int32_t max_nodes, const int32_t *keep_d, int32_t nkeep,
+                      int32_t *roi_nodes_d, int32_t *g2r_d, int32_t *roi_count_h,
+                      uintptr_t stream);
+
 /* Allocation-free variant of orsp_roi_bfs (no counterpart in the reference).
- * For callers that cannot allocate device memory while routing - e.g. code
- * running during CUDA stream capture, or a host application whose own
- * allocator owns all device memory - this call allocates nothing: its work
- * buffers live in one fixed device array inside liborsp.so (about 8.5 MB,
- * held on every GPU that loads the library until exit).  Same arguments,
- * semantics and results as orsp_roi_bfs, for graphs of at most
- * ORSP_ROI_BFS_NOALLOC_MAX_NODES nodes; larger graphs get ORSP_ERR_ARG.
- * The first call on a device looks up the array's device address; make that
+ * For callers that cannot allocate device memory while routing: a host
+ * application whose own caching allocator reserves the GPU's memory up front
+ * and allows no other cudaMalloc / cudaFree on the routing path.  This call
+ * allocates nothing: its work buffers live in one fixed device array inside
+ * liborsp.so (about 8.5 MB, held on every GPU that loads the library until
+ * exit).  Same arguments, semantics and results as orsp_roi_bfs, for graphs
+ * of at most ORSP_ROI_BFS_NOALLOC_MAX_NODES nodes; larger graphs get
+ * ORSP_ERR_ARG.  The first call on a device looks up the array's device
+ * address (once per device, in the device's primary context); make that
  * first call before any stream capture.  All calls on a device share the
- * array, so calls that overlap on the GPU (other streams, other threads)
- * race and must be serialised by the caller. */
+ * array, and all calls on one graph share its small pinned result buffer, so
+ * calls that overlap on the GPU (other streams, other threads) race and must
+ * be serialised by the caller. */
 #define ORSP_ROI_BFS_NOALLOC_MAX_NODES 524288
 ORSP_API int orsp_roi_bfs_noalloc(orsp_graph *g, int32_t src, int32_t dst, int32_t max_depth,
                          int32_t max_nodes, int32_t *roi_nodes_d, int32_t *g2r_d,

@@ -9,6 +9,7 @@
  *                        SimpleDijkstra.find_path_multisource_multisink
  *                                                                 UPF:1889-1989
  *   oracle_roi_bfs       ROIExtractor.extract_roi_bfs            UPF:1636-1734
+ *   oracle_roi_bfs_keep  the same with portal seeds (must-keep)  UPF:1700-1731
  *   oracle_path_to_edges PathFinderRouter._path_to_edges         UPF:5463-5476
  *
  * Arithmetic: the reference adds path costs in Python float64 (UPF:1871) and
@@ -168,8 +169,22 @@ int oracle_dijkstra(int32_t N, const int32_t *indptr, const int32_t *indices, co
  * the reference steps them.  roi_out needs room for N ids; returns the ROI
  * size after truncation to max_nodes (-1 on allocation failure).
  */
+int32_t oracle_roi_bfs_keep(int32_t N, const int32_t *indptr, const int32_t *indices, int32_t src,
+                            int32_t dst, int32_t max_depth, int32_t max_nodes, const int32_t *keep,
+                            int32_t nkeep, int32_t *roi_out);
+
 int32_t oracle_roi_bfs(int32_t N, const int32_t *indptr, const int32_t *indices, int32_t src,
                        int32_t dst, int32_t max_depth, int32_t max_nodes, int32_t *roi_out) {
+  return oracle_roi_bfs_keep(N, indptr, indices, src, dst, max_depth, max_nodes, 0, 0, roi_out);
+}
+
+/* The same with portal seeds (UPF:1700-1731): must_keep = [src, dst] plus
+ * each keep node not yet in it; the ones not in the ROI are appended in that
+ * order; on truncation, for the k-th list position (ascending) that holds a
+ * must-keep node, a position >= max_nodes is swapped with position k. */
+int32_t oracle_roi_bfs_keep(int32_t N, const int32_t *indptr, const int32_t *indices, int32_t src,
+                            int32_t dst, int32_t max_depth, int32_t max_nodes, const int32_t *keep,
+                            int32_t nkeep, int32_t *roi_out) {
   uint8_t *seen = (uint8_t *)calloc((size_t)N, 1);
   int32_t *qs = (int32_t *)malloc((size_t)N * 4), *qs2 = (int32_t *)malloc((size_t)N * 4);
   int32_t *qd = (int32_t *)malloc((size_t)N * 4), *qd2 = (int32_t *)malloc((size_t)N * 4);
@@ -218,20 +233,42 @@ int32_t oracle_roi_bfs(int32_t N, const int32_t *indptr, const int32_t *indices,
   int32_t cnt = 0;
   for (int32_t v = 0; v < N; ++v)
     if (seen[v]) roi_out[cnt++] = v;
+  /* must_keep = [src, dst] + keep nodes not already in it */
+  int32_t *mk = (int32_t *)malloc((size_t)(nkeep + 2) * 4);
+  int32_t nmk = 0;
+  mk[nmk++] = src;
+  mk[nmk++] = dst;
+  for (int32_t i = 0; i < nkeep; ++i) {
+    int dup = 0;
+    for (int32_t j = 0; j < nmk; ++j) dup |= mk[j] == keep[i];
+    if (!dup) mk[nmk++] = keep[i];
+  }
+  /* missing must-keep nodes appended in list order */
+  for (int32_t j = 0; j < nmk; ++j) {
+    if (seen[mk[j]]) continue;
+    int dup = 0;
+    for (int32_t i = 0; i < cnt; ++i) dup |= roi_out[i] == mk[j];
+    if (!dup) roi_out[cnt++] = mk[j];
+  }
   if (cnt > max_nodes) {
-    int32_t kept[2];
-    int nk = 0;
-    for (int32_t i = 0; i < cnt && nk < 2; ++i)
-      if (roi_out[i] == src || roi_out[i] == dst) kept[nk++] = i;
-    for (int k = 0; k < nk; ++k) {
+    int32_t *kept = (int32_t *)malloc((size_t)nmk * 4);
+    int32_t nk = 0;
+    for (int32_t i = 0; i < cnt; ++i) {
+      int is_keep = 0;
+      for (int32_t j = 0; j < nmk; ++j) is_keep |= roi_out[i] == mk[j];
+      if (is_keep) kept[nk++] = i;
+    }
+    for (int32_t k = 0; k < nk; ++k) {
       if (kept[k] >= max_nodes) {
         int32_t t = roi_out[kept[k]];
         roi_out[kept[k]] = roi_out[k];
         roi_out[k] = t;
       }
     }
+    free(kept);
     cnt = max_nodes;
   }
+  free(mk);
   free(seen); free(qs); free(qs2); free(qd); free(qd2);
   return cnt;
 }

@@ -43,6 +43,8 @@ def _load():
         lib.oracle_dijkstra.restype = ctypes.c_int
         lib.oracle_roi_bfs.argtypes = [i32, P, P, i32, i32, i32, i32, P]
         lib.oracle_roi_bfs.restype = i32
+        lib.oracle_roi_bfs_keep.argtypes = [i32, P, P, i32, i32, i32, i32, P, i32, P]
+        lib.oracle_roi_bfs_keep.restype = i32
         lib.oracle_path_to_edges.argtypes = [P, P, P, i32, P]
         lib.oracle_path_to_edges.restype = i32
         lib.oracle_batch_bbox.argtypes = [i32, P, P, P, i32, i32, i32, i32, P, P, P, P, i32, P]
@@ -93,15 +95,17 @@ def dijkstra(indptr, indices, cost, seeds, dst=-1, roi_map=None, seed_cost=None,
     return path[:rc].copy(), dist, parent, int(best[0])
 
 
-def roi_bfs(indptr, indices, src, dst, max_depth, max_nodes=50_000):
-    """(roi_nodes int32[R], global_to_roi int32[N])."""
+def roi_bfs(indptr, indices, src, dst, max_depth, max_nodes=50_000, keep=None):
+    """(roi_nodes int32[R], global_to_roi int32[N]); keep: extra must-keep
+    nodes (the portal seeds of extract_roi_bfs, UPF:1700-1731)."""
     lib = _load()
     indptr = _c(indptr, np.int32)
     indices = _c(indices, np.int32)
     N = indptr.shape[0] - 1
     out = np.empty(N, dtype=np.int32)
-    n = lib.oracle_roi_bfs(N, _p(indptr), _p(indices), int(src), int(dst), int(max_depth),
-                           int(max_nodes), _p(out))
+    kp = _c(np.asarray([] if keep is None else keep, dtype=np.int32), np.int32)
+    n = lib.oracle_roi_bfs_keep(N, _p(indptr), _p(indices), int(src), int(dst), int(max_depth),
+                                int(max_nodes), _p(kp), int(kp.size), _p(out))
     if n < 0:
         raise RuntimeError("oracle_roi_bfs failed")
     roi = out[:n].copy()

@@ -39,16 +39,27 @@ def _import(ref):
     return upf, pd
 
 
-def run_reference(lat, src, dst, *, ref="/root/reference", max_iterations=30, pres_fac_init=0.5,
-                  pres_fac_mult=1.5, hist_gain=1.0, seed=0, search=None, record=None):
+def reference_root(ref=None) -> str:
+    """The OrthoRoute source tree: `ref`, else $ORTHOROUTE_REFERENCE."""
+    ref = ref or os.environ.get("ORTHOROUTE_REFERENCE")
+    if not ref:
+        raise RuntimeError("set ORTHOROUTE_REFERENCE to the OrthoRoute source tree (or pass ref=)")
+    return ref
+
+
+def run_reference(lat, src, dst, *, ref=None, max_iterations=30, pres_fac_init=0.5,
+                  pres_fac_mult=1.5, hist_gain=1.0, seed=0, search=None, record=None, on_init=None,
+                  on_iteration=None):
     """Routes nets (src[i] -> dst[i]) with the reference router.
 
     search: optional callable(indptr, indices, src, dst, costs, roi_nodes, g2r) -> path list or None
             that replaces SimpleDijkstra.find_path_roi.
     record: optional list; receives one dict per search call
             (iteration, src, dst, costs-id, roi_nodes, path).
+    on_init: optional callable(router), called after initialize_graph.
+    on_iteration: optional callable(it, over_sum, over_cnt) after each iteration.
     Returns dict(result, trace=[(it, over_sum, over_cnt)], paths, seconds)."""
-    upf, pd = _import(ref)
+    upf, pd = _import(reference_root(ref))
     os.environ["ORTHO_PRES_FAC_MULT"] = repr(float(pres_fac_mult))
     os.environ["ORTHO_HIST_GAIN"] = repr(float(hist_gain))
     pitch = 0.5
@@ -93,10 +104,14 @@ def run_reference(lat, src, dst, *, ref="/root/reference", max_iterations=30, pr
         router = upf.PathFinderRouter(cfg, use_gpu=False)
         router.initialize_graph(board)
         assert router.lattice.x_steps == lat.nx and router.lattice.y_steps == lat.ny, "lattice injection failed"
+        if on_init is not None:
+            on_init(router)
         trace = []
 
         def it_cb(it, tracks, vias, over_sum, over_cnt):
             trace.append((it, int(over_sum), int(over_cnt)))
+            if on_iteration is not None:
+                on_iteration(it, over_sum, over_cnt)
 
         reqs = [(f"N{i}", int(s), int(d)) for i, (s, d) in enumerate(zip(src, dst))]
         random.seed(seed)

@@ -6,11 +6,11 @@ Public entry points mirror the reference router's hot-path interfaces:
 * ``DeviceEdgeAccountant`` - router.accounting (EdgeAccountant interface)
 * ``DeviceROIExtractor``   - router.roi_extractor (ROIExtractor interface)
 * ``PathFinder``           - the negotiation loop on the device kernels
-* ``install``              - wires the GPU solver into a reference PathFinderRouter
+* ``install``              - wires the whole B200 path into a reference PathFinderRouter
+                             (orthoroute_b200.dropin: solver, accountant, ROI, via steps)
 """
 from .lattice import Lattice, Board, build_lattice  # noqa: F401
 
-from .shim import install  # noqa: F401,E402
 
 __all__ = ["Lattice", "Board", "build_lattice", "GpuSolver", "DeviceGraph", "DeviceEdgeAccountant",
            "DeviceROIExtractor", "PathFinder", "NegotiationConfig", "install"]
@@ -31,6 +31,10 @@ def __getattr__(name):
         from .roi import DeviceROIExtractor
 
         return DeviceROIExtractor
+    if name == "install":
+        from .dropin import install
+
+        return install
     if name in ("PathFinder", "NegotiationConfig"):
         from . import negotiate
 

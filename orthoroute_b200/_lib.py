@@ -48,10 +48,12 @@ _SIGS = {
     "orsp_graph_max_degree": (ctypes.c_int, [_P, ctypes.POINTER(_i32)]),
     "orsp_graph_is_lattice": (ctypes.c_int, [_P, ctypes.POINTER(_i32)]),
     "orsp_lattice_max_layers": (ctypes.c_int, [_i32, ctypes.POINTER(_i32)]),
+    "orsp_graph_cost_generation": (ctypes.c_int, [_P, _P, ctypes.c_uint64]),
     "orsp_sssp": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _f32, _P, _P, _i32,
                                  ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
     "orsp_sssp_box": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _f32, _P, _P, _i32,
                                      ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
+    "orsp_sssp_roi_nodes": (ctypes.c_int, [_P, _P, _i32, _i32, _P, _i64, _P, _i32, ctypes.POINTER(_i32), _u]),
     "orsp_batch_set_plan": (ctypes.c_int, [_P, _i32, _P, _P, _P, _P, _P]),
     "orsp_warm_conv3d": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _i32, _i32, _i32, _i32, _i32, _i32, _u]),
     "orsp_warm_wgrad": (ctypes.c_int, [_P, _P, _P, _P, _P, _i32, _i32, _i32, _i32, _i32, _u]),
@@ -76,6 +78,7 @@ _SIGS = {
     "orsp_sssp_batch_ranges": (ctypes.c_int, [_P, _P, _i32, _P, _P, _P, _P, _f32, _P, _P, _i32, _P, _u]),
     "orsp_roi_bfs": (ctypes.c_int, [_P, _i32, _i32, _i32, _i32, _P, _P, ctypes.POINTER(_i32), _u]),
     "orsp_roi_bfs_noalloc": (ctypes.c_int, [_P, _i32, _i32, _i32, _i32, _P, _P, ctypes.POINTER(_i32), _u]),
+    "orsp_roi_bfs_keep": (ctypes.c_int, [_P, _i32, _i32, _i32, _i32, _P, _i32, _P, _P, ctypes.POINTER(_i32), _u]),
     "orsp_roi_box_map": (ctypes.c_int, [_P, _P, _P, _u]),
     "orsp_path_to_edges": (ctypes.c_int, [_P, _P, _i32, _P, ctypes.POINTER(_i32), _u]),
     "orsp_update_costs": (ctypes.c_int, [_i64, _P, _P, _P, _P, _P, _P, _P, _f32, _f32, _f32, _f32,

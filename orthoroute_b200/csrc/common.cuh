@@ -97,6 +97,21 @@ struct Graph {
   size_t lat_ws_bytes = 0;
   void *lat_ctl_h = nullptr;      // pinned mirror of the control block
   void *lat_box_d = nullptr;      // tile table of a single-box search
+  // ROI searches (orsp_sssp_roi_nodes, ROI-masked tile sweeps): a global_to_roi
+  // map kept at -1 between calls (each call scatters its ROI in and clears it
+  // again), a sink mask kept at 0 the same way, the ROI's bounding box as it is
+  // reduced on the device, and a one-int seed slot
+  int32_t *roi_map = nullptr;
+  uint8_t *sink_mask = nullptr;
+  int *roi_bb = nullptr;
+  int32_t *seed_one = nullptr;
+  // gathered-weight cache (orsp_graph_cost_generation): the cost array and
+  // caller-declared generation the whole of wslot was last gathered from
+  // (generation 0: not reusable), and the declaration for the next search
+  const float *w4_cost = nullptr;
+  uint64_t w4_gen = 0;
+  const float *decl_cost = nullptr;
+  uint64_t decl_gen = 0;
 };
 
 // Optional timing of a search kernel (CUDA events on the launching stream),
@@ -163,6 +178,21 @@ int run_lattice_boxes(Graph *g, const float *cost_d, int32_t nseeds, const int32
 // later launches never reallocate it (a reallocation synchronises).
 int reserve_lattice_ws(Graph *g, int64_t ntiles);
 int finish_lattice_search(Graph *g, int32_t *rounds_h);
+// One search on a recognised lattice restricted to a node-set ROI: nodes with
+// roi_map_d[v] >= 0 (roi_map_d NULL: every node), with the out-edges of the
+// nodes marked in sink_d (may be NULL) blocked.  The ROI's bounding box is
+// reduced on the device, from the node list roi_nodes_d[0..n_roi) when given,
+// else from roi_map_d; the in-edge weights are gathered inside that box with
+// every edge that leaves the ROI, enters it from outside or leaves a sink set
+// to +inf, and the tile sweeps run over the box.  `dist` is reset to +inf
+// everywhere, so a backtrace may walk it with the whole lattice as its box.
+// Seeds outside the ROI are ignored.  finish_lattice_search reports the status.
+int run_lattice_roi(Graph *g, const float *cost_d, int32_t nseeds, const int32_t *seeds_d,
+                    const float *seed_cost_d, const int32_t *roi_map_d, const int32_t *roi_nodes_d,
+                    int64_t n_roi, const uint8_t *sink_d, uint32_t *dist, cudaStream_t st);
+// The ROI map and sink mask of orsp_sssp_roi_nodes / orsp_sssp_multi (lazily
+// allocated, -1 / 0 everywhere).
+int ensure_roi_arrays(Graph *g);
 
 }  // namespace orsp
 

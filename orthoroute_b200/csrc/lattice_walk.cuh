@@ -11,8 +11,9 @@
 // (d[u], rank u) below (d[v], rank v)) needs one float4 and four distances,
 // all independent loads: one memory round trip per step of the walk, where a
 // walk over the transposed CSR needs three dependent ones (row pointer, source
-// list, distance).  Ranks are node ids (box searches rank nodes in id order,
-// and a box's own distance slice is laid out in that order too).
+// list, distance).  Ranks are node ids by default (box searches rank nodes in
+// id order, and a box's own distance slice is laid out in that order too);
+// ROI searches pass the ROI index (global_to_roi) as the rank.
 #pragma once
 
 #include "common.cuh"
@@ -22,6 +23,19 @@ namespace orsp {
 struct LatWalkGeom {
   int32_t nx, ny, nz;
   int8_t axis[64];  // 1: x moves (H layer), 2: y moves (V layer), 0: none
+};
+
+// Rank of a node for the tie-break: its id.
+struct LatRankId {
+  __device__ __forceinline__ int64_t operator()(int64_t v) const { return v; }
+};
+
+// Rank of a node inside a node-set ROI: its index in the ROI list
+// (global_to_roi[v]); nodes outside the ROI never qualify as parents, since
+// their distances stay +inf.
+struct LatRankRoi {
+  const int32_t *g2r;
+  __device__ __forceinline__ int64_t operator()(int64_t v) const { return __ldg(&g2r[v]); }
 };
 
 // Coordinates of a node id.
@@ -51,13 +65,14 @@ __device__ __forceinline__ bool lat_slot_nbr(const LatWalkGeom &G, const LatBox 
 }
 
 // One step of the walk at v = (x, y, z) with distance bits dv.  DIST(x, y, z)
-// gives the distance bits of a node inside the box.  Returns the slot of the
-// parent (and its coordinates and distance bits), or -1 when no in-neighbour
-// qualifies.
-template <class DIST>
+// gives the distance bits of a node inside the box, RANK(node) its rank.
+// Returns the slot of the parent (and its coordinates and distance bits), or
+// -1 when no in-neighbour qualifies.
+template <class DIST, class RANK = LatRankId>
 __device__ __forceinline__ int lat_parent(const LatWalkGeom &G, const LatBox &B, const float4 *__restrict__ w4,
                                           DIST dist, int32_t x, int32_t y, int32_t z, unsigned dv,
-                                          int32_t &px, int32_t &py, int32_t &pz, unsigned &pdu) {
+                                          int32_t &px, int32_t &py, int32_t &pz, unsigned &pdu,
+                                          RANK rank = RANK()) {
   const int64_t v = ((int64_t)z * G.ny + y) * G.nx + x;
   const float4 wv = __ldcg(&w4[v]);
   const float wk[4] = {wv.x, wv.y, wv.z, wv.w};
@@ -75,9 +90,9 @@ __device__ __forceinline__ int lat_parent(const LatWalkGeom &G, const LatBox &B,
   for (int s = 0; s < 4; ++s) {
     if (!ok[s] || du[s] == ORSP_INF_BITS) continue;
     if (f_bits(__fadd_rn(bits_f(du[s]), wk[s])) != dv) continue;
-    const int64_t u = ((int64_t)uz[s] * G.ny + uy[s]) * G.nx + ux[s];
-    if (!(du[s] < dv || (du[s] == dv && u < v))) continue;
-    const unsigned long long key = ((unsigned long long)du[s] << 32) | (unsigned long long)(uint32_t)u;
+    const int64_t ru = rank(((int64_t)uz[s] * G.ny + uy[s]) * G.nx + ux[s]);
+    if (!(du[s] < dv || (du[s] == dv && ru < rank(v)))) continue;
+    const unsigned long long key = ((unsigned long long)du[s] << 32) | (unsigned long long)(uint32_t)ru;
     if (key < best) {
       best = key;
       bs = s;
@@ -124,10 +139,10 @@ __device__ __forceinline__ bool lat_run_cell(const LatWalkGeom &G, const LatBox 
 // parent is the next current node.  Each lane's parent is the one the
 // sequential walk computes at that node (same distances, same rule), so the
 // nodes are those of the one-step walk; a round advances by up to 32 nodes.
-template <class DIST, class STOP>
+template <class DIST, class STOP, class RANK = LatRankId>
 __device__ __forceinline__ int lat_walk_warp(const LatWalkGeom &G, const LatBox &B, const float4 *__restrict__ w4,
                                              DIST dist, STOP stop, int32_t x, int32_t y, int32_t z, unsigned dv,
-                                             int32_t *out, int32_t cap) {
+                                             int32_t *out, int32_t cap, RANK rank = RANK()) {
   const int lane = threadIdx.x & 31;
   int len = 0;
   int s = 0;  // predicted slot: the direction of the last step
@@ -140,7 +155,7 @@ __device__ __forceinline__ int lat_walk_warp(const LatWalkGeom &G, const LatBox 
     int ps = -1;
     int32_t px = 0, py = 0, pz = 0;
     unsigned pdu = 0;
-    if (valid && dc != ORSP_INF_BITS && !is_stop) ps = lat_parent(G, B, w4, dist, cx, cy, cz, dc, px, py, pz, pdu);
+    if (valid && dc != ORSP_INF_BITS && !is_stop) ps = lat_parent(G, B, w4, dist, cx, cy, cz, dc, px, py, pz, pdu, rank);
     const bool cont = valid && !is_stop && ps == s && lane < 31;
     const unsigned m = __ballot_sync(ORSP_FULL_MASK, cont);
     const int last = __ffs(~m) - 1;  // lane 31 never continues

@@ -37,6 +37,26 @@ int ensure_scratch(Graph *g, size_t bytes) {
   return ORSP_OK;
 }
 
+int ensure_roi_arrays(Graph *g) {
+  bool fresh = false;
+  if (!g->roi_map) {
+    ORSP_CUDA(cudaMalloc(&g->roi_map, (size_t)g->N * 4));
+    ORSP_CUDA(cudaMemset(g->roi_map, 0xff, (size_t)g->N * 4));
+    fresh = true;
+  }
+  if (!g->sink_mask) {
+    ORSP_CUDA(cudaMalloc(&g->sink_mask, (size_t)g->N));
+    ORSP_CUDA(cudaMemset(g->sink_mask, 0, (size_t)g->N));
+    fresh = true;
+  }
+  if (!g->roi_bb) ORSP_CUDA(cudaMalloc(&g->roi_bb, 64));
+  if (!g->seed_one) ORSP_CUDA(cudaMalloc(&g->seed_one, 64));
+  // the memsets run on the legacy stream, which a caller's non-blocking
+  // stream does not wait for
+  if (fresh) ORSP_CUDA(cudaDeviceSynchronize());
+  return ORSP_OK;
+}
+
 }  // namespace orsp
 
 using namespace orsp;
@@ -187,6 +207,10 @@ extern "C" int orsp_graph_destroy(orsp_graph *g) {
     if (e) cudaEventDestroy(e);
   cudaFree(g->box_g2r);
   cudaFree(g->edge_src);
+  cudaFree(g->roi_map);
+  cudaFree(g->sink_mask);
+  cudaFree(g->roi_bb);
+  cudaFree(g->seed_one);
   if (g->pinned) cudaFreeHost(g->pinned);
   free_lattice(g);
   delete g;

@@ -23,6 +23,7 @@
 // most once (stamp[t] = last round it was queued for), so a tile is only ever
 // processed by one CTA per round and owns its nodes' distances.
 #include <algorithm>
+#include <climits>
 #include <cstdlib>
 #include <vector>
 
@@ -65,6 +66,7 @@ struct LatParams {
   unsigned max_rounds;
   unsigned long long wait_ns, budget_ns;
   int selfcont;
+  const int32_t *roi_map;  // node-set ROI searches: seeds outside it are ignored
 };
 
 __global__ void fill_kernel(uint32_t *p, int64_t n, uint32_t v) {
@@ -113,6 +115,105 @@ __global__ void gather_box_kernel(const int32_t *__restrict__ slot_eid, const fl
     const int32_t e0 = slot_eid[v], e1 = slot_eid[n + v], e2 = slot_eid[2 * n + v], e3 = slot_eid[3 * n + v];
     w[v] = make_float4(e0 >= 0 ? __ldg(&cost[e0]) : INF_F, e1 >= 0 ? __ldg(&cost[e1]) : INF_F,
                        e2 >= 0 ? __ldg(&cost[e2]) : INF_F, e3 >= 0 ? __ldg(&cost[e3]) : INF_F);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Node-set ROI searches (global_to_roi maps, as SimpleDijkstra.find_path_roi
+// takes them, UPF:1801-1887): the tile sweeps run over the ROI's bounding box,
+// on weights in which every edge that leaves or enters the ROI is +inf.
+
+struct RoiGeom {
+  int32_t nx, ny, nz;
+  int8_t axis[64];
+};
+
+// Bounding box of the ROI, as running maxima bb[6] = {-x0, x1, -y0, y1, -z0,
+// z1} (bb starts far below any coordinate): over the node list when given,
+// else over every node v with roi_map[v] >= 0.
+__global__ void roi_bbox_kernel(const int32_t *__restrict__ nodes, int64_t n, const int32_t *__restrict__ roi_map,
+                                int32_t nx, int32_t ny, int64_t N, int *bb) {
+  int m[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) m[k] = INT_MIN;
+  const int64_t plane = (int64_t)nx * ny;
+  const int64_t s = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += s) {
+    const int64_t v = nodes ? (int64_t)__ldg(&nodes[i]) : i;
+    if (v < 0 || v >= N) continue;
+    if (!nodes && __ldg(&roi_map[v]) < 0) continue;
+    const int32_t z = (int32_t)(v / plane);
+    const int64_t r = v - (int64_t)z * plane;
+    const int32_t y = (int32_t)(r / nx), x = (int32_t)(r - (int64_t)y * nx);
+    m[0] = max(m[0], -x);
+    m[1] = max(m[1], x);
+    m[2] = max(m[2], -y);
+    m[3] = max(m[3], y);
+    m[4] = max(m[4], -z);
+    m[5] = max(m[5], z);
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const int w = __reduce_max_sync(ORSP_FULL_MASK, m[k]);
+    if ((threadIdx.x & 31) == 0 && w != INT_MIN) atomicMax(&bb[k], w);
+  }
+}
+
+// The searched box from the running maxima (an empty ROI gives a box with
+// no cells and no tiles).
+template <int TX, int TY>
+__global__ void roi_box_finish_kernel(const int *bb, LatBox *box) {
+  LatBox B;
+  if (bb[1] < 0) {
+    B.x0 = 0; B.x1 = -1; B.y0 = 0; B.y1 = -1; B.z0 = 0; B.z1 = -1;
+    B.ntx = 0;
+    B.nty = 0;
+  } else {
+    B.x0 = -bb[0]; B.x1 = bb[1]; B.y0 = -bb[2]; B.y1 = bb[3]; B.z0 = -bb[4]; B.z1 = bb[5];
+    B.ntx = (B.x1 - B.x0 + TX) / TX;
+    B.nty = (B.y1 - B.y0 + TY) / TY;
+  }
+  B.tile0 = 0;
+  B.pad = 0;
+  B.dbase = -1;
+  *box = B;
+}
+
+// In-edge weights of the box's nodes, as gather_kernel, with +inf on every
+// edge u -> v where u or v lies outside the ROI (roi_map < 0; NULL: no
+// restriction) or u is a sink (sink[u] != 0; NULL: none).  Grid-stride over
+// the box read from device memory.
+__global__ void gather_roi_kernel(const int32_t *__restrict__ slot_eid, const float *__restrict__ cost,
+                                  float4 *__restrict__ w, int64_t n, RoiGeom G, const LatBox *__restrict__ box,
+                                  const int32_t *__restrict__ roi_map, const uint8_t *__restrict__ sink) {
+  const float INF_F = __int_as_float(0x7f800000);
+  const LatBox B = *box;
+  const int64_t bw = B.x1 - B.x0 + 1, bh = B.y1 - B.y0 + 1, bd = B.z1 - B.z0 + 1;
+  if (bw <= 0 || bh <= 0 || bd <= 0) return;
+  const int64_t plane = bw * bh, count = plane * bd;
+  const int64_t nxy = (int64_t)G.nx * G.ny;
+  const int64_t s = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += s) {
+    const int64_t zz = i / plane;
+    const int64_t r = i - zz * plane;
+    const int64_t yy = r / bw, xx = r - yy * bw;
+    const int32_t gz = B.z0 + (int32_t)zz;
+    const int64_t v = (int64_t)gz * nxy + (int64_t)(B.y0 + yy) * G.nx + (B.x0 + xx);
+    const bool vin = !roi_map || __ldg(&roi_map[v]) >= 0;
+    const int64_t step = G.axis[gz] == 1 ? 1 : G.nx;
+    const int64_t from[4] = {v - step, v + step, v - nxy, v + nxy};
+    float o[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int32_t e = __ldg(&slot_eid[k * n + v]);
+      bool ok = e >= 0 && vin;
+      if (ok) {
+        const int64_t u = from[k];
+        ok = (!roi_map || __ldg(&roi_map[u]) >= 0) && !(sink && __ldg(&sink[u]));
+      }
+      o[k] = ok ? __ldg(&cost[e]) : INF_F;
+    }
+    w[v] = make_float4(o[0], o[1], o[2], o[3]);
   }
 }
 
@@ -181,6 +282,7 @@ __global__ void lattice_seed_kernel(LatParams p, int32_t nseeds, const int32_t *
   for (int i = threadIdx.x; i < nseeds; i += blockDim.x) {
     const int32_t s = seeds[i];
     if (s < 0 || s >= plane * p.nz) continue;
+    if (p.roi_map && __ldg(&p.roi_map[s]) < 0) continue;
     const int32_t z = s / plane, r = s - z * plane, y = r / p.nx, x = r - y * p.nx;
     int bi = -1;
     LatBox B;
@@ -1208,12 +1310,23 @@ int run_lattice_boxes(Graph *g, const float *cost_d, int32_t nseeds, const int32
                       b[5] == g->nz - 1);
   }
   // overlapping boxes (own distances) may hold more cells than the lattice:
-  // then one gather of every node is cheaper than one per box
+  // then one gather of every node is cheaper than one per box.  A whole
+  // gather is skipped when the caller declared, for this search, the same
+  // cost array and generation as the last whole gather's.
+  const uint64_t decl = g->decl_cost == cost_d ? g->decl_gen : 0;
+  g->decl_cost = nullptr;
+  g->decl_gen = 0;
   if (whole || (priv && vol_sum >= N)) {
-    gather_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 148 * 32), 256, 0, st>>>(
-        g->slot_eid, cost_d, (float4 *)g->wslot, N);
-    ORSP_CUDA(cudaGetLastError());
+    if (!(decl != 0 && g->w4_cost == cost_d && g->w4_gen == decl)) {
+      gather_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 148 * 32), 256, 0, st>>>(
+          g->slot_eid, cost_d, (float4 *)g->wslot, N);
+      ORSP_CUDA(cudaGetLastError());
+      g->w4_cost = cost_d;
+      g->w4_gen = decl;
+    }
   } else {
+    g->w4_cost = nullptr;  // part of wslot is rewritten
+    g->w4_gen = 0;
     for (int32_t i = 0; i < nbox; ++i) {
       const int32_t *b = boxes_h + 6 * (int64_t)i;
       const int32_t bw = b[1] - b[0] + 1, bh = b[3] - b[2] + 1;
@@ -1267,6 +1380,63 @@ int run_lattice_search(Graph *g, const float *cost_d, int32_t nseeds, const int3
                            opt);
 }
 
+int run_lattice_roi(Graph *g, const float *cost_d, int32_t nseeds, const int32_t *seeds_d,
+                    const float *seed_cost_d, const int32_t *roi_map_d, const int32_t *roi_nodes_d,
+                    int64_t n_roi, const uint8_t *sink_d, uint32_t *dist, cudaStream_t st) {
+  const int64_t N = g->N;
+  const int TX = lattice_tile_w(), TY = 16;
+  if (!g->lat_box_d) ORSP_CUDA(cudaMalloc(&g->lat_box_d, sizeof(LatBox)));
+  int rc = ensure_roi_arrays(g);
+  if (rc) return rc;
+  LatBox *box_d = (LatBox *)g->lat_box_d;
+  const int gblocks = g->num_sms * 8;
+  if (!roi_map_d && !roi_nodes_d) {
+    const int32_t full[6] = {0, g->nx - 1, 0, g->ny - 1, 0, g->nz - 1};
+    LatBox *hb = (LatBox *)((char *)g->pinned + 1024);
+    make_lat_boxes(full, 1, hb, TX);
+    ORSP_CUDA(cudaMemcpyAsync(box_d, hb, sizeof(LatBox), cudaMemcpyHostToDevice, st));
+  } else {
+    // running maxima start at 0x80808080, below every coordinate
+    ORSP_CUDA(cudaMemsetAsync(g->roi_bb, 0x80, 6 * sizeof(int), st));
+    const int64_t n = roi_nodes_d ? n_roi : N;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, gblocks));
+    roi_bbox_kernel<<<blocks, 256, 0, st>>>(roi_nodes_d, n, roi_map_d, g->nx, g->ny, N, g->roi_bb);
+    ORSP_CUDA(cudaGetLastError());
+    if (TX == 32) roi_box_finish_kernel<32, 16><<<1, 1, 0, st>>>(g->roi_bb, box_d);
+    else roi_box_finish_kernel<16, 16><<<1, 1, 0, st>>>(g->roi_bb, box_d);
+    ORSP_CUDA(cudaGetLastError());
+  }
+  RoiGeom G{};
+  G.nx = g->nx;
+  G.ny = g->ny;
+  G.nz = g->nz;
+  for (int z = 0; z < 64; ++z) G.axis[z] = z < g->nz ? g->layer_axis[z] : 0;
+  gather_roi_kernel<<<(int)std::min<int64_t>((N + 255) / 256, gblocks), 256, 0, st>>>(
+      g->slot_eid, cost_d, (float4 *)g->wslot, N, G, box_d, roi_map_d, sink_d);
+  ORSP_CUDA(cudaGetLastError());
+  g->w4_cost = nullptr;  // masked weights: not reusable by a whole search
+  g->w4_gen = 0;
+  g->decl_cost = nullptr;
+  g->decl_gen = 0;
+  fill_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 148 * 32), 256, 0, st>>>(dist, N, ORSP_INF_BITS);
+  ORSP_CUDA(cudaGetLastError());
+  LatParams p{};
+  p.nx = g->nx;
+  p.ny = g->ny;
+  p.nz = g->nz;
+  p.nbox = 1;
+  p.seed_per_box = 0;
+  p.boxes = box_d;
+  p.w4 = (const float4 *)g->wslot;
+  p.dist = dist;
+  p.roi_map = roi_map_d;
+  for (int z = 0; z < 64; ++z) p.axis[z] = z < g->nz ? g->layer_axis[z] : 0;
+  // the box is known on the device only: size the tile arrays for the lattice
+  const int64_t ntiles = (int64_t)((g->nx - 1 + TX) / TX) * ((g->ny - 1 + TY) / TY);
+  if (TX == 32) return launch_lattice<32, 16>(g, p, ntiles, g->nz, nseeds, seeds_d, seed_cost_d, st, nullptr);
+  return launch_lattice<16, 16>(g, p, ntiles, g->nz, nseeds, seeds_d, seed_cost_d, st, nullptr);
+}
+
 int finish_lattice_search(Graph *g, int32_t *rounds_h) {
   const LatCtl *c = (const LatCtl *)g->lat_ctl_h;
   if (rounds_h) *rounds_h = (int32_t)c->rounds;
@@ -1279,6 +1449,16 @@ int finish_lattice_search(Graph *g, int32_t *rounds_h) {
 }
 
 }  // namespace orsp
+
+extern "C" int orsp_graph_cost_generation(orsp_graph *g, const float *cost_d, uint64_t generation) {
+  if (!g || !cost_d) {
+    orsp::set_error("cost_generation: NULL argument");
+    return ORSP_ERR_ARG;
+  }
+  g->decl_cost = cost_d;
+  g->decl_gen = generation;
+  return ORSP_OK;
+}
 
 extern "C" int orsp_lattice_max_layers(int32_t tile_w, int32_t *out) {
   if (!out || (tile_w != 0 && tile_w != 16 && tile_w != 32)) {

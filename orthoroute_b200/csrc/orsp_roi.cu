@@ -232,6 +232,70 @@ __global__ void truncate_kernel(int32_t *roi, const int32_t *count_in, int32_t m
   *count_out = cnt;
 }
 
+// The same truncation with a general must-keep list, as extract_roi_bfs does
+// with portal seeds (UPF:1700-1731): must_keep = [src, dst] followed by the
+// keep nodes not already in it (list order); the ones missing from the ROI
+// are appended after the ascending part in that order; then, if the list is
+// longer than max_nodes, the k-th must-keep position (ascending) at or past
+// max_nodes is swapped with position k and the list is cut to max_nodes.
+// One thread; the ascending part is binary-searched.  MAX_KEEP bounds the
+// list (checked on the host).
+constexpr int MAX_KEEP = 256;
+__global__ void keep_truncate_kernel(int32_t *roi, const int32_t *count_in, int32_t max_nodes, int32_t src,
+                                     int32_t dst, const int32_t *keep, int32_t nkeep, int32_t *count_out) {
+  if (threadIdx.x != 0) return;
+  int32_t mk[MAX_KEEP + 2];
+  int nmk = 0;
+  mk[nmk++] = src;
+  if (dst != src) mk[nmk++] = dst;
+  for (int i = 0; i < nkeep; ++i) {
+    const int32_t v = keep[i];
+    bool dup = false;
+    for (int j = 0; j < nmk; ++j) dup |= mk[j] == v;
+    if (!dup) mk[nmk++] = v;
+  }
+  const int n0 = *count_in;
+  int n = n0;
+  int32_t pos[MAX_KEEP + 2];
+  for (int j = 0; j < nmk; ++j) {
+    int lo = 0, hi = n0;  // first position with roi[p] >= mk[j]
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (roi[mid] < mk[j]) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo < n0 && roi[lo] == mk[j]) {
+      pos[j] = lo;
+    } else {
+      roi[n] = mk[j];
+      pos[j] = n++;
+    }
+  }
+  int cnt = n;
+  if (n > max_nodes) {
+    // positions in ascending order (insertion sort of a short list)
+    for (int a = 1; a < nmk; ++a) {
+      const int32_t t = pos[a];
+      int b = a - 1;
+      while (b >= 0 && pos[b] > t) {
+        pos[b + 1] = pos[b];
+        --b;
+      }
+      pos[b + 1] = t;
+    }
+    for (int k = 0; k < nmk; ++k) {
+      const int p = pos[k];
+      if (p >= max_nodes) {
+        const int32_t t = roi[p];
+        roi[p] = roi[k];
+        roi[k] = t;
+      }
+    }
+    cnt = max_nodes;
+  }
+  *count_out = cnt;
+}
+
 __global__ void fill_i32_kernel(int32_t *p, int64_t n, int32_t v) {
   const int64_t s = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += s) p[i] = v;
@@ -283,9 +347,30 @@ extern "C" int orsp_roi_box_map(orsp_graph *g, const int32_t *box_h, int32_t *g2
   return ORSP_OK;
 }
 
+static int roi_bfs_impl(orsp_graph *g, int32_t src, int32_t dst, int32_t max_depth, int32_t max_nodes,
+                        const int32_t *keep_d, int32_t nkeep, int32_t *roi_nodes_d, int32_t *g2r_d,
+                        int32_t *roi_count_h, uintptr_t stream);
+
 extern "C" int orsp_roi_bfs(orsp_graph *g, int32_t src, int32_t dst, int32_t max_depth,
                             int32_t max_nodes, int32_t *roi_nodes_d, int32_t *g2r_d,
                             int32_t *roi_count_h, uintptr_t stream) {
+  return roi_bfs_impl(g, src, dst, max_depth, max_nodes, nullptr, 0, roi_nodes_d, g2r_d, roi_count_h, stream);
+}
+
+extern "C" int orsp_roi_bfs_keep(orsp_graph *g, int32_t src, int32_t dst, int32_t max_depth,
+                                 int32_t max_nodes, const int32_t *keep_d, int32_t nkeep,
+                                 int32_t *roi_nodes_d, int32_t *g2r_d, int32_t *roi_count_h,
+                                 uintptr_t stream) {
+  if (nkeep < 0 || nkeep > MAX_KEEP || (nkeep > 0 && !keep_d)) {
+    set_error("roi_bfs_keep: nkeep must be 0.." + std::to_string(MAX_KEEP) + " with a keep list");
+    return ORSP_ERR_ARG;
+  }
+  return roi_bfs_impl(g, src, dst, max_depth, max_nodes, keep_d, nkeep, roi_nodes_d, g2r_d, roi_count_h, stream);
+}
+
+static int roi_bfs_impl(orsp_graph *g, int32_t src, int32_t dst, int32_t max_depth, int32_t max_nodes,
+                        const int32_t *keep_d, int32_t nkeep, int32_t *roi_nodes_d, int32_t *g2r_d,
+                        int32_t *roi_count_h, uintptr_t stream) {
   if (!g || !roi_nodes_d || !roi_count_h) { set_error("roi_bfs: NULL argument"); return ORSP_ERR_ARG; }
   if (src < 0 || src >= g->N || dst < 0 || dst >= g->N) { set_error("roi_bfs: src/dst out of range"); return ORSP_ERR_ARG; }
   if (max_nodes <= 0) { set_error("roi_bfs: max_nodes must be > 0"); return ORSP_ERR_ARG; }
@@ -318,7 +403,10 @@ extern "C" int orsp_roi_bfs(orsp_graph *g, int32_t src, int32_t dst, int32_t max
   ORSP_CUDA(cudaGetLastError());
   write_tiles_kernel<<<ntiles, CMP_THREADS, 0, st>>>(seen, g->N, tiles, roi_nodes_d);
   ORSP_CUDA(cudaGetLastError());
-  truncate_kernel<<<1, 32, 0, st>>>(roi_nodes_d, misc + 4, max_nodes, src, dst, misc + 5);
+  if (nkeep > 0)
+    keep_truncate_kernel<<<1, 32, 0, st>>>(roi_nodes_d, misc + 4, max_nodes, src, dst, keep_d, nkeep, misc + 5);
+  else
+    truncate_kernel<<<1, 32, 0, st>>>(roi_nodes_d, misc + 4, max_nodes, src, dst, misc + 5);
   ORSP_CUDA(cudaGetLastError());
   if (g2r_d) {
     fill_i32_kernel<<<std::min<int64_t>((N + 255) / 256, 4096), 256, 0, st>>>(g2r_d, N, -1);
@@ -339,14 +427,15 @@ extern "C" int orsp_roi_bfs(orsp_graph *g, int32_t src, int32_t dst, int32_t max
 //
 // orsp_roi_bfs keeps its work buffers (visit marks, the four wave queues and
 // the compaction tiles) in device memory that the library allocates with
-// cudaMalloc on first use.  Some callers cannot allow that: code running
-// while a stream is being captured into a CUDA graph, or inside a host that
-// owns all device memory through its own allocator and forbids allocations
-// on the routing path.  orsp_roi_bfs_noalloc gives them the same extraction
-// with its work buffers in one file-scope device array, so the call itself
-// allocates nothing.  The array is sized for graphs of at most
-// ORSP_ROI_BFS_NOALLOC_MAX_NODES nodes and every GPU that loads the library
-// holds it (about 8.5 MB) until the process exits.
+// cudaMalloc on first use.  Some callers cannot allow that: a host
+// application whose own caching allocator has reserved the GPU's memory up
+// front and forbids any other cudaMalloc / cudaFree on the routing path
+// (a cudaFree there also synchronises the whole device).
+// orsp_roi_bfs_noalloc gives them the same extraction with its work buffers
+// in one file-scope device array, so the call itself allocates nothing.  The
+// array is sized for graphs of at most ORSP_ROI_BFS_NOALLOC_MAX_NODES nodes
+// and every GPU that loads the library holds it (about 8.5 MB) until the
+// process exits.
 namespace {
 
 constexpr size_t kNaSeenBytes = ((size_t)ORSP_ROI_BFS_NOALLOC_MAX_NODES + 15) & ~(size_t)15;
@@ -363,7 +452,11 @@ std::mutex g_na_mutex;
 void *g_na_ptr[kNaMaxDevices] = {};
 
 // Device address of the array on `device` (which must be current).  Looked up
-// once per device: host code cannot use the symbol itself as a device address.
+// once per device, by the first call on it: in host code the symbol is only a
+// host-side stand-in, not a device address.  The address is cached by device
+// ordinal, so the call assumes the device's primary context (the runtime
+// API's default); a caller that switches driver-API contexts on one device
+// would get an address from another context.
 int noalloc_scratch(int device, unsigned char **out) {
   std::lock_guard<std::mutex> lock(g_na_mutex);
   if (device < 0 || device >= kNaMaxDevices) {
@@ -428,7 +521,8 @@ extern "C" int orsp_roi_bfs_noalloc(orsp_graph *g, int32_t src, int32_t dst, int
                                                                                  misc + 5, g2r_d);
     ORSP_CUDA(cudaGetLastError());
   }
-  // g->pinned was allocated when the graph was created, not here.
+  // g->pinned was allocated when the graph was created, not here; it is one
+  // buffer per graph, so overlapping calls on one graph race on it too.
   ORSP_CUDA(cudaMemcpyAsync(g->pinned, misc, 24, cudaMemcpyDeviceToHost, st));
   ORSP_CUDA(cudaStreamSynchronize(st));
   const int32_t *h = (const int32_t *)g->pinned;

@@ -361,6 +361,8 @@ struct LatBacktraceParams {
   const float *seed_cost;
   int32_t nseeds;
   int32_t dst;
+  const int32_t *dst_d;     // when set, the target is read here (< 0: no path)
+  const int32_t *rank_map;  // node-set ROI: ranks are global_to_roi (NULL: node ids)
   int32_t *path_out;
   int32_t path_cap;
   SsspCtl *ctl;
@@ -371,10 +373,15 @@ __global__ void lat_backtrace_kernel(LatBacktraceParams p) {
   SsspCtl *ctl = p.ctl;
   if (ctl->err) return;
   const LatBox &B = p.box;
+  const int32_t dst = p.dst_d ? *p.dst_d : p.dst;
+  if (dst < 0) {
+    if (lane == 0) { ctl->path_len = 0; ctl->status = 1; }
+    return;
+  }
   int32_t x, y, z;
-  lat_xyz(p.geom, p.dst, x, y, z);
+  lat_xyz(p.geom, dst, x, y, z);
   const bool in = x >= B.x0 && x <= B.x1 && y >= B.y0 && y <= B.y1 && z >= B.z0 && z <= B.z1;
-  unsigned dv = in ? __ldcg(&p.dist[p.dst]) : ORSP_INF_BITS;
+  unsigned dv = in ? __ldcg(&p.dist[dst]) : ORSP_INF_BITS;
   if (dv == ORSP_INF_BITS) {
     if (lane == 0) { ctl->path_len = 0; ctl->status = 1; }
     return;
@@ -393,7 +400,10 @@ __global__ void lat_backtrace_kernel(LatBacktraceParams p) {
       if (seeds[i] == v && f_bits(seed_cost ? seed_cost[i] : 0.0f) == d) return true;
     return false;
   };
-  int len = lat_walk_warp(p.geom, B, p.w4, dget, at_start, x, y, z, dv, p.path_out, p.path_cap);
+  int len;
+  if (p.rank_map) len = lat_walk_warp(p.geom, B, p.w4, dget, at_start, x, y, z, dv, p.path_out, p.path_cap,
+                                      orsp::LatRankRoi{p.rank_map});
+  else len = lat_walk_warp(p.geom, B, p.w4, dget, at_start, x, y, z, dv, p.path_out, p.path_cap);
   int err = 0;
   if (len == -1) err = DEV_ERR_PATH_OVERFLOW;
   else if (len < 0) err = DEV_ERR_INTERNAL;
@@ -450,6 +460,21 @@ __global__ void pick_target_kernel(const uint32_t *dist, const int32_t *roi_map,
   }
   if (threadIdx.x == 0) *best = s_t[0];
 }
+
+// global_to_roi[roi_nodes[i]] = i (a repeated node keeps its last index, as
+// numpy's fancy assignment global_to_roi[roi_nodes] = arange(R) does), or,
+// with clear, back to -1.
+__global__ void roi_scatter_kernel(const int32_t *nodes, int64_t n, int32_t N, int32_t *map, int clear) {
+  const int64_t s = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += s) {
+    const int32_t v = nodes[i];
+    if (v < 0 || v >= N) continue;
+    if (clear) map[v] = -1;
+    else atomicMax(&map[v], (int32_t)i);
+  }
+}
+
+__global__ void put_i32_kernel(int32_t *p, int32_t v) { *p = v; }
 
 __global__ void mark_kernel(uint8_t *mask, int32_t n, const int32_t *nodes, int32_t N, uint8_t v) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -616,15 +641,21 @@ static int sssp_impl(orsp_graph *g, const float *cost_d, int32_t nseeds, const i
   // (boxes deeper than a shared-memory tile holds, about 33 layers at tile
   // width 16, also take the generic search)
   const int depth = box_h ? box_h[5] - box_h[4] + 1 : g->nz;
-  const bool lattice = g->lattice_ok && roi_map_d == nullptr && lattice_tile_fits(depth) &&
-                       !(impl && std::string(impl) == "generic");
+  const bool lattice = g->lattice_ok && lattice_tile_fits(depth) && !(impl && std::string(impl) == "generic");
+  // a node-set ROI on a lattice: tile sweeps over the ROI's bounding box on
+  // ROI-masked weights, ranks from the ROI map in the backtrace
+  const bool lattice_roi = lattice && roi_map_d != nullptr;
   if (box_h && !lattice) {
     if (!g->box_g2r) ORSP_CUDA(cudaMalloc(&g->box_g2r, (size_t)g->N * 4));
     rc = orsp_roi_box_map(g, box_h, g->box_g2r, stream);
     if (rc) return rc;
     roi_map_d = g->box_g2r;
   }
-  if (lattice) {
+  if (lattice_roi) {
+    rc = run_lattice_roi(g, cost_d, nseeds, seeds_d, seed_cost_d, roi_map_d, nullptr, 0, nullptr, dist, st);
+    if (rc) return rc;
+    ORSP_CUDA(cudaMemsetAsync(g->ctl, 0, sizeof(SsspCtl), st));
+  } else if (lattice) {
     rc = run_lattice_search(g, cost_d, nseeds, seeds_d, seed_cost_d, box_h, dist, st);
     if (rc) return rc;
     ORSP_CUDA(cudaMemsetAsync(g->ctl, 0, sizeof(SsspCtl), st));
@@ -642,7 +673,8 @@ static int sssp_impl(orsp_graph *g, const float *cost_d, int32_t nseeds, const i
     b.geom.nz = g->nz;
     for (int z = 0; z < 64; ++z) b.geom.axis[z] = z < g->nz ? g->layer_axis[z] : 0;
     const int32_t full[6] = {0, g->nx - 1, 0, g->ny - 1, 0, g->nz - 1};
-    const int32_t *bx = box_h ? box_h : full;
+    const int32_t *bx = (box_h && !lattice_roi) ? box_h : full;
+    b.rank_map = lattice_roi ? roi_map_d : nullptr;
     b.box.x0 = bx[0];
     b.box.x1 = bx[1];
     b.box.y0 = bx[2];
@@ -697,6 +729,117 @@ static int sssp_impl(orsp_graph *g, const float *cost_d, int32_t nseeds, const i
   return ORSP_OK;
 }
 
+// Backtrace parameters of a lattice search over the whole lattice (distances
+// +inf outside the searched box).
+static LatBacktraceParams lat_bt_full(orsp_graph *g, const uint32_t *dist, const int32_t *seeds_d,
+                                      const float *seed_cost_d, int32_t nseeds, int32_t dst,
+                                      const int32_t *dst_d, const int32_t *rank_map, int32_t *path_out_d,
+                                      int32_t path_cap) {
+  LatBacktraceParams b{};
+  b.w4 = (const float4 *)g->wslot;
+  b.dist = dist;
+  b.geom.nx = g->nx;
+  b.geom.ny = g->ny;
+  b.geom.nz = g->nz;
+  for (int z = 0; z < 64; ++z) b.geom.axis[z] = z < g->nz ? g->layer_axis[z] : 0;
+  b.box.x0 = 0;
+  b.box.x1 = g->nx - 1;
+  b.box.y0 = 0;
+  b.box.y1 = g->ny - 1;
+  b.box.z0 = 0;
+  b.box.z1 = g->nz - 1;
+  b.box.dbase = -1;
+  b.seeds = seeds_d;
+  b.seed_cost = seed_cost_d;
+  b.nseeds = nseeds;
+  b.dst = dst;
+  b.dst_d = dst_d;
+  b.rank_map = rank_map;
+  b.path_out = path_out_d;
+  b.path_cap = path_cap;
+  b.ctl = (SsspCtl *)g->ctl;
+  return b;
+}
+
+static bool use_lattice_roi(const orsp_graph *g) {
+  const char *impl = getenv("ORSP_SSSP_IMPL");
+  return g->lattice_ok && lattice_tile_fits(g->nz) && !(impl && std::string(impl) == "generic");
+}
+
+extern "C" int orsp_sssp_roi_nodes(orsp_graph *g, const float *cost_d, int32_t src, int32_t dst,
+                                   const int32_t *roi_nodes_d, int64_t n_roi, int32_t *path_out_d,
+                                   int32_t path_cap, int32_t *path_len_h, uintptr_t stream) {
+  if (!g || !cost_d || !roi_nodes_d || n_roi <= 0 || !path_out_d || path_cap <= 0 || !path_len_h) {
+    set_error("sssp_roi_nodes: NULL argument, empty ROI or path_cap <= 0");
+    return ORSP_ERR_ARG;
+  }
+  if (src < 0 || src >= g->N || dst < 0 || dst >= g->N) { set_error("sssp_roi_nodes: src/dst out of range"); return ORSP_ERR_ARG; }
+  ORSP_CUDA(cudaSetDevice(g->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = ensure_single_ws(g, true);
+  if (rc) return rc;
+  rc = ensure_roi_arrays(g);
+  if (rc) return rc;
+  *path_len_h = 0;
+  const int sblocks = (int)std::max<int64_t>(1, std::min<int64_t>((n_roi + 255) / 256, 1024));
+  roi_scatter_kernel<<<sblocks, 256, 0, st>>>(roi_nodes_d, n_roi, g->N, g->roi_map, 0);
+  ORSP_CUDA(cudaGetLastError());
+  put_i32_kernel<<<1, 1, 0, st>>>(g->seed_one, src);
+  ORSP_CUDA(cudaGetLastError());
+  const bool lattice = use_lattice_roi(g);
+  // a failed launch still puts the map back to -1 for the next call
+  auto fail = [&](int code) {
+    roi_scatter_kernel<<<sblocks, 256, 0, st>>>(roi_nodes_d, n_roi, g->N, g->roi_map, 1);
+    cudaStreamSynchronize(st);
+    return code;
+  };
+  if (lattice) {
+    rc = run_lattice_roi(g, cost_d, 1, g->seed_one, nullptr, g->roi_map, roi_nodes_d, n_roi, nullptr, g->dist, st);
+    if (rc) return fail(rc);
+    ORSP_CUDA(cudaMemsetAsync(g->ctl, 0, sizeof(SsspCtl), st));
+    LatBacktraceParams b = lat_bt_full(g, g->dist, g->seed_one, nullptr, 1, dst, nullptr, g->roi_map, path_out_d,
+                                       path_cap);
+    lat_backtrace_kernel<<<1, 32, 0, st>>>(b);
+    ORSP_CUDA(cudaGetLastError());
+  } else {
+    rc = run_grid_search(g, cost_d, 1, g->seed_one, nullptr, dst, g->roi_map, nullptr, 0.0f, g->dist, st);
+    if (rc) return fail(rc);
+    BacktraceParams b{};
+    b.cost = cost_d;
+    b.roi_map = g->roi_map;
+    b.rptr = g->rptr;
+    b.rsrc = g->rsrc;
+    b.reid = g->reid;
+    b.dist = g->dist;
+    b.seeds = g->seed_one;
+    b.seed_cost = nullptr;
+    b.nseeds = 1;
+    b.dst = dst;
+    b.path_out = path_out_d;
+    b.path_cap = path_cap;
+    b.ctl = (SsspCtl *)g->ctl;
+    backtrace_kernel<<<1, 32, 0, st>>>(b);
+    ORSP_CUDA(cudaGetLastError());
+  }
+  // the map goes back to -1 for the next call
+  roi_scatter_kernel<<<sblocks, 256, 0, st>>>(roi_nodes_d, n_roi, g->N, g->roi_map, 1);
+  ORSP_CUDA(cudaGetLastError());
+  ORSP_CUDA(cudaMemcpyAsync(g->ctl_h, g->ctl, sizeof(SsspCtl), cudaMemcpyDeviceToHost, st));
+  ORSP_CUDA(cudaStreamSynchronize(st));
+  const SsspCtl *c = (const SsspCtl *)g->ctl_h;
+  if (lattice) {
+    rc = finish_lattice_search(g, nullptr);
+    if (rc) return rc;
+  }
+  if (c->err) return dev_status_to_orsp(c->err);
+  *path_len_h = c->path_len;
+  if (c->status == 1 || c->path_len < 2) {
+    *path_len_h = 0;
+    return ORSP_NO_PATH;
+  }
+  return ORSP_OK;
+}
+
 extern "C" int orsp_sssp(orsp_graph *g, const float *cost_d, int32_t nseeds,
                          const int32_t *seeds_d, const float *seed_cost_d,
                          int32_t dst, const int32_t *roi_map_d, float delta,
@@ -738,6 +881,45 @@ extern "C" int orsp_sssp_multi(orsp_graph *g, const float *cost_d, int32_t nseed
   cudaStream_t st = (cudaStream_t)stream;
   int rc = ensure_single_ws(g, true);
   if (rc) return rc;
+  if (use_lattice_roi(g)) {
+    // tile sweeps with the targets' out-edges blocked (a target is settled
+    // but never expanded, UPF:1941-1950), then the winner and the lattice walk
+    rc = ensure_roi_arrays(g);
+    if (rc) return rc;
+    const int mblocks = std::max(1, std::min(1024, (ntargets + 255) / 256));
+    mark_kernel<<<mblocks, 256, 0, st>>>(g->sink_mask, ntargets, targets_d, g->N, 1);
+    ORSP_CUDA(cudaGetLastError());
+    rc = run_lattice_roi(g, cost_d, nseeds, seeds_d, seed_cost_d, roi_map_d, nullptr, 0, g->sink_mask, g->dist, st);
+    if (rc) {  // the sink mask goes back to 0 for the next call
+      mark_kernel<<<mblocks, 256, 0, st>>>(g->sink_mask, ntargets, targets_d, g->N, 0);
+      cudaStreamSynchronize(st);
+      return rc;
+    }
+    ORSP_CUDA(cudaMemsetAsync(g->ctl, 0, sizeof(SsspCtl), st));
+    int32_t *best_l = g->seed_one + 8;
+    pick_target_kernel<<<1, 256, 0, st>>>(g->dist, roi_map_d, ntargets, targets_d, target_cost_d, g->N, best_l);
+    ORSP_CUDA(cudaGetLastError());
+    LatBacktraceParams b = lat_bt_full(g, g->dist, seeds_d, seed_cost_d, nseeds, -1, best_l, roi_map_d, path_out_d,
+                                       path_cap);
+    lat_backtrace_kernel<<<1, 32, 0, st>>>(b);
+    ORSP_CUDA(cudaGetLastError());
+    mark_kernel<<<mblocks, 256, 0, st>>>(g->sink_mask, ntargets, targets_d, g->N, 0);
+    ORSP_CUDA(cudaGetLastError());
+    ORSP_CUDA(cudaMemcpyAsync(g->ctl_h, g->ctl, sizeof(SsspCtl), cudaMemcpyDeviceToHost, st));
+    ORSP_CUDA(cudaMemcpyAsync((char *)g->pinned + 64, best_l, 4, cudaMemcpyDeviceToHost, st));
+    ORSP_CUDA(cudaStreamSynchronize(st));
+    const SsspCtl *c = (const SsspCtl *)g->ctl_h;
+    if (best_target_h) *best_target_h = *(const int32_t *)((const char *)g->pinned + 64);
+    rc = finish_lattice_search(g, nullptr);
+    if (rc) return rc;
+    if (c->err) return dev_status_to_orsp(c->err);
+    *path_len_h = c->path_len;
+    if (c->status == 1 || c->path_len < 2) {
+      *path_len_h = 0;
+      return ORSP_NO_PATH;
+    }
+    return ORSP_OK;
+  }
   // scratch: sink mask (N bytes) + the winning target
   const size_t mask_b = ((size_t)g->N + 255) & ~(size_t)255;
   rc = ensure_scratch(g, mask_b + 256);

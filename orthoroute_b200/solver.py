@@ -110,11 +110,19 @@ class DeviceGraph:
     # --------------------------------------------------------------- searches
     def sssp(self, cost: torch.Tensor, seeds, dst: int = -1, roi_map: Optional[torch.Tensor] = None,
              seed_cost: Optional[torch.Tensor] = None, delta: Optional[float] = None,
-             dist_out: Optional[torch.Tensor] = None, path_cap: Optional[int] = None):
+             dist_out: Optional[torch.Tensor] = None, path_cap: Optional[int] = None,
+             cost_generation: Optional[int] = None):
         """One search (orsp_sssp: the lattice tile sweep or the generic grid
-        search).  Returns (status, path tensor (device, int32, possibly empty),
-        rounds)."""
+        search).  cost_generation (non-zero): the caller's identifier of the
+        cost array's current contents, declared for this search
+        (orsp_graph_cost_generation); a whole-lattice search then reuses the
+        weights gathered by an earlier search with the same array and
+        generation.  Returns (status, path tensor (device, int32, possibly
+        empty), rounds)."""
         lib = _lib.load()
+        if cost_generation:
+            check(lib.orsp_graph_cost_generation(self._h, ptr(cost), int(cost_generation)),
+                  "orsp_graph_cost_generation")
         if isinstance(seeds, (int, np.integer)):
             # one seed: a device fill instead of a host->device copy
             if self._seed_buf is None:
@@ -134,6 +142,20 @@ class DeviceGraph:
                                  ctypes.byref(plen), ctypes.byref(rounds), _stream()), "orsp_sssp")
         path = pbuf[: plen.value] if (dst >= 0 and st == _lib.ORSP_OK) else None
         return st, path, int(rounds.value)
+
+    def sssp_roi_nodes(self, cost: torch.Tensor, src: int, dst: int, roi_nodes: torch.Tensor,
+                       path_cap: Optional[int] = None):
+        """One search src -> dst over the ROI given as its node list (device
+        int32; ROI index = position).  Returns (status, path tensor or None)."""
+        lib = _lib.load()
+        cap = int(path_cap or min(self.N + 1, DEFAULT_PATH_CAP))
+        pbuf = self._path_buffer(cap)
+        plen = ctypes.c_int32(0)
+        st = check(lib.orsp_sssp_roi_nodes(self._h, ptr(cost), int(src), int(dst), ptr(roi_nodes),
+                                           int(roi_nodes.numel()), ptr(pbuf), cap, ctypes.byref(plen), _stream()),
+                   "orsp_sssp_roi_nodes")
+        path = pbuf[: plen.value] if st == _lib.ORSP_OK else None
+        return st, path
 
     def sssp_box(self, cost: torch.Tensor, src: int, dst: int, box, delta: Optional[float] = None,
                  dist_out: Optional[torch.Tensor] = None, path_cap: Optional[int] = None):
@@ -229,6 +251,18 @@ class DeviceGraph:
                                ptr(g2r), ctypes.byref(cnt), _stream()), "orsp_roi_bfs")
         return roi[: cnt.value], g2r
 
+    def roi_bfs_keep(self, src: int, dst: int, max_depth: int, max_nodes: int, keep) -> torch.Tensor:
+        """Bidirectional BFS ROI with extra must-keep nodes (portal seeds).
+        Returns roi_nodes (device int32[R])."""
+        lib = _lib.load()
+        roi = torch.empty(self.N, dtype=torch.int32, device=self.device)
+        kp = as_device(np.asarray(keep, dtype=np.int32), torch.int32, self.device)
+        cnt = ctypes.c_int32(0)
+        check(lib.orsp_roi_bfs_keep(self._h, int(src), int(dst), int(max_depth), int(max_nodes), ptr(kp),
+                                    int(kp.numel()), ptr(roi), None, ctypes.byref(cnt), _stream()),
+              "orsp_roi_bfs_keep")
+        return roi[: cnt.value]
+
     def path_to_edges(self, path: torch.Tensor) -> torch.Tensor:
         lib = _lib.load()
         n = int(path.numel())
@@ -256,14 +290,23 @@ class GpuSolver:
         self.lattice = lattice
         self.N = self.dg.N
         self._cost_cache = (None, None)
+        # the ROI extractor whose last result this solver may reuse on the device
+        self.roi_source = None
+        self._full_roi = None
 
     def _cost(self, costs) -> torch.Tensor:
-        """Device copy of the cost array.  The router calls once per net with the
-        same host array, which it also rewrites in place between iterations
-        (via pooling, UPF:3381/3443/5298), so the cached device copy is reused
-        only when the host bits are unchanged."""
+        """Device copy of the cost array.  A host array of the drop-in
+        accountant (orthoroute_b200.dropin) carries a write counter, so its
+        device copy is reused until the host array is written (O(1) per call).
+        Any other host array is compared by value with the last one: the
+        router calls once per net with the same array, which it also rewrites
+        in place between iterations (via pooling, UPF:3381/3443/5298)."""
         if isinstance(costs, torch.Tensor):
             return as_device(costs, torch.float32, self.dg.device)
+        mirror = getattr(costs, "_mirror", None)
+        if mirror is not None:
+            owner, name = mirror
+            return owner.device_array(name)
         if hasattr(costs, "__cuda_array_interface__"):  # cupy array from a GPU-mode router
             return as_device(torch.as_tensor(costs, device=self.dg.device), torch.float32, self.dg.device)
         host = np.ascontiguousarray(np.asarray(costs), dtype=np.float32)
@@ -275,21 +318,61 @@ class GpuSolver:
         self._cost_cache = (host.copy(), t)
         return t
 
+    def _is_full_roi(self, roi_nodes) -> bool:
+        """roi_nodes == arange(N) (the reference's full-graph ROI for long nets,
+        UPF:4656-4660); checked once per array object."""
+        if len(roi_nodes) != self.N or isinstance(roi_nodes, torch.Tensor):
+            return False
+        if self._full_roi is not None and self._full_roi[0] is roi_nodes:
+            return self._full_roi[1]
+        a = np.asarray(roi_nodes)
+        full = bool(int(a[0]) == 0 and int(a[-1]) == self.N - 1 and
+                    np.array_equal(a, np.arange(self.N, dtype=a.dtype)))
+        self._full_roi = (roi_nodes, full)
+        return full
+
+    def _roi_device(self, roi_nodes, global_to_roi):
+        """The ROI node list on the device, or None when global_to_roi is not
+        the inverse of roi_nodes (then the caller's map is used as given).
+        The check samples positions of the list (both ends, the middle)."""
+        if isinstance(roi_nodes, torch.Tensor):
+            return as_device(roi_nodes, torch.int32, self.dg.device)
+        n = len(roi_nodes)
+        if global_to_roi is not None and not isinstance(global_to_roi, torch.Tensor):
+            for k in {0, n // 2, n - 1}:
+                if int(global_to_roi[int(roi_nodes[k])]) != k:
+                    return None
+        src = self.roi_source
+        if src is not None:
+            dev = src.device_roi_for(roi_nodes)
+            if dev is not None:
+                return dev
+        return torch.from_numpy(np.ascontiguousarray(roi_nodes, dtype=np.int32)).to(self.dg.device)
+
     def find_path_roi_gpu(self, src: int, dst: int, costs, roi_nodes, global_to_roi) -> Optional[List[int]]:
         """CUDADijkstra.find_path_roi_gpu (CD:4909): node path src..dst in global
         ids, or None.  Semantics of SimpleDijkstra.find_path_roi: the search is
-        restricted to nodes with global_to_roi >= 0 and ties between equal
-        distances go to the smaller ROI index."""
+        restricted to the ROI and ties between equal distances go to the
+        smaller ROI index.  The ROI goes to the device as its node list (O(R)
+        per call); global_to_roi is rebuilt there from it."""
         cost = self._cost(costs)
-        n_roi = len(roi_nodes)
-        full = n_roi == self.N and int(roi_nodes[0]) == 0 and int(roi_nodes[-1]) == self.N - 1
-        g2r = None if full else as_device(global_to_roi, torch.int32, self.dg.device)
-        if g2r is not None and (int(global_to_roi[src]) < 0 or int(global_to_roi[dst]) < 0):
+        if len(roi_nodes) == 0:
             return None
-        st, path, _ = self.dg.sssp(cost, int(src), int(dst), roi_map=g2r)
+        if self._is_full_roi(roi_nodes):
+            st, path, _ = self.dg.sssp(cost, int(src), int(dst))
+        else:
+            roi_d = self._roi_device(roi_nodes, global_to_roi)
+            if roi_d is None:
+                g2r = as_device(global_to_roi, torch.int32, self.dg.device)
+                st, path, _ = self.dg.sssp(cost, int(src), int(dst), roi_map=g2r)
+            else:
+                st, path = self.dg.sssp_roi_nodes(cost, int(src), int(dst), roi_d)
         if st != _lib.ORSP_OK or path is None or path.numel() < 2:
             return None
         return path.cpu().tolist()
+
+    # SimpleDijkstra.find_path_roi (UPF:1801) has the same signature
+    find_path_roi = find_path_roi_gpu
 
     def find_path_multisource_multisink(self, src_seeds, dst_targets, costs, roi_nodes, global_to_roi):
         """SimpleDijkstra.find_path_multisource_multisink (UPF:1889-1989):

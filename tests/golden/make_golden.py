@@ -1,8 +1,8 @@
 """Generates the golden vectors in tests/golden/ by running the reference's own
-CPU code (OrthoRoute, imported from its source tree; default /root/reference).
+CPU code (OrthoRoute, imported from its source tree: --ref or $ORTHOROUTE_REFERENCE).
 
 Run from the repository root:
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref <OrthoRoute tree>]  (default: $ORTHOROUTE_REFERENCE)
 
 Outputs (small .npz files, committed):
   golden_dijkstra.npz   SimpleDijkstra.find_path_roi (UPF:1801-1887) on
@@ -349,7 +349,9 @@ def gen_via(upf, graph, lat, rng):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("ORTHOROUTE_REFERENCE"),
+                    required=not os.environ.get("ORTHOROUTE_REFERENCE"),
+                    help="OrthoRoute source tree (default: $ORTHOROUTE_REFERENCE)")
     args = ap.parse_args()
     upf = import_reference(args.ref)
     rng = np.random.default_rng(20261203)

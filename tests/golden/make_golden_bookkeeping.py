@@ -1,7 +1,7 @@
 """Golden vectors for the per-iteration negotiation bookkeeping, produced by
 the reference's own methods on a real router state.
 
-    python tests/golden/make_golden_bookkeeping.py [--ref /root/reference]
+    python tests/golden/make_golden_bookkeeping.py [--ref <OrthoRoute tree>]  (default: $ORTHOROUTE_REFERENCE)
 
 A small board is routed for a few iterations by the unmodified reference
 router (oracle/ref_harness.py), then, on that router's state:
@@ -19,6 +19,7 @@ unified_pathfinder.py).  Net names are stored by index (net k is "N{k}").
 from __future__ import annotations
 
 import argparse
+import os
 import random
 import sys
 from pathlib import Path
@@ -32,7 +33,9 @@ sys.path.insert(0, str(REPO))
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("ORTHOROUTE_REFERENCE"),
+                    required=not os.environ.get("ORTHOROUTE_REFERENCE"),
+                    help="OrthoRoute source tree (default: $ORTHOROUTE_REFERENCE)")
     args = ap.parse_args()
     from oracle.ref_harness import run_reference
     from orthoroute_b200.lattice import board_uniform_pins

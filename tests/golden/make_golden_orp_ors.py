@@ -1,7 +1,7 @@
 """Golden files for the .ORP / .ORS formats and the headless board mapping,
 produced by the reference's own code on a hand-made board.
 
-    python tests/golden/make_golden_orp_ors.py [--ref /root/reference]
+    python tests/golden/make_golden_orp_ors.py [--ref <OrthoRoute tree>]  (default: $ORTHOROUTE_REFERENCE)
 
 From the reference (orthoroute/infrastructure/serialization/orp_exporter.py,
 ors_exporter.py, main.py and algorithms/manhattan/unified_pathfinder.py):
@@ -236,7 +236,9 @@ def jsonable(o):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("ORTHOROUTE_REFERENCE"),
+                    required=not os.environ.get("ORTHOROUTE_REFERENCE"),
+                    help="OrthoRoute source tree (default: $ORTHOROUTE_REFERENCE)")
     args = ap.parse_args()
     os.environ["PYTHONDONTWRITEBYTECODE"] = "1"
     sys.dont_write_bytecode = True

@@ -14,7 +14,8 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-REF = Path(os.environ.get("ORTHOROUTE_REFERENCE", "/root/reference"))
+# the reference source tree, named by ORTHOROUTE_REFERENCE (skipped when unset)
+REF = Path(os.environ.get("ORTHOROUTE_REFERENCE") or "/nonexistent")
 pytestmark = [pytest.mark.skipif(not (REF / "orthoroute").exists(), reason="reference source tree not available"),
               pytest.mark.filterwarnings("ignore::DeprecationWarning")]
 

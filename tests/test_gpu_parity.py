@@ -626,3 +626,36 @@ def test_seed_on_tile_edge_single_layer_box(impl, monkeypatch):
                                        cuda(np.array([box], np.int32)), path_cap=512)
         L = int(lens[0])
         assert L == len(ref) and nodes[0, :L].cpu().tolist() == ref.tolist()
+
+
+def test_cost_generation_reuses_gathered_weights_only_when_declared():
+    """orsp_graph_cost_generation: a whole-lattice search with the same array
+    and generation as the last whole gather reuses the gathered weights; a new
+    generation, an undeclared search or a box / ROI search in between gathers
+    again, so every search sees the current costs."""
+    lat = build_lattice(64, 48, 6)
+    w = uniform_weights(lat, seed=5, blocked_frac=0.05)
+    dg = DeviceGraph.from_lattice(lat)
+    wt = torch.from_numpy(w).cuda()
+    dist = torch.empty(lat.N, dtype=torch.float32, device="cuda")
+    rng = np.random.default_rng(2)
+
+    def check(src, cost_host, gen):
+        st, _, _ = dg.sssp(wt, int(src), -1, dist_out=dist, cost_generation=gen)
+        _, ref, _, _ = O.dijkstra(lat.indptr, lat.indices, cost_host, [int(src)])
+        assert st == 0 and np.array_equal(_bits(dist.cpu().numpy()), _bits(ref)), (src, gen)
+
+    s = rng.choice(lat.N, size=6, replace=False)
+    check(s[0], w, 7)
+    check(s[1], w, 7)          # reused
+    w2 = w.copy()
+    w2[::3] = np.float32(2.5)
+    wt.copy_(torch.from_numpy(w2))
+    check(s[2], w2, 8)         # new generation: gathered again
+    dg.sssp_box(wt, int(s[3]), -1, (0, 20, 0, 20, 0, lat.nz - 1))
+    check(s[3], w2, 8)         # a box search rewrote part of the weights
+    w3 = w2.copy()
+    w3[1::5] = np.float32(1.25)
+    wt.copy_(torch.from_numpy(w3))
+    check(s[4], w3, None)      # undeclared: always gathered
+    check(s[5], w3, 9)

@@ -19,7 +19,8 @@ import pytest
 import oracle as O
 from orthoroute_b200.lattice import build_lattice
 
-REF = Path(os.environ.get("ORTHOROUTE_REFERENCE", "/root/reference"))
+# the reference source tree, named by ORTHOROUTE_REFERENCE (skipped when unset)
+REF = Path(os.environ.get("ORTHOROUTE_REFERENCE") or "/nonexistent")
 pytestmark = pytest.mark.skipif(not (REF / "orthoroute").exists(), reason="reference source tree not available")
 
 
@@ -89,6 +90,29 @@ def test_roi_bfs_equals_reference_on_random_cases(upf, seed):
         roi, g2r = O.roi_bfs(lat.indptr, lat.indices, s, d, min(depth, 150), max_nodes)
         assert np.array_equal(roi, np.asarray(ref, np.int32)), (s, d, depth, max_nodes)
         assert np.array_equal(g2r[roi], np.arange(len(roi)))
+
+
+@pytest.mark.timeout(600)
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_roi_bfs_with_portal_seeds_equals_reference(upf, seed):
+    """extract_roi_bfs with portal_seeds: missing seeds appended as must-keep
+    nodes, and kept through the truncation swap (UPF:1700-1731)."""
+    rng = np.random.default_rng(250 + seed)
+    lat = build_lattice(int(rng.integers(10, 30)), int(rng.integers(10, 30)), int(rng.integers(2, 6)))
+    g = _Graph(lat.indptr, lat.indices)
+    for _ in range(16):
+        max_nodes = int(rng.choice([50_000, 800, 200, 60, 5]))
+        ex = upf.ROIExtractor(g, use_gpu=False, lattice=None)
+        ex.max_roi_nodes = max_nodes
+        s, d = (int(v) for v in rng.choice(lat.N, size=2, replace=False))
+        depth = int(rng.integers(1, 30))
+        # seeds near and far, with repeats and with src / dst among them
+        seeds = [(int(v), float(rng.random())) for v in rng.choice(lat.N, size=int(rng.integers(1, 9)))]
+        seeds += [(s, 0.0), seeds[0]]
+        ref, _ = ex.extract_roi_bfs(s, d, initial_radius=depth, portal_seeds=seeds)
+        roi, g2r = O.roi_bfs(lat.indptr, lat.indices, s, d, min(depth, 150), max_nodes,
+                             keep=[n for n, _ in seeds])
+        assert np.array_equal(roi, np.asarray(ref, np.int32)), (s, d, depth, max_nodes)
 
 
 @pytest.mark.parametrize("seed", [1, 2, 3, 4])

@@ -1,8 +1,9 @@
 """orsp_roi_bfs_noalloc: ROI extraction for callers that cannot allocate device
-memory while they route (for example code running during CUDA stream capture,
-or an application whose own allocator owns all device memory).  Its work
-buffers are one fixed array inside the library; the results must equal those
-of the allocating entry point orsp_roi_bfs, call after call.
+memory while they route (an application whose own caching allocator has
+reserved the GPU's memory and allows no other cudaMalloc / cudaFree on the
+routing path).  Its work buffers are one fixed array inside the library; the
+results must equal those of the allocating entry point orsp_roi_bfs, call
+after call.
 
 This file is collected last on purpose, so that a run stopping at the first
 failure has already run every other test."""
@@ -49,6 +50,24 @@ def test_noalloc_roi_matches_allocating_entry_point_on_consecutive_calls():
         assert np.array_equal(roi_na, roi)
         assert np.array_equal(g2r_na, g2r)
         assert len(roi_na) > 0 and s in set(roi_na.tolist()) and d in set(roi_na.tolist())
+
+
+def test_noalloc_roi_at_the_array_limit():
+    """A graph of exactly ORSP_ROI_BFS_NOALLOC_MAX_NODES nodes fills the visit
+    marks, queues and compaction tiles to their ends."""
+    lib = _lib.load()
+    lat = build_lattice(1024, 256, 2)  # 524 288 nodes, both axes on both layers
+    assert lat.N == MAX_NODES
+    dg = DeviceGraph.from_lattice(lat)
+    # deep searches from the two ends of the node range (the last node and
+    # the last compaction tile are marked), a shallow one between them
+    for s, d, depth, max_nodes in ((0, lat.N - 1, 150, MAX_NODES), (77, 5000, 12, 900),
+                                   (lat.N - 1, 0, 150, MAX_NODES)):
+        rc_na, roi_na, g2r_na = _extract(lib.orsp_roi_bfs_noalloc, dg, s, d, depth, max_nodes)
+        rc, roi, g2r = _extract(lib.orsp_roi_bfs, dg, s, d, depth, max_nodes)
+        assert rc_na == rc == _lib.ORSP_OK, lib.orsp_last_error()
+        assert np.array_equal(roi_na, roi)
+        assert np.array_equal(g2r_na, g2r)
 
 
 def test_noalloc_roi_rejects_graphs_beyond_its_array():
