@@ -387,6 +387,28 @@ def route_c3(dev, with_cpu: bool):
     rw = pf.route(b.src, b.dst, mode="batched", history_init=h0)
     pf.cfg = cfg
     warm_sec = t_pred + rw.seconds + (0.0 if rw.converged else rb.seconds)
+    # ablation: the same schedule from a non-learned prior (RUDY wire density,
+    # warm.rudy_prediction) at the scale chosen for it on the same held-out
+    # boards as the network's
+    from orthoroute_b200.warm import history_from_prediction, pretrained_rudy_scale, rudy_prediction
+
+    rudy_scale = pretrained_rudy_scale()
+    ablation = None
+    if rudy_scale is not None:
+        t0 = time.perf_counter()
+        hr = history_from_prediction(b.lattice, rudy_prediction(b.lattice, b.src, b.dst), rudy_scale)
+        t_rudy = time.perf_counter() - t0
+        pf.cfg = warm_cfg
+        ra = pf.route(b.src, b.dst, mode="batched", history_init=hr)
+        pf.cfg = cfg
+        a_sec = t_rudy + ra.seconds + (0.0 if ra.converged else rb.seconds)
+        ablation = {"prior": "RUDY (half-perimeter wire length spread over each net's bounding box), not learned",
+                    "history_scale": rudy_scale, "sec_batched_prior": round(a_sec, 3),
+                    "converged": bool(ra.converged), "iterations": len(ra.iterations),
+                    "searches": int(sum(s_.nets_searched for s_ in ra.iterations)),
+                    "speedup_vs_plain": round(rs.seconds / a_sec, 2),
+                    "wirelength_delta_pct": round(100.0 * (ra.wirelength - rb.wirelength) / max(1, rb.wirelength), 3),
+                    "vias_delta_pct": round(100.0 * (ra.vias - rb.vias) / max(1, rb.vias), 3)}
     out = {
         "workload": "600x600x18 lattice, 8000 nets between 2x50 connector footprints, bbox+10 ROI, "
                     "per-net live costs, offenders rerouted, disjoint-round order",
@@ -423,6 +445,7 @@ def route_c3(dev, with_cpu: bool):
             "vias_delta_pct": round(100.0 * (rw.vias - rb.vias) / max(1, rb.vias), 3),
             "overuse_trace": [s.over_sum for s in rw.iterations],
         },
+        "ablation_non_learned_prior": ablation,
     }
     if with_cpu:
         # The C oracle of one box search (heap Dijkstra, fp32) on a sample of

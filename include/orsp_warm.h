@@ -26,6 +26,23 @@ ORSP_API int orsp_warm_conv3d(const void *X, const void *mask, const void *Wt, c
                               float *Yf, int32_t D, int32_t H, int32_t W, int32_t Cin, int32_t Cout,
                               int32_t relu, uintptr_t stream);
 
+/* The same convolution (same arguments and results up to the summation
+ * order of the fp32 accumulation) on the 5th-generation tensor cores:
+ * tcgen05.mma with bf16 operands staged in shared memory in the canonical
+ * K-major layout and the fp32 accumulator in tensor memory (128 voxels x
+ * Cout per tile), persistent CTAs.  Cin and Cout multiples of 16, Cout <= 64,
+ * and all 27 x Cin x Cout weights within shared memory (Cin x Cout <= 2048
+ * for Cout <= 32; Cin <= 32 for Cout = 64).  A wait that expires (2 s) is
+ * recorded for orsp_warm_tc_status. */
+ORSP_API int orsp_warm_conv3d_tc(const void *X, const void *mask, const void *Wt, const float *bias, void *Y,
+                                 float *Yf, int32_t D, int32_t H, int32_t W, int32_t Cin, int32_t Cout,
+                                 int32_t relu, uintptr_t stream);
+
+/* 1 in *expired if a tensor-core convolution gave up on a wait since the
+ * last call (then its output is incomplete), else 0; clears the record.
+ * Synchronises with the device. */
+ORSP_API int orsp_warm_tc_status(int32_t *expired);
+
 /* Weight and bias gradients of a convolution: dW[tap][ci][co] +=
  * sum_v X[v+tap][ci] * G[v][co] and db[co] += sum_v G[v][co] (db optional),
  * with G = dY, or dY where Yo > 0 when the layer's ReLU output Yo is given.

@@ -27,6 +27,7 @@ SOURCES = [
     "orsp_via.cu",
     "orsp_route.cu",
     "orsp_warm.cu",
+    "orsp_warm_tc.cu",
     "orsp_bookkeeping.cu",
     "orsp_geometry.cu",
 ]

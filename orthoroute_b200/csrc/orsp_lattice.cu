@@ -534,7 +534,7 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
   unsigned long long ts0 = 0;
   if (threadIdx.x == 0) ts0 = dev_globaltimer();
   if (threadIdx.x < 5) s_act[threadIdx.x] = 0;
-  if (threadIdx.x < 3) s_flags[threadIdx.x] = 0;
+  if (threadIdx.x < 6) s_flags[threadIdx.x] = 0;
   if (s_nb && threadIdx.x < 4) {  // neighbour tiles in the box: left, right, down, up (-1: box edge)
     const int d = threadIdx.x;
     s_nb[d] = d == 0 ? (tx > 0 ? t - 1 : -1)
@@ -639,13 +639,20 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
 
   // ---- sweep cycles.  Each cycle: the planar runs (x-runs on H layers and
   // y-runs on V layers touch disjoint layers, so they run side by side), then
-  // the via runs along z.
+  // the via runs along z.  s_flags[c % 3] records a planar change in cycle c,
+  // s_flags[3 + c % 3] a via change.  A pass that changes nothing leaves every
+  // constraint it checks satisfied, so once a planar pass changes nothing
+  // after a via pass that changed nothing, the tile is at its fixpoint and the
+  // cycle's via pass is skipped.
   bool converged = false;
   int cyc = 0;
   const int nplan = nh * th + nv * tw;
   const bool full = tw == TX && th == TY;
   for (; cyc < MAX_CYCLES; ++cyc) {
-    if (threadIdx.x == 0) s_flags[(cyc + 1) % 3] = 0;
+    if (threadIdx.x == 0) {
+      s_flags[(cyc + 1) % 3] = 0;
+      s_flags[3 + (cyc + 1) % 3] = 0;
+    }
     bool chg = false;
     if (full) {
       for (int rr = threadIdx.x; rr < nplan; rr += (TX * TY)) {
@@ -683,15 +690,18 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
         chg |= sweep_run(cell, ds, wlo + wo, whi + wo, ws, n);
       }
     }
+    if (chg) s_flags[cyc % 3] = 1;
     tile_sync<TX * TY, SPEC>();
+    if (cyc > 0 && !s_flags[cyc % 3] && !s_flags[3 + (cyc - 1) % 3]) { converged = true; break; }
+    chg = false;
     for (int c = threadIdx.x; c < tw * th; c += (TX * TY)) {
       const int xx = c % tw + 1, yy = c / tw + 1;
       const int wo = (yy - 1) * WSX + (xx - 1);
       chg |= zrun<PS, WPS>(sd + yy * SX + xx, wdn + wo, wup + wo, nzb);
     }
-    if (chg) s_flags[cyc % 3] = 1;
+    if (chg) s_flags[3 + cyc % 3] = 1;
     tile_sync<TX * TY, SPEC>();
-    if (!s_flags[cyc % 3]) { converged = true; break; }
+    if (!s_flags[cyc % 3] && !s_flags[3 + cyc % 3]) { converged = true; break; }
   }
   unsigned long long ts2 = 0;
   if (threadIdx.x == 0) {
@@ -756,7 +766,7 @@ template <int TX, int TY, bool PRIV>
 __global__ void __launch_bounds__(TX * TY, 1) lattice_tile_kernel(LatParams p) {
   extern __shared__ float sd[];
   __shared__ LayerLists s_layers;
-  __shared__ int s_flags[3];
+  __shared__ int s_flags[6];
   __shared__ int s_act[5];
   __shared__ int s_tile;
   LatCtl *ctl = p.ctl;
@@ -848,7 +858,7 @@ template <int TX, int TY, bool PRIV, bool DEEP = false, int MINB = 1>
 __global__ void __launch_bounds__(TX * TY, MINB) lattice_async_kernel(LatParams p) {
   extern __shared__ float sd[];
   __shared__ LayerLists s_layers;
-  __shared__ int s_flags[3];
+  __shared__ int s_flags[6];
   __shared__ int s_act[5];
   __shared__ int s_nb[4];
   __shared__ int s_tile;
@@ -984,7 +994,7 @@ __global__ void __launch_bounds__(TX * TY + 32, 1) lattice_spec_kernel(LatParams
   constexpr int NW = TX * TY;
   extern __shared__ float sd[];
   __shared__ LayerLists s_layers;
-  __shared__ int s_flags[3];
+  __shared__ int s_flags[6];
   __shared__ int s_act[2][5];
   __shared__ volatile int s_cur;
   __shared__ volatile int s_done;

@@ -1,0 +1,302 @@
+// The warm-start network's 3x3x3 convolution on the 5th-generation tensor
+// cores: tcgen05.mma (kind::f16, bf16 operands, fp32 accumulator in TMEM).
+//
+// Implicit GEMM, as conv3d_kernel in orsp_warm.cu: M = 128 voxels along x of
+// one (z, y) row, N = Cout, K = 27 taps x Cin.  Each CTA is persistent:
+//   - it stages every tap's weights once, B[n][k] = Wt[tap][k][n], in shared
+//     memory in the K-major canonical UMMA layout without swizzle (core
+//     matrices of 8 rows x 16 bytes, rows contiguous; the two 8-element halves
+//     of a 16-wide K slice 128 bytes apart, 8-row groups 256 bytes apart);
+//   - per tile and per input plane (dz) all 128 threads gather the nine
+//     (dy, dx) im2col blocks A[m][k] = X[z+dz][y+dy][x0+m+dx][k] in the same
+//     layout (16-byte loads, zero outside the grid, the optional ReLU mask
+//     applied on the way), fence them to the async proxy, and one thread
+//     issues the 9 x Cin/16 MMAs (K = 16 each) into the TMEM accumulator and
+//     commits them to an mbarrier;
+//   - the epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM
+//     lanes 32w..32w+31, i.e. voxels 32w..32w+31), adds the bias, applies the
+//     ReLU and stores bf16 or fp32.
+// Every mbarrier wait is bounded by the global timer; on expiry the kernel
+// records an error, waits once more (bounded) for its MMAs, frees its TMEM
+// and returns.  Single-GPU code: no TMA, no multicast.
+#include <algorithm>
+#include <cstdint>
+
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "orsp_warm.h"
+
+namespace {
+
+constexpr int TC_M = 128;        // voxels per tile: the MMA's M and the accumulator's TMEM lanes
+constexpr int TC_THREADS = 128;  // four warps, one per 32-lane quarter of TMEM
+constexpr unsigned long long TC_WAIT_NS = 2000000000ull;
+
+__device__ int g_tc_err = 0;     // set by a kernel whose wait expired (orsp_warm_tc_status)
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor of a K-major operand without swizzle:
+// start address, leading byte offset (between the K halves), stride byte
+// offset (between 8-row groups), all in 16-byte units; version 1 (sm_100).
+__device__ __forceinline__ uint64_t umma_smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((addr >> 4) & 0x3FFFu);
+  d |= static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16;
+  d |= static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32;
+  d |= static_cast<uint64_t>(1) << 46;
+  return d;
+}
+
+// Instruction descriptor: fp32 accumulator, bf16 A and B, both K-major,
+// N >> 3 and M >> 4.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(N >> 3) << 17) |
+         (static_cast<uint32_t>(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t"
+      "}"
+      :
+      : "r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t"
+      "}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for the phase with the given parity to complete, at most TC_WAIT_NS.
+__device__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  const unsigned long long t0 = dev_globaltimer();
+  for (;;) {
+    if (mbar_try(bar, parity)) return true;
+    if (dev_globaltimer() - t0 > TC_WAIT_NS) return false;
+  }
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Bytes of shared memory for Cin, Cout: all weights, nine im2col blocks of
+// one plane, the mbarrier and the TMEM address slot.
+__host__ __device__ constexpr size_t tc_smem_bytes(int Cin, int Cout) {
+  return static_cast<size_t>(27) * (Cin / 16) * Cout * 32 + static_cast<size_t>(9) * (Cin / 16) * 4096 + 64;
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1) conv3d_tc_kernel(
+    const __nv_bfloat16 *__restrict__ X, const __nv_bfloat16 *__restrict__ Mk, const __nv_bfloat16 *__restrict__ Wt,
+    const float *__restrict__ bias, __nv_bfloat16 *__restrict__ Y, float *__restrict__ Yf, int D, int H, int W,
+    int Cin, int Cout, int relu) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int KC = Cin >> 4;
+  const int bblk = Cout * 32;  // bytes of one (tap, 16-wide K slice) weight block
+  unsigned char *sB = sm;
+  unsigned char *sA = sm + static_cast<size_t>(27) * KC * bblk;
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sA + static_cast<size_t>(9) * KC * 4096);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t ncols = Cout <= 32 ? 32u : 64u;
+
+  // weights: one 16-byte unit = 8 consecutive k of one n
+  const int units_per_tap = Cin * Cout / 8;
+  for (int i = tid; i < 27 * units_per_tap; i += TC_THREADS) {
+    const int tap = i / units_per_tap, r = i - tap * units_per_tap;
+    const int kg = r / Cout, n = r - kg * Cout;  // kg: 8-element group of k
+    const __nv_bfloat16 *src = Wt + (static_cast<int64_t>(tap) * Cin + kg * 8) * Cout + n;
+    uint32_t v[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const uint32_t lo = __bfloat16_as_ushort(src[(2 * j) * Cout]);
+      const uint32_t hi = __bfloat16_as_ushort(src[(2 * j + 1) * Cout]);
+      v[j] = lo | (hi << 16);
+    }
+    unsigned char *dst = sB + (tap * KC + (kg >> 1)) * bblk + (n >> 3) * 256 + (kg & 1) * 128 + (n & 7) * 16;
+    *reinterpret_cast<uint4 *>(dst) = make_uint4(v[0], v[1], v[2], v[3]);
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = umma_idesc_bf16(TC_M, Cout);
+  const uint32_t bar_a = smem_addr(bar);
+  uint32_t phase = 0;
+  bool ok = true;
+
+  const int ntx = (W + TC_M - 1) / TC_M;
+  const int64_t ntiles = static_cast<int64_t>(D) * H * ntx;
+  for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+    const int tx = static_cast<int>(t % ntx);
+    const int64_t zy = t / ntx;
+    const int y = static_cast<int>(zy % H), z = static_cast<int>(zy / H);
+    const int x0 = tx * TC_M;
+    for (int dzi = 0; dzi < 3 && ok; ++dzi) {
+      const int zz = z + dzi - 1;
+      const bool zok = zz >= 0 && zz < D;
+      // im2col blocks of the nine (dy, dx) taps of plane zz: unit = 8
+      // channels of one voxel; consecutive threads take consecutive voxels
+      for (int i = tid; i < 9 * KC * TC_M * 2; i += TC_THREADS) {
+        const int kh = i & 1, m = (i >> 1) & (TC_M - 1), rest = i >> 8;
+        const int kc = rest % KC, tap9 = rest / KC;
+        const int yy = y + tap9 / 3 - 1, xx = x0 + m + tap9 % 3 - 1;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (zok && yy >= 0 && yy < H && xx >= 0 && xx < W && x0 + m < W) {
+          const int64_t off = ((static_cast<int64_t>(zz) * H + yy) * W + xx) * Cin + kc * 16 + kh * 8;
+          v = *reinterpret_cast<const uint4 *>(X + off);
+          if (Mk) {
+            const uint4 mk = *reinterpret_cast<const uint4 *>(Mk + off);
+            __nv_bfloat16 *pv = reinterpret_cast<__nv_bfloat16 *>(&v);
+            const __nv_bfloat16 *pm = reinterpret_cast<const __nv_bfloat16 *>(&mk);
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+              if (!(__bfloat162float(pm[q]) > 0.0f)) pv[q] = __float2bfloat16(0.0f);
+          }
+        }
+        unsigned char *dst = sA + (tap9 * KC + kc) * 4096 + (m >> 3) * 256 + kh * 128 + (m & 7) * 16;
+        *reinterpret_cast<uint4 *>(dst) = v;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      tc_fence_before();
+      __syncthreads();
+      tc_fence_after();
+      if (tid == 0) {
+        for (int tap9 = 0; tap9 < 9; ++tap9)
+          for (int kc = 0; kc < KC; ++kc) {
+            const uint64_t a = umma_smem_desc(smem_addr(sA + (tap9 * KC + kc) * 4096), 128, 256);
+            const uint64_t b = umma_smem_desc(smem_addr(sB + ((dzi * 9 + tap9) * KC + kc) * bblk), 128, 256);
+            mma_bf16(tmem, a, b, idesc, (dzi | tap9 | kc) != 0 ? 1u : 0u);
+          }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_a)
+                     : "memory");
+      }
+      // the MMAs read the im2col blocks: wait before they are overwritten
+      // (the outcome is made uniform over the CTA, so that every thread
+      // takes the same path through the barriers and warp-wide TMEM loads)
+      ok = __syncthreads_and(mbar_wait(bar_a, phase) ? 1 : 0) != 0;
+      phase ^= 1u;
+      tc_fence_after();
+    }
+    if (!ok) break;
+    // epilogue: warp w holds voxels 32w..32w+31, one TMEM lane each
+    const int m = warp * 32 + lane, xx = x0 + m;
+    for (int c0 = 0; c0 < Cout; c0 += 16) {
+      uint32_t r[16];
+      tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0), r);
+      if (xx < W) {
+        const int64_t o = ((static_cast<int64_t>(z) * H + y) * W + xx) * Cout + c0;
+        float f[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          float v = __uint_as_float(r[j]) + (bias ? bias[c0 + j] : 0.0f);
+          f[j] = relu ? fmaxf(v, 0.0f) : v;
+        }
+        if (Yf) {
+#pragma unroll
+          for (int j = 0; j < 16; j += 4)
+            *reinterpret_cast<float4 *>(Yf + o + j) = make_float4(f[j], f[j + 1], f[j + 2], f[j + 3]);
+        } else {
+          uint32_t p[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            p[j] = static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16(f[2 * j]))) |
+                   (static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16(f[2 * j + 1]))) << 16);
+          *reinterpret_cast<uint4 *>(Y + o) = make_uint4(p[0], p[1], p[2], p[3]);
+          *reinterpret_cast<uint4 *>(Y + o + 8) = make_uint4(p[4], p[5], p[6], p[7]);
+        }
+      }
+    }
+    // the next tile's first MMA overwrites the accumulator
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+  }
+  if (!ok) {
+    // a wait expired: record it and give the MMAs in flight one more bounded
+    // wait before the accumulator is freed
+    if (tid == 0) atomicExch(&g_tc_err, 1);
+    mbar_wait(bar_a, phase ^ 1u);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+  }
+}
+
+}  // namespace
+
+using namespace orsp;
+
+extern "C" int orsp_warm_conv3d_tc(const void *X, const void *mask, const void *Wt, const float *bias, void *Y,
+                                   float *Yf, int32_t D, int32_t H, int32_t W, int32_t Cin, int32_t Cout,
+                                   int32_t relu, uintptr_t stream) {
+  if (!X || !Wt || (!Y && !Yf) || D <= 0 || H <= 0 || W <= 0 || Cin <= 0 || Cin % 16 || Cout <= 0 ||
+      Cout % 16 || Cout > 64) {
+    set_error("warm_conv3d_tc: bad arguments (Cin, Cout multiples of 16, Cout <= 64)");
+    return ORSP_ERR_ARG;
+  }
+  const size_t smem = tc_smem_bytes(Cin, Cout);
+  if (smem > 227 * 1024) {
+    set_error("warm_conv3d_tc: weights of this Cin x Cout do not fit in shared memory");
+    return ORSP_ERR_ARG;
+  }
+  int dev = 0, sms = 0;
+  ORSP_CUDA(cudaGetDevice(&dev));
+  ORSP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  ORSP_CUDA(cudaFuncSetAttribute(conv3d_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int64_t ntiles = static_cast<int64_t>(D) * H * ((W + TC_M - 1) / TC_M);
+  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(ntiles, sms)));
+  conv3d_tc_kernel<<<grid, TC_THREADS, smem, (cudaStream_t)stream>>>(
+      (const __nv_bfloat16 *)X, (const __nv_bfloat16 *)mask, (const __nv_bfloat16 *)Wt, bias,
+      (__nv_bfloat16 *)Y, Yf, D, H, W, Cin, Cout, relu);
+  ORSP_CUDA(cudaGetLastError());
+  return ORSP_OK;
+}
+
+extern "C" int orsp_warm_tc_status(int32_t *expired) {
+  if (!expired) { set_error("warm_tc_status: NULL argument"); return ORSP_ERR_ARG; }
+  int v = 0, zero = 0;
+  ORSP_CUDA(cudaMemcpyFromSymbol(&v, g_tc_err, sizeof(int)));
+  ORSP_CUDA(cudaMemcpyToSymbol(g_tc_err, &zero, sizeof(int)));
+  *expired = v;
+  return ORSP_OK;
+}

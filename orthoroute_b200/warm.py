@@ -23,6 +23,7 @@ net bounding-box coverage, H-layer flag, V-layer flag, layer position.
 from __future__ import annotations
 
 import math
+import os
 from dataclasses import dataclass
 from typing import Dict, List, Optional, Tuple
 
@@ -120,6 +121,33 @@ def history_from_prediction(lat: Lattice, pred: np.ndarray, scale: float = 1.0) 
     return (p[lat.edge_src(), kind] * scale).astype(np.float32)
 
 
+def rudy_prediction(lat: Lattice, src: np.ndarray, dst: np.ndarray) -> np.ndarray:
+    """A non-learned congestion prior in the network's output format
+    ([nz][ny][nx][2], log1p domain): RUDY, each net's half-perimeter wire
+    length (w + h) spread uniformly over its bounding box (w x h cells), summed
+    over nets, per cell in x/y and the same on every layer and edge kind.
+    It is the baseline the learned prediction is compared with: the same
+    history mapping and scale search apply to both."""
+    nx, ny, nz = lat.nx, lat.ny, lat.nz
+    sx, sy, _ = (np.asarray(v).astype(np.int64) for v in lat.coords(np.asarray(src)))
+    dx, dy, _ = (np.asarray(v).astype(np.int64) for v in lat.coords(np.asarray(dst)))
+    x0, x1 = np.minimum(sx, dx), np.maximum(sx, dx) + 1
+    y0, y1 = np.minimum(sy, dy), np.maximum(sy, dy) + 1
+    w = (x1 - x0).astype(np.float64)
+    h = (y1 - y0).astype(np.float64)
+    dens = (w + h) / (w * h)
+    acc = np.zeros((ny + 1, nx + 1), np.float64)
+    np.add.at(acc, (y0, x0), dens)
+    np.add.at(acc, (y0, x1), -dens)
+    np.add.at(acc, (y1, x0), -dens)
+    np.add.at(acc, (y1, x1), dens)
+    rudy = acc.cumsum(0).cumsum(1)[:ny, :nx] / nz  # wire per routing layer and cell
+    p = np.log1p(np.maximum(rudy, 0.0)).astype(np.float32)
+    out = np.empty((nz, ny, nx, 2), np.float32)
+    out[:] = p[None, :, :, None]
+    return out
+
+
 # ----------------------------------------------------------------- the net
 @dataclass
 class Layer:
@@ -157,6 +185,16 @@ class WarmNet:
         self.v = {k: torch.zeros_like(v) for k, v in self.m.items()}
         self.t = 0
         self._packed: Dict[str, torch.Tensor] = {}
+        # convolution kernel: "tc" (tcgen05.mma with a TMEM accumulator,
+        # orsp_warm_conv3d_tc) or "wmma" (orsp_warm_conv3d); ORSP_WARM_CONV
+        # overrides the default
+        self.conv_impl = os.environ.get("ORSP_WARM_CONV", "wmma")
+
+    def _conv_call(self, *args):
+        lib = _lib.load()
+        if self.conv_impl == "tc":
+            return check(lib.orsp_warm_conv3d_tc(*args), "orsp_warm_conv3d_tc")
+        return check(lib.orsp_warm_conv3d(*args), "orsp_warm_conv3d")
 
     # weights as the conv kernel reads them
     def _pack(self, name: str, transpose: bool) -> torch.Tensor:
@@ -178,9 +216,8 @@ class WarmNet:
         else:
             y = torch.empty(D, H, W, l.cout, dtype=torch.bfloat16, device=self.device)
             yb, yf = y, None
-        check(_lib.load().orsp_warm_conv3d(ptr(x), None, ptr(self._packed[name]), ptr(self.b[name]), ptr(yb),
-                                           ptr(yf), D, H, W, l.cin, l.cout, 1 if l.relu else 0, _st()),
-              "orsp_warm_conv3d")
+        self._conv_call(ptr(x), None, ptr(self._packed[name]), ptr(self.b[name]), ptr(yb), ptr(yf), D, H, W, l.cin,
+                        l.cout, 1 if l.relu else 0, _st())
         return y
 
     def _pool(self, x, D, H, W):
@@ -245,8 +282,7 @@ class WarmNet:
             return None
         wt = self._pack(name, True)
         dx = torch.empty(D, H, W, l.cin, dtype=torch.bfloat16, device=self.device)
-        check(lib.orsp_warm_conv3d(ptr(dy), ptr(mask), ptr(wt), None, ptr(dx), None, D, H, W, l.cout, l.cin, 0,
-                                   _st()), "orsp_warm_conv3d")
+        self._conv_call(ptr(dy), ptr(mask), ptr(wt), None, ptr(dx), None, D, H, W, l.cout, l.cin, 0, _st())
         return dx
 
     def backward(self, a: dict, dout: torch.Tensor):
@@ -326,8 +362,15 @@ def load_pretrained(path=None, device=None) -> Tuple["WarmNet", float]:
     history scale."""
     st = dict(np.load(path or DEFAULT_WEIGHTS))
     net = WarmNet(C=32, device=device)
-    net.load_state({k: v.astype(np.float32) for k, v in st.items() if k != "scale"})
+    net.load_state({k: v.astype(np.float32) for k, v in st.items() if k.startswith(("w_", "b_"))})
     return net, float(st.get("scale", 1.0))
+
+
+def pretrained_rudy_scale(path=None) -> Optional[float]:
+    """The history scale chosen for the RUDY prior on the same held-out
+    boards as the network's (None if the shipped file has none)."""
+    st = np.load(path or DEFAULT_WEIGHTS)
+    return float(st["rudy_scale"]) if "rudy_scale" in st.files else None
 
 
 def warm_history(net: "WarmNet", lat: Lattice, src, dst, scale: float) -> np.ndarray:

@@ -1,6 +1,7 @@
 """Training data, training and evaluation of the history warm start.
 
     python -m orthoroute_b200.warm_train [--boards 14] [--heldout 2] [--size 600] [--epochs 30]
+                                         [--scale-size 600] [--rudy-scales 1,4,16]
                                          [--out orthoroute_b200/data/warm_history.npz]
 
 Boards: seeded connector-footprint boards (2x50-pin footprints, one net per
@@ -28,7 +29,7 @@ import torch
 
 from .lattice import board_footprints
 from .negotiate import NegotiationConfig, PathFinder
-from .warm import WarmNet, board_features, history_from_prediction, node_targets
+from .warm import WarmNet, board_features, history_from_prediction, node_targets, rudy_prediction
 
 DENSITY = 8000 / (600 * 600)
 DEFAULT_OUT = Path(__file__).resolve().parent / "data" / "warm_history.npz"
@@ -109,11 +110,15 @@ def eval_loss(net: WarmNet, data: List[dict]) -> float:
     return tot / max(1, len(data))
 
 
-def warm_route(net: WarmNet, board, scale: float, mode: str = "batched", device=None, max_iterations: int = 60):
-    """Routes `board` from the predicted history; returns (RouteResult,
-    seconds spent on features + inference + mapping)."""
+def warm_route(net, board, scale: float, mode: str = "batched", device=None, max_iterations: int = 60):
+    """Routes `board` from a predicted history; returns (RouteResult, seconds
+    spent on features + prediction + mapping).  `net` is a WarmNet or the
+    string "rudy" (the non-learned prior, warm.rudy_prediction)."""
     t0 = time.perf_counter()
-    pred = net.predict(board_features(board.lattice, board.src, board.dst))
+    if isinstance(net, str):
+        pred = rudy_prediction(board.lattice, board.src, board.dst)
+    else:
+        pred = net.predict(board_features(board.lattice, board.src, board.dst))
     h0 = history_from_prediction(board.lattice, pred, scale)
     torch.cuda.synchronize()
     t_pred = time.perf_counter() - t0
@@ -122,12 +127,14 @@ def warm_route(net: WarmNet, board, scale: float, mode: str = "batched", device=
     return r, t_pred
 
 
-def choose_scale(net: WarmNet, size: int, nz: int, seeds: List[int], scales=(0.25, 0.5, 1.0)) -> dict:
+def choose_scale(net, size: int, nz: int, seeds: List[int], scales=(0.25, 0.5, 1.0)) -> dict:
+    """The history scale (for a WarmNet or "rudy") that converges on most
+    boards with the fewest iterations (ties: least time)."""
+    boards = [make_board(size, nz, sd) for sd in seeds]
     res = {}
     for s in scales:
         its, secs, conv = 0, 0.0, 0
-        for sd in seeds:
-            b = make_board(size, nz, sd)
+        for b in boards:
             r, tp = warm_route(net, b, s)
             its += len(r.iterations)
             secs += r.seconds + tp
@@ -151,7 +158,9 @@ def main(argv: Optional[List[str]] = None):
     ap.add_argument("--blur", type=int, default=2, help="target averaged over (2 blur + 1)^2 cells in x/y")
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--scale-boards", type=int, default=2, help="held-out boards used to choose the scale")
+    ap.add_argument("--scale-size", type=int, default=0, help="size of those boards (0: --size)")
     ap.add_argument("--scales", default="1,4,16")
+    ap.add_argument("--rudy-scales", default="", help="scales tried for the RUDY prior (empty: no ablation)")
     ap.add_argument("--out", default=str(DEFAULT_OUT))
     ap.add_argument("--summary", default=None)
     args = ap.parse_args(argv)
@@ -176,17 +185,32 @@ def main(argv: Optional[List[str]] = None):
         zero.w[k].zero_()
     base_loss = eval_loss(zero, held)  # predicting zero history everywhere
     scales = tuple(float(v) for v in args.scales.split(","))
-    sc = choose_scale(net, args.size, args.nz, seeds[args.boards:][: args.scale_boards], scales)
-    plain_its = sum(d["iterations"] for d in held[: args.scale_boards])
-    plain_secs = sum(d["seconds"] for d in held[: args.scale_boards])
+    ssize = args.scale_size or args.size
+    sseeds = seeds[args.boards:][: args.scale_boards]
+    sc = choose_scale(net, ssize, args.nz, sseeds, scales)
+    if ssize == args.size:
+        plain_its = sum(d["iterations"] for d in held[: args.scale_boards])
+        plain_secs = sum(d["seconds"] for d in held[: args.scale_boards])
+    else:  # the scale boards are of another size: route them plainly here
+        plain = [make_sample(ssize, args.nz, sd, blur=args.blur) for sd in sseeds]
+        plain_its = sum(d["iterations"] for d in plain)
+        plain_secs = sum(d["seconds"] for d in plain)
+    rudy = None
+    if args.rudy_scales:
+        rudy = choose_scale("rudy", ssize, args.nz, sseeds, tuple(float(v) for v in args.rudy_scales.split(",")))
     st = net.state()
     st["scale"] = np.float32(sc["scale"])
+    if rudy is not None:
+        st["rudy_scale"] = np.float32(rudy["scale"])
     Path(args.out).parent.mkdir(parents=True, exist_ok=True)
     np.savez_compressed(args.out, **{k: (v.astype(np.float16) if k.startswith("w_") else v) for k, v in st.items()})
     summary = {"boards": args.boards, "heldout": args.heldout, "size": args.size, "nz": args.nz,
                "epochs": args.epochs, "train_loss": losses, "heldout_loss": held_loss,
                "heldout_loss_zero_prediction": base_loss, "scale": sc["scale"],
                "scale_table": {str(k): v for k, v in sc["table"].items()},
+               "scale_boards": {"size": ssize, "seeds": sseeds},
+               "rudy_scale": None if rudy is None else rudy["scale"],
+               "rudy_scale_table": None if rudy is None else {str(k): v for k, v in rudy["table"].items()},
                "heldout_plain_iterations": plain_its, "heldout_plain_seconds": plain_secs,
                "crop": args.crop, "steps": args.steps, "boost": args.boost, "blur": args.blur, "lr": args.lr,
                "sec_data": round(t_data, 1), "sec_train": round(t_train, 1),
