@@ -542,6 +542,23 @@ def sweep_c4(dev, nsearch: int = 4096):
     same_oracle = all(
         (l1[k] < 2 and rl[j] < 2) or (l1[k] == rl[j] and np.array_equal(n1[k, : l1[k]], rn[j, : rl[j]]))
         for j, k in enumerate(pick))
+    # E_relaxed on the same sample: in-box out-edges of the nodes settled
+    # before the target (distance below the target's), against the box edges
+    # the sweep's edge rate counts
+    esrc = lat.edge_src()
+    xs, ys, zs = (np.asarray(v) for v in lat.coords(np.arange(lat.N)))
+    relaxed = boxed = 0
+    for k in pick:
+        bx = boxes[k]
+        inbox = ((xs >= bx[0]) & (xs <= bx[1]) & (ys >= bx[2]) & (ys <= bx[3]) & (zs >= bx[4]) & (zs <= bx[5]))
+        g2r = np.where(inbox, np.arange(lat.N), -1).astype(np.int32)
+        _, dist, _, _ = O.dijkstra(lat.indptr, lat.indices, w, [int(src[k])], dst=int(dst[k]), roi_map=g2r)
+        dd = dist[int(dst[k])]
+        settled = np.isfinite(dist) & (dist <= dd) & inbox
+        e_in = inbox[esrc] & inbox[lat.indices]
+        relaxed += int((settled[esrc] & e_in).sum())
+        boxed += int(e_in.sum())
+    relaxed_frac = relaxed / max(1, boxed)
     return {
         "workload": f"{nsearch} box searches on a 400x400x16 lattice, sides log-uniform per axis "
                     "(x,y 20..400, z 4..16), 3% blocked, shared fp32 costs",
@@ -550,8 +567,12 @@ def sweep_c4(dev, nsearch: int = 4096):
         "searches_per_s_one_per_launch": round(nsearch / t_single, 1),
         "searches_per_s_default_plan": round(nsearch / t_default, 1),
         "searches_per_s_tuned": round(nsearch / t_tuned, 1),
-        "gteps_tuned": round(roi_edges / t_tuned / 1e9, 3),
-        "gteps_unit": "directed ROI edges of all searches per second",
+        "box_edges_per_s_tuned": round(roi_edges / t_tuned / 1e9, 3),
+        "box_edges_unit": "G directed ROI edges of all searches per second",
+        "gteps_tuned": round(relaxed_frac * roi_edges / t_tuned / 1e9, 3),
+        "gteps_unit": "G E_relaxed per second: in-box out-edges of the nodes settled before each target, "
+                      "as a fraction of the box edges measured by the oracle on the 64-search sample "
+                      f"({relaxed_frac:.3f}) and applied to all box edges",
         "speedup_tuned_vs_one_per_launch": round(t_single / t_tuned, 2),
         "sec_tuning": round(t_tune, 2),
         "plan": [{k: v for k, v in b.items()} for b in tune.plan],

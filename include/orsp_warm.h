@@ -38,6 +38,14 @@ ORSP_API int orsp_warm_conv3d_tc(const void *X, const void *mask, const void *Wt
                                  float *Yf, int32_t D, int32_t H, int32_t W, int32_t Cin, int32_t Cout,
                                  int32_t relu, uintptr_t stream);
 
+/* The weight and bias gradients of orsp_warm_wgrad on the tensor cores
+ * (tcgen05.mma, both operands MN-major, one TMEM accumulator per group of
+ * 128 / Cin taps, partial sums added to dW with fp32 atomics).  Cin, Cout
+ * multiples of 16, at most 64, with ceil(27 Cin / 128) x Cout <= 512
+ * accumulator columns. */
+ORSP_API int orsp_warm_wgrad_tc(const void *X, const void *dY, const void *Yo, float *dW, float *db, int32_t D,
+                                int32_t H, int32_t W, int32_t Cin, int32_t Cout, uintptr_t stream);
+
 /* 1 in *expired if a tensor-core convolution gave up on a wait since the
  * last call (then its output is incomplete), else 0; clears the record.
  * Synchronises with the device. */

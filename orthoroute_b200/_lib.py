@@ -58,6 +58,7 @@ _SIGS = {
     "orsp_warm_conv3d": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _i32, _i32, _i32, _i32, _i32, _i32, _u]),
     "orsp_warm_conv3d_tc": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _i32, _i32, _i32, _i32, _i32, _i32, _u]),
     "orsp_warm_tc_status": (ctypes.c_int, [ctypes.POINTER(_i32)]),
+    "orsp_warm_wgrad_tc": (ctypes.c_int, [_P, _P, _P, _P, _P, _i32, _i32, _i32, _i32, _i32, _u]),
     "orsp_warm_wgrad": (ctypes.c_int, [_P, _P, _P, _P, _P, _i32, _i32, _i32, _i32, _i32, _u]),
     "orsp_warm_pool": (ctypes.c_int, [_P, _P, _i32, _i32, _i32, _i32, _u]),
     "orsp_warm_spread": (ctypes.c_int, [_P, _P, _i32, _i32, _i32, _i32, _f32, _u]),

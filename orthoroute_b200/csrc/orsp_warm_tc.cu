@@ -262,6 +262,175 @@ __global__ void __launch_bounds__(TC_THREADS, 1) conv3d_tc_kernel(
   }
 }
 
+// Instruction descriptor with both operands MN-major (bit 15: A, bit 16: B).
+__host__ __device__ constexpr uint32_t umma_idesc_bf16_mn(int M, int N) {
+  return umma_idesc_bf16(M, N) | (1u << 15) | (1u << 16);
+}
+
+constexpr int WG_K = 32;  // voxels per stage of the weight gradient: two K = 16 MMAs
+
+__host__ __device__ constexpr int wg_taps_per_tile(int Cin) { return 128 / Cin; }
+__host__ __device__ constexpr int wg_mtiles(int Cin) { return (27 + 128 / Cin - 1) / (128 / Cin); }
+__host__ __device__ constexpr size_t wg_smem_bytes(int Cin, int Cout) {
+  return static_cast<size_t>(wg_mtiles(Cin)) * 2 * 4096 + static_cast<size_t>(2) * Cout * 32 + 64;
+}
+__host__ __device__ constexpr uint32_t wg_tmem_cols(int Cin, int Cout) {
+  return wg_mtiles(Cin) * Cout <= 32 ? 32u : wg_mtiles(Cin) * Cout <= 64 ? 64u : wg_mtiles(Cin) * Cout <= 128 ? 128u
+         : wg_mtiles(Cin) * Cout <= 256 ? 256u : 512u;
+}
+
+// Weight gradient dW[tap][ci][co] += sum_v X[v + tap][ci] G[v][co] (G = dY,
+// or dY where Yo > 0) on tcgen05: D[m][n] = sum_k A[m][k] B[n][k] with
+// m = (tap slot, ci), 128 / Cin taps per 128-row M tile (one TMEM
+// accumulator of Cout columns per M tile), n = co, k = voxels, 32 voxels of
+// one (z, y) row per stage.  For a fixed voxel both operands are contiguous
+// along M or N (channels last), so A and B are MN-major: core matrices of 8
+// voxels x 8 channels (16 bytes), K groups 128 bytes apart, 8-channel groups
+// 256 bytes apart.  Persistent CTAs each sum a share of the voxels in TMEM
+// and add their partial sums to dW with fp32 atomics at the end.
+__global__ void __launch_bounds__(TC_THREADS, 1) wgrad_tc_kernel(
+    const __nv_bfloat16 *__restrict__ X, const __nv_bfloat16 *__restrict__ dY, const __nv_bfloat16 *__restrict__ Yo,
+    float *__restrict__ dW, int D, int H, int W, int Cin, int Cout) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int TPM = wg_taps_per_tile(Cin), MT = wg_mtiles(Cin);
+  const int bblk = Cout * 32;
+  unsigned char *sA = sm;                                  // [MT][2 k-steps] blocks of 4096 bytes
+  unsigned char *sB = sm + static_cast<size_t>(MT) * 2 * 4096;  // [2 k-steps] blocks of Cout * 32 bytes
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sB + 2 * bblk);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t ncols = wg_tmem_cols(Cin, Cout);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = umma_idesc_bf16_mn(TC_M, Cout);
+  const uint32_t bar_a = smem_addr(bar);
+  uint32_t phase = 0;
+  bool ok = true, any = false;
+  const int nxc = (W + WG_K - 1) / WG_K;
+  const int64_t nchunks = static_cast<int64_t>(D) * H * nxc;
+  const int cg_in = Cin / 8, cg_out = Cout / 8;
+  for (int64_t t = blockIdx.x; t < nchunks && ok; t += gridDim.x) {
+    const int xc = static_cast<int>(t % nxc);
+    const int64_t zy = t / nxc;
+    const int y = static_cast<int>(zy % H), z = static_cast<int>(zy / H);
+    const int x0 = xc * WG_K;
+    // B: G of the chunk's 32 voxels, 8 output channels per unit
+    for (int i = tid; i < WG_K * cg_out; i += TC_THREADS) {
+      const int k = i % WG_K, g = i / WG_K;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (x0 + k < W) {
+        const int64_t off = ((static_cast<int64_t>(z) * H + y) * W + x0 + k) * Cout + g * 8;
+        v = *reinterpret_cast<const uint4 *>(dY + off);
+        if (Yo) {
+          const uint4 mk = *reinterpret_cast<const uint4 *>(Yo + off);
+          __nv_bfloat16 *pv = reinterpret_cast<__nv_bfloat16 *>(&v);
+          const __nv_bfloat16 *pm = reinterpret_cast<const __nv_bfloat16 *>(&mk);
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            if (!(__bfloat162float(pm[q]) > 0.0f)) pv[q] = __float2bfloat16(0.0f);
+        }
+      }
+      const int ks = k >> 4, kk = k & 15;
+      *reinterpret_cast<uint4 *>(sB + ks * bblk + g * 256 + (kk >> 3) * 128 + (kk & 7) * 16) = v;
+    }
+    // A: the shifted inputs of the taps of every M tile, 8 input channels per unit
+    for (int i = tid; i < MT * TPM * cg_in * WG_K; i += TC_THREADS) {
+      const int k = i % WG_K;
+      int r = i / WG_K;
+      const int cg = r % cg_in;
+      r /= cg_in;
+      const int slot = r % TPM, mt = r / TPM;
+      const int tap = mt * TPM + slot;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (tap < 27 && x0 + k < W) {
+        const int zz = z + tap / 9 - 1, yy = y + (tap / 3) % 3 - 1, xx = x0 + k + tap % 3 - 1;
+        if (zz >= 0 && zz < D && yy >= 0 && yy < H && xx >= 0 && xx < W)
+          v = *reinterpret_cast<const uint4 *>(X + ((static_cast<int64_t>(zz) * H + yy) * W + xx) * Cin + cg * 8);
+      }
+      const int mg = slot * cg_in + cg;  // 8-row group of m = slot * Cin + 8 cg
+      const int ks = k >> 4, kk = k & 15;
+      *reinterpret_cast<uint4 *>(sA + (mt * 2 + ks) * 4096 + mg * 256 + (kk >> 3) * 128 + (kk & 7) * 16) = v;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (tid == 0) {
+      for (int mt = 0; mt < MT; ++mt)
+        for (int ks = 0; ks < 2; ++ks) {
+          const uint64_t a = umma_smem_desc(smem_addr(sA + (mt * 2 + ks) * 4096), 128, 256);
+          const uint64_t b = umma_smem_desc(smem_addr(sB + ks * bblk), 128, 256);
+          mma_bf16(tmem + static_cast<uint32_t>(mt * Cout), a, b, idesc, (any || ks) ? 1u : 0u);
+        }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_a)
+                   : "memory");
+    }
+    ok = __syncthreads_and(mbar_wait(bar_a, phase) ? 1 : 0) != 0;
+    phase ^= 1u;
+    tc_fence_after();
+    any = true;
+  }
+  if (ok && any) {
+    // partial sums: warp w holds rows m = 32w..32w+31 of every M tile
+    const int m = warp * 32 + lane, slot = m / Cin, ci = m % Cin;
+    for (int mt = 0; mt < MT; ++mt) {
+      const int tap = mt * TPM + slot;
+      for (int c0 = 0; c0 < Cout; c0 += 16) {
+        uint32_t r[16];
+        tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(mt * Cout + c0), r);
+        if (tap < 27) {
+          float *dst = dW + (static_cast<int64_t>(tap) * Cin + ci) * Cout + c0;
+#pragma unroll
+          for (int j = 0; j < 16; ++j) atomicAdd(dst + j, __uint_as_float(r[j]));
+        }
+      }
+    }
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(&g_tc_err, 1);
+    mbar_wait(bar_a, phase ^ 1u);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+  }
+}
+
+// db[co] += sum_v G[v][co] (G = dY, or dY where Yo > 0): one block per
+// chunk of voxels, per-thread channel sums, one atomic per channel and block.
+__global__ void bias_sum_kernel(const __nv_bfloat16 *__restrict__ dY, const __nv_bfloat16 *__restrict__ Yo,
+                                float *__restrict__ db, int64_t nvox, int Cout) {
+  extern __shared__ float s_db[];
+  for (int c = threadIdx.x; c < Cout; c += blockDim.x) s_db[c] = 0.0f;
+  __syncthreads();
+  const int per = blockDim.x / Cout;  // voxels in flight per block step
+  const int co = threadIdx.x % Cout, lane_v = threadIdx.x / Cout;
+  float acc = 0.0f;
+  if (lane_v < per)
+    for (int64_t v = static_cast<int64_t>(blockIdx.x) * per + lane_v; v < nvox; v += static_cast<int64_t>(gridDim.x) * per) {
+      const int64_t o = v * Cout + co;
+      const float g = __bfloat162float(dY[o]);
+      acc += (!Yo || __bfloat162float(Yo[o]) > 0.0f) ? g : 0.0f;
+    }
+  if (lane_v < per) atomicAdd(&s_db[co], acc);
+  __syncthreads();
+  for (int c = threadIdx.x; c < Cout; c += blockDim.x) atomicAdd(&db[c], s_db[c]);
+}
+
 }  // namespace
 
 using namespace orsp;
@@ -298,5 +467,34 @@ extern "C" int orsp_warm_tc_status(int32_t *expired) {
   ORSP_CUDA(cudaMemcpyFromSymbol(&v, g_tc_err, sizeof(int)));
   ORSP_CUDA(cudaMemcpyToSymbol(g_tc_err, &zero, sizeof(int)));
   *expired = v;
+  return ORSP_OK;
+}
+
+extern "C" int orsp_warm_wgrad_tc(const void *X, const void *dY, const void *Yo, float *dW, float *db, int32_t D,
+                                  int32_t H, int32_t W, int32_t Cin, int32_t Cout, uintptr_t stream) {
+  if (!X || !dY || !dW || D <= 0 || H <= 0 || W <= 0 || Cin <= 0 || Cin % 16 || Cin > 64 || Cout <= 0 ||
+      Cout % 16 || Cout > 64 || wg_mtiles(Cin) * Cout > 512) {
+    set_error("warm_wgrad_tc: bad arguments (Cin, Cout multiples of 16, at most 64, accumulators within TMEM)");
+    return ORSP_ERR_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t smem = wg_smem_bytes(Cin, Cout);
+  int dev = 0, sms = 0;
+  ORSP_CUDA(cudaGetDevice(&dev));
+  ORSP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  ORSP_CUDA(cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int64_t nchunks = static_cast<int64_t>(D) * H * ((W + WG_K - 1) / WG_K);
+  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(nchunks, sms)));
+  wgrad_tc_kernel<<<grid, TC_THREADS, smem, st>>>((const __nv_bfloat16 *)X, (const __nv_bfloat16 *)dY,
+                                                  (const __nv_bfloat16 *)Yo, dW, D, H, W, Cin, Cout);
+  ORSP_CUDA(cudaGetLastError());
+  if (db) {
+    const int64_t nvox = static_cast<int64_t>(D) * H * W;
+    const int threads = (256 / Cout) * Cout;
+    const int blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((nvox + 255) / 256, sms * 8)));
+    bias_sum_kernel<<<blocks, threads, Cout * sizeof(float), st>>>((const __nv_bfloat16 *)dY,
+                                                                   (const __nv_bfloat16 *)Yo, db, nvox, Cout);
+    ORSP_CUDA(cudaGetLastError());
+  }
   return ORSP_OK;
 }

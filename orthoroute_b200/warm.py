@@ -276,8 +276,9 @@ class WarmNet:
         l = next(z for z in self.layers if z.name == name)
         lib = _lib.load()
         mask = y_out if l.relu else None
-        check(lib.orsp_warm_wgrad(ptr(x_in), ptr(dy), ptr(mask), ptr(self.gw[name]), ptr(self.gb[name]), D, H, W,
-                                  l.cin, l.cout, _st()), "orsp_warm_wgrad")
+        wgrad = lib.orsp_warm_wgrad_tc if self.conv_impl == "tc" else lib.orsp_warm_wgrad
+        check(wgrad(ptr(x_in), ptr(dy), ptr(mask), ptr(self.gw[name]), ptr(self.gb[name]), D, H, W, l.cin, l.cout,
+                    _st()), "orsp_warm_wgrad")
         if not need_dx:
             return None
         wt = self._pack(name, True)

@@ -88,3 +88,56 @@ def test_warm_forward_tc_equals_wmma():
     b = net.forward(x).float().cpu()
     assert _status() == 0
     assert _rel(b, a) < 1e-2
+
+
+@pytest.mark.parametrize("cin,cout,masked,W", [(16, 32, True, 70), (32, 32, False, 41), (32, 16, True, 96)])
+def test_wgrad_tc_matches_wmma(cin, cout, masked, W):
+    """orsp_warm_wgrad_tc against orsp_warm_wgrad: the same bf16 products
+    summed in fp32 in another order (relative L2 error 1e-4), weights and
+    biases, accumulated into existing values."""
+    from orthoroute_b200 import _lib
+    from orthoroute_b200._lib import ptr
+
+    D, H = 3, 6
+    g = torch.Generator().manual_seed(11 + cin + cout + W)
+    x = torch.randn(D, H, W, cin, generator=g).cuda().to(torch.bfloat16)
+    dy = torch.randn(D, H, W, cout, generator=g).cuda().to(torch.bfloat16)
+    yo = torch.randn(D, H, W, cout, generator=g).cuda().to(torch.bfloat16) if masked else None
+    lib = _lib.load()
+    base_w = torch.randn(27 * cin * cout, generator=g).cuda()
+    base_b = torch.randn(cout, generator=g).cuda()
+    dw_tc, db_tc = base_w.clone(), base_b.clone()
+    dw_mm, db_mm = base_w.clone(), base_b.clone()
+    assert lib.orsp_warm_wgrad_tc(ptr(x), ptr(dy), ptr(yo), ptr(dw_tc), ptr(db_tc), D, H, W, cin, cout, 0) == 0, \
+        lib.orsp_last_error()
+    assert lib.orsp_warm_wgrad(ptr(x), ptr(dy), ptr(yo), ptr(dw_mm), ptr(db_mm), D, H, W, cin, cout, 0) == 0
+    torch.cuda.synchronize()
+    assert _status() == 0
+    assert _rel((dw_tc - base_w).cpu(), (dw_mm - base_w).cpu()) < 1e-4
+    assert _rel((db_tc - base_b).cpu(), (db_mm - base_b).cpu()) < 1e-4
+
+
+def test_warm_gradients_tc_match_oracle():
+    """A forward and backward pass of the whole network on the tensor-core
+    kernels against the fp32 oracle's gradients (1e-1, as the WMMA path)."""
+    from orthoroute_b200.warm import WarmNet
+
+    net = WarmNet(C=32, seed=3)
+    net.conv_impl = "tc"
+    g = torch.Generator().manual_seed(4)
+    for k in net.w:
+        net.b[k].copy_(torch.randn(net.b[k].shape, generator=g) * 0.05)
+    D, H, W = 3, 32, 40
+    x = _bf(torch.rand(D, H, W, 16, generator=g))
+    t = torch.rand(D, H, W, 2, generator=g)
+    params = {k: (_bf(net.w[k].cpu()), net.b[k].cpu()) for k in net.w}
+    out, act = net.forward(x.cuda().to(torch.bfloat16), keep=True)
+    loss, dout = net.loss_grad(out, t.cuda().contiguous())
+    net.backward(act, dout)
+    torch.cuda.synchronize()
+    assert _status() == 0
+    ref_loss, ref_g = R.grads(params, x, t)
+    assert abs(float(loss) - float(ref_loss)) < 5e-2 * float(ref_loss)
+    err = {k: (round(_rel(net.gw[k].cpu(), ref_g[k][0]), 4), round(_rel(net.gb[k].cpu(), ref_g[k][1]), 4))
+           for k in net.w}
+    assert max(max(v) for v in err.values()) < 1e-1, err
