@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstdlib>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -1162,9 +1163,30 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   }
   else kfn = priv ? (void *)lattice_tile_kernel<TX, TY, true> : (void *)lattice_tile_kernel<TX, TY, false>;
   const int threads = TX * TY + (spec ? 32 : 0);
-  ORSP_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int occ = 0;
-  ORSP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, threads, smem));
+  // the attribute and the occupancy per (kernel, block, shared memory) and
+  // device: set and queried once, not on every search
+  struct OccEntry {
+    void *fn;
+    int threads, device;
+    size_t smem;
+    int occ;
+  };
+  static OccEntry occ_cache[32];
+  static int occ_n = 0;
+  static std::mutex occ_mu;
+  int occ = -1;
+  {
+    std::lock_guard<std::mutex> lock(occ_mu);
+    for (int i = 0; i < occ_n; ++i)
+      if (occ_cache[i].fn == kfn && occ_cache[i].threads == threads && occ_cache[i].smem == smem &&
+          occ_cache[i].device == g->device)
+        occ = occ_cache[i].occ;
+    if (occ < 0) {
+      ORSP_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      ORSP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, threads, smem));
+      if (occ_n < 32) occ_cache[occ_n++] = OccEntry{kfn, threads, g->device, smem, occ};
+    }
+  }
   if (occ < 1) {
     orsp::set_error("lattice search: kernel does not fit on an SM");
     return ORSP_ERR_ARG;
