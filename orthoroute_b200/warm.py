@@ -57,8 +57,14 @@ def _box_blur(a: np.ndarray, r: int) -> np.ndarray:
     return (s / n).astype(np.float32)
 
 
-def board_features(lat: Lattice, src: np.ndarray, dst: np.ndarray) -> np.ndarray:
-    """float32 [nz][ny][nx][16] input features of a board (host)."""
+FEATURES = 2  # feature set of newly built networks (see board_features)
+
+
+def board_features(lat: Lattice, src: np.ndarray, dst: np.ndarray, version: int = FEATURES) -> np.ndarray:
+    """float32 [nz][ny][nx][16] input features of a board (host).  Channels:
+    0 pins on the pin layer, 1 blurred pin density, 2 airwire crossing density,
+    3 bounding-box coverage, 4 / 5 H / V layer, 6 layer position; version 2
+    adds 7, log1p of the RUDY wire density (rudy_density)."""
     nx, ny, nz = lat.nx, lat.ny, lat.nz
     sx, sy, sz = (np.asarray(v) for v in lat.coords(np.asarray(src)))
     dx, dy, dz = (np.asarray(v) for v in lat.coords(np.asarray(dst)))
@@ -91,6 +97,8 @@ def board_features(lat: Lattice, src: np.ndarray, dst: np.ndarray) -> np.ndarray
         f[z, :, :, 4] = 1.0 if "h" in d else 0.0
         f[z, :, :, 5] = 1.0 if "v" in d else 0.0
         f[z, :, :, 6] = z / max(1, nz - 1)
+    if version >= 2:
+        f[:, :, :, 7] = np.log1p(rudy_density(lat, src, dst)).astype(np.float32)[None]
     return f
 
 
@@ -121,13 +129,10 @@ def history_from_prediction(lat: Lattice, pred: np.ndarray, scale: float = 1.0) 
     return (p[lat.edge_src(), kind] * scale).astype(np.float32)
 
 
-def rudy_prediction(lat: Lattice, src: np.ndarray, dst: np.ndarray) -> np.ndarray:
-    """A non-learned congestion prior in the network's output format
-    ([nz][ny][nx][2], log1p domain): RUDY, each net's half-perimeter wire
-    length (w + h) spread uniformly over its bounding box (w x h cells), summed
-    over nets, per cell in x/y and the same on every layer and edge kind.
-    It is the baseline the learned prediction is compared with: the same
-    history mapping and scale search apply to both."""
+def rudy_density(lat: Lattice, src: np.ndarray, dst: np.ndarray) -> np.ndarray:
+    """RUDY wire density per cell and routing layer, float64 [ny][nx]: each
+    net's half-perimeter wire length (w + h) spread uniformly over its bounding
+    box (w x h cells), summed over nets, divided by the layer count."""
     nx, ny, nz = lat.nx, lat.ny, lat.nz
     sx, sy, _ = (np.asarray(v).astype(np.int64) for v in lat.coords(np.asarray(src)))
     dx, dy, _ = (np.asarray(v).astype(np.int64) for v in lat.coords(np.asarray(dst)))
@@ -141,9 +146,17 @@ def rudy_prediction(lat: Lattice, src: np.ndarray, dst: np.ndarray) -> np.ndarra
     np.add.at(acc, (y0, x1), -dens)
     np.add.at(acc, (y1, x0), -dens)
     np.add.at(acc, (y1, x1), dens)
-    rudy = acc.cumsum(0).cumsum(1)[:ny, :nx] / nz  # wire per routing layer and cell
-    p = np.log1p(np.maximum(rudy, 0.0)).astype(np.float32)
-    out = np.empty((nz, ny, nx, 2), np.float32)
+    return np.maximum(acc.cumsum(0).cumsum(1)[:ny, :nx] / nz, 0.0)
+
+
+def rudy_prediction(lat: Lattice, src: np.ndarray, dst: np.ndarray) -> np.ndarray:
+    """A non-learned congestion prior in the network's output format
+    ([nz][ny][nx][2], log1p domain): log1p of the RUDY density
+    (rudy_density), the same on every layer and edge kind.  It is the
+    baseline the learned prediction is compared with: the same history
+    mapping and scale search apply to both."""
+    p = np.log1p(rudy_density(lat, src, dst)).astype(np.float32)
+    out = np.empty((lat.nz, lat.ny, lat.nx, 2), np.float32)
     out[:] = p[None, :, :, None]
     return out
 
@@ -189,6 +202,7 @@ class WarmNet:
         # orsp_warm_conv3d_tc) or "wmma" (orsp_warm_conv3d); ORSP_WARM_CONV
         # overrides the default
         self.conv_impl = os.environ.get("ORSP_WARM_CONV", "wmma")
+        self.features = FEATURES  # input feature set (board_features version)
 
     def _conv_call(self, *args):
         lib = _lib.load()
@@ -364,6 +378,7 @@ def load_pretrained(path=None, device=None) -> Tuple["WarmNet", float]:
     st = dict(np.load(path or DEFAULT_WEIGHTS))
     net = WarmNet(C=32, device=device)
     net.load_state({k: v.astype(np.float32) for k, v in st.items() if k.startswith(("w_", "b_"))})
+    net.features = int(st.get("features", 1))  # files written before version 2 carry no version
     return net, float(st.get("scale", 1.0))
 
 
@@ -376,7 +391,7 @@ def pretrained_rudy_scale(path=None) -> Optional[float]:
 
 def warm_history(net: "WarmNet", lat: Lattice, src, dst, scale: float) -> np.ndarray:
     """Initial per-edge history for a board: features -> net -> edges."""
-    pred = net.predict(board_features(lat, np.asarray(src), np.asarray(dst)))
+    pred = net.predict(board_features(lat, np.asarray(src), np.asarray(dst), net.features))
     return history_from_prediction(lat, pred, scale)
 
 
@@ -401,9 +416,9 @@ def _main(argv=None):
     nets = int(round(8000 / (600 * 600) * a.size * a.size))
     b = board_footprints(a.size, a.size, a.nz, nets, None, seed=a.seed)
     t0 = time.perf_counter()
-    feats = board_features(b.lattice, b.src, b.dst)
-    t_feat = time.perf_counter() - t0
     net, scale = load_pretrained()
+    feats = board_features(b.lattice, b.src, b.dst, net.features)
+    t_feat = time.perf_counter() - t0
     x = torch.from_numpy(feats).cuda().to(torch.bfloat16)
     net.forward(x)  # warm-up
     torch.cuda.synchronize()

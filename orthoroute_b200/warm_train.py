@@ -118,7 +118,7 @@ def warm_route(net, board, scale: float, mode: str = "batched", device=None, max
     if isinstance(net, str):
         pred = rudy_prediction(board.lattice, board.src, board.dst)
     else:
-        pred = net.predict(board_features(board.lattice, board.src, board.dst))
+        pred = net.predict(board_features(board.lattice, board.src, board.dst, net.features))
     h0 = history_from_prediction(board.lattice, pred, scale)
     torch.cuda.synchronize()
     t_pred = time.perf_counter() - t0
@@ -200,6 +200,7 @@ def main(argv: Optional[List[str]] = None):
         rudy = choose_scale("rudy", ssize, args.nz, sseeds, tuple(float(v) for v in args.rudy_scales.split(",")))
     st = net.state()
     st["scale"] = np.float32(sc["scale"])
+    st["features"] = np.int32(net.features)
     if rudy is not None:
         st["rudy_scale"] = np.float32(rudy["scale"])
     Path(args.out).parent.mkdir(parents=True, exist_ok=True)

@@ -13,7 +13,10 @@ def test_features_targets_and_history_mapping():
     assert f.shape == (6, 64, 64, 16) and f.dtype == np.float32
     assert f[0, :, :, 0].sum() == 2 * len(b.src)  # every pin once, on the pin layer
     assert f[1:, :, :, 0].sum() == 0
-    assert (f[..., 7:] == 0).all()
+    assert (f[..., 8:] == 0).all()
+    # channel 7 (feature set 2): log1p of the RUDY density, the same on every layer
+    assert f[..., 7].max() > 0 and np.array_equal(f[0, :, :, 7], f[-1, :, :, 7])
+    assert (board_features(lat, b.src, b.dst, version=1)[..., 7:] == 0).all()
     assert f[..., 4].sum() > 0 and f[..., 5].sum() > 0
     rng = np.random.default_rng(0)
     hist = np.zeros(lat.E, np.float32)
