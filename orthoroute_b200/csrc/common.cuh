@@ -190,6 +190,12 @@ int finish_lattice_search(Graph *g, int32_t *rounds_h);
 int run_lattice_roi(Graph *g, const float *cost_d, int32_t nseeds, const int32_t *seeds_d,
                     const float *seed_cost_d, const int32_t *roi_map_d, const int32_t *roi_nodes_d,
                     int64_t n_roi, const uint8_t *sink_d, uint32_t *dist, cudaStream_t st);
+// One search over a node-list ROI whose global_to_roi map is roi_map_d (ROI
+// index = rank, -1 outside), by one CTA of the batch kernel; *len_h gets the
+// batch kernel's path_len (nodes, 0 = no path, < 0 a per-search status).
+int run_roi_nodes_cta(Graph *g, const float *cost_d, const int32_t *src_d, const int32_t *dst_d,
+                      const int32_t *roi_map_d, const int32_t *roi_nodes_d, int64_t n_roi, int32_t *path_out_d,
+                      int32_t path_cap, int32_t *path_len_d, cudaStream_t st, int32_t *len_h);
 // The ROI map and sink mask of orsp_sssp_roi_nodes / orsp_sssp_multi (lazily
 // allocated, -1 / 0 everywhere).
 int ensure_roi_arrays(Graph *g);

@@ -42,7 +42,11 @@ struct BatchParams {
   FastDiv div_nx, div_plane;
   int32_t K;
   const int32_t *src, *dst, *bbox, *order;
-  int range_mode;  // bbox holds [lo, hi) node ranges (2 per search) instead of boxes
+  int range_mode;  // 1: bbox holds [lo, hi) node ranges (2 per search) instead of boxes;
+                   // 2: one node-set ROI, ids through roi_map / roi_nodes
+  const int32_t *roi_map;    // mode 2: global_to_roi (-1 outside)
+  const int32_t *roi_nodes;  // mode 2: the ROI's nodes by ROI index
+  int32_t n_roi;
   int32_t *path_nodes, *path_edges, *path_len;
   int32_t path_cap;
   char *ws;
@@ -59,16 +63,25 @@ struct BatchParams {
 // A search's ROI: an inclusive lattice box (local id = row-major position in
 // the box), or a node-id range [lo, lo+V) of a graph made of concatenated
 // ROI-local CSRs (local id = node - lo).  Both orders follow the global id.
+// Or (mapped) a node-set ROI: local id = global_to_roi[node], the ROI index,
+// which is also the reference's rank.
 struct Box {
   int32_t x0, y0, z0, W, H, D;
   FastDiv dw, dwh;
   int32_t V;
   int32_t lo;    // range mode: first node
   bool range;
+  bool mapped;
 };
 
 __device__ __forceinline__ bool box_local(const BatchParams &p, const Box &b, int32_t gid,
                                           int32_t *lid) {
+  if (b.mapped) {
+    const int32_t l = __ldg(&p.roi_map[gid]);
+    if (l < 0) return false;
+    *lid = l;
+    return true;
+  }
   if (b.range) {
     if (gid < b.lo || gid - b.lo >= b.V) return false;
     *lid = gid - b.lo;
@@ -85,6 +98,7 @@ __device__ __forceinline__ bool box_local(const BatchParams &p, const Box &b, in
 }
 
 __device__ __forceinline__ int32_t box_global(const BatchParams &p, const Box &b, int32_t lid) {
+  if (b.mapped) return __ldg(&p.roi_nodes[lid]);
   if (b.range) return b.lo + lid;
   const uint32_t lz = b.dwh.div((uint32_t)lid);
   const uint32_t r = (uint32_t)lid - lz * (uint32_t)(b.W * b.H);
@@ -317,7 +331,18 @@ __global__ void __launch_bounds__(BATCH_THREADS) batch_bbox_kernel(BatchParams p
     if (it >= p.K) break;
     const int k = p.order ? p.order[it] : it;
     Box b;
-    if (p.range_mode) {
+    b.mapped = false;
+    if (p.range_mode == 2) {
+      b.mapped = true;
+      b.range = false;
+      b.lo = 0;
+      b.V = p.n_roi;
+      b.x0 = b.y0 = b.z0 = 0;
+      b.W = b.V;
+      b.H = b.D = 1;
+      b.dw.init(1u);
+      b.dwh.init(1u);
+    } else if (p.range_mode) {
       const int32_t *rg = p.bbox + 2 * (int64_t)k;
       b.range = true;
       b.lo = rg[0];
@@ -490,7 +515,8 @@ int grow_dev(void **p, size_t *have, size_t need) {
 int run_batch_cta(orsp_graph *g, const float *cost_d, int32_t K, const std::vector<int32_t> &items, const int32_t *src_d,
                   const int32_t *dst_d, const int32_t *bbox_d, const std::vector<int32_t> &bb, int range_mode,
                   float delta, const std::vector<float> &delta_k, int ctas_per_sm, int32_t *path_nodes_d,
-                  int32_t *path_edges_d, int32_t path_cap, int32_t *path_len_d, cudaStream_t st) {
+                  int32_t *path_edges_d, int32_t path_cap, int32_t *path_len_d, cudaStream_t st,
+                  const int32_t *roi_map_d = nullptr, const int32_t *roi_nodes_d = nullptr) {
   const int32_t n = (int32_t)items.size();
   if (n == 0) return ORSP_OK;
   const int per = range_mode ? 2 : 6;
@@ -532,6 +558,9 @@ int run_batch_cta(orsp_graph *g, const float *cost_d, int32_t K, const std::vect
   p.dst = dst_d;
   p.bbox = bbox_d;
   p.range_mode = range_mode;
+  p.roi_map = roi_map_d;
+  p.roi_nodes = roi_nodes_d;
+  p.n_roi = range_mode == 2 ? bb[1] - bb[0] : 0;
   p.path_nodes = path_nodes_d;
   p.path_edges = path_edges_d;
   p.path_len = path_len_d;
@@ -862,3 +891,22 @@ extern "C" int orsp_sssp_batch_ranges(orsp_graph *g, const float *cost_d, int32_
   return run_batch(g, cost_d, K, src_d, dst_d, ranges_d, 1, order_d, delta, path_nodes_d, path_edges_d,
                    path_cap, path_len_d, stream);
 }
+
+namespace orsp {
+
+int run_roi_nodes_cta(Graph *gr, const float *cost_d, const int32_t *src_d, const int32_t *dst_d,
+                      const int32_t *roi_map_d, const int32_t *roi_nodes_d, int64_t n_roi, int32_t *path_out_d,
+                      int32_t path_cap, int32_t *path_len_d, cudaStream_t st, int32_t *len_h) {
+  if (n_roi >= INT32_MAX) { set_error("sssp_roi_nodes: ROI too large"); return ORSP_ERR_ARG; }
+  orsp_graph *g = static_cast<orsp_graph *>(gr);
+  const std::vector<int32_t> items{0}, bb{0, (int32_t)n_roi};
+  const std::vector<float> no_dk;
+  int rc = run_batch_cta(g, cost_d, 1, items, src_d, dst_d, nullptr, bb, 2, 0.0f, no_dk, 1, path_out_d, nullptr,
+                         path_cap, path_len_d, st, roi_map_d, roi_nodes_d);
+  if (rc) return rc;
+  ORSP_CUDA(cudaMemcpyAsync(len_h, path_len_d, 4, cudaMemcpyDeviceToHost, st));
+  ORSP_CUDA(cudaStreamSynchronize(st));
+  return ORSP_OK;
+}
+
+}  // namespace orsp

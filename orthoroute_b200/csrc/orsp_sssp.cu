@@ -766,6 +766,18 @@ static bool use_lattice_roi(const orsp_graph *g) {
   return g->lattice_ok && lattice_tile_fits(g->nz) && !(impl && std::string(impl) == "generic");
 }
 
+// Node-list ROIs off the tile lattice: the one-CTA search (block-local
+// rounds, no grid barrier) up to ORSP_ROI_CTA_MAX nodes (default 1 << 20),
+// else the grid search.  ORSP_ROI_NODES_IMPL=grid|cta forces one.
+static bool use_roi_cta(int64_t n_roi) {
+  const char *impl = getenv("ORSP_ROI_NODES_IMPL");
+  if (impl && std::string(impl) == "grid") return false;
+  if (impl && std::string(impl) == "cta") return true;
+  const char *m = getenv("ORSP_ROI_CTA_MAX");
+  const int64_t lim = (m && *m) ? atoll(m) : (int64_t)1 << 20;
+  return n_roi <= lim;
+}
+
 extern "C" int orsp_sssp_roi_nodes(orsp_graph *g, const float *cost_d, int32_t src, int32_t dst,
                                    const int32_t *roi_nodes_d, int64_t n_roi, int32_t *path_out_d,
                                    int32_t path_cap, int32_t *path_len_h, uintptr_t stream) {
@@ -801,6 +813,27 @@ extern "C" int orsp_sssp_roi_nodes(orsp_graph *g, const float *cost_d, int32_t s
                                        path_cap);
     lat_backtrace_kernel<<<1, 32, 0, st>>>(b);
     ORSP_CUDA(cudaGetLastError());
+  } else if (use_roi_cta(n_roi)) {
+    // one CTA: block-local near-far rounds over ROI-local distances
+    put_i32_kernel<<<1, 1, 0, st>>>(g->seed_one + 1, dst);
+    ORSP_CUDA(cudaGetLastError());
+    int32_t len = 0;
+    rc = run_roi_nodes_cta(g, cost_d, g->seed_one, g->seed_one + 1, g->roi_map, roi_nodes_d, n_roi, path_out_d,
+                           path_cap, g->seed_one + 2, st, &len);
+    if (rc) return fail(rc);
+    roi_scatter_kernel<<<sblocks, 256, 0, st>>>(roi_nodes_d, n_roi, g->N, g->roi_map, 1);
+    ORSP_CUDA(cudaGetLastError());
+    ORSP_CUDA(cudaStreamSynchronize(st));
+    switch (len) {
+      case -1: case 0: case 1: return ORSP_NO_PATH;  // endpoint outside the ROI, unreachable, src == dst
+      case -2: set_error("sssp_roi_nodes: work queue overflow"); return ORSP_ERR_OVERFLOW;
+      case -3: set_error("sssp_roi_nodes: path longer than path_cap"); return ORSP_ERR_OVERFLOW;
+      case -4: set_error("sssp_roi_nodes: round or time limit reached"); return ORSP_ERR_TIMEOUT;
+      default: break;
+    }
+    if (len < 0) { set_error("sssp_roi_nodes: no predecessor on the shortest-path tree"); return ORSP_ERR_INTERNAL; }
+    *path_len_h = len;
+    return ORSP_OK;
   } else {
     rc = run_grid_search(g, cost_d, 1, g->seed_one, nullptr, dst, g->roi_map, nullptr, 0.0f, g->dist, st);
     if (rc) return fail(rc);

@@ -85,6 +85,40 @@ def test_roi_node_list_searches_match_oracle():
             assert got2 == got, (nx, ny, nz, case)
 
 
+@pytest.mark.parametrize("impl", ["cta", "grid"])
+def test_roi_node_list_off_lattice_matches_oracle(impl, monkeypatch):
+    """orsp_sssp_roi_nodes on a graph that is not a tile lattice (the
+    reference's own Lattice3D shape: inner-layer planar edges, full via
+    stacks with duplicate via edges, no lattice geometry given): the one-CTA
+    search (ROI-local distances through global_to_roi) and the grid search
+    against the oracle, with repeated ROI nodes, ties and endpoints outside
+    the ROI."""
+    monkeypatch.setenv("ORSP_ROI_NODES_IMPL", impl)
+    rng = np.random.default_rng(57)
+    for nx, ny, nz in ((50, 40, 6), (31, 67, 4)):
+        lat = build_lattice(nx, ny, nz, planar="inner", vias="full", duplicate_vias=True)
+        dg = DeviceGraph(lat.indptr, lat.indices)
+        assert not dg.is_lattice
+        for case in range(16):
+            w = uniform_weights(lat, seed=100 + case, blocked_frac=float(rng.choice([0.0, 0.1])))
+            if case % 3 == 0:
+                w = np.where(np.isfinite(w), np.floor(w * 2), w).astype(np.float32)
+            s, d = (int(v) for v in rng.choice(lat.N, size=2, replace=False))
+            roi, _ = O.roi_bfs(lat.indptr, lat.indices, s, d, int(rng.integers(2, 50)),
+                               int(rng.choice([50_000, 2500, 300])))
+            roi = roi.astype(np.int32)
+            if case % 4 == 1:
+                roi = np.concatenate([roi, rng.choice(lat.N, size=7).astype(np.int32), roi[:2]])
+            if case % 5 == 2:
+                roi = roi[roi != s]
+            g2r = np.full(lat.N, -1, np.int32)
+            g2r[roi] = np.arange(len(roi), dtype=np.int32)
+            ref, *_ = O.dijkstra(lat.indptr, lat.indices, w, [s], dst=d, roi_map=g2r)
+            st, path = dg.sssp_roi_nodes(torch.from_numpy(w).cuda(), s, d, torch.from_numpy(roi).cuda())
+            got = path.cpu().tolist() if st == _lib.ORSP_OK else None
+            assert got == (ref.tolist() if len(ref) > 1 else None), (nx, ny, nz, case, st)
+
+
 def test_roi_map_distances_bit_exact_and_generic_agrees(monkeypatch):
     """Distances of a ROI search (tile sweeps) are the oracle's bit for bit
     inside the ROI and +inf outside; the generic near-far search gives the
