@@ -142,6 +142,20 @@ ORSP_API int orsp_sssp(orsp_graph *g, const float *cost_d, int32_t nseeds,
               int32_t *path_out_d, int32_t path_cap, int32_t *path_len_h,
               int32_t *rounds_h, uintptr_t stream);
 
+/* nsrc whole-graph single-source searches (no target): row i of
+ * dist_out_d (fp32[nsrc][N], device) receives the distances from src_h[i]
+ * (host), bit for bit those of orsp_sssp with that source.  On a recognised
+ * lattice up to per_launch sources (0: all) share one persistent launch, each
+ * a whole-lattice box with its own distance row, so the tile queue
+ * interleaves their wavefronts and the launch is bound by tile visits rather
+ * than by one wave's hop latency.  Other graphs run orsp_sssp per source.
+ * The batched counterpart of SimpleDijkstra.find_path_roi over the full
+ * graph (UPF:1801-1887) for many sources, as CUDADijkstra.find_paths_on_rois
+ * (CD:2014-2086) batches ROI searches.  A cost-generation declaration covers
+ * the whole call. */
+ORSP_API int orsp_sssp_sources(orsp_graph *g, const float *cost_d, int32_t nsrc, const int32_t *src_h,
+                               float *dist_out_d, int32_t per_launch, uintptr_t stream);
+
 /* One search from src to dst over the ROI given as its node list (the
  * roi_nodes array SimpleDijkstra.find_path_roi, UPF:1801-1887, and
  * CUDADijkstra.find_path_roi_gpu, CD:4909-4996, take, int32[n_roi], device):

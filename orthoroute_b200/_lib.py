@@ -53,6 +53,7 @@ _SIGS = {
                                  ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
     "orsp_sssp_box": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _f32, _P, _P, _i32,
                                      ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
+    "orsp_sssp_sources": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _u]),
     "orsp_sssp_roi_nodes": (ctypes.c_int, [_P, _P, _i32, _i32, _P, _i64, _P, _i32, ctypes.POINTER(_i32), _u]),
     "orsp_batch_set_plan": (ctypes.c_int, [_P, _i32, _P, _P, _P, _P, _P]),
     "orsp_warm_conv3d": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _i32, _i32, _i32, _i32, _i32, _i32, _u]),

@@ -910,3 +910,89 @@ int run_roi_nodes_cta(Graph *gr, const float *cost_d, const int32_t *src_d, cons
 }
 
 }  // namespace orsp
+
+// Many whole-graph single-source searches.  On a recognised lattice, up to
+// per_launch sources share one persistent launch: each source is a box
+// covering the whole lattice with its own distance slice, and the slices are
+// the caller's output rows, so the tile queue interleaves the wavefronts of
+// all of them.  Elsewhere one grid search per source.
+extern "C" int orsp_sssp_sources(orsp_graph *g, const float *cost_d, int32_t nsrc, const int32_t *src_h,
+                                 float *dist_out_d, int32_t per_launch, uintptr_t stream) {
+  if (!g || !cost_d || nsrc < 0 || (nsrc > 0 && (!src_h || !dist_out_d)) || per_launch < 0) {
+    set_error("sssp_sources: NULL argument or negative count");
+    return ORSP_ERR_ARG;
+  }
+  for (int32_t i = 0; i < nsrc; ++i)
+    if (src_h[i] < 0 || src_h[i] >= g->N) { set_error("sssp_sources: source out of range"); return ORSP_ERR_ARG; }
+  if (nsrc == 0) return ORSP_OK;
+  ORSP_CUDA(cudaSetDevice(g->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const char *impl = getenv("ORSP_SSSP_IMPL");
+  const bool lattice = g->lattice_ok && lattice_tile_fits(g->nz) && !(impl && std::string(impl) == "generic");
+  if (!lattice) {
+    for (int32_t i = 0; i < nsrc; ++i) {
+      int rc = grow_dev((void **)&g->batch_idx, &g->batch_idx_bytes, 256);
+      if (rc) return rc;
+      ORSP_CUDA(cudaMemcpyAsync(g->batch_idx, &src_h[i], 4, cudaMemcpyHostToDevice, st));
+      int32_t len = 0;
+      rc = orsp_sssp(g, cost_d, 1, g->batch_idx, nullptr, -1, nullptr, 0.0f, dist_out_d + (int64_t)i * g->N,
+                     nullptr, 0, &len, nullptr, stream);
+      if (rc != ORSP_OK && rc != ORSP_NO_PATH) return rc;
+    }
+    return ORSP_OK;
+  }
+  const int32_t per = per_launch > 0 ? std::min(per_launch, nsrc) : nsrc;
+  const int32_t full[6] = {0, g->nx - 1, 0, g->ny - 1, 0, g->nz - 1};
+  std::vector<int32_t> boxes((size_t)per * 6);
+  for (int32_t j = 0; j < per; ++j)
+    for (int c = 0; c < 6; ++c) boxes[(size_t)j * 6 + c] = full[c];
+  const size_t tab = (size_t)per * sizeof(LatBox) + (size_t)per * 4 + 256;
+  if (g->blat_tab_bytes < tab) {
+    cudaFree(g->blat_tab_d);
+    if (g->blat_tab_h) cudaFreeHost(g->blat_tab_h);
+    g->blat_tab_d = nullptr;
+    g->blat_tab_h = nullptr;
+    g->blat_tab_bytes = 0;
+    ORSP_CUDA(cudaMalloc(&g->blat_tab_d, tab));
+    ORSP_CUDA(cudaMallocHost(&g->blat_tab_h, tab));
+    g->blat_tab_bytes = tab;
+  }
+  const uint64_t decl = g->decl_cost == cost_d ? g->decl_gen : 0;
+  for (int32_t a = 0; a < nsrc; a += per) {
+    const int32_t m = std::min(per, nsrc - a);
+    LatBox *hb = (LatBox *)g->blat_tab_h;
+    int32_t *h_src = (int32_t *)(hb + m);
+    // the staging buffer is reused: the previous chunk was synchronised
+    const int64_t ntiles = make_lat_boxes(boxes.data(), m, hb);
+    for (int32_t j = 0; j < m; ++j) {
+      hb[j].dbase = (int64_t)j * g->N;
+      h_src[j] = src_h[a + j];
+    }
+    ORSP_CUDA(cudaMemcpyAsync(g->blat_tab_d, g->blat_tab_h, (size_t)m * sizeof(LatBox) + (size_t)m * 4,
+                              cudaMemcpyHostToDevice, st));
+    const LatBox *db = (const LatBox *)g->blat_tab_d;
+    const int32_t *d_src = (const int32_t *)(db + m);
+    int rc = reserve_lattice_ws(g, ntiles);
+    if (rc) return rc;
+    LatOptions opt;
+    opt.private_dist = true;
+    opt.private_count = (int64_t)m * g->N;
+    // every chunk after the first reuses the gathered weights of this call
+    if (decl) g->decl_cost = cost_d, g->decl_gen = decl;
+    else if (a > 0) g->decl_cost = cost_d, g->decl_gen = ~0ull;
+    rc = run_lattice_boxes(g, cost_d, m, d_src, nullptr, m, boxes.data(), db,
+                           (uint32_t *)(dist_out_d + (int64_t)a * g->N), st, &opt);
+    if (rc) return rc;
+    ORSP_CUDA(cudaStreamSynchronize(st));
+    rc = finish_lattice_search(g, nullptr);
+    if (rc) return rc;
+    if (!decl && a == 0) {  // the gather of this call: generation ~0 until the next undeclared search
+      g->w4_gen = ~0ull;
+    }
+  }
+  if (!decl) {  // a generation this call made up must not match a caller's later declaration
+    g->w4_cost = nullptr;
+    g->w4_gen = 0;
+  }
+  return ORSP_OK;
+}

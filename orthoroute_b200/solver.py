@@ -143,6 +143,23 @@ class DeviceGraph:
         path = pbuf[: plen.value] if (dst >= 0 and st == _lib.ORSP_OK) else None
         return st, path, int(rounds.value)
 
+    def sssp_sources(self, cost: torch.Tensor, sources, dist_out: torch.Tensor, per_launch: int = 0,
+                     cost_generation: Optional[int] = None) -> int:
+        """Full searches from every source (orsp_sssp_sources): row i of
+        dist_out (device fp32 [len(sources), N]) receives the distances from
+        sources[i]; on a lattice up to per_launch sources (0: all) share one
+        launch.  Returns the status."""
+        lib = _lib.load()
+        src = np.ascontiguousarray(np.asarray(sources, dtype=np.int32).ravel())
+        if dist_out.dtype != torch.float32 or not dist_out.is_contiguous() or dist_out.numel() != src.size * self.N:
+            raise ValueError("dist_out must be a contiguous float32 tensor of len(sources) * N")
+        if cost_generation:
+            check(lib.orsp_graph_cost_generation(self._h, ptr(cost), int(cost_generation)),
+                  "orsp_graph_cost_generation")
+        return check(lib.orsp_sssp_sources(self._h, ptr(cost), int(src.size),
+                                           src.ctypes.data_as(ctypes.c_void_p), ptr(dist_out), int(per_launch),
+                                           _stream()), "orsp_sssp_sources")
+
     def sssp_roi_nodes(self, cost: torch.Tensor, src: int, dst: int, roi_nodes: torch.Tensor,
                        path_cap: Optional[int] = None):
         """One search src -> dst over the ROI given as its node list (device

@@ -150,6 +150,39 @@ def test_sssp_full_distances_bit_exact(shape, blocked, planar, impl, monkeypatch
             assert np.array_equal(_bits(dist.cpu().numpy()), _bits(ref_dist)), f"src {s} delta {delta}"
 
 
+@pytest.mark.parametrize("impl", ["lattice16", "lattice32", "generic"])
+@pytest.mark.parametrize("shape,blocked,per_launch", [((60, 50, 6), 0.05, 0), ((33, 17, 12), 0.0, 3),
+                                                      ((128, 96, 4), 0.03, 2)])
+def test_sssp_sources_distances_bit_exact(shape, blocked, per_launch, impl, monkeypatch):
+    """Many sources in one launch (whole-lattice boxes with their own
+    distance rows, orsp_sssp_sources), in chunks of per_launch, a repeated
+    source included: every row bit-identical to the oracle's full search, and
+    a cost generation declared for the whole call."""
+    _lattice_env(monkeypatch, impl)
+    lat = build_lattice(*shape)
+    w = uniform_weights(lat, seed=3 * sum(shape), blocked_frac=blocked)
+    dg = DeviceGraph.from_lattice(lat)
+    wt = cuda(w)
+    rng = np.random.default_rng(17)
+    src = [int(v) for v in rng.choice(lat.N, size=6, replace=False)]
+    src.append(src[1])
+    for gen in (None, 5):
+        dist = torch.full((len(src), lat.N), float("nan"), dtype=torch.float32, device="cuda")
+        assert dg.sssp_sources(wt, src, dist, per_launch=per_launch, cost_generation=gen) == _lib.ORSP_OK
+        got = dist.cpu().numpy()
+        for i, s in enumerate(src):
+            _, ref_dist, _, _ = O.dijkstra(lat.indptr, lat.indices, w, [s])
+            assert np.array_equal(_bits(got[i]), _bits(ref_dist)), (i, s, gen)
+    # a single search after the call gathers the weights again when undeclared
+    w2 = w.copy()
+    w2[::7] = np.float32(1.5)
+    wt.copy_(cuda(w2))
+    d1 = torch.empty(lat.N, dtype=torch.float32, device="cuda")
+    assert dg.sssp(wt, src[0], -1, dist_out=d1)[0] == _lib.ORSP_OK
+    _, ref2, _, _ = O.dijkstra(lat.indptr, lat.indices, w2, [src[0]])
+    assert np.array_equal(_bits(d1.cpu().numpy()), _bits(ref2))
+
+
 def test_sssp_paths_random_targets_and_rois():
     lat = build_lattice(70, 40, 6)
     w = uniform_weights(lat, seed=11, blocked_frac=0.04)
