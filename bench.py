@@ -45,6 +45,7 @@ sys.path.insert(0, str(REPO))
 METRIC = "sec to zero-overuse route, batched+warm vs plain, 1 B200; SSSP GTEPS & HBM GB/s"
 NX, NY, NZ = 1000, 1000, 12
 NSRC = 64
+PER_LAUNCH = 16
 BLOCKED = 0.05
 SEED = 20261203
 # DRAM bytes (read + write) per lattice node of one lattice_async_kernel launch,
@@ -191,9 +192,11 @@ def cpu_baseline(lat, w, sources, threads: int, budget_s: float = 20.0):
                       f"({t:.1f} s wall)"}
 
 
-def parity_all_sources(dg, wt, lat, w, sources, threads: int):
+def parity_all_sources(dg, wt, lat, w, sources, threads: int, per_launch: int = 0):
     """Every source's distances against the C oracle, bit for bit (the oracle
-    runs one source per host thread while the GPU computes the next)."""
+    runs one source per host thread while the GPU computes the next), from
+    the one-source search and, with per_launch > 0, from the many-source
+    launch (orsp_sssp_sources) as well."""
     import torch
 
     import oracle as O
@@ -207,15 +210,24 @@ def parity_all_sources(dg, wt, lat, w, sources, threads: int):
     def ref(s):
         return O.dijkstra(lat.indptr, lat.indices, w, [int(s)])[1].view(np.uint32)
 
+    rows = None
+    if per_launch > 0:
+        rows = torch.empty(len(sources), lat.N, dtype=torch.float32, device=wt.device)
+        for a in range(0, len(sources), per_launch):
+            dg.sssp_sources(wt, sources[a:a + per_launch], rows[a:a + per_launch], per_launch=per_launch)
     with ThreadPoolExecutor(max_workers=threads) as ex:
         for b0 in range(0, len(sources), threads):
             batch = sources[b0:b0 + threads]
             futs = [ex.submit(ref, s) for s in batch]
-            for s, f in zip(batch, futs):
+            for i, (s, f) in enumerate(zip(batch, futs)):
                 dg.sssp(wt, int(s), -1, dist_out=dist)
                 got = dist.cpu().numpy().view(np.uint32)
-                ok = ok and bool(np.array_equal(got, f.result()))
+                want = f.result()
+                ok = ok and bool(np.array_equal(got, want))
+                if rows is not None:
+                    ok = ok and bool(np.array_equal(rows[b0 + i].cpu().numpy().view(np.uint32), want))
     return {"sources_checked": len(sources), "identical_to_oracle": ok,
+            "paths_checked": "one-source searches" + (f" and {per_launch}-source launches" if rows is not None else ""),
             "oracle": f"C heap Dijkstra (fp32), {threads} host threads, {time.perf_counter() - t0:.1f} s"}
 
 
@@ -602,7 +614,8 @@ def run_ours(args, world, rank, local):
     # parity before timing: every source's distances bit-exact vs the oracle
     parity = None
     if rank == 0 and not args.no_check:
-        parity = parity_all_sources(dg, wt, lat, w, sources, threads=os.cpu_count() or 1)
+        parity = parity_all_sources(dg, wt, lat, w, sources, threads=os.cpu_count() or 1,
+                                    per_launch=min(args.per_launch, len(sources)))
         if not parity["identical_to_oracle"]:
             raise SystemExit("parity check failed: distances differ from the oracle")
 
@@ -616,42 +629,83 @@ def run_ours(args, world, rank, local):
     e_relaxed = sum(e for e, _ in per_src)
     bytes_alg = sum(12 * e + 16 * n for e, n in per_src)
 
-    # the weights stay unchanged through the timed steps: every search
+    # The weights stay unchanged through the timed steps: every search
     # declares generation 1 of them, so the whole-lattice weight gather runs
-    # once, not once per source (orsp_graph_cost_generation)
-    def step():
-        for s in sources:
-            dg.sssp(wt, int(s), -1, dist_out=dist, cost_generation=1)
+    # once, not once per source (orsp_graph_cost_generation).
+    # Headline step (per_launch > 0): orsp_sssp_sources, per_launch sources
+    # per launch, each with its own distance row (all rows stay in HBM).
+    # The one-source-at-a-time sweep is timed beside it ("single_search").
+    per = min(args.per_launch, len(sources)) if args.per_launch > 0 else 0
+    dist_all = torch.empty(len(sources), lat.N, dtype=torch.float32, device=dev) if per else None
 
-    for _ in range(args.warmup):
-        step()
-    lib.orsp_profile_enable(1)
-    kms = ctypes.c_float()
-    clocks = ClockSampler(dev.index)
-    barrier(world)
-    torch.cuda.synchronize(dev)
-    clocks.start()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    kernel_ms = 0.0
-    ev0.record(stream)
-    for _ in range(args.steps):
+    def single_step(prof=None):
         for s in sources:
             dg.sssp(wt, int(s), -1, dist_out=dist, cost_generation=1)
-            lib.orsp_profile_last(ctypes.byref(kms))
-            kernel_ms += kms.value
-    ev1.record(stream)
-    torch.cuda.synchronize(dev)
-    barrier(world)
-    clk = clocks.stop()
-    lib.orsp_profile_enable(0)
-    ms = ev0.elapsed_time(ev1)
-    ms_max = reduce_max(ms, world)
+            if prof is not None:
+                prof()
+
+    def batch_step(prof=None):
+        for a in range(0, len(sources), per):
+            dg.sssp_sources(wt, sources[a:a + per], dist_all[a:a + per], per_launch=per, cost_generation=1)
+            if prof is not None:
+                prof()
+
+    kms = ctypes.c_float()
+    c8 = (ctypes.c_int64 * 8)()
+    acc = {"ms": 0.0, "visits": 0, "n": 0}
+
+    def prof():
+        lib.orsp_profile_last(ctypes.byref(kms))
+        lib.orsp_profile_counters(c8)
+        acc["ms"] += kms.value
+        acc["visits"] += int(c8[1])
+        acc["n"] += 1
+
+    def timed(step_fn, with_clocks):
+        for _ in range(args.warmup):
+            step_fn()
+        acc.update(ms=0.0, visits=0, n=0)
+        lib.orsp_profile_enable(1)
+        clocks = ClockSampler(dev.index) if with_clocks else None
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        if clocks:
+            clocks.start()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step_fn(prof)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        clk = clocks.stop() if clocks else None
+        lib.orsp_profile_enable(0)
+        return reduce_max(ev0.elapsed_time(ev1), world), dict(acc), clk
+
     total_edges = reduce_sum(e_relaxed * args.steps, world)
+    ntiles = ((lat.nx + 15) // 16) * ((lat.ny + 15) // 16)
+    s_ms, s_acc, s_clk = timed(single_step, with_clocks=not per)
+    single = {"ms_per_search": round(s_ms / args.steps / len(sources), 4),
+              "gteps": round(total_edges / (s_ms / 1e3) / 1e9, 4),
+              "avg_launch_ms": round(s_acc["ms"] / max(1, s_acc["n"]), 4),
+              "visits_per_tile": round(s_acc["visits"] / max(1, s_acc["n"]) / ntiles, 2)}
+    if per:
+        ms_max, b_acc, clk = timed(batch_step, with_clocks=True)
+        launches = b_acc["n"]
+        kernel_ms = b_acc["ms"]
+        srcs_per_launch = len(sources) * args.steps / launches
+        visits_per_tile = b_acc["visits"] / (len(sources) * args.steps) / ntiles
+    else:
+        ms_max, clk = s_ms, s_clk
+        launches = s_acc["n"]
+        kernel_ms = s_acc["ms"]
+        srcs_per_launch = 1
+        visits_per_tile = single["visits_per_tile"]
     value = total_edges / (ms_max / 1e3) / 1e9
-    launches = args.steps * len(sources)
     avg_kernel_ms = kernel_ms / launches
-    achieved = (bytes_alg / len(sources)) / (avg_kernel_ms / 1e3) / 1e9
+    bytes_per_launch = bytes_alg / len(sources) * srcs_per_launch
+    achieved = bytes_per_launch / (avg_kernel_ms / 1e3) / 1e9
     peak, peak_kind = _peaks()
 
     # end to end through the public API with host buffers: each step uploads
@@ -659,12 +713,13 @@ def run_ours(args, world, rank, local):
     # search i (copy stream, two device and two pinned host buffers) overlaps
     # search i + 1
     w_pin = torch.from_numpy(w).pin_memory()
-    d_pin = [torch.empty(lat.N, dtype=torch.float32).pin_memory() for _ in range(2)]
-    dbuf = [dist, torch.empty_like(dist)]
     copy_stream = torch.cuda.Stream(device=dev)
-    done = [torch.cuda.Event(), torch.cuda.Event()]
     for _ in range(1):
         wt.copy_(w_pin, non_blocking=True)
+    rows = per if per else 1
+    d_pin = [torch.empty(rows, lat.N, dtype=torch.float32).pin_memory() for _ in range(2)]
+    dbuf = [dist_all, dist_all] if per else [dist.view(1, -1), torch.empty_like(dist).view(1, -1)]
+    done = [torch.cuda.Event(), torch.cuda.Event()]
     barrier(world)
     torch.cuda.synchronize(dev)
     e0 = torch.cuda.Event(enable_timing=True)
@@ -675,15 +730,21 @@ def run_ours(args, world, rank, local):
     for step_i in range(e2e_steps):
         wt.copy_(w_pin, non_blocking=True)
         gen = 1000 + step_i  # new weights every step: gathered once per step
-        for s in sources:
+        for a in range(0, len(sources), rows):
             b = k & 1
-            stream.wait_event(done[b])  # the buffer's previous read-back has finished
-            dg.sssp(wt, int(s), -1, dist_out=dbuf[b], cost_generation=gen)
+            if per:  # chunk a of the sources into its own rows of dist_all
+                dg.sssp_sources(wt, sources[a:a + rows], dist_all[a:a + rows], per_launch=rows,
+                                cost_generation=gen)
+                out = dist_all[a:a + rows]
+            else:
+                stream.wait_event(done[b])  # the buffer's previous read-back has finished
+                dg.sssp(wt, int(sources[a]), -1, dist_out=dbuf[b].view(-1), cost_generation=gen)
+                out = dbuf[b]
             ready = torch.cuda.Event()
             ready.record(stream)
             copy_stream.wait_event(ready)
             with torch.cuda.stream(copy_stream):
-                d_pin[b].copy_(dbuf[b], non_blocking=True)
+                d_pin[b][: out.shape[0]].copy_(out, non_blocking=True)
                 done[b].record(copy_stream)
             k += 1
     stream.wait_stream(copy_stream)
@@ -716,6 +777,7 @@ def run_ours(args, world, rank, local):
         "data": "synthetic (seeded lattice and weights)",
         "config": {
             "workload": f"sssp_{args.nx}x{args.ny}x{args.nz}_{len(sources)}src_full",
+            "sources_per_launch": per if per else 1,
             "nodes": lat.N,
             "edges": lat.E,
             "sources_per_step": len(sources),
@@ -725,15 +787,17 @@ def run_ours(args, world, rank, local):
         },
         "e2e": {"value": round(e2e_value, 4), "unit": "GTEPS",
                 "h2d_bytes_per_step": int(w.nbytes), "d2h_bytes_per_step": int(lat.N * 4 * len(sources))},
-        # per search: fill, seed and the tile search (the weight gather ran
+        # per launch: fill, seed and the tile search (the weight gather ran
         # before the timed region, once for the unchanged weights)
         "gpu_launches": int(launches * 3),
+        "single_search": single,
+        "visits_per_tile": round(visits_per_tile, 2),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 5),
-                     "traffic": int(LAT_DRAM_BYTES_PER_NODE * lat.N),
+                     "traffic": int(LAT_DRAM_BYTES_PER_NODE * lat.N * srcs_per_launch),
                      "traffic_source": "ncu dram bytes of a 600x600x12 launch, scaled by node count",
                      "kernel": "lattice_async_kernel", "peak_kind": peak_kind,
-                     "bytes_per_launch": int(bytes_alg / len(sources)),
+                     "bytes_per_launch": int(bytes_per_launch),
                      "avg_launch_ms": round(avg_kernel_ms, 4)},
         "clocks": clk,
         "parity": parity,
@@ -804,6 +868,8 @@ def main():
     ap.add_argument("--ny", type=int, default=NY)
     ap.add_argument("--nz", type=int, default=NZ)
     ap.add_argument("--sources", type=int, default=NSRC)
+    ap.add_argument("--per-launch", type=int, default=PER_LAUNCH,
+                    help="sources per tile-search launch (orsp_sssp_sources); 0: one search per launch")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-check", action="store_true", help="skip the parity check before timing")
     ap.add_argument("--no-route", action="store_true", help="skip the routing measurements")

@@ -152,7 +152,8 @@ ORSP_API int orsp_sssp(orsp_graph *g, const float *cost_d, int32_t nseeds,
  * The batched counterpart of SimpleDijkstra.find_path_roi over the full
  * graph (UPF:1801-1887) for many sources, as CUDADijkstra.find_paths_on_rois
  * (CD:2014-2086) batches ROI searches.  A cost-generation declaration covers
- * the whole call. */
+ * the whole call; orsp_profile_last / orsp_profile_counters report the sum
+ * over the call's launches. */
 ORSP_API int orsp_sssp_sources(orsp_graph *g, const float *cost_d, int32_t nsrc, const int32_t *src_h,
                                float *dist_out_d, int32_t per_launch, uintptr_t stream);
 

@@ -958,6 +958,9 @@ extern "C" int orsp_sssp_sources(orsp_graph *g, const float *cost_d, int32_t nsr
     g->blat_tab_bytes = tab;
   }
   const uint64_t decl = g->decl_cost == cost_d ? g->decl_gen : 0;
+  // profiling: kernel time and counters summed over the chunks
+  float ksum = 0.0f;
+  int64_t csum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (int32_t a = 0; a < nsrc; a += per) {
     const int32_t m = std::min(per, nsrc - a);
     LatBox *hb = (LatBox *)g->blat_tab_h;
@@ -986,6 +989,13 @@ extern "C" int orsp_sssp_sources(orsp_graph *g, const float *cost_d, int32_t nsr
     ORSP_CUDA(cudaStreamSynchronize(st));
     rc = finish_lattice_search(g, nullptr);
     if (rc) return rc;
+    for (int i = 0; i < 8; ++i) csum[i] += g_counters[i];
+    if (g_timer.on && g_timer.pending) {
+      float ms = 0.0f;
+      ORSP_CUDA(cudaEventElapsedTime(&ms, g_timer.a, g_timer.b));
+      ksum += ms;
+      g_timer.pending = false;
+    }
     if (!decl && a == 0) {  // the gather of this call: generation ~0 until the next undeclared search
       g->w4_gen = ~0ull;
     }
@@ -994,5 +1004,7 @@ extern "C" int orsp_sssp_sources(orsp_graph *g, const float *cost_d, int32_t nsr
     g->w4_cost = nullptr;
     g->w4_gen = 0;
   }
+  for (int i = 0; i < 8; ++i) g_counters[i] = csum[i];
+  if (g_timer.on) g_timer.last_ms = ksum;
   return ORSP_OK;
 }

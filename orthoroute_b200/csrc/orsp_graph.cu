@@ -14,6 +14,10 @@ void set_error(const std::string &msg) { g_last_error = msg; }
 
 int cuda_fail(cudaError_t e, const char *what) {
   set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  // a failed launch or call leaves its (non-sticky) error as the thread's
+  // last error; clear it, so that the caller's next unrelated check does not
+  // report it again
+  (void)cudaGetLastError();
   return e == cudaErrorMemoryAllocation ? ORSP_ERR_NOMEM : ORSP_ERR_CUDA;
 }
 

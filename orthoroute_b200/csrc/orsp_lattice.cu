@@ -1173,28 +1173,47 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   }
   else kfn = priv ? (void *)lattice_tile_kernel<TX, TY, true> : (void *)lattice_tile_kernel<TX, TY, false>;
   const int threads = TX * TY + (spec ? 32 : 0);
-  // the attribute and the occupancy per (kernel, block, shared memory) and
-  // device: set and queried once, not on every search
+  // The shared-memory cap is a per-kernel attribute: it is raised to the
+  // largest tile once per (kernel, device), never lowered, so a launch with a
+  // smaller tile does not invalidate a cached larger one.  The occupancy is
+  // cached per (kernel, block, shared memory, device).
   struct OccEntry {
     void *fn;
     int threads, device;
     size_t smem;
     int occ;
   };
-  static OccEntry occ_cache[32];
+  struct CapEntry {
+    void *fn;
+    int device;
+  };
+  static OccEntry occ_cache[64];
   static int occ_n = 0;
+  static CapEntry cap_set[32];
+  static int cap_n = 0;
   static std::mutex occ_mu;
   int occ = -1;
   {
     std::lock_guard<std::mutex> lock(occ_mu);
+    bool capped = false;
+    for (int i = 0; i < cap_n; ++i) capped = capped || (cap_set[i].fn == kfn && cap_set[i].device == g->device);
+    if (!capped) {
+      // the opt-in maximum less the kernel's static shared memory
+      cudaFuncAttributes fa{};
+      ORSP_CUDA(cudaFuncGetAttributes(&fa, kfn));
+      int optin = 0;
+      ORSP_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, g->device));
+      ORSP_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     optin - (int)fa.sharedSizeBytes));
+      if (cap_n < 32) cap_set[cap_n++] = CapEntry{kfn, g->device};
+    }
     for (int i = 0; i < occ_n; ++i)
       if (occ_cache[i].fn == kfn && occ_cache[i].threads == threads && occ_cache[i].smem == smem &&
           occ_cache[i].device == g->device)
         occ = occ_cache[i].occ;
     if (occ < 0) {
-      ORSP_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       ORSP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, threads, smem));
-      if (occ_n < 32) occ_cache[occ_n++] = OccEntry{kfn, threads, g->device, smem, occ};
+      if (occ_n < 64) occ_cache[occ_n++] = OccEntry{kfn, threads, g->device, smem, occ};
     }
   }
   if (occ < 1) {

@@ -55,7 +55,7 @@ def test_roi_node_list_searches_match_oracle():
     order and repeated, fractional costs with exact ties, blocked edges, and
     src / dst outside the ROI."""
     rng = np.random.default_rng(31)
-    for nx, ny, nz in ((60, 44, 4), (37, 53, 6), (90, 20, 2)):
+    for nx, ny, nz in ((60, 44, 4), (37, 53, 6), (90, 20, 3)):
         lat = build_lattice(nx, ny, nz)
         dg = DeviceGraph.from_lattice(lat)
         assert dg.is_lattice
