@@ -68,7 +68,6 @@ struct LatParams {
   unsigned long long wait_ns, budget_ns;
   int selfcont;
   const int32_t *roi_map;  // node-set ROI searches: seeds outside it are ignored
-  int prepop;              // reserve the next queue position when a visit starts from a backlog
 };
 
 __global__ void fill_kernel(uint32_t *p, int64_t n, uint32_t v) {
@@ -872,17 +871,12 @@ __global__ void __launch_bounds__(TX * TY, MINB) lattice_async_kernel(LatParams 
   unsigned long long sched_ns = 0;
   __shared__ int s_cont;
   if (threadIdx.x == 0) s_cont = -1;
-  // (thread 0) queue position reserved ahead for the next pop, or -1: with
-  // p.prepop, a pop that found its tile already waiting (a backlog) reserves
-  // the next position at once, so that atomic overlaps the visit
-  long long next_pos = -1;
   for (;;) {
     if (threadIdx.x == 0 && s_cont < 0) {
       const unsigned long long tq = dev_globaltimer();
       int t = -1;
       if (!ld_acquire_u32((const unsigned *)&ctl->err)) {
-        const unsigned pos = next_pos >= 0 ? (unsigned)next_pos : atomicAdd(&ctl->head, 1u);
-        next_pos = -1;
+        const unsigned pos = atomicAdd(&ctl->head, 1u);
         int *slot = &p.qslot[pos % p.qcap];
         const unsigned long long t0 = dev_globaltimer();
         for (unsigned spins = 0;; ++spins) {
@@ -890,7 +884,6 @@ __global__ void __launch_bounds__(TX * TY, MINB) lattice_async_kernel(LatParams 
           if (v >= 0) {
             atomicExch(slot, -1);
             t = v;
-            if (p.prepop && spins == 0) next_pos = atomicAdd(&ctl->head, 1u);
             break;
           }
           if (ld_acquire_u32((const unsigned *)&ctl->pending) == 0) break;  // fixpoint reached
@@ -933,10 +926,7 @@ __global__ void __launch_bounds__(TX * TY, MINB) lattice_async_kernel(LatParams 
       // (halo changed meanwhile) or not converged
       s_cont = -1;
       if (s_act[4] || atomicCAS(&p.tstate[t], 2, 0) != 2) {
-        // (a CTA that holds a reserved queue position queues the tile again
-        // instead, so that the tile waiting at that position is taken after
-        // one visit)
-        if (p.selfcont && next_pos < 0) {
+        if (p.selfcont) {
           // visit it again at once: the interior and weights are already in
           // shared memory, so only the halo is read again, and there is no
           // queue handoff.  Visiting again (state 2) is published before the
@@ -1225,8 +1215,6 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   p.wait_ns = env_u64("ORSP_WAIT_NS", 2000000000ull);
   // ORSP_LAT_SELF=0: a tile to visit again goes back to the queue instead
   p.selfcont = (int)env_u64("ORSP_LAT_SELF", 1);
-  // ORSP_LAT_PREPOP=1: reserve the next queue position early under a backlog
-  p.prepop = (int)env_u64("ORSP_LAT_PREPOP", 0);
   p.budget_ns = env_u64("ORSP_BUDGET_NS", 20000000000ull);
   void *args[] = {&p};
   if (orsp::g_timer.on) ORSP_CUDA(cudaEventRecord(orsp::g_timer.a, st));
