@@ -140,7 +140,7 @@ struct LatBox {
   int32_t x0, x1, y0, y1, z0, z1;
   int32_t ntx, nty;  // tiles along x and y
   int32_t tile0;     // id of the box's first tile
-  int32_t pad;
+  int32_t pad;       // the box's distance slice for the TMA staging (LatOptions::tma_slices)
   int64_t dbase;     // -1: distances indexed by node id in the shared array;
                      // >= 0: the box's own slice, box-local row-major from here
 };
@@ -160,6 +160,8 @@ struct LatOptions {
   bool fill_box_only = false;  // reset distances inside the boxes only (the caller's backtrace checks the box)
   bool copy_ctl = true;        // copy the control block to the pinned mirror (finish_lattice_search)
   int *err_d = nullptr;        // out: device address of the launch's error word
+  int64_t tma_slices = 0;      // > 0: every box is the whole lattice, box j's distances in slice j of N
+                               // cells from `dist` (LatBox.pad = j); allows the TMA staging
 };
 // One box (nullptr: the whole lattice).  Stages its tile table through the
 // graph's pinned buffer, so the calling entry point must synchronise before

@@ -969,6 +969,7 @@ extern "C" int orsp_sssp_sources(orsp_graph *g, const float *cost_d, int32_t nsr
     const int64_t ntiles = make_lat_boxes(boxes.data(), m, hb);
     for (int32_t j = 0; j < m; ++j) {
       hb[j].dbase = (int64_t)j * g->N;
+      hb[j].pad = j;  // TMA staging: slice j
       h_src[j] = src_h[a + j];
     }
     ORSP_CUDA(cudaMemcpyAsync(g->blat_tab_d, g->blat_tab_h, (size_t)m * sizeof(LatBox) + (size_t)m * 4,
@@ -980,6 +981,7 @@ extern "C" int orsp_sssp_sources(orsp_graph *g, const float *cost_d, int32_t nsr
     LatOptions opt;
     opt.private_dist = true;
     opt.private_count = (int64_t)m * g->N;
+    opt.tma_slices = m;
     // every chunk after the first reuses the gathered weights of this call
     if (decl) g->decl_cost = cost_d, g->decl_gen = decl;
     else if (a > 0) g->decl_cost = cost_d, g->decl_gen = ~0ull;

@@ -22,6 +22,9 @@
 // the tile itself if it did not converge).  Each tile is in a round's list at
 // most once (stamp[t] = last round it was queued for), so a tile is only ever
 // processed by one CTA per round and owns its nodes' distances.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <climits>
 #include <cstdlib>
@@ -487,6 +490,75 @@ __device__ __forceinline__ void tile_sync() {
   else __syncthreads();
 }
 
+// Tensor-memory-accelerator staging of a whole-lattice tile (ORSP_LAT_TMA=1):
+// two cp.async.bulk.tensor loads per fresh visit, completing on one mbarrier,
+// bring the tile's in-edge weights (box {4, TX, TY, nzb} of the float4 array
+// seen as fp32 [nz][ny][nx][4]) and its distances with a halo (box
+// {TX + 8, TY + 2, nzb} of the u32 distances [slice][nz][ny][nx], starting at
+// x = X0 - 4 so that the start is 16-byte aligned) into a staging area; the
+// threads then copy them into the sweep layout (odd row strides), as the
+// plain loads do.  Out-of-lattice cells of the box are zero-filled by the
+// copy engine and replaced by +inf (halo) or ignored (interior) in the copy.
+// The tensor maps cover this GPU's memory only and no load is multicast.
+struct TmaCtx {
+  const CUtensorMap *tw, *td;  // the kernel's __grid_constant__ tensor maps
+  uint32_t mbar;               // shared address of the CTA's mbarrier
+  unsigned phase;              // parity of the next completion
+  float *sw;                   // staging: weights [nzb][TY][TX] float4
+  uint32_t *sdd;               // staging: distances [nzb][TY + 2][TX + 8]
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void *ptr) {
+  return (uint32_t)__cvta_generic_to_shared(ptr);
+}
+
+// Thread 0 issues the two loads of the tile at (X0, Y0) of distance slice
+// `slice`; every thread then waits (bounded) for their completion.
+template <int TX, int TY>
+__device__ __forceinline__ void tma_stage(const LatParams &p, int32_t X0, int32_t Y0, int32_t z0, int nzb,
+                                          int slice, TmaCtx &tc) {
+  if (threadIdx.x == 0) {
+    const uint32_t bytes = (uint32_t)nzb * (uint32_t)(TY * TX * 16 + (TY + 2) * (TX + 8) * 4);
+    // distances other CTAs published (acquired through the tile state) are
+    // read by the async proxy; the staging's earlier generic reads come
+    // before its async-proxy writes
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc.mbar), "r"(bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+        ::"r"(smem_addr(tc.sw)), "l"((uint64_t)tc.tw), "r"(0), "r"(X0), "r"(Y0), "r"(z0), "r"(tc.mbar)
+        : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+        ::"r"(smem_addr(tc.sdd)), "l"((uint64_t)tc.td), "r"(X0 - 4), "r"(Y0 - 1), "r"(z0), "r"(slice), "r"(tc.mbar)
+        : "memory");
+  }
+  // bounded wait: past wait_ns the search is failed with a timeout, and the
+  // wait goes on for one more wait_ns so that the copies are not left in
+  // flight into shared memory that the next visit reuses
+  const unsigned long long t0 = dev_globaltimer();
+  bool timed_out = false;
+  for (unsigned spins = 0;; ++spins) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n selp.u32 %0, 1, 0, P;\n}"
+        : "=r"(ok)
+        : "r"(tc.mbar), "r"(tc.phase)
+        : "memory");
+    if (ok) break;
+    if ((spins & 63u) == 63u) {
+      const unsigned long long dt = dev_globaltimer() - t0;
+      if (!timed_out && dt > p.wait_ns) {
+        atomicCAS(&p.ctl->err, DEV_OK, DEV_ERR_TIMEOUT);
+        timed_out = true;
+      }
+      if (dt > 2 * p.wait_ns) break;
+    }
+  }
+  tc.phase ^= 1u;
+}
+
 // Layer lists of the box being visited: H layers (x-runs) and V layers
 // (y-runs) as offsets from the box's z0.  Recomputed when a CTA moves to a
 // tile of another box.
@@ -496,9 +568,10 @@ struct LayerLists {
   int box;
 };
 
-template <int TX, int TY, bool PRIV, bool SPEC, bool DEEP = false>
+template <int TX, int TY, bool PRIV, bool SPEC, bool DEEP = false, bool TMA = false>
 __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *sd, LayerLists &L, int *s_flags,
-                                             int *s_act, int *s_nb = nullptr, bool warm = false) {
+                                             int *s_act, int *s_nb = nullptr, bool warm = false,
+                                             TmaCtx *tma = nullptr) {
   const int bi = box_of_tile(p, t);
   const LatBox B = load_box(p, bi);
   if (threadIdx.x == 0 && L.box != bi) {
@@ -548,7 +621,52 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
   // weights are read-only.  A thread's first halo cells are loaded before its
   // column (one thread per column (x, y), up to 18 layers in flight at a
   // time), so their round trip overlaps the column's.
-  {
+  bool staged = false;
+  if constexpr (TMA) {
+    if (!warm) {
+      tma_stage<TX, TY>(p, X0, Y0, B.z0, nzb, PRIV ? B.pad : 0, *tma);
+      constexpr int DX = TX + 8, DY = TY + 2;
+      const uint32_t *sdd = tma->sdd;
+      const float4 *sw4 = (const float4 *)tma->sw;
+      const int c = threadIdx.x;
+      if (c < th * tw) {
+        const int yy = c / tw + 1, xx = c - (yy - 1) * tw + 1;
+        const int s0 = yy * SX + xx, w0 = (yy - 1) * WSX + (xx - 1);
+        for (int z = 0; z < nzb; ++z) {
+          const float dv = __uint_as_float(sdd[(z * DY + yy) * DX + xx + 3]);
+          const float4 wv = sw4[(z * TY + yy - 1) * TX + xx - 1];
+          const int wi = z * WPS + w0;
+          sd[z * PS + s0] = dv;
+          orig[wi] = dv;
+          wlo[wi] = wv.x;
+          whi[wi] = wv.y;
+          wdn[wi] = wv.z;
+          wup[wi] = wv.w;
+        }
+      }
+      const int nhh = 2 * nh * th, nvh = 2 * nv * tw;
+      for (int i = threadIdx.x; i < nhh + nvh; i += (TX * TY)) {
+        int z, xx, yy;
+        if (i < nhh) {
+          const int rowi = i >> 1;
+          z = s_hl[rowi / th];
+          yy = rowi % th + 1;
+          xx = (i & 1) ? tw + 1 : 0;
+        } else {
+          const int coli = (i - nhh) >> 1;
+          z = s_vl[coli / tw];
+          xx = coli % tw + 1;
+          yy = ((i - nhh) & 1) ? th + 1 : 0;
+        }
+        const int32_t gx = X0 + xx - 1, gy = Y0 + yy - 1;
+        float v = INF_F;
+        if (gx >= B.x0 && gx <= B.x1 && gy >= B.y0 && gy <= B.y1) v = __uint_as_float(sdd[(z * DY + yy) * DX + xx + 3]);
+        sd[z * PS + yy * SX + xx] = v;
+      }
+      staged = true;
+    }
+  }
+  if (!staged) {
     const int nhh = 2 * nh * th, nvh = 2 * nv * tw;
     constexpr int HB = 4;  // halo cells per thread in the first batch
     float hv[HB];
@@ -855,16 +973,40 @@ __device__ bool activate_tile(const LatParams &p, int t) {
 // in 18-layer blocks); compiled separately so that each layer range gets its
 // own register allocation.  MINB: CTAs per SM the registers are sized for
 // (2 fits a 16 x 16 tile of up to 12 layers in 128 registers per thread).
-template <int TX, int TY, bool PRIV, bool DEEP = false, int MINB = 1>
-__global__ void __launch_bounds__(TX * TY, MINB) lattice_async_kernel(LatParams p) {
-  extern __shared__ float sd[];
+//
+// TMA: fresh visits stage the tile with tensor loads (TmaCtx); every box is
+// the whole lattice (the tensor maps and the staging are sized for p.nz
+// layers), distances in slices of N cells (LatBox.pad = slice).  tmw / tmd
+// are unused otherwise.
+template <int TX, int TY, bool PRIV, bool DEEP = false, int MINB = 1, bool TMA = false>
+__global__ void __launch_bounds__(TX * TY, MINB)
+    lattice_async_kernel(LatParams p, const __grid_constant__ CUtensorMap tmw, const __grid_constant__ CUtensorMap tmd) {
+  extern __shared__ __align__(128) float sd[];
   __shared__ LayerLists s_layers;
   __shared__ int s_flags[6];
   __shared__ int s_act[5];
   __shared__ int s_nb[4];
   __shared__ int s_tile;
+  __shared__ __align__(8) unsigned long long s_mbar;
   LatCtl *ctl = p.ctl;
   const unsigned long long t_start = dev_globaltimer();
+  TmaCtx tma{};
+  if constexpr (TMA) {
+    constexpr int PS = (TY + 2) * (TX + 3), WPS = TY * (TX + 1);
+    const int64_t off = ((int64_t)p.nz * PS + 5 * (int64_t)p.nz * WPS + 31) & ~(int64_t)31;
+    tma.tw = &tmw;
+    tma.td = &tmd;
+    tma.mbar = smem_addr(&s_mbar);
+    tma.phase = 0;
+    tma.sw = sd + off;
+    tma.sdd = (uint32_t *)(sd + off + (int64_t)p.nz * TY * TX * 4);
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tma.mbar) : "memory");
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tmw) : "memory");
+      asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tmd) : "memory");
+    }
+  }
   if (threadIdx.x == 0) s_layers.box = -1;
   __syncthreads();
   unsigned visits = 0;
@@ -910,7 +1052,7 @@ __global__ void __launch_bounds__(TX * TY, MINB) lattice_async_kernel(LatParams 
     const int t = warm ? s_cont : s_tile;
     __syncthreads();
     if (t < 0) break;
-    process_tile<TX, TY, PRIV, false, DEEP>(p, t, sd, s_layers, s_flags, s_act, s_nb, warm);
+    process_tile<TX, TY, PRIV, false, DEEP, TMA>(p, t, sd, s_layers, s_flags, s_act, s_nb, warm, &tma);
     // neighbours are activated by threads 0..3 in parallel, after this
     // tile's distances are visible
     unsigned long long ta = 0;
@@ -1115,6 +1257,54 @@ int grow_ws(orsp::Graph *g, size_t need) {
   return ORSP_OK;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library); nullptr when unavailable.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!tried) {
+    tried = true;
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)f;
+    else
+      (void)cudaGetLastError();
+  }
+  return fn;
+}
+
+// The two tensor maps of the TMA staging: weights as fp32 [nz][ny][nx][4]
+// (box {4, TX, TY, nzb}) and distances as u32 [slices][nz][ny][nx] (box
+// {TX + 8, TY + 2, nzb, 1}).  False (plain loads) when a stride or base is
+// not 16-byte aligned or the encoder refuses.
+bool encode_lattice_maps(const orsp::Graph *g, const LatParams &p, int TX, int TY, int nzb, int64_t slices,
+                         CUtensorMap *tmw, CUtensorMap *tmd) {
+  const int64_t nx = g->nx, ny = g->ny, nz = g->nz, N = (int64_t)g->N;
+  if (nx % 4 != 0 || ((uintptr_t)p.dist & 15) != 0 || ((uintptr_t)p.w4 & 15) != 0) return false;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return false;
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  const cuuint64_t dw[4] = {4, (cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+  const cuuint64_t sw[3] = {16, (cuuint64_t)(16 * nx), (cuuint64_t)(16 * nx * ny)};
+  const cuuint32_t bw[4] = {4, (cuuint32_t)TX, (cuuint32_t)TY, (cuuint32_t)nzb};
+  if (enc(tmw, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)p.w4, dw, sw, bw, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  const cuuint64_t dd[4] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)slices};
+  const cuuint64_t sdd[3] = {(cuuint64_t)(4 * nx), (cuuint64_t)(4 * nx * ny), (cuuint64_t)(4 * N)};
+  const cuuint32_t bd[4] = {(cuuint32_t)(TX + 8), (cuuint32_t)(TY + 2), (cuuint32_t)nzb, 1};
+  if (enc(tmd, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, (void *)p.dist, dd, sdd, bd, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  return true;
+}
+
 template <int TX, int TY>
 int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_t nseeds, const int32_t *seeds,
                    const float *seed_cost, cudaStream_t st, orsp::LatOptions *opt) {
@@ -1138,7 +1328,7 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   if (async) ORSP_CUDA(cudaMemsetAsync(p.qslot, 0xff, (size_t)qcap * 4, st));
   lattice_seed_kernel<TX, TY><<<1, 256, 0, st>>>(p, nseeds, seeds, seed_cost);
   ORSP_CUDA(cudaGetLastError());
-  const size_t smem = ((size_t)nzb * (TY + 2) * (TX + 3) + (size_t)5 * nzb * TY * (TX + 1)) * sizeof(float);
+  size_t smem = ((size_t)nzb * (TY + 2) * (TX + 3) + (size_t)5 * nzb * TY * (TX + 1)) * sizeof(float);
   if (smem > 227 * 1024) {
     orsp::set_error("lattice search: too many layers for the shared-memory tile");
     return ORSP_ERR_ARG;
@@ -1149,12 +1339,28 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   // ORSP_LAT_BLOCKS_PER_SM: CTAs per SM (tiles of up to 12 layers at width
   // 16 have an instantiation sized for 2)
   const int want = (int)env_u64("ORSP_LAT_BLOCKS_PER_SM", 1);
+  // ORSP_LAT_TMA=1: tensor-load staging of fresh visits, for whole-lattice
+  // boxes (opt->tma_slices: distance slices of N cells, box j in slice j)
+  CUtensorMap tmw{}, tmd{};
+  bool tma = false;
+  if constexpr (TX == 16) {
+    if (async && !spec && want < 2 && nzb <= 12 && nzb == g->nz && opt && opt->tma_slices > 0 &&
+        env_u64("ORSP_LAT_TMA", 0) != 0)
+      tma = encode_lattice_maps(g, p, TX, TY, nzb, opt->tma_slices, &tmw, &tmd);
+  }
+  if (tma) {
+    const size_t base = (((size_t)nzb * (TY + 2) * (TX + 3) + (size_t)5 * nzb * TY * (TX + 1)) + 31) & ~(size_t)31;
+    smem = (base + (size_t)nzb * TY * TX * 4 + (size_t)nzb * (TY + 2) * (TX + 8)) * sizeof(float);
+  }
   void *kfn;
   if (spec) kfn = priv ? (void *)lattice_spec_kernel<TX, TY, true> : (void *)lattice_spec_kernel<TX, TY, false>;
   else if (async) {
     kfn = priv ? (void *)lattice_async_kernel<TX, TY, true> : (void *)lattice_async_kernel<TX, TY, false>;
     if constexpr (TX == 16) {  // deeper tiles: the instantiation with 18-layer column loads
-      if (nzb > 12)
+      if (tma)
+        kfn = priv ? (void *)lattice_async_kernel<TX, TY, true, false, 1, true>
+                   : (void *)lattice_async_kernel<TX, TY, false, false, 1, true>;
+      else if (nzb > 12)
         kfn = priv ? (void *)lattice_async_kernel<TX, TY, true, true> : (void *)lattice_async_kernel<TX, TY, false, true>;
       else if (want >= 2)
         kfn = priv ? (void *)lattice_async_kernel<TX, TY, true, false, 2>
@@ -1216,7 +1422,7 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   // ORSP_LAT_SELF=0: a tile to visit again goes back to the queue instead
   p.selfcont = (int)env_u64("ORSP_LAT_SELF", 1);
   p.budget_ns = env_u64("ORSP_BUDGET_NS", 20000000000ull);
-  void *args[] = {&p};
+  void *args[] = {&p, &tmw, &tmd};  // the tile and spec kernels take p only
   if (orsp::g_timer.on) ORSP_CUDA(cudaEventRecord(orsp::g_timer.a, st));
   // Cooperative launch in both schedules: every CTA is resident, so a CTA
   // waiting for a queue slot never blocks the CTA that will fill it.

@@ -656,7 +656,9 @@ static int sssp_impl(orsp_graph *g, const float *cost_d, int32_t nseeds, const i
     if (rc) return rc;
     ORSP_CUDA(cudaMemsetAsync(g->ctl, 0, sizeof(SsspCtl), st));
   } else if (lattice) {
-    rc = run_lattice_search(g, cost_d, nseeds, seeds_d, seed_cost_d, box_h, dist, st);
+    LatOptions lopt;
+    lopt.tma_slices = box_h ? 0 : 1;  // the whole lattice: TMA staging allowed
+    rc = run_lattice_search(g, cost_d, nseeds, seeds_d, seed_cost_d, box_h, dist, st, &lopt);
     if (rc) return rc;
     ORSP_CUDA(cudaMemsetAsync(g->ctl, 0, sizeof(SsspCtl), st));
   } else {

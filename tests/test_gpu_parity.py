@@ -122,14 +122,16 @@ def test_sssp_reference_lattice_duplicate_vias(golden):
 def _lattice_env(monkeypatch, impl):
     """Selects the search implementation: generic near-far, or the tile sweeps
     with tile width 16/32 and the asynchronous, warp-specialised or round
-    schedule."""
+    schedule, with plain or tensor-load (TMA) staging of whole-lattice tiles."""
     monkeypatch.setenv("ORSP_SSSP_IMPL", "generic" if impl == "generic" else "auto")
     monkeypatch.setenv("ORSP_LAT_TILE", "32" if impl == "lattice32" else "16")
     monkeypatch.setenv("ORSP_LAT_ASYNC", "0" if impl.endswith("rounds") else "1")
     monkeypatch.setenv("ORSP_LAT_SPEC", "1" if impl.endswith("spec") else "0")
+    monkeypatch.setenv("ORSP_LAT_TMA", "1" if impl.endswith("tma") else "0")
 
 
-@pytest.mark.parametrize("impl", ["lattice16", "lattice32", "lattice16-rounds", "lattice16-spec", "generic"])
+@pytest.mark.parametrize("impl", ["lattice16", "lattice32", "lattice16-rounds", "lattice16-spec", "lattice16-tma",
+                                  "generic"])
 @pytest.mark.parametrize("shape,blocked,planar", [((60, 50, 6), 0.05, "all"), ((33, 17, 12), 0.0, "all"),
                                                   ((128, 96, 4), 0.03, "all"), ((45, 70, 6), 0.02, "inner")])
 def test_sssp_full_distances_bit_exact(shape, blocked, planar, impl, monkeypatch):
@@ -150,9 +152,9 @@ def test_sssp_full_distances_bit_exact(shape, blocked, planar, impl, monkeypatch
             assert np.array_equal(_bits(dist.cpu().numpy()), _bits(ref_dist)), f"src {s} delta {delta}"
 
 
-@pytest.mark.parametrize("impl", ["lattice16", "lattice32", "generic"])
+@pytest.mark.parametrize("impl", ["lattice16", "lattice32", "lattice16-tma", "generic"])
 @pytest.mark.parametrize("shape,blocked,per_launch", [((60, 50, 6), 0.05, 0), ((33, 17, 12), 0.0, 3),
-                                                      ((128, 96, 4), 0.03, 2)])
+                                                      ((128, 96, 4), 0.03, 2), ((64, 40, 12), 0.02, 4)])
 def test_sssp_sources_distances_bit_exact(shape, blocked, per_launch, impl, monkeypatch):
     """Many sources in one launch (whole-lattice boxes with their own
     distance rows, orsp_sssp_sources), in chunks of per_launch, a repeated
