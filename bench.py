@@ -4,9 +4,12 @@
 Workload (one "step"): the single-source SSSP sweep on the 1000x1000x12
 alternating-H/V lattice with adjacent-layer vias (12.0 M nodes, 45.98 M
 directed edges, int32 CSR), fp32 weights uniform in [1,2) on planar edges,
-3.0 on vias, 5 % of edges blocked (+inf), seeded; 64 random sources run one at
-a time as full searches over the whole grid.  Distances are checked bit for
-bit against the CPU oracle on a sample before timing.
+3.0 on vias, 5 % of edges blocked (+inf), seeded; 64 random sources as full
+searches over the whole grid, 16 sources per tile-search launch
+(orsp_sssp_sources, --per-launch; 0 runs them one at a time).  The
+one-source-at-a-time sweep is timed beside it ("single_search").  Every
+source's distances are checked bit for bit against the CPU oracle before
+timing, from both modes.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
