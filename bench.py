@@ -294,6 +294,102 @@ def route_dropin(dev, with_cpu: bool):
     return out
 
 
+def roi_searches(dev, nsamp: int = 48, ncheck: int = 8):
+    """BFS-ROI searches as the reference's _route_all issues them: for net
+    (s, d), find_path_roi over extract_roi_bfs(s, d) with depth min(max(60,
+    0.75 * manhattan), 150) and at most 50 000 nodes (UPF:1619-1734,
+    4614-4785), on the config-1 board (100x100x4, 200 nets) and the config-3
+    board (600x600x18, 8 000 nets), nsamp nets each, fp32 costs uniform in
+    [1, 2) with vias at 3.  Per search (the synchronous C-ABI call, ROI
+    already on the device): the tile-sweep ROI search against the generic
+    grid kernel it replaced ("before").  On the same boards built as the
+    reference's own Lattice3D graph (inner-layer planar edges, full via
+    stacks with duplicated via edges, not a tile lattice): the one-CTA search
+    against the grid kernel.  Paths must agree across implementations and
+    with the oracle on ncheck nets."""
+    import torch
+
+    import oracle as O
+    from orthoroute_b200 import _lib
+    from orthoroute_b200.lattice import board_footprints, board_uniform_pins, build_lattice, uniform_weights
+    from orthoroute_b200.solver import DeviceGraph
+
+    O.build_oracle()
+    out = {}
+    keys = ("ORSP_SSSP_IMPL", "ORSP_ROI_NODES_IMPL")
+    saved = {k: os.environ.get(k) for k in keys}
+    try:
+        for name, (nx, ny, nz), make in (
+                ("c1", (100, 100, 4), lambda: board_uniform_pins(100, 100, 4, 200, seed=1)),
+                ("c3", (600, 600, 18), lambda: board_footprints(600, 600, 18, 8000, None, seed=3))):
+            b = make()
+            rng = np.random.default_rng(5)
+            pick = rng.choice(len(b.src), size=min(nsamp, len(b.src)), replace=False)
+            nets = [(int(b.src[i]), int(b.dst[i])) for i in pick]
+            row = {}
+            for shape, lat in (("lattice", b.lattice),
+                               ("reference_lattice3d", build_lattice(nx, ny, nz, planar="inner", vias="full",
+                                                                     duplicate_vias=True))):
+                w = uniform_weights(lat, seed=11)
+                wt = torch.from_numpy(w).to(dev)
+                dg = (DeviceGraph.from_lattice(lat, device=dev) if shape == "lattice"
+                      else DeviceGraph(lat.indptr, lat.indices, device=dev))
+                rois = []
+                for s_, d_ in nets:
+                    (sx, sy, _), (dx, dy, _) = lat.coords(s_), lat.coords(d_)
+                    depth = min(max(60, int(0.75 * (abs(int(dx) - int(sx)) + abs(int(dy) - int(sy))))), 150)
+                    roi, _ = dg.roi_bfs(s_, d_, depth, 50_000, want_g2r=False)
+                    rois.append(roi.clone())
+                impls = ({"tile_sweeps": {"ORSP_SSSP_IMPL": "auto"}, "grid_before": {"ORSP_SSSP_IMPL": "generic",
+                                                                                      "ORSP_ROI_NODES_IMPL": "grid"}}
+                         if shape == "lattice" else
+                         {"one_cta": {"ORSP_ROI_NODES_IMPL": "cta"}, "grid_before": {"ORSP_ROI_NODES_IMPL": "grid"}})
+                res, paths = {}, {}
+                for iname, env in impls.items():
+                    for k in keys:
+                        os.environ.pop(k, None)
+                    os.environ.update(env)
+                    for (s_, d_), roi in list(zip(nets, rois))[:4]:  # warm-up
+                        dg.sssp_roi_nodes(wt, s_, d_, roi)
+                    torch.cuda.synchronize(dev)
+                    got = []
+                    t0 = time.perf_counter()
+                    for (s_, d_), roi in zip(nets, rois):
+                        st, pth = dg.sssp_roi_nodes(wt, s_, d_, roi)
+                        got.append(pth.cpu().numpy().copy() if st == _lib.ORSP_OK else None)
+                    dt = time.perf_counter() - t0
+                    res[iname] = {"ms_per_search": round(dt / len(nets) * 1e3, 3)}
+                    paths[iname] = got
+                names = list(impls)
+                same = all((a is None and c is None) or (a is not None and c is not None and np.array_equal(a, c))
+                           for a, c in zip(paths[names[0]], paths[names[1]]))
+                ok = True
+                for (s_, d_), roi, pth in list(zip(nets, rois, paths[names[0]]))[:ncheck]:
+                    r = roi.cpu().numpy()
+                    g2r = np.full(lat.N, -1, np.int32)
+                    g2r[r] = np.arange(len(r), dtype=np.int32)
+                    ref, *_ = O.dijkstra(lat.indptr, lat.indices, w, [s_], dst=d_, roi_map=g2r)
+                    want = ref if len(ref) > 1 else None
+                    ok = ok and ((pth is None and want is None) or
+                                 (pth is not None and want is not None and np.array_equal(pth, want)))
+                res["speedup"] = round(res[names[1]]["ms_per_search"] / res[names[0]]["ms_per_search"], 2)
+                res["mean_roi_nodes"] = int(np.mean([len(r) for r in rois]))
+                res["identical_paths"] = bool(same)
+                res["identical_to_oracle"] = bool(ok)
+                row[shape] = res
+                dg.close()
+            out[name] = row
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    out["workload"] = (f"{nsamp} BFS-ROI searches per board (reference radius rule, <= 50 000 nodes), "
+                       f"synchronous calls; oracle checked on {ncheck}")
+    return out
+
+
 def route_c1(dev, with_cpu: bool):
     """The 100x100x4 board (200 two-pin nets, pins uniform on the top
     layer, seeded) routed to zero overuse with per-net live costs, offenders
@@ -763,6 +859,7 @@ def run_ours(args, world, rank, local):
         routing = {"c1": route_c1(dev, with_cpu=with_cpu)}
         if world == 1:
             routing["dropin"] = route_dropin(dev, with_cpu=with_cpu)
+            routing["roi_searches"] = roi_searches(dev)
             routing["c3"] = route_c3(dev, with_cpu=with_cpu)
     batch_sweep = sweep_c4(dev) if (world == 1 and not args.no_sweep) else None
     result = {
