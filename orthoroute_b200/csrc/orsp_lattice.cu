@@ -233,6 +233,7 @@ __device__ __forceinline__ LatBox load_box(const LatParams &p, int b) {
   B.ntx = __ldg(q + 6);
   B.nty = __ldg(q + 7);
   B.tile0 = __ldg(q + 8);
+  B.pad = __ldg(q + 9);
   B.dbase = __ldg((const long long *)(p.boxes + b) + 5);
   return B;
 }
