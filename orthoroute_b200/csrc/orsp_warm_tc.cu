@@ -7,15 +7,17 @@
 //     memory in the K-major canonical UMMA layout without swizzle (core
 //     matrices of 8 rows x 16 bytes, rows contiguous; the two 8-element halves
 //     of a 16-wide K slice 128 bytes apart, 8-row groups 256 bytes apart);
-//   - per tile and per input plane (dz) all 128 threads gather the nine
-//     (dy, dx) im2col blocks A[m][k] = X[z+dz][y+dy][x0+m+dx][k] in the same
-//     layout (16-byte loads, zero outside the grid, the optional ReLU mask
-//     applied on the way), fence them to the async proxy, and one thread
-//     issues the 9 x Cin/16 MMAs (K = 16 each) into the TMEM accumulator and
-//     commits them to an mbarrier;
-//   - the epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM
-//     lanes 32w..32w+31, i.e. voxels 32w..32w+31), adds the bias, applies the
-//     ReLU and stores bf16 or fp32.
+//   - per tile, nine stages (dz, dy): 256 threads copy one input row into
+//     the three (dx) im2col blocks A[m][k] = X[z+dz][y+dy][x0+m+dx][k] of a
+//     stage buffer in the same layout (cp.async, zero outside the grid; the
+//     optional ReLU mask through registers), and one thread issues the
+//     3 x Cin/16 MMAs (K = 16 each) into the TMEM accumulator and commits them
+//     to the buffer's mbarrier, while the copies of the next stages are in
+//     flight (a ring of up to four buffers);
+//   - the epilogue reads the accumulator with tcgen05.ld (warps w and w + 4
+//     share TMEM lanes 32 (w % 4) .., i.e. those voxels, and split the output
+//     channels), adds the bias, applies the ReLU and stores bf16 or fp32.
+// The weight gradient (wgrad_tc_kernel) is a second tcgen05 GEMM.
 // Every mbarrier wait is bounded by the global timer; on expiry the kernel
 // records an error, waits once more (bounded) for its MMAs, frees its TMEM
 // and returns.  Single-GPU code: no TMA, no multicast.
@@ -105,29 +107,70 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// Bytes of shared memory for Cin, Cout: all weights, nine im2col blocks of
-// one plane, the mbarrier and the TMEM address slot.
-__host__ __device__ constexpr size_t tc_smem_bytes(int Cin, int Cout) {
-  return static_cast<size_t>(27) * (Cin / 16) * Cout * 32 + static_cast<size_t>(9) * (Cin / 16) * 4096 + 64;
+// Shared memory of the convolution: all weights (27 taps x Cin/16 K slices
+// x Cout rows of 32 bytes), NS stage buffers (3 taps x Cin/16 blocks of
+// 4096 bytes), NS mbarriers and the TMEM address slot.
+__host__ __device__ constexpr size_t cv_weight_bytes(int Cin, int Cout) {
+  return static_cast<size_t>(27) * (Cin / 16) * Cout * 32;
+}
+__host__ __device__ constexpr size_t cv_stage_bytes(int Cin) { return static_cast<size_t>(3) * (Cin / 16) * 4096; }
+__host__ __device__ constexpr size_t cv_smem_bytes(int Cin, int Cout, int ns) {
+  return cv_weight_bytes(Cin, Cout) + ns * cv_stage_bytes(Cin) + 8 * ns + 64;
+}
+// Stage buffers that fit beside the weights in 200 KB (at most 4; 0 when
+// fewer than 2 fit).
+inline int cv_stages(int Cin, int Cout) {
+  const size_t budget = 200 * 1024;
+  const size_t w = cv_weight_bytes(Cin, Cout), sb = cv_stage_bytes(Cin);
+  if (w + 2 * sb + 8 * 2 + 64 > budget) return 0;
+  int ns = 2;
+  while (ns < 4 && cv_smem_bytes(Cin, Cout, ns + 1) <= budget) ++ns;
+  return ns;
 }
 
-__global__ void __launch_bounds__(TC_THREADS, 1) conv3d_tc_kernel(
+// 16-byte global -> shared copy that fills zeros when `bytes` is 0.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, int bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Waits until at most n (0..2) of this thread's copy groups are pending.
+__device__ __forceinline__ void cp_async_wait(int n) {
+  if (n <= 0) asm volatile("cp.async.wait_group 0;" ::: "memory");
+  else if (n == 1) asm volatile("cp.async.wait_group 1;" ::: "memory");
+  else asm volatile("cp.async.wait_group 2;" ::: "memory");
+}
+
+constexpr int CV_THREADS = 256;  // eight warps gather; warps w and w + 4 share TMEM lanes 32 (w % 4)..
+
+// Pipelined implicit GEMM.  A stage is one input row (plane z + dz, row
+// y + dy) of a tile: the 130 voxels x0 - 1 .. x0 + 128 are read once, 16
+// bytes at a time with cp.async (zero fill outside the grid), and written to
+// the three shifted im2col blocks of the taps dx = -1, 0, 1 (row m of tap dx
+// holds voxel x0 + m + dx).  Stages run through a ring of NS buffers: while
+// the tensor core consumes stage s, the copies of stages s + 1 .. s + NS - 1
+// are in flight.  Buffer b's mbarrier completes when the MMAs of the stage
+// last held in b are done (tcgen05.commit), which is what a refill of b waits
+// for; the 9th stage of a tile also releases the epilogue.  With the ReLU
+// mask the gather goes through registers (plain loads and shared stores).
+__global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
     const __nv_bfloat16 *__restrict__ X, const __nv_bfloat16 *__restrict__ Mk, const __nv_bfloat16 *__restrict__ Wt,
     const float *__restrict__ bias, __nv_bfloat16 *__restrict__ Y, float *__restrict__ Yf, int D, int H, int W,
-    int Cin, int Cout, int relu) {
+    int Cin, int Cout, int relu, int NS) {
   extern __shared__ __align__(1024) unsigned char sm[];
-  const int KC = Cin >> 4;
+  const int KC = Cin >> 4, CG = Cin >> 3;
   const int bblk = Cout * 32;  // bytes of one (tap, 16-wide K slice) weight block
+  const size_t SBY = cv_stage_bytes(Cin);
   unsigned char *sB = sm;
-  unsigned char *sA = sm + static_cast<size_t>(27) * KC * bblk;
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sA + static_cast<size_t>(9) * KC * 4096);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+  unsigned char *sA = sm + cv_weight_bytes(Cin, Cout);
+  unsigned long long *bars = reinterpret_cast<unsigned long long *>(sA + NS * SBY);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + NS);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t ncols = Cout <= 32 ? 32u : 64u;
 
   // weights: one 16-byte unit = 8 consecutive k of one n
   const int units_per_tap = Cin * Cout / 8;
-  for (int i = tid; i < 27 * units_per_tap; i += TC_THREADS) {
+  for (int i = tid; i < 27 * units_per_tap; i += CV_THREADS) {
     const int tap = i / units_per_tap, r = i - tap * units_per_tap;
     const int kg = r / Cout, n = r - kg * Cout;  // kg: 8-element group of k
     const __nv_bfloat16 *src = Wt + (static_cast<int64_t>(tap) * Cin + kg * 8) * Cout + n;
@@ -142,7 +185,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) conv3d_tc_kernel(
     *reinterpret_cast<uint4 *>(dst) = make_uint4(v[0], v[1], v[2], v[3]);
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    for (int b = 0; b < NS; ++b)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bars + b)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -157,31 +201,42 @@ __global__ void __launch_bounds__(TC_THREADS, 1) conv3d_tc_kernel(
   tc_fence_after();
   const uint32_t tmem = *tslot;
   const uint32_t idesc = umma_idesc_bf16(TC_M, Cout);
-  const uint32_t bar_a = smem_addr(bar);
-  uint32_t phase = 0;
-  bool ok = true;
 
   const int ntx = (W + TC_M - 1) / TC_M;
   const int64_t ntiles = static_cast<int64_t>(D) * H * ntx;
-  for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-    const int tx = static_cast<int>(t % ntx);
-    const int64_t zy = t / ntx;
-    const int y = static_cast<int>(zy % H), z = static_cast<int>(zy / H);
-    const int x0 = tx * TC_M;
-    for (int dzi = 0; dzi < 3 && ok; ++dzi) {
-      const int zz = z + dzi - 1;
-      const bool zok = zz >= 0 && zz < D;
-      // im2col blocks of the nine (dy, dx) taps of plane zz: unit = 8
-      // channels of one voxel; consecutive threads take consecutive voxels
-      for (int i = tid; i < 9 * KC * TC_M * 2; i += TC_THREADS) {
-        const int kh = i & 1, m = (i >> 1) & (TC_M - 1), rest = i >> 8;
-        const int kc = rest % KC, tap9 = rest / KC;
-        const int yy = y + tap9 / 3 - 1, xx = x0 + m + tap9 % 3 - 1;
-        uint4 v = make_uint4(0, 0, 0, 0);
-        if (zok && yy >= 0 && yy < H && xx >= 0 && xx < W && x0 + m < W) {
-          const int64_t off = ((static_cast<int64_t>(zz) * H + yy) * W + xx) * Cin + kc * 16 + kh * 8;
-          v = *reinterpret_cast<const uint4 *>(X + off);
-          if (Mk) {
+  const int64_t my_tiles = ntiles > blockIdx.x ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const int64_t nst = my_tiles * 9;
+
+  // copies of stage s into buffer s % NS (nothing past the last stage); one
+  // commit group per call on every thread, so the group counts stay uniform
+  auto issue = [&](int64_t s) {
+    if (s < nst) {
+      const int64_t t = blockIdx.x + (s / 9) * static_cast<int64_t>(gridDim.x);
+      const int st9 = static_cast<int>(s % 9);
+      const int tx = static_cast<int>(t % ntx);
+      const int64_t zy = t / ntx;
+      const int y = static_cast<int>(zy % H), z = static_cast<int>(zy / H);
+      const int zz = z + st9 / 3 - 1, yy = y + st9 % 3 - 1, x0 = tx * TC_M;
+      const bool rowok = zz >= 0 && zz < D && yy >= 0 && yy < H;
+      unsigned char *buf = sA + static_cast<size_t>(s % NS) * SBY;
+      for (int i = tid; i < (TC_M + 2) * CG; i += CV_THREADS) {
+        const int vx = i / CG, cg = i - vx * CG;
+        const int xx = x0 - 1 + vx;
+        const bool in = rowok && xx >= 0 && xx < W;
+        const int64_t off = in ? ((static_cast<int64_t>(zz) * H + yy) * W + xx) * Cin + cg * 8 : 0;
+        const int kc = cg >> 1, kh = cg & 1;
+        if (!Mk) {
+#pragma unroll
+          for (int dxi = 0; dxi < 3; ++dxi) {
+            const int m = vx - dxi;
+            if (m >= 0 && m < TC_M)
+              cp_async16(buf + (dxi * KC + kc) * 4096 + (m >> 3) * 256 + kh * 128 + (m & 7) * 16, X + off,
+                         in ? 16 : 0);
+          }
+        } else {
+          uint4 v = make_uint4(0, 0, 0, 0);
+          if (in) {
+            v = *reinterpret_cast<const uint4 *>(X + off);
             const uint4 mk = *reinterpret_cast<const uint4 *>(Mk + off);
             __nv_bfloat16 *pv = reinterpret_cast<__nv_bfloat16 *>(&v);
             const __nv_bfloat16 *pm = reinterpret_cast<const __nv_bfloat16 *>(&mk);
@@ -189,70 +244,101 @@ __global__ void __launch_bounds__(TC_THREADS, 1) conv3d_tc_kernel(
             for (int q = 0; q < 8; ++q)
               if (!(__bfloat162float(pm[q]) > 0.0f)) pv[q] = __float2bfloat16(0.0f);
           }
-        }
-        unsigned char *dst = sA + (tap9 * KC + kc) * 4096 + (m >> 3) * 256 + kh * 128 + (m & 7) * 16;
-        *reinterpret_cast<uint4 *>(dst) = v;
-      }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      tc_fence_before();
-      __syncthreads();
-      tc_fence_after();
-      if (tid == 0) {
-        for (int tap9 = 0; tap9 < 9; ++tap9)
-          for (int kc = 0; kc < KC; ++kc) {
-            const uint64_t a = umma_smem_desc(smem_addr(sA + (tap9 * KC + kc) * 4096), 128, 256);
-            const uint64_t b = umma_smem_desc(smem_addr(sB + ((dzi * 9 + tap9) * KC + kc) * bblk), 128, 256);
-            mma_bf16(tmem, a, b, idesc, (dzi | tap9 | kc) != 0 ? 1u : 0u);
+#pragma unroll
+          for (int dxi = 0; dxi < 3; ++dxi) {
+            const int m = vx - dxi;
+            if (m >= 0 && m < TC_M)
+              *reinterpret_cast<uint4 *>(buf + (dxi * KC + kc) * 4096 + (m >> 3) * 256 + kh * 128 + (m & 7) * 16) =
+                  v;
           }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_a)
-                     : "memory");
-      }
-      // the MMAs read the im2col blocks: wait before they are overwritten
-      // (the outcome is made uniform over the CTA, so that every thread
-      // takes the same path through the barriers and warp-wide TMEM loads)
-      ok = __syncthreads_and(mbar_wait(bar_a, phase) ? 1 : 0) != 0;
-      phase ^= 1u;
-      tc_fence_after();
-    }
-    if (!ok) break;
-    // epilogue: warp w holds voxels 32w..32w+31, one TMEM lane each
-    const int m = warp * 32 + lane, xx = x0 + m;
-    for (int c0 = 0; c0 < Cout; c0 += 16) {
-      uint32_t r[16];
-      tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0), r);
-      if (xx < W) {
-        const int64_t o = ((static_cast<int64_t>(z) * H + y) * W + xx) * Cout + c0;
-        float f[16];
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          float v = __uint_as_float(r[j]) + (bias ? bias[c0 + j] : 0.0f);
-          f[j] = relu ? fmaxf(v, 0.0f) : v;
-        }
-        if (Yf) {
-#pragma unroll
-          for (int j = 0; j < 16; j += 4)
-            *reinterpret_cast<float4 *>(Yf + o + j) = make_float4(f[j], f[j + 1], f[j + 2], f[j + 3]);
-        } else {
-          uint32_t p[8];
-#pragma unroll
-          for (int j = 0; j < 8; ++j)
-            p[j] = static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16(f[2 * j]))) |
-                   (static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16(f[2 * j + 1]))) << 16);
-          *reinterpret_cast<uint4 *>(Y + o) = make_uint4(p[0], p[1], p[2], p[3]);
-          *reinterpret_cast<uint4 *>(Y + o + 8) = make_uint4(p[4], p[5], p[6], p[7]);
         }
       }
     }
-    // the next tile's first MMA overwrites the accumulator
+    cp_async_commit();
+  };
+
+  for (int64_t s = 0; s < NS - 1; ++s) issue(s);
+  bool ok = true;
+  int64_t s = 0, issued = -1;  // issued: the last stage whose MMAs were committed
+  for (; s < nst; ++s) {
+    const int b = static_cast<int>(s % NS);
+    const int st9 = static_cast<int>(s % 9);
+    // this thread's copies of stage s have landed; hand them to the async
+    // proxy, then every thread's (and a failed wait anywhere ends the loop)
+    cp_async_wait(NS - 2);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
-    __syncthreads();
+    ok = __syncthreads_and(ok ? 1 : 0) != 0;
     tc_fence_after();
+    if (!ok) break;
+    if (tid == 0) {
+      const int tapz = (st9 / 3) * 9 + (st9 % 3) * 3;  // (dz, dy) part of the tap index
+#pragma unroll 1
+      for (int dxi = 0; dxi < 3; ++dxi)
+        for (int kc = 0; kc < KC; ++kc) {
+          const uint64_t a = umma_smem_desc(smem_addr(sA + b * SBY + (dxi * KC + kc) * 4096), 128, 256);
+          const uint64_t bd = umma_smem_desc(smem_addr(sB + ((tapz + dxi) * KC + kc) * bblk), 128, 256);
+          mma_bf16(tmem, a, bd, idesc, (st9 | dxi | kc) != 0 ? 1u : 0u);
+        }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_addr(bars + b))
+                   : "memory");
+    }
+    issued = s;
+    // refill the buffer of stage s - 1 with stage s + NS - 1 once its MMAs
+    // are done (for s = 0 that buffer has not been used yet)
+    if (s >= 1) ok = mbar_wait(smem_addr(bars + (s - 1) % NS), static_cast<uint32_t>(((s - 1) / NS) & 1));
+    issue(s + NS - 1);
+    if (st9 == 8) {
+      // last stage of the tile: the accumulator is final once its MMAs are
+      ok = __syncthreads_and((ok && mbar_wait(smem_addr(bars + b), static_cast<uint32_t>((s / NS) & 1))) ? 1 : 0) != 0;
+      if (!ok) break;
+      tc_fence_after();
+      const int64_t t = blockIdx.x + (s / 9) * static_cast<int64_t>(gridDim.x);
+      const int tx = static_cast<int>(t % ntx);
+      const int64_t zy = t / ntx;
+      const int y = static_cast<int>(zy % H), z = static_cast<int>(zy / H);
+      // warp w: voxels 32 (w % 4) .. + 31 (its TMEM lanes), channel blocks
+      // of 16 starting at 16 (w / 4), every second one
+      const int m = (warp & 3) * 32 + lane, xx = tx * TC_M + m;
+      for (int c0 = (warp >> 2) * 16; c0 < Cout; c0 += 32) {
+        uint32_t r[16];
+        tmem_ld16(tmem + (static_cast<uint32_t>((warp & 3) * 32) << 16) + static_cast<uint32_t>(c0), r);
+        if (xx < W) {
+          const int64_t o = ((static_cast<int64_t>(z) * H + y) * W + xx) * Cout + c0;
+          float f[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const float v = __uint_as_float(r[j]) + (bias ? bias[c0 + j] : 0.0f);
+            f[j] = relu ? fmaxf(v, 0.0f) : v;
+          }
+          if (Yf) {
+#pragma unroll
+            for (int j = 0; j < 16; j += 4)
+              *reinterpret_cast<float4 *>(Yf + o + j) = make_float4(f[j], f[j + 1], f[j + 2], f[j + 3]);
+          } else {
+            uint32_t p[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              p[j] = static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16(f[2 * j]))) |
+                     (static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16(f[2 * j + 1]))) << 16);
+            *reinterpret_cast<uint4 *>(Y + o) = make_uint4(p[0], p[1], p[2], p[3]);
+            *reinterpret_cast<uint4 *>(Y + o + 8) = make_uint4(p[4], p[5], p[6], p[7]);
+          }
+        }
+      }
+      // the next tile's first MMA overwrites the accumulator: these loads
+      // are ordered before it by the next iteration's barrier
+      tc_fence_before();
+    }
   }
+  cp_async_wait(0);
   if (!ok) {
-    // a wait expired: record it and give the MMAs in flight one more bounded
-    // wait before the accumulator is freed
+    // a wait expired: record it and give the MMAs in flight one more
+    // bounded wait (the last stage committed, which completes after all
+    // earlier ones) before the accumulator is freed
     if (tid == 0) atomicExch(&g_tc_err, 1);
-    mbar_wait(bar_a, phase ^ 1u);
+    if (issued >= 0) mbar_wait(smem_addr(bars + issued % NS), static_cast<uint32_t>((issued / NS) & 1));
   }
   tc_fence_before();
   __syncthreads();
@@ -443,20 +529,21 @@ extern "C" int orsp_warm_conv3d_tc(const void *X, const void *mask, const void *
     set_error("warm_conv3d_tc: bad arguments (Cin, Cout multiples of 16, Cout <= 64)");
     return ORSP_ERR_ARG;
   }
-  const size_t smem = tc_smem_bytes(Cin, Cout);
-  if (smem > 227 * 1024) {
-    set_error("warm_conv3d_tc: weights of this Cin x Cout do not fit in shared memory");
+  const int ns = cv_stages(Cin, Cout);
+  if (ns < 2) {
+    set_error("warm_conv3d_tc: weights of this Cin x Cout and two stages do not fit in shared memory");
     return ORSP_ERR_ARG;
   }
+  const size_t smem = cv_smem_bytes(Cin, Cout, ns);
   int dev = 0, sms = 0;
   ORSP_CUDA(cudaGetDevice(&dev));
   ORSP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   ORSP_CUDA(cudaFuncSetAttribute(conv3d_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t ntiles = static_cast<int64_t>(D) * H * ((W + TC_M - 1) / TC_M);
   const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(ntiles, sms)));
-  conv3d_tc_kernel<<<grid, TC_THREADS, smem, (cudaStream_t)stream>>>(
+  conv3d_tc_kernel<<<grid, CV_THREADS, smem, (cudaStream_t)stream>>>(
       (const __nv_bfloat16 *)X, (const __nv_bfloat16 *)mask, (const __nv_bfloat16 *)Wt, bias,
-      (__nv_bfloat16 *)Y, Yf, D, H, W, Cin, Cout, relu);
+      (__nv_bfloat16 *)Y, Yf, D, H, W, Cin, Cout, relu, ns);
   ORSP_CUDA(cudaGetLastError());
   return ORSP_OK;
 }
