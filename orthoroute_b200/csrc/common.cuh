@@ -160,6 +160,7 @@ struct LatOptions {
   bool fill_box_only = false;  // reset distances inside the boxes only (the caller's backtrace checks the box)
   bool copy_ctl = true;        // copy the control block to the pinned mirror (finish_lattice_search)
   int *err_d = nullptr;        // out: device address of the launch's error word
+  int blocks_per_sm = 0;       // CTAs per SM (0: one); ORSP_LAT_BLOCKS_PER_SM overrides
   int64_t tma_slices = 0;      // > 0: every box is the whole lattice, box j's distances in slice j of N
                                // cells from `dist` (LatBox.pad = j); allows the TMA staging
 };

@@ -1339,7 +1339,7 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   const bool spec = async && env_u64("ORSP_LAT_SPEC", 0) != 0;
   // ORSP_LAT_BLOCKS_PER_SM: CTAs per SM (tiles of up to 12 layers at width
   // 16 have an instantiation sized for 2)
-  const int want = (int)env_u64("ORSP_LAT_BLOCKS_PER_SM", 1);
+  const int want = (int)env_u64("ORSP_LAT_BLOCKS_PER_SM", (opt && opt->blocks_per_sm > 0) ? opt->blocks_per_sm : 1);
   // ORSP_LAT_TMA=1: tensor-load staging of fresh visits, for whole-lattice
   // boxes (opt->tma_slices: distance slices of N cells, box j in slice j)
   CUtensorMap tmw{}, tmd{};
