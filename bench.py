@@ -51,12 +51,13 @@ NSRC = 64
 PER_LAUNCH = 16
 BLOCKED = 0.05
 SEED = 20261203
-# DRAM bytes (read + write) per lattice node of one lattice_async_kernel launch,
-# from ncu (dram__bytes_read.sum + dram__bytes_write.sum) on one full search of
-# a 600x600x12 lattice: 95.78 MB for 4.32 M nodes.  The search settles every
-# node, and its traffic is the gathered weights plus the distances read once,
-# so it scales with the node count.
-LAT_DRAM_BYTES_PER_NODE = 94.55e6 / (600 * 600 * 12)
+# DRAM bytes (read + write) per lattice node and source of lattice_async_kernel
+# in a many-source launch, from ncu (dram__bytes_read.sum + dram__bytes_write.sum)
+# on a 4-source launch of the 1000x1000x12 lattice: 826.78 + 181.27 MB for
+# 4 x 12.0 M node-sources.  Every search settles every node; the traffic is
+# the distance slices read and written about once plus the shared weights, so
+# it grows with the sources per launch.
+LAT_DRAM_BYTES_PER_NODE = (826.783488e6 + 181.271296e6) / (4 * 1000 * 1000 * 12)
 
 
 def _peaks():
@@ -895,7 +896,7 @@ def run_ours(args, world, rank, local):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 5),
                      "traffic": int(LAT_DRAM_BYTES_PER_NODE * lat.N * srcs_per_launch),
-                     "traffic_source": "ncu dram bytes of a 600x600x12 launch, scaled by node count",
+                     "traffic_source": "ncu dram bytes of a 4-source launch of this lattice, scaled by sources per launch",
                      "kernel": "lattice_async_kernel", "peak_kind": peak_kind,
                      "bytes_per_launch": int(bytes_per_launch),
                      "avg_launch_ms": round(avg_kernel_ms, 4)},
