@@ -959,6 +959,30 @@ def run_reference(args, world, rank, local):
     }
 
 
+def profile_case(args):
+    """A small case of the timed kernel for ncu captures: the bench lattice
+    and weights, three orsp_sssp_sources launches of --per-launch new sources
+    each (capture the third: -k regex:lattice_async -s 2 -c 1).  Prints one
+    line; no timing."""
+    import torch
+
+    from orthoroute_b200.build import build_library
+    from orthoroute_b200.solver import DeviceGraph
+
+    build_library()
+    per = max(1, args.per_launch)
+    lat, w, sources = make_workload(SEED, args.nx, args.ny, args.nz, 3 * per)
+    dev = torch.device("cuda", 0)
+    dg = DeviceGraph.from_lattice(lat, device=dev)
+    wt = torch.from_numpy(w).to(dev)
+    dist = torch.empty(per, lat.N, dtype=torch.float32, device=dev)
+    for k in range(3):
+        dg.sssp_sources(wt, sources[k * per:(k + 1) * per], dist, per_launch=per, cost_generation=1)
+    torch.cuda.synchronize(dev)
+    print(json.dumps({"profile_case": f"{args.nx}x{args.ny}x{args.nz}", "launches": 3, "sources_per_launch": per,
+                      "settled_last_row": int(torch.isfinite(dist[-1]).sum().item())}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -975,7 +999,12 @@ def main():
     ap.add_argument("--no-check", action="store_true", help="skip the parity check before timing")
     ap.add_argument("--no-route", action="store_true", help="skip the routing measurements")
     ap.add_argument("--no-sweep", action="store_true", help="skip the batched uneven-ROI sweep")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run three --per-launch source launches for an ncu capture and exit")
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args)
+        return
     world, rank, local = dist_setup()
     try:
         if args.impl == "reference":
