@@ -219,8 +219,14 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
       const int zz = z + st9 / 3 - 1, yy = y + st9 % 3 - 1, x0 = tx * TC_M;
       const bool rowok = zz >= 0 && zz < D && yy >= 0 && yy < H;
       unsigned char *buf = sA + static_cast<size_t>(s % NS) * SBY;
-      for (int i = tid; i < (TC_M + 2) * CG; i += CV_THREADS) {
-        const int vx = i / CG, cg = i - vx * CG;
+      // unit i: groups of 8 voxels x CG channel groups, channel-group major
+      // inside a group, so the 8 lanes of a 16-byte store phase write 8
+      // consecutive rows of one core-matrix column (128 contiguous bytes,
+      // no bank conflict) while a warp still reads 512 contiguous bytes
+      for (int i = tid; i < ((TC_M + 2 + 7) / 8) * 8 * CG; i += CV_THREADS) {
+        const int grp = i / (8 * CG), r8 = i - grp * 8 * CG;
+        const int cg = r8 >> 3, vx = grp * 8 + (r8 & 7);
+        if (vx >= TC_M + 2) continue;
         const int xx = x0 - 1 + vx;
         const bool in = rowok && xx >= 0 && xx < W;
         const int64_t off = in ? ((static_cast<int64_t>(zz) * H + yy) * W + xx) * Cin + cg * 8 : 0;
