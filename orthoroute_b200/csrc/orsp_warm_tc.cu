@@ -22,6 +22,7 @@
 // records an error, waits once more (bounded) for its MMAs, frees its TMEM
 // and returns.  Single-GPU code: no TMA, no multicast.
 #include <algorithm>
+#include <climits>
 #include <cstdint>
 
 #include <cuda_bf16.h>
@@ -153,12 +154,15 @@ constexpr int CV_THREADS = 256;  // eight warps gather; warps w and w + 4 share 
 // last held in b are done (tcgen05.commit), which is what a refill of b waits
 // for; the 9th stage of a tile also releases the epilogue.  With the ReLU
 // mask the gather goes through registers (plain loads and shared stores).
+// CG = Cin / 8 (2, 4 or 8), a template parameter so that the gather's unit
+// arithmetic is resolved at compile time.
+template <int CG>
 __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
     const __nv_bfloat16 *__restrict__ X, const __nv_bfloat16 *__restrict__ Mk, const __nv_bfloat16 *__restrict__ Wt,
     const float *__restrict__ bias, __nv_bfloat16 *__restrict__ Y, float *__restrict__ Yf, int D, int H, int W,
     int Cin, int Cout, int relu, int NS) {
   extern __shared__ __align__(1024) unsigned char sm[];
-  const int KC = Cin >> 4, CG = Cin >> 3;
+  const int KC = Cin >> 4;
   const int bblk = Cout * 32;  // bytes of one (tap, 16-wide K slice) weight block
   const size_t SBY = cv_stage_bytes(Cin);
   unsigned char *sB = sm;
@@ -209,6 +213,36 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
 
   // copies of stage s into buffer s % NS (nothing past the last stage); one
   // commit group per call on every thread, so the group counts stay uniform
+  // This thread's share of a stage is the same for every stage: units
+  // u = tid + j * CV_THREADS of (groups of 8 voxels) x CG channel groups,
+  // channel-group major inside a group, so the 8 lanes of a 16-byte store
+  // phase write 8 consecutive rows of one core-matrix column (128 contiguous
+  // bytes, no bank conflict) while a warp reads 512 contiguous bytes.  Per
+  // unit: x offset from x0, element offset in the row and the three tap
+  // destinations (-1 where the shifted row falls outside the tile).
+  constexpr int CIN = CG * 8, KCC = CG / 2;
+  constexpr int UNITS = (TC_M + 2 + 7) / 8 * 8 * CG;
+  constexpr int UPT = (UNITS + CV_THREADS - 1) / CV_THREADS;
+  int u_x[UPT], u_off[UPT], u_dst[UPT][3];
+#pragma unroll
+  for (int j = 0; j < UPT; ++j) {
+    const int i = tid + j * CV_THREADS;
+    const int grp = i / (8 * CG), r8 = i % (8 * CG);
+    const int cg = r8 >> 3, vx = grp * 8 + (r8 & 7);
+    const bool unit = i < UNITS && vx < TC_M + 2;
+    u_x[j] = unit ? vx - 1 : INT_MIN / 2;
+    u_off[j] = (vx - 1) * CIN + cg * 8;
+#pragma unroll
+    for (int dxi = 0; dxi < 3; ++dxi) {
+      const int m = vx - dxi;
+      u_dst[j][dxi] = (unit && m >= 0 && m < TC_M)
+                          ? (dxi * KCC + (cg >> 1)) * 4096 + (m >> 3) * 256 + (cg & 1) * 128 + (m & 7) * 16
+                          : -1;
+    }
+  }
+
+  // copies of stage s into buffer s % NS (nothing past the last stage); one
+  // commit group per call on every thread, so the group counts stay uniform
   auto issue = [&](int64_t s) {
     if (s < nst) {
       const int64_t t = blockIdx.x + (s / 9) * static_cast<int64_t>(gridDim.x);
@@ -219,31 +253,21 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
       const int zz = z + st9 / 3 - 1, yy = y + st9 % 3 - 1, x0 = tx * TC_M;
       const bool rowok = zz >= 0 && zz < D && yy >= 0 && yy < H;
       unsigned char *buf = sA + static_cast<size_t>(s % NS) * SBY;
-      // unit i: groups of 8 voxels x CG channel groups, channel-group major
-      // inside a group, so the 8 lanes of a 16-byte store phase write 8
-      // consecutive rows of one core-matrix column (128 contiguous bytes,
-      // no bank conflict) while a warp still reads 512 contiguous bytes
-      for (int i = tid; i < ((TC_M + 2 + 7) / 8) * 8 * CG; i += CV_THREADS) {
-        const int grp = i / (8 * CG), r8 = i - grp * 8 * CG;
-        const int cg = r8 >> 3, vx = grp * 8 + (r8 & 7);
-        if (vx >= TC_M + 2) continue;
-        const int xx = x0 - 1 + vx;
+      const __nv_bfloat16 *row = X + ((static_cast<int64_t>(rowok ? zz : 0) * H + (rowok ? yy : 0)) * W + x0) * CIN;
+#pragma unroll
+      for (int j = 0; j < UPT; ++j) {
+        const int xx = x0 + u_x[j];
         const bool in = rowok && xx >= 0 && xx < W;
-        const int64_t off = in ? ((static_cast<int64_t>(zz) * H + yy) * W + xx) * Cin + cg * 8 : 0;
-        const int kc = cg >> 1, kh = cg & 1;
+        const __nv_bfloat16 *src = in ? row + u_off[j] : X;
         if (!Mk) {
 #pragma unroll
-          for (int dxi = 0; dxi < 3; ++dxi) {
-            const int m = vx - dxi;
-            if (m >= 0 && m < TC_M)
-              cp_async16(buf + (dxi * KC + kc) * 4096 + (m >> 3) * 256 + kh * 128 + (m & 7) * 16, X + off,
-                         in ? 16 : 0);
-          }
+          for (int dxi = 0; dxi < 3; ++dxi)
+            if (u_dst[j][dxi] >= 0) cp_async16(buf + u_dst[j][dxi], src, in ? 16 : 0);
         } else {
           uint4 v = make_uint4(0, 0, 0, 0);
           if (in) {
-            v = *reinterpret_cast<const uint4 *>(X + off);
-            const uint4 mk = *reinterpret_cast<const uint4 *>(Mk + off);
+            v = *reinterpret_cast<const uint4 *>(src);
+            const uint4 mk = *reinterpret_cast<const uint4 *>(Mk + (src - X));
             __nv_bfloat16 *pv = reinterpret_cast<__nv_bfloat16 *>(&v);
             const __nv_bfloat16 *pm = reinterpret_cast<const __nv_bfloat16 *>(&mk);
 #pragma unroll
@@ -251,12 +275,8 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
               if (!(__bfloat162float(pm[q]) > 0.0f)) pv[q] = __float2bfloat16(0.0f);
           }
 #pragma unroll
-          for (int dxi = 0; dxi < 3; ++dxi) {
-            const int m = vx - dxi;
-            if (m >= 0 && m < TC_M)
-              *reinterpret_cast<uint4 *>(buf + (dxi * KC + kc) * 4096 + (m >> 3) * 256 + kh * 128 + (m & 7) * 16) =
-                  v;
-          }
+          for (int dxi = 0; dxi < 3; ++dxi)
+            if (u_dst[j][dxi] >= 0) *reinterpret_cast<uint4 *>(buf + u_dst[j][dxi]) = v;
         }
       }
     }
@@ -544,12 +564,19 @@ extern "C" int orsp_warm_conv3d_tc(const void *X, const void *mask, const void *
   int dev = 0, sms = 0;
   ORSP_CUDA(cudaGetDevice(&dev));
   ORSP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  ORSP_CUDA(cudaFuncSetAttribute(conv3d_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  void (*kfn)(const __nv_bfloat16 *, const __nv_bfloat16 *, const __nv_bfloat16 *, const float *, __nv_bfloat16 *,
+              float *, int, int, int, int, int, int, int) =
+      Cin == 16 ? conv3d_tc_kernel<2> : Cin == 32 ? conv3d_tc_kernel<4> : Cin == 64 ? conv3d_tc_kernel<8> : nullptr;
+  if (!kfn) {
+    set_error("warm_conv3d_tc: Cin must be 16, 32 or 64");
+    return ORSP_ERR_ARG;
+  }
+  ORSP_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t ntiles = static_cast<int64_t>(D) * H * ((W + TC_M - 1) / TC_M);
   const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(ntiles, sms)));
-  conv3d_tc_kernel<<<grid, CV_THREADS, smem, (cudaStream_t)stream>>>(
-      (const __nv_bfloat16 *)X, (const __nv_bfloat16 *)mask, (const __nv_bfloat16 *)Wt, bias,
-      (__nv_bfloat16 *)Y, Yf, D, H, W, Cin, Cout, relu, ns);
+  kfn<<<grid, CV_THREADS, smem, (cudaStream_t)stream>>>((const __nv_bfloat16 *)X, (const __nv_bfloat16 *)mask,
+                                                        (const __nv_bfloat16 *)Wt, bias, (__nv_bfloat16 *)Y, Yf, D, H,
+                                                        W, Cin, Cout, relu, ns);
   ORSP_CUDA(cudaGetLastError());
   return ORSP_OK;
 }
