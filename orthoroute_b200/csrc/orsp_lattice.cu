@@ -37,6 +37,19 @@ namespace {
 
 constexpr int MAX_CYCLES = 64;
 
+// Layer strides (floats) of a tile's shared arrays: distances with their
+// halo, (TY + 2) rows of TX + 3, and the interior arrays (weights, loaded
+// distances), TY rows of TX + 1, each padded to 8 (mod 16).  A warp's x- or
+// y-runs cover two layers of the same kind, which are two layers apart (H
+// and V layers alternate), so a layer offset of 2 x stride = 16 (mod 32)
+// puts the second layer's rows on the other half of the banks.
+__host__ __device__ constexpr int pad_8_mod_16(int v) { return v + ((8 - v % 16) + 16) % 16; }
+__host__ __device__ constexpr int tile_ps(int TX, int TY) { return pad_8_mod_16((TY + 2) * (TX + 3)); }
+__host__ __device__ constexpr int tile_wps(int TX, int TY) { return pad_8_mod_16(TY * (TX + 1)); }
+// Floats of shared memory per layer of a tile (distances, four weight
+// arrays, loaded distances).
+__host__ __device__ constexpr int tile_floats_per_layer(int TX, int TY) { return tile_ps(TX, TY) + 5 * tile_wps(TX, TY); }
+
 struct LatCtl {
   GridBarrier bar;
   int err;
@@ -450,8 +463,10 @@ __device__ __forceinline__ bool zrun(float *col, const float *wdn, const float *
 // improved values.  Called by all threads of the CTA.  Shared memory:
 // distances with a one-cell halo [nzb][TY+2][TX+3], then the interior in-edge
 // weights [4][nzb][TY][TX+1] and the interior distances as loaded
-// [nzb][TY][TX+1] (odd row strides: the row walks of the x-sweep and the
-// column walks of the y- and z-sweeps are bank-conflict free).
+// [nzb][TY][TX+1], layers tile_ps / tile_wps floats apart (odd row strides:
+// the row walks of the x-sweep and the column walks of the y- and z-sweeps
+// are bank-conflict free within a layer; the padded layer strides keep the
+// two layers of one warp apart).
 // The distances and in-edge weights of one tile column (cells s0 + z * PS /
 // w0 + z * WPS in shared memory) in blocks of ZB layers, each block's loads
 // all issued before its stores.
@@ -589,9 +604,9 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
   const int *s_hl = L.hl, *s_vl = L.vl;
   const int nh = L.nh, nv = L.nv;
   constexpr int SX = TX + 3;
-  constexpr int PS = (TY + 2) * SX;
+  constexpr int PS = tile_ps(TX, TY);
   constexpr int WSX = TX + 1;
-  constexpr int WPS = TY * WSX;
+  constexpr int WPS = tile_wps(TX, TY);
   const float INF_F = __int_as_float(0x7f800000);
   const int lt = t - B.tile0;
   const int tx = lt % B.ntx, ty = lt / B.ntx;
@@ -993,8 +1008,7 @@ __global__ void __launch_bounds__(TX * TY, MINB)
   const unsigned long long t_start = dev_globaltimer();
   TmaCtx tma{};
   if constexpr (TMA) {
-    constexpr int PS = (TY + 2) * (TX + 3), WPS = TY * (TX + 1);
-    const int64_t off = ((int64_t)p.nz * PS + 5 * (int64_t)p.nz * WPS + 31) & ~(int64_t)31;
+    const int64_t off = ((int64_t)p.nz * tile_floats_per_layer(TX, TY) + 31) & ~(int64_t)31;
     tma.tw = &tmw;
     tma.td = &tmd;
     tma.mbar = smem_addr(&s_mbar);
@@ -1329,7 +1343,7 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   if (async) ORSP_CUDA(cudaMemsetAsync(p.qslot, 0xff, (size_t)qcap * 4, st));
   lattice_seed_kernel<TX, TY><<<1, 256, 0, st>>>(p, nseeds, seeds, seed_cost);
   ORSP_CUDA(cudaGetLastError());
-  size_t smem = ((size_t)nzb * (TY + 2) * (TX + 3) + (size_t)5 * nzb * TY * (TX + 1)) * sizeof(float);
+  size_t smem = (size_t)nzb * tile_floats_per_layer(TX, TY) * sizeof(float);
   if (smem > 227 * 1024) {
     orsp::set_error("lattice search: too many layers for the shared-memory tile");
     return ORSP_ERR_ARG;
@@ -1350,7 +1364,7 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
       tma = encode_lattice_maps(g, p, TX, TY, nzb, opt->tma_slices, &tmw, &tmd);
   }
   if (tma) {
-    const size_t base = (((size_t)nzb * (TY + 2) * (TX + 3) + (size_t)5 * nzb * TY * (TX + 1)) + 31) & ~(size_t)31;
+    const size_t base = ((size_t)nzb * tile_floats_per_layer(TX, TY) + 31) & ~(size_t)31;
     smem = (base + (size_t)nzb * TY * TX * 4 + (size_t)nzb * (TY + 2) * (TX + 8)) * sizeof(float);
   }
   void *kfn;
@@ -1515,7 +1529,7 @@ int lattice_tile_w() { return env_u64("ORSP_LAT_TILE", 16) == 32 ? 32 : 16; }
 
 bool lattice_tile_fits(int nzb, int tile_w) {
   const int TX = tile_w ? tile_w : lattice_tile_w(), TY = 16;
-  const size_t smem = ((size_t)nzb * (TY + 2) * (TX + 3) + (size_t)5 * nzb * TY * (TX + 1)) * sizeof(float);
+  const size_t smem = (size_t)nzb * tile_floats_per_layer(TX, TY) * sizeof(float);
   return smem <= 227 * 1024;
 }
 
