@@ -1147,8 +1147,8 @@ __device__ void finish_visit(const LatParams &p, int t, const int *act) {
 // after the next handoff - so it never waits for work that only its own
 // finished tile would create.  The flags of visit k stay intact until visit
 // k + 2 starts, and the scheduler reads them before handoff k + 2.
-template <int TX, int TY, bool PRIV>
-__global__ void __launch_bounds__(TX * TY + 32, 1) lattice_spec_kernel(LatParams p) {
+template <int TX, int TY, bool PRIV, int MINB = 1>
+__global__ void __launch_bounds__(TX * TY + 32, MINB) lattice_spec_kernel(LatParams p) {
   constexpr int NW = TX * TY;
   extern __shared__ float sd[];
   __shared__ LayerLists s_layers;
@@ -1368,7 +1368,13 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
     smem = (base + (size_t)nzb * TY * TX * 4 + (size_t)nzb * (TY + 2) * (TX + 8)) * sizeof(float);
   }
   void *kfn;
-  if (spec) kfn = priv ? (void *)lattice_spec_kernel<TX, TY, true> : (void *)lattice_spec_kernel<TX, TY, false>;
+  if (spec) {
+    kfn = priv ? (void *)lattice_spec_kernel<TX, TY, true> : (void *)lattice_spec_kernel<TX, TY, false>;
+    if constexpr (TX == 16) {  // two CTAs per SM: the instantiation held to their register share
+      if (want >= 2 && nzb <= 12)
+        kfn = priv ? (void *)lattice_spec_kernel<TX, TY, true, 2> : (void *)lattice_spec_kernel<TX, TY, false, 2>;
+    }
+  }
   else if (async) {
     kfn = priv ? (void *)lattice_async_kernel<TX, TY, true> : (void *)lattice_async_kernel<TX, TY, false>;
     if constexpr (TX == 16) {  // deeper tiles: the instantiation with 18-layer column loads

@@ -152,7 +152,7 @@ def test_sssp_full_distances_bit_exact(shape, blocked, planar, impl, monkeypatch
             assert np.array_equal(_bits(dist.cpu().numpy()), _bits(ref_dist)), f"src {s} delta {delta}"
 
 
-@pytest.mark.parametrize("impl", ["lattice16", "lattice32", "lattice16-tma", "generic"])
+@pytest.mark.parametrize("impl", ["lattice16", "lattice32", "lattice16-tma", "lattice16-spec", "generic"])
 @pytest.mark.parametrize("shape,blocked,per_launch", [((60, 50, 6), 0.05, 0), ((33, 17, 12), 0.0, 3),
                                                       ((128, 96, 4), 0.03, 2), ((64, 40, 12), 0.02, 4)])
 def test_sssp_sources_distances_bit_exact(shape, blocked, per_launch, impl, monkeypatch):
