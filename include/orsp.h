@@ -94,9 +94,15 @@ ORSP_API int orsp_graph_csr(orsp_graph *g, const int32_t **indptr_d,
 ORSP_API int orsp_graph_max_degree(orsp_graph *g, int32_t *out);
 /* 1 when the graph was recognised as an H/V routing lattice (every edge a
  * unit step along its layer's axis or a via between adjacent layers, no
- * parallel edges): full-graph and box searches then use the tile sweeps and
- * orsp_route_nets is available.  0 otherwise.  (No reference counterpart:
- * the reference has one search path for every graph.) */
+ * parallel edges): full-graph, box and ROI searches then use the tile sweeps
+ * and orsp_route_nets is available.  2 for the same planar structure with
+ * column vias, as the reference's Lattice3D builds them (vias between any
+ * two layers of a column, up to two parallel edges each,
+ * unified_pathfinder.py:1136-1172, 1264-1276): single, ROI, multi-target and
+ * many-source searches use the tile sweeps with a per-column via pass;
+ * batched box searches take the one-CTA kernel and orsp_route_nets is not
+ * available.  0 otherwise.  (No reference counterpart: the reference has one
+ * search path for every graph.) */
 ORSP_API int orsp_graph_is_lattice(orsp_graph *g, int32_t *out);
 /* Deepest box (layers) that one shared-memory tile of the lattice search holds
  * at tile width tile_w (16 or 32; 0: the library's width).  Single and

@@ -131,7 +131,7 @@ def tune_batch(dg: DeviceGraph, cost: torch.Tensor, src: torch.Tensor, dst: torc
     s, d = src[pt].contiguous(), dst[pt].contiguous()
     b = torch.from_numpy(boxes[pick]).to(src.device)
     plans = {"default": None, "cta": [{"max_nodes": int(ub), **c} for ub, c in zip(bounds, cta_best)]}
-    if dg.is_lattice:
+    if getattr(dg, "lattice_kind", int(dg.is_lattice)) == 1:  # batched tile sweeps need adjacent-layer vias
         for cut in range(len(bounds)):
             for tw in (16, 32):
                 plans[f"sweeps>={cut}/tile{tw}"] = [

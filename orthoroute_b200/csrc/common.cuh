@@ -93,6 +93,14 @@ struct Graph {
   int8_t layer_axis[64] = {};     // 0: no planar edges, 1: x, 2: y
   int32_t *slot_eid = nullptr;    // [4][N] in-edge id per slot (-1 absent)
   float *wslot = nullptr;         // [N] float4: gathered in-edge weights per node, by slot
+  // column vias (the reference's Lattice3D: vias between any two layers of a
+  // column, up to two parallel edges each): slots 2 and 3 stay empty and
+  // every via in-edge of node v from layer za is in vcol_eid[(k * nz + za) * N
+  // + v] (k = 0, 1: the parallel edges, smaller id first, -1 absent); wcol
+  // [nz][N] holds the gathered weight, the smaller of the parallel edges'
+  bool cvia = false;
+  int32_t *vcol_eid = nullptr;
+  float *wcol = nullptr;
   void *lat_ws = nullptr;         // tile lists, stamps and control block
   size_t lat_ws_bytes = 0;
   void *lat_ctl_h = nullptr;      // pinned mirror of the control block

@@ -1,7 +1,9 @@
 // Predecessor walk on the H/V routing lattice.
 //
 // On the lattice every node v = (x, y, z) has at most four in-neighbours, one
-// per slot of the gathered in-edge weights w4[v] (orsp_lattice.cu):
+// per slot of the gathered in-edge weights w4[v] (orsp_lattice.cu), or, with
+// column vias, its two planar in-neighbours and one via from every other
+// layer of its column (LatWalkGeom::wcol):
 //   slot 0: the lower neighbour along the layer's axis (x-1 on H layers, y-1 on
 //           V layers), slot 1: the upper one (x+1 / y+1),
 //   slot 2: the via from below (z-1), slot 3: the via from above (z+1).
@@ -23,6 +25,11 @@ namespace orsp {
 struct LatWalkGeom {
   int32_t nx, ny, nz;
   int8_t axis[64];  // 1: x moves (H layer), 2: y moves (V layer), 0: none
+  // column vias (the reference's Lattice3D): a node's via in-edges come from
+  // every layer of its column, with weights wcol[v * nzp + za] (slots 2 and 3
+  // are empty); NULL on a lattice with adjacent vias only
+  const float *wcol = nullptr;
+  int32_t nzp = 0;
 };
 
 // Rank of a node for the tie-break: its id.
@@ -98,6 +105,32 @@ __device__ __forceinline__ int lat_parent(const LatWalkGeom &G, const LatBox &B,
       bs = s;
     }
   }
+  if (G.wcol) {
+    // column vias: a parent in any other layer of the box in this column
+    // (slot 4 + its layer)
+    const float *wr = G.wcol + v * G.nzp;
+    for (int32_t za = B.z0; za <= B.z1; ++za) {
+      if (za == z) continue;
+      const float w = __ldg(&wr[za]);
+      if (!(w < __int_as_float(0x7f800000))) continue;
+      const unsigned d = dist(x, y, za);
+      if (d == ORSP_INF_BITS || f_bits(__fadd_rn(bits_f(d), w)) != dv) continue;
+      const int64_t ru = rank(((int64_t)za * G.ny + y) * G.nx + x);
+      if (!(d < dv || (d == dv && ru < rank(v)))) continue;
+      const unsigned long long key = ((unsigned long long)d << 32) | (unsigned long long)(uint32_t)ru;
+      if (key < best) {
+        best = key;
+        bs = 4 + za;
+      }
+    }
+    if (bs >= 4) {
+      px = x;
+      py = y;
+      pz = bs - 4;
+      pdu = (unsigned)(best >> 32);
+      return bs;
+    }
+  }
   if (bs >= 0) {
     px = ux[bs];
     py = uy[bs];
@@ -120,8 +153,10 @@ __device__ __forceinline__ bool lat_run_cell(const LatWalkGeom &G, const LatBox 
     if (G.axis[z] == 1) cx += d;
     else if (G.axis[z] == 2) cy += d;
     else if (i) return false;
-  } else {
+  } else if (s < 4) {
     cz += s == 2 ? -i : i;
+  } else if (i) {
+    return false;  // a column via (slot 4 + layer) is a single step
   }
   return cx >= B.x0 && cx <= B.x1 && cy >= B.y0 && cy <= B.y1 && cz >= B.z0 && cz <= B.z1;
 }

@@ -825,7 +825,7 @@ static int run_batch(orsp_graph *g, const float *cost_d, int32_t K, const int32_
   for (int tw : {16, 32}) {
     std::vector<int32_t> lat_items;
     for (int i = 0; i < nb; ++i)
-      if (tuned && g->plan_impl[i] == 1 && g->lattice_ok && g->plan_tile[i] == tw)
+      if (tuned && g->plan_impl[i] == 1 && g->lattice_ok && !g->cvia && g->plan_tile[i] == tw)
         for (int32_t k : bucket[i])
           if (tile_ok(k, tw)) lat_items.push_back(k);
     if (lat_items.empty()) continue;
@@ -842,7 +842,7 @@ static int run_batch(orsp_graph *g, const float *cost_d, int32_t K, const int32_
   }
   for (int i = 0; i < nb; ++i) {
     std::vector<int32_t> items;
-    if (tuned && g->plan_impl[i] == 1 && g->lattice_ok) {
+    if (tuned && g->plan_impl[i] == 1 && g->lattice_ok && !g->cvia) {
       for (int32_t k : bucket[i])
         if (!tile_ok(k, g->plan_tile[i])) items.push_back(k);
     } else {

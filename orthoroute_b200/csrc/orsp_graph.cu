@@ -237,6 +237,6 @@ extern "C" int orsp_graph_max_degree(orsp_graph *g, int32_t *out) {
 
 extern "C" int orsp_graph_is_lattice(orsp_graph *g, int32_t *out) {
   if (!g || !out) { set_error("NULL argument"); return ORSP_ERR_ARG; }
-  *out = g->lattice_ok ? 1 : 0;
+  *out = g->lattice_ok ? (g->cvia ? 2 : 1) : 0;
   return ORSP_OK;
 }

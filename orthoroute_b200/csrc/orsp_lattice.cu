@@ -84,6 +84,9 @@ struct LatParams {
   unsigned long long wait_ns, budget_ns;
   int selfcont;
   const int32_t *roi_map;  // node-set ROI searches: seeds outside it are ignored
+  const float *wcol;       // column vias: gathered via weights [N][nzp] (Graph::wcol)
+  int32_t nzp;             // nz rounded up to 4
+  int64_t N;
 };
 
 __global__ void fill_kernel(uint32_t *p, int64_t n, uint32_t v) {
@@ -231,6 +234,45 @@ __global__ void gather_roi_kernel(const int32_t *__restrict__ slot_eid, const fl
       o[k] = ok ? __ldg(&cost[e]) : INF_F;
     }
     w[v] = make_float4(o[0], o[1], o[2], o[3]);
+  }
+}
+
+// Column-via weights of the nodes of a box (column vias, Graph::cvia):
+// wcol[v * nzp + za] (nzp = nz rounded up to 4) = the smaller cost of the (up to two) parallel vias from
+// layer za of v's column into v, for every layer za of the box; +inf where
+// there is none, where u or v lies outside the ROI (roi_map < 0; NULL: no
+// restriction) or u is a sink (sink[u] != 0; NULL: none).  The box is read
+// from device memory (bx) or given by value (bx NULL).
+__global__ void gather_col_kernel(const int32_t *__restrict__ vcol_eid, const float *__restrict__ cost,
+                                  float *__restrict__ wcol, int64_t n, int32_t nx, int32_t ny, int32_t nz, int32_t nzp,
+                                  const LatBox *__restrict__ bx, LatBox bv, const int32_t *__restrict__ roi_map,
+                                  const uint8_t *__restrict__ sink) {
+  const float INF_F = __int_as_float(0x7f800000);
+  const LatBox B = bx ? *bx : bv;
+  const int64_t bw = B.x1 - B.x0 + 1, bh = B.y1 - B.y0 + 1, bd = B.z1 - B.z0 + 1;
+  if (bw <= 0 || bh <= 0 || bd <= 0) return;
+  const int64_t plane = bw * bh, cells = plane * bd, count = cells * bd;
+  const int64_t nxy = (int64_t)nx * ny;
+  const int64_t s = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += s) {
+    const int64_t za = B.z0 + i / cells;  // source layer
+    const int64_t c = i - (i / cells) * cells;
+    const int64_t zz = c / plane, r = c - zz * plane;
+    const int64_t yy = r / bw, xx = r - yy * bw;
+    const int64_t col = (int64_t)(B.y0 + yy) * nx + (B.x0 + xx);
+    const int64_t v = (int64_t)(B.z0 + zz) * nxy + col;
+    const int32_t e0 = __ldg(&vcol_eid[za * n + v]), e1 = __ldg(&vcol_eid[((int64_t)nz + za) * n + v]);
+    float w = INF_F;
+    if (e0 >= 0) {
+      const int64_t u = za * nxy + col;
+      bool ok = !roi_map || (__ldg(&roi_map[v]) >= 0 && __ldg(&roi_map[u]) >= 0);
+      ok = ok && !(sink && __ldg(&sink[u]));
+      if (ok) {
+        w = __ldg(&cost[e0]);
+        if (e1 >= 0) w = fminf(w, __ldg(&cost[e1]));
+      }
+    }
+    wcol[v * nzp + za] = w;
   }
 }
 
@@ -575,6 +617,39 @@ __device__ __forceinline__ void tma_stage(const LatParams &p, int32_t X0, int32_
   tc.phase ^= 1u;
 }
 
+// Via pass of one column with column vias: for each layer zb of the box in
+// turn, d[zb] = min(d[zb], fl(d[za] + w(za -> zb))) over every layer za of the
+// box (Gauss-Seidel, so a later layer sees an earlier one's new value), the
+// in-weights read as float4 rows wcol[v * nzp ..] (+inf where no via).  col:
+// the column's distances in shared memory, layer stride PS; v0: the node of
+// the column's layer z0.  Returns whether any distance decreased.  The sweep
+// cycles of the visit repeat it until nothing changes.
+template <int PS>
+__device__ __forceinline__ bool zcol_pass(float *col, const float *__restrict__ wcol, int32_t nzp, int64_t v0,
+                                          int64_t nxy, int32_t z0, int32_t nzb) {
+  const float INF_F = __int_as_float(0x7f800000);
+  bool chg = false;
+  const int q0 = z0 >> 2, q1 = (z0 + nzb - 1) >> 2;
+  for (int zb = 0; zb < nzb; ++zb) {
+    const float4 *wr = reinterpret_cast<const float4 *>(wcol + (v0 + (int64_t)zb * nxy) * nzp);
+    float best = col[zb * PS];
+    for (int q = q0; q <= q1; ++q) {
+      const float4 w = __ldg(&wr[q]);
+      const float wk[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int za = 4 * q + j - z0;
+        if (za >= 0 && za < nzb && wk[j] < INF_F) best = fminf(best, __fadd_rn(col[za * PS], wk[j]));
+      }
+    }
+    if (best < col[zb * PS]) {
+      col[zb * PS] = best;
+      chg = true;
+    }
+  }
+  return chg;
+}
+
 // Layer lists of the box being visited: H layers (x-runs) and V layers
 // (y-runs) as offsets from the box's z0.  Recomputed when a CTA moves to a
 // tile of another box.
@@ -584,7 +659,7 @@ struct LayerLists {
   int box;
 };
 
-template <int TX, int TY, bool PRIV, bool SPEC, bool DEEP = false, bool TMA = false>
+template <int TX, int TY, bool PRIV, bool SPEC, bool DEEP = false, bool TMA = false, bool CV = false>
 __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *sd, LayerLists &L, int *s_flags,
                                              int *s_act, int *s_nb = nullptr, bool warm = false,
                                              TmaCtx *tma = nullptr) {
@@ -831,8 +906,13 @@ __device__ __forceinline__ void process_tile(const LatParams &p, int t, float *s
     chg = false;
     for (int c = threadIdx.x; c < tw * th; c += (TX * TY)) {
       const int xx = c % tw + 1, yy = c / tw + 1;
-      const int wo = (yy - 1) * WSX + (xx - 1);
-      chg |= zrun<PS, WPS>(sd + yy * SX + xx, wdn + wo, wup + wo, nzb);
+      if constexpr (CV) {
+        const int64_t v0 = (int64_t)B.z0 * nxy + col0 + (int64_t)(yy - 1) * p.nx + (xx - 1);
+        chg |= zcol_pass<PS>(sd + yy * SX + xx, p.wcol, p.nzp, v0, nxy, B.z0, nzb);
+      } else {
+        const int wo = (yy - 1) * WSX + (xx - 1);
+        chg |= zrun<PS, WPS>(sd + yy * SX + xx, wdn + wo, wup + wo, nzb);
+      }
     }
     if (chg) s_flags[3 + cyc % 3] = 1;
     tile_sync<TX * TY, SPEC>();
@@ -994,7 +1074,7 @@ __device__ bool activate_tile(const LatParams &p, int t) {
 // the whole lattice (the tensor maps and the staging are sized for p.nz
 // layers), distances in slices of N cells (LatBox.pad = slice).  tmw / tmd
 // are unused otherwise.
-template <int TX, int TY, bool PRIV, bool DEEP = false, int MINB = 1, bool TMA = false>
+template <int TX, int TY, bool PRIV, bool DEEP = false, int MINB = 1, bool TMA = false, bool CV = false>
 __global__ void __launch_bounds__(TX * TY, MINB)
     lattice_async_kernel(LatParams p, const __grid_constant__ CUtensorMap tmw, const __grid_constant__ CUtensorMap tmd) {
   extern __shared__ __align__(128) float sd[];
@@ -1067,7 +1147,7 @@ __global__ void __launch_bounds__(TX * TY, MINB)
     const int t = warm ? s_cont : s_tile;
     __syncthreads();
     if (t < 0) break;
-    process_tile<TX, TY, PRIV, false, DEEP, TMA>(p, t, sd, s_layers, s_flags, s_act, s_nb, warm, &tma);
+    process_tile<TX, TY, PRIV, false, DEEP, TMA, CV>(p, t, sd, s_layers, s_flags, s_act, s_nb, warm, &tma);
     // neighbours are activated by threads 0..3 in parallel, after this
     // tile's distances are visible
     unsigned long long ta = 0;
@@ -1272,6 +1352,29 @@ int grow_ws(orsp::Graph *g, size_t need) {
   return ORSP_OK;
 }
 
+// Column-via weights for the nodes of a box: box_h (host, 6 ints) or box_d
+// (device), with the ROI / sink masks of a node-set ROI search.
+int gather_col_box(orsp::Graph *g, const float *cost_d, const int32_t *box_h, const LatBox *box_d,
+                   const int32_t *roi_map_d, const uint8_t *sink_d, cudaStream_t st) {
+  LatBox bv{};
+  int64_t count = (int64_t)g->N * g->nz;  // upper bound when the box is on the device
+  if (box_h) {
+    bv.x0 = box_h[0];
+    bv.x1 = box_h[1];
+    bv.y0 = box_h[2];
+    bv.y1 = box_h[3];
+    bv.z0 = box_h[4];
+    bv.z1 = box_h[5];
+    const int64_t d = box_h[5] - box_h[4] + 1;
+    count = (int64_t)(box_h[1] - box_h[0] + 1) * (box_h[3] - box_h[2] + 1) * d * d;
+  }
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((count + 255) / 256, (int64_t)g->num_sms * 16));
+  gather_col_kernel<<<blocks, 256, 0, st>>>(g->vcol_eid, cost_d, g->wcol, g->N, g->nx, g->ny, g->nz,
+                                             (g->nz + 3) & ~3, box_d, bv, roi_map_d, sink_d);
+  ORSP_CUDA(cudaGetLastError());
+  return ORSP_OK;
+}
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against the driver library); nullptr when unavailable.
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -1323,7 +1426,8 @@ bool encode_lattice_maps(const orsp::Graph *g, const LatParams &p, int TX, int T
 template <int TX, int TY>
 int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_t nseeds, const int32_t *seeds,
                    const float *seed_cost, cudaStream_t st, orsp::LatOptions *opt) {
-  const bool async = env_u64("ORSP_LAT_ASYNC", 1) != 0;
+  // (column vias always take the asynchronous schedule)
+  const bool async = p.wcol != nullptr || env_u64("ORSP_LAT_ASYNC", 1) != 0;
   const WsLayout L = ws_layout(g, ntiles);
   const size_t list_b = L.list_b, q_b = L.q_b;
   const unsigned qcap = L.qcap;
@@ -1350,7 +1454,7 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   }
   const bool priv = opt && opt->private_dist;
   // ORSP_LAT_SPEC=1: the warp-specialised asynchronous schedule
-  const bool spec = async && env_u64("ORSP_LAT_SPEC", 0) != 0;
+  const bool spec = async && !p.wcol && env_u64("ORSP_LAT_SPEC", 0) != 0;
   // ORSP_LAT_BLOCKS_PER_SM: CTAs per SM (tiles of up to 12 layers at width
   // 16 have an instantiation sized for 2)
   const int want = (int)env_u64("ORSP_LAT_BLOCKS_PER_SM", (opt && opt->blocks_per_sm > 0) ? opt->blocks_per_sm : 1);
@@ -1359,7 +1463,7 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   CUtensorMap tmw{}, tmd{};
   bool tma = false;
   if constexpr (TX == 16) {
-    if (async && !spec && want < 2 && nzb <= 12 && nzb == g->nz && opt && opt->tma_slices > 0 &&
+    if (async && !spec && !p.wcol && want < 2 && nzb <= 12 && nzb == g->nz && opt && opt->tma_slices > 0 &&
         env_u64("ORSP_LAT_TMA", 0) != 0)
       tma = encode_lattice_maps(g, p, TX, TY, nzb, opt->tma_slices, &tmw, &tmd);
   }
@@ -1368,7 +1472,19 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
     smem = (base + (size_t)nzb * TY * TX * 4 + (size_t)nzb * (TY + 2) * (TX + 8)) * sizeof(float);
   }
   void *kfn;
-  if (spec) {
+  if (p.wcol) {
+    // column vias: the asynchronous schedule with the column via pass, one
+    // CTA per SM, tile width 16
+    if constexpr (TX == 16) {
+      kfn = nzb > 12 ? (priv ? (void *)lattice_async_kernel<TX, TY, true, true, 1, false, true>
+                             : (void *)lattice_async_kernel<TX, TY, false, true, 1, false, true>)
+                     : (priv ? (void *)lattice_async_kernel<TX, TY, true, false, 1, false, true>
+                             : (void *)lattice_async_kernel<TX, TY, false, false, 1, false, true>);
+    } else {
+      orsp::set_error("lattice search: column vias need tile width 16");
+      return ORSP_ERR_ARG;
+    }
+  } else if (spec) {
     kfn = priv ? (void *)lattice_spec_kernel<TX, TY, true> : (void *)lattice_spec_kernel<TX, TY, false>;
     if constexpr (TX == 16) {  // two CTAs per SM: the instantiation held to their register share
       if (want >= 2 && nzb <= 12)
@@ -1474,13 +1590,21 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
 
 namespace orsp {
 
+// Recognises the routing lattice: every planar edge a unit step along its
+// layer's single routing axis, no parallel planar edges, and vias either all
+// between adjacent layers without parallel edges (slots 2 and 3) or, as in
+// the reference's Lattice3D (all-pairs blind/buried vias, duplicated via
+// edges, unified_pathfinder.py:1136-1172, 1264-1276), between any two layers
+// of a column with at most two parallel edges each (column vias, g->cvia).
 int analyze_lattice(Graph *g, const int32_t *indptr_h, const int32_t *indices_h) {
   g->lattice_ok = false;
+  g->cvia = false;
   if (g->nx <= 0 || g->ny <= 0 || g->nz <= 0 || g->nz > 64) return ORSP_OK;
   const int32_t N = g->N, nx = g->nx, ny = g->ny;
   const int64_t nxy = (int64_t)nx * ny;
   std::vector<int8_t> axis(g->nz, -1);
   std::vector<int32_t> slot((size_t)4 * N, -1);
+  bool adjacent_vias = true;  // every via spans one layer, no parallel vias
   for (int32_t u = 0; u < N; ++u) {
     const int32_t zu = (int32_t)(u / nxy);
     const int32_t ru = (int32_t)(u - zu * nxy);
@@ -1500,20 +1624,58 @@ int analyze_lattice(Graph *g, const int32_t *indptr_h, const int32_t *indices_h)
         if (axis[zu] == -1) axis[zu] = (int8_t)ax;
         else if (axis[zu] != ax) return ORSP_OK;  // both axes on one layer
         s = (dx + dy > 0) ? 0 : 1;  // entering v from its lower / upper neighbour
-      } else if (dx == 0 && dy == 0 && (dz == 1 || dz == -1)) {
+      } else if (dx == 0 && dy == 0) {
+        if (dz != 1 && dz != -1) {
+          adjacent_vias = false;  // a via spanning layers: column vias
+          continue;
+        }
         s = dz > 0 ? 2 : 3;  // via from below / from above
       } else {
-        return ORSP_OK;  // span > 1 or diagonal: not this lattice
+        return ORSP_OK;  // diagonal: not this lattice
       }
       int32_t &slotref = slot[(size_t)s * N + v];
-      if (slotref != -1) return ORSP_OK;  // parallel edges
+      if (slotref != -1) {
+        if (s < 2) return ORSP_OK;  // parallel planar edges
+        adjacent_vias = false;      // parallel vias: column vias
+        continue;
+      }
       slotref = k;
     }
+  }
+  std::vector<int32_t> vcol;
+  if (!adjacent_vias) {
+    // column vias: every via in-edge of v by source layer, two parallel
+    // edges at most (edge ids ascend with u and k, so k = 0 is the smaller)
+    vcol.assign((size_t)2 * g->nz * N, -1);
+    for (int32_t u = 0; u < N; ++u) {
+      const int32_t zu = (int32_t)(u / nxy);
+      const int64_t cu = u - (int64_t)zu * nxy;
+      for (int32_t k = indptr_h[u]; k < indptr_h[u + 1]; ++k) {
+        const int32_t v = indices_h[k];
+        const int32_t zv = (int32_t)(v / nxy);
+        if (zv == zu || v - (int64_t)zv * nxy != cu) continue;  // planar (checked above)
+        int32_t *e0 = &vcol[((size_t)0 * g->nz + zu) * N + v];
+        int32_t *e1 = &vcol[((size_t)1 * g->nz + zu) * N + v];
+        if (*e0 < 0) *e0 = k;
+        else if (*e1 < 0) *e1 = k;
+        else return ORSP_OK;  // three parallel vias
+      }
+    }
+    for (int32_t v = 0; v < N; ++v) slot[(size_t)2 * N + v] = slot[(size_t)3 * N + v] = -1;
   }
   for (int z = 0; z < g->nz; ++z) g->layer_axis[z] = axis[z] < 0 ? 0 : axis[z];
   ORSP_CUDA(cudaMalloc(&g->slot_eid, slot.size() * sizeof(int32_t)));
   ORSP_CUDA(cudaMemcpy(g->slot_eid, slot.data(), slot.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   ORSP_CUDA(cudaMalloc(&g->wslot, slot.size() * sizeof(float)));
+  if (!adjacent_vias) {
+    ORSP_CUDA(cudaMalloc(&g->vcol_eid, vcol.size() * sizeof(int32_t)));
+    ORSP_CUDA(cudaMemcpy(g->vcol_eid, vcol.data(), vcol.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    // weights of every via in-edge of a node by source layer, nz rounded up
+    // to 4 so that a node's row is whole float4s; layers without a via hold
+    // +inf after each gather of the box, the rest is never read
+    ORSP_CUDA(cudaMalloc(&g->wcol, (size_t)((g->nz + 3) & ~3) * N * sizeof(float)));
+    g->cvia = true;
+  }
   g->lattice_ok = true;
   return ORSP_OK;
 }
@@ -1521,6 +1683,11 @@ int analyze_lattice(Graph *g, const int32_t *indptr_h, const int32_t *indices_h)
 void free_lattice(Graph *g) {
   cudaFree(g->slot_eid);
   cudaFree(g->wslot);
+  cudaFree(g->vcol_eid);
+  cudaFree(g->wcol);
+  g->vcol_eid = nullptr;
+  g->wcol = nullptr;
+  g->cvia = false;
   cudaFree(g->lat_ws);
   cudaFree(g->lat_box_d);
   if (g->lat_ctl_h) cudaFreeHost(g->lat_ctl_h);
@@ -1599,6 +1766,11 @@ int run_lattice_boxes(Graph *g, const float *cost_d, int32_t nseeds, const int32
       gather_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 148 * 32), 256, 0, st>>>(
           g->slot_eid, cost_d, (float4 *)g->wslot, N);
       ORSP_CUDA(cudaGetLastError());
+      if (g->cvia) {
+        const int32_t full[6] = {0, g->nx - 1, 0, g->ny - 1, 0, g->nz - 1};
+        int rc = gather_col_box(g, cost_d, full, nullptr, nullptr, nullptr, st);
+        if (rc) return rc;
+      }
       g->w4_cost = cost_d;
       g->w4_gen = decl;
     }
@@ -1612,6 +1784,10 @@ int run_lattice_boxes(Graph *g, const float *cost_d, int32_t nseeds, const int32
       gather_box_kernel<<<(int)std::min<int64_t>((count + 255) / 256, 148 * 32), 256, 0, st>>>(
           g->slot_eid, cost_d, (float4 *)g->wslot, N, g->nx, g->ny, b[0], bw, b[2], bh, b[4], count);
       ORSP_CUDA(cudaGetLastError());
+      if (g->cvia) {
+        int rc = gather_col_box(g, cost_d, b, nullptr, nullptr, nullptr, st);
+        if (rc) return rc;
+      }
     }
   }
   if (priv) {
@@ -1639,6 +1815,9 @@ int run_lattice_boxes(Graph *g, const float *cost_d, int32_t nseeds, const int32
   p.seed_per_box = priv ? 1 : 0;
   p.boxes = lboxes_d;
   p.w4 = (const float4 *)g->wslot;
+  p.wcol = g->cvia ? g->wcol : nullptr;
+  p.nzp = (g->nz + 3) & ~3;
+  p.N = N;
   p.dist = dist;
   for (int z = 0; z < 64; ++z) p.axis[z] = z < g->nz ? g->layer_axis[z] : 0;
   if (TX == 32) return launch_lattice<32, 16>(g, p, ntiles, nzb, nseeds, seeds_d, seed_cost_d, st, opt);
@@ -1692,6 +1871,10 @@ int run_lattice_roi(Graph *g, const float *cost_d, int32_t nseeds, const int32_t
   gather_roi_kernel<<<(int)std::min<int64_t>((N + 255) / 256, gblocks), 256, 0, st>>>(
       g->slot_eid, cost_d, (float4 *)g->wslot, N, G, box_d, roi_map_d, sink_d);
   ORSP_CUDA(cudaGetLastError());
+  if (g->cvia) {
+    rc = gather_col_box(g, cost_d, nullptr, box_d, roi_map_d, sink_d, st);
+    if (rc) return rc;
+  }
   g->w4_cost = nullptr;  // masked weights: not reusable by a whole search
   g->w4_gen = 0;
   g->decl_cost = nullptr;
@@ -1706,6 +1889,9 @@ int run_lattice_roi(Graph *g, const float *cost_d, int32_t nseeds, const int32_t
   p.seed_per_box = 0;
   p.boxes = box_d;
   p.w4 = (const float4 *)g->wslot;
+  p.wcol = g->cvia ? g->wcol : nullptr;
+  p.nzp = (g->nz + 3) & ~3;
+  p.N = N;
   p.dist = dist;
   p.roi_map = roi_map_d;
   for (int z = 0; z < 64; ++z) p.axis[z] = z < g->nz ? g->layer_axis[z] : 0;

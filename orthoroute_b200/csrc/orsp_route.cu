@@ -184,7 +184,10 @@ extern "C" int orsp_route_nets(orsp_graph *g, int32_t M, const int32_t *src_h, c
     set_error("route_nets: NULL array");
     return ORSP_ERR_ARG;
   }
-  if (!g->lattice_ok) { set_error("route_nets: needs a graph recognised as an H/V lattice"); return ORSP_ERR_ARG; }
+  if (!g->lattice_ok || g->cvia) {
+    set_error("route_nets: needs a graph recognised as an H/V lattice with adjacent-layer vias");
+    return ORSP_ERR_ARG;
+  }
   // groups: [group_ptr[q], group_ptr[q+1]) of the order; NULL = one net each
   std::vector<int32_t> gp;
   if (group_ptr_h) {

@@ -700,6 +700,8 @@ static int sssp_impl(orsp_graph *g, const float *cost_d, int32_t nseeds, const i
     b.geom.ny = g->ny;
     b.geom.nz = g->nz;
     for (int z = 0; z < 64; ++z) b.geom.axis[z] = z < g->nz ? g->layer_axis[z] : 0;
+    b.geom.wcol = g->cvia ? g->wcol : nullptr;
+    b.geom.nzp = (g->nz + 3) & ~3;
     const int32_t full[6] = {0, g->nx - 1, 0, g->ny - 1, 0, g->nz - 1};
     const int32_t *bx = (box_h && !lattice_roi) ? box_h : full;
     b.rank_map = lattice_roi ? roi_map_d : nullptr;
@@ -770,6 +772,8 @@ static LatBacktraceParams lat_bt_full(orsp_graph *g, const uint32_t *dist, const
   b.geom.ny = g->ny;
   b.geom.nz = g->nz;
   for (int z = 0; z < 64; ++z) b.geom.axis[z] = z < g->nz ? g->layer_axis[z] : 0;
+  b.geom.wcol = g->cvia ? g->wcol : nullptr;
+  b.geom.nzp = (g->nz + 3) & ~3;
   b.box.x0 = 0;
   b.box.x1 = g->nx - 1;
   b.box.y0 = 0;
