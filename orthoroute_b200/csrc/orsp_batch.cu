@@ -27,9 +27,6 @@
 namespace {
 
 constexpr int BATCH_THREADS = 512;
-// Warps whose items have more out-edges than this relax item by item with
-// the edges spread over the lanes.
-constexpr int WIDE_DEG = 8;
 
 // per-search status in path_len (< 0)
 constexpr int ST_ARG = -1;
@@ -175,52 +172,30 @@ __device__ void block_search(const BatchParams &p, const Box &b, int32_t src_l, 
         const int maxdeg = __reduce_max_sync(ORSP_FULL_MASK, deg);
         const float d = bits_f(dbits);
         unsigned fmin_local = ORSP_INF_BITS;
-        // relaxation of edge e from a node at distance ds
-        auto relax = [&](int e, float ds, bool &pn, bool &pf, int2 &item) {
-          const int32_t w = __ldg(&p.indices[e]);
-          int32_t lw;
-          if (box_local(p, b, w, &lw)) {
-            const float nd = __fadd_rn(ds, __ldg(&p.cost[e]));
-            if (nd < INF_F) {
-              const unsigned nb = f_bits(nd);
-              if (nb < dist_ld<SMEM>(dist, lw)) {
-                const unsigned old = atomicMin(&dist[lw], nb);
-                if (nb < old) {
-                  item = make_int2(lw, (int)nb);
-                  if (nd < T) pn = true; else pf = true;
+        for (int k = 0; k < maxdeg; ++k) {
+          bool pn = false, pf = false;
+          int2 item = make_int2(0, 0);
+          if (k < deg) {
+            const int e = beg + k;
+            const int32_t w = __ldg(&p.indices[e]);
+            int32_t lw;
+            if (box_local(p, b, w, &lw)) {
+              const float nd = __fadd_rn(d, __ldg(&p.cost[e]));
+              if (nd < INF_F) {
+                const unsigned nb = f_bits(nd);
+                if (nb < dist_ld<SMEM>(dist, lw)) {
+                  const unsigned old = atomicMin(&dist[lw], nb);
+                  if (nb < old) {
+                    item = make_int2(lw, (int)nb);
+                    if (nd < T) pn = true; else pf = true;
+                  }
                 }
               }
             }
           }
-        };
-        if (maxdeg > WIDE_DEG) {
-          // high-degree nodes (dense via stacks): item by item, each item's
-          // out-edges spread over the lanes (one round of coalesced loads
-          // per item instead of deg dependent ones)
-          unsigned todo = __ballot_sync(ORSP_FULL_MASK, deg > 0);
-          while (todo) {
-            const int sl = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const int eb = __shfl_sync(ORSP_FULL_MASK, beg, sl), ee = __shfl_sync(ORSP_FULL_MASK, end, sl);
-            const float ds = __shfl_sync(ORSP_FULL_MASK, d, sl);
-            for (int k0 = eb; k0 < ee; k0 += 32) {
-              bool pn = false, pf = false;
-              int2 item = make_int2(0, 0);
-              if (k0 + lane < ee) relax(k0 + lane, ds, pn, pf, item);
-              warp_append(outq, out_cnt, p.qcap, pn, item, &c->err);
-              warp_append(farq, far_cnt, p.qcap, pf, item, &c->err);
-              if (pf && (unsigned)item.y < fmin_local) fmin_local = (unsigned)item.y;
-            }
-          }
-        } else {
-          for (int k = 0; k < maxdeg; ++k) {
-            bool pn = false, pf = false;
-            int2 item = make_int2(0, 0);
-            if (k < deg) relax(beg + k, d, pn, pf, item);
-            warp_append(outq, out_cnt, p.qcap, pn, item, &c->err);
-            warp_append(farq, far_cnt, p.qcap, pf, item, &c->err);
-            if (pf && (unsigned)item.y < fmin_local) fmin_local = (unsigned)item.y;
-          }
+          warp_append(outq, out_cnt, p.qcap, pn, item, &c->err);
+          warp_append(farq, far_cnt, p.qcap, pf, item, &c->err);
+          if (pf && (unsigned)item.y < fmin_local) fmin_local = (unsigned)item.y;
         }
         const unsigned wm = warp_min_u32(fmin_local);
         if (lane == 0 && wm != ORSP_INF_BITS) atomicMin(&c->fmin[g % 4], wm);

@@ -131,10 +131,6 @@ __global__ void seed_kernel(SsspParams p, int32_t nseeds, const int32_t *seeds,
   }
 }
 
-// Warps whose items have more out-edges than this relax item by item with
-// the edges spread over the lanes.
-constexpr int WIDE_DEG = 8;
-
 __global__ void __launch_bounds__(512) sssp_grid_kernel(SsspParams p) {
   SsspCtl *ctl = p.ctl;
   const unsigned nblocks = gridDim.x;
@@ -183,51 +179,29 @@ __global__ void __launch_bounds__(512) sssp_grid_kernel(SsspParams p) {
         const int maxdeg = __reduce_max_sync(ORSP_FULL_MASK, deg);
         const float d = bits_f(dbits);
         unsigned fmin_local = ORSP_INF_BITS;
-        // relaxation of edge e from a node at distance ds
-        auto relax = [&](int e, float ds, bool &pn, bool &pf, int2 &item) {
-          const int w = __ldg(&p.indices[e]);
-          if (!p.roi_map || __ldg(&p.roi_map[w]) >= 0) {
-            const float nd = __fadd_rn(ds, __ldg(&p.cost[e]));
-            if (nd < INF_F) {
-              const unsigned nb = f_bits(nd);
-              if (nb < __ldcg(&p.dist[w])) {
-                const unsigned old = atomicMin(&p.dist[w], nb);
-                if (nb < old) {
-                  item = make_int2(w, (int)nb);
-                  if (nd < T) pn = true; else pf = true;
+        for (int k = 0; k < maxdeg; ++k) {
+          bool pn = false, pf = false;
+          int2 item = make_int2(0, 0);
+          if (k < deg) {
+            const int e = beg + k;
+            const int w = __ldg(&p.indices[e]);
+            if (!p.roi_map || __ldg(&p.roi_map[w]) >= 0) {
+              const float nd = __fadd_rn(d, __ldg(&p.cost[e]));
+              if (nd < INF_F) {
+                const unsigned nb = f_bits(nd);
+                if (nb < __ldcg(&p.dist[w])) {
+                  const unsigned old = atomicMin(&p.dist[w], nb);
+                  if (nb < old) {
+                    item = make_int2(w, (int)nb);
+                    if (nd < T) pn = true; else pf = true;
+                  }
                 }
               }
             }
           }
-        };
-        if (maxdeg > WIDE_DEG) {
-          // high-degree nodes (dense via stacks): the warp takes its items one
-          // at a time and spreads each item's out-edges over the lanes, one
-          // round of coalesced loads per item instead of deg dependent ones
-          unsigned todo = __ballot_sync(ORSP_FULL_MASK, deg > 0);
-          while (todo) {
-            const int sl = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const int b = __shfl_sync(ORSP_FULL_MASK, beg, sl), e = __shfl_sync(ORSP_FULL_MASK, end, sl);
-            const float ds = __shfl_sync(ORSP_FULL_MASK, d, sl);
-            for (int k0 = b; k0 < e; k0 += 32) {
-              bool pn = false, pf = false;
-              int2 item = make_int2(0, 0);
-              if (k0 + lane < e) relax(k0 + lane, ds, pn, pf, item);
-              warp_append(outq, out_cnt, p.qcap, pn, item, &ctl->err);
-              warp_append(farq, far_cnt, p.fcap, pf, item, &ctl->err);
-              if (pf) fmin_local = fmin_local < item.y ? fmin_local : (unsigned)item.y;
-            }
-          }
-        } else {
-          for (int k = 0; k < maxdeg; ++k) {
-            bool pn = false, pf = false;
-            int2 item = make_int2(0, 0);
-            if (k < deg) relax(beg + k, d, pn, pf, item);
-            warp_append(outq, out_cnt, p.qcap, pn, item, &ctl->err);
-            warp_append(farq, far_cnt, p.fcap, pf, item, &ctl->err);
-            if (pf) fmin_local = fmin_local < item.y ? fmin_local : (unsigned)item.y;
-          }
+          warp_append(outq, out_cnt, p.qcap, pn, item, &ctl->err);
+          warp_append(farq, far_cnt, p.fcap, pf, item, &ctl->err);
+          if (pf) fmin_local = fmin_local < item.y ? fmin_local : (unsigned)item.y;
         }
         const unsigned wm = warp_min_u32(fmin_local);
         if (lane == 0 && wm != ORSP_INF_BITS) atomicMin(far_min, wm);
