@@ -169,6 +169,7 @@ struct LatOptions {
   bool copy_ctl = true;        // copy the control block to the pinned mirror (finish_lattice_search)
   int *err_d = nullptr;        // out: device address of the launch's error word
   int blocks_per_sm = 0;       // CTAs per SM (0: one); ORSP_LAT_BLOCKS_PER_SM overrides
+  int spec = 0;                // 1: the warp-specialised schedule; ORSP_LAT_SPEC overrides
   int64_t tma_slices = 0;      // > 0: every box is the whole lattice, box j's distances in slice j of N
                                // cells from `dist` (LatBox.pad = j); allows the TMA staging
 };

@@ -986,6 +986,11 @@ extern "C" int orsp_sssp_sources(orsp_graph *g, const float *cost_d, int32_t nsr
     // overlaps the other's sweeps (measured 0.50 against 0.77 ms per source
     // on 1000x1000x12 at 16 sources per launch)
     opt.blocks_per_sm = 2;
+    // and, for tiles of up to 12 layers (the instantiation sized for two
+    // CTAs per SM), the warp-specialised schedule: its scheduler warp takes
+    // the queue handoff off the workers' path (0.449 against 0.473 ms per
+    // source on 1000x1000x12)
+    opt.spec = g->nz <= 12 ? 1 : 0;
     // every chunk after the first reuses the gathered weights of this call
     if (decl) g->decl_cost = cost_d, g->decl_gen = decl;
     else if (a > 0) g->decl_cost = cost_d, g->decl_gen = ~0ull;

@@ -1454,7 +1454,7 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   }
   const bool priv = opt && opt->private_dist;
   // ORSP_LAT_SPEC=1: the warp-specialised asynchronous schedule
-  const bool spec = async && !p.wcol && env_u64("ORSP_LAT_SPEC", 0) != 0;
+  const bool spec = async && !p.wcol && env_u64("ORSP_LAT_SPEC", (opt && opt->spec) ? 1 : 0) != 0;
   // ORSP_LAT_BLOCKS_PER_SM: CTAs per SM (tiles of up to 12 layers at width
   // 16 have an instantiation sized for 2)
   const int want = (int)env_u64("ORSP_LAT_BLOCKS_PER_SM", (opt && opt->blocks_per_sm > 0) ? opt->blocks_per_sm : 1);
