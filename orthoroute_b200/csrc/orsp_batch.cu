@@ -416,6 +416,7 @@ int env_int(const char *name, int dflt) {
 struct LatBt {
   const float4 *w4;         // gathered in-edge weights (fresh inside the boxes)
   const int32_t *slot_eid;  // [4][N] in-edge id per slot
+  const int32_t *vcol_eid;  // column vias: [2][nz][N] via in-edge ids by source layer (NULL: none)
   int64_t N;
   const uint32_t *dist;  // slice arena
   orsp::LatWalkGeom geom;
@@ -480,7 +481,12 @@ __global__ void lat_batch_backtrace_kernel(LatBt p) {
   if (edges) {
     for (int i = lane; i < len - 1; i += 32) {
       const int32_t u = nodes[i], w = nodes[i + 1];
-      edges[i] = __ldg(&p.slot_eid[(int64_t)orsp::lat_edge_slot(p.geom, u, w) * p.N + w]);
+      const int64_t plane = (int64_t)p.geom.nx * p.geom.ny;
+      const int64_t zu = u / plane, zw = w / plane;
+      if (p.vcol_eid && zu != zw)  // a column via: the first CSR edge u -> w (the smaller id)
+        edges[i] = __ldg(&p.vcol_eid[zu * p.N + w]);
+      else
+        edges[i] = __ldg(&p.slot_eid[(int64_t)orsp::lat_edge_slot(p.geom, u, w) * p.N + w]);
     }
   }
   __syncwarp();
@@ -696,6 +702,9 @@ int run_batch_lat(orsp_graph *g, const float *cost_d, int32_t K, const std::vect
     LatBt bt{};
     bt.w4 = (const float4 *)g->wslot;
     bt.slot_eid = g->slot_eid;
+    bt.vcol_eid = g->cvia ? g->vcol_eid : nullptr;
+    bt.geom.wcol = g->cvia ? g->wcol : nullptr;
+    bt.geom.nzp = (g->nz + 3) & ~3;
     bt.N = g->N;
     bt.dist = g->blat_dist;
     bt.geom.nx = g->nx;
@@ -800,7 +809,7 @@ static int run_batch(orsp_graph *g, const float *cost_d, int32_t K, const int32_
   for (int tw : {16, 32}) {
     std::vector<int32_t> lat_items;
     for (int i = 0; i < nb; ++i)
-      if (tuned && g->plan_impl[i] == 1 && g->lattice_ok && !g->cvia && g->plan_tile[i] == tw)
+      if (tuned && g->plan_impl[i] == 1 && g->lattice_ok && !(g->cvia && tw != 16) && g->plan_tile[i] == tw)
         for (int32_t k : bucket[i])
           if (tile_ok(k, tw)) lat_items.push_back(k);
     if (lat_items.empty()) continue;
@@ -817,7 +826,7 @@ static int run_batch(orsp_graph *g, const float *cost_d, int32_t K, const int32_
   }
   for (int i = 0; i < nb; ++i) {
     std::vector<int32_t> items;
-    if (tuned && g->plan_impl[i] == 1 && g->lattice_ok && !g->cvia) {
+    if (tuned && g->plan_impl[i] == 1 && g->lattice_ok && !(g->cvia && g->plan_tile[i] != 16)) {
       for (int32_t k : bucket[i])
         if (!tile_ok(k, g->plan_tile[i])) items.push_back(k);
     } else {

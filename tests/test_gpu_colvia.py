@@ -157,3 +157,33 @@ def test_column_via_multi_target_and_sources():
     for i, s in enumerate(src):
         _, ref_dist, _, _ = O.dijkstra(lat.indptr, lat.indices, w, [s])
         assert np.array_equal(_bits(got[i]), _bits(ref_dist)), (i, s)
+
+
+@pytest.mark.parametrize("plan", [None, [{"max_nodes": 1 << 40, "impl": 1, "tile_w": 16}],
+                                  [{"max_nodes": 1 << 40, "impl": 1, "tile_w": 32}]])
+def test_column_via_batched_boxes_match_oracle(plan):
+    """Batched box searches on a column-via lattice: one CTA per search, the
+    tile sweeps with a distance slice per box and the column via pass, and a
+    tile-32 plan (which column vias send to the one-CTA kernel): every path
+    and every edge list (a via step maps to the first CSR edge) equal the
+    oracle's."""
+    from orthoroute_b200.lattice import random_boxes
+
+    lat = _ref_lattice(48, 36, 6)
+    w = _weights(lat, 5, 0.03, False)
+    dg = DeviceGraph.from_lattice(lat)
+    dg.set_batch_plan(plan)
+    boxes, src, dst = random_boxes(lat, 120, seed=9, lo=(2, 2, 1), hi=(48, 36, 6))
+    cap = 2048
+    nodes, edges, lens = dg.batch_bbox(torch.from_numpy(w).cuda(), torch.from_numpy(src).cuda(),
+                                       torch.from_numpy(dst).cuda(), torch.from_numpy(boxes).cuda(), path_cap=cap)
+    ref_nodes, ref_lens = O.batch_bbox(lat.indptr, lat.indices, w, lat.nx, lat.ny, lat.nz, src, dst, boxes, cap)
+    lens, nodes, edges = lens.cpu().numpy(), nodes.cpu().numpy(), edges.cpu().numpy()
+    for k in range(len(src)):
+        L = int(ref_lens[k])
+        if L < 2:
+            assert lens[k] < 2, k
+            continue
+        assert lens[k] == L, k
+        assert np.array_equal(nodes[k, :L], ref_nodes[k, :L]), k
+        assert np.array_equal(edges[k, : L - 1], O.path_to_edges(lat.indptr, lat.indices, ref_nodes[k, :L])), k
