@@ -7,17 +7,16 @@
 //     memory in the K-major canonical UMMA layout without swizzle (core
 //     matrices of 8 rows x 16 bytes, rows contiguous; the two 8-element halves
 //     of a 16-wide K slice 128 bytes apart, 8-row groups 256 bytes apart);
-//   - per tile, nine stages (dz, dy): 512 threads copy one input row into
+//   - per tile, nine stages (dz, dy): 256 threads copy one input row into
 //     the three (dx) im2col blocks A[m][k] = X[z+dz][y+dy][x0+m+dx][k] of a
 //     stage buffer in the same layout (cp.async, zero outside the grid; the
 //     optional ReLU mask through registers), and one thread issues the
 //     3 x Cin/16 MMAs (K = 16 each) into the TMEM accumulator and commits them
 //     to the buffer's mbarrier, while the copies of the next stages are in
 //     flight (a ring of up to four buffers);
-//   - the epilogue reads the accumulator with tcgen05.ld (warps w, w + 4,
-//     w + 8 and w + 12 share TMEM lanes 32 (w % 4) .., i.e. those voxels, and
-//     split the output channels), adds the bias, applies the ReLU and stores
-//     bf16 or fp32.
+//   - the epilogue reads the accumulator with tcgen05.ld (warps w and w + 4
+//     share TMEM lanes 32 (w % 4) .., i.e. those voxels, and split the output
+//     channels), adds the bias, applies the ReLU and stores bf16 or fp32.
 // The weight gradient (wgrad_tc_kernel) is a second tcgen05 GEMM.
 // Every mbarrier wait is bounded by the global timer; on expiry the kernel
 // records an error, waits once more (bounded) for its MMAs, frees its TMEM
@@ -143,10 +142,7 @@ __device__ __forceinline__ void cp_async_wait(int n) {
   else asm volatile("cp.async.wait_group 2;" ::: "memory");
 }
 
-// sixteen warps gather (latency hiding for the copies); warps w, w + 4, w + 8
-// and w + 12 share TMEM lanes 32 (w % 4) .. + 31 and split the channels
-constexpr int CV_THREADS = 512;
-constexpr int CV_WARPS = CV_THREADS / 32;
+constexpr int CV_THREADS = 256;  // eight warps gather; warps w and w + 4 share TMEM lanes 32 (w % 4)..
 
 // Pipelined implicit GEMM.  A stage is one input row (plane z + dz, row
 // y + dy) of a tile: the 130 voxels x0 - 1 .. x0 + 128 are read once, 16
@@ -329,9 +325,9 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
       const int64_t zy = t / ntx;
       const int y = static_cast<int>(zy % H), z = static_cast<int>(zy / H);
       // warp w: voxels 32 (w % 4) .. + 31 (its TMEM lanes), channel blocks
-      // of 16 starting at 16 (w / 4), every (CV_WARPS / 4)-th one
+      // of 16 starting at 16 (w / 4), every second one
       const int m = (warp & 3) * 32 + lane, xx = tx * TC_M + m;
-      for (int c0 = (warp >> 2) * 16; c0 < Cout; c0 += 16 * (CV_WARPS / 4)) {
+      for (int c0 = (warp >> 2) * 16; c0 < Cout; c0 += 32) {
         uint32_t r[16];
         tmem_ld16(tmem + (static_cast<uint32_t>((warp & 3) * 32) << 16) + static_cast<uint32_t>(c0), r);
         if (xx < W) {
