@@ -809,6 +809,11 @@ def run_ours(args, world, rank, local):
         srcs_per_launch = 1
         visits_per_tile = single["visits_per_tile"]
     value = total_edges / (ms_max / 1e3) / 1e9
+    # the tile-search kernel of the timed step: many-source launches of up
+    # to 12 layers take the warp-specialised schedule (ORSP_LAT_SPEC overrides)
+    spec_env = os.environ.get("ORSP_LAT_SPEC")
+    spec = (spec_env not in (None, "") and spec_env != "0") if spec_env not in (None, "") else bool(per and lat.nz <= 12)
+    timed_kernel = "lattice_spec_kernel" if spec else "lattice_async_kernel"
     avg_kernel_ms = kernel_ms / launches
     bytes_per_launch = bytes_alg / len(sources) * srcs_per_launch
     achieved = bytes_per_launch / (avg_kernel_ms / 1e3) / 1e9
@@ -903,7 +908,7 @@ def run_ours(args, world, rank, local):
                      "frac": round(achieved / peak, 5),
                      "traffic": int(LAT_DRAM_BYTES_PER_NODE * lat.N * srcs_per_launch),
                      "traffic_source": "ncu dram bytes of a 4-source launch of this lattice, scaled by sources per launch",
-                     "kernel": "lattice_async_kernel", "peak_kind": peak_kind,
+                     "kernel": timed_kernel, "peak_kind": peak_kind,
                      "bytes_per_launch": int(bytes_per_launch),
                      "avg_launch_ms": round(avg_kernel_ms, 4)},
         "clocks": clk,
