@@ -2,7 +2,7 @@
 
     python -m orthoroute_b200.headless board.ORP [-o board.ORS] [--max-iterations 200]
                                        [--mode batched|plain] [--warm] [--pitch 0.4]
-                                       [--no-portals]
+                                       [--no-portals] [--vias adjacent|full]
 
 The steps are those of the reference's `main.py headless` (main.py:287-622):
 read the board (orp.read_orp / orp_to_board_data), build the routing lattice
@@ -77,6 +77,7 @@ class HeadlessProblem:
     # search endpoints per task: src / dst, or the F.Cu nodes of both portals
     search_src: np.ndarray = None
     search_dst: np.ndarray = None
+    vias: str = "adjacent"  # the lattice's via set: "adjacent" or "full" (the reference's)
 
 
 def routing_bounds(board_data: dict) -> Tuple[float, float, float, float]:
@@ -111,17 +112,21 @@ def _pad_key(pad: dict, comp: str, pad_id: str) -> str:
 
 
 def build_problem(board_data: dict, pitch: float = DEFAULT_PITCH, portals: bool = False,
-                  escape_seed: int = 42) -> HeadlessProblem:
+                  escape_seed: int = 42, vias: str = "adjacent") -> HeadlessProblem:
     """The routing lattice and tasks of a board_data dict.  With portals, the
     pads escape to portals first (escapes.plan_escapes) and a net whose two
     pads both have one is routed between its portals, as the reference does
-    with its default portal_enabled (unified_pathfinder.py:2629-2641)."""
+    with its default portal_enabled (unified_pathfinder.py:2629-2641).
+    vias: "adjacent" (vias between neighbouring layers) or "full", the
+    reference's via set (Lattice3D.get_legal_via_pairs, UPF:1136-1172: F.Cu
+    to every routing layer and every pair of routing layers), searched as a
+    column-via lattice."""
     nz = int(board_data.get("layers", 2))
     names = list(board_data.get("layer_names") or [])
     if len(names) < nz:
         names = default_layer_names(nz)
     gx0, gy0, nx, ny = grid_geometry(routing_bounds(board_data), pitch)
-    lat = build_lattice(nx, ny, nz, planar="inner" if nz > 2 else "all", vias="adjacent")
+    lat = build_lattice(nx, ny, nz, planar="inner" if nz > 2 else "all", vias=vias)
     plane = nx * ny
 
     def snap(p) -> int:
@@ -165,6 +170,7 @@ def build_problem(board_data: dict, pitch: float = DEFAULT_PITCH, portals: bool 
             pad_nodes[key] = snap(p)
     prob = HeadlessProblem(lat, [], np.zeros(0, np.int32), np.zeros(0, np.int32), {}, gx0, gy0, pitch, names,
                            layer_directions(nz), pad_nodes, [(c, members[c]) for c in order], net_pads)
+    prob.vias = vias
     # a one-layer board has no routing layer to enter (the reference's
     # fallback there names layers 1 and 2, outside its lattice): pad to pad
     if portals and nz >= 2:
@@ -220,7 +226,7 @@ def forced_overuse(prob: HeadlessProblem) -> int:
     two layers an F.Cu node has no planar edges and one via edge each way, so
     every F.Cu search endpoint that several searches leave (or several enter)
     keeps that directed edge overused.  0 on boards of one or two layers."""
-    if prob.lattice.nz <= 2:
+    if prob.lattice.nz <= 2 or prob.vias == "full":  # (full vias: an F.Cu node has one via to every layer)
         return 0
     plane = prob.lattice.nx * prob.lattice.ny
     out = 0
@@ -263,15 +269,20 @@ def headless_config(max_iterations: int = 200):
 
 
 def route_board(board_data: dict, pitch: float = DEFAULT_PITCH, max_iterations: int = 200, mode: str = "batched",
-                warm: bool = False, config=None, device=None, log=None, portals: bool = True):
+                warm: bool = False, config=None, device=None, log=None, portals: bool = True,
+                vias: str = "adjacent"):
     """Routes a board_data dict on the GPU (mode 'batched' or 'sequential'),
-    through pad-escape portals unless portals is False.  Returns (problem,
-    RouteResult, tracks, vias, iteration metrics)."""
+    through pad-escape portals unless portals is False, on a lattice with
+    adjacent or full (the reference's) vias.  Returns (problem, RouteResult,
+    tracks, vias, iteration metrics)."""
     from .geometry import generate_geometry
     from .negotiate import PathFinder
 
-    prob = build_problem(board_data, pitch, portals=portals)
+    prob = build_problem(board_data, pitch, portals=portals, vias=vias)
     cfg = config or headless_config(max_iterations)
+    if vias == "full" and cfg.batch_plan is None:
+        # the batched box searches on the tile sweeps (column vias)
+        cfg.batch_plan = [{"max_nodes": 1 << 40, "impl": 1, "tile_w": 16}]
     pf = PathFinder(prob.lattice, config=cfg, device=device)
     hist = None
     if warm:
@@ -300,15 +311,16 @@ def route_board(board_data: dict, pitch: float = DEFAULT_PITCH, max_iterations: 
 
 def run_headless(orp_file: str, output_file: Optional[str] = None, max_iterations: int = 200,
                  mode: str = "batched", warm: bool = False, pitch: float = DEFAULT_PITCH, log=print,
-                 portals: bool = True) -> dict:
+                 portals: bool = True, vias: str = "adjacent") -> dict:
     """ORP in, ORS out; returns a summary of the run."""
     from .ors import GeometryPayload, write_ors
 
     t0 = time.perf_counter()
     board_data = orp_to_board_data(read_orp(orp_file))
     out = Path(output_file) if output_file else Path(orp_file).with_suffix(".ORS")
+    via_style = vias
     prob, res, tracks, vias, metrics = route_board(board_data, pitch, max_iterations, mode, warm, log=log,
-                                                   portals=portals)
+                                                   portals=portals, vias=via_style)
     total = time.perf_counter() - t0
     routed = sum(1 for p in res.paths if p is not None and len(p) >= 2) + len(prob.trivial)
     meta = {"orthoroute_version": "0.1.0", "board_name": board_data.get("filename", "board"), "total_time": total,
@@ -320,7 +332,8 @@ def run_headless(orp_file: str, output_file: Optional[str] = None, max_iteration
     summary = {"ors": str(out), "nets": len(prob.names) + len(prob.trivial), "routed": routed,
                "converged": bool(res.converged), "iterations": len(metrics), "tracks": len(tracks),
                "vias": len(vias), "seconds_total": round(total, 3), "seconds_route": round(res.seconds, 3),
-               "lattice": [prob.lattice.nx, prob.lattice.ny, prob.lattice.nz], "portals": len(prob.portals),
+               "lattice": [prob.lattice.nx, prob.lattice.ny, prob.lattice.nz], "lattice_vias": via_style,
+               "portals": len(prob.portals),
                "escape_tracks": len(prob.escape_tracks), "portal_collisions": portal_collisions(prob),
                "forced_overuse": forced_overuse(prob)}
     if log and summary["portal_collisions"]:
@@ -340,9 +353,11 @@ def main(argv=None):
     ap.add_argument("--warm", action="store_true", help="start from the learned history prediction")
     ap.add_argument("--pitch", type=float, default=DEFAULT_PITCH)
     ap.add_argument("--no-portals", action="store_true", help="route pad to pad, without pad escapes")
+    ap.add_argument("--vias", choices=["adjacent", "full"], default="adjacent",
+                    help="vias between neighbouring layers, or the reference's full via set")
     a = ap.parse_args(argv)
     s = run_headless(a.orp, a.output, a.max_iterations, "batched" if a.mode == "batched" else "sequential", a.warm,
-                     a.pitch, portals=not a.no_portals)
+                     a.pitch, portals=not a.no_portals, vias=a.vias)
     return 0 if s["converged"] else 1
 
 

@@ -91,3 +91,21 @@ def test_headless_portals_match_oracle(tmp_path, mode):
     assert np.all(prob.search_src < plane) and np.all(prob.search_dst < plane)  # F.Cu seeds
     ref = route_plain(prob.lattice, prob.search_src, prob.search_dst, headless_config(30))
     _check(prob, ref, s, geom, meta)
+
+
+@pytest.mark.parametrize("mode", ["batched", "sequential"])
+def test_headless_full_vias_match_oracle(tmp_path, mode):
+    """The portal flow on the reference's via set (F.Cu to every routing
+    layer, every pair of routing layers): searched as a column-via lattice,
+    batched on the tile sweeps; every net's stubs, tracks and vias equal the
+    oracle loop's on the same lattice."""
+    b = board_uniform_pins(40, 32, 6, 30, seed=5)
+    orp = tmp_path / "board.orp"
+    ors = tmp_path / "board.ors"
+    write_orp(synthetic_board_data(b), orp)
+    s = run_headless(str(orp), str(ors), max_iterations=30, mode=mode, log=None, vias="full")
+    geom, meta = read_ors(ors)
+    prob = build_problem(orp_to_board_data(read_orp(orp)), portals=True, vias="full")
+    assert s["lattice_vias"] == "full" and s["forced_overuse"] == 0
+    ref = route_plain(prob.lattice, prob.search_src, prob.search_dst, headless_config(30))
+    _check(prob, ref, s, geom, meta)

@@ -231,3 +231,29 @@ def test_synthetic_board_round_trip(tmp_path):
         x, y, z = b.lattice.coords(a)
         px, py, pz = prob.lattice.coords(c)
         assert np.array_equal(px, x + ox) and np.array_equal(py, y + oy) and np.array_equal(pz, z)
+
+
+def test_full_via_lattice_problem():
+    """vias='full' builds the reference's via set (F.Cu to every routing layer
+    and every pair of routing layers), which the device recognises as a
+    column-via lattice; the same tasks as the adjacent-via lattice, and no
+    forced overuse at shared F.Cu endpoints (one via per layer pair)."""
+    from orthoroute_b200.headless import forced_overuse
+
+    b = board_uniform_pins(40, 32, 6, 30, seed=5)
+    bd = orp_to_board_data(board_data_to_orp(synthetic_board_data(b)))
+    pa = build_problem(bd, portals=True)
+    pf = build_problem(bd, portals=True, vias="full")
+    assert pf.vias == "full" and pa.vias == "adjacent"
+    assert np.array_equal(pa.search_src, pf.search_src) and np.array_equal(pa.search_dst, pf.search_dst)
+    lat = pf.lattice
+    plane = lat.nx * lat.ny
+    u = np.repeat(np.arange(lat.N), np.diff(lat.indptr))
+    v = lat.indices.astype(np.int64)
+    via = (u // plane) != (v // plane)
+    pairs = {(int(a), int(c)) for a, c in zip(u[via] // plane, v[via] // plane)}
+    routing = range(1, lat.nz - 1)
+    want = {(a, c) for a in routing for c in routing if a != c} | {(0, c) for c in routing} | {(c, 0) for c in routing}
+    assert pairs == want
+    pf.search_src[2] = pf.search_src[0]
+    assert forced_overuse(pf) == 0
