@@ -77,7 +77,7 @@ class HeadlessProblem:
     # search endpoints per task: src / dst, or the F.Cu nodes of both portals
     search_src: np.ndarray = None
     search_dst: np.ndarray = None
-    vias: str = "adjacent"  # the lattice's via set: "adjacent" or "full" (the reference's)
+    vias: str = "full"  # the lattice's via set: "full" (the reference's) or "adjacent"
 
 
 def routing_bounds(board_data: dict) -> Tuple[float, float, float, float]:
@@ -112,7 +112,7 @@ def _pad_key(pad: dict, comp: str, pad_id: str) -> str:
 
 
 def build_problem(board_data: dict, pitch: float = DEFAULT_PITCH, portals: bool = False,
-                  escape_seed: int = 42, vias: str = "adjacent") -> HeadlessProblem:
+                  escape_seed: int = 42, vias: str = "full") -> HeadlessProblem:
     """The routing lattice and tasks of a board_data dict.  With portals, the
     pads escape to portals first (escapes.plan_escapes) and a net whose two
     pads both have one is routed between its portals, as the reference does
@@ -270,7 +270,7 @@ def headless_config(max_iterations: int = 200):
 
 def route_board(board_data: dict, pitch: float = DEFAULT_PITCH, max_iterations: int = 200, mode: str = "batched",
                 warm: bool = False, config=None, device=None, log=None, portals: bool = True,
-                vias: str = "adjacent"):
+                vias: str = "full"):
     """Routes a board_data dict on the GPU (mode 'batched' or 'sequential'),
     through pad-escape portals unless portals is False, on a lattice with
     adjacent or full (the reference's) vias.  Returns (problem, RouteResult,
@@ -311,7 +311,7 @@ def route_board(board_data: dict, pitch: float = DEFAULT_PITCH, max_iterations: 
 
 def run_headless(orp_file: str, output_file: Optional[str] = None, max_iterations: int = 200,
                  mode: str = "batched", warm: bool = False, pitch: float = DEFAULT_PITCH, log=print,
-                 portals: bool = True, vias: str = "adjacent") -> dict:
+                 portals: bool = True, vias: str = "full") -> dict:
     """ORP in, ORS out; returns a summary of the run."""
     from .ors import GeometryPayload, write_ors
 
@@ -353,8 +353,9 @@ def main(argv=None):
     ap.add_argument("--warm", action="store_true", help="start from the learned history prediction")
     ap.add_argument("--pitch", type=float, default=DEFAULT_PITCH)
     ap.add_argument("--no-portals", action="store_true", help="route pad to pad, without pad escapes")
-    ap.add_argument("--vias", choices=["adjacent", "full"], default="adjacent",
-                    help="vias between neighbouring layers, or the reference's full via set")
+    ap.add_argument("--vias", choices=["adjacent", "full"], default="full",
+                    help="the reference's via set (F.Cu to every routing layer, every pair of routing layers; the "
+                         "default), or vias between neighbouring layers only")
     a = ap.parse_args(argv)
     s = run_headless(a.orp, a.output, a.max_iterations, "batched" if a.mode == "batched" else "sequential", a.warm,
                      a.pitch, portals=not a.no_portals, vias=a.vias)

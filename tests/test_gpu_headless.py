@@ -94,18 +94,20 @@ def test_headless_portals_match_oracle(tmp_path, mode):
 
 
 @pytest.mark.parametrize("mode", ["batched", "sequential"])
-def test_headless_full_vias_match_oracle(tmp_path, mode):
-    """The portal flow on the reference's via set (F.Cu to every routing
-    layer, every pair of routing layers): searched as a column-via lattice,
-    batched on the tile sweeps; every net's stubs, tracks and vias equal the
-    oracle loop's on the same lattice."""
+@pytest.mark.parametrize("vias", ["full", "adjacent"])
+def test_headless_via_sets_match_oracle(tmp_path, mode, vias):
+    """The portal flow on both via sets: the reference's (F.Cu to every
+    routing layer, every pair of routing layers; the default, searched as a
+    column-via lattice, batched on the tile sweeps) and adjacent-layer vias
+    (the device routing loop in sequential mode); every net's stubs, tracks
+    and vias equal the oracle loop's on the same lattice."""
     b = board_uniform_pins(40, 32, 6, 30, seed=5)
     orp = tmp_path / "board.orp"
     ors = tmp_path / "board.ors"
     write_orp(synthetic_board_data(b), orp)
-    s = run_headless(str(orp), str(ors), max_iterations=30, mode=mode, log=None, vias="full")
+    s = run_headless(str(orp), str(ors), max_iterations=30, mode=mode, log=None, vias=vias)
     geom, meta = read_ors(ors)
-    prob = build_problem(orp_to_board_data(read_orp(orp)), portals=True, vias="full")
-    assert s["lattice_vias"] == "full" and s["forced_overuse"] == 0
+    prob = build_problem(orp_to_board_data(read_orp(orp)), portals=True, vias=vias)
+    assert s["lattice_vias"] == vias and (vias == "adjacent" or s["forced_overuse"] == 0)
     ref = route_plain(prob.lattice, prob.search_src, prob.search_dst, headless_config(30))
     _check(prob, ref, s, geom, meta)

@@ -133,7 +133,8 @@ def test_forced_overuse_bound():
     from orthoroute_b200.headless import forced_overuse
 
     b = board_uniform_pins(40, 32, 6, 30, seed=5)
-    prob = build_problem(orp_to_board_data(board_data_to_orp(synthetic_board_data(b))), portals=True)
+    prob = build_problem(orp_to_board_data(board_data_to_orp(synthetic_board_data(b))), portals=True,
+                         vias="adjacent")
     assert int(max(prob.search_src.max(), prob.search_dst.max())) < prob.lattice.nx * prob.lattice.ny  # F.Cu
     assert forced_overuse(prob) == 0
     s0, d0 = int(prob.search_src[0]), int(prob.search_dst[0])
@@ -143,7 +144,7 @@ def test_forced_overuse_bound():
     prob.search_dst[3] = d0  # two searches enter d0
     assert forced_overuse(prob) == 2
     b2 = board_uniform_pins(30, 24, 2, 12, seed=3)
-    p2 = build_problem(synthetic_board_data(b2), portals=True)
+    p2 = build_problem(synthetic_board_data(b2), portals=True, vias="adjacent")
     p2.search_src[1] = p2.search_src[0]
     assert forced_overuse(p2) == 0
 
@@ -242,8 +243,8 @@ def test_full_via_lattice_problem():
 
     b = board_uniform_pins(40, 32, 6, 30, seed=5)
     bd = orp_to_board_data(board_data_to_orp(synthetic_board_data(b)))
-    pa = build_problem(bd, portals=True)
-    pf = build_problem(bd, portals=True, vias="full")
+    pa = build_problem(bd, portals=True, vias="adjacent")
+    pf = build_problem(bd, portals=True)
     assert pf.vias == "full" and pa.vias == "adjacent"
     assert np.array_equal(pa.search_src, pf.search_src) and np.array_equal(pa.search_dst, pf.search_dst)
     lat = pf.lattice
