@@ -49,9 +49,6 @@ METRIC = "sec to zero-overuse route, batched+warm vs plain, 1 B200; SSSP GTEPS &
 NX, NY, NZ = 1000, 1000, 12
 NSRC = 64
 PER_LAUNCH = 16
-# batch plan of the config-3 batched rounds (DeviceGraph.set_batch_plan; None:
-# one CTA per box)
-C3_BATCH_PLAN = None
 BLOCKED = 0.05
 SEED = 20261203
 # DRAM bytes (read + write) per lattice node and source of the tile search in
@@ -462,8 +459,7 @@ def route_c3(dev, with_cpu: bool):
 
     b = board_footprints(600, 600, 18, 8000, None, seed=3)
     cfg = NegotiationConfig(max_iterations=40, cost_update="net", reroute="offenders", roi_margin=10,
-                            full_graph_retry=False, net_order="disjoint", stall_grow=10, stall_iterations=2,
-                            batch_plan=C3_BATCH_PLAN)
+                            full_graph_retry=False, net_order="disjoint", stall_grow=10, stall_iterations=2)
     pf = PathFinder(b.lattice, config=cfg, device=dev)
     # parity at full lattice size: iteration 1 of the first 200 nets, GPU
     # (batched) against the oracle loop, per net and in the final usage
