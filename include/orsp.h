@@ -99,9 +99,9 @@ ORSP_API int orsp_graph_max_degree(orsp_graph *g, int32_t *out);
  * column vias, as the reference's Lattice3D builds them (vias between any
  * two layers of a column, up to two parallel edges each,
  * unified_pathfinder.py:1136-1172, 1264-1276): single, ROI, multi-target and
- * many-source and batched box searches use the tile sweeps with a
- * per-column via pass (batched plans at tile width 16; width 32 takes the
- * one-CTA kernel); orsp_route_nets is not available.  0 otherwise.  (No reference counterpart: the reference has one
+ * many-source and batched box searches and orsp_route_nets use the tile
+ * sweeps with a per-column via pass (tile width 16; batched plans at width
+ * 32 take the one-CTA kernel).  0 otherwise.  (No reference counterpart: the reference has one
  * search path for every graph.) */
 ORSP_API int orsp_graph_is_lattice(orsp_graph *g, int32_t *out);
 /* Deepest box (layers) that one shared-memory tile of the lattice search holds

@@ -72,6 +72,7 @@ __global__ void route_commit_kernel(const int32_t *order, const int32_t *edges, 
 struct RouteBt {
   const float4 *w4;         // gathered in-edge weights (fresh inside the group's boxes)
   const int32_t *slot_eid;  // [4][N] in-edge id per slot
+  const int32_t *vcol_eid;  // column vias: [2][nz][N] via in-edge ids by source layer (NULL: none)
   int64_t N;
   const uint32_t *dist;
   LatWalkGeom geom;
@@ -142,7 +143,12 @@ __global__ void route_backtrace_kernel(RouteBt p) {
   __syncwarp();
   for (int i = lane; i < len - 1; i += 32) {
     const int32_t u = nodes[i], w = nodes[i + 1];
-    edges[i] = __ldg(&p.slot_eid[(int64_t)lat_edge_slot(p.geom, u, w) * p.N + w]);
+    const int64_t plane = (int64_t)p.geom.nx * p.geom.ny;
+    const int64_t zu = u / plane, zw = w / plane;
+    if (p.vcol_eid && zu != zw)  // a column via: the first CSR edge u -> w (the smaller id)
+      edges[i] = __ldg(&p.vcol_eid[zu * p.N + w]);
+    else
+      edges[i] = __ldg(&p.slot_eid[(int64_t)lat_edge_slot(p.geom, u, w) * p.N + w]);
   }
   __syncwarp();
   if (lane == 0) *len_out = len;
@@ -184,10 +190,7 @@ extern "C" int orsp_route_nets(orsp_graph *g, int32_t M, const int32_t *src_h, c
     set_error("route_nets: NULL array");
     return ORSP_ERR_ARG;
   }
-  if (!g->lattice_ok || g->cvia) {
-    set_error("route_nets: needs a graph recognised as an H/V lattice with adjacent-layer vias");
-    return ORSP_ERR_ARG;
-  }
+  if (!g->lattice_ok) { set_error("route_nets: needs a graph recognised as an H/V lattice"); return ORSP_ERR_ARG; }
   // groups: [group_ptr[q], group_ptr[q+1]) of the order; NULL = one net each
   std::vector<int32_t> gp;
   if (group_ptr_h) {
@@ -285,6 +288,8 @@ extern "C" int orsp_route_nets(orsp_graph *g, int32_t M, const int32_t *src_h, c
   geom.ny = g->ny;
   geom.nz = g->nz;
   for (int z = 0; z < 64; ++z) geom.axis[z] = z < g->nz ? g->layer_axis[z] : 0;
+  geom.wcol = g->cvia ? g->wcol : nullptr;
+  geom.nzp = (g->nz + 3) & ~3;
   // Steps 1-4 of one group, enqueued on the stream.
   auto enqueue_group = [&](int32_t q) -> int {
     int rc = ORSP_OK;
@@ -301,6 +306,7 @@ extern "C" int orsp_route_nets(orsp_graph *g, int32_t M, const int32_t *src_h, c
     RouteBt bt{};
     bt.w4 = (const float4 *)g->wslot;
     bt.slot_eid = g->slot_eid;
+    bt.vcol_eid = g->cvia ? g->vcol_eid : nullptr;
     bt.N = g->N;
     bt.dist = g->dist;
     bt.geom = geom;

@@ -71,14 +71,13 @@ class DeviceGraph:
         il = ctypes.c_int32()
         check(lib.orsp_graph_is_lattice(self._h, ctypes.byref(il)), "orsp_graph_is_lattice")
         # 1: H/V lattice with adjacent-layer vias; 2: the same with column
-        # vias (the reference's Lattice3D): tile-sweep searches, but no
-        # device routing loop and no batched tile sweeps
+        # vias (the reference's Lattice3D), searched with a per-column via pass
         self.lattice_kind = int(il.value)
         self.is_lattice = self.lattice_kind != 0
         ml = ctypes.c_int32()
         check(lib.orsp_lattice_max_layers(0, ctypes.byref(ml)), "orsp_lattice_max_layers")
         # the device routing loop needs every box in one shared-memory tile
-        self.route_loop_ok = self.lattice_kind == 1 and self.nz <= int(ml.value)
+        self.route_loop_ok = self.is_lattice and self.nz <= int(ml.value)
         self.indptr_host = indptr
         self.indices_host = indices
         self._path_buf = None

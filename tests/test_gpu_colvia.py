@@ -38,7 +38,7 @@ def test_reference_golden_graph_is_a_column_via_lattice(golden):
     g = golden("golden_dijkstra.npz")
     nx, ny, nz = (int(v) for v in g["ref_dims"])
     dg = DeviceGraph(g["ref_indptr"], g["ref_indices"], nx, ny, nz)
-    assert dg.lattice_kind == 2 and not dg.route_loop_ok
+    assert dg.lattice_kind == 2 and dg.route_loop_ok
     solver = GpuSolver(dg)
     roi = np.arange(dg.N, dtype=np.int32)
     for k in range(int(g["nref"])):
@@ -187,3 +187,30 @@ def test_column_via_batched_boxes_match_oracle(plan):
         assert lens[k] == L, k
         assert np.array_equal(nodes[k, :L], ref_nodes[k, :L]), k
         assert np.array_equal(edges[k, : L - 1], O.path_to_edges(lat.indptr, lat.indices, ref_nodes[k, :L])), k
+
+
+@pytest.mark.parametrize("order", ["index", "disjoint"])
+def test_column_via_negotiation_matches_oracle(order):
+    """The negotiation loop with per-net live costs on a column-via lattice
+    (the device routing loop, one net or one group of disjoint boxes per
+    launch): batched and sequential runs equal the oracle loop per iteration,
+    per net and in the final edge usage."""
+    from oracle.negotiate import route_plain
+    from orthoroute_b200.lattice import board_uniform_pins
+    from orthoroute_b200.negotiate import NegotiationConfig, PathFinder
+
+    b = board_uniform_pins(40, 34, 6, 60, seed=8)
+    lat = _ref_lattice(40, 34, 6)
+    cfg = NegotiationConfig(max_iterations=5, reroute="offenders", roi_margin=3, cost_update="net",
+                            full_graph_retry=False, net_order=order)
+    ref = route_plain(lat, b.src, b.dst, cfg)
+    pf = PathFinder(lat, config=cfg)
+    assert pf.dg.lattice_kind == 2 and pf.dg.route_loop_ok
+    rb = pf.route(b.src, b.dst, mode="batched")
+    rs = pf.route(b.src, b.dst, mode="sequential")
+    tr_ref = [(s, c) for s, c, _ in ref["trace"]]
+    assert rb.overuse_trace() == tr_ref and rs.overuse_trace() == tr_ref
+    for k in range(len(b.src)):
+        assert np.array_equal(rb.paths[k], ref["paths"][k]), k
+        assert np.array_equal(rs.paths[k], ref["paths"][k]), k
+    assert np.array_equal(rb.edge_usage, ref["usage"]) and np.array_equal(rs.edge_usage, ref["usage"])
