@@ -164,6 +164,13 @@ def barrier(world: int):
         dist.barrier()
 
 
+def workload_config(args, lat, nsrc: int, world: int) -> dict:
+    """The workload description both arms print (the same keys and values)."""
+    return {"workload": f"sssp_{args.nx}x{args.ny}x{args.nz}_{nsrc}src_full", "nodes": lat.N, "edges": lat.E,
+            "sources_per_step": nsrc, "weights": "fp32 uniform [1,2) planar, 3.0 via, 5% +inf",
+            "l2": "inputs larger than L2 (CSR + weights + distances ~0.6 GB)", "parallelism": f"replicas x{world}"}
+
+
 def make_workload(seed: int, nx=NX, ny=NY, nz=NZ, nsrc=NSRC):
     from orthoroute_b200.lattice import build_lattice, uniform_weights
 
@@ -887,16 +894,8 @@ def run_ours(args, world, rank, local):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded lattice and weights)",
-        "config": {
-            "workload": f"sssp_{args.nx}x{args.ny}x{args.nz}_{len(sources)}src_full",
-            "sources_per_launch": per if per else 1,
-            "nodes": lat.N,
-            "edges": lat.E,
-            "sources_per_step": len(sources),
-            "weights": "fp32 uniform [1,2) planar, 3.0 via, 5% +inf",
-            "l2": "inputs larger than L2 (CSR + weights + distances ~0.6 GB)",
-            "parallelism": f"replicas x{world}",
-        },
+        "config": workload_config(args, lat, len(sources), world),
+        "sources_per_launch": per if per else 1,
         "e2e": {"value": round(e2e_value, 4), "unit": "GTEPS",
                 "h2d_bytes_per_step": int(w.nbytes), "d2h_bytes_per_step": int(lat.N * 4 * len(sources))},
         # per launch: fill, seed and the tile search (the weight gather ran
@@ -962,8 +961,7 @@ def run_reference(args, world, rank, local):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded lattice and weights)",
-        "config": {"workload": f"sssp_{args.nx}x{args.ny}x{args.nz}_{len(sources)}src_full",
-                   "nodes": lat.N, "edges": lat.E},
+        "config": workload_config(args, lat, len(sources), world),
         "cpu_baseline": {"value": round(v, 6), "unit": "GTEPS", "cores": threads, "kind": "port",
                          "sample": f"{len(sample)} full searches per step, one per host thread"},
         "e2e": {"value": round(v, 6), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
