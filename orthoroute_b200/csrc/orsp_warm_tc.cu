@@ -7,13 +7,13 @@
 //     memory in the K-major canonical UMMA layout without swizzle (core
 //     matrices of 8 rows x 16 bytes, rows contiguous; the two 8-element halves
 //     of a 16-wide K slice 128 bytes apart, 8-row groups 256 bytes apart);
-//   - per tile, nine stages (dz, dy): 256 threads copy one input row into
-//     the three (dx) im2col blocks A[m][k] = X[z+dz][y+dy][x0+m+dx][k] of a
-//     stage buffer in the same layout (cp.async, zero outside the grid; the
-//     optional ReLU mask through registers), and one thread issues the
-//     3 x Cin/16 MMAs (K = 16 each) into the TMEM accumulator and commits them
-//     to the buffer's mbarrier, while the copies of the next stages are in
-//     flight (a ring of up to four buffers);
+//   - per tile, nine stages (dz, dy): 256 threads copy one input row once
+//     into a stage buffer (cp.async, zero outside the grid; the optional ReLU
+//     mask through registers), whose 16-byte rows serve the three (dx) taps
+//     A[m][k] = X[z+dz][y+dy][x0+m+dx][k] as descriptors one row apart, and
+//     one thread issues the 3 x Cin/16 MMAs (K = 16 each) into the TMEM
+//     accumulator and commits them to the buffer's mbarrier, while the copies
+//     of the next stages are in flight (a ring of up to six buffers);
 //   - the epilogue reads the accumulator with tcgen05.ld (warps w and w + 4
 //     share TMEM lanes 32 (w % 4) .., i.e. those voxels, and split the output
 //     channels), adds the bias, applies the ReLU and stores bf16 or fp32.
@@ -109,23 +109,28 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 }
 
 // Shared memory of the convolution: all weights (27 taps x Cin/16 K slices
-// x Cout rows of 32 bytes), NS stage buffers (3 taps x Cin/16 blocks of
-// 4096 bytes), NS mbarriers and the TMEM address slot.
+// x Cout rows of 32 bytes), NS stage buffers, NS mbarriers and the TMEM
+// address slot.  A stage buffer holds one input row of TC_M + 2 voxels as
+// Cin / 8 planes (8 channels each) of 16-byte rows, CV_PLANE bytes apart:
+// row r of plane cg at cg * CV_PLANE + r * 16.
+constexpr int CV_PLANE = (TC_M + 2) * 16;
 __host__ __device__ constexpr size_t cv_weight_bytes(int Cin, int Cout) {
   return static_cast<size_t>(27) * (Cin / 16) * Cout * 32;
 }
-__host__ __device__ constexpr size_t cv_stage_bytes(int Cin) { return static_cast<size_t>(3) * (Cin / 16) * 4096; }
+__host__ __device__ constexpr size_t cv_stage_bytes(int Cin) {
+  return (static_cast<size_t>(Cin / 8) * CV_PLANE + 127) & ~static_cast<size_t>(127);
+}
 __host__ __device__ constexpr size_t cv_smem_bytes(int Cin, int Cout, int ns) {
   return cv_weight_bytes(Cin, Cout) + ns * cv_stage_bytes(Cin) + 8 * ns + 64;
 }
-// Stage buffers that fit beside the weights in 200 KB (at most 4; 0 when
+// Stage buffers that fit beside the weights in 200 KB (at most 6; 0 when
 // fewer than 2 fit).
 inline int cv_stages(int Cin, int Cout) {
   const size_t budget = 200 * 1024;
   const size_t w = cv_weight_bytes(Cin, Cout), sb = cv_stage_bytes(Cin);
   if (w + 2 * sb + 8 * 2 + 64 > budget) return 0;
   int ns = 2;
-  while (ns < 4 && cv_smem_bytes(Cin, Cout, ns + 1) <= budget) ++ns;
+  while (ns < 6 && cv_smem_bytes(Cin, Cout, ns + 1) <= budget) ++ns;
   return ns;
 }
 
@@ -135,20 +140,26 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src, int bytes
                : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-// Waits until at most n (0..2) of this thread's copy groups are pending.
+// Waits until at most n (0..4) of this thread's copy groups are pending.
 __device__ __forceinline__ void cp_async_wait(int n) {
   if (n <= 0) asm volatile("cp.async.wait_group 0;" ::: "memory");
   else if (n == 1) asm volatile("cp.async.wait_group 1;" ::: "memory");
-  else asm volatile("cp.async.wait_group 2;" ::: "memory");
+  else if (n == 2) asm volatile("cp.async.wait_group 2;" ::: "memory");
+  else if (n == 3) asm volatile("cp.async.wait_group 3;" ::: "memory");
+  else asm volatile("cp.async.wait_group 4;" ::: "memory");
 }
 
 constexpr int CV_THREADS = 256;  // eight warps gather; warps w and w + 4 share TMEM lanes 32 (w % 4)..
 
 // Pipelined implicit GEMM.  A stage is one input row (plane z + dz, row
-// y + dy) of a tile: the 130 voxels x0 - 1 .. x0 + 128 are read once, 16
-// bytes at a time with cp.async (zero fill outside the grid), and written to
-// the three shifted im2col blocks of the taps dx = -1, 0, 1 (row m of tap dx
-// holds voxel x0 + m + dx).  Stages run through a ring of NS buffers: while
+// y + dy) of a tile: the 130 voxels x0 - 1 .. x0 + 128 are copied once, 16
+// bytes at a time with cp.async (zero fill outside the grid), into the
+// stage's channel planes.  The A operand of tap dx is that buffer itself: in
+// the K-major layout without swizzle, a stride of 128 bytes between 8-row
+// core-matrix groups puts row m at 16 m bytes, so the descriptor of tap dx
+// starts (dx + 1) rows in (row m of tap dx = voxel x0 + m + dx), with the
+// planes of a 16-channel K slice CV_PLANE bytes apart.  One copy serves the
+// three taps.  Stages run through a ring of NS buffers: while
 // the tensor core consumes stage s, the copies of stages s + 1 .. s + NS - 1
 // are in flight.  Buffer b's mbarrier completes when the MMAs of the stage
 // last held in b are done (tcgen05.commit), which is what a refill of b waits
@@ -214,31 +225,22 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
   // copies of stage s into buffer s % NS (nothing past the last stage); one
   // commit group per call on every thread, so the group counts stay uniform
   // This thread's share of a stage is the same for every stage: units
-  // u = tid + j * CV_THREADS of (groups of 8 voxels) x CG channel groups,
-  // channel-group major inside a group, so the 8 lanes of a 16-byte store
-  // phase write 8 consecutive rows of one core-matrix column (128 contiguous
-  // bytes, no bank conflict) while a warp reads 512 contiguous bytes.  Per
-  // unit: x offset from x0, element offset in the row and the three tap
-  // destinations (-1 where the shifted row falls outside the tile).
-  constexpr int CIN = CG * 8, KCC = CG / 2;
-  constexpr int UNITS = (TC_M + 2 + 7) / 8 * 8 * CG;
+  // u = tid + j * CV_THREADS of (130 voxels) x CG channel groups, channel
+  // group fastest, so a warp reads 512 contiguous bytes and the 8 lanes of a
+  // 16-byte store phase hit all 32 banks (planes CV_PLANE = 8 banks apart).
+  // Per unit: x offset from x0, element offset in the row, destination.
+  constexpr int CIN = CG * 8;
+  constexpr int UNITS = (TC_M + 2) * CG;
   constexpr int UPT = (UNITS + CV_THREADS - 1) / CV_THREADS;
-  int u_x[UPT], u_off[UPT], u_dst[UPT][3];
+  int u_x[UPT], u_off[UPT], u_dst[UPT];
 #pragma unroll
   for (int j = 0; j < UPT; ++j) {
     const int i = tid + j * CV_THREADS;
-    const int grp = i / (8 * CG), r8 = i % (8 * CG);
-    const int cg = r8 >> 3, vx = grp * 8 + (r8 & 7);
-    const bool unit = i < UNITS && vx < TC_M + 2;
+    const int vx = i / CG, cg = i % CG;
+    const bool unit = i < UNITS;
     u_x[j] = unit ? vx - 1 : INT_MIN / 2;
     u_off[j] = (vx - 1) * CIN + cg * 8;
-#pragma unroll
-    for (int dxi = 0; dxi < 3; ++dxi) {
-      const int m = vx - dxi;
-      u_dst[j][dxi] = (unit && m >= 0 && m < TC_M)
-                          ? (dxi * KCC + (cg >> 1)) * 4096 + (m >> 3) * 256 + (cg & 1) * 128 + (m & 7) * 16
-                          : -1;
-    }
+    u_dst[j] = unit ? cg * CV_PLANE + vx * 16 : -1;
   }
 
   // copies of stage s into buffer s % NS (nothing past the last stage); one
@@ -259,10 +261,9 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
         const int xx = x0 + u_x[j];
         const bool in = rowok && xx >= 0 && xx < W;
         const __nv_bfloat16 *src = in ? row + u_off[j] : X;
+        if (u_dst[j] < 0) continue;
         if (!Mk) {
-#pragma unroll
-          for (int dxi = 0; dxi < 3; ++dxi)
-            if (u_dst[j][dxi] >= 0) cp_async16(buf + u_dst[j][dxi], src, in ? 16 : 0);
+          cp_async16(buf + u_dst[j], src, in ? 16 : 0);
         } else {
           uint4 v = make_uint4(0, 0, 0, 0);
           if (in) {
@@ -274,9 +275,7 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
             for (int q = 0; q < 8; ++q)
               if (!(__bfloat162float(pm[q]) > 0.0f)) pv[q] = __float2bfloat16(0.0f);
           }
-#pragma unroll
-          for (int dxi = 0; dxi < 3; ++dxi)
-            if (u_dst[j][dxi] >= 0) *reinterpret_cast<uint4 *>(buf + u_dst[j][dxi]) = v;
+          *reinterpret_cast<uint4 *>(buf + u_dst[j]) = v;
         }
       }
     }
@@ -302,7 +301,8 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
 #pragma unroll 1
       for (int dxi = 0; dxi < 3; ++dxi)
         for (int kc = 0; kc < KC; ++kc) {
-          const uint64_t a = umma_smem_desc(smem_addr(sA + b * SBY + (dxi * KC + kc) * 4096), 128, 256);
+          const uint64_t a =
+              umma_smem_desc(smem_addr(sA + b * SBY + (2 * kc) * CV_PLANE + dxi * 16), CV_PLANE, 128);
           const uint64_t bd = umma_smem_desc(smem_addr(sB + ((tapz + dxi) * KC + kc) * bblk), 128, 256);
           mma_bf16(tmem, a, bd, idesc, (st9 | dxi | kc) != 0 ? 1u : 0u);
         }
