@@ -124,12 +124,11 @@ __host__ __device__ constexpr size_t cv_smem_bytes(int Cin, int Cout, int ns) {
   return cv_weight_bytes(Cin, Cout) + ns * cv_stage_bytes(Cin) + 8 * ns + 64;
 }
 // Stage buffers that fit beside the weights in 200 KB (at most 6; 0 when
-// fewer than 2 fit).
+// fewer than 3 fit).
 inline int cv_stages(int Cin, int Cout) {
   const size_t budget = 200 * 1024;
-  const size_t w = cv_weight_bytes(Cin, Cout), sb = cv_stage_bytes(Cin);
-  if (w + 2 * sb + 8 * 2 + 64 > budget) return 0;
-  int ns = 2;
+  if (cv_smem_bytes(Cin, Cout, 3) > budget) return 0;
+  int ns = 3;
   while (ns < 6 && cv_smem_bytes(Cin, Cout, ns + 1) <= budget) ++ns;
   return ns;
 }
@@ -160,8 +159,8 @@ constexpr int CV_THREADS = 256;  // eight warps gather; warps w and w + 4 share 
 // starts (dx + 1) rows in (row m of tap dx = voxel x0 + m + dx), with the
 // planes of a 16-channel K slice CV_PLANE bytes apart.  One copy serves the
 // three taps.  Stages run through a ring of NS buffers: while
-// the tensor core consumes stage s, the copies of stages s + 1 .. s + NS - 1
-// are in flight.  Buffer b's mbarrier completes when the MMAs of the stage
+// the tensor core consumes stages s - 1 and s, the copies of stages
+// s + 1 .. s + NS - 2 are in flight.  Buffer b's mbarrier completes when the MMAs of the stage
 // last held in b are done (tcgen05.commit), which is what a refill of b waits
 // for; the 9th stage of a tile also releases the epilogue.  With the ReLU
 // mask the gather goes through registers (plain loads and shared stores).
@@ -282,7 +281,9 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
     cp_async_commit();
   };
 
-  for (int64_t s = 0; s < NS - 1; ++s) issue(s);
+  // the copies run NS - 2 stages ahead; a buffer is refilled two stages
+  // after its MMAs were issued, so their completion is not waited for at once
+  for (int64_t s = 0; s < NS - 2; ++s) issue(s);
   bool ok = true;
   int64_t s = 0, issued = -1;  // issued: the last stage whose MMAs were committed
   for (; s < nst; ++s) {
@@ -290,7 +291,7 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
     const int st9 = static_cast<int>(s % 9);
     // this thread's copies of stage s have landed; hand them to the async
     // proxy, then every thread's (and a failed wait anywhere ends the loop)
-    cp_async_wait(NS - 2);
+    cp_async_wait(NS - 3);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     ok = __syncthreads_and(ok ? 1 : 0) != 0;
@@ -311,10 +312,10 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
                    : "memory");
     }
     issued = s;
-    // refill the buffer of stage s - 1 with stage s + NS - 1 once its MMAs
-    // are done (for s = 0 that buffer has not been used yet)
-    if (s >= 1) ok = mbar_wait(smem_addr(bars + (s - 1) % NS), static_cast<uint32_t>(((s - 1) / NS) & 1));
-    issue(s + NS - 1);
+    // refill the buffer of stage s - 2 with stage s + NS - 2 once its MMAs
+    // are done (for s < 2 that buffer has not been used yet)
+    if (s >= 2) ok = mbar_wait(smem_addr(bars + (s - 2) % NS), static_cast<uint32_t>(((s - 2) / NS) & 1));
+    issue(s + NS - 2);
     if (st9 == 8) {
       // last stage of the tile: the accumulator is final once its MMAs are
       ok = __syncthreads_and((ok && mbar_wait(smem_addr(bars + b), static_cast<uint32_t>((s / NS) & 1))) ? 1 : 0) != 0;
