@@ -242,18 +242,42 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
     u_dst[j] = unit ? cg * CV_PLANE + vx * 16 : -1;
   }
 
-  // copies of stage s into buffer s % NS (nothing past the last stage); one
+  // Stage cursors advance by one stage at a time (no division per stage):
+  // stage index within the tile (dz * 3 + dy), ring buffer and its phase
+  // parity, and the tile with its coordinates (divisions once per tile).
+  const int ntiles32 = static_cast<int>(ntiles);
+  const int nst32 = static_cast<int>(nst);
+  struct Cursor {
+    int st9, buf, par, t, tx, y, z;
+  };
+  auto tile_coords = [&](Cursor &c) {
+    c.tx = c.t % ntx;
+    const int zy = c.t / ntx;
+    c.y = zy % H;
+    c.z = zy / H;
+  };
+  auto advance = [&](Cursor &c) {
+    if (++c.buf == NS) {
+      c.buf = 0;
+      c.par ^= 1;
+    }
+    if (++c.st9 == 9) {
+      c.st9 = 0;
+      c.t += gridDim.x;
+      if (c.t < ntiles32) tile_coords(c);
+    }
+  };
+
+  // copies of the stage at cursor ci (nothing past the last stage); one
   // commit group per call on every thread, so the group counts stay uniform
-  auto issue = [&](int64_t s) {
-    if (s < nst) {
-      const int64_t t = blockIdx.x + (s / 9) * static_cast<int64_t>(gridDim.x);
-      const int st9 = static_cast<int>(s % 9);
-      const int tx = static_cast<int>(t % ntx);
-      const int64_t zy = t / ntx;
-      const int y = static_cast<int>(zy % H), z = static_cast<int>(zy / H);
-      const int zz = z + st9 / 3 - 1, yy = y + st9 % 3 - 1, x0 = tx * TC_M;
+  Cursor ci{0, 0, 0, static_cast<int>(blockIdx.x), 0, 0, 0};
+  tile_coords(ci);
+  int si = 0;  // the stage ci points at
+  auto issue = [&]() {
+    if (si < nst32) {
+      const int zz = ci.z + ci.st9 / 3 - 1, yy = ci.y + ci.st9 % 3 - 1, x0 = ci.tx * TC_M;
       const bool rowok = zz >= 0 && zz < D && yy >= 0 && yy < H;
-      unsigned char *buf = sA + static_cast<size_t>(s % NS) * SBY;
+      unsigned char *buf = sA + static_cast<size_t>(ci.buf) * SBY;
       const __nv_bfloat16 *row = X + ((static_cast<int64_t>(rowok ? zz : 0) * H + (rowok ? yy : 0)) * W + x0) * CIN;
 #pragma unroll
       for (int j = 0; j < UPT; ++j) {
@@ -277,18 +301,23 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
           *reinterpret_cast<uint4 *>(buf + u_dst[j]) = v;
         }
       }
+      advance(ci);
     }
+    ++si;
     cp_async_commit();
   };
 
   // the copies run NS - 2 stages ahead; a buffer is refilled two stages
   // after its MMAs were issued, so their completion is not waited for at once
-  for (int64_t s = 0; s < NS - 2; ++s) issue(s);
+  for (int k = 0; k < NS - 2; ++k) issue();
   bool ok = true;
-  int64_t s = 0, issued = -1;  // issued: the last stage whose MMAs were committed
-  for (; s < nst; ++s) {
-    const int b = static_cast<int>(s % NS);
-    const int st9 = static_cast<int>(s % 9);
+  Cursor cc{0, 0, 0, static_cast<int>(blockIdx.x), 0, 0, 0};  // the stage consumed
+  tile_coords(cc);
+  Cursor cw{0, 0, 0, static_cast<int>(blockIdx.x), 0, 0, 0};  // two stages behind: the buffer refilled next
+  int s = 0, issued_buf = -1, issued_par = 0;  // the last stage whose MMAs were committed
+  for (; s < nst32; ++s) {
+    const int b = cc.buf;
+    const int st9 = cc.st9;
     // this thread's copies of stage s have landed; hand them to the async
     // proxy, then every thread's (and a failed wait anywhere ends the loop)
     cp_async_wait(NS - 3);
@@ -311,20 +340,21 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
                        smem_addr(bars + b))
                    : "memory");
     }
-    issued = s;
+    issued_buf = b;
+    issued_par = cc.par;
     // refill the buffer of stage s - 2 with stage s + NS - 2 once its MMAs
     // are done (for s < 2 that buffer has not been used yet)
-    if (s >= 2) ok = mbar_wait(smem_addr(bars + (s - 2) % NS), static_cast<uint32_t>(((s - 2) / NS) & 1));
-    issue(s + NS - 2);
+    if (s >= 2) {
+      ok = mbar_wait(smem_addr(bars + cw.buf), static_cast<uint32_t>(cw.par));
+      advance(cw);
+    }
+    issue();
     if (st9 == 8) {
       // last stage of the tile: the accumulator is final once its MMAs are
-      ok = __syncthreads_and((ok && mbar_wait(smem_addr(bars + b), static_cast<uint32_t>((s / NS) & 1))) ? 1 : 0) != 0;
+      ok = __syncthreads_and((ok && mbar_wait(smem_addr(bars + b), static_cast<uint32_t>(cc.par))) ? 1 : 0) != 0;
       if (!ok) break;
       tc_fence_after();
-      const int64_t t = blockIdx.x + (s / 9) * static_cast<int64_t>(gridDim.x);
-      const int tx = static_cast<int>(t % ntx);
-      const int64_t zy = t / ntx;
-      const int y = static_cast<int>(zy % H), z = static_cast<int>(zy / H);
+      const int tx = cc.tx, y = cc.y, z = cc.z;
       // warp w: voxels 32 (w % 4) .. + 31 (its TMEM lanes), channel blocks
       // of 16 starting at 16 (w / 4), every second one
       const int m = (warp & 3) * 32 + lane, xx = tx * TC_M + m;
@@ -358,6 +388,7 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
       // are ordered before it by the next iteration's barrier
       tc_fence_before();
     }
+    advance(cc);
   }
   cp_async_wait(0);
   if (!ok) {
@@ -365,7 +396,7 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
     // bounded wait (the last stage committed, which completes after all
     // earlier ones) before the accumulator is freed
     if (tid == 0) atomicExch(&g_tc_err, 1);
-    if (issued >= 0) mbar_wait(smem_addr(bars + issued % NS), static_cast<uint32_t>((issued / NS) & 1));
+    if (issued_buf >= 0) mbar_wait(smem_addr(bars + issued_buf), static_cast<uint32_t>(issued_par));
   }
   tc_fence_before();
   __syncthreads();
@@ -574,6 +605,10 @@ extern "C" int orsp_warm_conv3d_tc(const void *X, const void *mask, const void *
   }
   ORSP_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t ntiles = static_cast<int64_t>(D) * H * ((W + TC_M - 1) / TC_M);
+  if (ntiles * 9 > INT32_MAX) {
+    set_error("warm_conv3d_tc: grid too large (the stage counters are 32-bit)");
+    return ORSP_ERR_ARG;
+  }
   const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(ntiles, sms)));
   kfn<<<grid, CV_THREADS, smem, (cudaStream_t)stream>>>((const __nv_bfloat16 *)X, (const __nv_bfloat16 *)mask,
                                                         (const __nv_bfloat16 *)Wt, bias, (__nv_bfloat16 *)Y, Yf, D, H,
