@@ -201,7 +201,7 @@ class WarmNet:
         # convolution kernel: "tc" (tcgen05.mma with a TMEM accumulator,
         # orsp_warm_conv3d_tc) or "wmma" (orsp_warm_conv3d); ORSP_WARM_CONV
         # overrides the default
-        self.conv_impl = os.environ.get("ORSP_WARM_CONV", "wmma")
+        self.conv_impl = os.environ.get("ORSP_WARM_CONV", "tc")
         self.features = FEATURES  # input feature set (board_features version)
 
     def _conv_call(self, *args):
