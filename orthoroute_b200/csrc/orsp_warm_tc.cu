@@ -465,10 +465,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) wgrad_tc_kernel(
   const int nxc = (W + WG_K - 1) / WG_K;
   const int64_t nchunks = static_cast<int64_t>(D) * H * nxc;
   const int cg_in = Cin / 8, cg_out = Cout / 8;
-  for (int64_t t = blockIdx.x; t < nchunks && ok; t += gridDim.x) {
-    const int xc = static_cast<int>(t % nxc);
-    const int64_t zy = t / nxc;
-    const int y = static_cast<int>(zy % H), z = static_cast<int>(zy / H);
+  // 32-bit chunk arithmetic (the host rejects grids with more chunks)
+  for (int t = blockIdx.x; t < static_cast<int>(nchunks) && ok; t += gridDim.x) {
+    const int xc = t % nxc;
+    const int zy = t / nxc;
+    const int y = zy % H, z = zy / H;
     const int x0 = xc * WG_K;
     // B: G of the chunk's 32 voxels, 8 output channels per unit
     for (int i = tid; i < WG_K * cg_out; i += TC_THREADS) {
@@ -640,6 +641,10 @@ extern "C" int orsp_warm_wgrad_tc(const void *X, const void *dY, const void *Yo,
   ORSP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   ORSP_CUDA(cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t nchunks = static_cast<int64_t>(D) * H * ((W + WG_K - 1) / WG_K);
+  if (nchunks > INT32_MAX) {
+    set_error("warm_wgrad_tc: grid too large (the chunk counter is 32-bit)");
+    return ORSP_ERR_ARG;
+  }
   const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(nchunks, sms)));
   wgrad_tc_kernel<<<grid, TC_THREADS, smem, st>>>((const __nv_bfloat16 *)X, (const __nv_bfloat16 *)dY,
                                                   (const __nv_bfloat16 *)Yo, dW, D, H, W, Cin, Cout);
