@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "fastdiv.cuh"
 
 namespace {
 
@@ -107,6 +108,36 @@ __global__ void fill_box_kernel(uint32_t *p, int32_t nx, int32_t ny, int32_t x0,
   }
 }
 
+// Cell i of a box (x fastest, then y, then z) as coordinates: multiply-high
+// divisions while the box has fewer than 2^32 cells (the common case),
+// 64-bit divisions otherwise.
+struct BoxIndex {
+  FastDiv fw, fp;
+  uint32_t w;
+  bool fast;
+  __device__ __forceinline__ void init(int64_t bw, int64_t bh, int64_t count) {
+    fast = count < ((int64_t)1 << 32) && bw * bh < ((int64_t)1 << 31);
+    w = (uint32_t)bw;
+    if (fast) {
+      fw.init((uint32_t)bw);
+      fp.init((uint32_t)(bw * bh));
+    }
+  }
+  __device__ __forceinline__ void split(int64_t i, int64_t plane, int32_t &z, int32_t &y, int32_t &x) const {
+    if (fast) {
+      const uint32_t u = (uint32_t)i, zz = fp.div(u), r = u - zz * (uint32_t)plane, yy = fw.div(r);
+      z = (int32_t)zz;
+      y = (int32_t)yy;
+      x = (int32_t)(r - yy * w);
+    } else {
+      const int64_t zz = i / plane, r = i - zz * plane, yy = r / w;
+      z = (int32_t)zz;
+      y = (int32_t)yy;
+      x = (int32_t)(r - yy * w);
+    }
+  }
+};
+
 // In-edge weights of node v as one float4 {from lower axis neighbour, from
 // upper axis neighbour, via from below, via from above}; +inf where absent.
 __global__ void gather_kernel(const int32_t *__restrict__ slot_eid, const float *__restrict__ cost,
@@ -127,10 +158,11 @@ __global__ void gather_box_kernel(const int32_t *__restrict__ slot_eid, const fl
   const float INF_F = __int_as_float(0x7f800000);
   const int64_t s = (int64_t)gridDim.x * blockDim.x;
   const int64_t plane = (int64_t)bw * bh;
+  BoxIndex bi;
+  bi.init(bw, bh, count);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += s) {
-    const int64_t z = i / plane;
-    const int64_t r = i - z * plane;
-    const int32_t y = (int32_t)(r / bw), x = (int32_t)(r - (int64_t)y * bw);
+    int32_t z, y, x;
+    bi.split(i, plane, z, y, x);
     const int64_t v = ((int64_t)(z0 + z) * ny + (y0 + y)) * nx + (x0 + x);
     const int32_t e0 = slot_eid[v], e1 = slot_eid[n + v], e2 = slot_eid[2 * n + v], e3 = slot_eid[3 * n + v];
     w[v] = make_float4(e0 >= 0 ? __ldg(&cost[e0]) : INF_F, e1 >= 0 ? __ldg(&cost[e1]) : INF_F,
@@ -213,10 +245,11 @@ __global__ void gather_roi_kernel(const int32_t *__restrict__ slot_eid, const fl
   const int64_t plane = bw * bh, count = plane * bd;
   const int64_t nxy = (int64_t)G.nx * G.ny;
   const int64_t s = (int64_t)gridDim.x * blockDim.x;
+  BoxIndex bi;
+  bi.init(bw, bh, count);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += s) {
-    const int64_t zz = i / plane;
-    const int64_t r = i - zz * plane;
-    const int64_t yy = r / bw, xx = r - yy * bw;
+    int32_t zz, yy, xx;
+    bi.split(i, plane, zz, yy, xx);
     const int32_t gz = B.z0 + (int32_t)zz;
     const int64_t v = (int64_t)gz * nxy + (int64_t)(B.y0 + yy) * G.nx + (B.x0 + xx);
     const bool vin = !roi_map || __ldg(&roi_map[v]) >= 0;
@@ -254,11 +287,15 @@ __global__ void gather_col_kernel(const int32_t *__restrict__ vcol_eid, const fl
   const int64_t plane = bw * bh, cells = plane * bd, count = cells * bd;
   const int64_t nxy = (int64_t)nx * ny;
   const int64_t s = (int64_t)gridDim.x * blockDim.x;
+  // cells of the box stacked bd times (one copy per source layer): the
+  // "layer" coordinate of this split runs over bd * bd
+  BoxIndex bi;
+  bi.init(bw, bh, count);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += s) {
-    const int64_t za = B.z0 + i / cells;  // source layer
-    const int64_t c = i - (i / cells) * cells;
-    const int64_t zz = c / plane, r = c - zz * plane;
-    const int64_t yy = r / bw, xx = r - yy * bw;
+    int32_t zq, yy, xx;
+    bi.split(i, plane, zq, yy, xx);
+    const int64_t za = B.z0 + zq / (int32_t)bd;  // source layer
+    const int32_t zz = zq - (int32_t)((za - B.z0) * bd);
     const int64_t col = (int64_t)(B.y0 + yy) * nx + (B.x0 + xx);
     const int64_t v = (int64_t)(B.z0 + zz) * nxy + col;
     const int32_t e0 = __ldg(&vcol_eid[za * n + v]), e1 = __ldg(&vcol_eid[((int64_t)nz + za) * n + v]);
