@@ -190,13 +190,16 @@ __global__ void roi_bbox_kernel(const int32_t *__restrict__ nodes, int64_t n, co
   for (int k = 0; k < 6; ++k) m[k] = INT_MIN;
   const int64_t plane = (int64_t)nx * ny;
   const int64_t s = (int64_t)gridDim.x * blockDim.x;
+  // node ids are int32 (N < 2^31): multiply-high divisions
+  FastDiv fp, fx;
+  fp.init((uint32_t)plane);
+  fx.init((uint32_t)nx);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += s) {
     const int64_t v = nodes ? (int64_t)__ldg(&nodes[i]) : i;
     if (v < 0 || v >= N) continue;
     if (!nodes && __ldg(&roi_map[v]) < 0) continue;
-    const int32_t z = (int32_t)(v / plane);
-    const int64_t r = v - (int64_t)z * plane;
-    const int32_t y = (int32_t)(r / nx), x = (int32_t)(r - (int64_t)y * nx);
+    const uint32_t u = (uint32_t)v, zu = fp.div(u), r = u - zu * (uint32_t)plane, yu = fx.div(r);
+    const int32_t z = (int32_t)zu, y = (int32_t)yu, x = (int32_t)(r - yu * (uint32_t)nx);
     m[0] = max(m[0], -x);
     m[1] = max(m[1], x);
     m[2] = max(m[2], -y);
