@@ -496,12 +496,12 @@ def route_c3(dev, with_cpu: bool):
 
     import torch
 
-    from orthoroute_b200.warm import load_pretrained, warm_history
+    from orthoroute_b200.warm import load_pretrained, warm_history_device
 
     net, scale = load_pretrained(device=dev)
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
-    h0 = warm_history(net, b.lattice, b.src, b.dst, scale)
+    h0 = warm_history_device(net, b.lattice, b.src, b.dst, scale)
     torch.cuda.synchronize(dev)
     t_pred = time.perf_counter() - t0
     # the warm run keeps the plain schedule (per-net live costs from the first

@@ -286,9 +286,9 @@ def route_board(board_data: dict, pitch: float = DEFAULT_PITCH, max_iterations: 
     pf = PathFinder(prob.lattice, config=cfg, device=device)
     hist = None
     if warm:
-        from .warm import load_pretrained, warm_history
+        from .warm import load_pretrained, warm_history_device
         net, scale = load_pretrained(device=pf.device)
-        hist = warm_history(net, prob.lattice, prob.search_src, prob.search_dst, scale)
+        hist = warm_history_device(net, prob.lattice, prob.search_src, prob.search_dst, scale)
     metrics = []
 
     def cb(s):

@@ -60,11 +60,30 @@ def _box_blur(a: np.ndarray, r: int) -> np.ndarray:
 FEATURES = 2  # feature set of newly built networks (see board_features)
 
 
-def board_features(lat: Lattice, src: np.ndarray, dst: np.ndarray, version: int = FEATURES) -> np.ndarray:
-    """float32 [nz][ny][nx][16] input features of a board (host).  Channels:
-    0 pins on the pin layer, 1 blurred pin density, 2 airwire crossing density,
-    3 bounding-box coverage, 4 / 5 H / V layer, 6 layer position; version 2
-    adds 7, log1p of the RUDY wire density (rudy_density)."""
+def _segment_points(a, b, c, d):
+    """The cells of every pin-to-pin segment rasterised at unit steps, as
+    np.rint(np.linspace(a, c, n)) and np.rint(np.linspace(b, d, n)) with
+    n = max(|c - a|, |d - b|) + 1 give them per segment (linspace's
+    k * step + start, its exact end point), for all segments at once."""
+    a, b, c, d = (np.asarray(v, np.int64) for v in (a, b, c, d))
+    n = np.maximum(np.abs(c - a), np.abs(d - b)) + 1
+    seg = np.repeat(np.arange(n.size), n)
+    k = np.arange(seg.size) - np.repeat(np.cumsum(n) - n, n)
+    div = np.maximum(n - 1, 1).astype(np.float64)
+
+    def coord(p, q):
+        step = (q - p).astype(np.float64) / div
+        y = k.astype(np.float64) * step[seg] + p[seg].astype(np.float64)
+        last = (k == n[seg] - 1) & (n[seg] > 1)
+        y[last] = q[seg][last]
+        return np.rint(y).astype(np.int64)
+
+    return coord(a, c), coord(b, d)
+
+
+def board_maps(lat: Lattice, src: np.ndarray, dst: np.ndarray, version: int = FEATURES) -> dict:
+    """The board-dependent 2-D maps of board_features (host, float32 [ny][nx]),
+    the pin layer, and the layer flags."""
     nx, ny, nz = lat.nx, lat.ny, lat.nz
     sx, sy, sz = (np.asarray(v) for v in lat.coords(np.asarray(src)))
     dx, dy, dz = (np.asarray(v) for v in lat.coords(np.asarray(dst)))
@@ -72,12 +91,9 @@ def board_features(lat: Lattice, src: np.ndarray, dst: np.ndarray, version: int 
     np.add.at(pins, (sy, sx), 1.0)
     np.add.at(pins, (dy, dx), 1.0)
     # airwire crossing density: each pin-to-pin segment rasterised at unit steps
-    air = np.zeros((ny, nx), np.float32)
-    for a, b, c, d in zip(sx, sy, dx, dy):
-        n = int(max(abs(int(c) - int(a)), abs(int(d) - int(b)))) + 1
-        xs = np.rint(np.linspace(a, c, n)).astype(np.int64)
-        ys = np.rint(np.linspace(b, d, n)).astype(np.int64)
-        air[ys, xs] += 1.0
+    # (integer counts, exact in float32)
+    xs, ys = _segment_points(sx, sy, dx, dy)
+    air = np.bincount(ys * nx + xs, minlength=ny * nx).astype(np.float32).reshape(ny, nx)
     cov = np.zeros((ny + 1, nx + 1), np.float32)
     x0, x1 = np.minimum(sx, dx), np.maximum(sx, dx) + 1
     y0, y1 = np.minimum(sy, dy), np.maximum(sy, dy) + 1
@@ -86,20 +102,57 @@ def board_features(lat: Lattice, src: np.ndarray, dst: np.ndarray, version: int 
     np.add.at(cov, (y1, x0), -1.0)
     np.add.at(cov, (y1, x1), 1.0)
     cov = cov.cumsum(0).cumsum(1)[:ny, :nx]
-    dirs = layer_directions(nz)
+    m = {"pin_layer": int(np.bincount(np.concatenate([sz, dz]).astype(np.int64), minlength=nz).argmax()),
+         "pins": pins, "pin_blur": _box_blur(pins, 4) * 4.0, "air": _box_blur(air, 2) / 8.0, "cov": cov / 32.0,
+         "dirs": layer_directions(nz)}
+    if version >= 2:
+        m["rudy"] = np.log1p(rudy_density(lat, src, dst)).astype(np.float32)
+    return m
+
+
+def board_features(lat: Lattice, src: np.ndarray, dst: np.ndarray, version: int = FEATURES) -> np.ndarray:
+    """float32 [nz][ny][nx][16] input features of a board (host).  Channels:
+    0 pins on the pin layer, 1 blurred pin density, 2 airwire crossing density,
+    3 bounding-box coverage, 4 / 5 H / V layer, 6 layer position; version 2
+    adds 7, log1p of the RUDY wire density (rudy_density)."""
+    nx, ny, nz = lat.nx, lat.ny, lat.nz
+    m = board_maps(lat, src, dst, version)
     f = np.zeros((nz, ny, nx, F_IN), np.float32)
-    pin_layer = int(np.bincount(np.concatenate([sz, dz]).astype(np.int64), minlength=nz).argmax())
-    f[pin_layer, :, :, 0] = pins
-    f[:, :, :, 1] = _box_blur(pins, 4)[None] * 4.0
-    f[:, :, :, 2] = _box_blur(air, 2)[None] / 8.0
-    f[:, :, :, 3] = cov[None] / 32.0
-    for z, d in enumerate(dirs):
+    f[m["pin_layer"], :, :, 0] = m["pins"]
+    f[:, :, :, 1] = m["pin_blur"][None]
+    f[:, :, :, 2] = m["air"][None]
+    f[:, :, :, 3] = m["cov"][None]
+    for z, d in enumerate(m["dirs"]):
         f[z, :, :, 4] = 1.0 if "h" in d else 0.0
         f[z, :, :, 5] = 1.0 if "v" in d else 0.0
         f[z, :, :, 6] = z / max(1, nz - 1)
     if version >= 2:
-        f[:, :, :, 7] = np.log1p(rudy_density(lat, src, dst)).astype(np.float32)[None]
+        f[:, :, :, 7] = m["rudy"][None]
     return f
+
+
+def board_features_device(lat: Lattice, src, dst, version: int = FEATURES, device=None) -> torch.Tensor:
+    """board_features assembled on the device, as the network reads it: bf16
+    [nz][H8][W8][16] with H, W padded to multiples of 8 with zeros.  The 2-D
+    maps come from board_maps (host, float32), so every value equals the
+    host array's after the same bf16 conversion."""
+    dev = torch.device(device) if device is not None else torch.device("cuda")
+    nx, ny, nz = lat.nx, lat.ny, lat.nz
+    m = board_maps(lat, src, dst, version)
+    Hp, Wp = (ny + 7) // 8 * 8, (nx + 7) // 8 * 8
+    f = torch.zeros((nz, Hp, Wp, F_IN), dtype=torch.float32, device=dev)
+    up = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    f[m["pin_layer"], :ny, :nx, 0] = up(m["pins"])
+    f[:, :ny, :nx, 1] = up(m["pin_blur"])[None]
+    f[:, :ny, :nx, 2] = up(m["air"])[None]
+    f[:, :ny, :nx, 3] = up(m["cov"])[None]
+    for z, d in enumerate(m["dirs"]):
+        f[z, :ny, :nx, 4] = 1.0 if "h" in d else 0.0
+        f[z, :ny, :nx, 5] = 1.0 if "v" in d else 0.0
+        f[z, :ny, :nx, 6] = z / max(1, nz - 1)
+    if version >= 2:
+        f[:, :ny, :nx, 7] = up(m["rudy"])[None]
+    return f.to(torch.bfloat16)
 
 
 def node_targets(lat: Lattice, history: np.ndarray, blur: int = 0) -> np.ndarray:
@@ -395,6 +448,21 @@ def warm_history(net: "WarmNet", lat: Lattice, src, dst, scale: float) -> np.nda
     return history_from_prediction(lat, pred, scale)
 
 
+def warm_history_device(net: "WarmNet", lat: Lattice, src, dst, scale: float) -> torch.Tensor:
+    """warm_history with the feature assembly, the forward pass and the
+    node -> edge mapping on the device: float32 [E] (device).  The mapping is
+    history_from_prediction's (expm1 of the clamped prediction in float64,
+    times scale, rounded to float32)."""
+    dev = net.device
+    x = board_features_device(lat, np.asarray(src), np.asarray(dst), net.features, device=dev)
+    out = net.forward(x)[:, :lat.ny, :lat.nx, :USED].float()
+    p = torch.expm1(torch.clamp(out.reshape(lat.N, 2).double(), min=0.0))
+    indptr = torch.from_numpy(np.ascontiguousarray(lat.indptr, dtype=np.int64)).to(dev)
+    es = torch.repeat_interleave(torch.arange(lat.N, device=dev), indptr[1:] - indptr[:-1])
+    ek = torch.from_numpy(np.ascontiguousarray(lat.edge_kind)).to(dev).long()
+    return (p[es, ek] * float(scale)).float()
+
+
 def _main(argv=None):
     """python -m orthoroute_b200.warm [--size 400] [--nz 18] [--seed 3] [--reps 3]:
     the shipped network's prediction for a footprint board at the backplane's
@@ -439,8 +507,15 @@ def _main(argv=None):
     torch.cuda.synchronize()
     conv_ms = e0.elapsed_time(e1) / a.reps
     flops = 2.0 * 27 * net.C * net.C * D * H * W
+    t_hist = {}
+    for name, fn in (("host", warm_history), ("device", warm_history_device)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn(net, b.lattice, b.src, b.dst, scale)
+        torch.cuda.synchronize()
+        t_hist[name] = round(time.perf_counter() - t0, 3)
     print(json.dumps({"board": f"{a.size}x{a.size}x{a.nz}", "voxels": D * H * W, "features_s": round(t_feat, 3),
-                      "forward_ms": round(fwd_ms, 2), "conv32_ms": round(conv_ms, 3),
+                      "warm_history_s": t_hist, "forward_ms": round(fwd_ms, 2), "conv32_ms": round(conv_ms, 3),
                       "conv32_tflops": round(flops / (conv_ms / 1e3) / 1e12, 1), "history_scale": scale}))
 
 

@@ -117,3 +117,23 @@ def test_shipped_warm_start_gains_over_zero_history():
     assert r0.converged and rw.converged
     assert sw < s0
     assert abs(rw.wirelength - r0.wirelength) <= 0.02 * r0.wirelength
+
+
+def test_warm_history_device_matches_host():
+    """warm_history_device (features assembled, run and mapped to edges on
+    the device) gives warm_history's per-edge history: the same network
+    outputs, the same float64 expm1 and scale up to the last bit of the
+    device's expm1, so at most one float32 ulp apart, on a board whose H and W
+    are not multiples of 8."""
+    from orthoroute_b200.lattice import board_footprints
+    from orthoroute_b200.warm import load_pretrained, warm_history, warm_history_device
+
+    b = board_footprints(203, 117, 18, 600, None, seed=5)
+    net, scale = load_pretrained()
+    h_host = warm_history(net, b.lattice, b.src, b.dst, scale)
+    h_dev = warm_history_device(net, b.lattice, b.src, b.dst, scale)
+    assert h_dev.dtype == torch.float32 and h_dev.is_cuda and h_dev.numel() == h_host.size
+    hd = h_dev.cpu().numpy()
+    ulp = np.abs(hd.view(np.int32).astype(np.int64) - h_host.view(np.int32).astype(np.int64))
+    assert int(ulp.max()) <= 1, int(ulp.max())
+    assert float(np.mean(ulp == 0)) > 0.999

@@ -30,3 +30,45 @@ def test_features_targets_and_history_mapping():
     back = history_from_prediction(lat, t, 1.0)
     assert np.allclose(back, hist, rtol=1e-5, atol=1e-5)
     assert np.allclose(history_from_prediction(lat, t, 0.5), 0.5 * hist, rtol=1e-5, atol=1e-5)
+
+
+def _air_loop(sx, sy, dx, dy, nx, ny):
+    air = np.zeros((ny, nx), np.float32)
+    for a, b, c, d in zip(sx, sy, dx, dy):
+        n = int(max(abs(int(c) - int(a)), abs(int(d) - int(b)))) + 1
+        xs = np.rint(np.linspace(a, c, n)).astype(np.int64)
+        ys = np.rint(np.linspace(b, d, n)).astype(np.int64)
+        air[ys, xs] += 1.0
+    return air
+
+
+def test_segment_rasterisation_matches_linspace():
+    """The all-segments rasterisation equals one np.linspace per segment,
+    cell for cell, including zero-length segments and ties at .5 steps."""
+    from orthoroute_b200.warm import _segment_points
+
+    rng = np.random.default_rng(11)
+    nx, ny = 97, 61
+    sx, dx = rng.integers(0, nx, 500), rng.integers(0, nx, 500)
+    sy, dy = rng.integers(0, ny, 500), rng.integers(0, ny, 500)
+    sx[:20], sy[:20] = dx[:20], dy[:20]           # zero length
+    sx[20:40], dx[20:40] = 3, 4                   # one-step x, long y
+    xs, ys = _segment_points(sx, sy, dx, dy)
+    air = np.bincount(ys * nx + xs, minlength=ny * nx).astype(np.float32).reshape(ny, nx)
+    assert np.array_equal(air, _air_loop(sx, sy, dx, dy, nx, ny))
+
+
+def test_device_feature_assembly_matches_host_on_cpu():
+    """board_features_device, run with device='cpu', equals board_features
+    after the bf16 conversion, with zeros in the padding to multiples of 8."""
+    import torch
+
+    from orthoroute_b200.warm import board_features_device
+
+    b = board_footprints(83, 45, 6, 60, None, seed=9)
+    lat = b.lattice
+    f = board_features(lat, b.src, b.dst)
+    fd = board_features_device(lat, b.src, b.dst, device="cpu")
+    assert fd.shape == (6, 48, 88, 16) and fd.dtype == torch.bfloat16
+    assert torch.equal(fd[:, :45, :83], torch.from_numpy(f).to(torch.bfloat16))
+    assert float(fd[:, 45:].abs().sum()) == 0 and float(fd[:, :, 83:].abs().sum()) == 0
