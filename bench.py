@@ -49,6 +49,9 @@ METRIC = "sec to zero-overuse route, batched+warm vs plain, 1 B200; SSSP GTEPS &
 NX, NY, NZ = 1000, 1000, 12
 NSRC = 64
 PER_LAUNCH = 16
+# backplane board (route_c3), batched + warm: nets per snapshot group and
+# repair rounds (orsp_route_nets_snapshot)
+C3_GROUP, C3_REPAIR = 32, 3
 BLOCKED = 0.05
 SEED = 20261203
 # DRAM bytes (read + write) per lattice node and source of the tile search in
@@ -458,7 +461,11 @@ def route_c3(dev, with_cpu: bool):
     per net, the device loop orsp_route_nets) vs batched (one launch per round
     of pairwise disjoint boxes).  Both take the nets in the same first-fit
     disjoint-round order and widen the box of a net that offends twice
-    running by 10 cells, so their routes are identical (checked here)."""
+    running by 10 cells, so their routes are identical (checked here).
+    Batched + warm: the learned history prior and snapshot groups of
+    C3_GROUP nets (orsp_route_nets_snapshot: one launch per group on one
+    cost snapshot, then C3_REPAIR repair rounds), a schedule of its own whose
+    wirelength and vias are reported against the plain routes."""
     from orthoroute_b200.lattice import board_footprints
     from orthoroute_b200.negotiate import NegotiationConfig, PathFinder
 
@@ -483,6 +490,16 @@ def route_c3(dev, with_cpu: bool):
     t_ref1 = time.perf_counter() - t0
     sub_same = [(s_, c_) for s_, c_, _ in ref1["trace"]] == r1.overuse_trace() and all(
         np.array_equal(x, y) for x, y in zip(r1.paths, ref1["paths"])) and np.array_equal(r1.edge_usage, ref1["usage"])
+    # the same check for the snapshot-group schedule of the warm run, on the
+    # first three groups
+    sub_s = 3 * C3_GROUP
+    cfg1s = dataclasses.replace(cfg1, group_nets=C3_GROUP, group_repair=C3_REPAIR)
+    pf1.cfg = cfg1s
+    r1s = pf1.route(b.src[:sub_s], b.dst[:sub_s], mode="batched")
+    ref1s = route_plain(b.lattice, b.src[:sub_s], b.dst[:sub_s], cfg1s)
+    sub_same_snap = [(s_, c_) for s_, c_, _ in ref1s["trace"]] == r1s.overuse_trace() and all(
+        np.array_equal(x, y) for x, y in zip(r1s.paths, ref1s["paths"])) and np.array_equal(r1s.edge_usage,
+                                                                                          ref1s["usage"])
     del pf1
     rb = pf.route(b.src, b.dst, mode="batched")
     rs = pf.route(b.src, b.dst, mode="sequential")
@@ -504,14 +521,26 @@ def route_c3(dev, with_cpu: bool):
     h0 = warm_history_device(net, b.lattice, b.src, b.dst, scale)
     torch.cuda.synchronize(dev)
     t_pred = time.perf_counter() - t0
-    # the warm run keeps the plain schedule (per-net live costs from the first
-    # iteration on); the independent first pass is faster by about 1 s here but
-    # adds about a quarter more vias
-    warm_cfg = dataclasses.replace(cfg, max_iterations=int(math.ceil(1.5 * len(rs.iterations))))
+    # the warm run: snapshot groups of C3_GROUP nets with C3_REPAIR repair
+    # rounds (per-net live costs between groups); the same prediction under
+    # the exact disjoint-round schedule, and the snapshot schedule from zero
+    # history, run beside it
+    warm_cfg = dataclasses.replace(cfg, max_iterations=int(math.ceil(1.5 * len(rs.iterations))),
+                                   group_nets=C3_GROUP, group_repair=C3_REPAIR)
     pf.cfg = warm_cfg
     rw = pf.route(b.src, b.dst, mode="batched", history_init=h0)
-    pf.cfg = cfg
     warm_sec = t_pred + rw.seconds + (0.0 if rw.converged else rb.seconds)
+    pf.cfg = dataclasses.replace(warm_cfg, group_nets=0, group_repair=0)
+    rwx = pf.route(b.src, b.dst, mode="batched", history_init=h0)
+    warm_exact_sec = t_pred + rwx.seconds + (0.0 if rwx.converged else rb.seconds)
+    pf.cfg = dataclasses.replace(warm_cfg, max_iterations=cfg.max_iterations)
+    rsc = pf.route(b.src, b.dst, mode="batched")
+    snap_sec = rsc.seconds + (0.0 if rsc.converged else rb.seconds)
+    pf.cfg = cfg
+
+    def _delta(r):
+        return {"wirelength_delta_pct": round(100.0 * (r.wirelength - rb.wirelength) / max(1, rb.wirelength), 3),
+                "vias_delta_pct": round(100.0 * (r.vias - rb.vias) / max(1, rb.vias), 3)}
     # ablation: the same schedule from a non-learned prior (RUDY wire density,
     # warm.rudy_prediction) at the scale chosen for it on the same held-out
     # boards as the network's
@@ -526,6 +555,7 @@ def route_c3(dev, with_cpu: bool):
         pf.cfg = warm_cfg
         ra = pf.route(b.src, b.dst, mode="batched", history_init=hr)
         pf.cfg = cfg
+        torch.cuda.synchronize(dev)
         a_sec = t_rudy + ra.seconds + (0.0 if ra.converged else rb.seconds)
         ablation = {"prior": "RUDY (half-perimeter wire length spread over each net's bounding box), not learned",
                     "history_scale": rudy_scale, "sec_batched_prior": round(a_sec, 3),
@@ -543,6 +573,9 @@ def route_c3(dev, with_cpu: bool):
         "iteration1_subset_identical_to_oracle": bool(sub_same),
         "iteration1_subset": f"first {sub} nets, iteration 1, batched GPU vs the oracle loop "
                              f"({t_ref1:.1f} s on 1 host core)",
+        "iteration1_subset_snapshot_identical_to_oracle": bool(sub_same_snap),
+        "iteration1_subset_snapshot": f"first {sub_s} nets, iteration 1 of the warm run's snapshot schedule "
+                                      f"(zero history), batched GPU vs the oracle loop",
         "converged": bool(rb.converged),
         "iterations": len(rb.iterations),
         "searches": searches,
@@ -561,7 +594,10 @@ def route_c3(dev, with_cpu: bool):
             "iterations": len(rw.iterations),
             "searches": int(sum(s.nets_searched for s in rw.iterations)),
             "history_scale": scale,
-            "schedule": "per-net live costs, one launch per round of disjoint boxes, from the predicted history",
+            "schedule": f"snapshot groups of {C3_GROUP} nets in the disjoint-round order, each searched in one "
+                        f"launch on the costs after the group's rip-ups, then up to {C3_REPAIR} rounds "
+                        "re-searching the nets that share an edge with an earlier net of the group; per-net live "
+                        "costs between groups; from the predicted history",
             "speedup_vs_plain": round(rs.seconds / warm_sec, 2),
             "speedup_vs_batched": round(rb.seconds / warm_sec, 2),
             "wirelength": rw.wirelength,
@@ -569,6 +605,15 @@ def route_c3(dev, with_cpu: bool):
             "wirelength_delta_pct": round(100.0 * (rw.wirelength - rb.wirelength) / max(1, rb.wirelength), 3),
             "vias_delta_pct": round(100.0 * (rw.vias - rb.vias) / max(1, rb.vias), 3),
             "overuse_trace": [s.over_sum for s in rw.iterations],
+            "exact_schedule": {"sec": round(warm_exact_sec, 3), "converged": bool(rwx.converged),
+                               "iterations": len(rwx.iterations),
+                               "searches": int(sum(s.nets_searched for s in rwx.iterations)),
+                               "speedup_vs_plain": round(rs.seconds / warm_exact_sec, 2),
+                               "note": "the same prediction, one launch per round of disjoint boxes", **_delta(rwx)},
+            "snapshot_from_zero_history": {"sec": round(snap_sec, 3), "converged": bool(rsc.converged),
+                                           "iterations": len(rsc.iterations),
+                                           "searches": int(sum(s.nets_searched for s in rsc.iterations)),
+                                           "speedup_vs_plain": round(rs.seconds / snap_sec, 2), **_delta(rsc)},
         },
         "ablation_non_learned_prior": ablation,
     }

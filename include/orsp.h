@@ -296,6 +296,32 @@ ORSP_API int orsp_route_nets(orsp_graph *g, int32_t M, const int32_t *src_h, con
                     int32_t *usage_d, float *present_d, const float *cap_d, const float *hist_d,
                     float pres_fac, float hist_w, float via_mult, float base_w, int32_t jitter,
                     uintptr_t stream);
+/* The same loop with snapshot groups: the boxes of a group may overlap.  A
+ * group's nets are ripped up together, searched in one tile-sweep launch on
+ * the costs after those rip-ups (each box on distances of its own), and
+ * committed together: within a group no net sees another, as the
+ * reference's batched GPU mode routes a batch of ROIs on one cost array
+ * (CUDADijkstra.find_paths_on_rois, CD:2014).  Usage is applied for the
+ * whole group before any live cost is recomputed, so every cost is computed
+ * from the final usage and the result does not depend on thread order.  Then
+ * up to repair_rounds rounds: the nets whose new path uses an edge that a
+ * net earlier in the group also uses (in the same round) are ripped up,
+ * searched again on the live costs (which hold every path of the group) and
+ * committed again; a round that flags no net ends the group's repair early
+ * (its launches find no work).  Of two nets of a round that share an edge,
+ * the later one in the order is routed again and then sees the earlier one's
+ * path, as it would one net at a time.
+ * *searches_out (optional) receives the searches made: K plus the repair
+ * searches.  A group of one net is the plain loop.  Other arguments as
+ * orsp_route_nets; repair_rounds is 0..64.  No reference counterpart for the
+ * repair rounds. */
+ORSP_API int orsp_route_nets_snapshot(orsp_graph *g, int32_t M, const int32_t *src_h, const int32_t *dst_h,
+                    const int32_t *box_h, int32_t K, const int32_t *order_h, int32_t G,
+                    const int32_t *group_ptr_h, int32_t repair_rounds, int32_t *net_nodes_d,
+                    int32_t *net_edges_d, int32_t path_cap, int32_t *net_lens_d, float *cost_d,
+                    const float *base_d, int32_t *usage_d, float *present_d, const float *cap_d,
+                    const float *hist_d, float pres_fac, float hist_w, float via_mult, float base_w,
+                    int32_t jitter, int64_t *searches_out, uintptr_t stream);
 
 /* ---- negotiation bookkeeping ------------------------------------------- */
 /* The per-iteration loops the reference runs in Python over all committed

@@ -70,6 +70,50 @@ def route_plain(lat, src, dst, cfg, base_cost=None, history_init=None, max_nets_
             t = t + jitter[e]
         return t.astype(np.float32)
 
+    def _snapshot_group(sel, repair):
+        """Rip up every net of sel, recompute the costs of the freed edges,
+        search all of sel on those costs, commit all and recompute the costs
+        of the new edges; then up to `repair` rounds over the nets whose path
+        uses an edge that an earlier net of the round also uses."""
+        nonlocal cost
+        sel = np.asarray(sel, dtype=np.int64)
+        for rep in range(repair + 1):
+            if rep:
+                first = {}
+                for j, k in enumerate(sel):
+                    for e in net_edges[k].tolist():
+                        first.setdefault(e, j)
+                flag = np.array([any(first[e] < j for e in net_edges[k].tolist()) for j, k in enumerate(sel)],
+                                dtype=bool)
+                sel = sel[flag]
+                if sel.size == 0:
+                    return
+            freed = [net_edges[k] for k in sel if net_edges[k].size]
+            for e in freed:
+                np.subtract.at(usage, e, 1)
+                np.maximum(usage, 0, out=usage)
+            if freed:
+                fe = np.concatenate(freed)
+                cost[fe] = live_cost(fe)
+            nodes, lens = O.batch_bbox(lat.indptr, lat.indices, cost, lat.nx, lat.ny, lat.nz, src[sel], dst[sel],
+                                       boxes[sel], cap_paths)
+            new = []
+            for j, k in enumerate(sel):
+                L = int(lens[j])
+                if L >= 2:
+                    p = nodes[j, :L].copy()
+                    net_paths[k] = p
+                    net_edges[k] = O.path_to_edges(lat.indptr, lat.indices, p)
+                    np.add.at(usage, net_edges[k], 1)
+                    new.append(net_edges[k])
+                else:
+                    net_paths[k] = np.zeros(0, np.int32)
+                    net_edges[k] = np.zeros(0, np.int32)
+            if new:
+                ne = np.concatenate(new)
+                cost[ne] = live_cost(ne)
+
+    cost = None
     for it in range(1, cfg.max_iterations + 1):
         if net_policy:
             cost = live_cost(np.arange(E))
@@ -102,6 +146,12 @@ def route_plain(lat, src, dst, cfg, base_cost=None, history_init=None, max_nets_
                     else:
                         net_paths[k] = np.zeros(0, np.int32)
                         net_edges[k] = np.zeros(0, np.int32)
+                idx = np.zeros(0, np.int64)
+            G = int(getattr(cfg, "group_nets", 0))
+            if G > 0:
+                # snapshot groups of G consecutive nets, then repair rounds
+                for a in range(0, len(idx), G):
+                    _snapshot_group(idx[a:a + G], max(0, int(getattr(cfg, "group_repair", 0))))
                 idx = np.zeros(0, np.int64)
             for k in idx:  # sequential: rip up, search on live costs, commit
                 e = net_edges[k]

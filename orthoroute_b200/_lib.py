@@ -75,6 +75,9 @@ _SIGS = {
     "orsp_emit_geometry": (ctypes.c_int, [_P, _i32, _P, _P, _P, _P, _P, _P, _P, _u]),
     "orsp_route_nets": (ctypes.c_int, [_P, _i32, _P, _P, _P, _i32, _P, _i32, _P, _P, _P, _i32, _P, _P, _P, _P, _P,
                                        _P, _P, _f32, _f32, _f32, _f32, _i32, _u]),
+    "orsp_route_nets_snapshot": (ctypes.c_int, [_P, _i32, _P, _P, _P, _i32, _P, _i32, _P, _i32, _P, _P, _i32, _P,
+                                                _P, _P, _P, _P, _P, _P, _f32, _f32, _f32, _f32, _i32,
+                                                ctypes.POINTER(_i64), _u]),
     "orsp_sssp_multi": (ctypes.c_int, [_P, _P, _i32, _P, _P, _i32, _P, _P, _P, _f32, _P, _i32,
                                        ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u]),
     "orsp_roi_from_bitmap": (ctypes.c_int, [_P, _P, _P, _u]),

@@ -87,6 +87,12 @@ struct Graph {
   size_t route_tab_bytes = 0;
   cudaStream_t route_stream = nullptr;    // orsp_route_nets: stream its graphs are captured on
   cudaEvent_t route_ev[2] = {nullptr, nullptr};  // ordering with the caller's stream
+  // snapshot groups (orsp_route_nets_snapshot): the boxes' own distance
+  // slices, per-net round flags and seeds, and the lowest group rank per edge
+  uint32_t *route_pdist = nullptr;
+  size_t route_pdist_bytes = 0;
+  int32_t *route_flags = nullptr;  // [3][kMaxGroup]: two rounds of flags, seeds
+  int32_t *route_owner = nullptr;  // [E], 0x7f7f7f7f between uses
   // H/V lattice description, set when every CSR edge is a unit step along the
   // layer's routing axis or a via to an adjacent layer (see orsp_lattice.cu)
   bool lattice_ok = false;

@@ -207,6 +207,9 @@ extern "C" int orsp_graph_destroy(orsp_graph *g) {
   cudaFree(g->route_tab_d);
   if (g->route_tab_h) cudaFreeHost(g->route_tab_h);
   if (g->route_stream) cudaStreamDestroy(g->route_stream);
+  cudaFree(g->route_pdist);
+  cudaFree(g->route_flags);
+  cudaFree(g->route_owner);
   for (cudaEvent_t e : g->route_ev)
     if (e) cudaEventDestroy(e);
   cudaFree(g->box_g2r);

@@ -170,6 +170,29 @@ __global__ void gather_box_kernel(const int32_t *__restrict__ slot_eid, const fl
   }
 }
 
+// The same gather for the nodes of several boxes in one launch: blockIdx.y
+// is the box (a device LatBox table), blockIdx.x strides over its cells.
+// Cells shared by two boxes are written twice with the same value.
+__global__ void gather_boxes_kernel(const int32_t *__restrict__ slot_eid, const float *__restrict__ cost,
+                                    float4 *__restrict__ w, int64_t n, int32_t nx, int32_t ny,
+                                    const LatBox *__restrict__ boxes) {
+  const float INF_F = __int_as_float(0x7f800000);
+  const LatBox B = boxes[blockIdx.y];
+  const int32_t bw = B.x1 - B.x0 + 1, bh = B.y1 - B.y0 + 1;
+  const int64_t plane = (int64_t)bw * bh, count = plane * (B.z1 - B.z0 + 1);
+  const int64_t s = (int64_t)gridDim.x * blockDim.x;
+  BoxIndex bi;
+  bi.init(bw, bh, count);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += s) {
+    int32_t z, y, x;
+    bi.split(i, plane, z, y, x);
+    const int64_t v = ((int64_t)(B.z0 + z) * ny + (B.y0 + y)) * nx + (B.x0 + x);
+    const int32_t e0 = slot_eid[v], e1 = slot_eid[n + v], e2 = slot_eid[2 * n + v], e3 = slot_eid[3 * n + v];
+    w[v] = make_float4(e0 >= 0 ? __ldg(&cost[e0]) : INF_F, e1 >= 0 ? __ldg(&cost[e1]) : INF_F,
+                       e2 >= 0 ? __ldg(&cost[e2]) : INF_F, e3 >= 0 ? __ldg(&cost[e3]) : INF_F);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Node-set ROI searches (global_to_roi maps, as SimpleDijkstra.find_path_roi
 // takes them, UPF:1801-1887): the tile sweeps run over the ROI's bounding box,
@@ -1817,16 +1840,31 @@ int run_lattice_boxes(Graph *g, const float *cost_d, int32_t nseeds, const int32
   } else {
     g->w4_cost = nullptr;  // part of wslot is rewritten
     g->w4_gen = 0;
-    for (int32_t i = 0; i < nbox; ++i) {
-      const int32_t *b = boxes_h + 6 * (int64_t)i;
-      const int32_t bw = b[1] - b[0] + 1, bh = b[3] - b[2] + 1;
-      const int64_t count = (int64_t)bw * bh * (b[5] - b[4] + 1);
-      gather_box_kernel<<<(int)std::min<int64_t>((count + 255) / 256, 148 * 32), 256, 0, st>>>(
-          g->slot_eid, cost_d, (float4 *)g->wslot, N, g->nx, g->ny, b[0], bw, b[2], bh, b[4], count);
+    if (!g->cvia && nbox > 1 && nbox <= 65535) {
+      // one launch for all boxes, as many blocks per box as the largest needs
+      // (within a grid of about 32 blocks per SM)
+      int64_t vmax = 1;
+      for (int32_t i = 0; i < nbox; ++i) {
+        const int32_t *b = boxes_h + 6 * (int64_t)i;
+        vmax = std::max<int64_t>(vmax, (int64_t)(b[1] - b[0] + 1) * (b[3] - b[2] + 1) * (b[5] - b[4] + 1));
+      }
+      const int64_t per = std::max<int64_t>(1, std::min<int64_t>((vmax + 255) / 256, 148 * 32 / nbox));
+      gather_boxes_kernel<<<dim3((unsigned)per, (unsigned)nbox), 256, 0, st>>>(g->slot_eid, cost_d,
+                                                                              (float4 *)g->wslot, N, g->nx,
+                                                                              g->ny, lboxes_d);
       ORSP_CUDA(cudaGetLastError());
-      if (g->cvia) {
-        int rc = gather_col_box(g, cost_d, b, nullptr, nullptr, nullptr, st);
-        if (rc) return rc;
+    } else {
+      for (int32_t i = 0; i < nbox; ++i) {
+        const int32_t *b = boxes_h + 6 * (int64_t)i;
+        const int32_t bw = b[1] - b[0] + 1, bh = b[3] - b[2] + 1;
+        const int64_t count = (int64_t)bw * bh * (b[5] - b[4] + 1);
+        gather_box_kernel<<<(int)std::min<int64_t>((count + 255) / 256, 148 * 32), 256, 0, st>>>(
+            g->slot_eid, cost_d, (float4 *)g->wslot, N, g->nx, g->ny, b[0], bw, b[2], bh, b[4], count);
+        ORSP_CUDA(cudaGetLastError());
+        if (g->cvia) {
+          int rc = gather_col_box(g, cost_d, b, nullptr, nullptr, nullptr, st);
+          if (rc) return rc;
+        }
       }
     }
   }

@@ -50,6 +50,7 @@ Cost policies (``NegotiationConfig.cost_update``):
 """
 from __future__ import annotations
 
+import ctypes
 import time
 from dataclasses import dataclass, field
 from typing import List, Optional
@@ -94,6 +95,13 @@ class NegotiationConfig:
     stall_iterations: int = 2
     first_pass: str = "sequential"  # per-net costs: "sequential", or "independent" (iteration 1 on fixed costs)
     batch_plan: Optional[list] = None  # DeviceGraph.set_batch_plan for the batched searches
+    # per-net costs, batched mode: 0 = each net sees every earlier net (one
+    # launch per round of disjoint boxes); G > 0 = snapshot groups of G
+    # consecutive nets of the order, searched together on the costs after the
+    # group's rip-ups and then committed together (the nets of a group do not
+    # see one another)
+    group_nets: int = 0
+    group_repair: int = 0  # snapshot groups: rounds of re-search for nets sharing an edge with an earlier group-mate
 
 
 @dataclass
@@ -196,6 +204,8 @@ class PathFinder:
         self.base = as_device(base, torch.float32, self.device)
         self.edge_kind = np.asarray(lattice.edge_kind)
         self.roi = DeviceROIExtractor(self.dg, lattice=lattice, return_device=True)
+        self._owner = None
+        self._searches = 0
 
     # ------------------------------------------------------------------
     def _offenders(self, acc, net_edges, net_lens, nets_all):
@@ -311,6 +321,24 @@ class PathFinder:
             ptr(acc.history), float(pres_fac), float(cfg.hist_cost_weight), float(cfg.via_cost_multiplier),
             float(cfg.base_cost_weight), 1 if cfg.add_jitter else 0, _stream()), "orsp_route_nets")
 
+    def _route_nets_snapshot(self, acc, pres_fac, order, G, src, dst, boxes, net_nodes, net_edges, net_lens):
+        """orsp_route_nets_snapshot over `order` (host int32) in groups of G
+        consecutive nets, with cfg.group_repair repair rounds; returns the
+        searches made."""
+        cfg = self.cfg
+        order = np.ascontiguousarray(order, dtype=np.int32)
+        boxes_c = np.ascontiguousarray(boxes, dtype=np.int32)
+        gp = np.ascontiguousarray(np.append(np.arange(0, order.size, G), order.size), dtype=np.int32)
+        n = ctypes.c_int64(0)
+        check(_lib.load().orsp_route_nets_snapshot(
+            self.dg.handle, int(len(src)), ptr(src), ptr(dst), ptr(boxes_c), int(order.size), ptr(order),
+            int(gp.size - 1), ptr(gp), int(max(0, cfg.group_repair)), ptr(net_nodes), ptr(net_edges),
+            int(net_nodes.shape[1]), ptr(net_lens), ptr(acc.total_cost), ptr(self.base), ptr(acc.usage),
+            ptr(acc.present), ptr(acc.capacity), ptr(acc.history), float(pres_fac), float(cfg.hist_cost_weight),
+            float(cfg.via_cost_multiplier), float(cfg.base_cost_weight), 1 if cfg.add_jitter else 0,
+            ctypes.byref(n), _stream()), "orsp_route_nets_snapshot")
+        return int(n.value)
+
     def _route_net_sequential(self, acc, pres_fac, idx, src, dst, boxes, net_nodes, net_edges, net_lens, delta):
         if self.cfg.native_loop and self.dg.route_loop_ok:
             self._route_nets_device(acc, pres_fac, idx.cpu().numpy(), None, src, dst, boxes, net_nodes, net_edges,
@@ -358,8 +386,14 @@ class PathFinder:
 
     def _route_net_batched(self, acc, pres_fac, idx, src_d, dst_d, boxes_d, boxes, order_levels, net_nodes,
                            net_edges, net_lens, delta, src=None, dst=None):
+        G = int(self.cfg.group_nets)
         if self.cfg.native_loop and self.dg.route_loop_ok and src is not None:
             idx_h = idx.cpu().numpy()
+            if G > 0:
+                n = self._route_nets_snapshot(acc, pres_fac, idx_h, G, src, dst, boxes, net_nodes, net_edges,
+                                              net_lens)
+                self._searches += n - int(idx_h.size)
+                return
             order, groups = level_groups(idx_h, level_schedule(boxes[idx_h]))
             self._route_nets_device(acc, pres_fac, order, groups, src, dst, boxes, net_nodes, net_edges, net_lens)
             return
@@ -368,26 +402,58 @@ class PathFinder:
         st = _stream()
         cost = acc.total_cost
         idx_h = idx.cpu().numpy()
-        lv = level_schedule(boxes[idx_h])
+        if G > 0:  # snapshot groups: consecutive chunks of the order
+            lv = (np.arange(len(idx_h)) // G).astype(np.int32)
+        else:
+            lv = level_schedule(boxes[idx_h])
         for L in range(int(lv.max()) + 1 if len(lv) else 0):
             sel = torch.from_numpy(idx_h[lv == L]).to(self.device)
-            K = int(sel.numel())
-            old_e = net_edges[sel].contiguous()
-            old_l = net_lens[sel].contiguous()
-            check(lib.orsp_commit_batch(K, ptr(old_e), ptr(old_l), cap, ptr(acc.usage), ptr(acc.present), -1, st),
-                  "orsp_commit_batch")
-            self._live_paths(acc, pres_fac, old_e, old_l)
-            nodes, edges, lens = self.dg.batch_bbox(cost, src_d[sel].contiguous(), dst_d[sel].contiguous(),
-                                                    boxes_d[sel].contiguous(), delta=delta, path_cap=cap)
-            if K and int(lens.min().item()) < 0:
-                bad = lens[lens < 0]
-                raise _lib.OrspError(int(bad[0]), "orsp_sssp_batch_bbox", "per-search failure status")
-            net_nodes[sel] = nodes
-            net_edges[sel] = edges
-            net_lens[sel] = lens
-            check(lib.orsp_commit_batch(K, ptr(edges), ptr(lens), cap, ptr(acc.usage), ptr(acc.present), 1, st),
-                  "orsp_commit_batch")
-            self._live_paths(acc, pres_fac, edges, lens)
+            for rep in range(1 + (max(0, int(self.cfg.group_repair)) if G > 0 else 0)):
+                if rep:
+                    # repair: the nets whose path shares an edge with an
+                    # earlier net of the same snapshot, searched again on the
+                    # live costs (which now hold every path of the group)
+                    sel = sel[self._group_conflicts(sel, net_edges, net_lens)]
+                    if sel.numel() == 0:
+                        break
+                K = int(sel.numel())
+                old_e = net_edges[sel].contiguous()
+                old_l = net_lens[sel].contiguous()
+                check(lib.orsp_commit_batch(K, ptr(old_e), ptr(old_l), cap, ptr(acc.usage), ptr(acc.present), -1,
+                                            st), "orsp_commit_batch")
+                self._live_paths(acc, pres_fac, old_e, old_l)
+                nodes, edges, lens = self.dg.batch_bbox(cost, src_d[sel].contiguous(), dst_d[sel].contiguous(),
+                                                        boxes_d[sel].contiguous(), delta=delta, path_cap=cap)
+                if K and int(lens.min().item()) < 0:
+                    bad = lens[lens < 0]
+                    raise _lib.OrspError(int(bad[0]), "orsp_sssp_batch_bbox", "per-search failure status")
+                net_nodes[sel] = nodes
+                net_edges[sel] = edges
+                net_lens[sel] = lens
+                check(lib.orsp_commit_batch(K, ptr(edges), ptr(lens), cap, ptr(acc.usage), ptr(acc.present), 1, st),
+                      "orsp_commit_batch")
+                self._live_paths(acc, pres_fac, edges, lens)
+                if rep:
+                    self._searches += K
+
+    def _group_conflicts(self, sel, net_edges, net_lens):
+        """Mask over sel: the nets whose path uses an edge that an earlier net
+        of sel (in sel's order) also uses."""
+        n = int(sel.numel())
+        cap = net_edges.shape[1]
+        lens = net_lens[sel].long()
+        valid = torch.arange(cap, device=self.device)[None, :] < (lens - 1).clamp_min(0)[:, None]
+        e = net_edges[sel].long()[valid]
+        r = torch.arange(n, device=self.device)[:, None].expand(n, cap)[valid]
+        if self._owner is None or self._owner.numel() != self.E:
+            self._owner = torch.full((self.E,), 1 << 30, dtype=torch.int64, device=self.device)
+        own = self._owner
+        own.scatter_reduce_(0, e, r, reduce="amin")
+        hit = own[e] < r
+        own[e] = 1 << 30
+        conf = torch.zeros(n, dtype=torch.bool, device=self.device)
+        conf[r[hit]] = True
+        return conf
 
     # ------------------------------------------------------------------
     def route(self, src, dst, mode: str = "batched", history_init=None, callback=None) -> RouteResult:
@@ -437,6 +503,7 @@ class PathFinder:
             raise ValueError("first_pass must be 'sequential' or 'independent'")
         for it in range(1, cfg.max_iterations + 1):
             t_it = time.perf_counter()
+            searches0 = self._searches
             acc.refresh_from_canonical()
             if net_policy:
                 self._live(acc, pres_fac)
@@ -490,7 +557,8 @@ class PathFinder:
             acc.refresh_from_canonical()
             over_sum, over_cnt = acc.compute_overuse()
             failed = int((net_lens < 2).sum().item())
-            stats.append(IterationStats(it, pres_fac, M - failed, failed, over_sum, over_cnt, int(idx.numel()),
+            stats.append(IterationStats(it, pres_fac, M - failed, failed, over_sum, over_cnt,
+                                        int(idx.numel()) + self._searches - searches0,
                                         time.perf_counter() - t_it))
             if callback is not None:
                 callback(stats[-1])

@@ -160,3 +160,70 @@ def test_negotiation_on_lattice_deeper_than_a_tile():
     assert r.overuse_trace() == [(s, c) for s, c, _ in ref["trace"]]
     for k in range(len(b.src)):
         assert np.array_equal(r.paths[k], ref["paths"][k]), f"net {k}"
+
+
+@pytest.mark.parametrize("G,R", [(8, 0), (8, 2), (32, 3)])
+def test_snapshot_groups_match_oracle(G, R):
+    """orsp_route_nets_snapshot (groups of G overlapping boxes searched on one
+    cost snapshot, then R repair rounds, all enqueued on the device) equals
+    the host loop of the same schedule (one batch launch per round) and the
+    oracle: overuse per iteration, every path, the final usage and live
+    costs, and the search count."""
+    import dataclasses
+
+    b = board_uniform_pins(56, 44, 6, 90, seed=12)
+    cfg = NegotiationConfig(max_iterations=6, reroute="offenders", roi_margin=4, cost_update="net",
+                            full_graph_retry=False, net_order="disjoint", group_nets=G, group_repair=R)
+    ref = route_plain(b.lattice, b.src, b.dst, cfg)
+    pf = PathFinder(b.lattice, config=cfg)
+    assert pf.dg.route_loop_ok
+    rd = pf.route(b.src, b.dst, mode="batched")
+    cost_dev = pf.acc.total_cost.cpu().numpy()
+    pf_h = PathFinder(b.lattice, config=dataclasses.replace(cfg, native_loop=False))
+    rh = pf_h.route(b.src, b.dst, mode="batched")
+    cost_host = pf_h.acc.total_cost.cpu().numpy()
+    tr_ref = [(s, c) for s, c, _ in ref["trace"]]
+    assert rd.overuse_trace() == tr_ref
+    assert rh.overuse_trace() == tr_ref
+    assert [s.nets_searched for s in rd.iterations] == [s.nets_searched for s in rh.iterations]
+    for k in range(len(b.src)):
+        assert np.array_equal(rd.paths[k], ref["paths"][k]), f"net {k} (device loop)"
+        assert np.array_equal(rh.paths[k], ref["paths"][k]), f"net {k} (host loop)"
+    assert np.array_equal(rd.edge_usage, ref["usage"])
+    assert np.array_equal(cost_dev.view(np.uint32), cost_host.view(np.uint32))
+
+
+def test_snapshot_group_of_one_is_the_plain_loop():
+    """Snapshot groups of one net (with repair rounds, which then never flag
+    a net) give the plain per-net loop's routes bit for bit."""
+    import dataclasses
+
+    b = board_uniform_pins(48, 40, 6, 70, seed=21)
+    cfg = NegotiationConfig(max_iterations=5, reroute="offenders", roi_margin=4, cost_update="net",
+                            full_graph_retry=False, net_order="disjoint")
+    r0 = PathFinder(b.lattice, config=cfg).route(b.src, b.dst, mode="batched")
+    r1 = PathFinder(b.lattice, config=dataclasses.replace(cfg, group_nets=1, group_repair=2)).route(
+        b.src, b.dst, mode="batched")
+    assert r0.overuse_trace() == r1.overuse_trace()
+    assert [s.nets_searched for s in r0.iterations] == [s.nets_searched for s in r1.iterations]
+    assert all(np.array_equal(x, y) for x, y in zip(r0.paths, r1.paths))
+    assert np.array_equal(r0.edge_usage, r1.edge_usage)
+
+
+def test_snapshot_groups_deep_boxes_full_vias():
+    """Snapshot groups on an 18-layer board (the deep-tile kernel on the
+    boxes' own distance slices) match the host loop of the schedule."""
+    import dataclasses
+
+    from orthoroute_b200.lattice import board_footprints
+
+    b = board_footprints(120, 100, 18, 160, None, seed=4)
+    cfg = NegotiationConfig(max_iterations=4, reroute="offenders", roi_margin=6, cost_update="net",
+                            full_graph_retry=False, net_order="disjoint", group_nets=16, group_repair=2)
+    pf = PathFinder(b.lattice, config=cfg)
+    rd = pf.route(b.src, b.dst, mode="batched")
+    rh = PathFinder(b.lattice, config=dataclasses.replace(cfg, native_loop=False)).route(b.src, b.dst,
+                                                                                         mode="batched")
+    assert rd.overuse_trace() == rh.overuse_trace()
+    assert all(np.array_equal(x, y) for x, y in zip(rd.paths, rh.paths))
+    assert np.array_equal(rd.edge_usage, rh.edge_usage)
