@@ -259,18 +259,19 @@ def merge_escapes(escape_tracks: List[dict], tracks: List[dict], vias: List[dict
     return t, v
 
 
-def headless_config(max_iterations: int = 200):
+def headless_config(max_iterations: int = 200, groups: int = 0, repair: int = 3):
     """The negotiation schedule of headless runs: per-net live costs, only
     offending nets rerouted, bbox + 10-cell ROIs with a full-lattice retry,
-    first-fit rounds of disjoint boxes."""
+    first-fit rounds of disjoint boxes; with groups > 0, batched runs take
+    snapshot groups of that many nets with `repair` repair rounds."""
     from .negotiate import NegotiationConfig
     return NegotiationConfig(max_iterations=max_iterations, cost_update="net", reroute="offenders", roi_margin=10,
-                             full_graph_retry=True, net_order="disjoint")
+                             full_graph_retry=True, net_order="disjoint", group_nets=groups, group_repair=repair)
 
 
 def route_board(board_data: dict, pitch: float = DEFAULT_PITCH, max_iterations: int = 200, mode: str = "batched",
                 warm: bool = False, config=None, device=None, log=None, portals: bool = True,
-                vias: str = "full"):
+                vias: str = "full", groups: int = 0):
     """Routes a board_data dict on the GPU (mode 'batched' or 'sequential'),
     through pad-escape portals unless portals is False, on a lattice with
     adjacent or full (the reference's) vias.  Returns (problem, RouteResult,
@@ -279,7 +280,7 @@ def route_board(board_data: dict, pitch: float = DEFAULT_PITCH, max_iterations: 
     from .negotiate import PathFinder
 
     prob = build_problem(board_data, pitch, portals=portals, vias=vias)
-    cfg = config or headless_config(max_iterations)
+    cfg = config or headless_config(max_iterations, groups=groups)
     if vias == "full" and cfg.batch_plan is None:
         # the batched box searches on the tile sweeps (column vias)
         cfg.batch_plan = [{"max_nodes": 1 << 40, "impl": 1, "tile_w": 16}]
@@ -311,7 +312,7 @@ def route_board(board_data: dict, pitch: float = DEFAULT_PITCH, max_iterations: 
 
 def run_headless(orp_file: str, output_file: Optional[str] = None, max_iterations: int = 200,
                  mode: str = "batched", warm: bool = False, pitch: float = DEFAULT_PITCH, log=print,
-                 portals: bool = True, vias: str = "full") -> dict:
+                 portals: bool = True, vias: str = "full", groups: int = 0) -> dict:
     """ORP in, ORS out; returns a summary of the run."""
     from .ors import GeometryPayload, write_ors
 
@@ -320,7 +321,7 @@ def run_headless(orp_file: str, output_file: Optional[str] = None, max_iteration
     out = Path(output_file) if output_file else Path(orp_file).with_suffix(".ORS")
     via_style = vias
     prob, res, tracks, vias, metrics = route_board(board_data, pitch, max_iterations, mode, warm, log=log,
-                                                   portals=portals, vias=via_style)
+                                                   portals=portals, vias=via_style, groups=groups)
     total = time.perf_counter() - t0
     routed = sum(1 for p in res.paths if p is not None and len(p) >= 2) + len(prob.trivial)
     meta = {"orthoroute_version": "0.1.0", "board_name": board_data.get("filename", "board"), "total_time": total,
@@ -333,6 +334,7 @@ def run_headless(orp_file: str, output_file: Optional[str] = None, max_iteration
                "converged": bool(res.converged), "iterations": len(metrics), "tracks": len(tracks),
                "vias": len(vias), "seconds_total": round(total, 3), "seconds_route": round(res.seconds, 3),
                "lattice": [prob.lattice.nx, prob.lattice.ny, prob.lattice.nz], "lattice_vias": via_style,
+               "snapshot_groups": groups, "searches": int(sum(s_.nets_searched for s_ in res.iterations)),
                "portals": len(prob.portals),
                "escape_tracks": len(prob.escape_tracks), "portal_collisions": portal_collisions(prob),
                "forced_overuse": forced_overuse(prob)}
@@ -356,9 +358,12 @@ def main(argv=None):
     ap.add_argument("--vias", choices=["adjacent", "full"], default="full",
                     help="the reference's via set (F.Cu to every routing layer, every pair of routing layers; the "
                          "default), or vias between neighbouring layers only")
+    ap.add_argument("--groups", type=int, default=0,
+                    help="batched mode: snapshot groups of this many nets (one launch per group, then repair "
+                         "rounds for nets sharing an edge); 0 keeps one launch per round of disjoint boxes")
     a = ap.parse_args(argv)
     s = run_headless(a.orp, a.output, a.max_iterations, "batched" if a.mode == "batched" else "sequential", a.warm,
-                     a.pitch, portals=not a.no_portals, vias=a.vias)
+                     a.pitch, portals=not a.no_portals, vias=a.vias, groups=a.groups)
     return 0 if s["converged"] else 1
 
 

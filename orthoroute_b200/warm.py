@@ -81,9 +81,36 @@ def _segment_points(a, b, c, d):
     return coord(a, c), coord(b, d)
 
 
-def board_maps(lat: Lattice, src: np.ndarray, dst: np.ndarray, version: int = FEATURES) -> dict:
+def _air_counts_device(sx, sy, dx, dy, nx: int, ny: int, device) -> np.ndarray:
+    """The airwire crossing counts of _segment_points, float32 [ny][nx], with
+    the rasterisation on `device`: the same float64 operations (one division,
+    one multiply, one add, each rounded once), linspace's exact end point and
+    round-half-even, so the same cells as on the host; counts are integers."""
+    dev = torch.device(device)
+    a, b, c, d = (torch.from_numpy(np.ascontiguousarray(v, dtype=np.int64)).to(dev) for v in (sx, sy, dx, dy))
+    n = torch.maximum((c - a).abs(), (d - b).abs()) + 1
+    seg = torch.repeat_interleave(torch.arange(n.numel(), device=dev), n)
+    start = torch.cumsum(n, 0) - n
+    k = torch.arange(seg.numel(), device=dev) - start[seg]
+    div = torch.clamp(n - 1, min=1).double()
+    ns = n[seg]
+    last = (k == ns - 1) & (ns > 1)
+
+    def coord(p, q):
+        step = (q - p).double() / div
+        y = k.double() * step[seg]
+        y = y + p[seg].double()
+        y = torch.where(last, q[seg].double(), y)
+        return torch.round(y).long()
+
+    cell = coord(b, d) * nx + coord(a, c)
+    return torch.bincount(cell, minlength=ny * nx).to(torch.float32).reshape(ny, nx).cpu().numpy()
+
+
+def board_maps(lat: Lattice, src: np.ndarray, dst: np.ndarray, version: int = FEATURES, device=None) -> dict:
     """The board-dependent 2-D maps of board_features (host, float32 [ny][nx]),
-    the pin layer, and the layer flags."""
+    the pin layer, and the layer flags; with `device`, the airwire
+    rasterisation runs there (the same cells)."""
     nx, ny, nz = lat.nx, lat.ny, lat.nz
     sx, sy, sz = (np.asarray(v) for v in lat.coords(np.asarray(src)))
     dx, dy, dz = (np.asarray(v) for v in lat.coords(np.asarray(dst)))
@@ -92,8 +119,11 @@ def board_maps(lat: Lattice, src: np.ndarray, dst: np.ndarray, version: int = FE
     np.add.at(pins, (dy, dx), 1.0)
     # airwire crossing density: each pin-to-pin segment rasterised at unit steps
     # (integer counts, exact in float32)
-    xs, ys = _segment_points(sx, sy, dx, dy)
-    air = np.bincount(ys * nx + xs, minlength=ny * nx).astype(np.float32).reshape(ny, nx)
+    if device is not None:
+        air = _air_counts_device(sx, sy, dx, dy, nx, ny, device)
+    else:
+        xs, ys = _segment_points(sx, sy, dx, dy)
+        air = np.bincount(ys * nx + xs, minlength=ny * nx).astype(np.float32).reshape(ny, nx)
     cov = np.zeros((ny + 1, nx + 1), np.float32)
     x0, x1 = np.minimum(sx, dx), np.maximum(sx, dx) + 1
     y0, y1 = np.minimum(sy, dy), np.maximum(sy, dy) + 1
@@ -138,7 +168,7 @@ def board_features_device(lat: Lattice, src, dst, version: int = FEATURES, devic
     host array's after the same bf16 conversion."""
     dev = torch.device(device) if device is not None else torch.device("cuda")
     nx, ny, nz = lat.nx, lat.ny, lat.nz
-    m = board_maps(lat, src, dst, version)
+    m = board_maps(lat, src, dst, version, device=dev)
     Hp, Wp = (ny + 7) // 8 * 8, (nx + 7) // 8 * 8
     f = torch.zeros((nz, Hp, Wp, F_IN), dtype=torch.float32, device=dev)
     up = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731

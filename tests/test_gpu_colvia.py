@@ -214,3 +214,25 @@ def test_column_via_negotiation_matches_oracle(order):
         assert np.array_equal(rb.paths[k], ref["paths"][k]), k
         assert np.array_equal(rs.paths[k], ref["paths"][k]), k
     assert np.array_equal(rb.edge_usage, ref["usage"]) and np.array_equal(rs.edge_usage, ref["usage"])
+
+
+def test_column_via_snapshot_groups_match_oracle():
+    """Snapshot groups with repair rounds (orsp_route_nets_snapshot) on a
+    column-via lattice: the device loop equals the oracle loop of the same
+    schedule per iteration, per net and in the final edge usage."""
+    from oracle.negotiate import route_plain
+    from orthoroute_b200.lattice import board_uniform_pins
+    from orthoroute_b200.negotiate import NegotiationConfig, PathFinder
+
+    b = board_uniform_pins(40, 34, 6, 60, seed=8)
+    lat = _ref_lattice(40, 34, 6)
+    cfg = NegotiationConfig(max_iterations=5, reroute="offenders", roi_margin=3, cost_update="net",
+                            full_graph_retry=False, net_order="disjoint", group_nets=12, group_repair=2)
+    ref = route_plain(lat, b.src, b.dst, cfg)
+    pf = PathFinder(lat, config=cfg)
+    assert pf.dg.lattice_kind == 2 and pf.dg.route_loop_ok
+    rb = pf.route(b.src, b.dst, mode="batched")
+    assert rb.overuse_trace() == [(s, c) for s, c, _ in ref["trace"]]
+    for k in range(len(b.src)):
+        assert np.array_equal(rb.paths[k], ref["paths"][k]), k
+    assert np.array_equal(rb.edge_usage, ref["usage"])

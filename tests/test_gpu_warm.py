@@ -128,7 +128,15 @@ def test_warm_history_device_matches_host():
     from orthoroute_b200.lattice import board_footprints
     from orthoroute_b200.warm import load_pretrained, warm_history, warm_history_device
 
+    from orthoroute_b200.warm import _air_counts_device, _segment_points
+
     b = board_footprints(203, 117, 18, 600, None, seed=5)
+    lat = b.lattice
+    sx, sy, _ = lat.coords(np.asarray(b.src))
+    dx, dy, _ = lat.coords(np.asarray(b.dst))
+    xs, ys = _segment_points(sx, sy, dx, dy)
+    air = np.bincount(ys * lat.nx + xs, minlength=lat.ny * lat.nx).astype(np.float32).reshape(lat.ny, lat.nx)
+    assert np.array_equal(_air_counts_device(sx, sy, dx, dy, lat.nx, lat.ny, "cuda"), air)
     net, scale = load_pretrained()
     h_host = warm_history(net, b.lattice, b.src, b.dst, scale)
     h_dev = warm_history_device(net, b.lattice, b.src, b.dst, scale)

@@ -56,6 +56,10 @@ def test_segment_rasterisation_matches_linspace():
     xs, ys = _segment_points(sx, sy, dx, dy)
     air = np.bincount(ys * nx + xs, minlength=ny * nx).astype(np.float32).reshape(ny, nx)
     assert np.array_equal(air, _air_loop(sx, sy, dx, dy, nx, ny))
+    # the torch form the device path runs, here on the CPU
+    from orthoroute_b200.warm import _air_counts_device
+
+    assert np.array_equal(_air_counts_device(sx, sy, dx, dy, nx, ny, "cpu"), air)
 
 
 def test_device_feature_assembly_matches_host_on_cpu():
