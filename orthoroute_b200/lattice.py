@@ -89,21 +89,17 @@ def build_lattice(
     via_cost: float = 3.0,
     duplicate_vias: bool = False,
 ) -> Lattice:
-    """Builds the CSR lattice described in the module docstring."""
+    """Builds the CSR lattice described in the module docstring.  Each node's
+    out-edges are in slot order: -x, +x, -y, +y (those its layer has), then
+    its vias by target layer (each twice with duplicate_vias).  The rows are
+    written layer by layer: the via targets of a layer are the same for all
+    its nodes, so a layer's via block is one scatter."""
     if planar not in ("all", "inner") or vias not in ("adjacent", "full"):
         raise ValueError("planar must be 'all'|'inner', vias 'adjacent'|'full'")
     N = nx * ny * nz
     if N >= 2**31:
         raise ValueError("lattice too large for int32 node ids")
     dirs = layer_directions(nz)
-    z, y, x = np.meshgrid(
-        np.arange(nz, dtype=np.int64), np.arange(ny, dtype=np.int64), np.arange(nx, dtype=np.int64), indexing="ij"
-    )
-    z = z.reshape(-1)
-    y = y.reshape(-1)
-    x = x.reshape(-1)
-    node = np.arange(N, dtype=np.int64)
-
     if planar == "all" or nz <= 2:
         planar_layer = np.ones(nz, dtype=bool)
     else:
@@ -111,29 +107,13 @@ def build_lattice(
         planar_layer[1 : nz - 1] = True
     has_h = np.array([d in ("h", "hv") for d in dirs]) & planar_layer
     has_v = np.array([d in ("v", "hv") for d in dirs]) & planar_layer
-
-    slots_tgt = []
-    slots_cost = []
-    # planar slots: -x, +x, -y, +y (only the ones the layer allows exist)
-    hz = has_h[z]
-    vz = has_v[z]
-    slots_tgt.append(np.where(hz & (x > 0), node - 1, -1))
-    slots_cost.append(np.float32(pitch))
-    slots_tgt.append(np.where(hz & (x < nx - 1), node + 1, -1))
-    slots_cost.append(np.float32(pitch))
-    slots_tgt.append(np.where(vz & (y > 0), node - nx, -1))
-    slots_cost.append(np.float32(pitch))
-    slots_tgt.append(np.where(vz & (y < ny - 1), node + nx, -1))
-    slots_cost.append(np.float32(pitch))
-
     plane = nx * ny
-    if vias == "adjacent":
-        for dz in (-1, 1):
-            tz = z + dz
-            ok = (tz >= 0) & (tz < nz)
-            slots_tgt.append(np.where(ok, node + dz * plane, -1))
-            slots_cost.append(np.float32(via_cost))
-    else:
+    r = np.arange(plane, dtype=np.int64)
+    xr = r % nx
+    yr = r // nx
+
+    # via targets of a node on layer zz, in slot order, and their costs
+    if vias == "full":
         # Lattice3D.get_legal_via_pairs (UPF:1136-1172): routing layers 1..nz-2
         # pairwise, plus F.Cu (0) <-> every routing layer; 2 layers: (0,1).
         if nz == 2:
@@ -143,30 +123,58 @@ def build_lattice(
             legal = {(a, b) for a in routing for b in routing if a != b}
             legal |= {(0, b) for b in routing} | {(b, 0) for b in routing}
         reps = 2 if duplicate_vias else 1
-        for tz in range(nz):
-            ok = np.array([(int(zz), tz) in legal for zz in range(nz)])[z]
-            span = np.abs(tz - z)
-            c = (via_cost * (1.0 + 0.15 * (span - 1))).astype(np.float32)
-            for _ in range(reps):
-                slots_tgt.append(np.where(ok, node + (tz - z) * plane, -1))
-                slots_cost.append(c)
+    via_t, via_c = [], []
+    for zz in range(nz):
+        if vias == "adjacent":
+            t = [zz + dz for dz in (-1, 1) if 0 <= zz + dz < nz]
+            c = [np.float32(via_cost)] * len(t)
+        else:
+            t = [tz for tz in range(nz) if (zz, tz) in legal for _ in range(reps)]
+            # cost grows by 15 % per layer spanned beyond the first
+            c = [np.float32(via_cost * (1.0 + 0.15 * (abs(tz - zz) - 1))) for tz in t]
+        via_t.append(np.asarray(t, dtype=np.int64))
+        via_c.append(np.asarray(c, dtype=np.float32))
 
-    tgt = np.stack(slots_tgt, axis=1)
-    S = tgt.shape[1]
-    cost = np.empty((N, S), dtype=np.float32)
-    for s, c in enumerate(slots_cost):
-        cost[:, s] = c
-    mask = tgt >= 0
-    deg = mask.sum(axis=1)
+    def planar_slots(zz):
+        out = []
+        if has_h[zz]:
+            out += [(xr > 0, -1), (xr < nx - 1, 1)]
+        if has_v[zz]:
+            out += [(yr > 0, -nx), (yr < ny - 1, nx)]
+        return out
+
+    deg = np.empty(N, dtype=np.int64)
+    for zz in range(nz):
+        d = np.full(plane, via_t[zz].size, dtype=np.int64)
+        for m, _ in planar_slots(zz):
+            d += m
+        deg[zz * plane:(zz + 1) * plane] = d
     indptr = np.zeros(N + 1, dtype=np.int64)
     np.cumsum(deg, out=indptr[1:])
-    if indptr[-1] >= 2**31:
+    E = int(indptr[-1])
+    if E >= 2**31:
         raise ValueError("too many edges for int32 CSR")
-    indices = tgt[mask].astype(np.int32)
-    base_cost = cost[mask].astype(np.float32)
-    src = np.repeat(node, deg)
-    edge_layer = (src // plane).astype(np.uint8)
-    edge_kind = ((indices.astype(np.int64) // plane) != (src // plane)).astype(np.uint8)
+    indices = np.empty(E, dtype=np.int32)
+    base_cost = np.empty(E, dtype=np.float32)
+    edge_kind = np.zeros(E, dtype=np.uint8)
+    edge_layer = np.empty(E, dtype=np.uint8)
+    pitch32 = np.float32(pitch)
+    for zz in range(nz):
+        a = zz * plane
+        start = indptr[a:a + plane]
+        k = np.zeros(plane, dtype=np.int64)
+        for m, step in planar_slots(zz):
+            pos = start[m] + k[m]
+            indices[pos] = a + r[m] + step
+            base_cost[pos] = pitch32
+            k += m
+        nv = via_t[zz].size
+        if nv:
+            pos = (start + k)[:, None] + np.arange(nv, dtype=np.int64)[None, :]
+            indices[pos] = via_t[zz][None, :] * plane + r[:, None]
+            base_cost[pos] = via_c[zz][None, :]
+            edge_kind[pos] = 1
+        edge_layer[indptr[a]:indptr[a + plane]] = zz
     return Lattice(
         nx=nx,
         ny=ny,
