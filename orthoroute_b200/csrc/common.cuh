@@ -178,6 +178,8 @@ struct LatOptions {
   int spec = 0;                // 1: the warp-specialised schedule; ORSP_LAT_SPEC overrides
   int64_t tma_slices = 0;      // > 0: every box is the whole lattice, box j's distances in slice j of N
                                // cells from `dist` (LatBox.pad = j); allows the TMA staging
+  const int32_t *active = nullptr;  // private_dist, device flags: a box with active[j] == 0 has no seed, and
+                                    // its weights and distances are neither gathered nor reset
 };
 // One box (nullptr: the whole lattice).  Stages its tile table through the
 // graph's pinned buffer, so the calling entry point must synchronise before

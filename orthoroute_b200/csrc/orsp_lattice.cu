@@ -84,6 +84,7 @@ struct LatParams {
   unsigned max_rounds;
   unsigned long long wait_ns, budget_ns;
   int selfcont;
+  int prefetch;            // warp-specialised schedule: L2 prefetch of the next tile's rows
   const int32_t *roi_map;  // node-set ROI searches: seeds outside it are ignored
   const float *wcol;       // column vias: gathered via weights [N][nzp] (Graph::wcol)
   int32_t nzp;             // nz rounded up to 4
@@ -93,6 +94,18 @@ struct LatParams {
 __global__ void fill_kernel(uint32_t *p, int64_t n, uint32_t v) {
   const int64_t s = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += s) p[i] = v;
+}
+
+// The fill of the boxes' own distance slices [dbase, dbase + volume), box
+// blockIdx.y, skipping boxes with active[j] == 0.
+__global__ void fill_slices_kernel(uint32_t *p, const LatBox *__restrict__ boxes, const int32_t *__restrict__ active,
+                                   uint32_t v) {
+  if (active && !active[blockIdx.y]) return;
+  const LatBox B = boxes[blockIdx.y];
+  const int64_t count = (int64_t)(B.x1 - B.x0 + 1) * (B.y1 - B.y0 + 1) * (B.z1 - B.z0 + 1);
+  uint32_t *q = p + B.dbase;
+  const int64_t s = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += s) q[i] = v;
 }
 
 // The same fill over the nodes of a box (x fastest).
@@ -171,11 +184,13 @@ __global__ void gather_box_kernel(const int32_t *__restrict__ slot_eid, const fl
 }
 
 // The same gather for the nodes of several boxes in one launch: blockIdx.y
-// is the box (a device LatBox table), blockIdx.x strides over its cells.
-// Cells shared by two boxes are written twice with the same value.
+// is the box (a device LatBox table), blockIdx.x strides over its cells;
+// boxes with active[j] == 0 are skipped (active NULL: none).  Cells shared by
+// two boxes are written twice with the same value.
 __global__ void gather_boxes_kernel(const int32_t *__restrict__ slot_eid, const float *__restrict__ cost,
                                     float4 *__restrict__ w, int64_t n, int32_t nx, int32_t ny,
-                                    const LatBox *__restrict__ boxes) {
+                                    const LatBox *__restrict__ boxes, const int32_t *__restrict__ active) {
+  if (active && !active[blockIdx.y]) return;
   const float INF_F = __int_as_float(0x7f800000);
   const LatBox B = boxes[blockIdx.y];
   const int32_t bw = B.x1 - B.x0 + 1, bh = B.y1 - B.y0 + 1;
@@ -1290,6 +1305,37 @@ __device__ void finish_visit(const LatParams &p, int t, const int *act) {
 // after the next handoff - so it never waits for work that only its own
 // finished tile would create.  The flags of visit k stay intact until visit
 // k + 2 starts, and the scheduler reads them before handoff k + 2.
+// Prefetch into L2, by one warp, of the rows a visit of tile t loads: per
+// layer of the box, each tile row's in-edge weights (16 B per node) and
+// distances, with the x-halo cells and the distance rows just above and
+// below the tile where the box has them (the y-halo).  Every address
+// prefetched lies inside the weight array or the box's distances.
+template <int TX, int TY, bool PRIV>
+__device__ __forceinline__ void prefetch_tile_l2(const LatParams &p, int t, int lane) {
+  const LatBox B = load_box(p, box_of_tile(p, t));
+  const int lt = t - B.tile0;
+  const int tx = lt % B.ntx, ty = lt / B.ntx;
+  const int32_t X0 = B.x0 + tx * TX, Y0 = B.y0 + ty * TY;
+  const int tw = min(TX, B.x1 - X0 + 1), th = min(TY, B.y1 - Y0 + 1);
+  const int nzb = B.z1 - B.z0 + 1;
+  const int64_t nxy = (int64_t)p.nx * p.ny;
+  const int ya = Y0 > B.y0 ? -1 : 0, yb = Y0 + th - 1 < B.y1 ? th : th - 1;
+  const int nrow = yb - ya + 1;
+  for (int i = lane; i < nzb * nrow; i += 32) {
+    const int zl = i / nrow, yy = ya + i % nrow;
+    const int32_t z = B.z0 + zl, y = Y0 + yy;
+    const uint32_t *d = &p.dist[dist_index<PRIV>(p, B, X0, y, z)];
+    // the row, with its x-halo cells where the box has them
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(X0 > B.x0 ? d - 1 : d) : "memory");
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(X0 + tw - 1 < B.x1 ? d + tw : d + tw - 1) : "memory");
+    if (yy >= 0 && yy < th) {
+      const float4 *w = &p.w4[(int64_t)z * nxy + (int64_t)y * p.nx + X0];
+      for (int c = 0; c < tw; c += 8) asm volatile("prefetch.global.L2 [%0];" ::"l"(w + c) : "memory");
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(w + tw - 1) : "memory");
+    }
+  }
+}
+
 template <int TX, int TY, bool PRIV, int MINB = 1>
 __global__ void __launch_bounds__(TX * TY + 32, MINB) lattice_spec_kernel(LatParams p) {
   constexpr int NW = TX * TY;
@@ -1366,6 +1412,8 @@ __global__ void __launch_bounds__(TX * TY + 32, MINB) lattice_spec_kernel(LatPar
       __threadfence_block();
     }
     next = __shfl_sync(0xffffffffu, next, 0);
+    // the workers are still on visit k: bring the next tile's rows into L2
+    if (next >= 0 && p.prefetch) prefetch_tile_l2<TX, TY, PRIV>(p, next, lane);
     __syncwarp();
     asm volatile("bar.sync 2, %0;" ::"r"(NW + 32) : "memory");  // handoff k + 1
     // the workers reached this barrier only after finishing visit k
@@ -1621,6 +1669,8 @@ int launch_lattice(orsp::Graph *g, LatParams &p, int64_t ntiles, int nzb, int32_
   p.wait_ns = env_u64("ORSP_WAIT_NS", 2000000000ull);
   // ORSP_LAT_SELF=0: a tile to visit again goes back to the queue instead
   p.selfcont = (int)env_u64("ORSP_LAT_SELF", 1);
+  // ORSP_LAT_PREFETCH=0: no L2 prefetch of the next tile by the scheduler warp
+  p.prefetch = (int)env_u64("ORSP_LAT_PREFETCH", 1);
   p.budget_ns = env_u64("ORSP_BUDGET_NS", 20000000000ull);
   void *args[] = {&p, &tmw, &tmd};  // the tile and spec kernels take p only
   if (orsp::g_timer.on) ORSP_CUDA(cudaEventRecord(orsp::g_timer.a, st));
@@ -1824,7 +1874,23 @@ int run_lattice_boxes(Graph *g, const float *cost_d, int32_t nseeds, const int32
   const uint64_t decl = g->decl_cost == cost_d ? g->decl_gen : 0;
   g->decl_cost = nullptr;
   g->decl_gen = 0;
-  if (whole || (priv && vol_sum >= N)) {
+  // boxes with their own slices and device activity flags: only the active
+  // boxes' weights are gathered and their slices reset (one launch each)
+  const bool by_flag = priv && opt->active && !g->cvia && nbox <= 65535;
+  int64_t vmax = 1;
+  for (int32_t i = 0; i < nbox; ++i) {
+    const int32_t *b = boxes_h + 6 * (int64_t)i;
+    vmax = std::max<int64_t>(vmax, (int64_t)(b[1] - b[0] + 1) * (b[3] - b[2] + 1) * (b[5] - b[4] + 1));
+  }
+  const unsigned per_box = (unsigned)std::max<int64_t>(1, std::min<int64_t>((vmax + 255) / 256,
+                                                                            148 * 32 / std::max(1, nbox)));
+  if (by_flag) {
+    g->w4_cost = nullptr;  // part of wslot is rewritten
+    g->w4_gen = 0;
+    gather_boxes_kernel<<<dim3(per_box, (unsigned)nbox), 256, 0, st>>>(g->slot_eid, cost_d, (float4 *)g->wslot, N,
+                                                                       g->nx, g->ny, lboxes_d, opt->active);
+    ORSP_CUDA(cudaGetLastError());
+  } else if (whole || (priv && vol_sum >= N)) {
     if (!(decl != 0 && g->w4_cost == cost_d && g->w4_gen == decl)) {
       gather_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 148 * 32), 256, 0, st>>>(
           g->slot_eid, cost_d, (float4 *)g->wslot, N);
@@ -1843,15 +1909,8 @@ int run_lattice_boxes(Graph *g, const float *cost_d, int32_t nseeds, const int32
     if (!g->cvia && nbox > 1 && nbox <= 65535) {
       // one launch for all boxes, as many blocks per box as the largest needs
       // (within a grid of about 32 blocks per SM)
-      int64_t vmax = 1;
-      for (int32_t i = 0; i < nbox; ++i) {
-        const int32_t *b = boxes_h + 6 * (int64_t)i;
-        vmax = std::max<int64_t>(vmax, (int64_t)(b[1] - b[0] + 1) * (b[3] - b[2] + 1) * (b[5] - b[4] + 1));
-      }
-      const int64_t per = std::max<int64_t>(1, std::min<int64_t>((vmax + 255) / 256, 148 * 32 / nbox));
-      gather_boxes_kernel<<<dim3((unsigned)per, (unsigned)nbox), 256, 0, st>>>(g->slot_eid, cost_d,
-                                                                              (float4 *)g->wslot, N, g->nx,
-                                                                              g->ny, lboxes_d);
+      gather_boxes_kernel<<<dim3(per_box, (unsigned)nbox), 256, 0, st>>>(g->slot_eid, cost_d, (float4 *)g->wslot,
+                                                                         N, g->nx, g->ny, lboxes_d, nullptr);
       ORSP_CUDA(cudaGetLastError());
     } else {
       for (int32_t i = 0; i < nbox; ++i) {
@@ -1868,7 +1927,10 @@ int run_lattice_boxes(Graph *g, const float *cost_d, int32_t nseeds, const int32
       }
     }
   }
-  if (priv) {
+  if (by_flag) {
+    fill_slices_kernel<<<dim3(per_box, (unsigned)nbox), 256, 0, st>>>(dist, lboxes_d, opt->active, ORSP_INF_BITS);
+    ORSP_CUDA(cudaGetLastError());
+  } else if (priv) {
     fill_kernel<<<(int)std::min<int64_t>((opt->private_count + 255) / 256, 148 * 32), 256, 0, st>>>(
         dist, opt->private_count, ORSP_INF_BITS);
     ORSP_CUDA(cudaGetLastError());

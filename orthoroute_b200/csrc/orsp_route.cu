@@ -421,6 +421,7 @@ static int route_nets_impl(orsp_graph *g, int32_t M, const int32_t *src_h, const
       opt.private_dist = true;
       opt.private_count = gcells[q];
       opt.copy_ctl = false;
+      opt.active = act;  // repair rounds: only the flagged boxes are gathered and reset
       int rc = run_lattice_boxes(g, cost_d, n, seed_r, nullptr, n, boxes_o.data() + (size_t)a * 6, d_box + a,
                                  g->route_pdist, st, &opt);
       if (rc) return rc;
