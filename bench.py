@@ -57,11 +57,12 @@ SEED = 20261203
 # DRAM bytes (read + write) per lattice node and source of the tile search in
 # a many-source launch (lattice_spec_kernel, two CTAs per SM), from ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) on a 4-source launch of the
-# 1000x1000x12 lattice (bench.py --profile-case --per-launch 4): 1001.63 +
-# 179.83 MB for 4 x 12.0 M node-sources.  Every search settles every node;
+# 1000x1000x12 lattice (bench.py --profile-case --per-launch 4), with the
+# scheduler warp's L2 prefetch: 971.27 + 178.85 MB for 4 x 12.0 M
+# node-sources.  Every search settles every node;
 # the traffic is the distance slices read and written about once plus the
 # shared weights, so it grows with the sources per launch.
-LAT_DRAM_BYTES_PER_NODE = (1001.632768e6 + 179.826432e6) / (4 * 1000 * 1000 * 12)
+LAT_DRAM_BYTES_PER_NODE = (971.270912e6 + 178.853888e6) / (4 * 1000 * 1000 * 12)
 
 
 def _peaks():
