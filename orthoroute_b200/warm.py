@@ -189,12 +189,10 @@ def node_targets(lat: Lattice, history: np.ndarray, blur: int = 0) -> np.ndarray
     """float32 [nz][ny][nx][2]: log1p of the mean history of each node's planar
     and via out-edges (0 where it has none), optionally averaged over a
     (2 blur + 1)^2 window in x/y (a smooth congestion map)."""
-    src = lat.edge_src()
-    kind = np.asarray(lat.edge_kind)
-    out = np.zeros((lat.N, 2), np.float64)
-    cnt = np.zeros((lat.N, 2), np.float64)
-    np.add.at(out, (src, kind.astype(np.int64)), history.astype(np.float64))
-    np.add.at(cnt, (src, kind.astype(np.int64)), 1.0)
+    # per (node, kind) sums in edge order
+    idx = lat.edge_src().astype(np.int64) * 2 + np.asarray(lat.edge_kind).astype(np.int64)
+    out = np.bincount(idx, weights=np.asarray(history, np.float64), minlength=2 * lat.N).reshape(lat.N, 2)
+    cnt = np.bincount(idx, minlength=2 * lat.N).astype(np.float64).reshape(lat.N, 2)
     mean = np.where(cnt > 0, out / np.maximum(cnt, 1), 0.0)
     t = np.log1p(mean).astype(np.float32).reshape(lat.nz, lat.ny, lat.nx, 2)
     if blur > 0:

@@ -29,16 +29,23 @@ import torch
 
 from .lattice import board_footprints
 from .negotiate import NegotiationConfig, PathFinder
-from .warm import WarmNet, board_features, history_from_prediction, node_targets, rudy_prediction
+from .warm import (WarmNet, board_features, board_features_device, history_from_prediction, node_targets,
+                   rudy_prediction)
 
 DENSITY = 8000 / (600 * 600)
 DEFAULT_OUT = Path(__file__).resolve().parent / "data" / "warm_history.npz"
 
 
+# snapshot groups of the routing schedule (0: one launch per round of
+# disjoint boxes), set from --group-nets / --group-repair
+SCHEDULE = {"group_nets": 0, "group_repair": 0}
+
+
 def route_config(max_iterations: int = 60) -> NegotiationConfig:
     """The routing schedule of the backplane benchmark."""
     return NegotiationConfig(max_iterations=max_iterations, cost_update="net", reroute="offenders", roi_margin=10,
-                             full_graph_retry=False, net_order="disjoint", stall_grow=10, stall_iterations=2)
+                             full_graph_retry=False, net_order="disjoint", stall_grow=10, stall_iterations=2,
+                             group_nets=SCHEDULE["group_nets"], group_repair=SCHEDULE["group_repair"])
 
 
 def make_board(size: int, nz: int, seed: int):
@@ -46,15 +53,24 @@ def make_board(size: int, nz: int, seed: int):
     return board_footprints(size, size, nz, nets, None, seed=seed)
 
 
-def make_sample(size: int, nz: int, seed: int, device=None, blur: int = 2) -> dict:
+def make_sample(size: int, nz: int, seed: int, device=None, blur: int = 2, on_device: bool = False) -> dict:
     """Routes one board with zero history; returns features, targets (the
-    final history, blurred over 2 blur + 1 cells in x/y) and stats."""
+    final history, blurred over 2 blur + 1 cells in x/y) and stats.  With
+    on_device, the features are the padded bf16 device tensor the network
+    reads (board_features_device: the same values as board_features after
+    the bf16 conversion) and size must be a multiple of 8."""
     b = make_board(size, nz, seed)
     pf = PathFinder(b.lattice, config=route_config(), device=device)
     r = pf.route(b.src, b.dst, mode="batched")
     hist = pf.acc.history.cpu().numpy()
-    return {"x": board_features(b.lattice, b.src, b.dst), "t": node_targets(b.lattice, hist, blur),
+    x = board_features_device(b.lattice, b.src, b.dst, device=pf.device) if on_device else \
+        board_features(b.lattice, b.src, b.dst)
+    return {"x": x, "t": node_targets(b.lattice, hist, blur),
             "iterations": len(r.iterations), "converged": r.converged, "seconds": r.seconds, "seed": seed}
+
+
+def _x_device(x) -> torch.Tensor:
+    return x if isinstance(x, torch.Tensor) else torch.from_numpy(x).cuda().to(torch.bfloat16)
 
 
 def _crop(a: torch.Tensor, y0: int, x0: int, c: int) -> torch.Tensor:
@@ -75,7 +91,7 @@ def train(net: WarmNet, data: List[dict], epochs: int, lr: float = 2e-3, seed: i
     crop x crop window (a multiple of 8) of a random board; otherwise one
     step per whole board."""
     rng = np.random.default_rng(seed)
-    xs = [torch.from_numpy(d["x"]).cuda().to(torch.bfloat16) for d in data]
+    xs = [_x_device(d["x"]) for d in data]
     ts = [torch.from_numpy(np.ascontiguousarray(d["t"])).cuda() for d in data]
     hist = []
     n_steps = steps_per_epoch if crop else len(data)
@@ -104,7 +120,7 @@ def train(net: WarmNet, data: List[dict], epochs: int, lr: float = 2e-3, seed: i
 def eval_loss(net: WarmNet, data: List[dict]) -> float:
     tot = 0.0
     for d in data:
-        out = net.forward(torch.from_numpy(d["x"]).cuda().to(torch.bfloat16))
+        out = net.forward(_x_device(d["x"]))
         loss, _ = net.loss_grad(out, torch.from_numpy(np.ascontiguousarray(d["t"])).cuda())
         tot += float(loss)
     return tot / max(1, len(data))
@@ -163,13 +179,20 @@ def main(argv: Optional[List[str]] = None):
     ap.add_argument("--rudy-scales", default="", help="scales tried for the RUDY prior (empty: no ablation)")
     ap.add_argument("--out", default=str(DEFAULT_OUT))
     ap.add_argument("--summary", default=None)
+    ap.add_argument("--group-nets", type=int, default=0,
+                    help="route targets and held-out boards in snapshot groups of this many nets (0: disjoint rounds)")
+    ap.add_argument("--group-repair", type=int, default=3, help="repair rounds of the snapshot groups")
+    ap.add_argument("--features-on-device", action="store_true",
+                    help="keep every board's features on the GPU as bf16 (many boards; size a multiple of 8)")
     args = ap.parse_args(argv)
+    SCHEDULE["group_nets"] = args.group_nets
+    SCHEDULE["group_repair"] = args.group_repair if args.group_nets > 0 else 0
     log = lambda m: print(m, flush=True)  # noqa: E731
     t0 = time.perf_counter()
     seeds = [args.seed + i for i in range(args.boards + args.heldout)]
     data = []
     for i, sd in enumerate(seeds):
-        data.append(make_sample(args.size, args.nz, sd, blur=args.blur))
+        data.append(make_sample(args.size, args.nz, sd, blur=args.blur, on_device=args.features_on_device))
         log(f"routed {i + 1}/{len(seeds)} boards ({data[-1]['iterations']} iterations, "
             f"{data[-1]['seconds']:.1f} s)")
     t_data = time.perf_counter() - t0
@@ -215,6 +238,7 @@ def main(argv: Optional[List[str]] = None):
                "heldout_plain_iterations": plain_its, "heldout_plain_seconds": plain_secs,
                "crop": args.crop, "steps": args.steps, "boost": args.boost, "blur": args.blur, "lr": args.lr,
                "sec_data": round(t_data, 1), "sec_train": round(t_train, 1),
+               "group_nets": SCHEDULE["group_nets"], "group_repair": SCHEDULE["group_repair"],
                "plain_iterations_mean": float(np.mean([d["iterations"] for d in data]))}
     log(json.dumps(summary))
     if args.summary:
