@@ -484,7 +484,15 @@ def warm_history_device(net: "WarmNet", lat: Lattice, src, dst, scale: float) ->
     dev = net.device
     x = board_features_device(lat, np.asarray(src), np.asarray(dst), net.features, device=dev)
     out = net.forward(x)[:, :lat.ny, :lat.nx, :USED].float()
-    p = torch.expm1(torch.clamp(out.reshape(lat.N, 2).double(), min=0.0))
+    return history_from_prediction_device(lat, out, scale)
+
+
+def history_from_prediction_device(lat: Lattice, pred: torch.Tensor, scale: float) -> torch.Tensor:
+    """history_from_prediction on the device: pred float32 [nz][ny][nx][2]
+    (device) -> float32 [E] (device); expm1 of the clamped prediction in
+    float64, times scale, rounded to float32."""
+    dev = pred.device
+    p = torch.expm1(torch.clamp(pred.reshape(lat.N, 2).double(), min=0.0))
     indptr = torch.from_numpy(np.ascontiguousarray(lat.indptr, dtype=np.int64)).to(dev)
     es = torch.repeat_interleave(torch.arange(lat.N, device=dev), indptr[1:] - indptr[:-1])
     ek = torch.from_numpy(np.ascontiguousarray(lat.edge_kind)).to(dev).long()

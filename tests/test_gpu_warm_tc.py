@@ -34,14 +34,20 @@ def _status():
     return v.value
 
 
-@pytest.mark.parametrize("cin,cout,relu,masked,W", [(16, 32, True, False, 70), (32, 32, False, True, 260),
-                                                    (32, 16, True, True, 128), (32, 64, True, False, 131),
-                                                    (16, 16, False, False, 9)])
-def test_conv3d_tc_matches_oracle_and_wmma(cin, cout, relu, masked, W):
+@pytest.mark.parametrize("cin,cout,relu,masked,W,D,H", [(16, 32, True, False, 70, 3, 5), (32, 32, False, True, 260, 3, 5),
+                                                        (32, 16, True, True, 128, 3, 5), (32, 64, True, False, 131, 3, 5),
+                                                        (16, 16, False, False, 9, 3, 5),
+                                                        (32, 32, True, True, 200, 6, 40),
+                                                        (32, 64, False, False, 131, 4, 60)])
+def test_conv3d_tc_matches_oracle_and_wmma(cin, cout, relu, masked, W, D, H):
+    """The tensor-core convolution against the fp32 oracle and the WMMA
+    kernel: partial and several tiles per row, with and without the ReLU
+    mask, bf16 and fp32 outputs; the last two shapes give every CTA about
+    three tiles (480 tiles on 148 CTAs), so the epilogue of one tile runs
+    beside the next tile's MMAs in both accumulators."""
     from orthoroute_b200 import _lib
     from orthoroute_b200._lib import ptr
 
-    D, H = 3, 5
     g = torch.Generator().manual_seed(cin + 3 * cout + W)
     x = _bf(torch.randn(D, H, W, cin, generator=g))
     m = _bf(torch.randn(D, H, W, cin, generator=g)) if masked else None
