@@ -73,6 +73,80 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+class NvmlClockSampler:
+    """SM clock, its maximum and the clock-event (throttle) reasons of one
+    GPU, read through NVML every 10 ms from a thread while the timed region
+    runs, plus one reading at start and one at stop (a region of a few
+    hundred ms still gets samples).  Only reads the GPU's state."""
+
+    REASONS = (("hw_slowdown", "HwSlowdown"), ("hw_thermal_slowdown", "HwThermalSlowdown"),
+               ("sw_thermal_slowdown", "SwThermalSlowdown"), ("sw_power_cap", "SwPowerCap"))
+
+    def __init__(self, device):
+        import pynvml
+
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        props = __import__("torch").cuda.get_device_properties(device)
+        h = None
+        try:
+            h = pynvml.nvmlDeviceGetHandleByUUID("GPU-" + str(props.uuid))
+        except Exception:
+            try:
+                h = pynvml.nvmlDeviceGetHandleByPciBusId(
+                    "%08X:%02X:%02X.0" % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id))
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(int(getattr(device, "index", 0) or 0))
+        self.h = h
+        self.bits = {name: getattr(pynvml, "nvmlClocksEventReason" + key,
+                                   getattr(pynvml, "nvmlClocksThrottleReason" + key, 0)) for name, key in self.REASONS}
+        self.reasons_fn = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+        self.rows = []
+        self.stop_flag = None
+        self.thread = None
+
+    def _read(self):
+        nv = self.nv
+        self.rows.append((nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM),
+                          nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM), int(self.reasons_fn(self.h))))
+
+    def start(self):
+        import threading
+
+        self.stop_flag = threading.Event()
+        self._read()
+
+        def loop():
+            while not self.stop_flag.wait(0.01):
+                try:
+                    self._read()
+                except Exception:
+                    return
+
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
+
+    def stop(self):
+        self.stop_flag.set()
+        self.thread.join(timeout=5)
+        self._read()
+        sm = [float(r[0]) for r in self.rows]
+        load = [v for v in sm if v > 0.5 * max(sm)] if sm else []
+        reasons = sorted({name for r in self.rows for name, bit in self.bits.items() if bit and (r[2] & bit)})
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": max(float(r[1]) for r in self.rows) if self.rows else None,
+                "reasons": reasons, "samples": len(self.rows), "sampler": "nvml, 10 ms"}
+
+
+def clock_sampler(device):
+    """The NVML sampler, else nvidia-smi's (200 ms)."""
+    try:
+        return NvmlClockSampler(device)
+    except Exception:
+        return ClockSampler(getattr(device, "index", 0) or 0)
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
 
@@ -833,7 +907,7 @@ def run_ours(args, world, rank, local):
             step_fn()
         acc.update(ms=0.0, visits=0, n=0)
         lib.orsp_profile_enable(1)
-        clocks = ClockSampler(dev.index) if with_clocks else None
+        clocks = clock_sampler(dev) if with_clocks else None
         barrier(world)
         torch.cuda.synchronize(dev)
         if clocks:
