@@ -21,6 +21,7 @@
 // Every mbarrier wait is bounded by the global timer; on expiry the kernel
 // records an error, waits once more (bounded) for its MMAs, frees its TMEM
 // and returns.  Single-GPU code: no TMA, no multicast.
+#include <cstdlib>
 #include <algorithm>
 #include <climits>
 #include <cstdint>
@@ -406,6 +407,291 @@ __global__ void __launch_bounds__(CV_THREADS, 1) conv3d_tc_kernel(
   }
 }
 
+// Warp-specialised form of the same convolution (the default;
+// ORSP_WARM_TC_WS=0 selects the kernel above).
+// Eight producer warps copy the stages and drain the accumulators; one MMA
+// warp (lane 0) issues the tensor-core MMAs.  No block barrier separates the
+// stages; per-buffer mbarriers hand them over:
+//   full[b]   the producers' copies of the stage in b have landed (256
+//             arrivals, each after its thread's cp.async group completed and
+//             a proxy fence);
+//   empty[b]  the MMAs that read b are done (tcgen05.commit);
+//   accf[a]   accumulator a holds a finished tile (tcgen05.commit after the
+//             tile's last stage);
+//   acce[a]   the producers have read accumulator a (256 arrivals).
+// Tiles alternate between two TMEM accumulators, so a tile's epilogue runs
+// while the MMAs of the next tile proceed.  The producers signal stage s
+// after issuing stage s + LAG (LAG = NS - 2, at most 4); a buffer is refilled
+// only after its previous stage's MMAs are done, so the copies of LAG stages
+// are in flight while the tensor core consumes.  Every wait is bounded; a
+// wait that expires sets a shared abort flag that ends every other wait.
+constexpr int WS_PROD = 256;
+constexpr int WS_THREADS = WS_PROD + 32;
+
+__host__ __device__ constexpr size_t ws_smem_bytes(int Cin, int Cout, int ns) {
+  return cv_weight_bytes(Cin, Cout) + ns * cv_stage_bytes(Cin) + 16 * ns + 64;
+}
+
+template <int CG>
+__global__ void __launch_bounds__(WS_THREADS, 1) conv3d_tc_ws_kernel(
+    const __nv_bfloat16 *__restrict__ X, const __nv_bfloat16 *__restrict__ Mk, const __nv_bfloat16 *__restrict__ Wt,
+    const float *__restrict__ bias, __nv_bfloat16 *__restrict__ Y, float *__restrict__ Yf, int D, int H, int W,
+    int Cin, int Cout, int relu, int NS) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  __shared__ volatile int s_abort;
+  const int KC = Cin >> 4;
+  const int bblk = Cout * 32;
+  const size_t SBY = cv_stage_bytes(Cin);
+  unsigned char *sB = sm;
+  unsigned char *sA = sm + cv_weight_bytes(Cin, Cout);
+  unsigned long long *full = reinterpret_cast<unsigned long long *>(sA + NS * SBY);
+  unsigned long long *empty = full + NS;
+  unsigned long long *accf = empty + NS;
+  unsigned long long *acce = accf + 2;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(acce + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t ncols1 = Cout <= 32 ? 32u : 64u, ncols = 2 * ncols1;
+
+  const int units_per_tap = Cin * Cout / 8;
+  for (int i = tid; i < 27 * units_per_tap; i += WS_THREADS) {
+    const int tap = i / units_per_tap, r = i - tap * units_per_tap;
+    const int kg = r / Cout, n = r - kg * Cout;
+    const __nv_bfloat16 *src = Wt + (static_cast<int64_t>(tap) * Cin + kg * 8) * Cout + n;
+    uint32_t v[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const uint32_t lo = __bfloat16_as_ushort(src[(2 * j) * Cout]);
+      const uint32_t hi = __bfloat16_as_ushort(src[(2 * j + 1) * Cout]);
+      v[j] = lo | (hi << 16);
+    }
+    unsigned char *dst = sB + (tap * KC + (kg >> 1)) * bblk + (n >> 3) * 256 + (kg & 1) * 128 + (n & 7) * 16;
+    *reinterpret_cast<uint4 *>(dst) = make_uint4(v[0], v[1], v[2], v[3]);
+  }
+  if (tid == 0) {
+    s_abort = 0;
+    for (int b = 0; b < NS; ++b) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(full + b)), "r"(WS_PROD) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(empty + b)) : "memory");
+    }
+    for (int a = 0; a < 2; ++a) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(accf + a)) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(acce + a)), "r"(WS_PROD) : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 8) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = umma_idesc_bf16(TC_M, Cout);
+
+  const int ntx = (W + TC_M - 1) / TC_M;
+  const int64_t ntiles = static_cast<int64_t>(D) * H * ntx;
+  const int64_t my_tiles = ntiles > blockIdx.x ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const int ntiles32 = static_cast<int>(ntiles);
+  const int nst32 = static_cast<int>(my_tiles * 9);
+  const int my32 = static_cast<int>(my_tiles);
+  struct Cursor {
+    int st9, buf, par, t, tx, y, z;
+  };
+  auto tile_coords = [&](Cursor &c) {
+    c.tx = c.t % ntx;
+    const int zy = c.t / ntx;
+    c.y = zy % H;
+    c.z = zy / H;
+  };
+  auto advance = [&](Cursor &c) {
+    if (++c.buf == NS) {
+      c.buf = 0;
+      c.par ^= 1;
+    }
+    if (++c.st9 == 9) {
+      c.st9 = 0;
+      c.t += gridDim.x;
+      if (c.t < ntiles32) tile_coords(c);
+    }
+  };
+  // a bounded wait that also ends when another role has given up
+  auto wait = [&](unsigned long long *bar, int parity) -> bool {
+    const uint32_t a = smem_addr(bar);
+    const unsigned long long t0 = dev_globaltimer();
+    for (;;) {
+      if (mbar_try(a, static_cast<uint32_t>(parity))) return true;
+      if (s_abort) return false;
+      if (dev_globaltimer() - t0 > TC_WAIT_NS) {
+        s_abort = 1;
+        atomicExch(&g_tc_err, 1);
+        return false;
+      }
+    }
+  };
+  const int LAG = NS - 2 < 4 ? NS - 2 : 4;
+
+  if (warp < 8) {
+    // ------------------------------------------------------------ producers
+    constexpr int CIN = CG * 8;
+    constexpr int UNITS = (TC_M + 2) * CG;
+    constexpr int UPT = (UNITS + WS_PROD - 1) / WS_PROD;
+    int u_x[UPT], u_off[UPT], u_dst[UPT];
+#pragma unroll
+    for (int j = 0; j < UPT; ++j) {
+      const int i = tid + j * WS_PROD;
+      const int vx = i / CG, cg = i % CG;
+      const bool unit = i < UNITS;
+      u_x[j] = unit ? vx - 1 : INT_MIN / 2;
+      u_off[j] = (vx - 1) * CIN + cg * 8;
+      u_dst[j] = unit ? cg * CV_PLANE + vx * 16 : -1;
+    }
+    auto epilogue = [&](int tx, int y, int z, int acc) {
+      const int m = (warp & 3) * 32 + lane, xx = tx * TC_M + m;
+      for (int c0 = (warp >> 2) * 16; c0 < Cout; c0 += 32) {
+        uint32_t r[16];
+        tmem_ld16(tmem + (static_cast<uint32_t>((warp & 3) * 32) << 16) + static_cast<uint32_t>(acc) * ncols1 +
+                      static_cast<uint32_t>(c0),
+                  r);
+        if (xx < W) {
+          const int64_t o = ((static_cast<int64_t>(z) * H + y) * W + xx) * Cout + c0;
+          float f[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const float v = __uint_as_float(r[j]) + (bias ? bias[c0 + j] : 0.0f);
+            f[j] = relu ? fmaxf(v, 0.0f) : v;
+          }
+          if (Yf) {
+#pragma unroll
+            for (int j = 0; j < 16; j += 4)
+              *reinterpret_cast<float4 *>(Yf + o + j) = make_float4(f[j], f[j + 1], f[j + 2], f[j + 3]);
+          } else {
+            uint32_t p[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              p[j] = static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16(f[2 * j]))) |
+                     (static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16(f[2 * j + 1]))) << 16);
+            *reinterpret_cast<uint4 *>(Y + o) = make_uint4(p[0], p[1], p[2], p[3]);
+            *reinterpret_cast<uint4 *>(Y + o + 8) = make_uint4(p[4], p[5], p[6], p[7]);
+          }
+        }
+      }
+    };
+    Cursor ci{0, 0, 0, static_cast<int>(blockIdx.x), 0, 0, 0};  // the stage issued next
+    tile_coords(ci);
+    Cursor cs{0, 0, 0, static_cast<int>(blockIdx.x), 0, 0, 0};  // the stage signalled next
+    Cursor et{0, 0, 0, static_cast<int>(blockIdx.x), 0, 0, 0};  // the tile drained next
+    tile_coords(et);
+    int ep_T = 0;
+    bool ok = true;
+    // drains tile ep_T (accumulator ep_T & 1) and frees the accumulator
+    auto drain = [&]() -> bool {
+      if (!wait(accf + (ep_T & 1), (ep_T >> 1) & 1)) return false;
+      tc_fence_after();
+      epilogue(et.tx, et.y, et.z, ep_T & 1);
+      tc_fence_before();
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(acce + (ep_T & 1))) : "memory");
+      ++ep_T;
+      et.t += gridDim.x;
+      if (et.t < ntiles32) tile_coords(et);
+      return true;
+    };
+    for (int s = 0; s < nst32 + LAG && ok; ++s) {
+      if (s < nst32) {
+        // the buffer's previous stage must have been consumed
+        if (s >= NS && !wait(empty + ci.buf, ci.par ^ 1)) {
+          ok = false;
+          break;
+        }
+        const int zz = ci.z + ci.st9 / 3 - 1, yy = ci.y + ci.st9 % 3 - 1, x0 = ci.tx * TC_M;
+        const bool rowok = zz >= 0 && zz < D && yy >= 0 && yy < H;
+        unsigned char *buf = sA + static_cast<size_t>(ci.buf) * SBY;
+        const __nv_bfloat16 *row = X + ((static_cast<int64_t>(rowok ? zz : 0) * H + (rowok ? yy : 0)) * W + x0) * CIN;
+#pragma unroll
+        for (int j = 0; j < UPT; ++j) {
+          const int xx = x0 + u_x[j];
+          const bool in = rowok && xx >= 0 && xx < W;
+          const __nv_bfloat16 *src = in ? row + u_off[j] : X;
+          if (u_dst[j] < 0) continue;
+          if (!Mk) {
+            cp_async16(buf + u_dst[j], src, in ? 16 : 0);
+          } else {
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (in) {
+              v = *reinterpret_cast<const uint4 *>(src);
+              const uint4 mk = *reinterpret_cast<const uint4 *>(Mk + (src - X));
+              __nv_bfloat16 *pv = reinterpret_cast<__nv_bfloat16 *>(&v);
+              const __nv_bfloat16 *pm = reinterpret_cast<const __nv_bfloat16 *>(&mk);
+#pragma unroll
+              for (int q = 0; q < 8; ++q)
+                if (!(__bfloat162float(pm[q]) > 0.0f)) pv[q] = __float2bfloat16(0.0f);
+            }
+            *reinterpret_cast<uint4 *>(buf + u_dst[j]) = v;
+          }
+        }
+        advance(ci);
+      }
+      cp_async_commit();
+      const int sd = s - LAG;
+      if (sd >= 0) {
+        // this thread's copies of stage sd have landed: hand them to the
+        // async proxy and count them in
+        cp_async_wait(LAG);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(full + cs.buf)) : "memory");
+        advance(cs);
+        // two stages of the next tile are handed over: drain the tile before
+        if (sd == 9 * ep_T + 10 && !drain()) ok = false;
+      }
+    }
+    while (ok && ep_T < my32) ok = drain();
+    cp_async_wait(0);
+  } else if (lane == 0) {
+    // ------------------------------------------------------------ MMA warp
+    Cursor cc{0, 0, 0, static_cast<int>(blockIdx.x), 0, 0, 0};
+    int T = 0, last_buf = -1, last_par = 0;
+    bool ok = true;
+    for (int s = 0; s < nst32; ++s) {
+      const int st9 = cc.st9, a = T & 1;
+      if (st9 == 0 && T >= 2 && !wait(acce + a, ((T - 2) >> 1) & 1)) { ok = false; break; }
+      if (!wait(full + cc.buf, cc.par)) { ok = false; break; }
+      tc_fence_after();
+      const int tapz = (st9 / 3) * 9 + (st9 % 3) * 3;
+#pragma unroll 1
+      for (int dxi = 0; dxi < 3; ++dxi)
+        for (int kc = 0; kc < KC; ++kc) {
+          const uint64_t ad =
+              umma_smem_desc(smem_addr(sA + cc.buf * SBY + (2 * kc) * CV_PLANE + dxi * 16), CV_PLANE, 128);
+          const uint64_t bd = umma_smem_desc(smem_addr(sB + ((tapz + dxi) * KC + kc) * bblk), 128, 256);
+          mma_bf16(tmem + static_cast<uint32_t>(a) * ncols1, ad, bd, idesc, (st9 | dxi | kc) != 0 ? 1u : 0u);
+        }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_addr(empty + cc.buf))
+                   : "memory");
+      if (st9 == 8)
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_addr(accf + a))
+                     : "memory");
+      last_buf = cc.buf;
+      last_par = cc.par;
+      if (st9 == 8) ++T;
+      advance(cc);
+    }
+    // after a failed wait, the MMAs in flight get one more bounded wait (the
+    // last commit completes after all earlier ones) before TMEM is freed
+    if (!ok && last_buf >= 0) mbar_wait(smem_addr(empty + last_buf), static_cast<uint32_t>(last_par));
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 8) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+  }
+}
+
 // Instruction descriptor with both operands MN-major (bit 15: A, bit 16: B).
 __host__ __device__ constexpr uint32_t umma_idesc_bf16_mn(int M, int N) {
   return umma_idesc_bf16(M, N) | (1u << 15) | (1u << 16);
@@ -611,6 +897,21 @@ extern "C" int orsp_warm_conv3d_tc(const void *X, const void *mask, const void *
     return ORSP_ERR_ARG;
   }
   const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(ntiles, sms)));
+  // the warp-specialised kernel (producer warps and an MMA warp handing
+  // stages over through mbarriers); ORSP_WARM_TC_WS=0: the kernel with one
+  // block barrier per stage
+  const char *ws = getenv("ORSP_WARM_TC_WS");
+  if (!(ws && ws[0] == '0')) {
+    decltype(kfn) kws = Cin == 16 ? conv3d_tc_ws_kernel<2> : Cin == 32 ? conv3d_tc_ws_kernel<4>
+                                                                       : conv3d_tc_ws_kernel<8>;
+    const size_t smem_ws = ws_smem_bytes(Cin, Cout, ns);
+    ORSP_CUDA(cudaFuncSetAttribute(kws, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ws));
+    kws<<<grid, WS_THREADS, smem_ws, (cudaStream_t)stream>>>((const __nv_bfloat16 *)X, (const __nv_bfloat16 *)mask,
+                                                             (const __nv_bfloat16 *)Wt, bias, (__nv_bfloat16 *)Y, Yf,
+                                                             D, H, W, Cin, Cout, relu, ns);
+    ORSP_CUDA(cudaGetLastError());
+    return ORSP_OK;
+  }
   kfn<<<grid, CV_THREADS, smem, (cudaStream_t)stream>>>((const __nv_bfloat16 *)X, (const __nv_bfloat16 *)mask,
                                                         (const __nv_bfloat16 *)Wt, bias, (__nv_bfloat16 *)Y, Yf, D, H,
                                                         W, Cin, Cout, relu, ns);

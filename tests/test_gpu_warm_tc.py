@@ -39,14 +39,19 @@ def _status():
                                                         (16, 16, False, False, 9, 3, 5),
                                                         (32, 32, True, True, 200, 6, 40),
                                                         (32, 64, False, False, 131, 4, 60)])
-def test_conv3d_tc_matches_oracle_and_wmma(cin, cout, relu, masked, W, D, H):
+@pytest.mark.parametrize("kernel", ["warp-specialised", "stage-barrier"])
+def test_conv3d_tc_matches_oracle_and_wmma(cin, cout, relu, masked, W, D, H, kernel, monkeypatch):
     """The tensor-core convolution against the fp32 oracle and the WMMA
     kernel: partial and several tiles per row, with and without the ReLU
     mask, bf16 and fp32 outputs; the last two shapes give every CTA about
     three tiles (480 tiles on 148 CTAs), so the epilogue of one tile runs
-    beside the next tile's MMAs in both accumulators."""
+    beside the next tile's MMAs in both accumulators.  Both kernels: the
+    warp-specialised one (producer warps, an MMA warp, mbarrier handoffs) and
+    the one with a block barrier per stage (ORSP_WARM_TC_WS=0)."""
     from orthoroute_b200 import _lib
     from orthoroute_b200._lib import ptr
+
+    monkeypatch.setenv("ORSP_WARM_TC_WS", "0" if kernel == "stage-barrier" else "1")
 
     g = torch.Generator().manual_seed(cin + 3 * cout + W)
     x = _bf(torch.randn(D, H, W, cin, generator=g))
