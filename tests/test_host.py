@@ -52,6 +52,14 @@ def test_host_validation_without_gpu():
     assert b"out of range" in L.orsp_last_error()
     rc = L.orsp_update_costs(10, None, None, None, None, None, None, None, 1.0, 1.0, 1.0, 1.0, 1, None, 0)
     assert rc == _lib.ORSP_ERR_ARG
+    # the snapshot routing loop: negative repair rounds, and no graph
+    n = ctypes.c_int64(-1)
+    rc = L.orsp_route_nets_snapshot(None, 1, None, None, None, 1, None, 0, None, -1, None, None, 16, None, None,
+                                    None, None, None, None, None, 1.0, 1.0, 1.0, 1.0, 0, ctypes.byref(n), 0)
+    assert rc == _lib.ORSP_ERR_ARG and b"repair_rounds" in L.orsp_last_error()
+    rc = L.orsp_route_nets_snapshot(None, 1, None, None, None, 1, None, 0, None, 2, None, None, 16, None, None,
+                                    None, None, None, None, None, 1.0, 1.0, 1.0, 1.0, 0, ctypes.byref(n), 0)
+    assert rc == _lib.ORSP_ERR_ARG and n.value == 0
 
 
 def test_fastdiv_exhaustive_samples(tmp_path):
