@@ -5,7 +5,12 @@ runs on the GPU (steps of PathFinderRouter._pathfinder_negotiation,
 orthoroute/algorithms/manhattan/unified_pathfinder.py:3548-4259, and
 _route_all, UPF:4441-4823): numpy float32 accounting in the reference's
 expression order and the C heap Dijkstra on box ROIs.  Used to check that the
-device loop gives bit-identical per-iteration overuse and final routes.
+device loop gives bit-identical per-iteration overuse and final routes.  It
+also restates the loop's snapshot-group schedule (cfg.group_nets /
+group_repair: groups of nets searched on one cost snapshot, as the
+reference's batched mode searches a batch of ROIs on one cost array,
+CD:2014, then repair rounds for nets that share an edge with an earlier net
+of the group), which orsp_route_nets_snapshot runs on the device.
 """
 from __future__ import annotations
 
