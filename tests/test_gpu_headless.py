@@ -111,3 +111,21 @@ def test_headless_via_sets_match_oracle(tmp_path, mode, vias):
     assert s["lattice_vias"] == vias and (vias == "adjacent" or s["forced_overuse"] == 0)
     ref = route_plain(prob.lattice, prob.search_src, prob.search_dst, headless_config(30))
     _check(prob, ref, s, geom, meta)
+
+
+@pytest.mark.parametrize("vias", ["full", "adjacent"])
+def test_headless_snapshot_groups_match_oracle(tmp_path, vias):
+    """`--groups`: the portal flow routed in snapshot groups of 8 nets with
+    3 repair rounds (orsp_route_nets_snapshot, on the column-via lattice of
+    the reference's via set or on adjacent vias); every net's stubs, tracks
+    and vias equal the oracle loop's of the same schedule."""
+    b = board_uniform_pins(40, 32, 6, 30, seed=5)
+    orp = tmp_path / "board.orp"
+    ors = tmp_path / "board.ors"
+    write_orp(synthetic_board_data(b), orp)
+    s = run_headless(str(orp), str(ors), max_iterations=30, mode="batched", log=None, vias=vias, groups=8)
+    geom, meta = read_ors(ors)
+    prob = build_problem(orp_to_board_data(read_orp(orp)), portals=True, vias=vias)
+    assert s["snapshot_groups"] == 8
+    ref = route_plain(prob.lattice, prob.search_src, prob.search_dst, headless_config(30, groups=8))
+    _check(prob, ref, s, geom, meta)
