@@ -1,16 +1,19 @@
 """Training data, training and evaluation of the history warm start.
 
-    python -m orthoroute_b200.warm_train [--boards 14] [--heldout 2] [--size 600] [--epochs 30]
-                                         [--scale-size 600] [--rudy-scales 1,4,16]
+    python -m orthoroute_b200.warm_train [--boards 500] [--heldout 50] [--size 200] [--epochs 30]
+                                         [--scale-size 600] [--scales 4,16,64] [--rudy-scales 1,4,16]
+                                         [--group-nets 32] [--group-repair 3]
                                          [--out orthoroute_b200/data/warm_history.npz]
 
 Boards: seeded connector-footprint boards (2x50-pin footprints, one net per
 pin) of size x size cells and 18 layers, with nets at the density of the
 600x600x18 backplane (8 000 nets on 360 000 cells); seeds from 2000, so the
 benchmark board (seed 3) is never seen.  Each board is routed to zero
-overuse by plain PathFinder (per-net live costs, zero initial history); its
-final history field, log1p per node and kind, averaged over 5x5 cells in x/y,
-is the training target.  Training takes random 200x200 windows (the net is
+overuse by PathFinder with per-net live costs from zero initial history, in
+snapshot groups of --group-nets nets with --group-repair repair rounds (the
+schedule the prediction later steers; --group-nets 0: one launch per round
+of disjoint boxes); its final history field, log1p per node and kind,
+averaged over 5x5 cells in x/y, is the training target.  Training takes random 200x200 windows (the net is
 fully convolutional).  The history scale used at routing time is chosen on
 the held-out boards: the one that converges on most boards with the fewest
 iterations (ties: least time).  The defaults reproduce the weights shipped
@@ -162,9 +165,9 @@ def choose_scale(net, size: int, nz: int, seeds: List[int], scales=(0.25, 0.5, 1
 
 def main(argv: Optional[List[str]] = None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--boards", type=int, default=14)
-    ap.add_argument("--heldout", type=int, default=2)
-    ap.add_argument("--size", type=int, default=600)
+    ap.add_argument("--boards", type=int, default=500)
+    ap.add_argument("--heldout", type=int, default=50)
+    ap.add_argument("--size", type=int, default=200)
     ap.add_argument("--nz", type=int, default=18)
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--seed", type=int, default=2000)
@@ -174,16 +177,17 @@ def main(argv: Optional[List[str]] = None):
     ap.add_argument("--blur", type=int, default=2, help="target averaged over (2 blur + 1)^2 cells in x/y")
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--scale-boards", type=int, default=2, help="held-out boards used to choose the scale")
-    ap.add_argument("--scale-size", type=int, default=0, help="size of those boards (0: --size)")
-    ap.add_argument("--scales", default="1,4,16")
-    ap.add_argument("--rudy-scales", default="", help="scales tried for the RUDY prior (empty: no ablation)")
+    ap.add_argument("--scale-size", type=int, default=600, help="size of those boards (0: --size)")
+    ap.add_argument("--scales", default="4,16,64")
+    ap.add_argument("--rudy-scales", default="1,4,16", help="scales tried for the RUDY prior (empty: no ablation)")
     ap.add_argument("--out", default=str(DEFAULT_OUT))
     ap.add_argument("--summary", default=None)
-    ap.add_argument("--group-nets", type=int, default=0,
+    ap.add_argument("--group-nets", type=int, default=32,
                     help="route targets and held-out boards in snapshot groups of this many nets (0: disjoint rounds)")
     ap.add_argument("--group-repair", type=int, default=3, help="repair rounds of the snapshot groups")
-    ap.add_argument("--features-on-device", action="store_true",
-                    help="keep every board's features on the GPU as bf16 (many boards; size a multiple of 8)")
+    ap.add_argument("--features-on-host", action="store_true",
+                    help="keep the boards' features on the host as float32 (default: on the GPU as bf16, size a "
+                         "multiple of 8)")
     args = ap.parse_args(argv)
     SCHEDULE["group_nets"] = args.group_nets
     SCHEDULE["group_repair"] = args.group_repair if args.group_nets > 0 else 0
@@ -192,7 +196,8 @@ def main(argv: Optional[List[str]] = None):
     seeds = [args.seed + i for i in range(args.boards + args.heldout)]
     data = []
     for i, sd in enumerate(seeds):
-        data.append(make_sample(args.size, args.nz, sd, blur=args.blur, on_device=args.features_on_device))
+        data.append(make_sample(args.size, args.nz, sd, blur=args.blur,
+                                on_device=not args.features_on_host and args.size % 8 == 0))
         log(f"routed {i + 1}/{len(seeds)} boards ({data[-1]['iterations']} iterations, "
             f"{data[-1]['seconds']:.1f} s)")
     t_data = time.perf_counter() - t0
