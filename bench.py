@@ -509,6 +509,19 @@ def route_c1(dev, with_cpu: bool):
     ref = route_plain(b.lattice, b.src, b.dst, cfg)
     out_same = [(s_, c_) for s_, c_, _ in ref["trace"]] == rb.overuse_trace() and all(
         np.array_equal(x, y) for x, y in zip(rb.paths, ref["paths"])) and np.array_equal(rb.edge_usage, ref["usage"])
+    # snapshot groups (the config-3 warm run's schedule) from zero history,
+    # against the oracle loop of the same schedule
+    import dataclasses
+
+    cfg_s = dataclasses.replace(cfg, net_order="disjoint", group_nets=C3_GROUP, group_repair=C3_REPAIR)
+    pf.cfg = cfg_s
+    pf.route(b.src, b.dst, mode="batched")  # warm-up of the snapshot workspaces
+    rg = pf.route(b.src, b.dst, mode="batched")
+    pf.cfg = cfg
+    ref_s = route_plain(b.lattice, b.src, b.dst, cfg_s)
+    snap_same = [(s_, c_) for s_, c_, _ in ref_s["trace"]] == rg.overuse_trace() and all(
+        np.array_equal(x, y) for x, y in zip(rg.paths, ref_s["paths"])) and np.array_equal(rg.edge_usage,
+                                                                                         ref_s["usage"])
     out = {
         "workload": "100x100x4 lattice, 200 two-pin nets, per-net live costs, offenders rerouted",
         "identical_to_oracle": bool(out_same and same),
@@ -521,6 +534,13 @@ def route_c1(dev, with_cpu: bool):
         "wirelength": rb.wirelength,
         "vias": rb.vias,
         "overuse_trace": [s.over_sum for s in rb.iterations],
+        "snapshot": {"schedule": f"snapshot groups of {C3_GROUP} nets in the disjoint-round order, {C3_REPAIR} "
+                                 "repair rounds, zero history",
+                     "identical_to_oracle": bool(snap_same), "converged": bool(rg.converged),
+                     "iterations": len(rg.iterations), "sec": round(rg.seconds, 4),
+                     "speedup_vs_plain": round(rs.seconds / rg.seconds, 2),
+                     "wirelength_delta_pct": round(100.0 * (rg.wirelength - rb.wirelength) / max(1, rb.wirelength), 3),
+                     "vias_delta_pct": round(100.0 * (rg.vias - rb.vias) / max(1, rb.vias), 3)},
     }
     if with_cpu:
         out["cpu_oracle_sec"] = round(ref["seconds"], 3)
