@@ -76,3 +76,24 @@ def test_device_feature_assembly_matches_host_on_cpu():
     assert fd.shape == (6, 48, 88, 16) and fd.dtype == torch.bfloat16
     assert torch.equal(fd[:, :45, :83], torch.from_numpy(f).to(torch.bfloat16))
     assert float(fd[:, 45:].abs().sum()) == 0 and float(fd[:, :, 83:].abs().sum()) == 0
+
+
+def test_history_mapping_device_form_on_cpu():
+    """history_from_prediction_device (the torch form bench.py and the warm
+    route use), run on the CPU, equals history_from_prediction to within one
+    float32 ulp (the two expm1 implementations may differ in the last bit),
+    with the same edge order."""
+    import torch
+
+    from orthoroute_b200.warm import history_from_prediction_device
+
+    b = board_footprints(64, 64, 6, 30, None, seed=7)
+    lat = b.lattice
+    rng = np.random.default_rng(3)
+    pred = (rng.standard_normal((lat.nz, lat.ny, lat.nx, 2)) * 0.7).astype(np.float32)
+    host = history_from_prediction(lat, pred, 4.0)
+    dev = history_from_prediction_device(lat, torch.from_numpy(pred), 4.0).numpy()
+    assert dev.dtype == np.float32 and dev.shape == host.shape
+    ulp = np.abs(dev.view(np.int32).astype(np.int64) - host.view(np.int32).astype(np.int64))
+    assert int(ulp.max()) <= 1
+    assert (host[np.all(pred.reshape(-1, 2)[lat.edge_src()] <= 0, axis=1)] == 0).all()
